@@ -1,0 +1,193 @@
+/*
+ * mcs.h -- C ABI of mcstreamer-b200, the B200 (sm_100a) implementation of JuMC's electron
+ * step (aluque/mcstreamer).  Plain pointers and sizes only; every entry point returns an
+ * int status (MCS_OK == 0) and mcs_last_error(ctx) gives the message of the last failure.
+ *
+ * The reference has no FFI: its "plugin API" is Julia multiple dispatch.  Each entry point
+ * below names the reference function it replaces (file:line inside the reference project);
+ * a Julia caller binds them with ccall (binding stubs are listed in INTEGRATION.md).
+ *
+ * Host buffer layouts equal the Julia memory layouts so Julia arrays pass without copies:
+ *   x, v   : 3 doubles per particle, interleaved   (Vector{SVector{3,Float64}})
+ *   w, s   : 1 double per particle                 (Vector{Float64})
+ *   active : 1 byte per particle (0/1)             (Vector{Bool})
+ *   rate   : neps columns of nrows doubles, process index fastest
+ *            (CollisionTable.rate, Matrix{Float64} of size (nrows, neps))
+ *
+ * Work is queued on the context's CUDA stream; calls that return data to the host
+ * (download, read, nparticles, moments, mcs_sync) synchronise and report the sticky
+ * device status (capacity, energy range, field magnitude, overflow, timeout) raised by
+ * earlier queued kernels.  A context is not thread-safe (the reference's advance! is
+ * likewise called from one task).
+ */
+#ifndef MCS_H
+#define MCS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCS_API __attribute__((visibility("default")))
+
+/* ---- status codes ---- */
+enum {
+    MCS_OK = 0,
+    MCS_ERR_ARG = 1,            /* invalid argument */
+    MCS_ERR_CUDA = 2,           /* CUDA runtime error */
+    MCS_ERR_CAPACITY = 3,       /* "Maximum number of particles reached" (population.jl:90) */
+    MCS_ERR_ENERGY_RANGE = 4,   /* energy beyond the table (util.jl:28 @assert 0 <= w <= 1) */
+    MCS_ERR_FIELD_TOO_HIGH = 5, /* |E| > 1e8 V/m (gridfields.jl:179-187) */
+    MCS_ERR_NONFINITE = 6,      /* NaN / Inf in particle state */
+    MCS_ERR_UNSUPPORTED = 7,    /* combination not implemented (e.g. user-defined process) */
+    MCS_ERR_OVERFLOW = 8,       /* a tile produced more secondaries than its staging holds */
+    MCS_ERR_NOMEM = 9,          /* device allocation failed */
+    MCS_ERR_TIMEOUT = 10        /* a bounded device-side wait gave up */
+};
+
+/* ---- collision process kinds (JuMC/src/electron.jl:70-84, collisions.jl:3) ---- */
+enum {
+    MCS_NULL = 0,
+    MCS_ELASTIC = 1,             /* param = mass_ratio                           */
+    MCS_EXCITATION = 2,          /* param = threshold (J)                         */
+    MCS_IONIZATION = 3,          /* param = threshold (J), equal energy sharing   */
+    MCS_ATTACHMENT = 4,          /* param = threshold (J), unused                 */
+    MCS_IONIZATION_UNIFORM = 5   /* param = threshold (J), secondary energy uniform on
+                                    [0, eps - threshold]; no counterpart in JuMC */
+};
+
+enum { MCS_FP64 = 0, MCS_FP32 = 1 };
+
+/* context flags */
+enum { MCS_FLAG_CLAMP_ENERGY = 1 }; /* energies beyond the table use the last column
+                                       instead of raising MCS_ERR_ENERGY_RANGE */
+
+/* charge arrays of a grid */
+enum { MCS_Q_FIXED = 0, /* tracker deposits: CollisionTracker -> fields.qfixed */
+       MCS_Q_PART = 1   /* particle deposits: density! -> fields.qpart */ };
+
+/* layout of the moments vector filled by mcs_moments (length MCS_MOMENTS_BASE + nrows) */
+enum {
+    MCS_M_COUNT = 0,   /* number of active particles */
+    MCS_M_W = 1,       /* sum w                         (population.jl:114-124 weight) */
+    MCS_M_X = 2,       /* sum x, y, z (2..4)            (Swarm.jl:126)              */
+    MCS_M_X2 = 5,      /* sum x^2, y^2, z^2 (5..7)      (Swarm.jl:127)              */
+    MCS_M_V = 8,       /* sum vx, vy, vz (8..10)        (Swarm.jl:152)              */
+    MCS_M_E = 11,      /* sum energy                                               */
+    MCS_M_WE = 12,     /* sum w*energy                  (population.jl:136-150)     */
+    MCS_M_EMAX = 13,   /* max energy over ALL particles (population.jl:156-158)     */
+    MCS_M_WX = 14,     /* sum w*x, w*y, w*z (14..16)    (population.jl:164-183)     */
+    MCS_M_WX2 = 17,    /* sum w*|x|^2                                              */
+    MCS_MOMENTS_BASE = 18 /* then sum of rate_j(energy) per table row (Swarm.jl:242-248) */
+};
+
+typedef struct mcs_ctx mcs_ctx;
+typedef struct mcs_table mcs_table;
+typedef struct mcs_grid mcs_grid;
+typedef struct mcs_field mcs_field;
+typedef struct mcs_pop mcs_pop;
+
+/* ---- context ---- */
+MCS_API int mcs_version(void);
+/* Creates a context on `device` with its own CUDA stream. */
+MCS_API int mcs_ctx_create(int device, mcs_ctx** out);
+MCS_API int mcs_ctx_destroy(mcs_ctx* ctx);
+MCS_API const char* mcs_last_error(const mcs_ctx* ctx);
+/* Use an external CUDA stream (cudaStream_t) instead of the context's own. */
+MCS_API int mcs_ctx_set_stream(mcs_ctx* ctx, void* stream);
+MCS_API void* mcs_ctx_stream(mcs_ctx* ctx);
+MCS_API int mcs_ctx_set_flags(mcs_ctx* ctx, uint32_t flags);
+/* Waits for queued work; returns (and clears) the sticky device status. */
+MCS_API int mcs_sync(mcs_ctx* ctx);
+
+/* ---- collision table: CollisionTable (JuMC/src/collisions.jl:9-22) as built by
+ *      load_lxcat (JuMC/src/lxcat.jl:17-134).  Energy grid LinRange(e0, emax, neps). ---- */
+MCS_API int mcs_table_create(mcs_ctx* ctx, int nrows, int neps, double e0, double emax,
+                             const double* rate, const int* kind, const double* param,
+                             double maxrate, mcs_table** out);
+MCS_API int mcs_table_destroy(mcs_table* t);
+
+/* ---- grids ---- */
+/* 3-D uniform mesh of nx*ny*nz cubic cells of side h, lower corner (x0,y0,z0).  Node
+ * field E: 3 values per node, (nx+1)(ny+1)(nz+1) nodes, x fastest.  Charge: int64 per
+ * node at 2^-32 elementary charges (cloud-in-cell).  `precision` selects the device copy
+ * of the node field (MCS_FP32 / MCS_FP64). */
+MCS_API int mcs_grid_create_cart3d(mcs_ctx* ctx, int nx, int ny, int nz, double h, double x0,
+                                   double y0, double z0, int precision, mcs_grid** out);
+/* Cylindrical Grid(R, L, M, N) (MCStreamer/src/grid.jl:4-42).  Face fields er, ez of
+ * (M+3)x(N+3) doubles indexed i + j*(M+3) (calloc_faces, grid.jl:71-72).  Charge arrays
+ * are cell densities (M+2)x(N+2), index i + j*(M+2) (calloc_centers, grid.jl:55-57). */
+MCS_API int mcs_grid_create_cyl(mcs_ctx* ctx, double R, double L, int M, int N, mcs_grid** out);
+MCS_API int mcs_grid_destroy(mcs_grid* g);
+/* cart3d: 3 doubles per node.  cyl: er followed by ez. */
+MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e);
+MCS_API int mcs_grid_zero(mcs_grid* g, int which);
+/* cart3d: int64 per node (2^-32 e).  Not available for cyl grids. */
+MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out);
+/* cyl: density per cell (weight/dV, poisson.jl:79-81).  cart3d: charge per node in e. */
+MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out);
+
+/* ---- fields: the `efield` callable of advance! ---- */
+/* FixedField (Swarm/src/Swarm.jl:28-32), generalised to any constant vector. */
+MCS_API int mcs_field_uniform(mcs_ctx* ctx, double ex, double ey, double ez, mcs_field** out);
+/* FieldInterp (MCStreamer/src/gridfields.jl:89-190) over a grid's stored field. */
+MCS_API int mcs_field_from_grid(mcs_grid* g, mcs_field** out);
+MCS_API int mcs_field_destroy(mcs_field* f);
+
+/* ---- population: Population (JuMC/src/population.jl:4-36, 26-36) ---- */
+/* `cells` = a cart3d grid stores positions as (cell index, in-cell offset) on that mesh;
+ * NULL stores absolute positions. */
+MCS_API int mcs_pop_create(mcs_ctx* ctx, int64_t capacity, int precision, mcs_grid* cells,
+                           mcs_pop** out);
+MCS_API int mcs_pop_destroy(mcs_pop* p);
+/* Philox key and step counter (uniform #k of slot i at step t = Philox(seed; i, t, k/4, tag)). */
+MCS_API int mcs_pop_set_seed(mcs_pop* p, uint64_t seed, uint32_t step);
+MCS_API int mcs_pop_get_step(mcs_pop* p, uint32_t* step);
+MCS_API int mcs_pop_upload(mcs_pop* p, const double* x, const double* v, const double* w,
+                           const double* s, const uint8_t* active, int64_t n);
+MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double* s,
+                             uint8_t* active, int64_t cap, int64_t* n);
+/* nparticles (population.jl:106): particles in use, active or not. */
+MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n);
+
+/* ---- the electron step ---- */
+/* advance!(mpopl, efield, dt, tracker) (JuMC/src/mixed_population.jl:24-54) with
+ * do_one_collision! (collisions.jl:159-192), collide (electron.jl:108-139), apply!
+ * (collisions.jl:96-123) and, when tracker != NULL, CollisionTracker (gridfields.jl:
+ * 198-224) depositing +w per ionization and -w per attachment into MCS_Q_FIXED. */
+MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt,
+                        mcs_grid* tracker);
+/* collisions!(mpopl, dt, tracker) (JuMC/src/mixed_population.jl:61-77). */
+MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* tracker);
+/* density!(grid, arr, mpopl, Electron, fields, val) (MCStreamer/src/poisson.jl:65-84)
+ * into MCS_Q_PART (accumulates; zero it with mcs_grid_zero). */
+MCS_API int mcs_deposit(mcs_pop* p, mcs_grid* g, double val);
+/* repack! (JuMC/src/population.jl:191-215), same permutation. */
+MCS_API int mcs_repack(mcs_pop* p);
+/* Swarm.resample!(popl, n0, tol) (Swarm/src/Swarm.jl:193-223). */
+MCS_API int mcs_swarm_resample(mcs_pop* p, int64_t n0, double tol);
+/* Stable sort of the population by cell key of grid g (out-of-grid particles last). */
+MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid* g);
+/* resample!(popl, fields, ntarget, nmax) (MCStreamer/src/resample.jl:7-77). */
+MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax);
+/* Moments over the population (layout MCS_M_*), table may be NULL (no rate sums). */
+MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout);
+
+/* Per-step moments of the fused swarm loop (MCS_STEP_MOMENTS doubles per step). */
+enum {
+    MCS_S_COUNT = 0, MCS_S_W = 1, MCS_S_X = 2 /* 2..4 */, MCS_S_X2 = 5 /* 5..7 */,
+    MCS_S_V = 8 /* 8..10 */, MCS_S_E = 11, MCS_STEP_MOMENTS = 12
+};
+/* The time loop of Swarm.swarm (Swarm/src/Swarm.jl:124-142) on the device: per step
+ * advance! with the per-step sums of Swarm.jl:126-127 fused into the step kernel, then
+ * (n0 > 0) Swarm.resample!(popl, n0, tol).  moments_out (host, may be NULL) receives
+ * nsteps*MCS_STEP_MOMENTS doubles; they stay on the device until the loop ends. */
+MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, int nsteps,
+                          int64_t n0, double tol, double* moments_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCS_H */

@@ -1,0 +1,132 @@
+"""ctypes binding of libmcs_b200.so (the C ABI declared in include/mcs.h).
+
+This is the same binding a Julia caller writes with ccall; the Python classes in
+jumc.py / swarm.py / streamer.py sit on top of it.  Loading fails loudly: there is no
+CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libmcs_b200.so"
+
+# status codes (include/mcs.h)
+OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_ENERGY_RANGE, ERR_FIELD_TOO_HIGH = 0, 1, 2, 3, 4, 5
+ERR_NONFINITE, ERR_UNSUPPORTED, ERR_OVERFLOW, ERR_NOMEM, ERR_TIMEOUT = 6, 7, 8, 9, 10
+STATUS_NAMES = {
+    0: "MCS_OK", 1: "MCS_ERR_ARG", 2: "MCS_ERR_CUDA", 3: "MCS_ERR_CAPACITY", 4: "MCS_ERR_ENERGY_RANGE",
+    5: "MCS_ERR_FIELD_TOO_HIGH", 6: "MCS_ERR_NONFINITE", 7: "MCS_ERR_UNSUPPORTED", 8: "MCS_ERR_OVERFLOW",
+    9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT",
+}
+# process kinds
+NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM = 0, 1, 2, 3, 4, 5
+FP64, FP32 = 0, 1
+FLAG_CLAMP_ENERGY = 1
+Q_FIXED, Q_PART = 0, 1
+MOMENTS_BASE = 18
+M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
+S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
+
+vp = C.c_void_p
+i32, i64, u32, u64, f64 = C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
+pd = C.POINTER(C.c_double)
+pi64 = C.POINTER(C.c_int64)
+pu8 = C.POINTER(C.c_uint8)
+pi32 = C.POINTER(C.c_int)
+ph = C.POINTER(C.c_void_p)
+
+SIGNATURES = {
+    "mcs_version": (i32, []),
+    "mcs_ctx_create": (i32, [i32, ph]),
+    "mcs_ctx_destroy": (i32, [vp]),
+    "mcs_last_error": (C.c_char_p, [vp]),
+    "mcs_ctx_set_stream": (i32, [vp, vp]),
+    "mcs_ctx_stream": (vp, [vp]),
+    "mcs_ctx_set_flags": (i32, [vp, u32]),
+    "mcs_sync": (i32, [vp]),
+    "mcs_table_create": (i32, [vp, i32, i32, f64, f64, pd, pi32, pd, f64, ph]),
+    "mcs_table_destroy": (i32, [vp]),
+    "mcs_grid_create_cart3d": (i32, [vp, i32, i32, i32, f64, f64, f64, f64, i32, ph]),
+    "mcs_grid_create_cyl": (i32, [vp, f64, f64, i32, i32, ph]),
+    "mcs_grid_destroy": (i32, [vp]),
+    "mcs_grid_set_efield": (i32, [vp, pd]),
+    "mcs_grid_zero": (i32, [vp, i32]),
+    "mcs_grid_read_fixed": (i32, [vp, i32, pi64]),
+    "mcs_grid_read_density": (i32, [vp, i32, pd]),
+    "mcs_field_uniform": (i32, [vp, f64, f64, f64, ph]),
+    "mcs_field_from_grid": (i32, [vp, ph]),
+    "mcs_field_destroy": (i32, [vp]),
+    "mcs_pop_create": (i32, [vp, i64, i32, vp, ph]),
+    "mcs_pop_destroy": (i32, [vp]),
+    "mcs_pop_set_seed": (i32, [vp, u64, u32]),
+    "mcs_pop_get_step": (i32, [vp, C.POINTER(C.c_uint32)]),
+    "mcs_pop_upload": (i32, [vp, pd, pd, pd, pd, pu8, i64]),
+    "mcs_pop_download": (i32, [vp, pd, pd, pd, pd, pu8, i64, pi64]),
+    "mcs_pop_nparticles": (i32, [vp, pi64]),
+    "mcs_advance": (i32, [vp, vp, vp, f64, vp]),
+    "mcs_collisions": (i32, [vp, vp, f64, vp]),
+    "mcs_deposit": (i32, [vp, vp, f64]),
+    "mcs_repack": (i32, [vp]),
+    "mcs_swarm_resample": (i32, [vp, i64, f64]),
+    "mcs_sort_cells": (i32, [vp, vp]),
+    "mcs_resample_cells": (i32, [vp, vp, i32, i32]),
+    "mcs_moments": (i32, [vp, vp, pd, i32]),
+    "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, pd]),
+}
+
+_lib = None
+
+
+class MCSError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """Load libmcs_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m mcstreamer_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int, ctx=None) -> None:
+    if code != OK:
+        msg = ""
+        if ctx is not None:
+            raw = lib().mcs_last_error(ctx)
+            msg = raw.decode() if raw else ""
+        raise MCSError(code, msg)
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(pd)
+
+
+def u8ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags.c_contiguous
+    return a.ctypes.data_as(pu8)
+
+
+def i64ptr(a: np.ndarray):
+    assert a.dtype == np.int64 and a.flags.c_contiguous
+    return a.ctypes.data_as(pi64)
+
+
+def i32ptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(pi32)

@@ -1,0 +1,594 @@
+// api.cu -- the extern "C" entry points declared in include/mcs.h.
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "host_util.h"
+#include "pop_ops.h"
+#include "step.cuh"
+
+using namespace mcs;
+
+namespace {
+
+int map_status(uint32_t st) {
+    if (st & ST_TIMEOUT) return MCS_ERR_TIMEOUT;
+    if (st & ST_CAPACITY) return MCS_ERR_CAPACITY;
+    if (st & ST_OVERFLOW) return MCS_ERR_OVERFLOW;
+    if (st & ST_ENERGY) return MCS_ERR_ENERGY_RANGE;
+    if (st & ST_FIELD) return MCS_ERR_FIELD_TOO_HIGH;
+    if (st & ST_NONFINITE) return MCS_ERR_NONFINITE;
+    return MCS_OK;
+}
+
+const char* status_text(int code) {
+    switch (code) {
+    case MCS_ERR_TIMEOUT: return "a bounded device-side wait gave up";
+    case MCS_ERR_CAPACITY: return "Maximum number of particles reached";
+    case MCS_ERR_OVERFLOW: return "a tile produced more secondaries than its staging holds";
+    case MCS_ERR_ENERGY_RANGE: return "particle energy outside the collision table";
+    case MCS_ERR_FIELD_TOO_HIGH: return "Too high electric field";
+    case MCS_ERR_NONFINITE: return "non-finite particle state";
+    default: return "";
+    }
+}
+
+int use_device(mcs_ctx* c) {
+    MCS_CK(c, cudaSetDevice(c->device));
+    return MCS_OK;
+}
+
+template <typename T>
+int dalloc(mcs_ctx* c, T** p, size_t count) {
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), count * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_err(c, MCS_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return MCS_OK;
+}
+
+int sync_status(mcs_ctx* c) {
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    uint32_t st = 0;
+    MCS_CK(c, cudaMemcpy(&st, c->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st) {
+        MCS_CK(c, cudaMemset(c->d_status, 0, sizeof(uint32_t)));
+        const int code = map_status(st);
+        return set_err(c, code, status_text(code));
+    }
+    return MCS_OK;
+}
+
+int ensure_staging(mcs_pop* p, size_t bytes) {
+    if (p->staging_bytes >= bytes) return MCS_OK;
+    if (p->staging) cudaFree(p->staging);
+    p->staging = nullptr;
+    p->staging_bytes = 0;
+    void* s = nullptr;
+    int st = dalloc(p->ctx, reinterpret_cast<char**>(&s), bytes);
+    if (st) return st;
+    p->staging = s;
+    p->staging_bytes = bytes;
+    return MCS_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" {
+
+MCS_API int mcs_version(void) { return 1; }
+
+MCS_API int mcs_ctx_create(int device, mcs_ctx** out) {
+    if (!out) return MCS_ERR_ARG;
+    *out = nullptr;
+    mcs_ctx* c = new (std::nothrow) mcs_ctx();
+    if (!c) return MCS_ERR_NOMEM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return MCS_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return MCS_ERR_CUDA; }
+    c->own_stream = true;
+    if (cudaMalloc(&c->d_status, sizeof(uint32_t)) != cudaSuccess) { cudaStreamDestroy(c->stream); delete c; return MCS_ERR_NOMEM; }
+    cudaMemset(c->d_status, 0, sizeof(uint32_t));
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaDeviceSynchronize() != cudaSuccess) { cudaFree(c->d_status); cudaStreamDestroy(c->stream); delete c; return MCS_ERR_CUDA; }
+    *out = c;
+    return MCS_OK;
+}
+
+MCS_API int mcs_ctx_destroy(mcs_ctx* c) {
+    if (!c) return MCS_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_status);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MCS_OK;
+}
+
+MCS_API const char* mcs_last_error(const mcs_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+MCS_API int mcs_ctx_set_stream(mcs_ctx* c, void* stream) {
+    if (!c) return MCS_ERR_ARG;
+    if (c->own_stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+    c->stream = static_cast<cudaStream_t>(stream);
+    c->own_stream = false;
+    return MCS_OK;
+}
+
+MCS_API void* mcs_ctx_stream(mcs_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+MCS_API int mcs_ctx_set_flags(mcs_ctx* c, uint32_t flags) {
+    if (!c) return MCS_ERR_ARG;
+    c->flags = flags;
+    return MCS_OK;
+}
+
+MCS_API int mcs_sync(mcs_ctx* c) {
+    if (!c) return MCS_ERR_ARG;
+    if (int st = use_device(c)) return st;
+    return sync_status(c);
+}
+
+// ---------------------------------------------------------------------------------------
+MCS_API int mcs_table_create(mcs_ctx* c, int nrows, int neps, double e0, double emax, const double* rate,
+                             const int* kind, const double* param, double maxrate, mcs_table** out) {
+    if (!c || !out || !rate || !kind || !param) return MCS_ERR_ARG;
+    *out = nullptr;
+    if (nrows < 1 || nrows > kMaxRows) return set_err(c, MCS_ERR_ARG, "nrows must be in [1, 32]");
+    if (neps < 2 || !(emax > e0) || !(maxrate > 0)) return set_err(c, MCS_ERR_ARG, "bad energy grid or maxrate");
+    for (int j = 0; j < nrows; ++j)
+        if (kind[j] < MCS_NULL || kind[j] > MCS_IONIZATION_UNIFORM)
+            return set_err(c, MCS_ERR_UNSUPPORTED, "unsupported collision process kind");
+    if (int st = use_device(c)) return st;
+    mcs_table* t = new (std::nothrow) mcs_table();
+    if (!t) return MCS_ERR_NOMEM;
+    t->ctx = c;
+    TableView& v = t->v;
+    v.nrows = nrows;
+    v.nrp = (nrows + 3) & ~3;
+    v.neps = neps;
+    v.e0 = e0;
+    v.emax = emax;
+    v.step = (emax - e0) / (double)(neps - 1);
+    v.maxrate = maxrate;
+    v.inv_maxrate = 1.0 / maxrate;
+    v.ke32 = (float)(0.5 * kElectronMass / v.step);
+    v.e0n32 = (float)(e0 / v.step);
+    v.maxrate32 = (float)maxrate;
+    for (int j = 0; j < kMaxRows; ++j) {
+        v.kind[j] = j < nrows ? kind[j] : MCS_NULL;
+        v.param[j] = j < nrows ? param[j] : 0.0;
+    }
+    const size_t n64 = (size_t)neps * nrows, n32 = (size_t)neps * v.nrp;
+    int st = dalloc(c, &t->d_rate64, n64);
+    if (!st) st = dalloc(c, &t->d_rate32, n32);
+    if (st) { cudaFree(t->d_rate64); delete t; return st; }
+    std::vector<float> r32(n32, 0.0f);
+    for (int k = 0; k < neps; ++k)
+        for (int j = 0; j < nrows; ++j) r32[(size_t)k * v.nrp + j] = (float)rate[(size_t)k * nrows + j];
+    cudaError_t e1 = cudaMemcpy(t->d_rate64, rate, n64 * sizeof(double), cudaMemcpyHostToDevice);
+    cudaError_t e2 = cudaMemcpy(t->d_rate32, r32.data(), n32 * sizeof(float), cudaMemcpyHostToDevice);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+        cudaFree(t->d_rate64); cudaFree(t->d_rate32); delete t;
+        return set_err(c, MCS_ERR_CUDA, "table upload failed");
+    }
+    v.rate64 = t->d_rate64;
+    v.rate32 = t->d_rate32;
+    *out = t;
+    return MCS_OK;
+}
+
+MCS_API int mcs_table_destroy(mcs_table* t) {
+    if (!t) return MCS_OK;
+    cudaSetDevice(t->ctx->device);
+    cudaStreamSynchronize(t->ctx->stream);
+    cudaFree(t->d_rate64);
+    cudaFree(t->d_rate32);
+    delete t;
+    return MCS_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+MCS_API int mcs_grid_create_cart3d(mcs_ctx* c, int nx, int ny, int nz, double h, double x0, double y0, double z0,
+                                   int precision, mcs_grid** out) {
+    if (!c || !out) return MCS_ERR_ARG;
+    *out = nullptr;
+    if (nx < 1 || ny < 1 || nz < 1 || !(h > 0)) return set_err(c, MCS_ERR_ARG, "bad mesh");
+    if ((double)nx * ny * nz >= 4294967295.0) return set_err(c, MCS_ERR_ARG, "mesh has too many cells");
+    if (precision != MCS_FP32 && precision != MCS_FP64) return set_err(c, MCS_ERR_ARG, "bad precision");
+    if (int st = use_device(c)) return st;
+    mcs_grid* g = new (std::nothrow) mcs_grid();
+    if (!g) return MCS_ERR_NOMEM;
+    g->ctx = c;
+    g->precision = precision;
+    GridView& v = g->v;
+    v.type = GRID_CART3D;
+    v.nx = nx; v.ny = ny; v.nz = nz;
+    v.h = h; v.inv_h = 1.0 / h; v.x0 = x0; v.y0 = y0; v.z0 = z0;
+    const size_t nodes = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+    g->nq = nodes;
+    int st = MCS_OK;
+    if (precision == MCS_FP32) st = dalloc(c, &g->d_e32, 4 * nodes);
+    else st = dalloc(c, &g->d_e64, 3 * nodes);
+    if (!st) st = dalloc(c, &g->d_q[0], nodes);
+    if (!st) st = dalloc(c, &g->d_q[1], nodes);
+    if (st) { cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_q[0]); delete g; return st; }
+    if (g->d_e32) cudaMemset(g->d_e32, 0, 4 * nodes * sizeof(float));
+    if (g->d_e64) cudaMemset(g->d_e64, 0, 3 * nodes * sizeof(double));
+    cudaMemset(g->d_q[0], 0, nodes * sizeof(long long));
+    cudaMemset(g->d_q[1], 0, nodes * sizeof(long long));
+    v.e32 = g->d_e32;
+    v.e64 = g->d_e64;
+    v.qfixed = g->d_q[0];
+    v.qpart = g->d_q[1];
+    *out = g;
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_create_cyl(mcs_ctx* c, double R, double L, int M, int N, mcs_grid** out) {
+    if (!c || !out) return MCS_ERR_ARG;
+    *out = nullptr;
+    if (M < 1 || N < 1 || !(R > 0) || !(L > 0)) return set_err(c, MCS_ERR_ARG, "bad cylindrical grid");
+    if (int st = use_device(c)) return st;
+    mcs_grid* g = new (std::nothrow) mcs_grid();
+    if (!g) return MCS_ERR_NOMEM;
+    g->ctx = c;
+    g->precision = MCS_FP64;
+    GridView& v = g->v;
+    v.type = GRID_CYL;
+    v.R = R; v.L = L; v.M = M; v.N = N;
+    v.dr = R / M;
+    v.dz = L / N;
+    const size_t faces = (size_t)(M + 3) * (N + 3), cells = (size_t)(M + 2) * (N + 2);
+    g->nq = cells;
+    int st = dalloc(c, &g->d_er, faces);
+    if (!st) st = dalloc(c, &g->d_ez, faces);
+    if (!st) st = dalloc(c, &g->d_q[0], cells);
+    if (!st) st = dalloc(c, &g->d_q[1], cells);
+    if (st) { cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_q[0]); delete g; return st; }
+    cudaMemset(g->d_er, 0, faces * sizeof(double));
+    cudaMemset(g->d_ez, 0, faces * sizeof(double));
+    cudaMemset(g->d_q[0], 0, cells * sizeof(long long));
+    cudaMemset(g->d_q[1], 0, cells * sizeof(long long));
+    v.er = g->d_er;
+    v.ez = g->d_ez;
+    v.qfixed = g->d_q[0];
+    v.qpart = g->d_q[1];
+    *out = g;
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_destroy(mcs_grid* g) {
+    if (!g) return MCS_OK;
+    cudaSetDevice(g->ctx->device);
+    cudaStreamSynchronize(g->ctx->stream);
+    cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_er); cudaFree(g->d_ez);
+    cudaFree(g->d_q[0]); cudaFree(g->d_q[1]);
+    delete g;
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e) {
+    if (!g || !e) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    if (g->v.type == GRID_CART3D) {
+        const size_t nodes = g->nq;
+        if (g->d_e32) {
+            std::vector<float> tmp(4 * nodes);
+            for (size_t i = 0; i < nodes; ++i) {
+                tmp[4 * i] = (float)e[3 * i];
+                tmp[4 * i + 1] = (float)e[3 * i + 1];
+                tmp[4 * i + 2] = (float)e[3 * i + 2];
+                tmp[4 * i + 3] = 0.0f;
+            }
+            MCS_CK(c, cudaMemcpy(g->d_e32, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
+        } else {
+            MCS_CK(c, cudaMemcpy(g->d_e64, e, 3 * nodes * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    } else {
+        const size_t faces = (size_t)(g->v.M + 3) * (g->v.N + 3);
+        MCS_CK(c, cudaMemcpy(g->d_er, e, faces * sizeof(double), cudaMemcpyHostToDevice));
+        MCS_CK(c, cudaMemcpy(g->d_ez, e + faces, faces * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_zero(mcs_grid* g, int which) {
+    if (!g || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaMemsetAsync(g->d_q[which], 0, g->nq * sizeof(long long), c->stream));
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out) {
+    if (!g || !out || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (int st = use_device(c)) return st;
+    const int st = sync_status(c);
+    MCS_CK(c, cudaMemcpy(out, g->d_q[which], g->nq * sizeof(long long), cudaMemcpyDeviceToHost));
+    return st;
+}
+
+MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out) {
+    if (!g || !out || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    std::vector<long long> q(g->nq);
+    const int st = mcs_grid_read_fixed(g, which, reinterpret_cast<int64_t*>(q.data()));
+    if (st == MCS_ERR_CUDA || st == MCS_ERR_ARG) return st;
+    if (g->v.type == GRID_CART3D) {
+        for (size_t i = 0; i < g->nq; ++i) out[i] = (double)q[i] * 0x1p-32;
+    } else {
+        const int M = g->v.M, N = g->v.N;
+        for (int j = 0; j < N + 2; ++j)
+            for (int i = 0; i < M + 2; ++i) {
+                const size_t k = (size_t)i + (size_t)j * (M + 2);
+                if (i < 1 || i > M) { out[k] = 0.0; continue; }
+                const double rc = ((double)(i - 1) + 0.5) * g->v.dr;  // grid.rc[i]
+                const double dV = 2.0 * M_PI * rc * g->v.dr * g->v.dz;  // grid.jl:76
+                out[k] = (double)q[k] * 0x1p-32 / dV;
+            }
+    }
+    return st;
+}
+
+// ---------------------------------------------------------------------------------------
+MCS_API int mcs_field_uniform(mcs_ctx* c, double ex, double ey, double ez, mcs_field** out) {
+    if (!c || !out) return MCS_ERR_ARG;
+    mcs_field* f = new (std::nothrow) mcs_field();
+    if (!f) return MCS_ERR_NOMEM;
+    f->ctx = c;
+    f->type = FIELD_UNIFORM;
+    f->e[0] = ex; f->e[1] = ey; f->e[2] = ez;
+    *out = f;
+    return MCS_OK;
+}
+
+MCS_API int mcs_field_from_grid(mcs_grid* g, mcs_field** out) {
+    if (!g || !out) return MCS_ERR_ARG;
+    mcs_field* f = new (std::nothrow) mcs_field();
+    if (!f) return MCS_ERR_NOMEM;
+    f->ctx = g->ctx;
+    f->type = FIELD_GRID;
+    f->grid = g;
+    *out = f;
+    return MCS_OK;
+}
+
+MCS_API int mcs_field_destroy(mcs_field* f) {
+    delete f;
+    return MCS_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+MCS_API int mcs_pop_create(mcs_ctx* c, int64_t capacity, int precision, mcs_grid* cells, mcs_pop** out) {
+    if (!c || !out) return MCS_ERR_ARG;
+    *out = nullptr;
+    if (capacity < 1 || capacity > 0xfffffff0LL) return set_err(c, MCS_ERR_ARG, "capacity must be in [1, 2^32-16]");
+    if (precision != MCS_FP32 && precision != MCS_FP64) return set_err(c, MCS_ERR_ARG, "bad precision");
+    if (cells && cells->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "cell layout needs a cart3d grid");
+    if (int st = use_device(c)) return st;
+    mcs_pop* p = new (std::nothrow) mcs_pop();
+    if (!p) return MCS_ERR_NOMEM;
+    p->ctx = c;
+    p->precision = precision;
+    p->cells = cells;
+    p->cap = capacity;
+    p->esz = precision == MCS_FP32 ? 4 : 8;
+    int st = MCS_OK;
+    for (int q = 0; q < 8 && !st; ++q) st = dalloc(c, reinterpret_cast<char**>(&p->f[q]), (size_t)capacity * p->esz);
+    if (!st) st = dalloc(c, &p->act, (size_t)capacity);
+    if (!st && cells) st = dalloc(c, &p->cell, (size_t)capacity);
+    if (!st) st = dalloc(c, &p->d_n, 2);
+    p->max_tiles = (capacity + 127) / 128 + 1;
+    if (!st) st = dalloc(c, &p->tile_status, (size_t)p->max_tiles);
+    size_t npart = (size_t)p->max_tiles * kStepMoments;
+    if (npart < (size_t)kMomentPartialsMin) npart = kMomentPartialsMin;
+    if (!st) st = dalloc(c, &p->tile_partials, npart);
+    if (!st) st = dalloc(c, &p->counters, 16);
+    if (!st) st = dalloc(c, &p->d_moments, MCS_MOMENTS_BASE + kMaxRows);
+    if (!st) st = dalloc(c, &p->u32a, (size_t)capacity);
+    if (!st) st = dalloc(c, &p->u32b, (size_t)capacity);
+    if (st) { mcs_pop_destroy(p); return st; }
+    cudaMemset(p->d_n, 0, 2 * sizeof(long long));
+    cudaMemset(p->tile_status, 0, (size_t)p->max_tiles * sizeof(unsigned long long));
+    cudaMemset(p->counters, 0, 16 * sizeof(uint32_t));
+    cudaMemset(p->act, 0, (size_t)capacity);
+    if (cudaDeviceSynchronize() != cudaSuccess) { mcs_pop_destroy(p); return set_err(c, MCS_ERR_CUDA, "pop init"); }
+    *out = p;
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_destroy(mcs_pop* p) {
+    if (!p) return MCS_OK;
+    cudaSetDevice(p->ctx->device);
+    cudaStreamSynchronize(p->ctx->stream);
+    for (int q = 0; q < 8; ++q) { cudaFree(p->f[q]); cudaFree(p->alt[q]); }
+    cudaFree(p->act); cudaFree(p->cell); cudaFree(p->d_n); cudaFree(p->tile_status);
+    cudaFree(p->tile_partials); cudaFree(p->counters); cudaFree(p->d_moments); cudaFree(p->staging);
+    cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act);
+    delete p;
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_set_seed(mcs_pop* p, uint64_t seed, uint32_t step) {
+    if (!p) return MCS_ERR_ARG;
+    p->seed = seed;
+    p->step = step;
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_get_step(mcs_pop* p, uint32_t* step) {
+    if (!p || !step) return MCS_ERR_ARG;
+    *step = p->step;
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_upload(mcs_pop* p, const double* x, const double* v, const double* w, const double* s,
+                           const uint8_t* active, int64_t n) {
+    if (!p || n < 0 || (n > 0 && (!x || !v || !w || !s || !active))) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (n > p->cap) return set_err(c, MCS_ERR_CAPACITY, "Maximum number of particles reached");
+    if (int st = use_device(c)) return st;
+    const size_t o_v = align256(3 * n * sizeof(double)), o_w = o_v + align256(3 * n * sizeof(double));
+    const size_t o_s = o_w + align256(n * sizeof(double)), o_a = o_s + align256(n * sizeof(double));
+    const size_t bytes = o_a + align256((size_t)n);
+    if (int st = ensure_staging(p, bytes)) return st;
+    char* b = static_cast<char*>(p->staging);
+    if (n > 0) {
+        MCS_CK(c, cudaMemcpyAsync(b, x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        MCS_CK(c, cudaMemcpyAsync(b + o_v, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        MCS_CK(c, cudaMemcpyAsync(b + o_w, w, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        MCS_CK(c, cudaMemcpyAsync(b + o_s, s, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        MCS_CK(c, cudaMemcpyAsync(b + o_a, active, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+        if (int st = launch_upload(p, reinterpret_cast<double*>(b), reinterpret_cast<double*>(b + o_v),
+                                   reinterpret_cast<double*>(b + o_w), reinterpret_cast<double*>(b + o_s),
+                                   reinterpret_cast<uint8_t*>(b + o_a), n))
+            return st;
+    }
+    const long long nn = n;
+    MCS_CK(c, cudaMemcpyAsync(p->d_n + p->cur, &nn, sizeof(nn), cudaMemcpyHostToDevice, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));  // nn and the host buffers are caller-owned
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n) {
+    if (!p || !n) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (int st = use_device(c)) return st;
+    long long v = 0;
+    MCS_CK(c, cudaMemcpyAsync(&v, p->d_n + p->cur, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+    const int st = sync_status(c);
+    *n = v;
+    return st;
+}
+
+MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double* s, uint8_t* active, int64_t cap,
+                             int64_t* n_out) {
+    if (!p || !n_out) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    int64_t n = 0;
+    int st = mcs_pop_nparticles(p, &n);
+    if (st == MCS_ERR_CUDA) return st;
+    *n_out = n;
+    if (n > cap) return set_err(c, MCS_ERR_ARG, "host buffers too small");
+    if (n == 0) return st;
+    if (!x || !v || !w || !s || !active) return MCS_ERR_ARG;
+    const size_t o_v = align256(3 * n * sizeof(double)), o_w = o_v + align256(3 * n * sizeof(double));
+    const size_t o_s = o_w + align256(n * sizeof(double)), o_a = o_s + align256(n * sizeof(double));
+    const size_t bytes = o_a + align256((size_t)n);
+    if (int e = ensure_staging(p, bytes)) return e;
+    char* b = static_cast<char*>(p->staging);
+    if (int e = launch_download(p, reinterpret_cast<double*>(b), reinterpret_cast<double*>(b + o_v),
+                                reinterpret_cast<double*>(b + o_w), reinterpret_cast<double*>(b + o_s),
+                                reinterpret_cast<uint8_t*>(b + o_a)))
+        return e;
+    MCS_CK(c, cudaMemcpyAsync(x, b, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(v, b + o_v, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(w, b + o_w, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(s, b + o_s, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(active, b + o_a, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    return st;
+}
+
+// ---------------------------------------------------------------------------------------
+MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* tracker) {
+    if (!p || !t || !f) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (!(dt >= 0)) return set_err(c, MCS_ERR_ARG, "dt must be >= 0");
+    if (f->type == FIELD_GRID && !f->grid) return MCS_ERR_ARG;
+    if (int st = use_device(c)) return st;
+    int st;
+    if (p->cells) {
+        if (f->type != FIELD_GRID || f->grid != p->cells)
+            return set_err(c, MCS_ERR_UNSUPPORTED, "a cell-layout population needs the field of its own mesh");
+        st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, f, dt, tracker, nullptr)
+                                      : launch_step_mesh<double>(p, t, f, dt, tracker, nullptr);
+    } else {
+        st = p->precision == MCS_FP32 ? launch_step_abs<float>(p, t, f, dt, tracker, nullptr)
+                                      : launch_step_abs<double>(p, t, f, dt, tracker, nullptr);
+    }
+    if (st) return st;
+    p->cur ^= 1;
+    p->step += 1;
+    return MCS_OK;
+}
+
+MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* tracker) {
+    if (!p || !t) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "collisions! on a cell-layout population");
+    if (int st = use_device(c)) return st;
+    const int st = p->precision == MCS_FP32 ? launch_collisions<float>(p, t, dt, tracker)
+                                            : launch_collisions<double>(p, t, dt, tracker);
+    if (st) return st;
+    p->cur ^= 1;
+    p->step += 1;
+    return MCS_OK;
+}
+
+MCS_API int mcs_deposit(mcs_pop* p, mcs_grid* g, double val) {
+    if (!p || !g) return MCS_ERR_ARG;
+    if (p->cells && p->cells != g) return set_err(p->ctx, MCS_ERR_UNSUPPORTED, "deposit onto another mesh");
+    if (int st = use_device(p->ctx)) return st;
+    return launch_deposit(p, g, val);
+}
+
+MCS_API int mcs_repack(mcs_pop* p) {
+    if (!p) return MCS_ERR_ARG;
+    if (int st = use_device(p->ctx)) return st;
+    return launch_repack(p);
+}
+
+MCS_API int mcs_swarm_resample(mcs_pop* p, int64_t n0, double tol) {
+    if (!p || n0 < 1) return MCS_ERR_ARG;
+    if (int st = use_device(p->ctx)) return st;
+    return launch_swarm_resample(p, n0, tol);
+}
+
+MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout) {
+    if (!p || !out) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    const int nm = MCS_MOMENTS_BASE + (t ? t->v.nrows : 0);
+    if (nout < nm) return set_err(c, MCS_ERR_ARG, "moments buffer too small");
+    if (int st = use_device(c)) return st;
+    if (int st = launch_moments(p, t, p->d_moments, nm)) return st;
+    MCS_CK(c, cudaMemcpyAsync(out, p->d_moments, nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return sync_status(c);
+}
+
+MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, int nsteps, int64_t n0,
+                          double tol, double* moments_out) {
+    if (!p || !t || !f || nsteps < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "swarm loop on a cell-layout population");
+    if (int st = use_device(c)) return st;
+    double* d_out = nullptr;
+    if (int st = dalloc(c, &d_out, (size_t)(nsteps > 0 ? nsteps : 1) * kStepMoments)) return st;
+    int st = MCS_OK;
+    for (int i = 0; i < nsteps && !st; ++i) {
+        double* mo = d_out + (size_t)i * kStepMoments;
+        st = p->precision == MCS_FP32 ? launch_step_abs<float>(p, t, f, dt, nullptr, mo)
+                                      : launch_step_abs<double>(p, t, f, dt, nullptr, mo);
+        if (st) break;
+        p->cur ^= 1;
+        p->step += 1;
+        if (n0 > 0) st = launch_swarm_resample(p, n0, tol);
+    }
+    if (!st && moments_out && nsteps > 0) {
+        cudaError_t e = cudaMemcpyAsync(moments_out, d_out, (size_t)nsteps * kStepMoments * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c->stream);
+        if (e != cudaSuccess) st = set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    const int st2 = sync_status(c);
+    cudaFree(d_out);
+    return st ? st : st2;
+}
+
+}  // extern "C"

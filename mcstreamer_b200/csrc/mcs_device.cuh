@@ -1,0 +1,174 @@
+// mcs_device.cuh -- device-side building blocks shared by every kernel of the library:
+// Philox4x32-10 streams, uniform conversion, status bits, the ordered-append tile
+// protocol (decoupled look-back) and block reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mcs {
+
+constexpr double kElementaryCharge = 1.6021766208e-19;  // JuMC/src/constants.jl:50
+constexpr double kElectronMass = 9.10938356e-31;        // JuMC/src/constants.jl:52
+
+// Sticky device status bits (atomicOr into the context's status word).
+enum : uint32_t {
+    ST_CAPACITY = 1u,    // population capacity exceeded (population.jl:90 assert)
+    ST_ENERGY = 2u,      // energy outside the collision table (util.jl:28 assert)
+    ST_FIELD = 4u,       // |E| > 1e8 V/m (gridfields.jl:179-187)
+    ST_NONFINITE = 8u,   // NaN/Inf in particle state
+    ST_OVERFLOW = 16u,   // a tile produced more secondaries than its staging holds
+    ST_TIMEOUT = 32u,    // a bounded wait gave up
+};
+
+// Philox stream tags (4th counter word); must match the oracle.
+enum : uint32_t { TAG_ADVANCE = 0, TAG_SWARM_RESAMPLE = 1, TAG_CELL_RESAMPLE = 2, TAG_INIT = 3,
+                  TAG_COLLISIONS = 4 };
+
+// Process kinds; must match include/mcs.h.
+enum : int { K_NULL = 0, K_ELASTIC = 1, K_EXCITATION = 2, K_IONIZATION = 3, K_ATTACHMENT = 4,
+             K_IONIZATION_UNIFORM = 5 };
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11).  Counter = {c0, c1, block, tag}, key = 64-bit seed.
+// ---------------------------------------------------------------------------------------
+struct U4 { uint32_t x, y, z, w; };
+
+__device__ __forceinline__ U4 philox10(U4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = U4{hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0};
+    }
+    return c;
+}
+
+// One particle's (or cell's) uniform stream: word #k comes from block k/4, lane k%4.
+struct Rng {
+    uint32_t k0, k1, c0, c1, tag, k;
+    U4 buf;
+    __device__ __forceinline__ void init(uint64_t seed, uint32_t a, uint32_t b, uint32_t t) {
+        k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32); c0 = a; c1 = b; tag = t; k = 0;
+    }
+    __device__ __forceinline__ uint32_t word() {
+        const uint32_t lane = k & 3u;
+        if (lane == 0) buf = philox10(U4{c0, c1, k >> 2, tag}, k0, k1);
+        ++k;
+        uint32_t r = buf.x;
+        r = lane == 1 ? buf.y : r;
+        r = lane == 2 ? buf.z : r;
+        r = lane == 3 ? buf.w : r;
+        return r;
+    }
+    // (w + 0.5) * 2^-32, bit-identical to the oracle's uniform.
+    __device__ __forceinline__ double u64() { return __fma_rn((double)word(), 0x1p-32, 0x1p-33); }
+    // float in (0, 1]: the float nearest to the same uniform (within one ulp).
+    __device__ __forceinline__ float u32() { return __uint2float_rn(word() | 1u) * 0x1p-32f; }
+};
+
+template <typename T> struct Uni;
+template <> struct Uni<double> { __device__ static double get(Rng& r) { return r.u64(); } };
+template <> struct Uni<float> { __device__ static float get(Rng& r) { return r.u32(); } };
+
+// ---------------------------------------------------------------------------------------
+// Precision-specific math.  FP64 follows the reference's operations; FP32 uses the SFU
+// approximations where the Monte Carlo tolerates their error (documented per call).
+// ---------------------------------------------------------------------------------------
+template <typename T> struct M;
+template <> struct M<double> {
+    __device__ static double nlog(double u) { return -log(u); }
+    __device__ static void dir(Rng& r, double& dx, double& dy, double& dz) {
+        // randsphere: JuMC/src/util.jl:4-12
+        const double phi = 6.283185307179586 * r.u64();
+        double s, c;
+        sincos(phi, &s, &c);
+        const double u = 2.0 * r.u64() - 1.0;
+        const double v = sqrt(1.0 - u * u);
+        dx = v * c; dy = v * s; dz = u;
+    }
+    __device__ static double sq(double x) { return sqrt(x); }
+};
+template <> struct M<float> {
+    __device__ static float nlog(float u) { return -__logf(u); }
+    __device__ static void dir(Rng& r, float& dx, float& dy, float& dz) {
+        // phi = 2*pi*U evaluated as (2U-1)*pi + pi so the SFU sees |arg| <= pi.
+        const float ph = fmaf(r.u32(), 6.28318530718f, -3.14159265359f);
+        float s, c;
+        __sincosf(ph, &s, &c);
+        const float u = fmaf(2.0f, r.u32(), -1.0f);
+        const float v = sqrtf(fmaxf(0.0f, 1.0f - u * u));
+        dx = -v * c; dy = -v * s; dz = u;
+    }
+    __device__ static float sq(float x) { return sqrtf(x); }
+};
+
+// ---------------------------------------------------------------------------------------
+// Block-wide helpers
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Ordered-append tile status word: [epoch:30][flag:2][value:32].
+// flag 1 = aggregate of this tile only, flag 2 = inclusive prefix through this tile.
+__device__ __forceinline__ unsigned long long tile_word(uint32_t epoch, uint32_t flag, uint32_t v) {
+    return ((unsigned long long)(epoch & 0x3fffffffu) << 34) | ((unsigned long long)flag << 32) | v;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Exclusive prefix of `count` over tiles [0, tile) by decoupled look-back (Merrill &
+// Garland 2016).  Tiles are handed out in increasing order by an atomic ticket, so every
+// predecessor is owned by a running CTA and the wait ends; it is still bounded, and on
+// timeout ST_TIMEOUT is raised and the returned prefix is flagged invalid (ok=false).
+// Called by one thread.
+__device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, uint32_t tile, uint32_t epoch,
+                                                  uint32_t count, uint32_t* st_word, bool* ok) {
+    *ok = true;
+    if (tile == 0) {
+        st_release_u64(&status[0], tile_word(epoch, 2, count));
+        return 0;
+    }
+    st_release_u64(&status[tile], tile_word(epoch, 1, count));
+    uint32_t excl = 0;
+    int64_t p = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    const uint32_t ep = epoch & 0x3fffffffu;
+    while (p >= 0) {
+        const unsigned long long s = ld_acquire_u64(&status[p]);
+        const uint32_t e = (uint32_t)(s >> 34);
+        const uint32_t f = (uint32_t)(s >> 32) & 3u;
+        if (e != ep || f == 0) {
+            if (++spins > (1u << 24)) {  // ~ seconds with the backoff below
+                atomicOr(st_word, ST_TIMEOUT);
+                *ok = false;
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        excl += (uint32_t)s;
+        if (f == 2) break;
+        --p;
+    }
+    st_release_u64(&status[tile], tile_word(epoch, 2, excl + count));
+    return excl;
+}
+
+}  // namespace mcs

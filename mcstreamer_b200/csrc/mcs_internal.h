@@ -1,0 +1,132 @@
+// mcs_internal.h -- host-side objects behind the opaque handles of include/mcs.h and the
+// plain-data views that kernels receive by value.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/mcs.h"
+
+namespace mcs {
+
+constexpr int kMaxRows = 32;      // table rows (processes incl. null)
+constexpr int kStepMoments = 12;  // fused per-step moments, see StepMoment
+enum StepMoment { SM_COUNT = 0, SM_W, SM_X, SM_Y, SM_Z, SM_XX, SM_YY, SM_ZZ, SM_VX, SM_VY, SM_VZ, SM_E };
+
+enum GridType { GRID_CART3D = 1, GRID_CYL = 2 };
+enum FieldType { FIELD_UNIFORM = 0, FIELD_GRID = 1 };
+
+// ---- kernel-side views (trivially copyable) ----
+struct TableView {
+    const double* rate64;   // [neps][nrows]
+    const float* rate32;    // [neps][nrp] (nrp = nrows rounded up to 4)
+    int nrows, nrp, neps;
+    double e0, emax, step, maxrate, inv_maxrate;
+    float ke32, e0n32, maxrate32;  // u = v^2*ke32 - e0n32 in grid units
+    int kind[kMaxRows];
+    double param[kMaxRows];
+};
+
+struct GridView {
+    int type;               // 0 none, GRID_CART3D, GRID_CYL
+    int nx, ny, nz;         // cart3d cells
+    double h, inv_h, x0, y0, z0;
+    const float* e32;       // cart3d node field, 4 floats per node (Ex,Ey,Ez,0)
+    const double* e64;      // cart3d node field, 3 doubles per node
+    double R, L, dr, dz;    // cyl
+    int M, N;
+    const double* er; const double* ez;  // cyl faces (M+3)x(N+3)
+    long long* qfixed;      // tracker deposits (int64, 2^-32 e)
+    long long* qpart;       // particle deposits
+};
+
+template <typename T>
+struct PopView {
+    T* f[8];                // x y z vx vy vz w s   (mesh layout: ox oy oz = in-cell offsets)
+    uint32_t* cell;         // mesh layout only
+    uint8_t* act;
+    const long long* n_in;  // particles at entry
+    long long* n_out;       // particles at exit (double-buffered count)
+    long long cap;
+};
+
+struct StepCtl {
+    unsigned long long seed;
+    uint32_t step, tag, flags, epoch;
+    uint32_t* status;         // sticky status word
+    unsigned long long* tile_status;
+    uint32_t* counters;       // [0] tile ticket, [1] CTA done count
+    double* tile_partials;    // [tile][kStepMoments]
+    double* moments_out;      // kStepMoments doubles or nullptr
+    double dt;
+};
+
+}  // namespace mcs
+
+// ---- opaque handle types ----
+struct mcs_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t flags = 0;
+    uint32_t* d_status = nullptr;
+    uint32_t epoch = 1;
+    int num_sms = 148;
+    std::string err;
+};
+
+struct mcs_table {
+    mcs_ctx* ctx = nullptr;
+    mcs::TableView v{};
+    double* d_rate64 = nullptr;
+    float* d_rate32 = nullptr;
+};
+
+struct mcs_grid {
+    mcs_ctx* ctx = nullptr;
+    mcs::GridView v{};
+    int precision = MCS_FP32;
+    float* d_e32 = nullptr;
+    double* d_e64 = nullptr;
+    double* d_er = nullptr;
+    double* d_ez = nullptr;
+    long long* d_q[2] = {nullptr, nullptr};
+    size_t nq = 0;          // entries per charge array
+};
+
+struct mcs_field {
+    mcs_ctx* ctx = nullptr;
+    int type = mcs::FIELD_UNIFORM;
+    double e[3] = {0, 0, 0};
+    mcs_grid* grid = nullptr;
+};
+
+struct mcs_pop {
+    mcs_ctx* ctx = nullptr;
+    int precision = MCS_FP64;
+    mcs_grid* cells = nullptr;     // mesh layout when non-null
+    long long cap = 0;
+    size_t esz = 8;                // bytes per float field
+    void* f[8] = {};
+    uint32_t* cell = nullptr;
+    uint8_t* act = nullptr;
+    long long* d_n = nullptr;      // [2] double-buffered count
+    int cur = 0;
+    unsigned long long seed = 0;
+    uint32_t step = 0;
+    uint32_t resample_calls = 0;
+    // scratch
+    unsigned long long* tile_status = nullptr;
+    long long max_tiles = 0;
+    double* tile_partials = nullptr;
+    uint32_t* counters = nullptr;  // 8 words
+    double* d_moments = nullptr;   // kStepMoments
+    void* staging = nullptr;       // host<->device transfer staging
+    size_t staging_bytes = 0;
+    uint32_t* u32a = nullptr;      // per-particle scratch (cap)
+    uint32_t* u32b = nullptr;      // per-particle scratch (cap)
+    void* alt[8] = {};             // permutation double buffer
+    uint32_t* alt_cell = nullptr;
+    uint8_t* alt_act = nullptr;
+};

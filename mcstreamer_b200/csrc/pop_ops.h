@@ -1,0 +1,16 @@
+// pop_ops.h -- launchers of the population-level kernels (pop_ops.cu).
+#pragma once
+#include "mcs_internal.h"
+
+namespace mcs {
+int launch_scan(mcs_pop* p, const uint32_t* in, uint32_t* out, const long long* n_dev, long long* total);
+int launch_repack(mcs_pop* p);
+int launch_swarm_resample(mcs_pop* p, long long n0, double tol);
+int launch_moments(mcs_pop* p, const mcs_table* t, double* d_out, int nm);
+int launch_deposit(mcs_pop* p, mcs_grid* g, double val);
+int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* dw, const double* ds,
+                  const uint8_t* da, long long n);
+int launch_download(mcs_pop* p, double* dx, double* dv, double* dw, double* ds, uint8_t* da);
+int grid_for(mcs_ctx* c, long long n, int block);
+constexpr int kMomentPartialsMin = 148 * 2 * (MCS_MOMENTS_BASE + kMaxRows);
+}  // namespace mcs

@@ -1,0 +1,377 @@
+// step.cuh -- the electron step (advance!, JuMC/src/mixed_population.jl:24-54) as one
+// persistent, tiled sm_100a kernel per field model:
+//
+//   * each CTA takes tiles of BLOCK*PPT consecutive slots from an atomic ticket;
+//   * every active particle is pushed, collided and tracked with its state in registers;
+//     uniforms come from its own Philox stream (seed; slot, step, k/4, tag);
+//   * secondaries are staged in shared memory, ranked by (parent slot, event #), and
+//     appended after the tiles before them (decoupled look-back on per-tile counts), so
+//     the population order equals the serial reference order (ascending parent index);
+//   * per-tile partial moments are reduced by the last CTA in tile order (deterministic).
+//
+// Included by step_f32.cu (FMA contraction on) and step_f64.cu (-fmad=false, so the FP64
+// operation sequence matches the reference's unfused arithmetic).
+#pragma once
+#include "mcs_device.cuh"
+#include "mcs_internal.h"
+
+namespace mcs {
+
+constexpr uint32_t FLAG_CLAMP = MCS_FLAG_CLAMP_ENERGY;
+
+// ---------------------------------------------------------------------------------------
+// Shared-memory copy of the per-row process description.
+// ---------------------------------------------------------------------------------------
+template <typename T>
+struct RowsSmem {
+    int kind[kMaxRows];
+    T par[kMaxRows];   // FP64: threshold (J) or mass ratio.  FP32: 2*th/m (v^2 units) or m/(M+m)
+};
+
+template <typename T>
+__device__ __forceinline__ void load_rows(RowsSmem<T>& r, const TableView& t) {
+    for (int j = threadIdx.x; j < kMaxRows; j += blockDim.x) {
+        const int kd = j < t.nrows ? t.kind[j] : K_NULL;
+        r.kind[j] = kd;
+        double p = j < t.nrows ? t.param[j] : 0.0;
+        if (sizeof(T) == 4) {
+            if (kd == K_ELASTIC) p = p / (1.0 + p);
+            else p = 2.0 * p / kElectronMass;
+        }
+        r.par[j] = (T)p;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Table lookup + process selection: do_one_collision!, JuMC/src/collisions.jl:159-192
+// (indweight util.jl:23-30, rate collisions.jl:35-39).  Returns the row or -1.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ int select_row64(const TableView& t, double eng, double xi, uint32_t flags,
+                                            uint32_t* status) {
+    const double x = eng - t.e0;
+    double fk = floor(x / t.step);                 // Julia fld: exact floor of the quotient
+    if (__fma_rn(fk, t.step, -x) > 0.0) fk -= 1.0;
+    long long k;
+    double w;
+    if (!(fk >= 0.0 && fk <= (double)(t.neps - 2))) {
+        const bool low = !(fk >= 0.0) && eng < t.e0;
+        k = low ? 0 : t.neps - 2;
+        w = low ? 1.0 : 0.0;
+        if (!(flags & FLAG_CLAMP)) atomicOr(status, ST_ENERGY);
+    } else {
+        k = (long long)fk;
+        const double tt = (double)(k + 1) / (double)(t.neps - 1);  // LinRange lerpi
+        const double ek1 = (1.0 - tt) * t.e0 + tt * t.emax;
+        w = (ek1 - eng) / t.step;
+    }
+    const double* c0 = t.rate64 + k * t.nrows;
+    const double* c1 = c0 + t.nrows;
+    for (int j = 0; j < t.nrows; ++j) {
+        const double nu = w * __ldg(c0 + j) + (1.0 - w) * __ldg(c1 + j);
+        if (nu > xi) return j;
+        xi -= nu;
+    }
+    return -1;
+}
+
+// FP32: u = v^2 * (m/2/step) - e0/step is the position on the energy grid.
+__device__ __forceinline__ int select_row32(const TableView& t, float v2, float xi, uint32_t flags,
+                                            uint32_t* status) {
+    const float u = fmaf(v2, t.ke32, -t.e0n32);
+    int k = (int)u;
+    float w;
+    if (!(u >= 0.0f && k <= t.neps - 2)) {
+        const bool low = !(u >= 0.0f);
+        k = low ? 0 : t.neps - 2;
+        w = low ? 1.0f : 0.0f;
+        if (!(flags & FLAG_CLAMP)) atomicOr(status, ST_ENERGY);
+    } else {
+        w = (float)(k + 1) - u;
+    }
+    const float4* c0 = reinterpret_cast<const float4*>(t.rate32 + (size_t)k * t.nrp);
+    const float4* c1 = reinterpret_cast<const float4*>(t.rate32 + (size_t)(k + 1) * t.nrp);
+    const int nq = t.nrp >> 2;
+    for (int q = 0; q < nq; ++q) {
+        const float4 a = __ldg(c0 + q), b = __ldg(c1 + q);
+        const int j = q << 2;
+        float nu = fmaf(w, a.x - b.x, b.x);
+        if (nu > xi) return j;
+        xi -= nu;
+        nu = fmaf(w, a.y - b.y, b.y);
+        if (nu > xi) return j + 1 < t.nrows ? j + 1 : -1;
+        xi -= nu;
+        nu = fmaf(w, a.z - b.z, b.z);
+        if (nu > xi) return j + 2 < t.nrows ? j + 2 : -1;
+        xi -= nu;
+        nu = fmaf(w, a.w - b.w, b.w);
+        if (nu > xi) return j + 3 < t.nrows ? j + 3 : -1;
+        xi -= nu;
+    }
+    return -1;
+}
+
+// Outcome of collide(): 0 state change / nothing, 1 new particle, 2 removal.
+enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2 };
+
+template <typename T>
+struct Sec { T vx, vy, vz, s; };
+
+// collide: JuMC/src/electron.jl:108-139.  FP64 follows the reference's expressions.
+__device__ __forceinline__ int collide64(int kind, double par, double eng, Rng& r, double& vx, double& vy,
+                                         double& vz, Sec<double>& sec) {
+    const double m = kElectronMass;
+    if (kind == K_ELASTIC) {
+        const double f = par / (1.0 + par);
+        const double cx = f * vx, cy = f * vy, cz = f * vz;
+        const double dx = vx - cx, dy = vy - cy, dz = vz - cz;
+        const double nrm = sqrt(dx * dx + dy * dy + dz * dz);
+        double ux, uy, uz;
+        M<double>::dir(r, ux, uy, uz);
+        vx = ux * nrm + cx; vy = uy * nrm + cy; vz = uz * nrm + cz;
+        return OUT_NONE;
+    }
+    if (kind == K_EXCITATION) {
+        const double E1 = fmax(0.0, eng - par);
+        const double va = sqrt(2.0 * E1 / m);
+        double ux, uy, uz;
+        M<double>::dir(r, ux, uy, uz);
+        vx = ux * va; vy = uy * va; vz = uz * va;
+        return OUT_NONE;
+    }
+    if (kind == K_IONIZATION || kind == K_IONIZATION_UNIFORM) {
+        double va1, va2;
+        if (kind == K_IONIZATION) {
+            const double E1 = fmax(0.0, eng - par) / 2.0;
+            va1 = va2 = sqrt(2.0 * E1 / m);
+        } else {
+            const double Ea = fmax(0.0, eng - par);
+            const double E2 = r.u64() * Ea;
+            const double E1 = Ea - E2;
+            va1 = sqrt(2.0 * E1 / m);
+            va2 = sqrt(2.0 * E2 / m);
+        }
+        double ux, uy, uz, wx, wy, wz;
+        M<double>::dir(r, ux, uy, uz);
+        M<double>::dir(r, wx, wy, wz);
+        sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
+        sec.s = -log(r.u64());
+        vx = ux * va1; vy = uy * va1; vz = uz * va1;
+        return OUT_NEW;
+    }
+    if (kind == K_ATTACHMENT) return OUT_REMOVE;
+    return OUT_NONE;
+}
+
+// FP32: energies in v^2 units (par = 2*threshold/m), same draws in the same order.
+__device__ __forceinline__ int collide32(int kind, float par, float v2, Rng& r, float& vx, float& vy,
+                                         float& vz, Sec<float>& sec) {
+    if (kind == K_ELASTIC) {
+        const float cx = par * vx, cy = par * vy, cz = par * vz;
+        const float dx = vx - cx, dy = vy - cy, dz = vz - cz;
+        const float nrm = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        float ux, uy, uz;
+        M<float>::dir(r, ux, uy, uz);
+        vx = fmaf(ux, nrm, cx); vy = fmaf(uy, nrm, cy); vz = fmaf(uz, nrm, cz);
+        return OUT_NONE;
+    }
+    if (kind == K_EXCITATION) {
+        const float va = sqrtf(fmaxf(0.0f, v2 - par));
+        float ux, uy, uz;
+        M<float>::dir(r, ux, uy, uz);
+        vx = ux * va; vy = uy * va; vz = uz * va;
+        return OUT_NONE;
+    }
+    if (kind == K_IONIZATION || kind == K_IONIZATION_UNIFORM) {
+        float va1, va2;
+        const float ea = fmaxf(0.0f, v2 - par);
+        if (kind == K_IONIZATION) {
+            va1 = va2 = sqrtf(0.5f * ea);
+        } else {
+            const float f2 = r.u32();
+            va1 = sqrtf(ea - f2 * ea);
+            va2 = sqrtf(f2 * ea);
+        }
+        float ux, uy, uz, wx, wy, wz;
+        M<float>::dir(r, ux, uy, uz);
+        M<float>::dir(r, wx, wy, wz);
+        sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
+        sec.s = M<float>::nlog(r.u32());
+        vx = ux * va1; vy = uy * va1; vz = uz * va1;
+        return OUT_NEW;
+    }
+    if (kind == K_ATTACHMENT) return OUT_REMOVE;
+    return OUT_NONE;
+}
+
+// ---------------------------------------------------------------------------------------
+// Deposits.  Int64 fixed point at 2^-32 elementary charges; the arithmetic is the oracle's
+// (seven rounded corners, the eighth takes the remainder: node sum == llrint(q*2^32)).
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void cic_fixed(long long* q, int nx, int ny, int ix, int iy, int iz, double fx,
+                                          double fy, double fz, double charge) {
+    const long long W = __double2ll_rn(charge * 0x1p32);
+    const double Wd = (double)W;
+    const double gx[2] = {1.0 - fx, fx}, gy[2] = {1.0 - fy, fy}, gz[2] = {1.0 - fz, fz};
+    const long long sy = nx + 1, sz = (long long)(nx + 1) * (ny + 1);
+    long long* b = q + ix + iy * sy + iz * sz;
+    long long acc = 0;
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+        const int a0 = c & 1, a1 = (c >> 1) & 1, a2 = (c >> 2) & 1;
+        const double wc = __dmul_rn(__dmul_rn(gx[a0], gy[a1]), gz[a2]);
+        const long long qb = __double2ll_rn(__dmul_rn(Wd, wc));
+        acc += qb;
+        if (qb) atomicAdd(reinterpret_cast<unsigned long long*>(b + a0 + a1 * sy + a2 * sz),
+                          (unsigned long long)qb);
+    }
+    const long long last = W - acc;
+    if (last) atomicAdd(reinterpret_cast<unsigned long long*>(b + 1 + sy + sz), (unsigned long long)last);
+}
+
+// Cell location on the 3-D mesh of an absolute position (checkbounds semantics: [0, n)).
+__device__ __forceinline__ bool cart_locate(const GridView& g, double x, double y, double z, int& ix, int& iy,
+                                            int& iz, double& fx, double& fy, double& fz) {
+    const double ux = (x - g.x0) / g.h, uy = (y - g.y0) / g.h, uz = (z - g.z0) / g.h;
+    const double flx = floor(ux), fly = floor(uy), flz = floor(uz);
+    if (!(flx >= 0.0 && flx < (double)g.nx && fly >= 0.0 && fly < (double)g.ny && flz >= 0.0 &&
+          flz < (double)g.nz))
+        return false;
+    ix = (int)flx; iy = (int)fly; iz = (int)flz;
+    fx = ux - flx; fy = uy - fly; fz = uz - flz;
+    return true;
+}
+
+// Cylindrical NGP cell (cellindex, MCStreamer/src/grid.jl:84-90); deposits only where
+// density!/track1 do (1 <= i <= M, 0 <= j <= N+1).  Stored as int64 weight sums;
+// density = q * 2^-32 / dV(i) on read.
+__device__ __forceinline__ void cyl_track(const GridView& g, long long* q, double x, double y, double z,
+                                          double charge) {
+    const double rho = sqrt(x * x + y * y);
+    double fi = floor(rho / g.dr);
+    if (__fma_rn(fi, g.dr, -rho) > 0.0) fi -= 1.0;
+    double fj = floor(z / g.dz);
+    if (__fma_rn(fj, g.dz, -z) > 0.0) fj -= 1.0;
+    fi += 1.0; fj += 1.0;
+    if (!(fi >= 1.0 && fi <= (double)g.M && fj >= 0.0 && fj <= (double)g.N + 1.0)) return;
+    const long long idx = (long long)fi + (long long)fj * (g.M + 2);
+    const long long W = __double2ll_rn(charge * 0x1p32);
+    atomicAdd(reinterpret_cast<unsigned long long*>(q + idx), (unsigned long long)W);
+}
+
+// CollisionTracker at an absolute position (gridfields.jl:203-224).
+__device__ __forceinline__ void track_abs(const GridView& g, double x, double y, double z, double charge) {
+    if (g.type == GRID_CART3D) {
+        int ix, iy, iz;
+        double fx, fy, fz;
+        if (cart_locate(g, x, y, z, ix, iy, iz, fx, fy, fz))
+            cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, fx, fy, fz, charge);
+    } else if (g.type == GRID_CYL) {
+        cyl_track(g, g.qfixed, x, y, z, charge);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Secondary staging (shared memory) and the ordered append.
+// ---------------------------------------------------------------------------------------
+template <typename T, int SCAP>
+struct Staging {
+    T f[8][SCAP];
+    uint32_t cell[SCAP];
+    uint32_t key[SCAP];   // (tile-local parent index << 8) | event #
+    uint8_t act[SCAP];
+    uint32_t count;
+};
+
+template <typename T, int SCAP>
+__device__ __forceinline__ void stage(Staging<T, SCAP>& st, uint32_t local, uint32_t ev, const T (&v)[8],
+                                      uint32_t cell, uint8_t act, uint32_t* status) {
+    const uint32_t pos = atomicAdd(&st.count, 1u);
+    if (pos < SCAP) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) st.f[q][pos] = v[q];
+        st.cell[pos] = cell;
+        st.key[pos] = (local << 8) | (ev & 0xffu);
+        st.act[pos] = act;
+    } else {
+        atomicOr(status, ST_OVERFLOW);
+    }
+}
+
+// Field models for the literal Yoshida push on absolute positions.
+struct FieldUniform {
+    double ex, ey, ez;
+    template <typename T>
+    __device__ __forceinline__ void operator()(const GridView&, T, T, T, T& e0, T& e1, T& e2, uint32_t*) const {
+        e0 = (T)ex; e1 = (T)ey; e2 = (T)ez;
+    }
+};
+
+// Cylindrical FieldInterp, MCStreamer/src/gridfields.jl:115-190 (FP64 face fields).
+struct FieldCyl {
+    template <typename T>
+    __device__ __forceinline__ void operator()(const GridView& g, T x0, T x1, T x2, T& e0, T& e1, T& e2,
+                                               uint32_t* status) const {
+        const double x = x0, y = x1, z = x2;
+        e0 = e1 = e2 = (T)0;
+        const double r0 = sqrt(x * x + y * y);
+        if (!((0.0 < r0 && r0 < g.R) && (0.0 < z && z < g.L))) return;
+        double r = r0;
+        if (r == 0.0) r = g.dr / 10.0;
+        const double qr = r / g.dr;
+        long long i = (long long)trunc(qr);
+        const double dr_ = qr - (double)i;
+        const double qz = z / g.dz;
+        long long j = (long long)trunc(qz);
+        const double dz_ = qz - (double)j;
+        long long i1, j1;
+        double dr1, dz1;
+        if (dr_ < 0.5) { i1 = i; dr1 = dr_ + 0.5; } else { i1 = i + 1; dr1 = dr_ - 0.5; }
+        if (dz_ < 0.5) { j1 = j; dz1 = dz_ + 0.5; } else { j1 = j + 1; dz1 = dz_ - 0.5; }
+        i += 1; j += 1;
+        const long long ld = g.M + 3;
+        const double* er = g.er;
+        const double* ez = g.ez;
+        const double er1 = __ldg(er + i + j1 * ld) * (1 - dr_) * (1 - dz1) + __ldg(er + i + 1 + j1 * ld) * dr_ * (1 - dz1) +
+                           __ldg(er + i + (j1 + 1) * ld) * (1 - dr_) * dz1 + __ldg(er + i + 1 + (j1 + 1) * ld) * dr_ * dz1;
+        const double ez1 = __ldg(ez + i1 + j * ld) * (1 - dr1) * (1 - dz_) + __ldg(ez + i1 + 1 + j * ld) * dr1 * (1 - dz_) +
+                           __ldg(ez + i1 + (j + 1) * ld) * (1 - dr1) * dz_ + __ldg(ez + i1 + 1 + (j + 1) * ld) * dr1 * dz_;
+        const double a = er1 * x / r, b = er1 * y / r;
+        if (sqrt(a * a + b * b + ez1 * ez1) > 1e8) atomicOr(status, ST_FIELD);
+        e0 = (T)a; e1 = (T)b; e2 = (T)ez1;
+    }
+};
+
+// Trilinear node-field gather at an absolute position (3-D mesh, zero outside).
+struct FieldCartAbs {
+    template <typename T>
+    __device__ __forceinline__ void operator()(const GridView& g, T x0, T x1, T x2, T& e0, T& e1, T& e2,
+                                               uint32_t*) const {
+        e0 = e1 = e2 = (T)0;
+        const double u[3] = {((double)x0 - g.x0) / g.h, ((double)x1 - g.y0) / g.h, ((double)x2 - g.z0) / g.h};
+        const int nc[3] = {g.nx, g.ny, g.nz};
+        long long ic[3];
+        double fr[3];
+        for (int d = 0; d < 3; ++d) {
+            if (!(u[d] > 0.0 && u[d] < (double)nc[d])) return;
+            double fl = floor(u[d]);
+            if (fl > nc[d] - 1) fl = nc[d] - 1;
+            ic[d] = (long long)fl;
+            fr[d] = u[d] - fl;
+        }
+        const long long sy = g.nx + 1, sz = (long long)(g.nx + 1) * (g.ny + 1);
+        const long long base = ic[0] + ic[1] * sy + ic[2] * sz;
+        double acc[3] = {0, 0, 0};
+        for (int b = 0; b < 8; ++b) {
+            const int a0 = b & 1, a1 = (b >> 1) & 1, a2 = (b >> 2) & 1;
+            const double wgt = (a0 ? fr[0] : 1.0 - fr[0]) * (a1 ? fr[1] : 1.0 - fr[1]) * (a2 ? fr[2] : 1.0 - fr[2]);
+            const long long nd = base + a0 + a1 * sy + a2 * sz;
+            for (int c = 0; c < 3; ++c) {
+                const double ev = g.e64 ? __ldg(g.e64 + 3 * nd + c) : (double)__ldg(g.e32 + 4 * nd + c);
+                acc[c] += wgt * ev;
+            }
+        }
+        e0 = (T)acc[0]; e1 = (T)acc[1]; e2 = (T)acc[2];
+    }
+};
+
+}  // namespace mcs

@@ -1,0 +1,57 @@
+// step_launch.cuh -- host launchers of the step kernels, instantiated per precision by
+// step_f32.cu and step_f64.cu.
+#pragma once
+#include "host_util.h"
+#include "step_kernel.cuh"
+
+namespace mcs {
+
+template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
+int launch_abs_variant(mcs_pop* p, const mcs_table* t, const GridView& fg, const GridView& tg, const Field& fld,
+                       double dt, double ax, double ay, double az, double* mom) {
+    mcs_ctx* c = p->ctx;
+    constexpr int TILE = BLOCK * PPT;
+    auto kern = k_step_abs<T, BLOCK, PPT, Field, CLOSED>;
+    const long long max_tiles = (p->cap + TILE - 1) / TILE;
+    const int grid = persistent_grid(c, kern, BLOCK, max_tiles);
+    YoshidaHost yh;
+    YoshidaC Y{yh.c1, yh.c2, yh.c3, yh.c4, yh.d1, yh.d2, yh.d3, (-kElementaryCharge) / kElectronMass};
+    StepCtl C = step_ctl(p, dt, TAG_ADVANCE, mom);
+    kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, fg, tg, C, fld, Y, ax, ay, az);
+    MCS_CK_LAUNCH(c);
+    return MCS_OK;
+}
+
+template <typename T, int BLOCK, int PPT>
+int launch_step_abs_impl(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* trk,
+                         double* mom) {
+    const GridView tg = grid_view(trk);
+    const double qm = (-kElementaryCharge) / kElectronMass;
+    if (f->type == FIELD_UNIFORM) {
+        FieldUniform fu{f->e[0], f->e[1], f->e[2]};
+        const GridView none = grid_view(nullptr);
+        if constexpr (sizeof(T) == 4)
+            return launch_abs_variant<T, BLOCK, PPT, FieldUniform, true>(p, t, none, tg, fu, dt, qm * f->e[0],
+                                                                         qm * f->e[1], qm * f->e[2], mom);
+        else
+            return launch_abs_variant<T, BLOCK, PPT, FieldUniform, false>(p, t, none, tg, fu, dt, 0, 0, 0, mom);
+    }
+    const GridView fg = grid_view(f->grid);
+    if (f->grid->v.type == GRID_CYL)
+        return launch_abs_variant<T, BLOCK, PPT, FieldCyl, false>(p, t, fg, tg, FieldCyl{}, dt, 0, 0, 0, mom);
+    return launch_abs_variant<T, BLOCK, PPT, FieldCartAbs, false>(p, t, fg, tg, FieldCartAbs{}, dt, 0, 0, 0, mom);
+}
+
+template <typename T, int BLOCK, int PPT>
+int launch_collisions_impl(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* trk) {
+    mcs_ctx* c = p->ctx;
+    constexpr int TILE = BLOCK * PPT;
+    auto kern = k_collisions<T, BLOCK, PPT>;
+    const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
+    StepCtl C = step_ctl(p, dt, TAG_COLLISIONS, nullptr);
+    kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, grid_view(trk), C);
+    MCS_CK_LAUNCH(c);
+    return MCS_OK;
+}
+
+}  // namespace mcs

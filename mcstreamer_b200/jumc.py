@@ -1,0 +1,263 @@
+"""Python mirror of JuMC's particle API over the C ABI.
+
+Names follow the reference (JuMC/src): Julia's mutating `f!` becomes `f`.  A Population
+lives on the GPU; `advance` is advance!(mpopl, efield, dt, tracker)
+(mixed_population.jl:24), `collisions` is collisions! (:61), `repack` is repack!
+(population.jl:191).  Every call goes through libmcs_b200.so; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from . import constants as co
+from .lxcat import LXCatTable
+
+
+class Context:
+    """One CUDA device + stream (mcs_ctx)."""
+
+    _default: dict[int, "Context"] = {}
+
+    def __init__(self, device: int = 0, clamp_energy: bool = False):
+        self.lib = L.lib()
+        h = C.c_void_p()
+        L.check(self.lib.mcs_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+        if clamp_energy:
+            self.set_flags(L.FLAG_CLAMP_ENERGY)
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = cls(device)
+        return cls._default[device]
+
+    def set_flags(self, flags: int) -> None:
+        L.check(self.lib.mcs_ctx_set_flags(self.h, flags), self.h)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        L.check(self.lib.mcs_ctx_set_stream(self.h, C.c_void_p(stream_ptr)), self.h)
+
+    def sync(self) -> None:
+        L.check(self.lib.mcs_sync(self.h), self.h)
+
+    def check(self, code: int) -> None:
+        L.check(code, self.h)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.mcs_ctx_destroy(self.h)
+            self.h = None
+
+
+class CollisionTable:
+    """CollisionTable (collisions.jl:9-22) resident on the device."""
+
+    def __init__(self, table: LXCatTable, ctx: Optional[Context] = None):
+        self.ctx = ctx or Context.default()
+        self.table = table
+        self.proc = table.proc
+        self.maxrate = table.maxrate
+        rate = table.rate_energy_major()
+        kinds = table.kinds
+        params = table.params
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_table_create(
+            self.ctx.h, rate.shape[1], rate.shape[0], table.energy.e0, table.energy.emax, L.dptr(rate),
+            L.i32ptr(kinds), L.dptr(params), table.maxrate, C.byref(h)))
+        self.h = h
+
+    def __len__(self) -> int:
+        return len(self.proc)
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.mcs_table_destroy(self.h)
+            self.h = None
+
+
+class FixedField:
+    """FixedField (Swarm/src/Swarm.jl:28-32): E = (0, 0, ez)."""
+
+    def __init__(self, ez: float, ctx: Optional[Context] = None, ex: float = 0.0, ey: float = 0.0):
+        self.ctx = ctx or Context.default()
+        self.ez = ez
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_field_uniform(self.ctx.h, ex, ey, ez, C.byref(h)))
+        self.h = h
+
+    def __call__(self, x):
+        return np.array([0.0, 0.0, self.ez])
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.mcs_field_destroy(self.h)
+            self.h = None
+
+
+@dataclass
+class ParticleArrays:
+    """Host copy of a population in the Julia StructArray layout."""
+
+    x: np.ndarray       # (n, 3) float64
+    v: np.ndarray       # (n, 3) float64
+    w: np.ndarray       # (n,) float64
+    s: np.ndarray       # (n,) float64
+    active: np.ndarray  # (n,) uint8
+
+    @property
+    def n(self) -> int:
+        return len(self.w)
+
+    @staticmethod
+    def empty(n: int) -> "ParticleArrays":
+        return ParticleArrays(np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n), np.zeros(n, np.uint8))
+
+    def copy(self) -> "ParticleArrays":
+        return ParticleArrays(self.x.copy(), self.v.copy(), self.w.copy(), self.s.copy(), self.active.copy())
+
+    def energy(self) -> np.ndarray:
+        return 0.5 * co.electron_mass * (self.v ** 2).sum(axis=1)
+
+
+class Population:
+    """Population (JuMC/src/population.jl:4-36) on the device.
+
+    precision: "fp64" (parity mode) or "fp32" (FP32 push/sampling, FP64 time and sums).
+    mesh: a grid created with Grid3D to store positions as (cell, in-cell offset).
+    """
+
+    def __init__(self, max_particles: int, particles: Optional[ParticleArrays], collisions: CollisionTable,
+                 precision: str = "fp64", seed: int = 0, step: int = 0, mesh=None, ctx: Optional[Context] = None):
+        self.ctx = ctx or collisions.ctx
+        self.collisions = collisions
+        self.capacity = int(max_particles)
+        self.precision = precision
+        prec = L.FP32 if precision == "fp32" else L.FP64
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_pop_create(self.ctx.h, self.capacity, prec,
+                                                   mesh.h if mesh is not None else None, C.byref(h)))
+        self.h = h
+        self.mesh = mesh
+        self.set_seed(seed, step)
+        if particles is not None:
+            self.upload(particles)
+
+    # ---- state transfer ----
+    def set_seed(self, seed: int, step: int = 0) -> None:
+        self.ctx.check(self.ctx.lib.mcs_pop_set_seed(self.h, C.c_uint64(seed), step))
+
+    @property
+    def step(self) -> int:
+        s = C.c_uint32()
+        self.ctx.check(self.ctx.lib.mcs_pop_get_step(self.h, C.byref(s)))
+        return s.value
+
+    def upload(self, p: ParticleArrays) -> None:
+        x = np.ascontiguousarray(p.x, dtype=np.float64)
+        v = np.ascontiguousarray(p.v, dtype=np.float64)
+        w = np.ascontiguousarray(p.w, dtype=np.float64)
+        s = np.ascontiguousarray(p.s, dtype=np.float64)
+        a = np.ascontiguousarray(p.active, dtype=np.uint8)
+        self.ctx.check(self.ctx.lib.mcs_pop_upload(self.h, L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a),
+                                                   len(w)))
+
+    def download(self) -> ParticleArrays:
+        n = self.nparticles()
+        out = ParticleArrays.empty(n)
+        nn = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_pop_download(self.h, L.dptr(out.x), L.dptr(out.v), L.dptr(out.w),
+                                                     L.dptr(out.s), L.u8ptr(out.active), n, C.byref(nn)))
+        return out
+
+    # ---- population.jl accessors ----
+    @property
+    def n(self) -> int:
+        return self.nparticles()
+
+    def nparticles(self) -> int:
+        n = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_pop_nparticles(self.h, C.byref(n)))
+        return n.value
+
+    def moments(self, table: Optional[CollisionTable] = None) -> np.ndarray:
+        nrows = len(table) if table is not None else 0
+        out = np.zeros(L.MOMENTS_BASE + nrows)
+        self.ctx.check(self.ctx.lib.mcs_moments(self.h, table.h if table is not None else None, L.dptr(out),
+                                                len(out)))
+        return out
+
+    def nactives(self) -> int:
+        return int(self.moments()[L.M_COUNT])
+
+    actives = nactives
+
+    def weight(self) -> float:
+        return float(self.moments()[L.M_W])
+
+    def meanenergy(self) -> float:
+        m = self.moments()
+        return float(m[L.M_WE] / m[L.M_W])
+
+    def maxenergy(self) -> float:
+        return float(self.moments()[L.M_EMAX])
+
+    def spread(self):
+        m = self.moments()
+        xm = m[L.M_WX:L.M_WX + 3] / m[L.M_W]
+        x2 = m[L.M_WX2] / m[L.M_W]
+        return xm, float(np.sqrt(x2 - xm @ xm))
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.mcs_pop_destroy(self.h)
+            self.h = None
+
+
+class MultiPopulation:
+    """MultiPopulation (mixed_population.jl:4-17) restricted to the electron population."""
+
+    def __init__(self, **index):
+        self.index = index
+
+    def __iter__(self):
+        return iter(self.index.values())
+
+
+def _pops(mpopl):
+    if isinstance(mpopl, Population):
+        return [mpopl]
+    return list(mpopl)
+
+
+def advance(mpopl, efield, dt: float, tracker=None) -> None:
+    """advance!(mpopl, efield, dt, tracker) (JuMC/src/mixed_population.jl:24-54)."""
+    for popl in _pops(mpopl):
+        popl.ctx.check(popl.ctx.lib.mcs_advance(popl.h, popl.collisions.h, efield.h, dt,
+                                                tracker.h if tracker is not None else None))
+
+
+def collisions(mpopl, dt: float, tracker=None) -> None:
+    """collisions!(mpopl, dt, tracker) (JuMC/src/mixed_population.jl:61-77)."""
+    for popl in _pops(mpopl):
+        popl.ctx.check(popl.ctx.lib.mcs_collisions(popl.h, popl.collisions.h, dt,
+                                                   tracker.h if tracker is not None else None))
+
+
+def repack(popl: Population) -> None:
+    """repack!(popl) (JuMC/src/population.jl:191-215)."""
+    popl.ctx.check(popl.ctx.lib.mcs_repack(popl.h))
+
+
+def nparticles(popl: Population) -> int:
+    return popl.nparticles()
+
+
+def nactives(popl: Population) -> int:
+    return popl.nactives()

@@ -1,0 +1,150 @@
+"""Python mirror of Swarm (Swarm/src/Swarm.jl): swarm transport coefficients from a
+JuMC run in a uniform field, with the time loop and its per-step sums on the GPU.
+
+swarm() follows Swarm.swarm (Swarm.jl:48-186): for each reduced field E/N a fresh
+population is advanced nt steps; per step the unweighted means <x>, <x^2> over active
+particles give sigma^2(t) (Swarm.jl:126-130) and Swarm.resample! keeps the population
+near n0 (:136-138).  Diffusion is half the slope of a least-squares line through the last
+100 sigma^2 values (:144-150), the drift W = <v_z> (:152), mobility -W/E (:153), the rate
+coefficients k_j = <nu_j(eps)> over active particles (:156, collrate :242-248), and
+nu = g.k, alpha = g+.k/|W|, eta = g-.k/|W| (:159-161).  The mean energy is the weighted
+mean of population.jl:136-150.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib as L
+from . import constants as co
+from .jumc import CollisionTable, Context, FixedField, ParticleArrays, Population
+from .lxcat import LXCatTable
+
+# Swarm.jl:26: NAIR_STP = bar / (k * 273.15)
+NAIR_STP = 1e5 / (1.38064852e-23 * 273.15)
+
+
+def gains(proc) -> np.ndarray:
+    """gains (Swarm.jl:229-239): +1 ionization, -1 attachment, 0 otherwise."""
+    out = []
+    for p in proc:
+        if p.kind == L.ATTACHMENT:
+            out.append(-1)
+        elif p.kind in (L.IONIZATION, L.IONIZATION_UNIFORM):
+            out.append(1)
+        else:
+            out.append(0)
+    return np.array(out, dtype=np.float64)
+
+
+def resample(popl: Population, n: int, tol: float = 0.1) -> None:
+    """Swarm.resample!(popl, n, tol) (Swarm.jl:193-223): Russian roulette / Poisson cloning."""
+    popl.ctx.check(popl.ctx.lib.mcs_swarm_resample(popl.h, int(n), float(tol)))
+
+
+def collrate(popl: Population, table: CollisionTable) -> np.ndarray:
+    """Mean over active particles of the rate vector (collrate, Swarm.jl:242-248)."""
+    m = popl.moments(table)
+    return m[L.MOMENTS_BASE:L.MOMENTS_BASE + len(table)] / m[L.M_COUNT]
+
+
+def diffusion_fit(t: np.ndarray, sigma2: np.ndarray, l: int = 100) -> np.ndarray:
+    """[ones(l) t] \\ sigma2 over the last l steps; returns D = slope/2 per axis (Swarm.jl:144-146)."""
+    tt = t[-l:]
+    A = np.stack([np.ones_like(tt), tt], axis=1)
+    coef, *_ = np.linalg.lstsq(A, sigma2[-l:], rcond=None)
+    return coef[1] / 2.0
+
+
+@dataclass
+class SwarmResult:
+    en: float
+    mobility: float
+    diffusion_l: float
+    diffusion_t: float
+    diffusion: float
+    nu: float
+    alpha: float
+    eta: float
+    drift: float
+    mean_energy: float
+    k: np.ndarray
+    steps: int
+    sigma2: np.ndarray = field(repr=False, default=None)
+    counts: np.ndarray = field(repr=False, default=None)
+
+
+def initial_particles(n0: int, init: str, seed: int, mean_ev: float = 1.0) -> ParticleArrays:
+    """Swarm.jl:104-106 starts all electrons at rest at the origin ("cold"); the benchmark
+    workloads start from an isotropic Maxwellian with <eps> = mean_ev ("maxwellian")."""
+    p = ParticleArrays.empty(n0)
+    p.w[:] = 1.0
+    p.active[:] = 1
+    rng = np.random.default_rng(seed)
+    if init == "maxwellian":
+        sig = np.sqrt((2.0 / 3.0) * mean_ev * co.eV / co.electron_mass)
+        p.v[:] = rng.normal(0.0, sig, (n0, 3))
+    p.s[:] = -np.log(1.0 - rng.random(n0))
+    return p
+
+
+def swarm_one(table: CollisionTable, en_td: float, density: float, n0: int, dt: float, nt: int,
+              maxp: Optional[int] = None, precision: str = "fp64", seed: int = 0, init: str = "cold",
+              resampling: bool = True, tol: float = 0.1, l: int = 100) -> SwarmResult:
+    """One E/N point of Swarm.swarm (Swarm.jl:102-173)."""
+    ctx = table.ctx
+    maxp = maxp or max(4 * n0, 1024)
+    pop = Population(maxp, initial_particles(n0, init, seed), table, precision=precision, seed=seed)
+    eb = en_td * density * co.Td
+    fld = FixedField(eb, ctx)
+    try:
+        mom = np.zeros((nt, L.STEP_MOMENTS))
+        ctx.check(ctx.lib.mcs_swarm_run(pop.h, table.h, fld.h, dt, nt, n0 if resampling else 0, tol,
+                                        L.dptr(mom)))
+        cnt = mom[:, L.S_COUNT]
+        X = mom[:, L.S_X:L.S_X + 3] / cnt[:, None]
+        X2 = mom[:, L.S_X2:L.S_X2 + 3] / cnt[:, None]
+        sigma2 = X2 - X ** 2
+        t = np.arange(nt) * dt
+        D = diffusion_fit(t, sigma2, min(l, nt))
+        mfin = pop.moments(table)
+        W = mfin[L.M_V + 2] / mfin[L.M_COUNT]
+        k = mfin[L.MOMENTS_BASE:L.MOMENTS_BASE + len(table)] / mfin[L.M_COUNT]
+        g = gains(table.proc)
+        return SwarmResult(
+            en=en_td, mobility=-W / eb, diffusion_l=D[2], diffusion_t=(D[0] + D[1]) / 2,
+            diffusion=(D[0] + D[1] + D[2]) / 3, nu=float(g @ k), alpha=float(np.maximum(g, 0) @ k / abs(W)),
+            eta=float(-np.minimum(g, 0) @ k / abs(W)), drift=W, mean_energy=mfin[L.M_WE] / mfin[L.M_W], k=k,
+            steps=nt, sigma2=sigma2, counts=cnt)
+    finally:
+        fld.close()
+        pop.close()
+
+
+def swarm(en: Sequence[float], table: LXCatTable, density: float = NAIR_STP, n0: int = 10_000,
+          dt: Optional[float] = None, trelax: float = 2e-9, nt: Optional[int] = None, precision: str = "fp64",
+          seed: int = 0, init: str = "cold", resampling: bool = True, ctx: Optional[Context] = None,
+          maxp: Optional[int] = None) -> list[SwarmResult]:
+    """Swarm.swarm(en; ...) (Swarm.jl:48-186).  dt defaults to 1/maxrate/4 and nt to
+    ceil(trelax/dt) as in Swarm.jl:76-77."""
+    ctab = CollisionTable(table, ctx)
+    dt = dt if dt is not None else 1.0 / table.maxrate / 4
+    nt = nt if nt is not None else int(np.ceil(trelax / dt))
+    try:
+        return [swarm_one(ctab, e, density, n0, dt, nt, maxp=maxp, precision=precision, seed=seed + i,
+                          init=init, resampling=resampling) for i, e in enumerate(en)]
+    finally:
+        ctab.close()
+
+
+def stats(samples: Sequence[Sequence[SwarmResult]]) -> dict[str, np.ndarray]:
+    """stats (Swarm.jl:253-269): mean and standard error std/sqrt(n) over replicas."""
+    keys = ["mobility", "diffusion_l", "diffusion_t", "diffusion", "nu", "alpha", "eta", "drift", "mean_energy"]
+    out: dict[str, np.ndarray] = {"en": np.array([r.en for r in samples[0]])}
+    for k in keys:
+        a = np.array([[getattr(r, k) for r in rep] for rep in samples])
+        out[k] = a.mean(axis=0)
+        out[k + "_err"] = a.std(axis=0, ddof=1) / np.sqrt(len(samples)) if len(samples) > 1 else np.zeros(a.shape[1])
+    return out

