@@ -123,6 +123,9 @@ MCS_API int mcs_grid_create_cyl(mcs_ctx* ctx, double R, double L, int M, int N, 
 MCS_API int mcs_grid_destroy(mcs_grid* g);
 /* cart3d: 3 doubles per node.  cyl: er followed by ez. */
 MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e);
+/* cart3d only: nodes [node0, node0 + count) of the node field (3 doubles per node), so a
+ * large field can be streamed from the host in pieces. */
+MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count, const double* e);
 MCS_API int mcs_grid_zero(mcs_grid* g, int which);
 /* cart3d: int64 per node (2^-32 e).  Not available for cyl grids. */
 MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out);
@@ -159,6 +162,12 @@ MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n);
  * 198-224) depositing +w per ionization and -w per attachment into MCS_Q_FIXED. */
 MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt,
                         mcs_grid* tracker);
+/* advance! followed by density!(deposit, val) of the post-step particles, fused in one
+ * kernel (the streamer step: push + collide + track + deposit).  Needs a cell-layout
+ * population whose mesh is the field, tracker (or NULL) and deposit grid.  Accumulates
+ * into MCS_Q_PART. */
+MCS_API int mcs_advance_deposit(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt,
+                                mcs_grid* tracker, mcs_grid* deposit, double val);
 /* collisions!(mpopl, dt, tracker) (JuMC/src/mixed_population.jl:61-77). */
 MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* tracker);
 /* density!(grid, arr, mpopl, Electron, fields, val) (MCStreamer/src/poisson.jl:65-84)

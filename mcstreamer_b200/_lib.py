@@ -53,6 +53,7 @@ SIGNATURES = {
     "mcs_grid_create_cyl": (i32, [vp, f64, f64, i32, i32, ph]),
     "mcs_grid_destroy": (i32, [vp]),
     "mcs_grid_set_efield": (i32, [vp, pd]),
+    "mcs_grid_set_efield_range": (i32, [vp, i64, i64, pd]),
     "mcs_grid_zero": (i32, [vp, i32]),
     "mcs_grid_read_fixed": (i32, [vp, i32, pi64]),
     "mcs_grid_read_density": (i32, [vp, i32, pd]),
@@ -67,6 +68,7 @@ SIGNATURES = {
     "mcs_pop_download": (i32, [vp, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_pop_nparticles": (i32, [vp, pi64]),
     "mcs_advance": (i32, [vp, vp, vp, f64, vp]),
+    "mcs_advance_deposit": (i32, [vp, vp, vp, f64, vp, vp, f64]),
     "mcs_collisions": (i32, [vp, vp, f64, vp]),
     "mcs_deposit": (i32, [vp, vp, f64]),
     "mcs_repack": (i32, [vp]),

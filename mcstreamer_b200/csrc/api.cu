@@ -299,6 +299,28 @@ MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e) {
     return MCS_OK;
 }
 
+MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count, const double* e) {
+    if (!g || !e || node0 < 0 || count < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "range upload needs a cart3d grid");
+    if ((size_t)(node0 + count) > g->nq) return set_err(c, MCS_ERR_ARG, "node range beyond the mesh");
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    if (g->d_e32) {
+        std::vector<float> tmp(4 * (size_t)count);
+        for (int64_t i = 0; i < count; ++i) {
+            tmp[4 * i] = (float)e[3 * i];
+            tmp[4 * i + 1] = (float)e[3 * i + 1];
+            tmp[4 * i + 2] = (float)e[3 * i + 2];
+            tmp[4 * i + 3] = 0.0f;
+        }
+        MCS_CK(c, cudaMemcpy(g->d_e32 + 4 * node0, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    } else {
+        MCS_CK(c, cudaMemcpy(g->d_e64 + 3 * node0, e, 3 * (size_t)count * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    return MCS_OK;
+}
+
 MCS_API int mcs_grid_zero(mcs_grid* g, int which) {
     if (!g || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
     mcs_ctx* c = g->ctx;
@@ -411,7 +433,7 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     for (int q = 0; q < 8; ++q) { cudaFree(p->f[q]); cudaFree(p->alt[q]); }
     cudaFree(p->act); cudaFree(p->cell); cudaFree(p->d_n); cudaFree(p->tile_status);
     cudaFree(p->tile_partials); cudaFree(p->counters); cudaFree(p->d_moments); cudaFree(p->staging);
-    cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act);
+    cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage);
     delete p;
     return MCS_OK;
 }
@@ -508,12 +530,31 @@ MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, doub
     if (p->cells) {
         if (f->type != FIELD_GRID || f->grid != p->cells)
             return set_err(c, MCS_ERR_UNSUPPORTED, "a cell-layout population needs the field of its own mesh");
-        st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, f, dt, tracker, nullptr)
-                                      : launch_step_mesh<double>(p, t, f, dt, tracker, nullptr);
+        if (tracker && tracker != p->cells)
+            return set_err(c, MCS_ERR_UNSUPPORTED, "a cell-layout population tracks onto its own mesh");
+        st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, 0.0, nullptr)
+                                      : launch_step_mesh<double>(p, t, dt, tracker != nullptr, 0.0, nullptr);
     } else {
         st = p->precision == MCS_FP32 ? launch_step_abs<float>(p, t, f, dt, tracker, nullptr)
                                       : launch_step_abs<double>(p, t, f, dt, tracker, nullptr);
     }
+    if (st) return st;
+    p->cur ^= 1;
+    p->step += 1;
+    return MCS_OK;
+}
+
+MCS_API int mcs_advance_deposit(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* tracker,
+                                mcs_grid* deposit, double val) {
+    if (!p || !t || !f || !deposit) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (!p->cells || deposit != p->cells || f->type != FIELD_GRID || f->grid != p->cells ||
+        (tracker && tracker != p->cells))
+        return set_err(c, MCS_ERR_UNSUPPORTED, "fused step+deposit needs a cell-layout population on one mesh");
+    if (!(dt >= 0)) return set_err(c, MCS_ERR_ARG, "dt must be >= 0");
+    if (int st = use_device(c)) return st;
+    const int st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, val, nullptr)
+                                            : launch_step_mesh<double>(p, t, dt, tracker != nullptr, val, nullptr);
     if (st) return st;
     p->cur ^= 1;
     p->step += 1;

@@ -99,8 +99,7 @@ template <typename T>
 int launch_step_abs(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* trk,
                     double* moments_out);
 template <typename T>
-int launch_step_mesh(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* trk,
-                     double* moments_out);
+int launch_step_mesh(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* moments_out);
 template <typename T>
 int launch_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* trk);
 

@@ -60,6 +60,9 @@ struct StepCtl {
     double* tile_partials;    // [tile][kStepMoments]
     double* moments_out;      // kStepMoments doubles or nullptr
     double dt;
+    char* stage;              // per-CTA secondary staging, stage_stride bytes per CTA
+    unsigned long long stage_stride;
+    uint32_t stage_cap;       // entries per CTA
 };
 
 }  // namespace mcs
@@ -129,4 +132,6 @@ struct mcs_pop {
     void* alt[8] = {};             // permutation double buffer
     uint32_t* alt_cell = nullptr;
     uint8_t* alt_act = nullptr;
+    void* stage = nullptr;         // secondary staging of the step kernels
+    size_t stage_bytes = 0;
 };

@@ -4,9 +4,10 @@
 //   * each CTA takes tiles of BLOCK*PPT consecutive slots from an atomic ticket;
 //   * every active particle is pushed, collided and tracked with its state in registers;
 //     uniforms come from its own Philox stream (seed; slot, step, k/4, tag);
-//   * secondaries are staged in shared memory, ranked by (parent slot, event #), and
-//     appended after the tiles before them (decoupled look-back on per-tile counts), so
-//     the population order equals the serial reference order (ascending parent index);
+//   * secondaries are staged in a per-CTA global buffer, ranked by (parent slot, event #)
+//     with a block scan of per-parent counts, and appended after the tiles before them
+//     (decoupled look-back on per-tile counts), so the population order equals the
+//     serial reference order (ascending parent index);
 //   * per-tile partial moments are reduced by the last CTA in tile order (deterministic).
 //
 // Included by step_f32.cu (FMA contraction on) and step_f64.cu (-fmad=false, so the FP64
@@ -110,8 +111,10 @@ __device__ __forceinline__ int select_row32(const TableView& t, float v2, float 
     return -1;
 }
 
-// Outcome of collide(): 0 state change / nothing, 1 new particle, 2 removal.
-enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2 };
+// Outcome of a collision: nothing (null), new particle, removal, velocity change.
+// collide64/collide32 report OUT_NONE for the velocity-changing kinds; collide_once
+// turns that into OUT_CHANGE.
+enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2, OUT_CHANGE = 3 };
 
 template <typename T>
 struct Sec { T vx, vy, vz, s; };
@@ -271,27 +274,39 @@ __device__ __forceinline__ void track_abs(const GridView& g, double x, double y,
 }
 
 // ---------------------------------------------------------------------------------------
-// Secondary staging (shared memory) and the ordered append.
+// Secondary staging: each CTA owns a slice of a global buffer (L2-resident while the tile
+// runs).  An entry carries its (tile-local parent index, event #) key; the final slot is
+// n_entry + (secondaries of earlier tiles) + (secondaries of earlier parents in the tile)
+// + event #, i.e. ascending parent slot then event order, the serial reference order.
 // ---------------------------------------------------------------------------------------
-template <typename T, int SCAP>
-struct Staging {
-    T f[8][SCAP];
-    uint32_t cell[SCAP];
-    uint32_t key[SCAP];   // (tile-local parent index << 8) | event #
-    uint8_t act[SCAP];
-    uint32_t count;
+template <typename T>
+struct Stage {
+    T* f[8];
+    uint32_t* cell;
+    uint32_t* key;   // (local << 16) | event
+    uint8_t* act;
+    uint32_t cap;
+    __device__ __forceinline__ void init(const StepCtl& C) {
+        char* b = C.stage + (unsigned long long)blockIdx.x * C.stage_stride;
+        cap = C.stage_cap;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] = reinterpret_cast<T*>(b + (size_t)q * cap * sizeof(T));
+        cell = reinterpret_cast<uint32_t*>(b + (size_t)8 * cap * sizeof(T));
+        key = cell + cap;
+        act = reinterpret_cast<uint8_t*>(key + cap);
+    }
 };
 
-template <typename T, int SCAP>
-__device__ __forceinline__ void stage(Staging<T, SCAP>& st, uint32_t local, uint32_t ev, const T (&v)[8],
-                                      uint32_t cell, uint8_t act, uint32_t* status) {
-    const uint32_t pos = atomicAdd(&st.count, 1u);
-    if (pos < SCAP) {
+template <typename T>
+__device__ __forceinline__ void stage(const Stage<T>& sg, uint32_t* count, uint32_t local, uint32_t ev,
+                                      const T (&v)[8], uint32_t cell, uint8_t act, uint32_t* status) {
+    const uint32_t pos = atomicAdd(count, 1u);
+    if (pos < sg.cap && ev < 65536u) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) st.f[q][pos] = v[q];
-        st.cell[pos] = cell;
-        st.key[pos] = (local << 8) | (ev & 0xffu);
-        st.act[pos] = act;
+        for (int q = 0; q < 8; ++q) sg.f[q][pos] = v[q];
+        sg.cell[pos] = cell;
+        sg.key[pos] = (local << 16) | ev;
+        sg.act[pos] = act;
     } else {
         atomicOr(status, ST_OVERFLOW);
     }

@@ -13,7 +13,7 @@ int launch_collisions<float>(mcs_pop* p, const mcs_table* t, double dt, mcs_grid
     return launch_collisions_impl<float, 256, 2>(p, t, dt, trk);
 }
 template <>
-int launch_step_mesh<float>(mcs_pop* p, const mcs_table*, const mcs_field*, double, mcs_grid*, double*) {
-    return set_err(p->ctx, MCS_ERR_UNSUPPORTED, "mesh layout step not built yet");
+int launch_step_mesh<float>(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
+    return launch_step_mesh_impl<float, 256, 2>(p, t, dt, tracking, dep_val, mom);
 }
 }  // namespace mcs

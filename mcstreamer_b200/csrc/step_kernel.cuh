@@ -1,4 +1,7 @@
-// step_kernel.cuh -- persistent tile skeleton + the absolute-position step kernels.
+// step_kernel.cuh -- persistent tile skeleton and the step kernels:
+//   k_step_abs   absolute positions (swarms, cylindrical parity mode, 3-D field)
+//   k_collisions collisions! (fixed-step collision sampling, no push)
+//   k_step_mesh  3-D mesh, (cell, in-cell offset) layout, fused tracker + deposit
 #pragma once
 #include "step.cuh"
 
@@ -8,13 +11,15 @@ struct YoshidaC {
     double c1, c2, c3, c4, d1, d2, d3, qm;  // electron.jl:38-46; qm = charge/mass
 };
 
-// Per-tile bookkeeping shared by all step kernels: rank staged secondaries, append them
-// after the preceding tiles, publish the new count, and reduce the tile's moments.
-template <typename T, int BLOCK, int SCAP>
+constexpr uint32_t kOutsideCell = 0xffffffffu;
+
+template <typename T, int BLOCK, int TILE>
 struct TileShared {
-    Staging<T, SCAP> st;
     RowsSmem<T> rows;
+    uint32_t cnt[TILE];              // secondaries per tile-local parent, then exclusive prefix
+    uint32_t wtot[BLOCK / 32];
     double red[BLOCK / 32][kStepMoments];
+    uint32_t count;                  // staged entries of the current tile
     uint32_t tile;
     uint32_t excl;
     int ok;
@@ -38,7 +43,7 @@ struct MomAcc {
     }
 };
 
-// Block-reduce one MomAcc per thread into out[kStepMoments] (fixed order, deterministic).
+// Block-reduce one accumulator per thread into out[kStepMoments] (fixed order).
 template <int BLOCK, typename SH>
 __device__ __forceinline__ void block_reduce_moments(SH& sh, const double (&m)[kStepMoments], double* out) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -56,14 +61,50 @@ __device__ __forceinline__ void block_reduce_moments(SH& sh, const double (&m)[k
     __syncthreads();
 }
 
-// Append the tile's staged secondaries after all earlier tiles' (called by all threads
-// after the particle loop and a __syncthreads); `writer` stores entry e into slot dst.
-template <typename T, int BLOCK, int SCAP, typename SH, typename Writer>
-__device__ __forceinline__ uint32_t tile_append(SH& sh, const StepCtl& C, long long tile, long long ntiles,
-                                                long long n_entry, long long cap, long long* n_out,
+// In-place exclusive scan of sh.cnt[0..TILE) by the whole block.
+template <int BLOCK, int TILE, typename SH>
+__device__ __forceinline__ void block_scan_counts(SH& sh) {
+    constexpr int PER = TILE / BLOCK;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t v[PER];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        v[q] = sh.cnt[threadIdx.x * PER + q];
+        sum += v[q];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sh.wtot[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int q = 0; q < BLOCK / 32; ++q) { const uint32_t t = sh.wtot[q]; sh.wtot[q] = acc; acc += t; }
+    }
+    __syncthreads();
+    uint32_t run = sh.wtot[wid] + incl - sum;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        sh.cnt[threadIdx.x * PER + q] = run;
+        run += v[q];
+    }
+    __syncthreads();
+}
+
+// Append the tile's staged secondaries after all earlier tiles' secondaries (called by all
+// threads after the particle loop and a __syncthreads).  `writer(e, dst)` stores staged
+// entry e into population slot dst.  Returns the number of staged entries.
+template <typename T, int BLOCK, int TILE, typename SH, typename Writer>
+__device__ __forceinline__ uint32_t tile_append(SH& sh, const Stage<T>& sg, const StepCtl& C, long long tile,
+                                                long long ntiles, long long n_entry, long long cap, long long* n_out,
                                                 const Writer& writer) {
-    uint32_t cnt = sh.st.count;
-    if (cnt > SCAP) cnt = SCAP;
+    uint32_t cnt = sh.count;
+    if (cnt > sg.cap) cnt = sg.cap;
+    block_scan_counts<BLOCK, TILE>(sh);
     if (threadIdx.x == 0) {
         bool ok;
         sh.excl = tile_lookback(C.tile_status, (uint32_t)tile, C.epoch, cnt, C.status, &ok);
@@ -75,14 +116,13 @@ __device__ __forceinline__ uint32_t tile_append(SH& sh, const StepCtl& C, long l
         }
     }
     __syncthreads();
-    for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
-        const uint32_t key = sh.st.key[e];
-        uint32_t rank = 0;
-        for (uint32_t q = 0; q < cnt; ++q) rank += sh.st.key[q] < key ? 1u : 0u;
-        const long long dst = n_entry + (long long)sh.excl + rank;
-        if (!sh.ok) continue;
-        if (dst >= cap) { atomicOr(C.status, ST_CAPACITY); continue; }
-        writer(e, dst);
+    if (sh.ok) {
+        for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
+            const uint32_t key = sg.key[e];
+            const long long dst = n_entry + (long long)sh.excl + sh.cnt[key >> 16] + (key & 0xffffu);
+            if (dst >= cap) { atomicOr(C.status, ST_CAPACITY); continue; }
+            writer(e, dst);
+        }
     }
     return cnt;
 }
@@ -123,187 +163,23 @@ __device__ __forceinline__ void grid_epilogue(SH& sh, const StepCtl& C, long lon
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// Absolute-position step (swarms, cylindrical parity mode, 3-D field on absolute positions).
-// CLOSED: uniform-field FP32 fast path.  The Yoshida composition is exact for a constant
-// force (its coefficients sum to 1 and the drift-kick weight to 1/2), so the trajectory
-// between real collisions is x0 + v0*tau + a*tau^2/2 and null sub-steps cost no push; the
-// sub-step sequence, draws and decisions are those of advance!.
-// ---------------------------------------------------------------------------------------
-template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
-__global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab, GridView fgrid, GridView tgrid,
-                                                    StepCtl C, Field field, YoshidaC Y, double ax, double ay,
-                                                    double az) {
-    constexpr int TILE = BLOCK * PPT;
-    constexpr int SCAP = TILE;
-    __shared__ TileShared<T, BLOCK, SCAP> sh;
-    load_rows(sh.rows, tab);
-    const long long n_entry = *P.n_in;
-    const long long ntiles = (n_entry + TILE - 1) / TILE;
-    const bool tracking = tgrid.type != 0 && tgrid.qfixed != nullptr;
-
-    for (;;) {
-        if (threadIdx.x == 0) {
-            sh.tile = atomicAdd(&C.counters[0], 1u);
-            sh.st.count = 0;
-        }
-        __syncthreads();
-        const long long tile = sh.tile;
-        if (tile >= ntiles) break;
-        const long long base = tile * TILE;
-
-#pragma unroll 1
-        for (int jj = 0; jj < PPT; ++jj) {
-            const uint32_t local = jj * BLOCK + threadIdx.x;
-            const long long i = base + local;
-            if (i >= n_entry || !P.act[i]) continue;
-            Rng rng;
-            rng.init(C.seed, (uint32_t)i, C.step, C.tag);
-            T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
-            T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
-            const T w = P.f[6][i];
-            double s = (double)P.f[7][i];
-            uint8_t act = 1;
-            uint32_t ev = 0;
-            double trem = C.dt;
-            float tau = 0.0f;  // CLOSED: time since the last real collision
-            while (trem > 0) {
-                double tn, t;
-                if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
-                else tn = s * tab.inv_maxrate;
-                bool collides;
-                if (trem > tn) { t = tn; collides = true; }
-                else { t = trem; collides = false; s -= t * tab.maxrate; }
-                if constexpr (CLOSED) {
-                    tau += (float)t;
-                } else {
-                    // advance_free_yoshida, JuMC/src/electron.jl:51-62
-                    T ex, ey, ez;
-                    T x1 = x + (T)(Y.c1 * t) * vx, y1 = y + (T)(Y.c1 * t) * vy, z1 = z + (T)(Y.c1 * t) * vz;
-                    field(fgrid, x1, y1, z1, ex, ey, ez, C.status);
-                    const T k1 = (T)((Y.d1 * t) * Y.qm);
-                    T vx1 = vx + k1 * ex, vy1 = vy + k1 * ey, vz1 = vz + k1 * ez;
-                    T x2 = x1 + (T)(Y.c2 * t) * vx1, y2 = y1 + (T)(Y.c2 * t) * vy1, z2 = z1 + (T)(Y.c2 * t) * vz1;
-                    field(fgrid, x2, y2, z2, ex, ey, ez, C.status);
-                    const T k2 = (T)((Y.d2 * t) * Y.qm);
-                    T vx2 = vx1 + k2 * ex, vy2 = vy1 + k2 * ey, vz2 = vz1 + k2 * ez;
-                    T x3 = x2 + (T)(Y.c3 * t) * vx2, y3 = y2 + (T)(Y.c3 * t) * vy2, z3 = z2 + (T)(Y.c3 * t) * vz2;
-                    field(fgrid, x3, y3, z3, ex, ey, ez, C.status);
-                    const T k3 = (T)((Y.d3 * t) * Y.qm);
-                    vx = vx2 + k3 * ex; vy = vy2 + k3 * ey; vz = vz2 + k3 * ez;
-                    x = x3 + (T)(Y.c4 * t) * vx; y = y3 + (T)(Y.c4 * t) * vy; z = z3 + (T)(Y.c4 * t) * vz;
-                }
-                if (collides) {
-                    // do_one_collision!, collisions.jl:159-192
-                    T cvx = vx, cvy = vy, cvz = vz;
-                    if constexpr (CLOSED) {
-                        cvx = fmaf((float)ax, tau, (float)vx);
-                        cvy = fmaf((float)ay, tau, (float)vy);
-                        cvz = fmaf((float)az, tau, (float)vz);
-                    }
-                    int j;
-                    double eng = 0.0;
-                    T v2 = (T)0;
-                    if constexpr (sizeof(T) == 8) {
-                        eng = 0.5 * kElectronMass * ((double)cvx * cvx + (double)cvy * cvy + (double)cvz * cvz);
-                        const double xi = rng.u64() * tab.maxrate;
-                        j = select_row64(tab, eng, xi, C.flags, C.status);
-                    } else {
-                        v2 = fmaf((float)cvx, (float)cvx, fmaf((float)cvy, (float)cvy, (float)cvz * (float)cvz));
-                        const float xi = rng.u32() * tab.maxrate32;
-                        j = select_row32(tab, (float)v2, xi, C.flags, C.status);
-                    }
-                    const int kind = j >= 0 ? sh.rows.kind[j] : K_NULL;
-                    if (kind != K_NULL) {
-                        if constexpr (CLOSED) {  // settle the segment at the collision time
-                            const float h2 = 0.5f * tau * tau;
-                            x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
-                            y = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
-                            z = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
-                            tau = 0.0f;
-                        }
-                        vx = cvx; vy = cvy; vz = cvz;
-                        Sec<T> sec;
-                        int out;
-                        if constexpr (sizeof(T) == 8) {
-                            Sec<double> s64;
-                            double a = vx, b = vy, c = vz;
-                            out = collide64(kind, (double)sh.rows.par[j], eng, rng, a, b, c, s64);
-                            vx = (T)a; vy = (T)b; vz = (T)c;
-                            sec.vx = (T)s64.vx; sec.vy = (T)s64.vy; sec.vz = (T)s64.vz; sec.s = (T)s64.s;
-                        } else {
-                            Sec<float> s32;
-                            float a = vx, b = vy, c = vz;
-                            out = collide32(kind, (float)sh.rows.par[j], (float)v2, rng, a, b, c, s32);
-                            vx = (T)a; vy = (T)b; vz = (T)c;
-                            sec.vx = (T)s32.vx; sec.vy = (T)s32.vy; sec.vz = (T)s32.vz; sec.s = (T)s32.s;
-                        }
-                        if (out == OUT_NEW) {
-                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
-                            const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
-                            if (ev >= 255) atomicOr(C.status, ST_OVERFLOW);
-                            stage(sh.st, local, ev++, vals, 0u, act, C.status);
-                        } else if (out == OUT_REMOVE) {
-                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
-                            act = 0;  // the particle keeps sub-stepping (mixed_population.jl:32)
-                        }
-                    }
-                    if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                    else s = (double)M<float>::nlog(rng.u32());
-                }
-                trem -= t;
-            }
-            if constexpr (CLOSED) {
-                const float h2 = 0.5f * tau * tau;
-                x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
-                y = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
-                z = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
-                vx = fmaf((float)ax, tau, (float)vx);
-                vy = fmaf((float)ay, tau, (float)vy);
-                vz = fmaf((float)az, tau, (float)vz);
-            }
-            P.f[0][i] = x; P.f[1][i] = y; P.f[2][i] = z;
-            P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
-            P.f[7][i] = (T)s;
-            if (!act) P.act[i] = 0;
-        }
-        __syncthreads();
-
-        const uint32_t cnt = tile_append<T, BLOCK, SCAP>(
-            sh, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) P.f[q][dst] = sh.st.f[q][e];
-                P.act[dst] = sh.st.act[e];
-            });
-
-        if (C.moments_out) {
-            MomAcc<T> acc;
-            acc.zero();
-            for (int jj = 0; jj < PPT; ++jj) {
-                const long long i = base + jj * BLOCK + threadIdx.x;
-                if (i < n_entry && P.act[i])
-                    acc.add(P.f[0][i], P.f[1][i], P.f[2][i], P.f[3][i], P.f[4][i], P.f[5][i], P.f[6][i]);
-            }
-            for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)
-                if (sh.st.act[e])
-                    acc.add(sh.st.f[0][e], sh.st.f[1][e], sh.st.f[2][e], sh.st.f[3][e], sh.st.f[4][e],
-                            sh.st.f[5][e], sh.st.f[6][e]);
-            block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
-        }
-        __syncthreads();
+// Fetch the next tile (or -1 when done); resets the per-tile staging count.
+template <typename SH>
+__device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long long ntiles) {
+    if (threadIdx.x == 0) {
+        sh.tile = atomicAdd(&C.counters[0], 1u);
+        sh.count = 0;
     }
-    grid_epilogue<BLOCK>(sh, C, ntiles, n_entry, P.n_out);
+    __syncthreads();
+    const long long tile = sh.tile;
+    return tile < ntiles ? tile : -1;
 }
 
-}  // namespace mcs
-
-namespace mcs {
-
 // Shared collision body: select a process for velocity (vx, vy, vz) and apply it in place.
-// Returns OUT_NONE / OUT_NEW (sec filled) / OUT_REMOVE; kind_out = the applied kind.
+// Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
 template <typename T, typename RowsT>
 __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Rng& rng, T& vx,
-                                            T& vy, T& vz, Sec<T>& sec, int& kind_out) {
+                                            T& vy, T& vz, Sec<T>& sec) {
     int j;
     double eng = 0.0;
     float v2 = 0.0f;
@@ -317,92 +193,229 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
         j = select_row32(tab, v2, xi, C.flags, C.status);
     }
     const int kind = j >= 0 ? rows.kind[j] : K_NULL;
-    kind_out = kind;
     if (kind == K_NULL) return OUT_NONE;
+    int out;
     if constexpr (sizeof(T) == 8) {
         Sec<double> s64;
         double a = vx, b = vy, c = vz;
-        const int out = collide64(kind, (double)rows.par[j], eng, rng, a, b, c, s64);
+        out = collide64(kind, (double)rows.par[j], eng, rng, a, b, c, s64);
         vx = a; vy = b; vz = c;
         sec.vx = s64.vx; sec.vy = s64.vy; sec.vz = s64.vz; sec.s = s64.s;
-        return out;
     } else {
         Sec<float> s32;
         float a = vx, b = vy, c = vz;
-        const int out = collide32(kind, (float)rows.par[j], v2, rng, a, b, c, s32);
+        out = collide32(kind, (float)rows.par[j], v2, rng, a, b, c, s32);
         vx = a; vy = b; vz = c;
         sec.vx = s32.vx; sec.vy = s32.vy; sec.vz = s32.vz; sec.s = s32.s;
-        return out;
     }
+    return out == OUT_NONE ? OUT_CHANGE : out;
 }
 
+// ---------------------------------------------------------------------------------------
+// Absolute-position step (swarms, cylindrical parity mode, 3-D field on absolute positions).
+// CLOSED: uniform-field FP32 fast path.  The Yoshida composition is exact for a constant
+// force (its drift coefficients sum to 1 and its drift-kick weight is 1/2), so the trajectory
+// between real collisions is x0 + v0*tau + a*tau^2/2 and null sub-steps cost no push; the
+// sub-step sequence, draws and decisions are those of advance!.
+// ---------------------------------------------------------------------------------------
+template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
+__global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab, GridView fgrid, GridView tgrid,
+                                                    StepCtl C, Field field, YoshidaC Y, double ax, double ay,
+                                                    double az) {
+    constexpr int TILE = BLOCK * PPT;
+    __shared__ TileShared<T, BLOCK, TILE> sh;
+    load_rows(sh.rows, tab);
+    Stage<T> sg;
+    sg.init(C);
+    const long long n_entry = *P.n_in;
+    const long long ntiles = (n_entry + TILE - 1) / TILE;
+    const bool tracking = tgrid.type != 0 && tgrid.qfixed != nullptr;
+
+    for (;;) {
+        const long long tile = next_tile(sh, C, ntiles);
+        if (tile < 0) break;
+        const long long base = tile * TILE;
+
+#pragma unroll 1
+        for (int jj = 0; jj < PPT; ++jj) {
+            const uint32_t local = jj * BLOCK + threadIdx.x;
+            const long long i = base + local;
+            uint32_t ev = 0;
+            if (i < n_entry && P.act[i]) {
+                Rng rng;
+                rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
+                T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
+                const T w = P.f[6][i];
+                double s = (double)P.f[7][i];
+                uint8_t act = 1;
+                double trem = C.dt;
+                float tau = 0.0f;  // CLOSED: time since the last real collision
+                while (trem > 0) {
+                    double tn, t;
+                    if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
+                    else tn = s * tab.inv_maxrate;
+                    bool collides;
+                    if (trem > tn) { t = tn; collides = true; }
+                    else { t = trem; collides = false; s -= t * tab.maxrate; }
+                    if constexpr (CLOSED) {
+                        tau += (float)t;
+                    } else {
+                        // advance_free_yoshida, JuMC/src/electron.jl:51-62
+                        T ex, ey, ez;
+                        T x1 = x + (T)(Y.c1 * t) * vx, y1 = y + (T)(Y.c1 * t) * vy, z1 = z + (T)(Y.c1 * t) * vz;
+                        field(fgrid, x1, y1, z1, ex, ey, ez, C.status);
+                        const T k1 = (T)((Y.d1 * t) * Y.qm);
+                        T vx1 = vx + k1 * ex, vy1 = vy + k1 * ey, vz1 = vz + k1 * ez;
+                        T x2 = x1 + (T)(Y.c2 * t) * vx1, y2 = y1 + (T)(Y.c2 * t) * vy1, z2 = z1 + (T)(Y.c2 * t) * vz1;
+                        field(fgrid, x2, y2, z2, ex, ey, ez, C.status);
+                        const T k2 = (T)((Y.d2 * t) * Y.qm);
+                        T vx2 = vx1 + k2 * ex, vy2 = vy1 + k2 * ey, vz2 = vz1 + k2 * ez;
+                        T x3 = x2 + (T)(Y.c3 * t) * vx2, y3 = y2 + (T)(Y.c3 * t) * vy2, z3 = z2 + (T)(Y.c3 * t) * vz2;
+                        field(fgrid, x3, y3, z3, ex, ey, ez, C.status);
+                        const T k3 = (T)((Y.d3 * t) * Y.qm);
+                        vx = vx2 + k3 * ex; vy = vy2 + k3 * ey; vz = vz2 + k3 * ez;
+                        x = x3 + (T)(Y.c4 * t) * vx; y = y3 + (T)(Y.c4 * t) * vy; z = z3 + (T)(Y.c4 * t) * vz;
+                    }
+                    if (collides) {
+                        // do_one_collision!, collisions.jl:159-192
+                        T cvx = vx, cvy = vy, cvz = vz;
+                        if constexpr (CLOSED) {
+                            cvx = fmaf((float)ax, tau, (float)vx);
+                            cvy = fmaf((float)ay, tau, (float)vy);
+                            cvz = fmaf((float)az, tau, (float)vz);
+                        }
+                        Sec<T> sec;
+                        const int out = collide_once<T>(sh.rows, tab, C, rng, cvx, cvy, cvz, sec);
+                        if (out != OUT_NONE) {
+                            if constexpr (CLOSED) {  // settle the segment at the collision time
+                                const float h2 = 0.5f * tau * tau;
+                                x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
+                                y = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
+                                z = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
+                                tau = 0.0f;
+                            }
+                            vx = cvx; vy = cvy; vz = cvz;
+                        }
+                        if (out == OUT_NEW) {
+                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
+                            const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
+                            stage(sg, &sh.count, local, ev++, vals, 0u, act, C.status);
+                        } else if (out == OUT_REMOVE) {
+                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
+                            act = 0;  // the particle keeps sub-stepping (mixed_population.jl:32)
+                        }
+                        if constexpr (sizeof(T) == 8) s = -log(rng.u64());
+                        else s = (double)M<float>::nlog(rng.u32());
+                    }
+                    trem -= t;
+                }
+                if constexpr (CLOSED) {
+                    const float h2 = 0.5f * tau * tau;
+                    x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
+                    y = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
+                    z = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
+                    vx = fmaf((float)ax, tau, (float)vx);
+                    vy = fmaf((float)ay, tau, (float)vy);
+                    vz = fmaf((float)az, tau, (float)vz);
+                }
+                P.f[0][i] = x; P.f[1][i] = y; P.f[2][i] = z;
+                P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
+                P.f[7][i] = (T)s;
+                if (!act) P.act[i] = 0;
+            }
+            sh.cnt[local] = ev;
+        }
+        __syncthreads();
+
+        const uint32_t cnt = tile_append<T, BLOCK, TILE>(
+            sh, sg, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) P.f[q][dst] = sg.f[q][e];
+                P.act[dst] = sg.act[e];
+            });
+
+        if (C.moments_out) {
+            MomAcc<T> acc;
+            acc.zero();
+            for (int jj = 0; jj < PPT; ++jj) {
+                const long long i = base + jj * BLOCK + threadIdx.x;
+                if (i < n_entry && P.act[i])
+                    acc.add(P.f[0][i], P.f[1][i], P.f[2][i], P.f[3][i], P.f[4][i], P.f[5][i], P.f[6][i]);
+            }
+            for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)
+                if (sg.act[e])
+                    acc.add(sg.f[0][e], sg.f[1][e], sg.f[2][e], sg.f[3][e], sg.f[4][e], sg.f[5][e], sg.f[6][e]);
+            block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
+        }
+        __syncthreads();
+    }
+    grid_epilogue<BLOCK>(sh, C, ntiles, n_entry, P.n_out);
+}
+
+// ---------------------------------------------------------------------------------------
 // collisions!(mpopl, dt, tracker): JuMC/src/mixed_population.jl:61-77 (no push).
+// ---------------------------------------------------------------------------------------
 template <typename T, int BLOCK, int PPT>
 __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView tab, GridView tgrid, StepCtl C) {
     constexpr int TILE = BLOCK * PPT;
-    constexpr int SCAP = TILE;
-    __shared__ TileShared<T, BLOCK, SCAP> sh;
+    __shared__ TileShared<T, BLOCK, TILE> sh;
     load_rows(sh.rows, tab);
+    Stage<T> sg;
+    sg.init(C);
     const long long n_entry = *P.n_in;
     const long long ntiles = (n_entry + TILE - 1) / TILE;
     const bool tracking = tgrid.type != 0 && tgrid.qfixed != nullptr;
     for (;;) {
-        if (threadIdx.x == 0) {
-            sh.tile = atomicAdd(&C.counters[0], 1u);
-            sh.st.count = 0;
-        }
-        __syncthreads();
-        const long long tile = sh.tile;
-        if (tile >= ntiles) break;
+        const long long tile = next_tile(sh, C, ntiles);
+        if (tile < 0) break;
         const long long base = tile * TILE;
         for (int jj = 0; jj < PPT; ++jj) {
             const uint32_t local = jj * BLOCK + threadIdx.x;
             const long long i = base + local;
-            if (i >= n_entry || !P.act[i]) continue;
-            double s = (double)P.f[7][i] - C.dt * tab.maxrate;
-            if (s <= 0) {
-                Rng rng;
-                rng.init(C.seed, (uint32_t)i, C.step, C.tag);
-                const T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
-                T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
-                const T w = P.f[6][i];
-                Sec<T> sec;
-                int kind;
-                const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec, kind);
-                if (out == OUT_NEW) {
-                    if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
-                    const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
-                    stage(sh.st, local, 0u, vals, 0u, (uint8_t)1, C.status);
-                } else if (out == OUT_REMOVE) {
-                    if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
-                    P.act[i] = 0;
+            uint32_t ev = 0;
+            if (i < n_entry && P.act[i]) {
+                double s = (double)P.f[7][i] - C.dt * tab.maxrate;
+                if (s <= 0) {
+                    Rng rng;
+                    rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                    const T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
+                    T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
+                    const T w = P.f[6][i];
+                    Sec<T> sec;
+                    const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
+                    if (out == OUT_NEW) {
+                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
+                        const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
+                        stage(sg, &sh.count, local, ev++, vals, 0u, (uint8_t)1, C.status);
+                    } else if (out == OUT_REMOVE) {
+                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
+                        P.act[i] = 0;
+                    }
+                    if constexpr (sizeof(T) == 8) s = -log(rng.u64());
+                    else s = (double)M<float>::nlog(rng.u32());
+                    P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
                 }
-                if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                else s = (double)M<float>::nlog(rng.u32());
-                P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
+                P.f[7][i] = (T)s;
             }
-            P.f[7][i] = (T)s;
+            sh.cnt[local] = ev;
         }
         __syncthreads();
-        tile_append<T, BLOCK, SCAP>(sh, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
+        tile_append<T, BLOCK, TILE>(sh, sg, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
 #pragma unroll
-            for (int q = 0; q < 8; ++q) P.f[q][dst] = sh.st.f[q][e];
-            P.act[dst] = sh.st.act[e];
+            for (int q = 0; q < 8; ++q) P.f[q][dst] = sg.f[q][e];
+            P.act[dst] = sg.act[e];
         });
         __syncthreads();
     }
     grid_epilogue<BLOCK>(sh, C, ntiles, n_entry, P.n_out);
 }
 
-}  // namespace mcs
-
-namespace mcs {
-
-constexpr uint32_t kOutsideCell = 0xffffffffu;
-
-// Trilinear field of one cell as a polynomial in the in-cell offset f in [0,1)^3:
-//   E(f) = a + fx*(bx + fy*(bxy + fz*bxyz) + fz*bxz) + fy*(by + fz*byz) + fz*bz
-// (24 coefficients held in registers while the particle stays in the cell).
+// ---------------------------------------------------------------------------------------
+// 3-D mesh layout.  The trilinear field of one cell as a polynomial in the in-cell offset
+// f in [0,1)^3:  E(f) = a + fx*(bx + fy*(bxy + fz*bxyz) + fz*bxz) + fy*(by + fz*byz) + fz*bz,
+// 24 coefficients held in registers while the particle stays in the cell.
+// ---------------------------------------------------------------------------------------
 template <typename T>
 struct CellField {
     T a[3], bx[3], by[3], bz[3], bxy[3], bxz[3], byz[3], bxyz[3];
@@ -438,7 +451,7 @@ struct CellField {
     }
 };
 
-// Node field of cell (ix,iy,iz): corners in the order (x fastest) 000,100,010,110,001,...
+// Node field of cell (ix,iy,iz): corners 000,100,010,110,001,101,011,111 (x fastest).
 template <typename T>
 __device__ __forceinline__ void load_cell_field(const GridView& g, int ix, int iy, int iz, CellField<T>& cf) {
     const long long sy = g.nx + 1, sz = (long long)(g.nx + 1) * (g.ny + 1);
@@ -461,7 +474,7 @@ __device__ __forceinline__ void load_cell_field(const GridView& g, int ix, int i
     cf.set(e);
 }
 
-// Renormalise (cell, offset) after a drift; returns true when the cell changed.
+// Renormalise (cell, offset) after a drift; returns true when the field must be reloaded.
 // Inside the mesh the offset is in [0,1) of cell (ix,iy,iz); outside (in == false) the
 // offset holds the absolute position in cell units and the field is zero.
 template <typename T>
@@ -472,28 +485,31 @@ __device__ __forceinline__ bool relocate(const GridView& g, int& ix, int& iy, in
     if (!in) { ic[0] = ic[1] = ic[2] = 0; }
     bool inside = true;
     const int nc[3] = {g.nx, g.ny, g.nz};
+    double cd[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         T fl = floor(o[d]);
         T r = o[d] - fl;
         if (r >= (T)1) { r -= (T)1; fl += (T)1; }
-        const double cd = (double)ic[d] + (double)fl;
-        inside = inside && cd >= 0.0 && cd < (double)nc[d];
-        ic[d] = (int)fmax(-2e9, fmin(2e9, cd));
+        cd[d] = (double)ic[d] + (double)fl;
+        inside = inside && cd[d] >= 0.0 && cd[d] < (double)nc[d];
         o[d] = r;
     }
     if (inside) {
-        ix = ic[0]; iy = ic[1]; iz = ic[2];
+        ix = (int)cd[0]; iy = (int)cd[1]; iz = (int)cd[2];
         ox = o[0]; oy = o[1]; oz = o[2];
     } else {
-        // absolute position in cell units
-        ox = (T)((double)ic[0] + (double)o[0]);
-        oy = (T)((double)ic[1] + (double)o[1]);
-        oz = (T)((double)ic[2] + (double)o[2]);
+        ox = (T)(cd[0] + (double)o[0]);
+        oy = (T)(cd[1] + (double)o[1]);
+        oz = (T)(cd[2] + (double)o[2]);
     }
-    const bool changed = inside != in || inside;
+    const bool reload = inside || in;
     in = inside;
-    return changed;
+    return reload;
+}
+
+__device__ __forceinline__ uint32_t cell_index(const GridView& g, bool in, int ix, int iy, int iz) {
+    return in ? (uint32_t)ix + (uint32_t)g.nx * ((uint32_t)iy + (uint32_t)g.ny * (uint32_t)iz) : kOutsideCell;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -505,9 +521,10 @@ template <typename T, int BLOCK, int PPT>
 __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
                                                      YoshidaC Y, double dep_val) {
     constexpr int TILE = BLOCK * PPT;
-    constexpr int SCAP = TILE;
-    __shared__ TileShared<T, BLOCK, SCAP> sh;
+    __shared__ TileShared<T, BLOCK, TILE> sh;
     load_rows(sh.rows, tab);
+    Stage<T> sg;
+    sg.init(C);
     const long long n_entry = *P.n_in;
     const long long ntiles = (n_entry + TILE - 1) / TILE;
     // drift / kick factors per unit time: offsets in cell units, velocities in m/s
@@ -515,120 +532,110 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
     const T kd1 = (T)(Y.d1 * Y.qm), kd2 = (T)(Y.d2 * Y.qm), kd3 = (T)(Y.d3 * Y.qm);
 
     for (;;) {
-        if (threadIdx.x == 0) {
-            sh.tile = atomicAdd(&C.counters[0], 1u);
-            sh.st.count = 0;
-        }
-        __syncthreads();
-        const long long tile = sh.tile;
-        if (tile >= ntiles) break;
+        const long long tile = next_tile(sh, C, ntiles);
+        if (tile < 0) break;
         const long long base = tile * TILE;
 
 #pragma unroll 1
         for (int jj = 0; jj < PPT; ++jj) {
             const uint32_t local = jj * BLOCK + threadIdx.x;
             const long long i = base + local;
-            if (i >= n_entry || !P.act[i]) continue;
-            Rng rng;
-            rng.init(C.seed, (uint32_t)i, C.step, C.tag);
-            const uint32_t cell0 = P.cell[i];
-            T ox = P.f[0][i], oy = P.f[1][i], oz = P.f[2][i];
-            T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
-            const T w = P.f[6][i];
-            double s = (double)P.f[7][i];
-            bool in = cell0 != kOutsideCell;
-            int ix = 0, iy = 0, iz = 0;
-            CellField<T> cf;
-            if (in) {
-                ix = (int)(cell0 % (uint32_t)g.nx);
-                const uint32_t r = cell0 / (uint32_t)g.nx;
-                iy = (int)(r % (uint32_t)g.ny);
-                iz = (int)(r / (uint32_t)g.ny);
-                load_cell_field(g, ix, iy, iz, cf);
-            } else {
-                cf.zero();
-            }
-            uint8_t act = 1;
             uint32_t ev = 0;
-            double trem = C.dt;
-            auto drift = [&](T c) {
-                ox += c * vx; oy += c * vy; oz += c * vz;
-                if (relocate(g, ix, iy, iz, in, ox, oy, oz)) {
-                    if (in) load_cell_field(g, ix, iy, iz, cf);
-                    else cf.zero();
+            if (i < n_entry && P.act[i]) {
+                Rng rng;
+                rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                const uint32_t cell0 = P.cell[i];
+                T ox = P.f[0][i], oy = P.f[1][i], oz = P.f[2][i];
+                T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
+                const T w = P.f[6][i];
+                double s = (double)P.f[7][i];
+                bool in = cell0 != kOutsideCell;
+                int ix = 0, iy = 0, iz = 0;
+                CellField<T> cf;
+                if (in) {
+                    ix = (int)(cell0 % (uint32_t)g.nx);
+                    const uint32_t r = cell0 / (uint32_t)g.nx;
+                    iy = (int)(r % (uint32_t)g.ny);
+                    iz = (int)(r / (uint32_t)g.ny);
+                    load_cell_field(g, ix, iy, iz, cf);
+                } else {
+                    cf.zero();
                 }
-            };
-            auto kick = [&](T k) {
-                T ex, ey, ez;
-                cf.eval(ox, oy, oz, ex, ey, ez);
-                vx += k * ex; vy += k * ey; vz += k * ez;
-            };
-            while (trem > 0) {
-                double tn, t;
-                if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
-                else tn = s * tab.inv_maxrate;
-                bool collides;
-                if (trem > tn) { t = tn; collides = true; }
-                else { t = trem; collides = false; s -= t * tab.maxrate; }
-                const T tt = (T)t;
-                // advance_free_yoshida (electron.jl:51-62) in cell units
-                drift(cd1 * tt);
-                kick(kd1 * tt);
-                drift(cd2 * tt);
-                kick(kd2 * tt);
-                drift(cd3 * tt);
-                kick(kd3 * tt);
-                drift(cd4 * tt);
-                if (collides) {
-                    Sec<T> sec;
-                    int kind;
-                    const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec, kind);
-                    if (out != OUT_NONE && tracking && in)
-                        cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
-                                  out == OUT_NEW ? (double)w : -(double)w);
-                    if (out == OUT_NEW) {
-                        const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
-                        const uint32_t cl = in ? (uint32_t)ix + (uint32_t)g.nx * ((uint32_t)iy + (uint32_t)g.ny * (uint32_t)iz)
-                                               : kOutsideCell;
-                        if (ev >= 255) atomicOr(C.status, ST_OVERFLOW);
-                        stage(sh.st, local, ev++, vals, cl, act, C.status);
-                    } else if (out == OUT_REMOVE) {
-                        act = 0;
+                uint8_t act = 1;
+                double trem = C.dt;
+                auto drift = [&](T c) {
+                    ox += c * vx; oy += c * vy; oz += c * vz;
+                    if (relocate(g, ix, iy, iz, in, ox, oy, oz)) {
+                        if (in) load_cell_field(g, ix, iy, iz, cf);
+                        else cf.zero();
                     }
-                    if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                    else s = (double)M<float>::nlog(rng.u32());
+                };
+                auto kick = [&](T k) {
+                    T ex, ey, ez;
+                    cf.eval(ox, oy, oz, ex, ey, ez);
+                    vx += k * ex; vy += k * ey; vz += k * ez;
+                };
+                while (trem > 0) {
+                    double tn, t;
+                    if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
+                    else tn = s * tab.inv_maxrate;
+                    bool collides;
+                    if (trem > tn) { t = tn; collides = true; }
+                    else { t = trem; collides = false; s -= t * tab.maxrate; }
+                    const T tt = (T)t;
+                    // advance_free_yoshida (electron.jl:51-62) in cell units
+                    drift(cd1 * tt);
+                    kick(kd1 * tt);
+                    drift(cd2 * tt);
+                    kick(kd2 * tt);
+                    drift(cd3 * tt);
+                    kick(kd3 * tt);
+                    drift(cd4 * tt);
+                    if (collides) {
+                        Sec<T> sec;
+                        const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
+                        if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
+                            cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
+                                      out == OUT_NEW ? (double)w : -(double)w);
+                        if (out == OUT_NEW) {
+                            const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
+                            stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
+                        } else if (out == OUT_REMOVE) {
+                            act = 0;
+                        }
+                        if constexpr (sizeof(T) == 8) s = -log(rng.u64());
+                        else s = (double)M<float>::nlog(rng.u32());
+                    }
+                    trem -= t;
                 }
-                trem -= t;
+                P.cell[i] = cell_index(g, in, ix, iy, iz);
+                P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;
+                P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
+                P.f[7][i] = (T)s;
+                if (!act) P.act[i] = 0;
+                if (dep_val != 0.0 && act && in)
+                    cic_fixed(g.qpart, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz, (double)w * dep_val);
             }
-            const uint32_t cl = in ? (uint32_t)ix + (uint32_t)g.nx * ((uint32_t)iy + (uint32_t)g.ny * (uint32_t)iz)
-                                   : kOutsideCell;
-            P.cell[i] = cl;
-            P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;
-            P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
-            P.f[7][i] = (T)s;
-            if (!act) P.act[i] = 0;
-            if (dep_val != 0.0 && act && in)
-                cic_fixed(g.qpart, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz, (double)w * dep_val);
+            sh.cnt[local] = ev;
         }
         __syncthreads();
 
-        const uint32_t cnt = tile_append<T, BLOCK, SCAP>(
-            sh, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
+        const uint32_t cnt = tile_append<T, BLOCK, TILE>(
+            sh, sg, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) P.f[q][dst] = sh.st.f[q][e];
-                P.cell[dst] = sh.st.cell[e];
-                P.act[dst] = sh.st.act[e];
+                for (int q = 0; q < 8; ++q) P.f[q][dst] = sg.f[q][e];
+                P.cell[dst] = sg.cell[e];
+                P.act[dst] = sg.act[e];
             });
-        // secondaries are deposited too (they are part of the post-step population)
+        // secondaries are part of the post-step population: deposit them too
         if (dep_val != 0.0) {
             for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
-                const uint32_t cl = sh.st.cell[e];
-                if (!sh.st.act[e] || cl == kOutsideCell) continue;
+                const uint32_t cl = sg.cell[e];
+                if (!sg.act[e] || cl == kOutsideCell) continue;
                 const int ex = (int)(cl % (uint32_t)g.nx);
                 const uint32_t r = cl / (uint32_t)g.nx;
                 cic_fixed(g.qpart, g.nx, g.ny, ex, (int)(r % (uint32_t)g.ny), (int)(r / (uint32_t)g.ny),
-                          (double)sh.st.f[0][e], (double)sh.st.f[1][e], (double)sh.st.f[2][e],
-                          (double)sh.st.f[6][e] * dep_val);
+                          (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], (double)sg.f[6][e] * dep_val);
             }
         }
         __syncthreads();

@@ -6,6 +6,27 @@
 
 namespace mcs {
 
+// Secondary staging of one launch: `grid` CTAs, each with room for 4*TILE + 2048 entries
+// (eight or more secondaries per particle and step before MCS_ERR_OVERFLOW).
+template <typename T, int TILE>
+int attach_stage(mcs_pop* p, int grid, StepCtl& C) {
+    const uint32_t cap = 4 * TILE + 2048;
+    const size_t stride = ((size_t)cap * (8 * sizeof(T) + 9) + 255) & ~(size_t)255;
+    const size_t bytes = stride * (size_t)grid;
+    if (p->stage_bytes < bytes) {
+        if (p->stage) cudaFree(p->stage);
+        p->stage = nullptr;
+        p->stage_bytes = 0;
+        cudaError_t e = cudaMalloc(&p->stage, bytes);
+        if (e != cudaSuccess) return set_err(p->ctx, MCS_ERR_NOMEM, std::string("staging: ") + cudaGetErrorString(e));
+        p->stage_bytes = bytes;
+    }
+    C.stage = static_cast<char*>(p->stage);
+    C.stage_stride = stride;
+    C.stage_cap = cap;
+    return MCS_OK;
+}
+
 template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
 int launch_abs_variant(mcs_pop* p, const mcs_table* t, const GridView& fg, const GridView& tg, const Field& fld,
                        double dt, double ax, double ay, double az, double* mom) {
@@ -17,6 +38,7 @@ int launch_abs_variant(mcs_pop* p, const mcs_table* t, const GridView& fg, const
     YoshidaHost yh;
     YoshidaC Y{yh.c1, yh.c2, yh.c3, yh.c4, yh.d1, yh.d2, yh.d3, (-kElementaryCharge) / kElectronMass};
     StepCtl C = step_ctl(p, dt, TAG_ADVANCE, mom);
+    if (int st = attach_stage<T, TILE>(p, grid, C)) return st;
     kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, fg, tg, C, fld, Y, ax, ay, az);
     MCS_CK_LAUNCH(c);
     return MCS_OK;
@@ -43,12 +65,28 @@ int launch_step_abs_impl(mcs_pop* p, const mcs_table* t, const mcs_field* f, dou
 }
 
 template <typename T, int BLOCK, int PPT>
+int launch_step_mesh_impl(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
+    mcs_ctx* c = p->ctx;
+    constexpr int TILE = BLOCK * PPT;
+    auto kern = k_step_mesh<T, BLOCK, PPT>;
+    const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
+    YoshidaHost yh;
+    YoshidaC Y{yh.c1, yh.c2, yh.c3, yh.c4, yh.d1, yh.d2, yh.d3, (-kElementaryCharge) / kElectronMass};
+    StepCtl C = step_ctl(p, dt, TAG_ADVANCE, mom);
+    if (int st = attach_stage<T, TILE>(p, grid, C)) return st;
+    kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, p->cells->v, tracking ? 1 : 0, C, Y, dep_val);
+    MCS_CK_LAUNCH(c);
+    return MCS_OK;
+}
+
+template <typename T, int BLOCK, int PPT>
 int launch_collisions_impl(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* trk) {
     mcs_ctx* c = p->ctx;
     constexpr int TILE = BLOCK * PPT;
     auto kern = k_collisions<T, BLOCK, PPT>;
     const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
     StepCtl C = step_ctl(p, dt, TAG_COLLISIONS, nullptr);
+    if (int st = attach_stage<T, TILE>(p, grid, C)) return st;
     kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, grid_view(trk), C);
     MCS_CK_LAUNCH(c);
     return MCS_OK;

@@ -142,7 +142,7 @@ class Population:
         prec = L.FP32 if precision == "fp32" else L.FP64
         h = C.c_void_p()
         self.ctx.check(self.ctx.lib.mcs_pop_create(self.ctx.h, self.capacity, prec,
-                                                   mesh.h if mesh is not None else None, C.byref(h)))
+                                                   mesh.h_ if mesh is not None else None, C.byref(h)))
         self.h = h
         self.mesh = mesh
         self.set_seed(seed, step)

@@ -1,0 +1,180 @@
+"""Python mirror of MCStreamer's particle-side call sites over the C ABI.
+
+* Grid3D: the 3-D uniform node mesh of the streamer workloads (node field, CIC int64
+  charge at 2^-32 e).  GridCyl: the reference's cylindrical Grid(R, L, M, N)
+  (MCStreamer/src/grid.jl:4-42) with its staggered face field.
+* FieldInterp(grid): the `efield` callable (gridfields.jl:89-190); CollisionTracker(grid):
+  the tracker of gridfields.jl:198-224 (qfixed); density(grid, popl, val): density!
+  (poisson.jl:65-84) into qpart.
+* advance_deposit: advance! + density! of the post-step state in one kernel.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+from scipy.special import erf
+
+from . import _lib as L
+from . import constants as co
+from .jumc import Context, Population
+
+
+class Grid3D:
+    """nx*ny*nz cubic cells of side h with lower corner `origin`; nodes (nx+1)(ny+1)(nz+1)."""
+
+    # the C handle is .h_ (.h is the cell size)
+    def __init__(self, nx: int, ny: int, nz: int, h: float, origin: Sequence[float] = (0.0, 0.0, 0.0),
+                 precision: str = "fp32", ctx: Optional[Context] = None):
+        self.ctx = ctx or Context.default()
+        self.nx, self.ny, self.nz, self.h = int(nx), int(ny), int(nz), float(h)
+        self.origin = tuple(float(o) for o in origin)
+        self.precision = precision
+        hd = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_grid_create_cart3d(
+            self.ctx.h, self.nx, self.ny, self.nz, self.h, *self.origin,
+            L.FP32 if precision == "fp32" else L.FP64, C.byref(hd)))
+        self.h_ = hd
+
+    @property
+    def nnodes(self) -> int:
+        return (self.nx + 1) * (self.ny + 1) * (self.nz + 1)
+
+    @property
+    def shape_nodes(self):
+        return (self.nz + 1, self.ny + 1, self.nx + 1)
+
+    def node_coords(self, k0: int, k1: int):
+        """Coordinates of nodes with z-plane index in [k0, k1), x fastest."""
+        x = self.origin[0] + self.h * np.arange(self.nx + 1)
+        y = self.origin[1] + self.h * np.arange(self.ny + 1)
+        z = self.origin[2] + self.h * np.arange(k0, k1)
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        return X.ravel(), Y.ravel(), Z.ravel()
+
+    def set_efield(self, e: np.ndarray) -> None:
+        e = np.ascontiguousarray(e, dtype=np.float64).reshape(-1)
+        assert e.size == 3 * self.nnodes
+        self.ctx.check(self.ctx.lib.mcs_grid_set_efield(self.h_, L.dptr(e)))
+
+    def set_efield_fn(self, fn, planes_per_chunk: int = 16) -> None:
+        """Fill the node field plane by plane from fn(x, y, z) -> (n, 3)."""
+        plane = (self.nx + 1) * (self.ny + 1)
+        for k0 in range(0, self.nz + 1, planes_per_chunk):
+            k1 = min(self.nz + 1, k0 + planes_per_chunk)
+            x, y, z = self.node_coords(k0, k1)
+            e = np.ascontiguousarray(fn(x, y, z), dtype=np.float64)
+            self.ctx.check(self.ctx.lib.mcs_grid_set_efield_range(self.h_, k0 * plane, (k1 - k0) * plane,
+                                                                  L.dptr(e)))
+
+    def zero(self, which: int = L.Q_PART) -> None:
+        self.ctx.check(self.ctx.lib.mcs_grid_zero(self.h_, which))
+
+    def read_fixed(self, which: int = L.Q_PART) -> np.ndarray:
+        out = np.zeros(self.nnodes, dtype=np.int64)
+        self.ctx.check(self.ctx.lib.mcs_grid_read_fixed(self.h_, which, L.i64ptr(out)))
+        return out
+
+    def cell_key(self, x: np.ndarray) -> np.ndarray:
+        u = (np.asarray(x) - np.asarray(self.origin)) / self.h
+        fl = np.floor(u).astype(np.int64)
+        inside = np.all((fl >= 0) & (fl < np.array([self.nx, self.ny, self.nz])), axis=1)
+        key = fl[:, 0] + self.nx * (fl[:, 1] + self.ny * fl[:, 2])
+        return np.where(inside, key, np.iinfo(np.int64).max)
+
+    def close(self) -> None:
+        if self.h_:
+            self.ctx.lib.mcs_grid_destroy(self.h_)
+            self.h_ = None
+
+
+class GridCyl:
+    """Cylindrical Grid(R, L, M, N) (MCStreamer/src/grid.jl:4-42)."""
+
+    def __init__(self, R: float, L_: float, M: int, N: int, ctx: Optional[Context] = None):
+        self.ctx = ctx or Context.default()
+        self.R, self.L, self.M, self.N = float(R), float(L_), int(M), int(N)
+        hd = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_grid_create_cyl(self.ctx.h, self.R, self.L, self.M, self.N, C.byref(hd)))
+        self.h_ = hd
+
+    def set_efield(self, er: np.ndarray, ez: np.ndarray) -> None:
+        """er, ez: (M+3, N+3) face arrays, index (i, j) from 0 (calloc_faces, grid.jl:71-72)."""
+        e = np.concatenate([np.asarray(er, np.float64).T.ravel(), np.asarray(ez, np.float64).T.ravel()])
+        self.ctx.check(self.ctx.lib.mcs_grid_set_efield(self.h_, L.dptr(np.ascontiguousarray(e))))
+
+    def zero(self, which: int = L.Q_PART) -> None:
+        self.ctx.check(self.ctx.lib.mcs_grid_zero(self.h_, which))
+
+    def read_density(self, which: int = L.Q_PART) -> np.ndarray:
+        out = np.zeros((self.M + 2) * (self.N + 2))
+        self.ctx.check(self.ctx.lib.mcs_grid_read_density(self.h_, which, L.dptr(out)))
+        return out.reshape(self.N + 2, self.M + 2).T   # (i, j) like calloc_centers
+
+    def close(self) -> None:
+        if self.h_:
+            self.ctx.lib.mcs_grid_destroy(self.h_)
+            self.h_ = None
+
+
+def _handle(g):
+    return g.h_ if g is not None else None
+
+
+class FieldInterp:
+    """FieldInterp (gridfields.jl:89-190): the field stored on a grid."""
+
+    def __init__(self, grid):
+        self.grid = grid
+        self.ctx = grid.ctx
+        hd = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_field_from_grid(grid.h_, C.byref(hd)))
+        self.h = hd
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.mcs_field_destroy(self.h)
+            self.h = None
+
+
+class CollisionTracker:
+    """CollisionTracker (gridfields.jl:198-224): +w per ionization, -w per attachment."""
+
+    def __init__(self, grid):
+        self.grid = grid
+        self.h = grid.h_
+
+
+def density(grid, popl: Population, val: float = 1.0) -> None:
+    """density!(grid, arr=qpart, mpopl, Electron, fields, val) (poisson.jl:65-84)."""
+    popl.ctx.check(popl.ctx.lib.mcs_deposit(popl.h, grid.h_, float(val)))
+
+
+def advance_deposit(popl: Population, efield: FieldInterp, dt: float, tracker: Optional[CollisionTracker],
+                    grid: Grid3D, val: float = -1.0) -> None:
+    """advance!(...) then density!(qpart, val) of the post-step particles, one kernel."""
+    popl.ctx.check(popl.ctx.lib.mcs_advance_deposit(popl.h, popl.collisions.h, efield.h, dt,
+                                                    tracker.h if tracker is not None else None, grid.h_,
+                                                    float(val)))
+
+
+# ---------------------------------------------------------------------------------------
+# Field of the streamer workloads: a uniform background plus a Gaussian charge cloud.
+# ---------------------------------------------------------------------------------------
+def gaussian_charge_field(centre: Sequence[float], sigma: float, rho_peak_e: float, e_bg=(0.0, 0.0, -15e6)):
+    """E = e_bg + Q(r)/(4 pi eps0 r^2) r_hat for rho = e*rho_peak_e*exp(-r^2/2sigma^2):
+    Q(r) = e*rho_peak_e*(2 pi sigma^2)^(3/2) [erf(r/(sqrt2 sigma)) - sqrt(2/pi)(r/sigma) exp(-r^2/2sigma^2)]."""
+    cx, cy, cz = centre
+    q0 = co.elementary_charge * rho_peak_e * (2 * np.pi * sigma ** 2) ** 1.5
+
+    def fn(x, y, z):
+        dx, dy, dz = x - cx, y - cy, z - cz
+        r = np.sqrt(dx * dx + dy * dy + dz * dz)
+        rs = r / sigma
+        Q = q0 * (erf(rs / np.sqrt(2)) - np.sqrt(2 / np.pi) * rs * np.exp(-0.5 * rs * rs))
+        with np.errstate(invalid="ignore", divide="ignore"):
+            f = np.where(r > 0, Q / (4 * np.pi * co.epsilon_0 * r ** 3), 0.0)
+        return np.stack([e_bg[0] + f * dx, e_bg[1] + f * dy, e_bg[2] + f * dz], axis=1)
+
+    return fn

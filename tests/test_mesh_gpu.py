@@ -1,0 +1,129 @@
+"""Streamer step on the 3-D mesh (cell + offset layout) against the CPU oracle:
+trilinear node-field gather, Yoshida push, collisions, collision tracker (int64 CIC into
+qfixed) and the fused particle deposit (int64 CIC into qpart)."""
+import numpy as np
+import pytest
+
+from mcstreamer_b200 import _lib as L
+from mcstreamer_b200 import constants as co
+from mcstreamer_b200 import jumc, lxcat, streamer
+from oracle import pyoracle as po
+from tests.helpers import broad, oracle_arrays, oracle_pop, particle_mismatch, vec_relerr
+
+NX, NY, NZ, H = 16, 16, 32, 4e-6
+CENTRE = (NX * H / 2, NY * H / 2, NZ * H / 2)
+
+
+def _field_nodes(grid):
+    fn = streamer.gaussian_charge_field(CENTRE, 10e-6, 2e21, e_bg=(0.0, 0.0, -15e6))
+    x, y, z = grid.node_coords(0, grid.nz + 1)
+    return fn(x, y, z)
+
+
+def _setup(ctx, n, precision, seed=21, spread=14e-6, emax_ev=120.0, weight=1e3, capf=3):
+    t = lxcat.synthetic_table(0, uniform_sharing=True)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.Grid3D(NX, NY, NZ, H, precision=precision, ctx=ctx)
+    e = _field_nodes(grid)
+    grid.set_efield(e)
+    e_or = e.astype(np.float32).astype(np.float64) if precision == "fp32" else e
+    p0 = broad(n, seed, emax_ev=emax_ev, x0=CENTRE, spread=spread)
+    p0.w[:] = weight
+    pop = jumc.Population(capf * n, p0, tab, precision=precision, seed=seed, mesh=grid)
+    otab = po.OracleTable.from_lxcat(t)
+    ofield = po.field_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0), e_or.reshape(-1))
+    return t, tab, grid, p0, pop, otab, ofield
+
+
+def _close(*objs):
+    for o in objs:
+        o.close()
+
+
+@pytest.mark.gpu
+def test_mesh_step_fp64_matches_oracle_with_tracker_and_deposit(ctx):
+    n = 32768
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp64")
+    # positions as the device holds them (cell + offset round trip)
+    p_dev = pop.download()
+    opop = oracle_pop(p_dev, 3 * n, 21)
+    trk = po.tracker_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0))
+    fld = streamer.FieldInterp(grid)
+    grid.zero(L.Q_FIXED)
+    grid.zero(L.Q_PART)
+    dt = 2e-13
+    streamer.advance_deposit(pop, fld, dt, streamer.CollisionTracker(grid), grid, -1.0)
+    assert po.advance(opop, otab, ofield, dt, tracker=trk) == 0
+    g, o = pop.download(), oracle_arrays(opop)
+    assert g.n == o.n and g.n > n
+    bad = particle_mismatch(g, o, 1e-12, xatol=1e-30, vatol=1e-30)
+    assert bad.sum() == 0, f"{bad.sum()} slots differ, worst {vec_relerr(g.x, o.x).max():.3g}"
+    qf = grid.read_fixed(L.Q_FIXED)
+    assert qf.sum() == trk._q.sum()
+    # per node: a few units of 2^-32 e from per-corner rounding of several deposits
+    assert np.abs(qf - trk._q).max() <= 8
+    # fused deposit == oracle density! of the oracle's post-step population
+    qp = grid.read_fixed(L.Q_PART)
+    dep = po.tracker_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0))
+    po.deposit(opop, dep, -1.0)
+    assert qp.sum() == dep._q.sum()
+    assert np.abs(qp - dep._q).max() <= 8
+    _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_step_fp32_within_tolerance(ctx):
+    n = 32768
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32")
+    p_dev = pop.download()
+    opop = oracle_pop(p_dev, 3 * n, 21)
+    fld = streamer.FieldInterp(grid)
+    dt = 2e-13
+    jumc.advance(pop, fld, dt)
+    assert po.advance(opop, otab, ofield, dt) == 0
+    g, o = pop.download(), oracle_arrays(opop)
+    bad = particle_mismatch(g, o, 1e-5, xatol=1e-13, vatol=1e-2, satol=1e-5, n=n)
+    assert bad.sum() / n < 2e-3, f"{bad.sum()} of {n} parents differ"
+    assert abs(g.n - o.n) <= max(8, 0.01 * (o.n - n))
+    _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_deposit_is_bit_exact(ctx):
+    n = 50000
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32", spread=20e-6)
+    rng = np.random.default_rng(3)
+    p0.w[:] = 10 ** rng.uniform(2, 4, n)
+    p0.active[::11] = 0
+    pop.upload(p0)
+    grid.zero(L.Q_PART)
+    streamer.density(grid, pop, -1.0)
+    q = grid.read_fixed(L.Q_PART)
+    dep = po.tracker_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0))
+    po.deposit(oracle_pop(p0, n, 0), dep, -1.0, quantize_f32=True)
+    np.testing.assert_array_equal(q, dep._q)
+    # total charge == sum of llrint(w * 2^32) over active in-mesh particles
+    inside = (grid.cell_key(p0.x) < np.iinfo(np.int64).max) & (p0.active == 1)
+    w32 = p0.w.astype(np.float32).astype(np.float64)
+    assert q.sum() == -np.sum(np.rint(w32[inside] * 2.0 ** 32).astype(np.int64))
+    _close(pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_particles_leaving_and_reentering(ctx):
+    """Fast particles near the faces leave the mesh (zero field outside, gridfields.jl:116)."""
+    n = 8192
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp64", spread=30e-6, emax_ev=400.0, capf=40)
+    p_dev = pop.download()
+    opop = oracle_pop(p_dev, 40 * n, 21)
+    fld = streamer.FieldInterp(grid)
+    for _ in range(6):
+        jumc.advance(pop, fld, 4e-13)
+        assert po.advance(opop, otab, ofield, 4e-13) == 0
+    g, o = pop.download(), oracle_arrays(opop)
+    outside = (grid.cell_key(o.x) == np.iinfo(np.int64).max).sum()
+    assert outside > 0
+    assert g.n == o.n
+    bad = particle_mismatch(g, o, 1e-11, xatol=1e-30, vatol=1e-30)
+    assert bad.sum() <= 2, f"{bad.sum()} slots differ"
+    _close(fld, pop, grid, tab)
