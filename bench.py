@@ -1,0 +1,416 @@
+#!/usr/bin/env python
+"""Throughput of the electron step (electron steps/s) on the streamer workload.
+
+A step is one launch of the fused streamer step over the whole population: Yoshida push
+in the trilinear node field, null-collision Monte Carlo (elastic, excitation, ionization,
+attachment), collision tracker (int64 CIC into qfixed) and the particle deposit (int64 CIC
+into qpart), preceded by zeroing qpart.  Default workload "cfg1": 128x128x256 mesh, h=4 um,
+4,194,304 particles (weight 1e3, Gaussian cloud sigma 50 um, 1 eV isotropic), synthetic
+gas 0, dt=2e-13 s, seed 1, FP32 push/sampling with FP64 time and int64 charge.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+N > 1 (torchrun, one rank per GPU): each rank steps its own shard of the cloud (same
+number of particles per rank: weak scaling) and the int64 particle-deposit grids are
+summed with an NCCL all-reduce every step, which is exact and order independent.
+--impl reference times the CPU restatement of the reference's algorithm (the oracle,
+all host threads) on a bounded sample of the same workload; only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "electron steps/s"
+UNIT = "electron-steps/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
+    ap.add_argument("--workload", default="cfg1")
+    ap.add_argument("--particles", type=int, default=None, help="override the particle count (per rank)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def alg_bytes_per_launch(n_active: float, n_sec: float, nodes: int) -> float:
+    """Algorithmic HBM bytes of one fused step launch: each active particle read once
+    (cell 4 + offset 12 + velocity 12 + w 4 + s 4 + active 1 = 37 B) and written once
+    (33 B, w unchanged), each secondary written once (37 B), the node field read once
+    (12 B per node) and the particle-charge grid read-modified-written once (16 B per node)."""
+    return n_active * 70.0 + n_sec * 37.0 + nodes * 12.0 + nodes * 16.0
+
+
+# ---------------------------------------------------------------------------------------
+class CpuSample:
+    """The oracle (FP64 CPU restatement) on a bounded sample of the workload: one step of
+    advance! with the tracker, then density! of the result, on the first M particles of
+    the same cloud (M sized so one step takes about `seconds`)."""
+
+    def __init__(self, spec, seconds: float, threads: int):
+        from mcstreamer_b200 import lxcat, workloads
+        from oracle import pyoracle as po
+        self.po, self.spec, self.threads = po, spec, threads
+        self.tab = po.OracleTable.from_lxcat(lxcat.synthetic_table(0))
+        plane = (spec.nx + 1) * (spec.ny + 1)
+        fn = workloads.streamer_field_fn(spec)
+        xs = spec.h * np.arange(spec.nx + 1)
+        ys = spec.h * np.arange(spec.ny + 1)
+        e = np.empty((spec.nodes, 3))
+        for k0 in range(0, spec.nz + 1, 32):
+            k1 = min(spec.nz + 1, k0 + 32)
+            Z, Y, X = np.meshgrid(spec.h * np.arange(k0, k1), ys, xs, indexing="ij")
+            e[k0 * plane:k1 * plane] = fn(X.ravel(), Y.ravel(), Z.ravel())
+        e = e.astype(np.float32).astype(np.float64)
+        self.field = po.field_cart3d(spec.nx, spec.ny, spec.nz, spec.h, (0.0, 0.0, 0.0), e.reshape(-1))
+        probe = min(spec.n, 65536)
+        self.parts = workloads.streamer_particles(workloads.streamer_spec(spec.name, n=probe))
+        dt = self.run()
+        m = int(min(spec.n, max(probe, probe * seconds / max(dt, 1e-3))))
+        m = max(probe, (m // 65536) * 65536) if m >= 65536 else m
+        if m != probe:
+            self.parts = workloads.streamer_particles(workloads.streamer_spec(spec.name, n=m))
+
+    def run(self) -> float:
+        po, spec, p = self.po, self.spec, self.parts
+        m = p.n
+        op = po.OraclePop(p.x, p.v, p.w, p.s, p.active, cap=2 * m, seed=spec.seed)
+        trk = po.tracker_cart3d(spec.nx, spec.ny, spec.nz, spec.h, (0.0, 0.0, 0.0))
+        dep = po.tracker_cart3d(spec.nx, spec.ny, spec.nz, spec.h, (0.0, 0.0, 0.0))
+        t0 = time.perf_counter()
+        po.advance(op, self.tab, self.field, spec.dt, tracker=trk, threads=self.threads)
+        po.deposit(op, dep, -1.0)
+        return time.perf_counter() - t0
+
+    def measure(self, reps: int = 1) -> dict:
+        dts = [self.run() for _ in range(reps)]
+        dt = min(dts)
+        m = self.parts.n
+        return {"value": m / dt, "unit": UNIT, "cores": self.threads, "kind": "port",
+                "sample": f"1 step (advance! + tracker + density!) of the first {m} particles of the same "
+                          f"cloud, FP64 oracle, {self.threads} threads, {dt:.2f} s per step"}
+
+
+def cpu_sample(spec, seconds: float, threads: int) -> dict:
+    return CpuSample(spec, seconds / 2, threads).measure(reps=2)
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.streamer_spec(args.workload)
+    threads = os.cpu_count() or 1
+    os.environ["ORACLE_THREADS"] = str(threads)
+    per_step = min(2.0, max(0.5, 60.0 / max(1, args.steps + args.warmup)))
+    cs = CpuSample(spec, per_step, threads)
+    for _ in range(args.warmup):
+        cs.run()
+    vals = [cs.measure() for _ in range(args.steps)]
+    v = statistics.median(x["value"] for x in vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * spec.n / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"streamer step {args.workload}", "particles": spec.n,
+                   "mesh": [spec.nx, spec.ny, spec.nz], "h": spec.h, "dt": spec.dt},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": vals[-1]["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------
+def run_mine(args):
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import jumc, lxcat, streamer, workloads
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    spec = workloads.streamer_spec(args.workload, n=args.particles)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    table = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
+    grid = streamer.Grid3D(spec.nx, spec.ny, spec.nz, spec.h, precision="fp32", ctx=ctx)
+    grid.set_efield_fn(workloads.streamer_field_fn(spec), planes_per_chunk=16)
+    parts = workloads.streamer_particles(spec, rank=rank)
+    seed = spec.seed + 1000 * rank
+    # the input batch: a snapshot restored (device to device) before every step, so each
+    # timed step is one push+collide+track+deposit launch over the same 4.2M-particle cloud
+    snap = jumc.Population(spec.n, parts, table, precision="fp32", seed=seed, mesh=grid)
+    pop = jumc.Population(2 * spec.n, None, table, precision="fp32", seed=seed, mesh=grid)
+    fld = streamer.FieldInterp(grid)
+    trk = streamer.CollisionTracker(grid)
+    qpart = torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}") if ws > 1 else None
+    n_active = float(parts.active.sum())
+
+    def restore():
+        ctx.check(ctx.lib.mcs_pop_copy(pop.h, snap.h))
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        grid.zero(L.Q_PART)
+        if ev is not None:
+            ev[1].record(stream)
+        streamer.advance_deposit(pop, fld, spec.dt, trk, grid, -1.0)
+        if ev is not None:
+            ev[2].record(stream)
+        if qpart is not None:
+            dist.all_reduce(qpart)
+        if ev is not None:
+            ev[3].record(stream)
+
+    grid.zero(L.Q_FIXED)
+    ctx.check(ctx.lib.mcs_pop_step_log(pop.h, 1))
+    for _ in range(args.warmup):
+        restore()
+        step()
+    torch.cuda.synchronize()
+    ctx.sync()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t0.record(stream)
+        for k in range(args.steps):
+            restore()
+            step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.sync()
+    bracket_ms = t0.elapsed_time(t1)
+    step_ms = float(sum(e[0].elapsed_time(e[3]) for e in evs))
+    kms = [e[1].elapsed_time(e[2]) for e in evs]
+    log = np.zeros((1, L.STEP_MOMENTS))
+    ctx.check(ctx.lib.mcs_pop_read_step_log(pop.h, L.dptr(log), 1))
+    n_post = float(log[0, L.S_COUNT])
+    sec_per_step = max(0.0, n_post - n_active)
+    clocks = clk.summary()
+    active_timed = n_active * args.steps
+
+    if dist is not None:
+        t = torch.tensor([step_ms, active_timed, bracket_ms], device=f"cuda:{local}", dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = t.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, active_all, bracket_max = float(mx[0]), float(sm[1]), float(mx[2])
+    else:
+        ms_max, active_all, bracket_max = step_ms, active_timed, bracket_ms
+    value = active_all / (ms_max * 1e-3)
+    kmean = float(np.mean(kms))
+    pk, pk_kind = peaks()
+    hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    alg = alg_bytes_per_launch(n_active, sec_per_step, spec.nodes)
+    achieved = alg / (kmean * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / f"traffic_k_step_mesh_{args.workload}.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+
+    e2e = None
+    if args.e2e_steps > 0:
+        e2e = run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, dist, local)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_sample(spec, args.cpu_seconds, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": f"streamer step {args.workload}: {spec.nx}x{spec.ny}x{spec.nz} mesh h={spec.h:g} m, "
+                            f"{spec.n} particles per GPU (w={spec.weight[0]:g}..{spec.weight[1]:g}), Gaussian cloud "
+                            f"sigma=50um, 1 eV isotropic, synthetic gas 0, dt={spec.dt:g} s, one push+collide+track+"
+                            f"CIC-deposit launch per step over the same input cloud",
+                "particles_per_gpu": spec.n, "active_per_step": n_active, "secondaries_per_step": sec_per_step,
+                "step_timing": "CUDA events around zero(qpart)+step kernel(+all-reduce) of each step, summed; the "
+                               "device-to-device restore of the input cloud between steps is outside the windows",
+                "ms_per_step_incl_restore": bracket_max / args.steps,
+                "l2": "inputs larger than L2 (particle arrays 37 B x 4.2M = 155 MB per GPU)",
+                "parallelism": f"dp{ws} (particle shards, int64 all-reduce of the deposit grid)" if ws > 1 else "1 GPU",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "kernel": "k_step_mesh<float,256,2>", "kernel_ms": kmean,
+                         "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, dist, local):
+    """The same step through the C ABI with host-resident particles: each step uploads the
+    input cloud from pinned host buffers, steps, and downloads the particles and the deposit
+    grid (the plain drop-in for a host-resident Julia population)."""
+    import ctypes as C
+
+    cap = pop.capacity
+    nodes = spec.nodes
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    n = parts.n
+    ix, iv = pinned((n, 3), torch.float64), pinned((n, 3), torch.float64)
+    iw, i_s, ia = pinned((n,), torch.float64), pinned((n,), torch.float64), pinned((n,), torch.uint8)
+    ix[:], iv[:], iw[:], i_s[:], ia[:] = parts.x, parts.v, parts.w, parts.s, parts.active
+    ox, ov = pinned((cap, 3), torch.float64), pinned((cap, 3), torch.float64)
+    ow, os_, oa = pinned((cap,), torch.float64), pinned((cap,), torch.float64), pinned((cap,), torch.uint8)
+    hq = pinned((nodes,), torch.int64)
+    lib = ctx.lib
+    nn = C.c_int64()
+    h2d = d2h = 0
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    active = 0.0
+    n_active = float(parts.active.sum())
+    for k in range(args.e2e_steps + 1):
+        if k == 1:
+            torch.cuda.synchronize()
+            t0.record(stream)
+            h2d = d2h = 0
+            active = 0.0
+        active += n_active
+        ctx.check(lib.mcs_pop_upload(pop.h, L.dptr(ix), L.dptr(iv), L.dptr(iw), L.dptr(i_s), L.u8ptr(ia), n))
+        h2d += n * 65
+        grid.zero(L.Q_PART)
+        ctx.check(lib.mcs_advance_deposit(pop.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0))
+        if ws > 1:
+            dist.all_reduce(torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}"))
+        ctx.check(lib.mcs_pop_download(pop.h, L.dptr(ox), L.dptr(ov), L.dptr(ow), L.dptr(os_), L.u8ptr(oa), cap,
+                                       C.byref(nn)))
+        ctx.check(lib.mcs_grid_read_fixed(grid.h_, L.Q_PART, L.i64ptr(hq)))
+        d2h += nn.value * 65 + nodes * 8
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    if ws > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
+        a = torch.tensor([active], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(a)
+        active = float(a[0])
+    return {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // args.e2e_steps,
+            "d2h_bytes_per_step": d2h // args.e2e_steps, "steps": args.e2e_steps,
+            "path": "mcs_pop_upload (pinned host, Julia layout) -> mcs_advance_deposit -> mcs_pop_download + "
+                    "mcs_grid_read_fixed"}
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_mine(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

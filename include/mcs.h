@@ -131,6 +131,9 @@ MCS_API int mcs_grid_zero(mcs_grid* g, int which);
 MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out);
 /* cyl: density per cell (weight/dV, poisson.jl:79-81).  cart3d: charge per node in e. */
 MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out);
+/* Device address and entry count of a charge array (int64), for collectives that sum the
+ * deposits of several processes (e.g. an NCCL int64 all-reduce). */
+MCS_API int mcs_grid_charge_ptr(mcs_grid* g, int which, void** dptr, int64_t* count);
 
 /* ---- fields: the `efield` callable of advance! ---- */
 /* FixedField (Swarm/src/Swarm.jl:28-32), generalised to any constant vector. */
@@ -152,6 +155,9 @@ MCS_API int mcs_pop_upload(mcs_pop* p, const double* x, const double* v, const d
                            const double* s, const uint8_t* active, int64_t n);
 MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double* s,
                              uint8_t* active, int64_t cap, int64_t* n);
+/* Device-to-device copy of a whole population (state, count, Philox key and step): a
+ * snapshot / restore point.  Same context, precision and layout; dst capacity >= src's. */
+MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src);
 /* nparticles (population.jl:106): particles in use, active or not. */
 MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n);
 
@@ -195,6 +201,12 @@ enum {
  * nsteps*MCS_STEP_MOMENTS doubles; they stay on the device until the loop ends. */
 MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, int nsteps,
                           int64_t n0, double tol, double* moments_out);
+/* Per-step diagnostics log (the sums MCStreamer reports every step, main.jl:269-279):
+ * with capacity > 0 every following advance! writes the MCS_STEP_MOMENTS sums of its
+ * post-step population into slot (steps since enabling) % capacity on the device;
+ * capacity 0 disables it.  read copies slots [0, nsteps) to the host. */
+MCS_API int mcs_pop_step_log(mcs_pop* p, int capacity);
+MCS_API int mcs_pop_read_step_log(mcs_pop* p, double* out, int nsteps);
 
 #ifdef __cplusplus
 }

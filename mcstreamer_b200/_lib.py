@@ -57,6 +57,7 @@ SIGNATURES = {
     "mcs_grid_zero": (i32, [vp, i32]),
     "mcs_grid_read_fixed": (i32, [vp, i32, pi64]),
     "mcs_grid_read_density": (i32, [vp, i32, pd]),
+    "mcs_grid_charge_ptr": (i32, [vp, i32, ph, pi64]),
     "mcs_field_uniform": (i32, [vp, f64, f64, f64, ph]),
     "mcs_field_from_grid": (i32, [vp, ph]),
     "mcs_field_destroy": (i32, [vp]),
@@ -67,6 +68,7 @@ SIGNATURES = {
     "mcs_pop_upload": (i32, [vp, pd, pd, pd, pd, pu8, i64]),
     "mcs_pop_download": (i32, [vp, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_pop_nparticles": (i32, [vp, pi64]),
+    "mcs_pop_copy": (i32, [vp, vp]),
     "mcs_advance": (i32, [vp, vp, vp, f64, vp]),
     "mcs_advance_deposit": (i32, [vp, vp, vp, f64, vp, vp, f64]),
     "mcs_collisions": (i32, [vp, vp, f64, vp]),
@@ -77,6 +79,8 @@ SIGNATURES = {
     "mcs_resample_cells": (i32, [vp, vp, i32, i32]),
     "mcs_moments": (i32, [vp, vp, pd, i32]),
     "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, pd]),
+    "mcs_pop_step_log": (i32, [vp, i32]),
+    "mcs_pop_read_step_log": (i32, [vp, pd, i32]),
 }
 
 _lib = None

@@ -76,6 +76,13 @@ int ensure_staging(mcs_pop* p, size_t bytes) {
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Slot of the per-step moments log for the step about to run (nullptr when disabled).
+double* log_slot(mcs_pop* p) {
+    if (!p->d_log || p->log_cap < 1) return nullptr;
+    const uint32_t k = (p->step - p->log_step0) % (uint32_t)p->log_cap;
+    return p->d_log + (size_t)k * kStepMoments;
+}
+
 }  // namespace
 
 extern "C" {
@@ -338,6 +345,13 @@ MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out) {
     return st;
 }
 
+MCS_API int mcs_grid_charge_ptr(mcs_grid* g, int which, void** dptr, int64_t* count) {
+    if (!g || !dptr || !count || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    *dptr = g->d_q[which];
+    *count = (int64_t)g->nq;
+    return MCS_OK;
+}
+
 MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out) {
     if (!g || !out || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
     std::vector<long long> q(g->nq);
@@ -433,7 +447,7 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     for (int q = 0; q < 8; ++q) { cudaFree(p->f[q]); cudaFree(p->alt[q]); }
     cudaFree(p->act); cudaFree(p->cell); cudaFree(p->d_n); cudaFree(p->tile_status);
     cudaFree(p->tile_partials); cudaFree(p->counters); cudaFree(p->d_moments); cudaFree(p->staging);
-    cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage);
+    cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage); cudaFree(p->d_log);
     delete p;
     return MCS_OK;
 }
@@ -476,6 +490,26 @@ MCS_API int mcs_pop_upload(mcs_pop* p, const double* x, const double* v, const d
     const long long nn = n;
     MCS_CK(c, cudaMemcpyAsync(p->d_n + p->cur, &nn, sizeof(nn), cudaMemcpyHostToDevice, c->stream));
     MCS_CK(c, cudaStreamSynchronize(c->stream));  // nn and the host buffers are caller-owned
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src) {
+    if (!dst || !src || dst->ctx != src->ctx) return MCS_ERR_ARG;
+    mcs_ctx* c = dst->ctx;
+    if (dst->precision != src->precision || dst->cells != src->cells)
+        return set_err(c, MCS_ERR_ARG, "populations differ in precision or layout");
+    if (dst->cap < src->cap) return set_err(c, MCS_ERR_CAPACITY, "destination capacity below source capacity");
+    if (int st = use_device(c)) return st;
+    const size_t n = (size_t)src->cap;
+    for (int q = 0; q < 8; ++q)
+        MCS_CK(c, cudaMemcpyAsync(dst->f[q], src->f[q], n * src->esz, cudaMemcpyDeviceToDevice, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(dst->act, src->act, n, cudaMemcpyDeviceToDevice, c->stream));
+    if (src->cell)
+        MCS_CK(c, cudaMemcpyAsync(dst->cell, src->cell, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(dst->d_n + dst->cur, src->d_n + src->cur, sizeof(long long), cudaMemcpyDeviceToDevice,
+                              c->stream));
+    dst->seed = src->seed;
+    dst->step = src->step;
     return MCS_OK;
 }
 
@@ -532,11 +566,11 @@ MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, doub
             return set_err(c, MCS_ERR_UNSUPPORTED, "a cell-layout population needs the field of its own mesh");
         if (tracker && tracker != p->cells)
             return set_err(c, MCS_ERR_UNSUPPORTED, "a cell-layout population tracks onto its own mesh");
-        st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, 0.0, nullptr)
-                                      : launch_step_mesh<double>(p, t, dt, tracker != nullptr, 0.0, nullptr);
+        st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, 0.0, log_slot(p))
+                                      : launch_step_mesh<double>(p, t, dt, tracker != nullptr, 0.0, log_slot(p));
     } else {
-        st = p->precision == MCS_FP32 ? launch_step_abs<float>(p, t, f, dt, tracker, nullptr)
-                                      : launch_step_abs<double>(p, t, f, dt, tracker, nullptr);
+        st = p->precision == MCS_FP32 ? launch_step_abs<float>(p, t, f, dt, tracker, log_slot(p))
+                                      : launch_step_abs<double>(p, t, f, dt, tracker, log_slot(p));
     }
     if (st) return st;
     p->cur ^= 1;
@@ -553,8 +587,8 @@ MCS_API int mcs_advance_deposit(mcs_pop* p, const mcs_table* t, const mcs_field*
         return set_err(c, MCS_ERR_UNSUPPORTED, "fused step+deposit needs a cell-layout population on one mesh");
     if (!(dt >= 0)) return set_err(c, MCS_ERR_ARG, "dt must be >= 0");
     if (int st = use_device(c)) return st;
-    const int st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, val, nullptr)
-                                            : launch_step_mesh<double>(p, t, dt, tracker != nullptr, val, nullptr);
+    const int st = p->precision == MCS_FP32 ? launch_step_mesh<float>(p, t, dt, tracker != nullptr, val, log_slot(p))
+                                            : launch_step_mesh<double>(p, t, dt, tracker != nullptr, val, log_slot(p));
     if (st) return st;
     p->cur ^= 1;
     p->step += 1;
@@ -601,6 +635,33 @@ MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout) {
     if (int st = use_device(c)) return st;
     if (int st = launch_moments(p, t, p->d_moments, nm)) return st;
     MCS_CK(c, cudaMemcpyAsync(out, p->d_moments, nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return sync_status(c);
+}
+
+MCS_API int mcs_pop_step_log(mcs_pop* p, int capacity) {
+    if (!p || capacity < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    cudaFree(p->d_log);
+    p->d_log = nullptr;
+    p->log_cap = 0;
+    if (capacity == 0) return MCS_OK;
+    if (int st = dalloc(c, &p->d_log, (size_t)capacity * kStepMoments)) return st;
+    MCS_CK(c, cudaMemset(p->d_log, 0, (size_t)capacity * kStepMoments * sizeof(double)));
+    p->log_cap = capacity;
+    p->log_step0 = p->step;
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_read_step_log(mcs_pop* p, double* out, int nsteps) {
+    if (!p || !out || nsteps < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (nsteps > p->log_cap) return set_err(c, MCS_ERR_ARG, "more steps than the log holds");
+    if (int st = use_device(c)) return st;
+    if (nsteps > 0)
+        MCS_CK(c, cudaMemcpyAsync(out, p->d_log, (size_t)nsteps * kStepMoments * sizeof(double),
+                                  cudaMemcpyDeviceToHost, c->stream));
     return sync_status(c);
 }
 

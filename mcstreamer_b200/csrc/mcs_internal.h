@@ -134,4 +134,7 @@ struct mcs_pop {
     uint8_t* alt_act = nullptr;
     void* stage = nullptr;         // secondary staging of the step kernels
     size_t stage_bytes = 0;
+    double* d_log = nullptr;       // per-step fused moments, log_cap entries of kStepMoments
+    int log_cap = 0;
+    uint32_t log_step0 = 0;
 };

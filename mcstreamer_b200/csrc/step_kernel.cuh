@@ -512,6 +512,21 @@ __device__ __forceinline__ uint32_t cell_index(const GridView& g, bool in, int i
     return in ? (uint32_t)ix + (uint32_t)g.nx * ((uint32_t)iy + (uint32_t)g.ny * (uint32_t)iz) : kOutsideCell;
 }
 
+// Absolute position of a (cell, offset) pair.
+__device__ __forceinline__ void mesh_abs(const GridView& g, uint32_t cell, double ox, double oy, double oz, double& x,
+                                         double& y, double& z) {
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    if (cell != kOutsideCell) {
+        cx = (double)(cell % (uint32_t)g.nx);
+        const uint32_t r = cell / (uint32_t)g.nx;
+        cy = (double)(r % (uint32_t)g.ny);
+        cz = (double)(r / (uint32_t)g.ny);
+    }
+    x = g.x0 + g.h * (cx + ox);
+    y = g.y0 + g.h * (cy + oy);
+    z = g.z0 + g.h * (cz + oz);
+}
+
 // ---------------------------------------------------------------------------------------
 // Mesh-layout step: advance! with the trilinear node-field gather of a 3-D mesh, the
 // collision tracker (+w ionization / -w attachment into qfixed, CIC int64) and, when
@@ -637,6 +652,24 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
                 cic_fixed(g.qpart, g.nx, g.ny, ex, (int)(r % (uint32_t)g.ny), (int)(r / (uint32_t)g.ny),
                           (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], (double)sg.f[6][e] * dep_val);
             }
+        }
+        if (C.moments_out) {
+            MomAcc<T> acc;
+            acc.zero();
+            double x, y, z;
+            for (int jj = 0; jj < PPT; ++jj) {
+                const long long i = base + jj * BLOCK + threadIdx.x;
+                if (i < n_entry && P.act[i]) {
+                    mesh_abs(g, P.cell[i], (double)P.f[0][i], (double)P.f[1][i], (double)P.f[2][i], x, y, z);
+                    acc.add(x, y, z, P.f[3][i], P.f[4][i], P.f[5][i], P.f[6][i]);
+                }
+            }
+            for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)
+                if (sg.act[e]) {
+                    mesh_abs(g, sg.cell[e], (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], x, y, z);
+                    acc.add(x, y, z, sg.f[3][e], sg.f[4][e], sg.f[5][e], sg.f[6][e]);
+                }
+            block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
         }
         __syncthreads();
     }

@@ -21,6 +21,14 @@ from . import constants as co
 from .jumc import Context, Population
 
 
+class DeviceArray:
+    """A 1-D device buffer owned by the library, described by __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
 class Grid3D:
     """nx*ny*nz cubic cells of side h with lower corner `origin`; nodes (nx+1)(ny+1)(nz+1)."""
 
@@ -75,6 +83,14 @@ class Grid3D:
         out = np.zeros(self.nnodes, dtype=np.int64)
         self.ctx.check(self.ctx.lib.mcs_grid_read_fixed(self.h_, which, L.i64ptr(out)))
         return out
+
+    def charge_array(self, which: int = L.Q_PART) -> "DeviceArray":
+        """The device int64 charge array, exposed through __cuda_array_interface__ (so a
+        collective library can sum it across processes in place)."""
+        p = C.c_void_p()
+        n = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_grid_charge_ptr(self.h_, which, C.byref(p), C.byref(n)))
+        return DeviceArray(p.value, n.value, "<i8")
 
     def cell_key(self, x: np.ndarray) -> np.ndarray:
         u = (np.asarray(x) - np.asarray(self.origin)) / self.h
