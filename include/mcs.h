@@ -5,7 +5,7 @@
  *
  * The reference has no FFI: its "plugin API" is Julia multiple dispatch.  Each entry point
  * below names the reference function it replaces (file:line inside the reference project);
- * a Julia caller binds them with ccall (binding stubs are listed in INTEGRATION.md).
+ * a Julia caller binds them with ccall.
  *
  * Host buffer layouts equal the Julia memory layouts so Julia arrays pass without copies:
  *   x, v   : 3 doubles per particle, interleaved   (Vector{SVector{3,Float64}})
@@ -189,6 +189,7 @@ MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid* g);
 MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax);
 /* Moments over the population (layout MCS_M_*), table may be NULL (no rate sums). */
 MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout);
+
 
 /* Per-step moments of the fused swarm loop (MCS_STEP_MOMENTS doubles per step). */
 enum {
