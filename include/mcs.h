@@ -190,6 +190,21 @@ MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax);
 /* Moments over the population (layout MCS_M_*), table may be NULL (no rate sums). */
 MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout);
 
+/* Allocation-free moments.  No counterpart in the reference: an addition for callers that
+ * must not allocate device memory when they ask for diagnostics -- e.g. a simulation loop
+ * held to a memory budget fixed at start-up, or a host application whose own allocator
+ * owns every device byte -- and that keep the particles in their own device arrays.
+ * arrays[0..6] = x, y, z, vx, vy, vz, w (device, float or double per `precision`), active =
+ * device bytes, n particles with absolute positions; writes the MCS_MOMENTS_BASE sums of
+ * layout MCS_M_* to moments_out (device) on `stream` (a cudaStream_t, NULL = default) of
+ * `device`.  It calls no allocator: its partial sums live in a fixed array inside the
+ * library (about 1.2 MB per device that loads it, kept until exit), so n is limited to
+ * MCS_NOALLOC_MAX_PARTICLES and larger n returns MCS_ERR_ARG.  The first call on a device
+ * looks up that array's device address; make it before capturing a stream.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised. */
+#define MCS_NOALLOC_MAX_PARTICLES 67108864LL
+MCS_API int mcs_moments_noalloc(int device, void* stream, int precision, const void* const* arrays,
+                                const uint8_t* active, int64_t n, double* moments_out);
 
 /* Per-step moments of the fused swarm loop (MCS_STEP_MOMENTS doubles per step). */
 enum {
