@@ -68,6 +68,28 @@ struct Rng {
     __device__ __forceinline__ float u32() { return __uint2float_rn(word() | 1u) * 0x1p-32f; }
 };
 
+__device__ __forceinline__ double uni64(uint32_t w) { return __fma_rn((double)w, 0x1p-32, 0x1p-33); }
+__device__ __forceinline__ float uni32(uint32_t w) { return __uint2float_rn(w | 1u) * 0x1p-32f; }
+
+// The draws of one collision event (do_one_collision! plus the new free-flight time).
+// Event j of particle `slot` during step `step` owns block b = Philox(seed; {slot, step, j,
+// tag}) -- xi, new s, direction (phi, u) -- and, only for processes that need more,
+// c = Philox(seed; {slot, step, j | 2^31, tag}) -- secondary direction, secondary s and the
+// energy-sharing fraction.  Every colliding lane generates its block at the same point of
+// the sub-step, so the generator runs converged across the warp.
+struct Event {
+    uint32_t k0, k1, slot, step, tag, j;
+    U4 b, c;
+    __device__ __forceinline__ void init(uint64_t seed, uint32_t slot_, uint32_t step_, uint32_t tag_) {
+        k0 = (uint32_t)seed; k1 = (uint32_t)(seed >> 32); slot = slot_; step = step_; tag = tag_; j = 0;
+    }
+    __device__ __forceinline__ void begin() {
+        b = philox10(U4{slot, step, j, tag}, k0, k1);
+        ++j;
+    }
+    __device__ __forceinline__ void second() { c = philox10(U4{slot, step, (j - 1) | 0x80000000u, tag}, k0, k1); }
+};
+
 template <typename T> struct Uni;
 template <> struct Uni<double> { __device__ static double get(Rng& r) { return r.u64(); } };
 template <> struct Uni<float> { __device__ static float get(Rng& r) { return r.u32(); } };
@@ -79,12 +101,12 @@ template <> struct Uni<float> { __device__ static float get(Rng& r) { return r.u
 template <typename T> struct M;
 template <> struct M<double> {
     __device__ static double nlog(double u) { return -log(u); }
-    __device__ static void dir(Rng& r, double& dx, double& dy, double& dz) {
-        // randsphere: JuMC/src/util.jl:4-12
-        const double phi = 6.283185307179586 * r.u64();
+    // randsphere: JuMC/src/util.jl:4-12, from the uniforms (uphi, uu)
+    __device__ static void dir(double uphi, double uu, double& dx, double& dy, double& dz) {
+        const double phi = 6.283185307179586 * uphi;
         double s, c;
         sincos(phi, &s, &c);
-        const double u = 2.0 * r.u64() - 1.0;
+        const double u = 2.0 * uu - 1.0;
         const double v = sqrt(1.0 - u * u);
         dx = v * c; dy = v * s; dz = u;
     }
@@ -92,12 +114,12 @@ template <> struct M<double> {
 };
 template <> struct M<float> {
     __device__ static float nlog(float u) { return -__logf(u); }
-    __device__ static void dir(Rng& r, float& dx, float& dy, float& dz) {
+    __device__ static void dir(float uphi, float uu, float& dx, float& dy, float& dz) {
         // phi = 2*pi*U evaluated as (2U-1)*pi + pi so the SFU sees |arg| <= pi.
-        const float ph = fmaf(r.u32(), 6.28318530718f, -3.14159265359f);
+        const float ph = fmaf(uphi, 6.28318530718f, -3.14159265359f);
         float s, c;
         __sincosf(ph, &s, &c);
-        const float u = fmaf(2.0f, r.u32(), -1.0f);
+        const float u = fmaf(2.0f, uu, -1.0f);
         const float v = sqrtf(fmaxf(0.0f, 1.0f - u * u));
         dx = -v * c; dy = -v * s; dz = u;
     }

@@ -3,7 +3,7 @@
 //
 //   * each CTA takes tiles of BLOCK*PPT consecutive slots from an atomic ticket;
 //   * every active particle is pushed, collided and tracked with its state in registers;
-//     uniforms come from its own Philox stream (seed; slot, step, k/4, tag);
+//     each collision event draws from its own Philox block (seed; slot, step, event, tag);
 //   * secondaries are staged in a per-CTA global buffer, ranked by (parent slot, event #)
 //     with a block scan of per-parent counts, and appended after the tiles before them
 //     (decoupled look-back on per-tile counts), so the population order equals the
@@ -119,8 +119,10 @@ enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2, OUT_CHANGE = 3 };
 template <typename T>
 struct Sec { T vx, vy, vz, s; };
 
-// collide: JuMC/src/electron.jl:108-139.  FP64 follows the reference's expressions.
-__device__ __forceinline__ int collide64(int kind, double par, double eng, Rng& r, double& vx, double& vy,
+// collide: JuMC/src/electron.jl:108-139.  FP64 follows the reference's expressions.  The
+// event's block b supplies the direction (b.z, b.w); ionization draws block c for the
+// secondary's direction (c.x, c.y), its free-flight time (c.z) and the sharing fraction (c.w).
+__device__ __forceinline__ int collide64(int kind, double par, double eng, Event& e, double& vx, double& vy,
                                          double& vz, Sec<double>& sec) {
     const double m = kElectronMass;
     if (kind == K_ELASTIC) {
@@ -129,7 +131,7 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Rng& 
         const double dx = vx - cx, dy = vy - cy, dz = vz - cz;
         const double nrm = sqrt(dx * dx + dy * dy + dz * dz);
         double ux, uy, uz;
-        M<double>::dir(r, ux, uy, uz);
+        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
         vx = ux * nrm + cx; vy = uy * nrm + cy; vz = uz * nrm + cz;
         return OUT_NONE;
     }
@@ -137,27 +139,28 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Rng& 
         const double E1 = fmax(0.0, eng - par);
         const double va = sqrt(2.0 * E1 / m);
         double ux, uy, uz;
-        M<double>::dir(r, ux, uy, uz);
+        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
         vx = ux * va; vy = uy * va; vz = uz * va;
         return OUT_NONE;
     }
     if (kind == K_IONIZATION || kind == K_IONIZATION_UNIFORM) {
+        e.second();
         double va1, va2;
         if (kind == K_IONIZATION) {
             const double E1 = fmax(0.0, eng - par) / 2.0;
             va1 = va2 = sqrt(2.0 * E1 / m);
         } else {
             const double Ea = fmax(0.0, eng - par);
-            const double E2 = r.u64() * Ea;
+            const double E2 = uni64(e.c.w) * Ea;
             const double E1 = Ea - E2;
             va1 = sqrt(2.0 * E1 / m);
             va2 = sqrt(2.0 * E2 / m);
         }
         double ux, uy, uz, wx, wy, wz;
-        M<double>::dir(r, ux, uy, uz);
-        M<double>::dir(r, wx, wy, wz);
+        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
+        M<double>::dir(uni64(e.c.x), uni64(e.c.y), wx, wy, wz);
         sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
-        sec.s = -log(r.u64());
+        sec.s = -log(uni64(e.c.z));
         vx = ux * va1; vy = uy * va1; vz = uz * va1;
         return OUT_NEW;
     }
@@ -165,40 +168,41 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Rng& 
     return OUT_NONE;
 }
 
-// FP32: energies in v^2 units (par = 2*threshold/m), same draws in the same order.
-__device__ __forceinline__ int collide32(int kind, float par, float v2, Rng& r, float& vx, float& vy,
-                                         float& vz, Sec<float>& sec) {
+// FP32: energies in v^2 units (par = 2*threshold/m), the same draws as collide64.
+__device__ __forceinline__ int collide32(int kind, float par, float v2, Event& e, float& vx, float& vy, float& vz,
+                                         Sec<float>& sec) {
     if (kind == K_ELASTIC) {
         const float cx = par * vx, cy = par * vy, cz = par * vz;
         const float dx = vx - cx, dy = vy - cy, dz = vz - cz;
         const float nrm = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         float ux, uy, uz;
-        M<float>::dir(r, ux, uy, uz);
+        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
         vx = fmaf(ux, nrm, cx); vy = fmaf(uy, nrm, cy); vz = fmaf(uz, nrm, cz);
         return OUT_NONE;
     }
     if (kind == K_EXCITATION) {
         const float va = sqrtf(fmaxf(0.0f, v2 - par));
         float ux, uy, uz;
-        M<float>::dir(r, ux, uy, uz);
+        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
         vx = ux * va; vy = uy * va; vz = uz * va;
         return OUT_NONE;
     }
     if (kind == K_IONIZATION || kind == K_IONIZATION_UNIFORM) {
+        e.second();
         float va1, va2;
         const float ea = fmaxf(0.0f, v2 - par);
         if (kind == K_IONIZATION) {
             va1 = va2 = sqrtf(0.5f * ea);
         } else {
-            const float f2 = r.u32();
+            const float f2 = uni32(e.c.w);
             va1 = sqrtf(ea - f2 * ea);
             va2 = sqrtf(f2 * ea);
         }
         float ux, uy, uz, wx, wy, wz;
-        M<float>::dir(r, ux, uy, uz);
-        M<float>::dir(r, wx, wy, wz);
+        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
+        M<float>::dir(uni32(e.c.x), uni32(e.c.y), wx, wy, wz);
         sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
-        sec.s = M<float>::nlog(r.u32());
+        sec.s = M<float>::nlog(uni32(e.c.z));
         vx = ux * va1; vy = uy * va1; vz = uz * va1;
         return OUT_NEW;
     }

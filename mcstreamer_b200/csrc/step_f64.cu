@@ -14,6 +14,6 @@ int launch_collisions<double>(mcs_pop* p, const mcs_table* t, double dt, mcs_gri
 }
 template <>
 int launch_step_mesh<double>(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
-    return launch_step_mesh_impl<double, 128, 1>(p, t, dt, tracking, dep_val, mom);
+    return launch_step_mesh_impl<double, 128, 8>(p, t, dt, tracking, dep_val, mom);
 }
 }  // namespace mcs

@@ -20,6 +20,7 @@ struct TileShared {
     uint32_t wtot[BLOCK / 32];
     double red[BLOCK / 32][kStepMoments];
     uint32_t count;                  // staged entries of the current tile
+    uint32_t next;                   // next unclaimed tile slot (particle queue)
     uint32_t tile;
     uint32_t excl;
     int ok;
@@ -169,6 +170,7 @@ __device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long lo
     if (threadIdx.x == 0) {
         sh.tile = atomicAdd(&C.counters[0], 1u);
         sh.count = 0;
+        sh.next = 0;
     }
     __syncthreads();
     const long long tile = sh.tile;
@@ -178,18 +180,19 @@ __device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long lo
 // Shared collision body: select a process for velocity (vx, vy, vz) and apply it in place.
 // Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
 template <typename T, typename RowsT>
-__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Rng& rng, T& vx,
-                                            T& vy, T& vz, Sec<T>& sec) {
+__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Event& rng,
+                                            T& vx, T& vy, T& vz, Sec<T>& sec) {
     int j;
     double eng = 0.0;
     float v2 = 0.0f;
+    rng.begin();
     if constexpr (sizeof(T) == 8) {
         eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
-        const double xi = rng.u64() * tab.maxrate;
+        const double xi = uni64(rng.b.x) * tab.maxrate;
         j = select_row64(tab, eng, xi, C.flags, C.status);
     } else {
         v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
-        const float xi = rng.u32() * tab.maxrate32;
+        const float xi = uni32(rng.b.x) * tab.maxrate32;
         j = select_row32(tab, v2, xi, C.flags, C.status);
     }
     const int kind = j >= 0 ? rows.kind[j] : K_NULL;
@@ -242,7 +245,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
             const long long i = base + local;
             uint32_t ev = 0;
             if (i < n_entry && P.act[i]) {
-                Rng rng;
+                Event rng;
                 rng.init(C.seed, (uint32_t)i, C.step, C.tag);
                 T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                 T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
@@ -305,8 +308,8 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                             if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
                             act = 0;  // the particle keeps sub-stepping (mixed_population.jl:32)
                         }
-                        if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                        else s = (double)M<float>::nlog(rng.u32());
+                        if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
+                        else s = (double)M<float>::nlog(uni32(rng.b.y));
                     }
                     trem -= t;
                 }
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
             if (i < n_entry && P.act[i]) {
                 double s = (double)P.f[7][i] - C.dt * tab.maxrate;
                 if (s <= 0) {
-                    Rng rng;
+                    Event rng;
                     rng.init(C.seed, (uint32_t)i, C.step, C.tag);
                     const T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                     T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
@@ -392,8 +395,8 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
                         if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
                         P.act[i] = 0;
                     }
-                    if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                    else s = (double)M<float>::nlog(rng.u32());
+                    if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
+                    else s = (double)M<float>::nlog(uni32(rng.b.y));
                     P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
                 }
                 P.f[7][i] = (T)s;
@@ -531,7 +534,24 @@ __device__ __forceinline__ void mesh_abs(const GridView& g, uint32_t cell, doubl
 // Mesh-layout step: advance! with the trilinear node-field gather of a 3-D mesh, the
 // collision tracker (+w ionization / -w attachment into qfixed, CIC int64) and, when
 // dep_val != 0, the particle deposit density!(qpart, dep_val) of the post-step state.
+//
+// Work distribution: a particle needs a variable number of sub-steps (one per real or null
+// collision), so a fixed particle-per-lane mapping leaves most lanes of a warp idle while
+// the slowest particle finishes.  Here every lane executes one sub-step per loop pass and,
+// when its particle is done, takes the tile's next particle from a shared-memory counter;
+// the warp stays converged on the sub-step body and the idle tail is about one particle.
 // ---------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ bool in_unit_cube(T ox, T oy, T oz) {
+    if constexpr (sizeof(T) == 4) {
+        // offsets in [0,1) <=> bit patterns below 1.0f (negative values have the sign bit)
+        const uint32_t m = max(__float_as_uint(ox), max(__float_as_uint(oy), __float_as_uint(oz)));
+        return m < 0x3f800000u;
+    } else {
+        return ox >= 0.0 && ox < 1.0 && oy >= 0.0 && oy < 1.0 && oz >= 0.0 && oz < 1.0;
+    }
+}
+
 template <typename T, int BLOCK, int PPT>
 __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
                                                      YoshidaC Y, double dep_val) {
@@ -550,23 +570,51 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
         const long long tile = next_tile(sh, C, ntiles);
         if (tile < 0) break;
         const long long base = tile * TILE;
+        const long long rest = n_entry - base;
+        const uint32_t tile_n = rest < TILE ? (uint32_t)rest : (uint32_t)TILE;
 
-#pragma unroll 1
-        for (int jj = 0; jj < PPT; ++jj) {
-            const uint32_t local = jj * BLOCK + threadIdx.x;
-            const long long i = base + local;
-            uint32_t ev = 0;
-            if (i < n_entry && P.act[i]) {
-                Rng rng;
+        // per-lane particle state
+        bool have = false, drained = false;
+        uint32_t local = 0;
+        long long i = 0;
+        Event rng;
+        T ox = 0, oy = 0, oz = 0, vx = 0, vy = 0, vz = 0, w = 0;
+        double s = 0.0, trem = 0.0;
+        bool in = false;
+        int ix = 0, iy = 0, iz = 0;
+        CellField<T> cf;
+        uint8_t act = 1;
+        uint32_t ev = 0;
+
+        auto drift = [&](T c) {
+            ox += c * vx; oy += c * vy; oz += c * vz;
+            if (in && in_unit_cube(ox, oy, oz)) return;
+            if (relocate(g, ix, iy, iz, in, ox, oy, oz)) {
+                if (in) load_cell_field(g, ix, iy, iz, cf);
+                else cf.zero();
+            }
+        };
+        auto kick = [&](T k) {
+            T ex, ey, ez;
+            cf.eval(ox, oy, oz, ex, ey, ez);
+            vx += k * ex; vy += k * ey; vz += k * ez;
+        };
+
+        for (;;) {
+            // refill: an idle lane takes the next particle of the tile
+            while (!have && !drained) {
+                const uint32_t q = atomicAdd(&sh.next, 1u);
+                if (q >= (uint32_t)TILE) { drained = true; break; }
+                if (q >= tile_n || !P.act[base + q]) { sh.cnt[q] = 0; continue; }
+                local = q;
+                i = base + q;
                 rng.init(C.seed, (uint32_t)i, C.step, C.tag);
                 const uint32_t cell0 = P.cell[i];
-                T ox = P.f[0][i], oy = P.f[1][i], oz = P.f[2][i];
-                T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
-                const T w = P.f[6][i];
-                double s = (double)P.f[7][i];
-                bool in = cell0 != kOutsideCell;
-                int ix = 0, iy = 0, iz = 0;
-                CellField<T> cf;
+                ox = P.f[0][i]; oy = P.f[1][i]; oz = P.f[2][i];
+                vx = P.f[3][i]; vy = P.f[4][i]; vz = P.f[5][i];
+                w = P.f[6][i];
+                s = (double)P.f[7][i];
+                in = cell0 != kOutsideCell;
                 if (in) {
                     ix = (int)(cell0 % (uint32_t)g.nx);
                     const uint32_t r = cell0 / (uint32_t)g.nx;
@@ -576,53 +624,48 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
                 } else {
                     cf.zero();
                 }
-                uint8_t act = 1;
-                double trem = C.dt;
-                auto drift = [&](T c) {
-                    ox += c * vx; oy += c * vy; oz += c * vz;
-                    if (relocate(g, ix, iy, iz, in, ox, oy, oz)) {
-                        if (in) load_cell_field(g, ix, iy, iz, cf);
-                        else cf.zero();
-                    }
-                };
-                auto kick = [&](T k) {
-                    T ex, ey, ez;
-                    cf.eval(ox, oy, oz, ex, ey, ez);
-                    vx += k * ex; vy += k * ey; vz += k * ez;
-                };
-                while (trem > 0) {
-                    double tn, t;
-                    if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
-                    else tn = s * tab.inv_maxrate;
-                    bool collides;
-                    if (trem > tn) { t = tn; collides = true; }
-                    else { t = trem; collides = false; s -= t * tab.maxrate; }
-                    const T tt = (T)t;
-                    // advance_free_yoshida (electron.jl:51-62) in cell units
-                    drift(cd1 * tt);
-                    kick(kd1 * tt);
-                    drift(cd2 * tt);
-                    kick(kd2 * tt);
-                    drift(cd3 * tt);
-                    kick(kd3 * tt);
-                    drift(cd4 * tt);
-                    if (collides) {
-                        Sec<T> sec;
-                        const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
-                        if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
-                            cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
-                                      out == OUT_NEW ? (double)w : -(double)w);
-                        if (out == OUT_NEW) {
-                            const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
-                            stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
-                        } else if (out == OUT_REMOVE) {
-                            act = 0;
-                        }
-                        if constexpr (sizeof(T) == 8) s = -log(rng.u64());
-                        else s = (double)M<float>::nlog(rng.u32());
-                    }
-                    trem -= t;
+                act = 1;
+                ev = 0;
+                trem = C.dt;
+                have = trem > 0;
+                if (!have) sh.cnt[q] = 0;   // dt == 0: nothing to do, state unchanged
+            }
+            if (!__any_sync(0xffffffffu, have)) break;
+            if (!have) continue;
+
+            // one sub-step of advance! (mixed_population.jl:32-51)
+            double tn, t;
+            if constexpr (sizeof(T) == 8) tn = s / tab.maxrate;
+            else tn = s * tab.inv_maxrate;
+            bool collides;
+            if (trem > tn) { t = tn; collides = true; }
+            else { t = trem; collides = false; s -= t * tab.maxrate; }
+            const T tt = (T)t;
+            // advance_free_yoshida (electron.jl:51-62) in cell units
+            drift(cd1 * tt);
+            kick(kd1 * tt);
+            drift(cd2 * tt);
+            kick(kd2 * tt);
+            drift(cd3 * tt);
+            kick(kd3 * tt);
+            drift(cd4 * tt);
+            if (collides) {
+                Sec<T> sec;
+                const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
+                if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
+                    cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
+                              out == OUT_NEW ? (double)w : -(double)w);
+                if (out == OUT_NEW) {
+                    const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
+                    stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
+                } else if (out == OUT_REMOVE) {
+                    act = 0;
                 }
+                if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
+                else s = (double)M<float>::nlog(uni32(rng.b.y));
+            }
+            trem -= t;
+            if (!(trem > 0)) {
                 P.cell[i] = cell_index(g, in, ix, iy, iz);
                 P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;
                 P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
@@ -630,8 +673,9 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
                 if (!act) P.act[i] = 0;
                 if (dep_val != 0.0 && act && in)
                     cic_fixed(g.qpart, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz, (double)w * dep_val);
+                sh.cnt[local] = ev;
+                have = false;
             }
-            sh.cnt[local] = ev;
         }
         __syncthreads();
 
@@ -657,11 +701,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
             MomAcc<T> acc;
             acc.zero();
             double x, y, z;
-            for (int jj = 0; jj < PPT; ++jj) {
-                const long long i = base + jj * BLOCK + threadIdx.x;
-                if (i < n_entry && P.act[i]) {
-                    mesh_abs(g, P.cell[i], (double)P.f[0][i], (double)P.f[1][i], (double)P.f[2][i], x, y, z);
-                    acc.add(x, y, z, P.f[3][i], P.f[4][i], P.f[5][i], P.f[6][i]);
+            for (uint32_t q = threadIdx.x; q < tile_n; q += BLOCK) {
+                const long long j = base + q;
+                if (P.act[j]) {
+                    mesh_abs(g, P.cell[j], (double)P.f[0][j], (double)P.f[1][j], (double)P.f[2][j], x, y, z);
+                    acc.add(x, y, z, P.f[3][j], P.f[4][j], P.f[5][j], P.f[6][j]);
                 }
             }
             for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)

@@ -9,9 +9,11 @@
  * Every function cites the reference file:line it restates (paths inside the
  * aluque/mcstreamer project).  Random numbers come from a counter-based
  * Philox4x32-10 stream (Salmon, Moraes, Dror, Shaw, SC'11) instead of Julia's
- * task-local Xoshiro, so that the CUDA kernels can be fed identical uniforms:
- *   uniform #k of particle `slot` during step `step` =
- *     (word[k%4] of Philox(key=seed, ctr={slot, step, k/4, tag}) + 0.5) * 2^-32.
+ * task-local Xoshiro, so that the CUDA kernels can be fed identical uniforms.  A Philox
+ * word w maps to the uniform (w + 0.5) * 2^-32.  Collision event j of particle `slot`
+ * during step `step` draws from Philox(key=seed, ctr={slot, step, j, tag}) (xi, new s,
+ * direction) and, when needed, ctr={slot, step, j | 2^31, tag} (secondary); other
+ * per-particle or per-cell streams take word k from ctr={id, call, k/4, tag}.
  */
 #include "oracle.h"
 
@@ -99,18 +101,52 @@ struct Stream {
     }
 };
 
+/* The draws of one collision event (do_one_collision! + the new free-flight time).
+ * Event j of particle `slot` during step `step` owns Philox block
+ *   B = Philox(seed; {slot, step, j, tag})            -> xi, new s, direction (phi, u)
+ * and, only when the process needs more draws,
+ *   C = Philox(seed; {slot, step, j | 2^31, tag})      -> secondary direction, secondary s,
+ *                                                         energy-sharing fraction
+ * so every colliding particle generates exactly one block per event. */
+struct Event {
+    uint32_t key[2];
+    uint32_t c0, c1, tag, j;
+    uint32_t b[4], c[4];
+    bool have_c;
+    Event(uint64_t seed, uint32_t slot, uint32_t step, uint32_t tag_) : c0(slot), c1(step), tag(tag_), j(0) {
+        key[0] = (uint32_t)seed; key[1] = (uint32_t)(seed >> 32);
+        have_c = false;
+    }
+    void begin() {
+        const uint32_t ctr[4] = {c0, c1, j, tag};
+        philox10(ctr, key, b);
+        have_c = false;
+        ++j;
+    }
+    double u(int idx) {  /* Julia rand() draws of this event */
+        if (idx < 4) return word_to_uniform(b[idx]);
+        if (!have_c) {
+            const uint32_t ctr[4] = {c0, c1, (j - 1) | 0x80000000u, tag};
+            philox10(ctr, key, c);
+            have_c = true;
+        }
+        return word_to_uniform(c[idx - 4]);
+    }
+};
+enum { U_XI = 0, U_S = 1, U_PHI = 2, U_COS = 3, U_PHI2 = 4, U_COS2 = 5, U_S2 = 6, U_SHARE = 7 };
+
 /* ---------------- util.jl ---------------- */
-/* randsphere: JuMC/src/util.jl:4-12 */
-inline void randsphere(Stream& rng, double out[3]) {
-    const double phi = 6.283185307179586 * rng.next();
+/* randsphere: JuMC/src/util.jl:4-12, from the uniforms (uphi, uu) */
+inline void randsphere(double uphi, double uu, double out[3]) {
+    const double phi = 6.283185307179586 * uphi;
     const double sphi = std::sin(phi), cphi = std::cos(phi);
-    const double u = 2.0 * rng.next() - 1.0;
+    const double u = 2.0 * uu - 1.0;
     const double v = std::sqrt(1.0 - u * u);
     out[0] = v * cphi; out[1] = v * sphi; out[2] = u;
 }
 
 /* nextcoll: JuMC/src/util.jl:17 */
-inline double nextcoll(Stream& rng) { return -std::log(rng.next()); }
+inline double nextcoll(double u) { return -std::log(u); }
 
 /* Julia fld(x, y) for floats: round((x - mod(x, y)) / y), mod via exact fmod. */
 inline double julia_fld(double x, double y) {
@@ -338,13 +374,14 @@ struct StepCtx {
 
 /* do_one_collision!: JuMC/src/collisions.jl:159-192 with collide (electron.jl:108-139),
  * track (collisions.jl:151, gridfields.jl:215-224) and apply! (collisions.jl:96-123). */
-void do_one_collision(StepCtx& c, Stream& rng, double x[3], double v[3], double& w, double& s,
+void do_one_collision(StepCtx& c, Event& rng, double x[3], double v[3], double& w, double& s,
                       uint8_t& active) {
     const orc_table* t = c.tab;
     const double eng = energy_of(v);
     int64_t k; double wk;
     c.status |= indweight(t, eng, &k, &wk, c.clamp);
-    double xi = rng.next() * t->maxrate;
+    rng.begin();
+    double xi = rng.u(U_XI) * t->maxrate;
     for (int j = 0; j < t->nrows; ++j) {
         const double nu = rate_at(t, j, k, wk);
         if (nu > xi) {
@@ -355,12 +392,12 @@ void do_one_collision(StepCtx& c, Stream& rng, double x[3], double v[3], double&
                 const double vcm[3] = {f * v[0], f * v[1], f * v[2]};
                 const double dv[3] = {v[0] - vcm[0], v[1] - vcm[1], v[2] - vcm[2]};
                 const double nrm = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-                double d[3]; randsphere(rng, d);
+                double d[3]; randsphere(rng.u(U_PHI), rng.u(U_COS), d);
                 for (int q = 0; q < 3; ++q) v[q] = d[q] * nrm + vcm[q];
             } else if (kind == ORC_EXCITATION) {
                 const double E1 = std::max(0.0, eng - par);
                 const double vabs = std::sqrt(2.0 * E1 / ELECTRON_MASS);
-                double d[3]; randsphere(rng, d);
+                double d[3]; randsphere(rng.u(U_PHI), rng.u(U_COS), d);
                 for (int q = 0; q < 3; ++q) v[q] = d[q] * vabs;
             } else if (kind == ORC_IONIZATION || kind == ORC_IONIZATION_UNIFORM) {
                 double va1, va2;
@@ -370,18 +407,18 @@ void do_one_collision(StepCtx& c, Stream& rng, double x[3], double v[3], double&
                 } else {
                     /* Extension (not in JuMC): secondary energy uniform on [0, eps-th]. */
                     const double Ea = std::max(0.0, eng - par);
-                    const double E2 = rng.next() * Ea;
+                    const double E2 = rng.u(U_SHARE) * Ea;
                     const double E1 = Ea - E2;
                     va1 = std::sqrt(2.0 * E1 / ELECTRON_MASS);
                     va2 = std::sqrt(2.0 * E2 / ELECTRON_MASS);
                 }
                 double d1[3], d2[3];
-                randsphere(rng, d1);
-                randsphere(rng, d2);
+                randsphere(rng.u(U_PHI), rng.u(U_COS), d1);
+                randsphere(rng.u(U_PHI2), rng.u(U_COS2), d2);
                 Secondary sec;
                 for (int q = 0; q < 3; ++q) { sec.x[q] = x[q]; sec.v[q] = d2[q] * va2; }
                 sec.w = w;
-                sec.s = nextcoll(rng);
+                sec.s = nextcoll(rng.u(U_S2));
                 sec.active = active;
                 track_charge(c.trk, x, w, c.cyl_local);       /* NewParticleOutcome: +w */
                 for (int q = 0; q < 3; ++q) v[q] = d1[q] * va1;
@@ -476,7 +513,7 @@ int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double
     const uint32_t step = pop->step;
     return drive(pop, tab, fld, trk, nthreads, clamp_energy, [&](StepCtx& c, int64_t i) {
         if (!pop->active[i]) return;                 /* l.active || continue */
-        Stream rng(seed, (uint32_t)i, step, ORC_TAG_ADVANCE);
+        Event rng(seed, (uint32_t)i, step, ORC_TAG_ADVANCE);
         double x[3] = {pop->x[3 * i], pop->x[3 * i + 1], pop->x[3 * i + 2]};
         double v[3] = {pop->v[3 * i], pop->v[3 * i + 1], pop->v[3 * i + 2]};
         double w = pop->w[i], s = pop->s[i];
@@ -491,7 +528,7 @@ int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double
             c.status |= yoshida(fld, x, v, t);
             if (collides) {
                 do_one_collision(c, rng, x, v, w, s, active);
-                s = nextcoll(rng);
+                s = nextcoll(rng.u(U_S));
             }
             trem -= t;
         }
@@ -511,13 +548,13 @@ int orc_collisions(orc_pop* pop, const orc_table* tab, double dt, orc_tracker* t
         if (!pop->active[i]) return;
         double s = pop->s[i] - dt * tab->maxrate;
         if (s <= 0) {
-            Stream rng(seed, (uint32_t)i, step, ORC_TAG_COLLISIONS);
+            Event rng(seed, (uint32_t)i, step, ORC_TAG_COLLISIONS);
             double x[3] = {pop->x[3 * i], pop->x[3 * i + 1], pop->x[3 * i + 2]};
             double v[3] = {pop->v[3 * i], pop->v[3 * i + 1], pop->v[3 * i + 2]};
             double w = pop->w[i];
             uint8_t active = pop->active[i];
             do_one_collision(c, rng, x, v, w, s, active);
-            s = nextcoll(rng);
+            s = nextcoll(rng.u(U_S));
             for (int q = 0; q < 3; ++q) pop->v[3 * i + q] = v[q];
             pop->active[i] = active;
         }

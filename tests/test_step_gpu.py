@@ -1,8 +1,9 @@
 """Per-particle parity of the electron step (advance!, collisions!) against the CPU oracle.
 
-Both sides consume identical Philox uniforms (slot, step, k), so a single step matches the
-FP64 oracle per particle (rel 1e-12 in FP64 mode) and, in FP32 mode, within rel 1e-5 except
-for particles whose discrete decisions flip (counted and bounded).
+Both sides consume identical Philox uniforms (one block per collision event, keyed by slot,
+step and event number), so a single step matches the FP64 oracle per particle (rel 1e-12 in
+FP64 mode) and, in FP32 mode, within rel 1e-5 except for particles whose discrete decisions
+flip (counted and bounded).
 """
 import numpy as np
 import pytest
@@ -44,7 +45,6 @@ def test_advance_fp64_one_step_matches_oracle(ctx, uniform_sharing):
     g, o = pop.download(), oracle_arrays(opop)
     assert g.n == o.n, (g.n, o.n)
     assert g.n > n, "no ionization happened; the test needs secondaries"
-    assert (o.active[:n] == 0).sum() > 0, "no attachment happened"
     bad = particle_mismatch(g, o, RTOL64, xatol=1e-30, vatol=1e-30)
     assert bad.sum() == 0, f"{bad.sum()} of {g.n} slots differ; worst x {relerr(g.x, o.x).max():.3g}"
     _close(pop, fld, tab)
@@ -61,6 +61,7 @@ def test_advance_fp64_multistep_matches_oracle(ctx):
         assert po.advance(opop, otab, of, 1e-13) == 0
     g, o = pop.download(), oracle_arrays(opop)
     assert g.n == o.n
+    assert (o.active == 0).sum() > 0, "no attachment happened; the test needs removals"
     bad = particle_mismatch(g, o, 1e-11, xatol=1e-30, vatol=1e-30)
     assert bad.sum() == 0, f"{bad.sum()} slots differ"
     assert pop.step == 20
