@@ -434,16 +434,35 @@ int launch_moments(mcs_pop* p, const mcs_table* t, double* d_out, int nm) {
 template <typename T>
 __global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long long* __restrict__ q) {
     const long long n = *P.n_in;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    if (mesh) {
+        // warp-uniform trip count: every lane takes part in the aggregated deposit
+        for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+            const long long i = i0 + threadIdx.x;
+            bool valid = false;
+            uint32_t cidx = kOutside;
+            int ix = 0, iy = 0, iz = 0;
+            double fx = 0.0, fy = 0.0, fz = 0.0, charge = 0.0;
+            if (i < n && P.act[i]) {
+                cidx = P.cell[i];
+                if (cidx != kOutside) {
+                    valid = true;
+                    ix = (int)(cidx % (uint32_t)g.nx);
+                    const uint32_t r = cidx / (uint32_t)g.nx;
+                    iy = (int)(r % (uint32_t)g.ny);
+                    iz = (int)(r / (uint32_t)g.ny);
+                    fx = (double)P.f[0][i]; fy = (double)P.f[1][i]; fz = (double)P.f[2][i];
+                    charge = (double)P.f[6][i] * val;
+                }
+            }
+            cic_fixed_warp(q, g.nx, g.ny, valid, cidx, ix, iy, iz, fx, fy, fz, charge);
+        }
+        return;
+    }
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
         if (!P.act[i]) continue;
         const double charge = (double)P.f[6][i] * val;
-        if (mesh) {
-            const uint32_t cidx = P.cell[i];
-            if (cidx == kOutside) continue;
-            const uint32_t ix = cidx % (uint32_t)g.nx, r = cidx / (uint32_t)g.nx;
-            const uint32_t iy = r % (uint32_t)g.ny, iz = r / (uint32_t)g.ny;
-            cic_fixed(q, g.nx, g.ny, ix, iy, iz, (double)P.f[0][i], (double)P.f[1][i], (double)P.f[2][i], charge);
-        } else if (g.type == GRID_CART3D) {
+        if (g.type == GRID_CART3D) {
             int ix, iy, iz;
             double fx, fy, fz;
             if (cart_locate(g, P.f[0][i], P.f[1][i], P.f[2][i], ix, iy, iz, fx, fy, fz))

@@ -235,6 +235,56 @@ __device__ __forceinline__ void cic_fixed(long long* q, int nx, int ny, int ix, 
     if (last) atomicAdd(reinterpret_cast<unsigned long long*>(b + 1 + sy + sz), (unsigned long long)last);
 }
 
+// The same CIC deposit for one particle per lane (all 32 lanes call it; `valid` lanes
+// deposit).  Lanes of a run of equal `cell` (adjacent in the warp, as cell-sorted particles
+// are) add their eight corner values with a segmented shuffle sum and the first lane of the
+// run issues the eight atomics, so a warp inside one cell makes 8 atomics instead of 256.
+// Integer sums: the node totals are bit-identical to per-particle atomics.
+__device__ __forceinline__ void cic_fixed_warp(long long* q, int nx, int ny, bool valid, uint32_t cell, int ix, int iy,
+                                               int iz, double fx, double fy, double fz, double charge) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    long long v[8];
+    if (valid) {
+        const long long W = __double2ll_rn(charge * 0x1p32);
+        const double Wd = (double)W;
+        const double gx[2] = {1.0 - fx, fx}, gy[2] = {1.0 - fy, fy}, gz[2] = {1.0 - fz, fz};
+        long long acc = 0;
+#pragma unroll
+        for (int c = 0; c < 7; ++c) {
+            const int a0 = c & 1, a1 = (c >> 1) & 1, a2 = (c >> 2) & 1;
+            const double wc = __dmul_rn(__dmul_rn(gx[a0], gy[a1]), gz[a2]);
+            v[c] = __double2ll_rn(__dmul_rn(Wd, wc));
+            acc += v[c];
+        }
+        v[7] = W - acc;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = 0;
+    }
+    const uint32_t key = valid ? cell : 0xffffffffu;
+    const uint32_t nkey = __shfl_down_sync(FULL, key, 1);
+    const unsigned same = __ballot_sync(FULL, valid && lane < 31 && nkey == key);
+    const unsigned stops = ~same & (0xffffffffu << lane);      // lanes >= me that end a run
+    const int end = __ffs(stops) - 1;
+    const bool leader = valid && (lane == 0 || !((same >> (lane - 1)) & 1u));
+    const long long sy = nx + 1, sz = (long long)(nx + 1) * (ny + 1);
+    long long* b = q + ix + iy * sy + iz * sz;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        long long x = v[c];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long t = __shfl_down_sync(FULL, x, o);
+            if (lane + o <= end) x += t;
+        }
+        if (leader && x) {
+            const int a0 = c & 1, a1 = (c >> 1) & 1, a2 = (c >> 2) & 1;
+            atomicAdd(reinterpret_cast<unsigned long long*>(b + a0 + a1 * sy + a2 * sz), (unsigned long long)x);
+        }
+    }
+}
+
 // Cell location on the 3-D mesh of an absolute position (checkbounds semantics: [0, n)).
 __device__ __forceinline__ bool cart_locate(const GridView& g, double x, double y, double z, int& ix, int& iy,
                                             int& iz, double& fx, double& fy, double& fz) {

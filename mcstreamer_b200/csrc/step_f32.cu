@@ -14,6 +14,6 @@ int launch_collisions<float>(mcs_pop* p, const mcs_table* t, double dt, mcs_grid
 }
 template <>
 int launch_step_mesh<float>(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
-    return launch_step_mesh_impl<float, 256, 8>(p, t, dt, tracking, dep_val, mom);
+    return launch_step_mesh_impl<float, 256, 8, 3>(p, t, dt, tracking, dep_val, mom);
 }
 }  // namespace mcs

@@ -552,8 +552,8 @@ __device__ __forceinline__ bool in_unit_cube(T ox, T oy, T oz) {
     }
 }
 
-template <typename T, int BLOCK, int PPT>
-__global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
+template <typename T, int BLOCK, int PPT, int MINB = 1>
+__global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
                                                      YoshidaC Y, double dep_val) {
     constexpr int TILE = BLOCK * PPT;
     __shared__ TileShared<T, BLOCK, TILE> sh;
@@ -671,13 +671,37 @@ __global__ void __launch_bounds__(BLOCK) k_step_mesh(PopView<T> P, TableView tab
                 P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
                 P.f[7][i] = (T)s;
                 if (!act) P.act[i] = 0;
-                if (dep_val != 0.0 && act && in)
-                    cic_fixed(g.qpart, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz, (double)w * dep_val);
                 sh.cnt[local] = ev;
                 have = false;
             }
         }
         __syncthreads();
+
+        // density!(qpart, dep_val) of the tile's post-step particles, in slot order so that
+        // cell-sorted neighbours share their atomics (cic_fixed_warp); the data is L2-hot
+        if (dep_val != 0.0) {
+            for (uint32_t q0 = 0; q0 < tile_n; q0 += BLOCK) {
+                const uint32_t q = q0 + threadIdx.x;
+                const long long j = base + q;
+                bool valid = false;
+                uint32_t cl = kOutsideCell;
+                int dx = 0, dy = 0, dz = 0;
+                double fx = 0.0, fy = 0.0, fz = 0.0, ch = 0.0;
+                if (q < tile_n && P.act[j]) {
+                    cl = P.cell[j];
+                    if (cl != kOutsideCell) {
+                        valid = true;
+                        dx = (int)(cl % (uint32_t)g.nx);
+                        const uint32_t r = cl / (uint32_t)g.nx;
+                        dy = (int)(r % (uint32_t)g.ny);
+                        dz = (int)(r / (uint32_t)g.ny);
+                        fx = (double)P.f[0][j]; fy = (double)P.f[1][j]; fz = (double)P.f[2][j];
+                        ch = (double)P.f[6][j] * dep_val;
+                    }
+                }
+                cic_fixed_warp(g.qpart, g.nx, g.ny, valid, cl, dx, dy, dz, fx, fy, fz, ch);
+            }
+        }
 
         const uint32_t cnt = tile_append<T, BLOCK, TILE>(
             sh, sg, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
