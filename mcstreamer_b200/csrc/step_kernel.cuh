@@ -600,7 +600,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             vx += k * ex; vy += k * ey; vz += k * ez;
         };
 
+        bool pending = false;   // finished particle not yet written back
         for (;;) {
+            // Finished lanes wait until a quarter of the warp is idle (or all of it), then
+            // write back and refill together: the store/load path runs with many lanes
+            // active instead of once per finishing lane.
+            const unsigned idle = __ballot_sync(0xffffffffu, !have);
+            if (idle != 0xffffffffu && __popc(idle) < 8) goto substep;
+            if (!have && pending) {
+                P.cell[i] = cell_index(g, in, ix, iy, iz);
+                P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;
+                P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
+                P.f[7][i] = (T)s;
+                if (!act) P.act[i] = 0;
+                sh.cnt[local] = ev;
+                pending = false;
+            }
             // refill: an idle lane takes the next particle of the tile
             while (!have && !drained) {
                 const uint32_t q = atomicAdd(&sh.next, 1u);
@@ -631,6 +646,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 if (!have) sh.cnt[q] = 0;   // dt == 0: nothing to do, state unchanged
             }
             if (!__any_sync(0xffffffffu, have)) break;
+        substep:
             if (!have) continue;
 
             // one sub-step of advance! (mixed_population.jl:32-51)
@@ -666,13 +682,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             }
             trem -= t;
             if (!(trem > 0)) {
-                P.cell[i] = cell_index(g, in, ix, iy, iz);
-                P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;
-                P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
-                P.f[7][i] = (T)s;
-                if (!act) P.act[i] = 0;
-                sh.cnt[local] = ev;
                 have = false;
+                pending = true;
             }
         }
         __syncthreads();
