@@ -448,6 +448,8 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     cudaFree(p->act); cudaFree(p->cell); cudaFree(p->d_n); cudaFree(p->tile_status);
     cudaFree(p->tile_partials); cudaFree(p->counters); cudaFree(p->d_moments); cudaFree(p->staging);
     cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage); cudaFree(p->d_log);
+    for (int q = 0; q < 2; ++q) { cudaFree(p->sort_key[q]); cudaFree(p->sort_val[q]); }
+    cudaFree(p->sort_hist); cudaFree(p->sort_hoff); cudaFree(p->seg_a); cudaFree(p->seg_b);
     delete p;
     return MCS_OK;
 }

@@ -134,6 +134,12 @@ struct mcs_pop {
     uint8_t* alt_act = nullptr;
     void* stage = nullptr;         // secondary staging of the step kernels
     size_t stage_bytes = 0;
+    uint32_t* sort_key[2] = {nullptr, nullptr};   // radix sort ping-pong (cap entries)
+    uint32_t* sort_val[2] = {nullptr, nullptr};
+    uint32_t* sort_hist = nullptr;                // [256][tiles] counts, then offsets
+    uint32_t* sort_hoff = nullptr;
+    uint32_t* seg_a = nullptr;                    // resample segment scratch (cap entries)
+    uint32_t* seg_b = nullptr;
     double* d_log = nullptr;       // per-step fused moments, log_cap entries of kStepMoments
     int log_cap = 0;
     uint32_t log_step0 = 0;

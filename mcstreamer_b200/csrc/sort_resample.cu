@@ -1,11 +1,409 @@
-// sort_resample.cu -- cell-key radix sort and per-cell resampling (placeholder entry points).
+// sort_resample.cu -- cell-key radix sort of the population and the per-cell Russian
+// roulette / splitting of MCStreamer's resample! (MCStreamer/src/resample.jl:7-84).
+//
+// mcs_sort_cells: stable LSD radix sort of (cell key, slot) with 8-bit digits; only as many
+// passes as the key range needs (keys are cell indices; inactive or out-of-grid particles
+// get the key `ncells` and go last).  Each pass: per-tile digit histograms, one device-wide
+// scan of the (digit, tile) table, and a stable scatter ranked with warp match-any.  A
+// final gather permutes every population array.  Stability keeps the particles of a cell
+// in ascending original slot order: the order in which the reference's serial passes
+// visit them.
+//
+// mcs_resample_cells: after the sort every cell is a contiguous segment.  One thread per
+// segment restates resample.jl's two passes serially in slot order (so the weight sums and
+// the roulette sequence are the reference's), first only counting the clones, then -- after
+// a scan of the counts gives each cell its place -- writing them.  Clones are appended in
+// cell order, which is the slot order of the sorted population (the serial reference's
+// append order).  Uniforms: one Philox stream per cell, ctr = {cell, call, k/4, tag}.
 #include "host_util.h"
+#include "pop_ops.h"
+#include "step.cuh"
+
+namespace mcs {
+
+namespace {
+
+constexpr int SB = 256;            // threads per block
+constexpr int SI = 16;             // keys per thread per tile
+constexpr int STILE = SB * SI;     // 4096 keys per tile
+constexpr int RADIX = 256;
+
+// ---- keys ----
+template <typename T>
+__global__ void k_keys(PopView<T> P, GridView g, int mesh, uint32_t ncells, uint32_t* __restrict__ key,
+                       uint32_t* __restrict__ val) {
+    const long long n = *P.n_in;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        uint32_t k = ncells;
+        if (P.act[i]) {
+            if (mesh) {
+                const uint32_t c = P.cell[i];
+                k = c == 0xffffffffu ? ncells : c;
+            } else if (g.type == GRID_CART3D) {
+                int ix, iy, iz;
+                double fx, fy, fz;
+                if (cart_locate(g, P.f[0][i], P.f[1][i], P.f[2][i], ix, iy, iz, fx, fy, fz))
+                    k = (uint32_t)ix + (uint32_t)g.nx * ((uint32_t)iy + (uint32_t)g.ny * (uint32_t)iz);
+            } else {
+                // cellindex, MCStreamer/src/grid.jl:84-90, over p's (0:M+1, 0:N+1)
+                const double x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
+                const double rho = sqrt(x * x + y * y);
+                double fi = floor(rho / g.dr);
+                if (__fma_rn(fi, g.dr, -rho) > 0.0) fi -= 1.0;
+                double fj = floor(z / g.dz);
+                if (__fma_rn(fj, g.dz, -z) > 0.0) fj -= 1.0;
+                fi += 1.0; fj += 1.0;
+                if (fi >= 0.0 && fi <= g.M + 1.0 && fj >= 0.0 && fj <= g.N + 1.0)
+                    k = (uint32_t)fi + (uint32_t)(g.M + 2) * (uint32_t)fj;
+            }
+        }
+        key[i] = k;
+        val[i] = (uint32_t)i;
+    }
+}
+
+// ---- radix pass: histogram ----
+__global__ void __launch_bounds__(SB) k_hist(const uint32_t* __restrict__ key, const long long* n_ptr, int shift,
+                                             uint32_t* __restrict__ hist, long long ntiles_max) {
+    __shared__ uint32_t h[RADIX];
+    const long long n = *n_ptr;
+    const long long ntiles = (n + STILE - 1) / STILE;
+    for (long long tile = blockIdx.x; tile < ntiles_max; tile += gridDim.x) {
+        for (int d = threadIdx.x; d < RADIX; d += SB) h[d] = 0;
+        __syncthreads();
+        if (tile < ntiles) {
+            const long long base = tile * STILE;
+            for (int it = 0; it < SI; ++it) {
+                const long long i = base + (long long)it * SB + threadIdx.x;
+                if (i < n) atomicAdd(&h[(key[i] >> shift) & 0xffu], 1u);
+            }
+        }
+        __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += SB) hist[(long long)d * ntiles_max + tile] = h[d];
+        __syncthreads();
+    }
+}
+
+// ---- radix pass: stable scatter.  Rounds of SB keys (thread t holds key r*SB + t), each
+// ranked by warp match-any and a per-digit prefix over the block's warps. ----
+__global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                const long long* n_ptr, int shift, const uint32_t* __restrict__ offs,
+                                                long long ntiles_max) {
+    constexpr int NW = SB / 32;
+    __shared__ uint32_t run[RADIX];          // keys of each digit placed by earlier rounds
+    __shared__ uint32_t wcnt[NW][RADIX];     // this round: per-warp digit counts -> exclusive prefix
+    __shared__ uint32_t base_off[RADIX];
+    const long long n = *n_ptr;
+    const long long ntiles = (n + STILE - 1) / STILE;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int d = threadIdx.x; d < RADIX; d += SB) {
+            run[d] = 0;
+            base_off[d] = offs[(long long)d * ntiles_max + tile];
+        }
+        __syncthreads();
+        const long long base = tile * STILE;
+        for (int r = 0; r < SI; ++r) {
+            for (int d = threadIdx.x; d < NW * RADIX; d += SB) (&wcnt[0][0])[d] = 0;
+            __syncthreads();
+            const long long i = base + (long long)r * SB + threadIdx.x;
+            const bool ok = i < n;
+            const uint32_t k = ok ? kin[i] : 0u;
+            const uint32_t v = ok ? vin[i] : 0u;
+            const uint32_t dg = ok ? ((k >> shift) & 0xffu) : 0x100u;
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            const uint32_t rank_w = __popc(peers & lt);
+            if (ok && rank_w == 0) wcnt[wid][dg] = __popc(peers);
+            __syncthreads();
+            // exclusive prefix over warps per digit, then fold into run[]
+            for (int d = threadIdx.x; d < RADIX; d += SB) {
+                uint32_t acc = run[d];
+                for (int w2 = 0; w2 < NW; ++w2) { const uint32_t c = wcnt[w2][d]; wcnt[w2][d] = acc; acc += c; }
+                run[d] = acc;
+            }
+            __syncthreads();
+            if (ok) {
+                const uint32_t pos = base_off[dg] + wcnt[wid][dg] + rank_w;
+                kout[pos] = k;
+                vout[pos] = v;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+struct DstArrays {
+    void* f[8];
+    uint32_t* cell;
+    uint8_t* act;
+};
+
+template <typename T>
+__global__ void k_gather(PopView<T> P, const uint32_t* __restrict__ perm, DstArrays d) {
+    const long long n = *P.n_in;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const uint32_t s = perm[j];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) static_cast<T*>(d.f[q])[j] = P.f[q][s];
+        if (d.cell) d.cell[j] = P.cell[s];
+        d.act[j] = P.act[s];
+    }
+}
+
+__global__ void k_set_ll(long long* p, long long v) { *p = v; }
+
+uint32_t grid_cells(const mcs_grid* g) {
+    if (g->v.type == GRID_CART3D) return (uint32_t)((long long)g->v.nx * g->v.ny * g->v.nz);
+    return (uint32_t)((g->v.M + 2) * (g->v.N + 2));
+}
+
+template <typename P>
+int ensure(mcs_ctx* c, P** p, size_t n) {
+    if (*p) return MCS_OK;
+    if (cudaMalloc(reinterpret_cast<void**>(p), (n ? n : 1) * sizeof(P)) != cudaSuccess) {
+        *p = nullptr;
+        return set_err(c, MCS_ERR_NOMEM, "sort / resample scratch allocation failed");
+    }
+    return MCS_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Per-cell resampling: resample.jl:16-76 restated for one segment (cell) per thread.
+// ---------------------------------------------------------------------------------------
+// Segment starts: seg_start[s] = first sorted slot of cell s (keys < ncells only).
+__global__ void k_seg_flags(const uint32_t* __restrict__ key, const long long* n_ptr, uint32_t ncells,
+                            uint32_t* __restrict__ flag) {
+    const long long n = *n_ptr;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+        const uint32_t k = key[j];
+        flag[j] = (k < ncells && (j == 0 || key[j - 1] != k)) ? 1u : 0u;
+    }
+}
+
+__global__ void k_seg_starts(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                             const long long* n_ptr, uint32_t* __restrict__ start) {
+    const long long n = *n_ptr;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+        if (flag[j]) start[pos[j]] = (uint32_t)j;
+}
+
+struct ResampleArgs {
+    const uint32_t* key;     // sorted keys
+    const uint32_t* start;   // segment starts
+    const long long* nseg;   // number of segments
+    const long long* n;      // particles (sorted)
+    uint32_t ncells;
+    int ntarget, nmax;
+    unsigned long long seed;
+    uint32_t call;
+};
+
+// One segment: pass 1 then pass 2 of resample!.  WRITE=false only counts the clones.
+template <typename T, bool WRITE>
+__device__ uint32_t resample_segment(const ResampleArgs& a, PopView<T>& P, long long s, long long clone_base,
+                                     long long cap, uint32_t* status) {
+    const long long n = *a.n;
+    const long long b = a.start[s];
+    const uint32_t cell = a.key[b];
+    long long e = b;
+    while (e < n && a.key[e] == cell) ++e;
+    Rng rng;
+    rng.init(a.seed, cell, a.call, TAG_CELL_RESAMPLE);
+    // pass 1 (resample.jl:16-29): count, total weight, first sample when p reaches nmax
+    long long p = 0;
+    double wtotal = 0.0, x = 0.0;
+    for (long long j = b; j < e; ++j) {
+        p += 1;
+        wtotal += (double)P.f[6][j];
+        if (p == a.nmax) x = 1.0 - pow(1.0 - rng.u64(), 1.0 / (double)a.ntarget);   // samplemin(ntarget)
+    }
+    // pass 2 (resample.jl:31-76)
+    long long pk = 0;
+    double wcum = 0.0;
+    uint32_t ncl = 0;
+    for (long long j = b; j < e; ++j) {
+        const double wj = (double)P.f[6][j];
+        if (p > a.nmax) {
+            while (wtotal * x < wcum + wj && pk < a.ntarget) {
+                pk += 1;
+                if (WRITE) {
+                    const long long d = clone_base + ncl;
+                    if (d < cap) {
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) P.f[q][d] = P.f[q][j];
+                        if (P.cell) P.cell[d] = P.cell[j];
+                        P.act[d] = P.act[j];
+                        P.f[6][d] = (T)(wtotal / (double)a.ntarget);
+                    } else {
+                        atomicOr(status, ST_CAPACITY);
+                    }
+                }
+                ++ncl;
+                if (pk < a.ntarget) x += (1.0 - pow(1.0 - rng.u64(), 1.0 / (double)(a.ntarget - pk))) * (1.0 - x);
+            }
+            wcum += wj;
+            if (WRITE) P.act[j] = 0;   // remove_particle!
+        } else if (p < a.ntarget && wj > 2) {
+            const double wnew = rint(wj / 2.0);   // Julia round: nearest, ties to even
+            if (WRITE) {
+                const long long d = clone_base + ncl;
+                if (d < cap) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) P.f[q][d] = P.f[q][j];
+                    if (P.cell) P.cell[d] = P.cell[j];
+                    P.act[d] = P.act[j];
+                    P.f[6][d] = (T)wnew;
+                } else {
+                    atomicOr(status, ST_CAPACITY);
+                }
+                P.f[6][j] = (T)(wj - wnew);
+            }
+            ++ncl;
+            p += 1;
+        }
+    }
+    return ncl;
+}
+
+template <typename T>
+__global__ void k_resample_count(ResampleArgs a, PopView<T> P, uint32_t* __restrict__ counts, uint32_t* status) {
+    const long long nseg = *a.nseg;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x)
+        counts[s] = resample_segment<T, false>(a, P, s, 0, 0, status);
+}
+
+template <typename T>
+__global__ void k_resample_write(ResampleArgs a, PopView<T> P, const uint32_t* __restrict__ offs,
+                                 const long long* total, uint32_t* status) {
+    const long long nseg = *a.nseg;
+    const long long n = *a.n;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x)
+        resample_segment<T, true>(a, P, s, n + (long long)offs[s], P.cap, status);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        long long m = n + *total;
+        if (m > P.cap) { m = P.cap; atomicOr(status, ST_CAPACITY); }
+        *P.n_out = m;
+    }
+}
+
+}  // namespace
+
+// Sort the population by cell key; on return the sorted keys are in *keys_out (device).
+template <typename T>
+int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
+    mcs_ctx* c = p->ctx;
+    const size_t cap = (size_t)p->cap;
+    const long long ntiles_max = (p->cap + STILE - 1) / STILE;
+    for (int q = 0; q < 2; ++q) {
+        if (int st = ensure(c, &p->sort_key[q], cap)) return st;
+        if (int st = ensure(c, &p->sort_val[q], cap)) return st;
+    }
+    if (int st = ensure(c, &p->sort_hist, (size_t)RADIX * ntiles_max)) return st;
+    if (int st = ensure(c, &p->sort_hoff, (size_t)RADIX * ntiles_max)) return st;
+    const uint32_t ncells = grid_cells(g);
+    int nbits = 1;
+    while (nbits < 32 && ((1ull << nbits) <= (unsigned long long)ncells)) ++nbits;
+    const int passes = (nbits + 7) / 8;
+    const int mesh = p->cells != nullptr;
+    const long long* n_dev = p->d_n + p->cur;
+    const int gr = grid_for(c, p->cap, 256);
+    k_keys<T><<<gr, 256, 0, c->stream>>>(pop_view<T>(p), g->v, mesh, ncells, p->sort_key[0], p->sort_val[0]);
+    MCS_CK_LAUNCH(c);
+    long long* nhist = reinterpret_cast<long long*>(p->counters + 8);
+    k_set_ll<<<1, 1, 0, c->stream>>>(nhist, (long long)RADIX * ntiles_max);
+    MCS_CK_LAUNCH(c);
+    int cur = 0;
+    long long gs = ntiles_max;
+    if (gs > (long long)c->num_sms * 8) gs = (long long)c->num_sms * 8;
+    for (int ps = 0; ps < passes; ++ps) {
+        const int shift = 8 * ps;
+        k_hist<<<(int)gs, SB, 0, c->stream>>>(p->sort_key[cur], n_dev, shift, p->sort_hist, ntiles_max);
+        MCS_CK_LAUNCH(c);
+        if (int st = launch_scan(p, p->sort_hist, p->sort_hoff, nhist, nullptr)) return st;
+        k_scatter<<<(int)gs, SB, 0, c->stream>>>(p->sort_key[cur], p->sort_val[cur], p->sort_key[cur ^ 1],
+                                                 p->sort_val[cur ^ 1], n_dev, shift, p->sort_hoff, ntiles_max);
+        MCS_CK_LAUNCH(c);
+        cur ^= 1;
+    }
+    // permute every population array into the second buffer set, then swap the sets
+    for (int q = 0; q < 8; ++q)
+        if (!p->alt[q] && cudaMalloc(&p->alt[q], cap * p->esz) != cudaSuccess)
+            return set_err(c, MCS_ERR_NOMEM, "sort buffers");
+    if (int st = ensure(c, &p->alt_act, cap)) return st;
+    if (p->cell)
+        if (int st = ensure(c, &p->alt_cell, cap)) return st;
+    DstArrays d;
+    for (int q = 0; q < 8; ++q) d.f[q] = p->alt[q];
+    d.cell = p->cell ? p->alt_cell : nullptr;
+    d.act = p->alt_act;
+    k_gather<T><<<gr, 256, 0, c->stream>>>(pop_view<T>(p), p->sort_val[cur], d);
+    MCS_CK_LAUNCH(c);
+    for (int q = 0; q < 8; ++q) std::swap(p->f[q], p->alt[q]);
+    std::swap(p->act, p->alt_act);
+    if (p->cell) std::swap(p->cell, p->alt_cell);
+    if (keys_out) *keys_out = p->sort_key[cur];
+    return MCS_OK;
+}
+
+template <typename T>
+int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
+    mcs_ctx* c = p->ctx;
+    uint32_t* keys = nullptr;
+    if (int st = sort_cells_t<T>(p, g, &keys)) return st;
+    if (int st = ensure(c, &p->seg_a, (size_t)p->cap)) return st;
+    if (int st = ensure(c, &p->seg_b, (size_t)p->cap)) return st;
+    const uint32_t ncells = grid_cells(g);
+    const long long* n_dev = p->d_n + p->cur;
+    long long* nseg = reinterpret_cast<long long*>(p->counters + 10);
+    long long* total = reinterpret_cast<long long*>(p->counters + 12);
+    const int gr = grid_for(c, p->cap, 256);
+    // segments: flags -> positions -> starts
+    k_seg_flags<<<gr, 256, 0, c->stream>>>(keys, n_dev, ncells, p->seg_a);
+    MCS_CK_LAUNCH(c);
+    if (int st = launch_scan(p, p->seg_a, p->seg_b, n_dev, nseg)) return st;
+    k_seg_starts<<<gr, 256, 0, c->stream>>>(p->seg_a, p->seg_b, n_dev, p->u32a);
+    MCS_CK_LAUNCH(c);
+    ResampleArgs a;
+    a.key = keys;
+    a.start = p->u32a;
+    a.nseg = nseg;
+    a.n = n_dev;
+    a.ncells = ncells;
+    a.ntarget = ntarget;
+    a.nmax = nmax;
+    a.seed = p->seed;
+    a.call = p->resample_calls++;
+    k_resample_count<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, c->d_status);
+    MCS_CK_LAUNCH(c);
+    if (int st = launch_scan(p, p->seg_a, p->seg_b, nseg, total)) return st;
+    PopView<T> P = pop_view<T>(p);
+    k_resample_write<T><<<gr, 128, 0, c->stream>>>(a, P, p->seg_b, total, c->d_status);
+    MCS_CK_LAUNCH(c);
+    p->cur ^= 1;
+    return MCS_OK;
+}
+
+}  // namespace mcs
+
+using namespace mcs;
 
 extern "C" {
-MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid*) {
-    return mcs::set_err(p ? p->ctx : nullptr, MCS_ERR_UNSUPPORTED, "sort not built yet");
+
+MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid* g) {
+    if (!p || !g) return MCS_ERR_ARG;
+    if (p->cells && p->cells != g) return set_err(p->ctx, MCS_ERR_UNSUPPORTED, "sort by another mesh");
+    if (cudaSetDevice(p->ctx->device) != cudaSuccess) return MCS_ERR_CUDA;
+    return p->precision == MCS_FP32 ? sort_cells_t<float>(p, g, nullptr) : sort_cells_t<double>(p, g, nullptr);
 }
-MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid*, int, int) {
-    return mcs::set_err(p ? p->ctx : nullptr, MCS_ERR_UNSUPPORTED, "resample not built yet");
+
+MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
+    if (!p || !g || ntarget < 1 || nmax < 1) return MCS_ERR_ARG;
+    if (p->cells && p->cells != g) return set_err(p->ctx, MCS_ERR_UNSUPPORTED, "resample on another mesh");
+    if (cudaSetDevice(p->ctx->device) != cudaSuccess) return MCS_ERR_CUDA;
+    return p->precision == MCS_FP32 ? resample_cells_t<float>(p, g, ntarget, nmax)
+                                    : resample_cells_t<double>(p, g, ntarget, nmax);
 }
-}
+
+}  // extern "C"

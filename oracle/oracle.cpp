@@ -701,7 +701,8 @@ int orc_sort_cells(orc_pop* pop, const orc_field* g) {
     const int64_t n = pop->n;
     std::vector<int64_t> key(n), idx(n);
     for (int64_t i = 0; i < n; ++i) {
-        int64_t k = orc_cell_key(g, &pop->x[3 * i]);
+        /* inactive and out-of-grid particles go last */
+        int64_t k = pop->active[i] ? orc_cell_key(g, &pop->x[3 * i]) : -1;
         key[i] = k < 0 ? INT64_MAX : k;
         idx[i] = i;
     }

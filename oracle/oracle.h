@@ -94,7 +94,7 @@ void orc_moments(const orc_pop* pop, const orc_table* tab, double* out); /* R13 
 /* ---- cells, deposit, resample ---- */
 /* cell key of a position: cart3d (ix + nx*(iy + ny*iz)) / cyl (i + (M+2)*j); -1 if out. */
 int64_t orc_cell_key(const orc_field* grid, const double x[3]);
-/* stable sort of the population by cell key (out-of-grid last), R11 ordering. */
+/* stable sort of the population by cell key (inactive and out-of-grid last), R11 ordering. */
 int orc_sort_cells(orc_pop* pop, const orc_field* grid);
 int orc_resample_cells(orc_pop* pop, const orc_field* grid, int ntarget, int nmax,
                        uint32_t call);                             /* R11 */

@@ -1,0 +1,95 @@
+"""Cell-key radix sort and per-cell resampling (resample!, MCStreamer/src/resample.jl:7-84)
+against the CPU oracle, which restates the reference's serial passes on the population
+sorted with a stable sort (so both append clones in the same order)."""
+import numpy as np
+import pytest
+
+from mcstreamer_b200 import constants as co
+from mcstreamer_b200 import jumc, lxcat, streamer
+from oracle import pyoracle as po
+from tests.helpers import broad, oracle_arrays, oracle_pop
+
+NX, NY, NZ, H = 8, 8, 16, 4e-6
+CENTRE = (NX * H / 2, NY * H / 2, NZ * H / 2)
+
+
+def _cloud(n, seed, spread=5e-6):
+    p = broad(n, seed, emax_ev=10.0, x0=CENTRE, spread=spread)
+    rng = np.random.default_rng(seed + 1)
+    p.w[:] = np.rint(10 ** rng.uniform(0, 3, n))      # integer weights 1..1000 (splits need w > 2)
+    p.active[rng.random(n) < 0.05] = 0
+    return p
+
+
+def _setup(ctx, n, precision="fp64", mesh=False, seed=7, capf=4):
+    t = lxcat.synthetic_table(0)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.Grid3D(NX, NY, NZ, H, precision=precision, ctx=ctx)
+    p0 = _cloud(n, seed)
+    pop = jumc.Population(capf * n, p0, tab, precision=precision, seed=seed, mesh=grid if mesh else None)
+    ofield = po.field_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0), np.zeros(3 * (NX + 1) * (NY + 1) * (NZ + 1)))
+    return tab, grid, p0, pop, ofield
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mesh", [False, True])
+def test_sort_is_stable_by_cell(ctx, mesh):
+    n = 200_000
+    tab, grid, p0, pop, ofield = _setup(ctx, n, mesh=mesh)
+    ctx.check(ctx.lib.mcs_sort_cells(pop.h, grid.h_))
+    g = pop.download()
+    key = np.where(p0.active == 1, grid.cell_key(p0.x), np.iinfo(np.int64).max)
+    order = np.argsort(key, kind="stable")
+    np.testing.assert_array_equal(g.active, p0.active[order])
+    np.testing.assert_array_equal(g.s, p0.s[order])
+    np.testing.assert_array_equal(g.w, p0.w[order])
+    if not mesh:
+        np.testing.assert_array_equal(g.x, p0.x[order])
+    # the oracle's restated sort gives the same permutation
+    op = oracle_pop(p0, n, 0)
+    po.sort_cells(op, ofield)
+    o = oracle_arrays(op)
+    np.testing.assert_array_equal(g.s, o.s)
+    pop.close(); grid.close(); tab.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ntarget,nmax", [(10, 15), (64, 96)])
+def test_resample_cells_matches_oracle(ctx, ntarget, nmax):
+    n = 150_000
+    tab, grid, p0, pop, ofield = _setup(ctx, n, mesh=False)
+    w0 = p0.w[p0.active == 1].sum()
+    ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, ntarget, nmax))
+    g = pop.download()
+    op = oracle_pop(p0, 4 * n, 7)
+    po.sort_cells(op, ofield)
+    assert po.resample_cells(op, ofield, ntarget, nmax, 0) == 0
+    o = oracle_arrays(op)
+    assert g.n == o.n and g.n > n
+    np.testing.assert_array_equal(g.active, o.active)
+    np.testing.assert_array_equal(g.x, o.x)
+    np.testing.assert_allclose(g.w, o.w, rtol=1e-12)
+    # resample! conserves the total weight (main.jl:303-304 asserts rtol 1e-5)
+    w1 = g.w[g.active == 1].sum()
+    assert w1 == pytest.approx(w0, rel=1e-9)
+    # overfull cells are left with at most ntarget equal-weight particles
+    keys = grid.cell_key(g.x[g.active == 1])
+    _, counts = np.unique(keys[keys < np.iinfo(np.int64).max], return_counts=True)
+    assert counts.max() <= max(ntarget, nmax)
+    pop.close(); grid.close(); tab.close()
+
+
+@pytest.mark.gpu
+def test_resample_cells_mesh_fp32_conserves_weight(ctx):
+    n = 150_000
+    tab, grid, p0, pop, ofield = _setup(ctx, n, precision="fp32", mesh=True)
+    w0 = p0.w[p0.active == 1].astype(np.float32).astype(np.float64).sum()
+    ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, 64, 96))
+    g = pop.download()
+    w1 = g.w[g.active == 1].sum()
+    assert w1 == pytest.approx(w0, rel=1e-5)
+    op = oracle_pop(p0, 4 * n, 7)
+    po.sort_cells(op, ofield)
+    po.resample_cells(op, ofield, 64, 96, 0)
+    assert abs(g.n - op.n) <= 0.01 * (op.n - n) + 8
+    pop.close(); grid.close(); tab.close()
