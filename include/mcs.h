@@ -213,10 +213,13 @@ enum {
 };
 /* The time loop of Swarm.swarm (Swarm/src/Swarm.jl:124-142) on the device: per step
  * advance! with the per-step sums of Swarm.jl:126-127 fused into the step kernel, then
- * (n0 > 0) Swarm.resample!(popl, n0, tol).  moments_out (host, may be NULL) receives
- * nsteps*MCS_STEP_MOMENTS doubles; they stay on the device until the loop ends. */
+ * (n0 > 0) Swarm.resample!(popl, n0, tol), then (repack_every > 0, every repack_every
+ * steps) repack!.  The reference never repacks a swarm -- its roulette leaves holes and
+ * the run stops at 0.9 maxp (Swarm.jl:139-141) -- so repack_every = 0 is its behaviour;
+ * repacking keeps long runs inside a small capacity.  moments_out (host, may be NULL)
+ * receives nsteps*MCS_STEP_MOMENTS doubles; they stay on the device until the loop ends. */
 MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, int nsteps,
-                          int64_t n0, double tol, double* moments_out);
+                          int64_t n0, double tol, int repack_every, double* moments_out);
 /* Per-step diagnostics log (the sums MCStreamer reports every step, main.jl:269-279):
  * with capacity > 0 every following advance! writes the MCS_STEP_MOMENTS sums of its
  * post-step population into slot (steps since enabling) % capacity on the device;

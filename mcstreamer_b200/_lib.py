@@ -78,7 +78,7 @@ SIGNATURES = {
     "mcs_sort_cells": (i32, [vp, vp]),
     "mcs_resample_cells": (i32, [vp, vp, i32, i32]),
     "mcs_moments": (i32, [vp, vp, pd, i32]),
-    "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, pd]),
+    "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, i32, pd]),
     "mcs_pop_step_log": (i32, [vp, i32]),
     "mcs_moments_noalloc": (i32, [i32, vp, i32, C.POINTER(C.c_void_p), pu8, i64, pd]),
     "mcs_pop_read_step_log": (i32, [vp, pd, i32]),

@@ -668,7 +668,7 @@ MCS_API int mcs_pop_read_step_log(mcs_pop* p, double* out, int nsteps) {
 }
 
 MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, int nsteps, int64_t n0,
-                          double tol, double* moments_out) {
+                          double tol, int repack_every, double* moments_out) {
     if (!p || !t || !f || nsteps < 0) return MCS_ERR_ARG;
     mcs_ctx* c = p->ctx;
     if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "swarm loop on a cell-layout population");
@@ -684,6 +684,7 @@ MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, do
         p->cur ^= 1;
         p->step += 1;
         if (n0 > 0) st = launch_swarm_resample(p, n0, tol);
+        if (!st && repack_every > 0 && (i + 1) % repack_every == 0) st = launch_repack(p);
     }
     if (!st && moments_out && nsteps > 0) {
         cudaError_t e = cudaMemcpyAsync(moments_out, d_out, (size_t)nsteps * kStepMoments * sizeof(double),

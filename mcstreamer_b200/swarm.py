@@ -92,8 +92,9 @@ def initial_particles(n0: int, init: str, seed: int, mean_ev: float = 1.0) -> Pa
 
 def swarm_one(table: CollisionTable, en_td: float, density: float, n0: int, dt: float, nt: int,
               maxp: Optional[int] = None, precision: str = "fp64", seed: int = 0, init: str = "cold",
-              resampling: bool = True, tol: float = 0.1, l: int = 100) -> SwarmResult:
-    """One E/N point of Swarm.swarm (Swarm.jl:102-173)."""
+              resampling: bool = True, tol: float = 0.1, l: int = 100, repack_every: int = 1) -> SwarmResult:
+    """One E/N point of Swarm.swarm (Swarm.jl:102-173).  repack_every > 0 compacts the holes
+    the roulette leaves (the reference lets them accumulate up to 0.9 maxp instead)."""
     ctx = table.ctx
     maxp = maxp or max(4 * n0, 1024)
     pop = Population(maxp, initial_particles(n0, init, seed), table, precision=precision, seed=seed)
@@ -102,7 +103,7 @@ def swarm_one(table: CollisionTable, en_td: float, density: float, n0: int, dt: 
     try:
         mom = np.zeros((nt, L.STEP_MOMENTS))
         ctx.check(ctx.lib.mcs_swarm_run(pop.h, table.h, fld.h, dt, nt, n0 if resampling else 0, tol,
-                                        L.dptr(mom)))
+                                        repack_every, L.dptr(mom)))
         cnt = mom[:, L.S_COUNT]
         X = mom[:, L.S_X:L.S_X + 3] / cnt[:, None]
         X2 = mom[:, L.S_X2:L.S_X2 + 3] / cnt[:, None]
