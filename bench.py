@@ -206,6 +206,7 @@ def run_mine(args):
     import torch
 
     from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import dist as mdist
     from mcstreamer_b200 import jumc, lxcat, streamer, workloads
 
     ws, rank, local = dist_env()
@@ -247,7 +248,7 @@ def run_mine(args):
         if ev is not None:
             ev[2].record(stream)
         if qpart is not None:
-            dist.all_reduce(qpart)
+            mdist.allreduce_int64_(qpart)
         if ev is not None:
             ev[3].record(stream)
 
@@ -346,6 +347,7 @@ def run_mine(args):
 
 
 def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, dist, local):
+    from mcstreamer_b200 import dist as mdist
     """The same step through the C ABI with host-resident particles: each step uploads the
     input cloud from pinned host buffers, steps, and downloads the particles and the deposit
     grid (the plain drop-in for a host-resident Julia population)."""
@@ -382,7 +384,7 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
         grid.zero(L.Q_PART)
         ctx.check(lib.mcs_advance_deposit(pop.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0))
         if ws > 1:
-            dist.all_reduce(torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}"))
+            mdist.allreduce_charge(grid, L.Q_PART)
         ctx.check(lib.mcs_pop_download(pop.h, L.dptr(ox), L.dptr(ov), L.dptr(ow), L.dptr(os_), L.u8ptr(oa), cap,
                                        C.byref(nn)))
         ctx.check(lib.mcs_grid_read_fixed(grid.h_, L.Q_PART, L.i64ptr(hq)))

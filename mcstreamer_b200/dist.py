@@ -1,0 +1,56 @@
+"""Multi-GPU layout of the electron step: one process per GPU over torch.distributed.
+
+* Swarm instances (E/N points, gases, replicas) are independent: they are dealt to ranks
+  by predicted work (electrons x steps, longest first) and need no collective.
+* The streamer step shards one particle population across ranks on a shared mesh.  The
+  only coupling is the deposit: each rank deposits its shard into its own int64 charge
+  grid and the grids are summed with an all-reduce, which is exact and independent of
+  the reduction order (int64 fixed point), so the result equals a one-GPU deposit of the
+  whole population.
+"""
+from __future__ import annotations
+
+import heapq
+from typing import Sequence
+
+
+def shard_bounds(n: int, rank: int, world: int) -> tuple[int, int]:
+    """Contiguous shard [lo, hi) of n items for `rank` (sizes differ by at most one)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("bad rank / world size")
+    base, extra = divmod(n, world)
+    lo = rank * base + min(rank, extra)
+    return lo, lo + base + (1 if rank < extra else 0)
+
+
+def balance_instances(work: Sequence[float], world: int) -> list[list[int]]:
+    """Deal instances to ranks, longest first, each to the least-loaded rank (ties to the
+    lower rank).  Deterministic: every rank computes the same assignment."""
+    order = sorted(range(len(work)), key=lambda i: (-work[i], i))
+    heap = [(0.0, r) for r in range(world)]
+    heapq.heapify(heap)
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        out[r].append(i)
+        heapq.heappush(heap, (load + float(work[i]), r))
+    for lst in out:
+        lst.sort()
+    return out
+
+
+def allreduce_int64_(tensor, group=None):
+    """Sum an int64 tensor over ranks in place (exact for fixed-point charges)."""
+    import torch
+    import torch.distributed as dist
+    if tensor.dtype != torch.int64:
+        raise TypeError("charge grids are int64 fixed point")
+    dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
+    return tensor
+
+
+def allreduce_charge(grid, which: int, group=None):
+    """All-reduce a grid's device charge array in place (the NCCL int64 sum of the shards)."""
+    import torch
+    t = torch.as_tensor(grid.charge_array(which), device=f"cuda:{grid.ctx.device}")
+    return allreduce_int64_(t, group)
