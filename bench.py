@@ -332,7 +332,7 @@ def run_mine(args):
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "k_step_mesh<float,256,2>", "kernel_ms": kmean,
+                         "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
                          "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -347,11 +347,12 @@ def run_mine(args):
 
 
 def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, dist, local):
-    from mcstreamer_b200 import dist as mdist
     """The same step through the C ABI with host-resident particles: each step uploads the
     input cloud from pinned host buffers, steps, and downloads the particles and the deposit
     grid (the plain drop-in for a host-resident Julia population)."""
     import ctypes as C
+
+    from mcstreamer_b200 import dist as mdist
 
     cap = pop.capacity
     nodes = spec.nodes
@@ -405,10 +406,254 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
                     "mcs_grid_read_fixed"}
 
 
+# ---------------------------------------------------------------------------------------
+# Batched swarms ("cfg3"): swarm solves/s of 256 uneven instances in one batch, against the
+# same solves run one after another through the plain single-population entry point.
+# ---------------------------------------------------------------------------------------
+BATCH_METRIC = "batched swarm solves/s"
+BATCH_UNIT = "solves/s"
+
+
+def batch_alg_bytes(n_active: float, n_sec: float) -> float:
+    """Algorithmic HBM bytes of one batched advance! launch: each active electron read once
+    (x, v 24 B + w 4 + s 4 + active 1 = 33 B) and written once (x, v, s: 28 B), each
+    secondary written once (37 B)."""
+    return n_active * 61.0 + n_sec * 37.0
+
+
+def batch_cpu_sample(spec, seconds: float, threads: int) -> dict:
+    """The oracle (FP64, all host threads) on instances of the workload: advance! +
+    Swarm.resample! per step, timed until `seconds` pass; electron steps/s scaled to solves/s."""
+    from mcstreamer_b200 import lxcat, workloads
+    from oracle import pyoracle as po
+    os.environ["ORACLE_THREADS"] = str(threads)
+    tabs = {}
+    done_e, t_used, ks = 0.0, 0.0, []
+    order = np.argsort(spec.n)[len(spec.n) // 2:]  # mid-to-large instances keep the threads busy
+    for k in order[::max(1, len(order) // 8)]:
+        g = int(spec.gas[k])
+        if g not in tabs:
+            tabs[g] = po.OracleTable.from_lxcat(lxcat.synthetic_table(g))
+        p0 = workloads.swarm_instance_particles(spec, int(k))
+        op = po.OraclePop(p0.x, p0.v, p0.w, p0.s, p0.active, cap=4 * len(p0.w), seed=int(spec.seeds[k]))
+        f = po.field_uniform(0, 0, float(spec.en_td[k]) * spec.density * 1e-21)
+        po.advance(op, tabs[g], f, spec.dt, clamp=True)
+        po.swarm_resample(op, int(spec.n[k]), 0.1)
+        t0 = time.perf_counter()
+        steps = 0
+        while time.perf_counter() - t0 < seconds / 4 and steps < 50:
+            n_before = float(po.moments(op)[0])
+            po.advance(op, tabs[g], f, spec.dt, clamp=True)
+            po.swarm_resample(op, int(spec.n[k]), 0.1)
+            done_e += n_before
+            steps += 1
+        t_used += time.perf_counter() - t0
+        ks.append((int(k), steps))
+        if t_used > seconds:
+            break
+    rate = done_e / t_used
+    solves = spec.k / (spec.steps * float(spec.n.sum()) / rate)
+    return {"value": solves, "unit": BATCH_UNIT, "cores": threads, "kind": "port",
+            "electron_steps_per_s": rate,
+            "sample": f"oracle FP64 advance!+Swarm.resample! on instances {ks} (instance, steps); "
+                      f"{done_e:.3g} electron steps in {t_used:.1f} s, scaled to {spec.k} solves x {spec.steps} steps"}
+
+
+def run_batch(args):
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import constants as co
+    from mcstreamer_b200 import jumc, lxcat, workloads
+    from mcstreamer_b200.batch import SwarmBatch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    spec = workloads.batched_swarms()
+    ctx = jumc.Context(local, clamp_energy=True)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    tables = {g: jumc.CollisionTable(lxcat.synthetic_table(g), ctx) for g in sorted(set(spec.gas.tolist()))}
+    caps = 2 * spec.n
+    ez = spec.en_td * spec.density * co.Td
+
+    def fill(b):
+        nbytes = 0
+        for k in range(spec.k):
+            p0 = workloads.swarm_instance_particles(spec, k)
+            b.add(tables[int(spec.gas[k])], float(ez[k]), int(spec.seeds[k]), int(spec.n[k]), int(caps[k]), p0)
+            nbytes += p0.n * (8 * 8 + 1)
+        return nbytes
+
+    b = SwarmBatch(ctx, spec.k, int(caps.sum()))
+    fill(b)
+    b.step(spec.dt, 2, graph=True)
+    chosen, times = b.autotune(spec.dt, trial_steps=2)
+    shape = SwarmBatch.variant_shape(chosen)
+    for _ in range(args.warmup):
+        b.step(spec.dt, 1, graph=True)
+    b.sync()
+    n_before = float(b.read_current()[:, L.S_COUNT].sum())
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            evs[k][0].record(stream)
+            b.step(spec.dt, 1, graph=True)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    b.sync()
+    step_ms = float(sum(a.elapsed_time(c) for a, c in evs)) / args.steps
+    cur = b.read_current()
+    n_after = float(cur[:, L.S_COUNT].sum())
+    kernel_ms, prof_step_ms = b.profile(spec.dt, 3)
+    clocks = clk.summary()
+    value = spec.k / (spec.steps * step_ms * 1e-3)
+    e_steps = 0.5 * (n_before + n_after) / (step_ms * 1e-3)
+    b.close()
+
+    # plain drop-in: each solve alone through mcs_swarm_run (FP32, and FP64 on a sample)
+    mom = np.zeros(L.MOMENTS_BASE)
+
+    def plain(precision: str, ks, steps: int, calls: bool = False) -> tuple[float, float]:
+        """Each solve alone: the fused loop entry point, or (calls=True) the per-step call
+        sequence of Swarm.jl:124-142 through the C ABI: advance!, the step sums, resample!,
+        repack!."""
+        t_ms, n_e = 0.0, 0.0
+
+        def run(pop, tab, fld, k, nsteps):
+            if not calls:
+                ctx.check(ctx.lib.mcs_swarm_run(pop.h, tab.h, fld.h, spec.dt, nsteps, int(spec.n[k]), 0.1, 1, None))
+                return
+            for _ in range(nsteps):
+                ctx.check(ctx.lib.mcs_advance(pop.h, tab.h, fld.h, spec.dt, None))
+                ctx.check(ctx.lib.mcs_moments(pop.h, None, L.dptr(mom), L.MOMENTS_BASE))
+                ctx.check(ctx.lib.mcs_swarm_resample(pop.h, int(spec.n[k]), 0.1))
+                ctx.check(ctx.lib.mcs_repack(pop.h))
+
+        for k in ks:
+            p0 = workloads.swarm_instance_particles(spec, int(k))
+            tab = tables[int(spec.gas[k])]
+            pop = jumc.Population(int(caps[k]), p0, tab, precision=precision, seed=int(spec.seeds[k]))
+            fld = jumc.FixedField(float(ez[k]), ctx)
+            run(pop, tab, fld, k, 1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(pop, tab, fld, k, steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_ms += e0.elapsed_time(e1) / steps
+            n_e += float(spec.n[k])
+            fld.close()
+            pop.close()
+        return t_ms, n_e
+
+    t32, _ = plain("fp32", range(spec.k), 3)
+    plain32 = spec.k / (spec.steps * t32 * 1e-3)
+    t32c, _ = plain("fp32", range(spec.k), 3, calls=True)
+    plain32c = spec.k / (spec.steps * t32c * 1e-3)
+    sample64 = list(range(0, spec.k, 16))
+    t64, n64 = plain("fp64", sample64, 2)
+    t64_all = t64 * float(spec.n.sum()) / n64
+    plain64 = spec.k / (spec.steps * t64_all * 1e-3)
+
+    # end to end through the public API: host particles uploaded into a fresh batch, steps,
+    # and every step the sums of all instances read back to the host
+    e2e_steps = max(3, min(args.steps, 20))
+    b2 = SwarmBatch(ctx, spec.k, int(caps.sum()))
+    b2.set_variant(chosen)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    up_bytes = fill(b2)
+    t_up = time.perf_counter() - t0
+    b2.step(spec.dt, 1, graph=True)
+    b2.read_current()
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        b2.step(spec.dt, 1, graph=True)
+        b2.read_current()
+    t_steps = (time.perf_counter() - t1) / e2e_steps
+    b2.close()
+    e2e_solves = spec.k / (t_up + spec.steps * t_steps)
+
+    pk, pk_kind = peaks()
+    hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
+    alg = batch_alg_bytes(0.5 * (n_before + n_after), 0.0)
+    achieved = alg / (kernel_ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        cpu = batch_cpu_sample(spec, args.cpu_seconds, os.cpu_count() or 1)
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {
+            "workload": f"batched swarms cfg3: {spec.k} instances, E/N log-spaced 10-1000 Td, electrons "
+                        f"log-uniform 4096-1048576 (total {int(spec.n.sum())}), synthetic gases 0/1/2, "
+                        f"N={spec.density:g} m^-3, dt={spec.dt:g} s, {spec.steps} steps per solve, Swarm.resample! "
+                        f"to the initial count every step, repack every step, one CUDA graph per batched step",
+            "solve_time_s": spec.steps * step_ms * 1e-3,
+            "electron_steps_per_s": e_steps,
+            "autotune": {"variant": chosen, "block": shape[0], "particles_per_thread": shape[1],
+                         "trial_ms": [round(float(t), 4) for t in times]},
+            "l2": "inputs larger than L2 (44.6M electrons x 33 B = 1.5 GB resident)",
+            "plain_drop_in": {
+                "fp32_solves_per_s": plain32, "fp32_ms_per_step_all": t32,
+                "fp32_calls_solves_per_s": plain32c, "fp32_calls_ms_per_step_all": t32c,
+                "speedup_fp32_calls": value / plain32c,
+                "fp64_solves_per_s": plain64, "fp64_ms_per_step_all_est": t64_all,
+                "fp64_sample": f"{len(sample64)} instances (every 16th), scaled by electron count",
+                "how": "each solve alone: mcs_swarm_run(FP32|FP64, repack_every=1), and (fp32_calls) the "
+                       "per-step ccall sequence mcs_advance + mcs_moments + mcs_swarm_resample + mcs_repack; "
+                       "CUDA events over 3 (FP32) / 2 (FP64) steps after one warm-up step",
+                "speedup_fp32": value / plain32, "speedup_fp64": value / plain64},
+            "parallelism": "1 GPU",
+        },
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "kernel": f"k_bstep<{shape[0]},{shape[1]}>", "kernel_ms": kernel_ms,
+                     "step_ms_no_graph": prof_step_ms, "alg_bytes_per_launch": alg,
+                     "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_solves, "unit": BATCH_UNIT,
+                "h2d_bytes_per_step": up_bytes / spec.steps, "d2h_bytes_per_step": spec.k * L.BATCH_MOMENTS * 8,
+                "path": "SwarmBatch.add from host arrays (Julia layout, uploaded once per solve; h2d bytes "
+                        "amortised over the solve's steps) -> SwarmBatch.step -> read_current every step",
+                "upload_s": t_up, "ms_per_step": t_steps * 1e3},
+        "clocks": clocks,
+        "gpu_launches": args.steps * 14,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_batch(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.batched_swarms()
+    threads = os.cpu_count() or 1
+    per = min(20.0, max(4.0, 120.0 / max(1, args.steps + args.warmup)))
+    vals = [batch_cpu_sample(spec, per, threads) for _ in range(max(1, min(args.steps, 3)))]
+    v = statistics.median(x["value"] for x in vals)
+    line = {
+        "impl": "reference", "metric": BATCH_METRIC, "value": v, "unit": BATCH_UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batched swarms cfg3", "instances": spec.k, "electrons": int(spec.n.sum())},
+        "cpu_baseline": {"value": v, "unit": BATCH_UNIT, "cores": threads, "kind": "port", "sample": vals[-1]["sample"]},
+        "e2e": {"value": v, "unit": BATCH_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "cfg3":
+        return run_reference_batch(args) if args.impl == "reference" else run_batch(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_mine(args)

@@ -88,6 +88,7 @@ typedef struct mcs_table mcs_table;
 typedef struct mcs_grid mcs_grid;
 typedef struct mcs_field mcs_field;
 typedef struct mcs_pop mcs_pop;
+typedef struct mcs_batch mcs_batch;
 
 /* ---- context ---- */
 MCS_API int mcs_version(void);
@@ -226,6 +227,47 @@ MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, do
  * capacity 0 disables it.  read copies slots [0, nsteps) to the host. */
 MCS_API int mcs_pop_step_log(mcs_pop* p, int capacity);
 MCS_API int mcs_pop_read_step_log(mcs_pop* p, double* out, int nsteps);
+
+/* ---- Batched swarms: many independent Swarm.swarm solves on one GPU -----------------
+ * Replaces the per-solve driver loop of Swarm/src/Swarm.jl:114-150 (one population, one
+ * E/N point, one gas per call) for a caller that runs many of them (E/N sweeps, gas
+ * mixtures, replicas).  Every instance is an FP32 swarm in a uniform field E with its own
+ * collision table, seed and resampling target; a step advances all of them with the
+ * sequence advance! -> Swarm.resample!(n0, tol) -> repack! that mcs_swarm_run(...,
+ * repack_every = 1) applies to one population, and each instance's particles evolve
+ * bit-identically to that single run with the same table, field and seed.
+ * Instances join (add) and leave (remove) between steps.  Per-step sums of every instance
+ * (MCS_BATCH_MOMENTS doubles: the MCS_STEP_MOMENTS sums, then the sum over actives of the
+ * rate of the table's first ionization row and of its square) stay on the device in a
+ * ring of MCS_BATCH_LOG steps. */
+enum { MCS_BATCH_MOMENTS = 14, MCS_BATCH_LOG = 64, MCS_BATCH_VARIANTS = 12 };
+MCS_API int mcs_batch_create(mcs_ctx* ctx, int max_instances, int64_t total_capacity, mcs_batch** out);
+MCS_API int mcs_batch_destroy(mcs_batch* b);
+/* Join: n particles in Julia layout (x, v as n x 3 row-major), region of `capacity` slots. */
+MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez, uint64_t seed,
+                          int64_t n0, double tol, int64_t capacity, const double* x, const double* v,
+                          const double* w, const double* s, const uint8_t* active, int64_t n, int* slot);
+MCS_API int mcs_batch_remove(mcs_batch* b, int slot);
+/* nsteps batched steps of length dt on the context's stream; use_graph replays one captured
+ * CUDA graph per step (re-captured when dt, the context flags or the variant change). */
+MCS_API int mcs_batch_step(mcs_batch* b, double dt, int nsteps, int use_graph);
+MCS_API int mcs_batch_sync(mcs_batch* b);
+/* Per-instance particle counts and completed steps (arrays of max_instances; NULL skips). */
+MCS_API int mcs_batch_state(mcs_batch* b, int64_t* n, uint32_t* steps);
+/* The sums of every slot's most recent step (max_instances x MCS_BATCH_MOMENTS), one copy. */
+MCS_API int mcs_batch_read_current(mcs_batch* b, double* out);
+/* The last `count` (<= MCS_BATCH_LOG) per-step sums of an instance, oldest first. */
+MCS_API int mcs_batch_read_log(mcs_batch* b, int slot, double* out, int count);
+MCS_API int mcs_batch_download(mcs_batch* b, int slot, double* x, double* v, double* w, double* s,
+                               uint8_t* active, int64_t capacity, int64_t* n_out);
+/* Time each (threads per block, particles per thread) variant of the batched step over
+ * trial_steps steps of the current state (restored afterwards) and keep the fastest. */
+MCS_API int mcs_batch_autotune(mcs_batch* b, double dt, int trial_steps, int* chosen, float* times_ms);
+/* nsteps steps without the graph, timing (CUDA events on the context's stream) the
+ * persistent advance! kernel and the whole step; per-step averages in ms. */
+MCS_API int mcs_batch_profile(mcs_batch* b, double dt, int nsteps, float* kernel_ms, float* step_ms);
+MCS_API int mcs_batch_set_variant(mcs_batch* b, int variant);
+MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt);
 
 #ifdef __cplusplus
 }

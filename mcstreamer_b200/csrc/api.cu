@@ -9,7 +9,7 @@
 
 using namespace mcs;
 
-namespace {
+namespace mcs {
 
 int map_status(uint32_t st) {
     if (st & ST_TIMEOUT) return MCS_ERR_TIMEOUT;
@@ -60,6 +60,10 @@ int sync_status(mcs_ctx* c) {
     }
     return MCS_OK;
 }
+
+}  // namespace mcs
+
+namespace {
 
 int ensure_staging(mcs_pop* p, size_t bytes) {
     if (p->staging_bytes >= bytes) return MCS_OK;

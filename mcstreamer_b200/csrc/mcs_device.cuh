@@ -160,11 +160,13 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // predecessor is owned by a running CTA and the wait ends; it is still bounded, and on
 // timeout ST_TIMEOUT is raised and the returned prefix is flagged invalid (ok=false).
 // Called by one thread.
-__device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, uint32_t tile, uint32_t epoch,
-                                                  uint32_t count, uint32_t* st_word, bool* ok) {
+// `first` is the first tile of the segment being scanned (0 for a whole population; the
+// first tile of an instance in a batch, so instances are prefixed independently).
+__device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* status, uint32_t first, uint32_t tile,
+                                                       uint32_t epoch, uint32_t count, uint32_t* st_word, bool* ok) {
     *ok = true;
-    if (tile == 0) {
-        st_release_u64(&status[0], tile_word(epoch, 2, count));
+    if (tile == first) {
+        st_release_u64(&status[tile], tile_word(epoch, 2, count));
         return 0;
     }
     st_release_u64(&status[tile], tile_word(epoch, 1, count));
@@ -172,7 +174,7 @@ __device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, ui
     int64_t p = (int64_t)tile - 1;
     uint32_t spins = 0;
     const uint32_t ep = epoch & 0x3fffffffu;
-    while (p >= 0) {
+    while (p >= (int64_t)first) {
         const unsigned long long s = ld_acquire_u64(&status[p]);
         const uint32_t e = (uint32_t)(s >> 34);
         const uint32_t f = (uint32_t)(s >> 32) & 3u;
@@ -191,6 +193,11 @@ __device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, ui
     }
     st_release_u64(&status[tile], tile_word(epoch, 2, excl + count));
     return excl;
+}
+
+__device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, uint32_t tile, uint32_t epoch,
+                                                  uint32_t count, uint32_t* st_word, bool* ok) {
+    return tile_lookback_from(status, 0u, tile, epoch, count, st_word, ok);
 }
 
 }  // namespace mcs

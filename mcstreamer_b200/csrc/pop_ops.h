@@ -12,5 +12,9 @@ int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* 
                   const uint8_t* da, long long n);
 int launch_download(mcs_pop* p, double* dx, double* dv, double* dw, double* ds, uint8_t* da);
 int grid_for(mcs_ctx* c, long long n, int block);
+int map_status(uint32_t st);
+const char* status_text(int code);
+// Wait for the context's stream and turn the sticky device status into an error code.
+int sync_status(mcs_ctx* c);
 constexpr int kMomentPartialsMin = 148 * 2 * (MCS_MOMENTS_BASE + kMaxRows);
 }  // namespace mcs

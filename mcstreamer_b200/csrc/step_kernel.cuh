@@ -27,6 +27,27 @@ struct TileShared {
     int last;
 };
 
+// Add one particle to the step sums m[0..kStepMoments).  Every product and sum is rounded
+// explicitly, so the bits do not depend on where the compiler contracts into FMAs and all
+// kernels that form these sums (single population, batched instances) agree exactly.
+template <int N>
+__device__ __forceinline__ void mom_add(double (&m)[N], double x, double y, double z, double vx, double vy, double vz,
+                                        double w) {
+    m[SM_COUNT] = __dadd_rn(m[SM_COUNT], 1.0);
+    m[SM_W] = __dadd_rn(m[SM_W], w);
+    m[SM_X] = __dadd_rn(m[SM_X], x);
+    m[SM_Y] = __dadd_rn(m[SM_Y], y);
+    m[SM_Z] = __dadd_rn(m[SM_Z], z);
+    m[SM_XX] = __dadd_rn(m[SM_XX], __dmul_rn(x, x));
+    m[SM_YY] = __dadd_rn(m[SM_YY], __dmul_rn(y, y));
+    m[SM_ZZ] = __dadd_rn(m[SM_ZZ], __dmul_rn(z, z));
+    m[SM_VX] = __dadd_rn(m[SM_VX], vx);
+    m[SM_VY] = __dadd_rn(m[SM_VY], vy);
+    m[SM_VZ] = __dadd_rn(m[SM_VZ], vz);
+    const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(vx, vx), __dmul_rn(vy, vy)), __dmul_rn(vz, vz));
+    m[SM_E] = __dadd_rn(m[SM_E], __dmul_rn(0.5 * kElectronMass, v2));
+}
+
 template <typename T>
 struct MomAcc {
     double m[kStepMoments];
@@ -35,12 +56,7 @@ struct MomAcc {
         for (int q = 0; q < kStepMoments; ++q) m[q] = 0.0;
     }
     __device__ __forceinline__ void add(double x, double y, double z, double vx, double vy, double vz, double w) {
-        m[SM_COUNT] += 1.0;
-        m[SM_W] += w;
-        m[SM_X] += x; m[SM_Y] += y; m[SM_Z] += z;
-        m[SM_XX] += x * x; m[SM_YY] += y * y; m[SM_ZZ] += z * z;
-        m[SM_VX] += vx; m[SM_VY] += vy; m[SM_VZ] += vz;
-        m[SM_E] += 0.5 * kElectronMass * (vx * vx + vy * vy + vz * vz);
+        mom_add(m, x, y, z, vx, vy, vz, w);
     }
 };
 
@@ -346,9 +362,15 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                 if (i < n_entry && P.act[i])
                     acc.add(P.f[0][i], P.f[1][i], P.f[2][i], P.f[3][i], P.f[4][i], P.f[5][i], P.f[6][i]);
             }
-            for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)
-                if (sg.act[e])
-                    acc.add(sg.f[0][e], sg.f[1][e], sg.f[2][e], sg.f[3][e], sg.f[4][e], sg.f[5][e], sg.f[6][e]);
+            // secondaries in their appended (serial) order, so the sums do not depend on the
+            // order in which lanes staged them
+            __syncthreads();
+            const long long d0 = n_entry + (long long)sh.excl;
+            for (uint32_t r = threadIdx.x; r < cnt; r += BLOCK) {
+                const long long d = d0 + r;
+                if (sh.ok && d < P.cap && P.act[d])
+                    acc.add(P.f[0][d], P.f[1][d], P.f[2][d], P.f[3][d], P.f[4][d], P.f[5][d], P.f[6][d]);
+            }
             block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
         }
         __syncthreads();
@@ -743,11 +765,16 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                     acc.add(x, y, z, P.f[3][j], P.f[4][j], P.f[5][j], P.f[6][j]);
                 }
             }
-            for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK)
-                if (sg.act[e]) {
-                    mesh_abs(g, sg.cell[e], (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], x, y, z);
-                    acc.add(x, y, z, sg.f[3][e], sg.f[4][e], sg.f[5][e], sg.f[6][e]);
+            // secondaries in their appended (serial) order (sums independent of staging order)
+            __syncthreads();
+            const long long d0 = n_entry + (long long)sh.excl;
+            for (uint32_t r = threadIdx.x; r < cnt; r += BLOCK) {
+                const long long d = d0 + r;
+                if (sh.ok && d < P.cap && P.act[d]) {
+                    mesh_abs(g, P.cell[d], (double)P.f[0][d], (double)P.f[1][d], (double)P.f[2][d], x, y, z);
+                    acc.add(x, y, z, P.f[3][d], P.f[4][d], P.f[5][d], P.f[6][d]);
                 }
+            }
             block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
         }
         __syncthreads();

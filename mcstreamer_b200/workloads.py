@@ -10,6 +10,11 @@ streamer(cfg): the 3-D streamer steps.
           log-uniform on [1e2, 1e4]; seed 2.
 Particles are generated on the host and sorted by cell key (the layout the cell-sorted
 resampling maintains), then uploaded.
+
+batched_swarms(): the batched swarm workload ("cfg3"): 256 instances with E/N log-spaced
+  10-1000 Td, electron counts log-uniform 4,096-1,048,576 and one of the synthetic gases
+  0, 1, 2 each (seeded, seed 3); N = 2.5e25 m^-3, dt = 1e-13 s, 5000 steps per solve,
+  isotropic Maxwellian at 1 eV, Swarm.resample! to the initial count (tol 0.1).
 """
 from __future__ import annotations
 
@@ -97,3 +102,38 @@ def streamer_particles(spec: StreamerSpec, rank: int = 0, chunk: int = 1 << 22) 
 def streamer_field_fn(spec: StreamerSpec):
     from .streamer import gaussian_charge_field
     return gaussian_charge_field(spec.centre, CHARGE_SIGMA, CHARGE_PEAK, e_bg=E_BACKGROUND)
+
+
+SWARM_DENSITY = 2.5e25   # m^-3
+SWARM_DT = 1e-13         # s
+
+
+@dataclass
+class BatchedSwarmSpec:
+    en_td: np.ndarray        # (K,) reduced fields
+    n: np.ndarray            # (K,) electrons per instance (also the resampling target)
+    gas: np.ndarray          # (K,) synthetic gas variant
+    seeds: np.ndarray        # (K,) per-instance Philox seeds
+    steps: int = 5000
+    dt: float = SWARM_DT
+    density: float = SWARM_DENSITY
+    mean_ev: float = 1.0
+
+    @property
+    def k(self) -> int:
+        return len(self.n)
+
+
+def batched_swarms(instances: int = 256, seed: int = 3, nmin: int = 4096, nmax: int = 1_048_576,
+                   gases: tuple = (0, 1, 2)) -> BatchedSwarmSpec:
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(nmin), np.log(nmax), instances)).astype(np.int64)
+    gas = np.asarray(gases)[rng.integers(0, len(gases), instances)]
+    return BatchedSwarmSpec(np.logspace(1.0, 3.0, instances), n, gas,
+                            np.arange(instances, dtype=np.uint64) + np.uint64(seed) * np.uint64(1_000_003))
+
+
+def swarm_instance_particles(spec: BatchedSwarmSpec, k: int) -> ParticleArrays:
+    """Initial electrons of instance k: isotropic Maxwellian at spec.mean_ev, at the origin."""
+    from .swarm import initial_particles
+    return initial_particles(int(spec.n[k]), "maxwellian", int(spec.seeds[k]), mean_ev=spec.mean_ev)
