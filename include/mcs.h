@@ -256,6 +256,9 @@ MCS_API int mcs_batch_sync(mcs_batch* b);
 MCS_API int mcs_batch_state(mcs_batch* b, int64_t* n, uint32_t* steps);
 /* The sums of every slot's most recent step (max_instances x MCS_BATCH_MOMENTS), one copy. */
 MCS_API int mcs_batch_read_current(mcs_batch* b, double* out);
+/* Every slot's ring of per-step sums (max_instances x MCS_BATCH_LOG x MCS_BATCH_MOMENTS;
+ * step t of a slot sits at t % MCS_BATCH_LOG) and its count of logged steps. */
+MCS_API int mcs_batch_read_logs(mcs_batch* b, double* ring, uint32_t* logpos);
 /* The last `count` (<= MCS_BATCH_LOG) per-step sums of an instance, oldest first. */
 MCS_API int mcs_batch_read_log(mcs_batch* b, int slot, double* out, int count);
 MCS_API int mcs_batch_download(mcs_batch* b, int slot, double* x, double* v, double* w, double* s,

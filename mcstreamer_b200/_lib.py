@@ -91,6 +91,7 @@ SIGNATURES = {
     "mcs_batch_state": (i32, [vp, pi64, C.POINTER(C.c_uint32)]),
     "mcs_batch_read_log": (i32, [vp, i32, pd, i32]),
     "mcs_batch_read_current": (i32, [vp, pd]),
+    "mcs_batch_read_logs": (i32, [vp, pd, C.POINTER(C.c_uint32)]),
     "mcs_batch_download": (i32, [vp, i32, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_batch_autotune": (i32, [vp, f64, i32, pi32, C.POINTER(C.c_float)]),
     "mcs_batch_profile": (i32, [vp, f64, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),

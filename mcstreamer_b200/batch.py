@@ -79,6 +79,13 @@ class SwarmBatch:
         self.ctx.check(self.ctx.lib.mcs_batch_read_current(self.h, L.dptr(out)))
         return out
 
+    def read_logs(self) -> tuple[np.ndarray, np.ndarray]:
+        """(ring, logged steps) of every slot: ring[k, t % BATCH_LOG] holds step t's sums."""
+        ring = np.zeros((self.max_instances, L.BATCH_LOG, L.BATCH_MOMENTS))
+        pos = np.zeros(self.max_instances, np.uint32)
+        self.ctx.check(self.ctx.lib.mcs_batch_read_logs(self.h, L.dptr(ring), pos.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return ring, pos
+
     def download(self, slot: int) -> ParticleArrays:
         n, _ = self.state()
         m = int(n[slot])

@@ -973,6 +973,19 @@ MCS_API int mcs_batch_read_current(mcs_batch* b, double* out) {
     return sync_status_b(b);
 }
 
+// The whole per-step ring of every slot ([max_instances][MCS_BATCH_LOG][MCS_BATCH_MOMENTS])
+// and each slot's count of logged steps, in two copies.
+MCS_API int mcs_batch_read_logs(mcs_batch* b, double* ring, uint32_t* logpos) {
+    if (!b || !ring || !logpos) return MCS_ERR_ARG;
+    mcs_ctx* c = b->ctx;
+    cudaError_t e = cudaMemcpyAsync(ring, b->d.log, sizeof(double) * kBM * kBatchLog * b->K, cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(logpos, b->d.logpos, sizeof(uint32_t) * b->K, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
+    return sync_status_b(b);
+}
+
 // Copy one instance's particles to the host (Julia layout).
 MCS_API int mcs_batch_download(mcs_batch* b, int slot, double* x, double* v, double* w, double* s, uint8_t* active,
                                int64_t cap, int64_t* n_out) {
