@@ -479,12 +479,18 @@ def run_batch(args):
     caps = 2 * spec.n
     ez = spec.en_td * spec.density * co.Td
 
-    def fill(b):
+    def fill(b, host: bool = False):
+        """Join every instance: electrons drawn on the device, or (host=True) generated on
+        the host and uploaded in the Julia layout.  Returns the host->device bytes."""
         nbytes = 0
         for k in range(spec.k):
-            p0 = workloads.swarm_instance_particles(spec, k)
-            b.add(tables[int(spec.gas[k])], float(ez[k]), int(spec.seeds[k]), int(spec.n[k]), int(caps[k]), p0)
-            nbytes += p0.n * (8 * 8 + 1)
+            if host:
+                p0 = workloads.swarm_instance_particles(spec, k)
+                b.add(tables[int(spec.gas[k])], float(ez[k]), int(spec.seeds[k]), int(spec.n[k]), int(caps[k]), p0)
+                nbytes += p0.n * (8 * 8 + 1)
+            else:
+                b.add_maxwellian(tables[int(spec.gas[k])], float(ez[k]), int(spec.seeds[k]), int(spec.n[k]),
+                                 int(caps[k]), int(spec.n[k]), spec.mean_ev)
         return nbytes
 
     b = SwarmBatch(ctx, spec.k, int(caps.sum()))
@@ -534,9 +540,9 @@ def run_batch(args):
                 ctx.check(ctx.lib.mcs_repack(pop.h))
 
         for k in ks:
-            p0 = workloads.swarm_instance_particles(spec, int(k))
             tab = tables[int(spec.gas[k])]
-            pop = jumc.Population(int(caps[k]), p0, tab, precision=precision, seed=int(spec.seeds[k]))
+            pop = jumc.Population(int(caps[k]), None, tab, precision=precision, seed=int(spec.seeds[k]))
+            pop.init_maxwellian(int(spec.n[k]), spec.mean_ev)
             fld = jumc.FixedField(float(ez[k]), ctx)
             run(pop, tab, fld, k, 1)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -566,7 +572,7 @@ def run_batch(args):
     b2.set_variant(chosen)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    up_bytes = fill(b2)
+    up_bytes = fill(b2, host=True)
     t_up = time.perf_counter() - t0
     b2.step(spec.dt, 1, graph=True)
     b2.read_current()
@@ -642,7 +648,6 @@ def run_serve(args):
     from mcstreamer_b200 import jumc, lxcat
     from mcstreamer_b200.serve import (StopRule, SwarmServer, percentiles, poisson_requests,
                                        serial_latencies)
-    from mcstreamer_b200.swarm import initial_particles
     from mcstreamer_b200.workloads import SWARM_DENSITY, SWARM_DT
 
     ws, rank, local = dist_env()
@@ -680,8 +685,8 @@ def run_serve(args):
     per_step = []
     for i, n in enumerate(sizes):
         tab = tables[i % 4]
-        p0 = initial_particles(int(n), "maxwellian", 7 + i, mean_ev=1.0)
-        pop = jumc.Population(2 * int(n), p0, tab, precision="fp32", seed=7 + i)
+        pop = jumc.Population(2 * int(n), None, tab, precision="fp32", seed=7 + i)
+        pop.init_maxwellian(int(n), 1.0)
         fld = jumc.FixedField(300.0 * SWARM_DENSITY * co.Td, ctx)
 
         def one():

@@ -158,6 +158,11 @@ MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double
                              uint8_t* active, int64_t cap, int64_t* n);
 /* Device-to-device copy of a whole population (state, count, Philox key and step): a
  * snapshot / restore point.  Same context, precision and layout; dst capacity >= src's. */
+/* Swarm initial condition drawn on the device: n electrons at the origin, weight 1,
+ * isotropic Maxwellian velocities of mean energy mean_energy_ev, s = -log(u); every
+ * electron's draws come from the population seed and its slot (Philox stream INIT).  The
+ * reference starts its swarms on the host (Swarm/src/Swarm.jl:104-106). */
+MCS_API int mcs_pop_init_maxwellian(mcs_pop* p, int64_t n, double mean_energy_ev);
 MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src);
 /* nparticles (population.jl:106): particles in use, active or not. */
 MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n);
@@ -247,7 +252,19 @@ MCS_API int mcs_batch_destroy(mcs_batch* b);
 MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez, uint64_t seed,
                           int64_t n0, double tol, int64_t capacity, const double* x, const double* v,
                           const double* w, const double* s, const uint8_t* active, int64_t n, int* slot);
+/* Join with electrons drawn on the device (no host data, no host wait): n electrons at the
+ * origin with weight 1 and isotropic Maxwellian velocities of mean energy mean_energy_ev,
+ * the same electrons mcs_pop_init_maxwellian draws for a population with this seed. */
+MCS_API int mcs_batch_add_maxwellian(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez,
+                                     uint64_t seed, int64_t n0, double tol, int64_t capacity, int64_t n,
+                                     double mean_energy_ev, int* slot);
+/* Leave (stream-ordered: steps already enqueued still advance the instance). */
 MCS_API int mcs_batch_remove(mcs_batch* b, int slot);
+/* Double-buffered diagnostics without stalling the stream: enqueue copies of every slot's
+ * ring, logged-step counts and the status word into pinned buffer buf (0 or 1), then wait
+ * for them later; the pointers stay valid until the next enqueue into the same buffer. */
+MCS_API int mcs_batch_logs_enqueue(mcs_batch* b, int buf);
+MCS_API int mcs_batch_logs_wait(mcs_batch* b, int buf, const double** ring, const uint32_t** logpos);
 /* nsteps batched steps of length dt on the context's stream; use_graph replays one captured
  * CUDA graph per step (re-captured when dt, the context flags or the variant change). */
 MCS_API int mcs_batch_step(mcs_batch* b, double dt, int nsteps, int use_graph);

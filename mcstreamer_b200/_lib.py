@@ -86,6 +86,10 @@ SIGNATURES = {
     "mcs_batch_destroy": (i32, [vp]),
     "mcs_batch_add": (i32, [vp, vp, f64, f64, f64, u64, i64, f64, i64, pd, pd, pd, pd, pu8, i64, pi32]),
     "mcs_batch_remove": (i32, [vp, i32]),
+    "mcs_batch_add_maxwellian": (i32, [vp, vp, f64, f64, f64, u64, i64, f64, i64, i64, f64, pi32]),
+    "mcs_batch_logs_enqueue": (i32, [vp, i32]),
+    "mcs_batch_logs_wait": (i32, [vp, i32, C.POINTER(pd), C.POINTER(C.POINTER(C.c_uint32))]),
+    "mcs_pop_init_maxwellian": (i32, [vp, i64, f64]),
     "mcs_batch_step": (i32, [vp, f64, i32, i32]),
     "mcs_batch_sync": (i32, [vp]),
     "mcs_batch_state": (i32, [vp, pi64, C.POINTER(C.c_uint32)]),

@@ -50,6 +50,27 @@ class SwarmBatch:
             L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), len(w), C.byref(slot)))
         return slot.value
 
+    def add_maxwellian(self, table: CollisionTable, ez: float, seed: int, n0: int, capacity: int, n: int,
+                       mean_ev: float = 1.0, tol: float = 0.1, ex: float = 0.0, ey: float = 0.0) -> int:
+        """Join with n electrons drawn on the device (stream-ordered, no host wait)."""
+        slot = C.c_int(-1)
+        self.ctx.check(self.ctx.lib.mcs_batch_add_maxwellian(
+            self.h, table.h, float(ex), float(ey), float(ez), C.c_uint64(seed), int(n0), float(tol), int(capacity),
+            int(n), float(mean_ev), C.byref(slot)))
+        return slot.value
+
+    def logs_enqueue(self, buf: int) -> None:
+        self.ctx.check(self.ctx.lib.mcs_batch_logs_enqueue(self.h, int(buf)))
+
+    def logs_wait(self, buf: int) -> tuple[np.ndarray, np.ndarray]:
+        """Views of pinned buffer `buf` (ring, logged steps); valid until its next enqueue."""
+        ring = L.pd()
+        pos = C.POINTER(C.c_uint32)()
+        self.ctx.check(self.ctx.lib.mcs_batch_logs_wait(self.h, int(buf), C.byref(ring), C.byref(pos)))
+        r = np.ctypeslib.as_array(ring, shape=(self.max_instances, L.BATCH_LOG, L.BATCH_MOMENTS))
+        p = np.ctypeslib.as_array(pos, shape=(self.max_instances,))
+        return r, p
+
     def remove(self, slot: int) -> None:
         self.ctx.check(self.ctx.lib.mcs_batch_remove(self.h, int(slot)))
 

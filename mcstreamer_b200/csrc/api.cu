@@ -499,6 +499,20 @@ MCS_API int mcs_pop_upload(mcs_pop* p, const double* x, const double* v, const d
     return MCS_OK;
 }
 
+MCS_API int mcs_pop_init_maxwellian(mcs_pop* p, int64_t n, double mean_energy_ev) {
+    if (!p || n < 0 || !(mean_energy_ev >= 0)) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "swarm initialisation of a cell-layout population");
+    if (n > p->cap) return set_err(c, MCS_ERR_CAPACITY, "Maximum number of particles reached");
+    if (int st = use_device(c)) return st;
+    if (n > 0)
+        if (int st = launch_init_maxwellian(p, n, maxwellian_sigma(mean_energy_ev))) return st;
+    const long long nn = n;
+    MCS_CK(c, cudaMemcpyAsync(p->d_n + p->cur, &nn, sizeof(nn), cudaMemcpyHostToDevice, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    return MCS_OK;
+}
+
 MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src) {
     if (!dst || !src || dst->ctx != src->ctx) return MCS_ERR_ARG;
     mcs_ctx* c = dst->ctx;

@@ -642,6 +642,31 @@ __global__ void k_bfinish(BatchDev B) {
     }
 }
 
+// Join without host data: the instance's descriptor and counters, and its electrons drawn
+// on the device (maxwellian_draw with the instance seed and instance-local slot).
+__global__ void k_binit(BatchDev B, int k, Inst I, long long n, double sigma) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        B.inst[k] = I;
+        B.n0buf[k] = n;
+        B.n1buf[k] = n;
+        B.step[k] = 0;
+        B.logpos[k] = 0;
+    }
+    for (long long il = blockIdx.x * (long long)blockDim.x + threadIdx.x; il < n; il += (long long)gridDim.x * blockDim.x) {
+        double vx, vy, vz, s;
+        maxwellian_draw(I.seed, (uint32_t)il, sigma, vx, vy, vz, s);
+        const long long i = I.base + il;
+        B.f[0][i] = 0.f; B.f[1][i] = 0.f; B.f[2][i] = 0.f;
+        B.f[3][i] = (float)vx; B.f[4][i] = (float)vy; B.f[5][i] = (float)vz;
+        B.f[6][i] = 1.f;
+        B.f[7][i] = (float)s;
+        B.act[i] = 1;
+    }
+}
+
+__global__ void k_bset_live(Inst* inst, int k, int live) { inst[k].live = live; }
+__global__ void k_bset_table(TableView* tabs, int idx, TableView v) { tabs[idx] = v; }
+
 }  // namespace mcs
 
 // ---------------------------------------------------------------------------------------
@@ -668,6 +693,11 @@ struct mcs_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int grid[16] = {};              // persistent grid per variant (resident CTAs x SMs)
+    // double-buffered pinned copies of the per-step rings (mcs_batch_logs_enqueue / wait)
+    double* hring[2] = {nullptr, nullptr};
+    uint32_t* hpos[2] = {nullptr, nullptr};
+    uint32_t* hstatus[2] = {nullptr, nullptr};
+    cudaEvent_t lev[2] = {nullptr, nullptr};
     std::vector<void*> allocs;
 };
 
@@ -812,17 +842,25 @@ MCS_API int mcs_batch_destroy(mcs_batch* b) {
     cudaStreamSynchronize(b->ctx->stream);
     drop_graph(b);
     for (void* p : b->allocs) cudaFree(p);
+    for (int q = 0; q < 2; ++q) {
+        if (b->hring[q]) cudaFreeHost(b->hring[q]);
+        if (b->hpos[q]) cudaFreeHost(b->hpos[q]);
+        if (b->hstatus[q]) cudaFreeHost(b->hstatus[q]);
+        if (b->lev[q]) cudaEventDestroy(b->lev[q]);
+    }
     delete b;
     return MCS_OK;
 }
 
-MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez, uint64_t seed,
-                          int64_t n0, double tol, int64_t capacity, const double* x, const double* v,
-                          const double* w, const double* s, const uint8_t* active, int64_t n, int* slot) {
-    if (!b || !t || !slot || capacity < 1 || n < 0 || n > capacity) return MCS_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// Host bookkeeping of a join: a free instance slot, a first-fit region of `capacity` slots
+// and the gas table's index (registered on the device, stream-ordered, when new).
+int place_instance(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez, uint64_t seed, int64_t n0,
+                   double tol, int64_t capacity, int* k_out, Inst* inst_out) {
     mcs_ctx* c = b->ctx;
-    if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
-    if (int st = sync_status(c)) return st;  // joins between steps only
     int k = -1;
     for (int q = 0; q < b->K; ++q)
         if (!b->hinst[q].live) { k = q; break; }
@@ -846,9 +884,9 @@ MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey
         if ((int)b->gases.size() >= kMaxGases) return set_err(c, MCS_ERR_ARG, "too many distinct tables");
         gas = (int)b->gases.size();
         b->gases.push_back(t);
-        if (cudaMemcpyAsync(b->d_tabs + gas, &t->v, sizeof(TableView), cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
-            cudaStreamSynchronize(c->stream) != cudaSuccess)
-            return set_err(c, MCS_ERR_CUDA, "table upload");
+        k_bset_table<<<1, 1, 0, c->stream>>>(b->d_tabs, gas, t->v);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
     }
     Inst I{};
     I.base = base;
@@ -863,6 +901,27 @@ MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey
         if (t->v.kind[j] == MCS_IONIZATION || t->v.kind[j] == MCS_IONIZATION_UNIFORM) { I.sel_row = j; break; }
     I.n0 = n0;
     I.tol = tol;
+    *k_out = k;
+    *inst_out = I;
+    return MCS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez, uint64_t seed,
+                          int64_t n0, double tol, int64_t capacity, const double* x, const double* v,
+                          const double* w, const double* s, const uint8_t* active, int64_t n, int* slot) {
+    if (!b || !t || !slot || capacity < 1 || n < 0 || n > capacity) return MCS_ERR_ARG;
+    if (n > 0 && (!x || !v || !w || !s || !active)) return MCS_ERR_ARG;
+    mcs_ctx* c = b->ctx;
+    if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
+    if (int st = sync_status(c)) return st;  // host arrays are copied between steps
+    int k = -1;
+    Inst I{};
+    if (int st = place_instance(b, t, ex, ey, ez, seed, n0, tol, capacity, &k, &I)) return st;
+    const long long base = I.base;
     // particles: host -> device staging (doubles) -> FP32 SoA region
     if (n > 0) {
         std::vector<float> tmp((size_t)n);
@@ -897,12 +956,74 @@ MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey
     return MCS_OK;
 }
 
+// Join with electrons drawn on the device: n electrons at the origin, weight 1, isotropic
+// Maxwellian velocities of mean energy mean_energy_ev.  Stream-ordered, no host wait.
+MCS_API int mcs_batch_add_maxwellian(mcs_batch* b, const mcs_table* t, double ex, double ey, double ez,
+                                     uint64_t seed, int64_t n0, double tol, int64_t capacity, int64_t n,
+                                     double mean_energy_ev, int* slot) {
+    if (!b || !t || !slot || capacity < 1 || n < 0 || n > capacity || !(mean_energy_ev >= 0)) return MCS_ERR_ARG;
+    mcs_ctx* c = b->ctx;
+    if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
+    int k = -1;
+    Inst I{};
+    if (int st = place_instance(b, t, ex, ey, ez, seed, n0, tol, capacity, &k, &I)) return st;
+    const int gr = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)c->num_sms * 8));
+    k_binit<<<gr, 256, 0, c->stream>>>(b->d, k, I, (long long)n, maxwellian_sigma(mean_energy_ev));
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
+    b->hinst[k] = I;
+    *slot = k;
+    return MCS_OK;
+}
+
+// Leave: stream-ordered, so steps already enqueued still advance the instance.
 MCS_API int mcs_batch_remove(mcs_batch* b, int slot) {
     if (!b || slot < 0 || slot >= b->K || !b->hinst[slot].live) return MCS_ERR_ARG;
     if (cudaSetDevice(b->ctx->device) != cudaSuccess) return MCS_ERR_CUDA;
-    if (int st = sync_status(b->ctx)) return st;
     b->hinst[slot].live = 0;
-    return upload_inst(b, slot);
+    k_bset_live<<<1, 1, 0, b->ctx->stream>>>(b->d.inst, slot, 0);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MCS_OK : set_err(b->ctx, MCS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// Enqueue copies of every slot's ring, logged-step counts and the status word into pinned
+// host buffer `buf` (0 or 1), then clear the device status; returns without waiting.
+MCS_API int mcs_batch_logs_enqueue(mcs_batch* b, int buf) {
+    if (!b || buf < 0 || buf > 1) return MCS_ERR_ARG;
+    mcs_ctx* c = b->ctx;
+    if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
+    const size_t ring_bytes = sizeof(double) * kBM * kBatchLog * b->K;
+    if (!b->hring[buf]) {
+        if (cudaHostAlloc(&b->hring[buf], ring_bytes, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&b->hpos[buf], sizeof(uint32_t) * b->K, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&b->hstatus[buf], sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->lev[buf], cudaEventDisableTiming) != cudaSuccess)
+            return set_err(c, MCS_ERR_NOMEM, "pinned log buffers");
+    }
+    cudaError_t e = cudaMemcpyAsync(b->hring[buf], b->d.log, ring_bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hpos[buf], b->d.logpos, sizeof(uint32_t) * b->K, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->hstatus[buf], c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b->lev[buf], c->stream);
+    return e == cudaSuccess ? MCS_OK : set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// Wait for buffer `buf`'s copies; *ring / *logpos point into the pinned buffer (valid until
+// the next enqueue into it).  A device status raised before the copy is returned here.
+MCS_API int mcs_batch_logs_wait(mcs_batch* b, int buf, const double** ring, const uint32_t** logpos) {
+    if (!b || buf < 0 || buf > 1 || !b->lev[buf] || !ring || !logpos) return MCS_ERR_ARG;
+    mcs_ctx* c = b->ctx;
+    if (cudaEventSynchronize(b->lev[buf]) != cudaSuccess) return set_err(c, MCS_ERR_CUDA, "log copy");
+    *ring = b->hring[buf];
+    *logpos = b->hpos[buf];
+    const uint32_t st = *b->hstatus[buf];
+    if (st) {
+        const int code = map_status(st);
+        if (code) return set_err(c, code, status_text(code));
+    }
+    return MCS_OK;
 }
 
 MCS_API int mcs_batch_step(mcs_batch* b, double dt, int nsteps, int use_graph) {

@@ -90,6 +90,25 @@ struct Event {
     __device__ __forceinline__ void second() { c = philox10(U4{slot, step, (j - 1) | 0x80000000u, tag}, k0, k1); }
 };
 
+// Initial electron of slot `slot`: an isotropic Maxwellian velocity whose components have
+// standard deviation `sigma` (m/s) and a free-flight s = -log(u).  Five uniforms of the
+// stream {slot, 0, k/4, TAG_INIT}: Box-Muller on (u0, u1) gives vx, vy and on (u2, u3) vz;
+// u4 gives s.
+__device__ __forceinline__ void maxwellian_draw(uint64_t seed, uint32_t slot, double sigma, double& vx, double& vy,
+                                                double& vz, double& s) {
+    Rng r;
+    r.init(seed, slot, 0u, TAG_INIT);
+    const double u0 = r.u64(), u1 = r.u64(), u2 = r.u64(), u3 = r.u64(), u4 = r.u64();
+    const double r0 = sqrt(-2.0 * log(u0)), r1 = sqrt(-2.0 * log(u2));
+    double s0, c0, s1, c1;
+    sincos(6.283185307179586 * u1, &s0, &c0);
+    sincos(6.283185307179586 * u3, &s1, &c1);
+    vx = sigma * (r0 * c0);
+    vy = sigma * (r0 * s0);
+    vz = sigma * (r1 * c1);
+    s = -log(u4);
+}
+
 template <typename T> struct Uni;
 template <> struct Uni<double> { __device__ static double get(Rng& r) { return r.u64(); } };
 template <> struct Uni<float> { __device__ static float get(Rng& r) { return r.u32(); } };

@@ -48,6 +48,31 @@ __global__ void k_upload(const double* __restrict__ x, const double* __restrict_
     }
 }
 
+// Initial swarm electrons at the origin, weight 1, Maxwellian velocities (maxwellian_draw).
+template <typename T>
+__global__ void k_init_maxwellian(PopView<T> P, long long n, unsigned long long seed, double sigma) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double vx, vy, vz, s;
+        maxwellian_draw(seed, (uint32_t)i, sigma, vx, vy, vz, s);
+        P.f[0][i] = (T)0; P.f[1][i] = (T)0; P.f[2][i] = (T)0;
+        P.f[3][i] = (T)vx; P.f[4][i] = (T)vy; P.f[5][i] = (T)vz;
+        P.f[6][i] = (T)1;
+        P.f[7][i] = (T)s;
+        P.act[i] = 1;
+    }
+}
+
+int launch_init_maxwellian(mcs_pop* p, long long n, double sigma) {
+    mcs_ctx* c = p->ctx;
+    const int gr = grid_for(c, n, 256);
+    if (p->precision == MCS_FP32)
+        k_init_maxwellian<float><<<gr, 256, 0, c->stream>>>(pop_view<float>(p), n, p->seed, sigma);
+    else
+        k_init_maxwellian<double><<<gr, 256, 0, c->stream>>>(pop_view<double>(p), n, p->seed, sigma);
+    MCS_CK_LAUNCH(c);
+    return MCS_OK;
+}
+
 template <typename T>
 __device__ __forceinline__ void abs_position(const PopView<T>& P, const GridView& g, int mesh, long long i, double& x,
                                              double& y, double& z) {

@@ -1,5 +1,8 @@
 // pop_ops.h -- launchers of the population-level kernels (pop_ops.cu).
 #pragma once
+#include <cmath>
+
+#include "mcs_device.cuh"
 #include "mcs_internal.h"
 
 namespace mcs {
@@ -12,6 +15,11 @@ int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* 
                   const uint8_t* da, long long n);
 int launch_download(mcs_pop* p, double* dx, double* dv, double* dw, double* ds, uint8_t* da);
 int grid_for(mcs_ctx* c, long long n, int block);
+int launch_init_maxwellian(mcs_pop* p, long long n, double sigma);
+// Standard deviation of each velocity component of a Maxwellian with mean energy mean_ev.
+inline double maxwellian_sigma(double mean_ev) {
+    return sqrt((2.0 / 3.0) * mean_ev * kElementaryCharge / kElectronMass);
+}
 int map_status(uint32_t st);
 const char* status_text(int code);
 // Wait for the context's stream and turn the sticky device status into an error code.

@@ -159,6 +159,10 @@ class Population:
         self.ctx.check(self.ctx.lib.mcs_pop_get_step(self.h, C.byref(s)))
         return s.value
 
+    def init_maxwellian(self, n: int, mean_ev: float = 1.0) -> None:
+        """n swarm electrons drawn on the device (origin, weight 1, isotropic Maxwellian)."""
+        self.ctx.check(self.ctx.lib.mcs_pop_init_maxwellian(self.h, int(n), float(mean_ev)))
+
     def upload(self, p: ParticleArrays) -> None:
         x = np.ascontiguousarray(p.x, dtype=np.float64)
         v = np.ascontiguousarray(p.v, dtype=np.float64)

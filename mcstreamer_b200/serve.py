@@ -117,16 +117,12 @@ class _Live:
     cap: int
     admitted: float
     next_T: int = 0
+    first_chunk: int = 0                        # first chunk whose steps include this request
     rows: list = field(default_factory=list)    # per-step sums, in step order
     nu: list = field(default_factory=list)      # per-step mean ionization rate
 
     def sums(self) -> np.ndarray:
         return np.concatenate(self.rows) if self.rows else np.zeros((0, L.BATCH_MOMENTS))
-
-
-def _particles(req: SwarmRequest):
-    from .swarm import initial_particles
-    return initial_particles(req.n, "maxwellian", req.seed, mean_ev=req.mean_ev)
 
 
 class SwarmServer:
@@ -159,20 +155,26 @@ class SwarmServer:
     def capacity_of(self, req: SwarmRequest) -> int:
         return max(64, int(self.capacity_factor * req.n))
 
-    def _admit(self, req: SwarmRequest, now: float) -> bool:
+    def _admit(self, req: SwarmRequest, now: float, first_chunk: int) -> bool:
         cap = self.capacity_of(req)
         if cap > self.free_slots or len(self.live) >= self.batch.max_instances:
             return False
         ez = req.en_td * self.density * co.Td
         try:
-            slot = self.batch.add(self.tables[req.gas], ez, req.seed, req.n, cap, _particles(req))
+            slot = self.batch.add_maxwellian(self.tables[req.gas], ez, req.seed, req.n, cap, req.n, req.mean_ev)
         except L.MCSError as e:
             if e.code in (L.ERR_NOMEM, L.ERR_CAPACITY):   # fragmented pool / no instance slot
                 return False
             raise
         self.free_slots -= cap
-        self.live[slot] = _Live(req, slot, cap, now, self.rule.first_check())
+        lv = _Live(req, slot, cap, now, self.rule.first_check())
+        lv.first_chunk = first_chunk
+        self.live[slot] = lv
         return True
+
+    def _retire(self, slot: int) -> None:
+        self.batch.remove(slot)
+        self.free_slots += self.live.pop(slot).cap
 
     def _respond(self, lv: _Live, T: int, k: float, err: float, settled: bool, now: float) -> SwarmResponse:
         s = lv.sums()[:T]
@@ -183,21 +185,20 @@ class SwarmServer:
         return SwarmResponse(lv.req.rid, lv.req.gas, lv.req.en_td, lv.req.n, T, k / self.density,
                              err / self.density, settled, drift, energy, lv.req.arrival, lv.admitted, now)
 
-    def _collect(self, nsteps: int, now: float) -> list[SwarmResponse]:
-        ring, pos = self.batch.read_logs()
+    def _collect(self, ring: np.ndarray, pos: np.ndarray, chunk_id: int, nsteps: int, now: float
+                 ) -> list[SwarmResponse]:
         done = []
         for slot, lv in list(self.live.items()):
+            if lv.first_chunk > chunk_id:        # joined after this chunk was enqueued
+                continue
             p = int(pos[slot])
-            idx = [(t % L.BATCH_LOG) for t in range(p - nsteps, p)]
-            rows = ring[slot, idx]
+            rows = ring[slot, [(t % L.BATCH_LOG) for t in range(p - nsteps, p)]]
             lv.rows.append(rows)
             lv.nu.extend((rows[:, L.B_NU] / np.maximum(rows[:, L.S_COUNT], 1.0)).tolist())
             T, k, err, settled, lv.next_T = self.rule.evaluate(np.asarray(lv.nu), lv.next_T)
             if T > 0:
                 done.append(self._respond(lv, T, k, err, settled, now))
-                self.batch.remove(slot)
-                self.free_slots += lv.cap
-                del self.live[slot]
+                self._retire(slot)
         return done
 
     def run(self, requests: Sequence[SwarmRequest], clock: Callable[[], float] = time.perf_counter,
@@ -206,41 +207,56 @@ class SwarmServer:
         """Serve `requests` (arrival times relative to the start).  realtime=False admits
         every request at once in arrival order (the arrival clock is ignored).  With a
         deadline (seconds) the run stops there; unfinished requests are left out of the
-        result and counted in self.unfinished."""
+        result and counted in self.unfinished.
+
+        The device always has the next chunk queued while the host reads the previous
+        chunk's per-step sums (two pinned log buffers): joins, leaves and the log copies are
+        stream-ordered, so the host never waits for the GPU except for the oldest chunk."""
         order = sorted(requests, key=lambda r: (r.arrival, r.rid))
         t0 = clock()
         nxt = 0
         queue: list[SwarmRequest] = []
         out: list[SwarmResponse] = []
+        inflight: list[tuple[int, int]] = []     # (chunk id, steps) enqueued, not yet read
+        chunk_id = 0
         self.unfinished = 0
-        while nxt < len(order) or queue or self.live:
+        while True:
             now = clock() - t0
             if deadline is not None and now > deadline:
+                for cid, k in inflight:
+                    self.batch.logs_wait(cid % 2)
                 self.unfinished = len(order) - nxt + len(queue) + len(self.live)
                 for slot in list(self.live):
-                    self.batch.remove(slot)
-                    self.free_slots += self.live.pop(slot).cap
+                    self._retire(slot)
+                self.batch.sync()
                 break
             while nxt < len(order) and (not realtime or order[nxt].arrival <= now):
                 queue.append(order[nxt])
                 nxt += 1
-            while queue and self._admit(queue[0], now):
+            while queue and self._admit(queue[0], now, chunk_id):
                 queue.pop(0)
-            if not self.live:
-                if queue:
-                    raise RuntimeError(f"request {queue[0].rid} does not fit the memory pool")
-                if nxt < len(order):
-                    time.sleep(max(0.0, min(0.01, order[nxt].arrival - (clock() - t0))))
+            if self.live and len(inflight) < 2:
+                k = self.chunk
+                self.batch.step(self.dt, k, graph=self.graph)
+                self.batch.logs_enqueue(chunk_id % 2)
+                inflight.append((chunk_id, k))
+                chunk_id += 1
+                self.gpu_steps += k
                 continue
-            # steps until the next retirement check; never beyond what the ring holds
-            k = min(self.chunk, L.BATCH_LOG)
-            self.batch.step(self.dt, k, graph=self.graph)
-            self.gpu_steps += k
-            done = self._collect(k, clock() - t0)
-            for r in done:
-                out.append(r)
-                if on_response:
-                    on_response(r)
+            if inflight:
+                cid, k = inflight.pop(0)
+                ring, pos = self.batch.logs_wait(cid % 2)
+                for r in self._collect(ring, pos, cid, k, clock() - t0):
+                    out.append(r)
+                    if on_response:
+                        on_response(r)
+                continue
+            if queue:
+                raise RuntimeError(f"request {queue[0].rid} does not fit the memory pool")
+            if nxt >= len(order):
+                break
+            time.sleep(max(0.0, min(0.01, order[nxt].arrival - (clock() - t0))))
+        self.batch.sync()
         return sorted(out, key=lambda r: r.rid)
 
     def close(self) -> None:

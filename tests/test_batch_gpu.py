@@ -146,3 +146,38 @@ def test_batched_solves_driver(ctx, tables):
         _, mom = _alone(ctx, sv.table, sv.en_td, sv.seed, sv.n0, sv.capacity, sv.nt)
         np.testing.assert_array_equal(r.sums[:, :L.STEP_MOMENTS], mom)
         assert r.steps == 30
+
+
+@pytest.mark.gpu
+def test_device_maxwellian_join_equals_population_init(ctx, tables):
+    nt, n, cap, seed, en = 15, 3000, 9000, 21, 500.0
+    pop = jumc.Population(cap, None, tables[1], precision="fp32", seed=seed)
+    pop.init_maxwellian(n, 2.0)
+    fld = jumc.FixedField(en * co.Td * DENS, ctx)
+    ctx.check(ctx.lib.mcs_swarm_run(pop.h, tables[1].h, fld.h, DT, nt, n, 0.1, 1, None))
+    alone = pop.download()
+    fld.close(); pop.close()
+    with SwarmBatch(ctx, 2, cap) as b:
+        k = b.add_maxwellian(tables[1], en * co.Td * DENS, seed, n, cap, n, 2.0)
+        b.step(DT, nt)
+        _same(b.download(k), alone)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-14), ("fp32", 1e-6)])
+def test_device_maxwellian_matches_restatement(ctx, tables, precision, rtol):
+    """The device draw against a restatement from the oracle's Philox uniforms (INIT stream)."""
+    from oracle import pyoracle as po
+    n, seed, mean_ev = 512, 77, 3.0
+    pop = jumc.Population(n, None, tables[0], precision=precision, seed=seed)
+    pop.init_maxwellian(n, mean_ev)
+    got = pop.download()
+    pop.close()
+    sigma = np.sqrt((2.0 / 3.0) * mean_ev * co.elementary_charge / co.electron_mass)
+    u = np.array([[po.uniform(seed, i, 0, 3, k) for k in range(5)] for i in range(n)])
+    r0, r1 = np.sqrt(-2.0 * np.log(u[:, 0])), np.sqrt(-2.0 * np.log(u[:, 2]))
+    v = sigma * np.stack([r0 * np.cos(2 * np.pi * u[:, 1]), r0 * np.sin(2 * np.pi * u[:, 1]),
+                          r1 * np.cos(2 * np.pi * u[:, 3])], axis=1)
+    np.testing.assert_allclose(got.v, v, rtol=rtol, atol=rtol * sigma)
+    np.testing.assert_allclose(got.s, -np.log(u[:, 4]), rtol=rtol, atol=0)
+    assert (got.x == 0).all() and (got.w == 1).all() and (got.active == 1).all()
