@@ -27,7 +27,18 @@ namespace mcs {
 constexpr int kMaxGases = 16;
 constexpr int kBatchLog = MCS_BATCH_LOG;  // per-instance ring of per-step sums
 constexpr int kBM = MCS_BATCH_MOMENTS;  // the 12 step sums + sum nu_ion, sum nu_ion^2
-constexpr int kBTile = 2048;        // tile of the scan / resample / repack passes
+constexpr int kRBlock = 256;        // threads of the resample / repack passes
+constexpr int kRItems = 16;         // contiguous slots per thread (one 16-byte load of flags)
+constexpr int kRTile = kRBlock * kRItems;
+constexpr int kSlotAlign = 16;      // instance regions start on 16-slot boundaries
+
+// Passes of a batched step (what the plan tiles over, per instance):
+//   PASS_STEP      advance! over [0, n)
+//   PASS_RESAMPLE  Swarm.resample! decisions + clone append over [0, n), survivors counted
+//   PASS_HOLES     repack!: inactive slots below A (A = actives) -> hole list
+//   PASS_MOVE      repack!: actives at or above A, from the end, -> holes
+enum : int { PASS_STEP = 0, PASS_RESAMPLE = 1, PASS_HOLES = 2, PASS_MOVE = 3 };
+enum : int { MODE_SKIP = 0, MODE_DROP = 1, MODE_CLONE = 2 };
 
 struct Inst {
     long long base, cap;
@@ -57,9 +68,12 @@ struct BatchDev {
     uint32_t* counters;             // [0] ticket, [1] CTA done, [2] epoch
     uint32_t* status;
     const TableView* tabs;
-    uint32_t* u32a;
-    uint32_t* u32b;
-    long long* tot;
+    uint32_t* holes;                // repack hole list (region-local slots), per slot
+    uint32_t* tile_inst;            // instance of each tile of the current pass
+    long long* rlo;                 // [K] first slot of the pass's range per instance
+    long long* tot;                 // [K] clones appended by Swarm.resample!
+    long long* actives;             // [K] actives after Swarm.resample! (A of repack!)
+    uint8_t* mode;                  // [K] MODE_* of this step's Swarm.resample!
     int K;
     uint32_t flags;
     char* stage;
@@ -69,25 +83,51 @@ struct BatchDev {
 };
 
 // ---------------------------------------------------------------------------------------
-// Plan: tile prefix over instances for a pass reading counts `nin` with tile size `tile`;
-// defaults the pass's output counts to its input counts and advances the epoch.
+// Plan of one pass: per instance a slot range [lo, hi) (see PASS_*), its tiles prefixed
+// over instances (tstart), the tile -> instance map, and the pass's per-instance setup;
+// advances the ordered-append epoch.  One block of 1024 threads.
 // ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_bplan(BatchDev B, int in_is_n1, int tile) {
+__device__ __forceinline__ int resample_mode(const Inst& I, double ncur_d) {
+    const long long ncur = (long long)ncur_d;
+    if (I.n0 <= 0 || ncur == 0 || fabs((double)(ncur - I.n0) / (double)I.n0) < I.tol) return MODE_SKIP;
+    return ncur > I.n0 ? MODE_DROP : MODE_CLONE;
+}
+
+// Slot range of instance k in a pass (after the pass's setup in k_bplan).
+__device__ __forceinline__ void pass_range(const BatchDev& B, int pass, int k, long long& lo, long long& hi) {
+    const int live = B.inst[k].live;
+    lo = 0;
+    if (pass == PASS_STEP) { hi = live ? B.n0buf[k] : 0; return; }
+    if (pass == PASS_RESAMPLE) { hi = live ? B.n1buf[k] : 0; return; }
+    const long long A = B.actives[k], n = B.n0buf[k];
+    const bool need = live && A < n;
+    if (pass == PASS_HOLES) { hi = need ? A : 0; return; }
+    lo = A;
+    hi = need ? n : A;
+}
+
+__global__ void __launch_bounds__(1024) k_bplan(BatchDev B, int pass, int tile) {
     __shared__ long long wsum[32];
-    const long long* nin = in_is_n1 ? B.n1buf : B.n0buf;
-    long long* nout = in_is_n1 ? B.n0buf : B.n1buf;
     const int per = (B.K + 1023) / 1024;
     long long loc = 0;
     for (int q = 0; q < per; ++q) {
         const int k = threadIdx.x * per + q;
-        if (k < B.K) {
-            const long long n = B.inst[k].live ? nin[k] : 0;
-            loc += (n + tile - 1) / tile;
-            nout[k] = nin[k];
+        if (k >= B.K) break;
+        if (pass == PASS_STEP) {
+            B.n1buf[k] = B.n0buf[k];
             B.done[k] = 0;
+        } else if (pass == PASS_RESAMPLE) {
+            const Inst I = B.inst[k];
+            B.n0buf[k] = B.n1buf[k];
+            B.tot[k] = 0;
+            B.actives[k] = 0;
+            B.mode[k] = (uint8_t)(I.live ? resample_mode(I, B.curm[(long long)k * kBM + SM_COUNT]) : MODE_SKIP);
         }
+        long long lo, hi;
+        pass_range(B, pass, k, lo, hi);
+        B.rlo[k] = lo;
+        loc += (hi - lo + tile - 1) / tile;
     }
-    // block exclusive scan of loc
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     long long incl = loc;
     for (int o = 1; o < 32; o <<= 1) {
@@ -107,21 +147,14 @@ __global__ void __launch_bounds__(1024) k_bplan(BatchDev B, int in_is_n1, int ti
     long long run = wsum[wid] + incl - loc;
     for (int q = 0; q < per; ++q) {
         const int k = threadIdx.x * per + q;
-        if (k < B.K) {
-            B.tstart[k] = run;
-            const long long n = B.inst[k].live ? nin[k] : 0;
-            run += (n + tile - 1) / tile;
-        }
+        if (k >= B.K) break;
+        B.tstart[k] = run;
+        long long lo, hi;
+        pass_range(B, pass, k, lo, hi);
+        const long long nt = (hi - lo + tile - 1) / tile;
+        for (long long t = 0; t < nt; ++t) B.tile_inst[run + t] = (uint32_t)k;
+        run += nt;
     }
-}
-
-__device__ __forceinline__ int find_inst(const long long* tstart, int K, long long g) {
-    int lo = 0, hi = K;  // largest k with tstart[k] <= g, among k < K
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (tstart[mid] <= g) lo = mid; else hi = mid;
-    }
-    return lo;
 }
 
 // Rate of row j at energy v2 (FP32 table), for the per-step rate estimator (collrate).
@@ -177,7 +210,7 @@ __global__ void __launch_bounds__(BLOCK) k_bstep(BatchDev B) {
             sh.count = 0;
             sh.next = 0;
             if (g < T) {
-                const int k = find_inst(B.tstart, B.K, g);
+                const int k = (int)B.tile_inst[g];
                 sh.k = k;
                 sh.I = B.inst[k];
                 sh.tab = B.tabs[sh.I.table];
@@ -443,91 +476,8 @@ __global__ void k_bempty_moments(BatchDev B) {
     }
 }
 
-// ---------------------------------------------------------------------------------------
-// Segmented (per-instance) exclusive scan of u32 counts (in == nullptr: active flags) over
-// the pass's tiles; totals per instance into B.tot.
-// ---------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_bscan(BatchDev B, int in_is_n1, const uint32_t* __restrict__ in,
-                                               uint32_t* __restrict__ out) {
-    constexpr int ITEMS = kBTile / 256;
-    __shared__ uint32_t s_warp[8];
-    __shared__ long long s_g, s_first, s_ntl, s_base, s_n;
-    __shared__ int s_k;
-    __shared__ uint32_t s_excl;
-    const long long T = B.tstart[B.K];
-    const uint32_t epoch = B.counters[2];
-    const long long* nin = in_is_n1 ? B.n1buf : B.n0buf;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            const long long g = atomicAdd(&B.counters[0], 1u);
-            s_g = g;
-            if (g < T) {
-                const int k = find_inst(B.tstart, B.K, g);
-                s_k = k;
-                s_first = B.tstart[k];
-                s_ntl = (k + 1 < B.K ? B.tstart[k + 1] : T) - s_first;
-                s_base = B.inst[k].base;
-                s_n = nin[k];
-            }
-        }
-        __syncthreads();
-        const long long g = s_g;
-        if (g >= T) break;
-        const long long lt = g - s_first;
-        const long long l0 = lt * kBTile + (long long)threadIdx.x * ITEMS;
-        uint32_t v[ITEMS];
-        uint32_t tsum = 0;
-#pragma unroll
-        for (int q = 0; q < ITEMS; ++q) {
-            const long long il = l0 + q;
-            uint32_t cv = 0;
-            if (il < s_n) cv = in ? in[s_base + il] : (uint32_t)(B.act[s_base + il] != 0);
-            v[q] = tsum;
-            tsum += cv;
-        }
-        uint32_t incl = tsum;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t yv = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += yv;
-        }
-        if (lane == 31) s_warp[wid] = incl;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for (int q = 0; q < 8; ++q) { const uint32_t t2 = s_warp[q]; s_warp[q] = acc; acc += t2; }
-            bool ok;
-            s_excl = tile_lookback_from(B.tstatus, (uint32_t)s_first, (uint32_t)g, epoch, acc, B.status, &ok);
-            if (lt == s_ntl - 1) B.tot[s_k] = (long long)s_excl + acc;
-        }
-        __syncthreads();
-        const uint32_t off = s_excl + s_warp[wid] + incl - tsum;
-#pragma unroll
-        for (int q = 0; q < ITEMS; ++q) {
-            const long long il = l0 + q;
-            if (il < s_n) out[s_base + il] = off + v[q];
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const uint32_t d = atomicAdd(&B.counters[1], 1u);
-        if (d == gridDim.x - 1) { B.counters[0] = 0; B.counters[1] = 0; }
-    }
-}
-
-// Zero totals of instances without tiles (their scans never run).
-__global__ void k_bzero_tot(BatchDev B) {
-    const long long T = B.tstart[B.K];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.K; k += gridDim.x * blockDim.x) {
-        const long long nt = (k + 1 < B.K ? B.tstart[k + 1] : T) - B.tstart[k];
-        if (nt == 0) B.tot[k] = 0;
-    }
-}
-
 __device__ long long poisson_sample_b(Rng& r, double lam) {
+    // Inversion below 10, PTRS (Hoermann 1993) above: the same algorithm as the population path.
     if (lam <= 0) return 0;
     if (lam < 10.0) {
         const double u = r.u64();
@@ -554,89 +504,260 @@ __device__ long long poisson_sample_b(Rng& r, double lam) {
     return (long long)floor(lam);
 }
 
-// Grid-stride over all live slots of all instances (pass reading n1).
-template <typename F>
-__device__ __forceinline__ void for_each_slot(const BatchDev& B, const long long* nin, F&& fn) {
-    for (int k = blockIdx.y; k < B.K; k += gridDim.y) {
-        const Inst I = B.inst[k];
-        if (!I.live) continue;
-        const long long n = nin[k];
-        for (long long il = blockIdx.x * (long long)blockDim.x + threadIdx.x; il < n; il += (long long)gridDim.x * blockDim.x)
-            fn(k, I, il);
-    }
-}
-
-// Swarm.resample! decisions (Swarm.jl:193-223) for every instance: drop, or Poisson clone counts.
-__global__ void k_bsres_count(BatchDev B) {
-    for_each_slot(B, B.n1buf, [&](int k, const Inst& I, long long il) {
-        const long long i = I.base + il;
-        uint32_t cnum = 0;
-        const long long ncur = (long long)B.curm[(long long)k * kBM + SM_COUNT];
-        const bool skip = I.n0 <= 0 || ncur == 0 || fabs((double)(ncur - I.n0) / (double)I.n0) < I.tol;
-        if (!skip && B.act[i]) {
-            Rng r;
-            r.init(I.seed, (uint32_t)il, B.step[k] + 1u, TAG_SWARM_RESAMPLE);
-            if (ncur > I.n0) {
-                if (r.u64() < (double)(ncur - I.n0) / (double)ncur) B.act[i] = 0;
-            } else {
-                cnum = (uint32_t)poisson_sample_b(r, (double)(I.n0 - ncur) / (double)ncur);
-            }
-        }
-        B.u32a[i] = cnum;
-    });
-}
-
 __device__ __forceinline__ void bcopy_slot(const BatchDev& B, long long dst, long long src) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) B.f[q][dst] = B.f[q][src];
     B.act[dst] = B.act[src];
 }
 
-__global__ void k_bsres_write(BatchDev B) {
-    for_each_slot(B, B.n1buf, [&](int k, const Inst& I, long long il) {
-        const long long i = I.base + il;
-        const uint32_t cnum = B.u32a[i];
-        const long long n = B.n1buf[k];
-        for (uint32_t j = 0; j < cnum; ++j) {
-            const long long dl = n + (long long)B.u32b[i] + j;
-            if (dl >= I.cap) { atomicOr(B.status, ST_CAPACITY); break; }
-            bcopy_slot(B, I.base + dl, i);
+// Tile header shared by the resample / repack passes: the next ticket and its instance.
+struct RShared {
+    long long g, first, ntl, base, lo, n, cap, A;
+    unsigned long long seed;
+    double pdrop, lam;
+    uint32_t step1, excl;
+    int k, mode, ok;
+    uint32_t wtot[kRBlock / 32];
+    uint32_t wtot2[kRBlock / 32];
+};
+
+__device__ __forceinline__ bool rtile_next(const BatchDev& B, RShared& sh, int pass) {
+    if (threadIdx.x == 0) {
+        const long long g = atomicAdd(&B.counters[0], 1u);
+        sh.g = g;
+        if (g < B.tstart[B.K]) {
+            const int k = (int)B.tile_inst[g];
+            const Inst I = B.inst[k];
+            sh.k = k;
+            sh.first = B.tstart[k];
+            sh.ntl = B.tstart[k + 1] - sh.first;
+            sh.base = I.base;
+            sh.cap = I.cap;
+            sh.lo = B.rlo[k];
+            sh.seed = I.seed;
+            if (pass == PASS_RESAMPLE) {
+                sh.n = B.n1buf[k];
+                sh.mode = B.mode[k];
+                const double ncur = B.curm[(long long)k * kBM + SM_COUNT];
+                sh.pdrop = (ncur - (double)I.n0) / ncur;
+                sh.lam = ((double)I.n0 - ncur) / ncur;
+                sh.step1 = B.step[k] + 1u;
+            } else {
+                sh.n = B.n0buf[k];
+                sh.A = B.actives[k];
+            }
         }
-    });
-    if (blockIdx.x == 0)
-        for (int k = blockIdx.y * blockDim.x + threadIdx.x; k < B.K; k += gridDim.y * blockDim.x) {
-            if (!B.inst[k].live) continue;
-            long long m = B.n1buf[k] + B.tot[k];
-            if (m > B.inst[k].cap) { m = B.inst[k].cap; atomicOr(B.status, ST_CAPACITY); }
-            B.n0buf[k] = m;
-        }
+    }
+    __syncthreads();
+    return sh.g < B.tstart[B.K];
 }
 
-// repack! (population.jl:191-215) per instance: holes below A get the actives at or
-// above A, taken from the end.
-__global__ void k_brepack_holes(BatchDev B) {
-    for_each_slot(B, B.n0buf, [&](int k, const Inst& I, long long il) {
-        const long long A = B.tot[k];
-        const long long i = I.base + il;
-        if (il < A && !B.act[i]) B.u32a[I.base + (il - (long long)B.u32b[i])] = (uint32_t)il;
-    });
+// Block-wide exclusive scan (slot order = thread order, kRItems consecutive slots per
+// thread) of per-thread totals; returns this thread's offset, block total in *total.
+__device__ __forceinline__ uint32_t rblock_scan(RShared& sh, uint32_t v, uint32_t* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();   // the previous scan's readers are done with sh.wtot
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sh.wtot[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (int q = 0; q < kRBlock / 32; ++q) { const uint32_t t = sh.wtot[q]; sh.wtot2[q] = a; a += t; }
+        sh.wtot[0] = a;
+    }
+    __syncthreads();
+    *total = sh.wtot[0];
+    return sh.wtot2[wid] + incl - v;
 }
 
-__global__ void k_brepack_move(BatchDev B) {
-    for_each_slot(B, B.n0buf, [&](int k, const Inst& I, long long il) {
-        const long long A = B.tot[k];
-        const long long i = I.base + il;
-        if (il >= A && B.act[i]) {
-            const long long q = A - 1 - (long long)B.u32b[i];
-            bcopy_slot(B, I.base + (long long)B.u32a[I.base + q], i);
+__device__ __forceinline__ void rpass_done(const BatchDev& B) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const uint32_t d = atomicAdd(&B.counters[1], 1u);
+        if (d == gridDim.x - 1) { B.counters[0] = 0; B.counters[1] = 0; }
+    }
+}
+
+// Active flags of this thread's kRItems slots starting at region-local l0 (slots at or
+// beyond `lim` read as inactive).  Regions start on 16-slot boundaries and l0 is a multiple
+// of 16, so one 16-byte load covers them.
+__device__ __forceinline__ void load_flags(const BatchDev& B, long long base, long long l0, long long lim,
+                                           uint8_t (&a)[kRItems]) {
+    if (l0 >= lim) {
+#pragma unroll
+        for (int q = 0; q < kRItems; ++q) a[q] = 0;
+        return;
+    }
+    const uint4 v = *reinterpret_cast<const uint4*>(B.act + base + l0);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < kRItems; ++q) a[q] = (l0 + q < lim) ? (uint8_t)((w[q >> 2] >> (8 * (q & 3))) & 0xffu) : 0;
+}
+
+// ---------------------------------------------------------------------------------------
+// Swarm.resample!(popl, n0, tol) (Swarm/src/Swarm.jl:193-223) of every instance in one
+// pass: roulette (drop mode) or Poisson clone counts (clone mode) from the stream
+// {slot, step, k/4, TAG_SWARM_RESAMPLE}, the clones appended after the instance's particles
+// in slot order (tile scan + look-back bounded to the instance's tiles), and the actives
+// after resampling counted into B.actives (the A of repack!).
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRBlock) k_bresample(BatchDev B) {
+    __shared__ RShared sh;
+    const uint32_t epoch = B.counters[2];
+    for (;;) {
+        if (!rtile_next(B, sh, PASS_RESAMPLE)) break;
+        const long long lt = sh.g - sh.first;
+        const long long l0 = lt * kRTile + (long long)threadIdx.x * kRItems;
+        const long long n = sh.n, base = sh.base;
+        uint8_t a[kRItems];
+        load_flags(B, base, l0, n, a);
+        uint32_t cnum[kRItems];
+        uint32_t alive = 0, csum = 0;
+#pragma unroll 1
+        for (int q = 0; q < kRItems; ++q) {
+            cnum[q] = 0;
+            if (!a[q]) continue;
+            if (sh.mode == MODE_DROP) {
+                Rng r;
+                r.init(sh.seed, (uint32_t)(l0 + q), sh.step1, TAG_SWARM_RESAMPLE);
+                if (r.u64() < sh.pdrop) { B.act[base + l0 + q] = 0; continue; }
+            } else if (sh.mode == MODE_CLONE) {
+                Rng r;
+                r.init(sh.seed, (uint32_t)(l0 + q), sh.step1, TAG_SWARM_RESAMPLE);
+                cnum[q] = (uint32_t)poisson_sample_b(r, sh.lam);
+                csum += cnum[q];
+            }
+            ++alive;
         }
-    });
+        // survivors of the roulette; the clones actually written are added by the
+        // instance's last tile below (clones are active)
+        uint32_t tot_alive;
+        rblock_scan(sh, alive, &tot_alive);
+        if (threadIdx.x == 0 && tot_alive) atomicAdd(reinterpret_cast<unsigned long long*>(&B.actives[sh.k]),
+                                                     (unsigned long long)tot_alive);
+        if (sh.mode == MODE_CLONE) {
+            uint32_t ctile;
+            const uint32_t off = rblock_scan(sh, csum, &ctile);
+            if (threadIdx.x == 0) {
+                bool ok;
+                sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, ctile, B.status, &ok);
+                sh.ok = ok;
+                if (lt == sh.ntl - 1) {
+                    long long m = n + (long long)sh.excl + ctile;
+                    if (m > sh.cap) { m = sh.cap; atomicOr(B.status, ST_CAPACITY); }
+                    B.tot[sh.k] = m - n;
+                    B.n0buf[sh.k] = m;
+                    if (m > n) atomicAdd(reinterpret_cast<unsigned long long*>(&B.actives[sh.k]),
+                                         (unsigned long long)(m - n));
+                }
+            }
+            __syncthreads();
+            if (sh.ok) {
+                long long d = n + (long long)sh.excl + off;
+                for (int q = 0; q < kRItems; ++q)
+                    for (uint32_t j = 0; j < cnum[q]; ++j, ++d) {
+                        if (d >= sh.cap) { atomicOr(B.status, ST_CAPACITY); break; }
+                        bcopy_slot(B, base + d, base + l0 + q);
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    rpass_done(B);
+}
+
+// ---------------------------------------------------------------------------------------
+// repack! (JuMC/src/population.jl:191-215) of every instance with holes: the k-th inactive
+// slot below A (ascending) receives the k-th active slot at or above A counted from the end
+// -- the pairing of the reference's two-pointer loop.  Pass 1 lists the holes in order.
+// ---------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kRBlock) k_brepack_holes(BatchDev B) {
+    __shared__ RShared sh;
+    const uint32_t epoch = B.counters[2];
+    for (;;) {
+        if (!rtile_next(B, sh, PASS_HOLES)) break;
+        const long long lt = sh.g - sh.first;
+        const long long l0 = lt * kRTile + (long long)threadIdx.x * kRItems;
+        const long long A = sh.A;
+        uint8_t a[kRItems];
+        load_flags(B, sh.base, l0, A, a);
+        uint32_t h = 0;
+#pragma unroll
+        for (int q = 0; q < kRItems; ++q) h += (l0 + q < A && !a[q]) ? 1u : 0u;
+        uint32_t htile;
+        const uint32_t off = rblock_scan(sh, h, &htile);
+        if (threadIdx.x == 0) {
+            bool ok;
+            sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, htile, B.status, &ok);
+            sh.ok = ok;
+        }
+        __syncthreads();
+        if (sh.ok && h) {
+            uint32_t r = sh.excl + off;
+            for (int q = 0; q < kRItems; ++q)
+                if (l0 + q < A && !a[q]) B.holes[sh.base + r++] = (uint32_t)(l0 + q);
+        }
+        __syncthreads();
+    }
+    rpass_done(B);
+}
+
+// Pass 2: the actives in [A, n), walked from the end (tile lt covers the lt-th block of
+// kRTile slots counted back from n), so the look-back prefix is the count of actives after
+// the tile and each active's rank from the end is its hole index.
+__global__ void __launch_bounds__(kRBlock) k_brepack_move(BatchDev B) {
+    __shared__ RShared sh;
+    const uint32_t epoch = B.counters[2];
+    for (;;) {
+        if (!rtile_next(B, sh, PASS_MOVE)) break;
+        const long long lt = sh.g - sh.first;
+        const long long A = sh.A, n = sh.n;
+        // this tile: slots [hi - kRTile, hi) with hi = n - lt*kRTile, clipped at A; thread t
+        // takes the t-th group of kRItems counted back from hi
+        const long long hi = n - lt * kRTile;
+        const long long top = hi - (long long)threadIdx.x * kRItems;     // exclusive
+        uint32_t m = 0;
+        bool act[kRItems];
+#pragma unroll
+        for (int q = 0; q < kRItems; ++q) {
+            const long long i = top - 1 - q;
+            act[q] = i >= A && B.act[sh.base + i];
+            m += act[q] ? 1u : 0u;
+        }
+        uint32_t mtile;
+        const uint32_t off = rblock_scan(sh, m, &mtile);
+        if (threadIdx.x == 0) {
+            bool ok;
+            sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, mtile, B.status, &ok);
+            sh.ok = ok;
+        }
+        __syncthreads();
+        if (sh.ok && m) {
+            uint32_t r = sh.excl + off;   // actives after this thread's group
+            for (int q = 0; q < kRItems; ++q)
+                if (act[q]) {
+                    const long long i = top - 1 - q;
+                    bcopy_slot(B, sh.base + (long long)B.holes[sh.base + r], sh.base + i);
+                    ++r;
+                }
+        }
+        __syncthreads();
+    }
+    rpass_done(B);
 }
 
 __global__ void k_bfinish(BatchDev B) {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < B.K; k += gridDim.x * blockDim.x) {
         if (!B.inst[k].live) continue;
-        B.n0buf[k] = B.tot[k];      // A = actives after repack
+        // A = actives after repack!; never more than the slots in use (a capacity error has
+        // been raised if the counts disagree)
+        B.n0buf[k] = min(B.actives[k], B.n0buf[k]);
         B.step[k] += 1;
         B.logpos[k] += 1;
     }
@@ -693,6 +814,7 @@ struct mcs_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int grid[16] = {};              // persistent grid per variant (resident CTAs x SMs)
+    int rgrid[3] = {};              // persistent grids of the resample / holes / move passes
     // double-buffered pinned copies of the per-step rings (mcs_batch_logs_enqueue / wait)
     double* hring[2] = {nullptr, nullptr};
     uint32_t* hpos[2] = {nullptr, nullptr};
@@ -740,28 +862,23 @@ int launch_variant(mcs_batch* b, int v, cudaStream_t s) {
 }
 
 // One batched step: plan + advance! + Swarm.resample! + repack!, all on stream s.
-// k0/k1 (optional) bracket the persistent step kernel.
+// One batched step on stream s: plan + advance! (k0/k1, optional, bracket the persistent
+// step kernel), Swarm.resample!, repack! (holes, then moves), counters.
 int enqueue_step(mcs_batch* b, int v, cudaStream_t s, cudaEvent_t k0 = nullptr, cudaEvent_t k1 = nullptr) {
     const int tile_step = kVariants[v].block * kVariants[v].ppt;
-    const dim3 g2((unsigned)std::max(1, b->ctx->num_sms * 2), (unsigned)std::min(b->K, 64));
-    k_bplan<<<1, 1024, 0, s>>>(b->d, 0, tile_step);
+    const int kb = (b->K + 255) / 256;
+    k_bplan<<<1, 1024, 0, s>>>(b->d, PASS_STEP, tile_step);
     if (k0) cudaEventRecord(k0, s);
     if (int st = launch_variant(b, v, s)) return st;
     if (k1) cudaEventRecord(k1, s);
-    k_bempty_moments<<<(b->K + 255) / 256, 256, 0, s>>>(b->d);
-    // Swarm.resample!
-    k_bplan<<<1, 1024, 0, s>>>(b->d, 1, kBTile);
-    k_bsres_count<<<g2, 256, 0, s>>>(b->d);
-    k_bzero_tot<<<(b->K + 255) / 256, 256, 0, s>>>(b->d);
-    k_bscan<<<b->ctx->num_sms * 4, 256, 0, s>>>(b->d, 1, b->d.u32a, b->d.u32b);
-    k_bsres_write<<<g2, 256, 0, s>>>(b->d);
-    // repack!
-    k_bplan<<<1, 1024, 0, s>>>(b->d, 0, kBTile);
-    k_bzero_tot<<<(b->K + 255) / 256, 256, 0, s>>>(b->d);
-    k_bscan<<<b->ctx->num_sms * 4, 256, 0, s>>>(b->d, 0, nullptr, b->d.u32b);
-    k_brepack_holes<<<g2, 256, 0, s>>>(b->d);
-    k_brepack_move<<<g2, 256, 0, s>>>(b->d);
-    k_bfinish<<<(b->K + 255) / 256, 256, 0, s>>>(b->d);
+    k_bempty_moments<<<kb, 256, 0, s>>>(b->d);
+    k_bplan<<<1, 1024, 0, s>>>(b->d, PASS_RESAMPLE, kRTile);
+    k_bresample<<<b->rgrid[0], kRBlock, 0, s>>>(b->d);
+    k_bplan<<<1, 1024, 0, s>>>(b->d, PASS_HOLES, kRTile);
+    k_brepack_holes<<<b->rgrid[1], kRBlock, 0, s>>>(b->d);
+    k_bplan<<<1, 1024, 0, s>>>(b->d, PASS_MOVE, kRTile);
+    k_brepack_move<<<b->rgrid[2], kRBlock, 0, s>>>(b->d);
+    k_bfinish<<<kb, 256, 0, s>>>(b->d);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MCS_OK : set_err(b->ctx, MCS_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -787,13 +904,14 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
     mcs_batch* b = new mcs_batch();
     b->ctx = c;
     b->K = max_instances;
-    b->total_cap = total_capacity;
+    // room for every region's rounding to kSlotAlign slots
+    b->total_cap = (total_capacity + kSlotAlign - 1) / kSlotAlign * kSlotAlign + (long long)kSlotAlign * max_instances;
     b->hinst.assign(max_instances, Inst{});
-    b->max_tiles = total_capacity / 128 + max_instances + 1;
+    b->max_tiles = b->total_cap / 128 + max_instances + 1;
     BatchDev& d = b->d;
     int st = MCS_OK;
-    for (int q = 0; q < 8 && !st; ++q) st = balloc(b, &d.f[q], (size_t)total_capacity);
-    if (!st) st = balloc(b, &d.act, (size_t)total_capacity);
+    for (int q = 0; q < 8 && !st; ++q) st = balloc(b, &d.f[q], (size_t)b->total_cap);
+    if (!st) st = balloc(b, &d.act, (size_t)b->total_cap);
     if (!st) st = balloc(b, &d.inst, (size_t)max_instances);
     if (!st) st = balloc(b, &d.n0buf, (size_t)max_instances);
     if (!st) st = balloc(b, &d.n1buf, (size_t)max_instances);
@@ -806,9 +924,12 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
     if (!st) st = balloc(b, &d.logpos, (size_t)max_instances);
     if (!st) st = balloc(b, &d.tstatus, (size_t)b->max_tiles);
     if (!st) st = balloc(b, &d.counters, 8);
-    if (!st) st = balloc(b, &d.u32a, (size_t)total_capacity);
-    if (!st) st = balloc(b, &d.u32b, (size_t)total_capacity);
+    if (!st) st = balloc(b, &d.holes, (size_t)b->total_cap);
+    if (!st) st = balloc(b, &d.tile_inst, (size_t)b->max_tiles);
+    if (!st) st = balloc(b, &d.rlo, (size_t)max_instances);
     if (!st) st = balloc(b, &d.tot, (size_t)max_instances);
+    if (!st) st = balloc(b, &d.actives, (size_t)max_instances);
+    if (!st) st = balloc(b, &d.mode, (size_t)max_instances);
     if (!st) st = balloc(b, &b->d_tabs, kMaxGases);
     // staging for the largest variant grid
     int maxgrid = 0;
@@ -820,6 +941,13 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
         maxgrid = std::max(maxgrid, b->grid[v]);
         const uint32_t cap = 4 * kVariants[v].block * kVariants[v].ppt + 2048;
         stride = std::max(stride, (((size_t)cap * (8 * sizeof(float) + 9)) + 255) & ~(size_t)255);
+    }
+    const void* rk[3] = {reinterpret_cast<const void*>(k_bresample), reinterpret_cast<const void*>(k_brepack_holes),
+                         reinterpret_cast<const void*>(k_brepack_move)};
+    for (int q = 0; q < 3; ++q) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rk[q], kRBlock, 0);
+        b->rgrid[q] = std::max(occ, 1) * c->num_sms;
     }
     char* stage = nullptr;
     if (!st) st = balloc(b, &stage, stride * (size_t)maxgrid);
@@ -870,13 +998,15 @@ int place_instance(mcs_batch* b, const mcs_table* t, double ex, double ey, doubl
     for (int q = 0; q < b->K; ++q)
         if (b->hinst[q].live) used.push_back({b->hinst[q].base, b->hinst[q].cap});
     std::sort(used.begin(), used.end());
+    // regions are kSlotAlign-aligned and a multiple of it long (16-byte loads of the flags)
+    const long long region = (capacity + kSlotAlign - 1) / kSlotAlign * kSlotAlign;
     long long base = 0;
     bool found = false;
     for (auto& u : used) {
-        if (u.first - base >= capacity) { found = true; break; }
-        base = u.first + u.second;
+        if (u.first - base >= region) { found = true; break; }
+        base = u.first + (u.second + kSlotAlign - 1) / kSlotAlign * kSlotAlign;
     }
-    if (!found && b->total_cap - base < capacity) return set_err(c, MCS_ERR_NOMEM, "no room for the instance");
+    if (!found && b->total_cap - base < region) return set_err(c, MCS_ERR_NOMEM, "no room for the instance");
     int gas = -1;
     for (size_t q = 0; q < b->gases.size(); ++q)
         if (b->gases[q] == t) gas = (int)q;
