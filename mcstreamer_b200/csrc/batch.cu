@@ -184,8 +184,8 @@ struct BShared {
 // Batched advance! (FP32, uniform field per instance, closed-form push between real
 // collisions): the body of k_step_abs<float,...,CLOSED> with instance indirection.
 // ---------------------------------------------------------------------------------------
-template <int BLOCK, int PPT>
-__global__ void __launch_bounds__(BLOCK) k_bstep(BatchDev B) {
+template <int BLOCK, int PPT, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
     constexpr int TILE = BLOCK * PPT;
     __shared__ BShared<BLOCK> sh;
     __shared__ uint32_t cnt[TILE];
@@ -798,6 +798,7 @@ using namespace mcs;
 struct BatchVariant {
     int block, ppt;
     const void* fn;
+    int minb = 0;   // resident CTAs per SM the register budget is set for (0: compiler's choice)
 };
 
 struct mcs_batch {
@@ -813,8 +814,10 @@ struct mcs_batch {
     int variant = -1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int grid[16] = {};              // persistent grid per variant (resident CTAs x SMs)
+    int grid[32] = {};              // persistent grid per variant (resident CTAs x SMs)
     int rgrid[3] = {};              // persistent grids of the resample / holes / move passes
+    unsigned long long stage_stride[32] = {};   // per-variant secondary staging slice per CTA
+    uint32_t stage_cap[32] = {};
     // double-buffered pinned copies of the per-step rings (mcs_batch_logs_enqueue / wait)
     double* hring[2] = {nullptr, nullptr};
     uint32_t* hpos[2] = {nullptr, nullptr};
@@ -825,15 +828,21 @@ struct mcs_batch {
 
 namespace {
 
-template <int BLOCK, int PPT>
-const void* bstep_fn() { return reinterpret_cast<const void*>(k_bstep<BLOCK, PPT>); }
+template <int BLOCK, int PPT, int MINB = 0>
+const void* bstep_fn() { return reinterpret_cast<const void*>(k_bstep<BLOCK, PPT, MINB>); }
 
+// The autotuner's space: threads per block x particles per thread, plus shapes that trade
+// registers for resident CTAs (MINB) and longer tiles (16 particles per thread).
 const BatchVariant kVariants[] = {
     {128, 1, bstep_fn<128, 1>()}, {128, 2, bstep_fn<128, 2>()}, {128, 4, bstep_fn<128, 4>()}, {128, 8, bstep_fn<128, 8>()},
     {256, 1, bstep_fn<256, 1>()}, {256, 2, bstep_fn<256, 2>()}, {256, 4, bstep_fn<256, 4>()}, {256, 8, bstep_fn<256, 8>()},
     {512, 1, bstep_fn<512, 1>()}, {512, 2, bstep_fn<512, 2>()}, {512, 4, bstep_fn<512, 4>()}, {512, 8, bstep_fn<512, 8>()},
+    {128, 16, bstep_fn<128, 16>()}, {256, 16, bstep_fn<256, 16>()},
+    {256, 8, bstep_fn<256, 8, 4>(), 4}, {256, 16, bstep_fn<256, 16, 4>(), 4},
+    {128, 8, bstep_fn<128, 8, 8>(), 8}, {512, 8, bstep_fn<512, 8, 2>(), 2},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+static_assert(kNumVariants == MCS_BATCH_VARIANTS, "variant table and header disagree");
 constexpr int kDefaultVariant = 5;  // 256 x 2
 
 template <typename P>
@@ -856,7 +865,10 @@ void drop_graph(mcs_batch* b) {
 
 int launch_variant(mcs_batch* b, int v, cudaStream_t s) {
     const BatchVariant& var = kVariants[v];
-    void* args[] = {&b->d};
+    BatchDev dv = b->d;
+    dv.stage_stride = b->stage_stride[v];
+    dv.stage_cap = b->stage_cap[v];
+    void* args[] = {&dv};
     const cudaError_t e = cudaLaunchKernel(var.fn, dim3(b->grid[v]), dim3(var.block), args, 0, s);
     return e == cudaSuccess ? MCS_OK : set_err(b->ctx, MCS_ERR_CUDA, cudaGetErrorString(e));
 }
@@ -931,16 +943,17 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
     if (!st) st = balloc(b, &d.actives, (size_t)max_instances);
     if (!st) st = balloc(b, &d.mode, (size_t)max_instances);
     if (!st) st = balloc(b, &b->d_tabs, kMaxGases);
-    // staging for the largest variant grid
-    int maxgrid = 0;
-    size_t stride = 0;
+    // secondary staging: per variant a slice of 4 x TILE + 2048 entries per resident CTA
+    size_t stage_bytes = 0;
     for (int v = 0; v < kNumVariants && !st; ++v) {
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kVariants[v].fn, kVariants[v].block, 0);
         b->grid[v] = std::max(occ, 1) * c->num_sms;
-        maxgrid = std::max(maxgrid, b->grid[v]);
         const uint32_t cap = 4 * kVariants[v].block * kVariants[v].ppt + 2048;
-        stride = std::max(stride, (((size_t)cap * (8 * sizeof(float) + 9)) + 255) & ~(size_t)255);
+        const size_t stride = (((size_t)cap * (8 * sizeof(float) + 9)) + 255) & ~(size_t)255;
+        b->stage_stride[v] = stride;
+        b->stage_cap[v] = cap;
+        stage_bytes = std::max(stage_bytes, stride * (size_t)b->grid[v]);
     }
     const void* rk[3] = {reinterpret_cast<const void*>(k_bresample), reinterpret_cast<const void*>(k_brepack_holes),
                          reinterpret_cast<const void*>(k_brepack_move)};
@@ -950,11 +963,11 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
         b->rgrid[q] = std::max(occ, 1) * c->num_sms;
     }
     char* stage = nullptr;
-    if (!st) st = balloc(b, &stage, stride * (size_t)maxgrid);
+    if (!st) st = balloc(b, &stage, stage_bytes);
     if (st) { mcs_batch_destroy(b); return st; }
     d.stage = stage;
-    d.stage_stride = stride;
-    d.stage_cap = (uint32_t)((stride - 255) / (8 * sizeof(float) + 9));
+    d.stage_stride = b->stage_stride[kDefaultVariant];
+    d.stage_cap = b->stage_cap[kDefaultVariant];
     d.status = c->d_status;
     d.tabs = b->d_tabs;
     d.K = max_instances;
@@ -1365,6 +1378,12 @@ MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt) {
     if (variant < 0 || variant >= kNumVariants || !block || !ppt) return MCS_ERR_ARG;
     *block = kVariants[variant].block;
     *ppt = kVariants[variant].ppt;
+    return MCS_OK;
+}
+
+MCS_API int mcs_batch_variant_min_blocks(int variant, int* min_blocks) {
+    if (variant < 0 || variant >= kNumVariants || !min_blocks) return MCS_ERR_ARG;
+    *min_blocks = kVariants[variant].minb;
     return MCS_OK;
 }
 
