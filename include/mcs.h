@@ -100,6 +100,14 @@ MCS_API const char* mcs_last_error(const mcs_ctx* ctx);
 MCS_API int mcs_ctx_set_stream(mcs_ctx* ctx, void* stream);
 MCS_API void* mcs_ctx_stream(mcs_ctx* ctx);
 MCS_API int mcs_ctx_set_flags(mcs_ctx* ctx, uint32_t flags);
+/* Tuning options of a context (no counterpart in the reference, which has no kernels).
+ * MCS_OPT_MESH_SHAPE selects the kernel shape of the FP32 mesh step (0 .. MCS_MESH_SHAPES-1,
+ * 0 = default); every shape computes the same result. */
+enum { MCS_OPT_MESH_SHAPE = 1, MCS_MESH_SHAPES = 8 };
+MCS_API int mcs_ctx_set_option(mcs_ctx* ctx, int option, int value);
+MCS_API int mcs_ctx_get_option(mcs_ctx* ctx, int option, int* value);
+/* (threads per block, particles per thread, resident CTAs per SM) of a mesh-step shape. */
+MCS_API int mcs_mesh_shape(int shape, int* block, int* ppt, int* min_blocks);
 /* Waits for queued work; returns (and clears) the sticky device status. */
 MCS_API int mcs_sync(mcs_ctx* ctx);
 
@@ -163,6 +171,20 @@ MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double
  * electron's draws come from the population seed and its slot (Philox stream INIT).  The
  * reference starts its swarms on the host (Swarm/src/Swarm.jl:104-106). */
 MCS_API int mcs_pop_init_maxwellian(mcs_pop* p, int64_t n, double mean_energy_ev);
+/* Streamer initial condition drawn on the device (no counterpart in the reference, which
+ * reads it from files: MCStreamer/src/initdens.jl): n electrons in a Gaussian cloud of
+ * standard deviation sigma (m) per axis around (cx, cy, cz), speed sqrt(2 E/m) for
+ * E = energy_ev in isotropic directions, weights log-uniform on [wmin, wmax], s = -log(u);
+ * stored in the population's layout (cell + offset on a mesh; not sorted). */
+MCS_API int mcs_pop_init_cloud(mcs_pop* p, int64_t n, double cx, double cy, double cz, double sigma,
+                               double energy_ev, double wmin, double wmax);
+/* Node field of a Gaussian charge e*rho_peak*exp(-r^2/2 sigma^2) centred at (cx, cy, cz)
+ * plus the uniform background (ebx, eby, ebz), from Gauss's law, computed on the device
+ * (cart3d grids). */
+/* The node field of a cart3d grid (3 doubles per node, x fastest), as stored. */
+MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e);
+MCS_API int mcs_grid_set_efield_gaussian(mcs_grid* g, double cx, double cy, double cz, double sigma,
+                                         double rho_peak, double ebx, double eby, double ebz);
 MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src);
 /* nparticles (population.jl:106): particles in use, active or not. */
 MCS_API int mcs_pop_nparticles(mcs_pop* p, int64_t* n);

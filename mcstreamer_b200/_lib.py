@@ -30,6 +30,7 @@ MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
 B_NU, B_NU2, BATCH_MOMENTS, BATCH_LOG, BATCH_VARIANTS = 12, 13, 14, 64, 18
+OPT_MESH_SHAPE, MESH_SHAPES = 1, 8
 
 vp = C.c_void_p
 i32, i64, u32, u64, f64 = C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
@@ -82,6 +83,9 @@ SIGNATURES = {
     "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, i32, pd]),
     "mcs_pop_step_log": (i32, [vp, i32]),
     "mcs_moments_noalloc": (i32, [i32, vp, i32, C.POINTER(C.c_void_p), pu8, i64, pd]),
+    "mcs_ctx_set_option": (i32, [vp, i32, i32]),
+    "mcs_ctx_get_option": (i32, [vp, i32, pi32]),
+    "mcs_mesh_shape": (i32, [i32, pi32, pi32, pi32]),
     "mcs_batch_create": (i32, [vp, i32, i64, ph]),
     "mcs_batch_destroy": (i32, [vp]),
     "mcs_batch_add": (i32, [vp, vp, f64, f64, f64, u64, i64, f64, i64, pd, pd, pd, pd, pu8, i64, pi32]),
@@ -90,6 +94,9 @@ SIGNATURES = {
     "mcs_batch_logs_enqueue": (i32, [vp, i32]),
     "mcs_batch_logs_wait": (i32, [vp, i32, C.POINTER(pd), C.POINTER(C.POINTER(C.c_uint32))]),
     "mcs_pop_init_maxwellian": (i32, [vp, i64, f64]),
+    "mcs_pop_init_cloud": (i32, [vp, i64, f64, f64, f64, f64, f64, f64, f64]),
+    "mcs_grid_set_efield_gaussian": (i32, [vp, f64, f64, f64, f64, f64, f64, f64, f64]),
+    "mcs_grid_read_efield": (i32, [vp, pd]),
     "mcs_batch_step": (i32, [vp, f64, i32, i32]),
     "mcs_batch_sync": (i32, [vp]),
     "mcs_batch_state": (i32, [vp, pi64, C.POINTER(C.c_uint32)]),

@@ -138,6 +138,27 @@ MCS_API int mcs_ctx_set_flags(mcs_ctx* c, uint32_t flags) {
     return MCS_OK;
 }
 
+MCS_API int mcs_ctx_set_option(mcs_ctx* c, int option, int value) {
+    if (!c) return MCS_ERR_ARG;
+    if (option == MCS_OPT_MESH_SHAPE) {
+        if (value < 0 || value >= MCS_MESH_SHAPES) return set_err(c, MCS_ERR_ARG, "no such mesh kernel shape");
+        c->mesh_shape = value;
+        return MCS_OK;
+    }
+    return set_err(c, MCS_ERR_ARG, "unknown option");
+}
+
+MCS_API int mcs_ctx_get_option(mcs_ctx* c, int option, int* value) {
+    if (!c || !value) return MCS_ERR_ARG;
+    if (option == MCS_OPT_MESH_SHAPE) { *value = c->mesh_shape; return MCS_OK; }
+    return set_err(c, MCS_ERR_ARG, "unknown option");
+}
+
+MCS_API int mcs_mesh_shape(int shape, int* block, int* ppt, int* min_blocks) {
+    if (!block || !ppt || !min_blocks) return MCS_ERR_ARG;
+    return mesh_shape_info(shape, block, ppt, min_blocks);
+}
+
 MCS_API int mcs_sync(mcs_ctx* c) {
     if (!c) return MCS_ERR_ARG;
     if (int st = use_device(c)) return st;
@@ -332,6 +353,23 @@ MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count,
     return MCS_OK;
 }
 
+MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e) {
+    if (!g || !e) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "field read-back needs a cart3d grid");
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    if (g->d_e32) {
+        std::vector<float> tmp(4 * g->nq);
+        MCS_CK(c, cudaMemcpy(tmp.data(), g->d_e32, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < g->nq; ++i)
+            for (int d = 0; d < 3; ++d) e[3 * i + d] = tmp[4 * i + d];
+    } else {
+        MCS_CK(c, cudaMemcpy(e, g->d_e64, 3 * g->nq * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return MCS_OK;
+}
+
 MCS_API int mcs_grid_zero(mcs_grid* g, int which) {
     if (!g || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
     mcs_ctx* c = g->ctx;
@@ -509,6 +547,35 @@ MCS_API int mcs_pop_init_maxwellian(mcs_pop* p, int64_t n, double mean_energy_ev
         if (int st = launch_init_maxwellian(p, n, maxwellian_sigma(mean_energy_ev))) return st;
     const long long nn = n;
     MCS_CK(c, cudaMemcpyAsync(p->d_n + p->cur, &nn, sizeof(nn), cudaMemcpyHostToDevice, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    return MCS_OK;
+}
+
+MCS_API int mcs_pop_init_cloud(mcs_pop* p, int64_t n, double cx, double cy, double cz, double sigma,
+                               double energy_ev, double wmin, double wmax) {
+    if (!p || n < 0 || !(sigma >= 0) || !(energy_ev >= 0) || !(wmin > 0) || !(wmax >= wmin)) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (n > p->cap) return set_err(c, MCS_ERR_CAPACITY, "Maximum number of particles reached");
+    if (int st = use_device(c)) return st;
+    const double ctr[3] = {cx, cy, cz};
+    if (n > 0)
+        if (int st = launch_init_cloud(p, n, ctr, sigma, sqrt(2.0 * energy_ev * kElementaryCharge / kElectronMass),
+                                       wmin, wmax))
+            return st;
+    const long long nn = n;
+    MCS_CK(c, cudaMemcpyAsync(p->d_n + p->cur, &nn, sizeof(nn), cudaMemcpyHostToDevice, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_set_efield_gaussian(mcs_grid* g, double cx, double cy, double cz, double sigma, double rho_peak,
+                                         double ebx, double eby, double ebz) {
+    if (!g || !(sigma > 0)) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "the Gaussian field needs a cart3d grid");
+    if (int st = use_device(c)) return st;
+    const double ctr[3] = {cx, cy, cz}, eb[3] = {ebx, eby, ebz};
+    if (int st = launch_efield_gaussian(g, ctr, sigma, rho_peak, eb)) return st;
     MCS_CK(c, cudaStreamSynchronize(c->stream));
     return MCS_OK;
 }

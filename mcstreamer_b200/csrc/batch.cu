@@ -843,7 +843,7 @@ const BatchVariant kVariants[] = {
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kNumVariants == MCS_BATCH_VARIANTS, "variant table and header disagree");
-constexpr int kDefaultVariant = 5;  // 256 x 2
+constexpr int kDefaultVariant = 15;  // 256 x 16 at 4 CTAs per SM (the autotuner's usual choice)
 
 template <typename P>
 int balloc(mcs_batch* b, P** p, size_t n) {

@@ -73,6 +73,7 @@ struct mcs_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     uint32_t flags = 0;
+    int mesh_shape = 0;            // kernel shape of the FP32 mesh step (MCS_OPT_MESH_SHAPE)
     uint32_t* d_status = nullptr;
     uint32_t epoch = 1;
     int num_sms = 148;

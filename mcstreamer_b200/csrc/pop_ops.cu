@@ -62,6 +62,116 @@ __global__ void k_init_maxwellian(PopView<T> P, long long n, unsigned long long 
     }
 }
 
+// Store absolute position (px, py, pz) of slot i in the population's layout: absolute, or
+// (cell, in-cell offset) on a mesh (offsets clamped below 1; outside the mesh: kOutside and
+// the position in cell units).
+template <typename T>
+__device__ __forceinline__ void put_position(const PopView<T>& P, const GridView& g, int mesh, long long i, double px,
+                                             double py, double pz) {
+    if (!mesh) {
+        P.f[0][i] = (T)px; P.f[1][i] = (T)py; P.f[2][i] = (T)pz;
+        return;
+    }
+    const double u[3] = {(px - g.x0) / g.h, (py - g.y0) / g.h, (pz - g.z0) / g.h};
+    const int nc[3] = {g.nx, g.ny, g.nz};
+    double fl[3];
+    bool in = true;
+    for (int d = 0; d < 3; ++d) {
+        fl[d] = floor(u[d]);
+        in = in && fl[d] >= 0.0 && fl[d] < (double)nc[d];
+    }
+    if (in) {
+        P.cell[i] = (uint32_t)((long long)fl[0] + (long long)g.nx * ((long long)fl[1] + (long long)g.ny * (long long)fl[2]));
+        for (int d = 0; d < 3; ++d) {
+            T r = (T)(u[d] - fl[d]);
+            if (r >= (T)1) r = sizeof(T) == 4 ? (T)0x1.fffffep-1f : (T)0x1.fffffffffffffp-1;
+            P.f[d][i] = r;
+        }
+    } else {
+        P.cell[i] = kOutside;
+        for (int d = 0; d < 3; ++d) P.f[d][i] = (T)u[d];
+    }
+}
+
+// A Gaussian cloud of electrons (the streamer workloads' initial condition): position
+// centre + N(0, sigma^2) per axis, speed sqrt(2 E / m) in an isotropic direction, weight
+// log-uniform on [wmin, wmax] (wmin when equal), s = -log(u).  Eight uniforms of the INIT
+// stream of slot i: Box-Muller on (u0,u1), (u2,u3) for the offsets, (u4,u5) direction,
+// u6 weight, u7 free flight.
+template <typename T>
+__global__ void k_init_cloud(PopView<T> P, GridView g, int mesh, long long n, unsigned long long seed, double cx,
+                             double cy, double cz, double sigma, double vabs, double wmin, double wmax) {
+    const double lw = log(wmax / wmin);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        Rng r;
+        r.init(seed, (uint32_t)i, 0u, TAG_INIT);
+        double u[8];
+        for (int q = 0; q < 8; ++q) u[q] = r.u64();
+        const double r0 = sqrt(-2.0 * log(u[0])), r1 = sqrt(-2.0 * log(u[2]));
+        double s0, c0, s1, c1;
+        sincos(6.283185307179586 * u[1], &s0, &c0);
+        sincos(6.283185307179586 * u[3], &s1, &c1);
+        put_position(P, g, mesh, i, cx + sigma * (r0 * c0), cy + sigma * (r0 * s0), cz + sigma * (r1 * c1));
+        const double uz = 2.0 * u[4] - 1.0, st = sqrt(1.0 - uz * uz);
+        double sp, cp;
+        sincos(6.283185307179586 * u[5], &sp, &cp);
+        P.f[3][i] = (T)(vabs * st * cp);
+        P.f[4][i] = (T)(vabs * st * sp);
+        P.f[5][i] = (T)(vabs * uz);
+        P.f[6][i] = (T)(wmin == wmax ? wmin : wmin * exp(lw * u[6]));
+        P.f[7][i] = (T)(-log(u[7]));
+        P.act[i] = 1;
+    }
+}
+
+int launch_init_cloud(mcs_pop* p, long long n, const double c[3], double sigma, double vabs, double wmin, double wmax) {
+    mcs_ctx* ctx = p->ctx;
+    const int gr = grid_for(ctx, n, 256);
+    const GridView gv = grid_view(p->cells);
+    const int mesh = p->cells != nullptr;
+    if (p->precision == MCS_FP32)
+        k_init_cloud<float><<<gr, 256, 0, ctx->stream>>>(pop_view<float>(p), gv, mesh, n, p->seed, c[0], c[1], c[2],
+                                                          sigma, vabs, wmin, wmax);
+    else
+        k_init_cloud<double><<<gr, 256, 0, ctx->stream>>>(pop_view<double>(p), gv, mesh, n, p->seed, c[0], c[1], c[2],
+                                                           sigma, vabs, wmin, wmax);
+    MCS_CK_LAUNCH(ctx);
+    return MCS_OK;
+}
+
+// Node field of a Gaussian charge rho = e * rho_peak * exp(-r^2 / 2 sigma^2) at c plus a
+// uniform background: E = e_bg + Q(r) / (4 pi eps0 r^2) r_hat with
+// Q(r) = e rho_peak (2 pi sigma^2)^(3/2) [erf(r / (sqrt2 sigma)) - sqrt(2/pi) (r/sigma) exp(-r^2/2sigma^2)]
+// (Gauss's law for the spherical charge).  FP64 arithmetic; stored as the grid's precision.
+__global__ void k_efield_gaussian(GridView g, float4* e32, double* e64, double cx, double cy, double cz, double sigma,
+                                  double q0, double ebx, double eby, double ebz) {
+    const long long nx1 = g.nx + 1, ny1 = g.ny + 1;
+    const long long nn = nx1 * ny1 * (long long)(g.nz + 1);
+    const double k4pe = 4.0 * 3.141592653589793 * 8.854187817620389e-12;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nn; q += (long long)gridDim.x * blockDim.x) {
+        const long long i = q % nx1, j = (q / nx1) % ny1, k = q / (nx1 * ny1);
+        const double dx = (g.x0 + g.h * (double)i) - cx, dy = (g.y0 + g.h * (double)j) - cy,
+                     dz = (g.z0 + g.h * (double)k) - cz;
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double rs = r / sigma;
+        const double Q = q0 * (erf(rs / 1.4142135623730951) - 0.7978845608028654 * rs * exp(-0.5 * rs * rs));
+        const double f = r > 0.0 ? Q / (k4pe * (r * r * r)) : 0.0;
+        const double ex = ebx + f * dx, ey = eby + f * dy, ez = ebz + f * dz;
+        if (e32) e32[q] = make_float4((float)ex, (float)ey, (float)ez, 0.0f);
+        else { e64[3 * q] = ex; e64[3 * q + 1] = ey; e64[3 * q + 2] = ez; }
+    }
+}
+
+int launch_efield_gaussian(mcs_grid* g, const double c[3], double sigma, double rho_peak, const double eb[3]) {
+    mcs_ctx* ctx = g->ctx;
+    const double q0 = kElementaryCharge * rho_peak * pow(2.0 * 3.141592653589793 * sigma * sigma, 1.5);
+    const int gr = grid_for(ctx, (long long)g->nq, 256);
+    k_efield_gaussian<<<gr, 256, 0, ctx->stream>>>(g->v, reinterpret_cast<float4*>(g->d_e32), g->d_e64, c[0], c[1],
+                                                    c[2], sigma, q0, eb[0], eb[1], eb[2]);
+    MCS_CK_LAUNCH(ctx);
+    return MCS_OK;
+}
+
 int launch_init_maxwellian(mcs_pop* p, long long n, double sigma) {
     mcs_ctx* c = p->ctx;
     const int gr = grid_for(c, n, 256);

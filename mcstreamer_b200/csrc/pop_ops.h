@@ -16,6 +16,8 @@ int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* 
 int launch_download(mcs_pop* p, double* dx, double* dv, double* dw, double* ds, uint8_t* da);
 int grid_for(mcs_ctx* c, long long n, int block);
 int launch_init_maxwellian(mcs_pop* p, long long n, double sigma);
+int launch_init_cloud(mcs_pop* p, long long n, const double c[3], double sigma, double vabs, double wmin, double wmax);
+int launch_efield_gaussian(mcs_grid* g, const double c[3], double sigma, double rho_peak, const double eb[3]);
 // Standard deviation of each velocity component of a Maxwellian with mean energy mean_ev.
 inline double maxwellian_sigma(double mean_ev) {
     return sqrt((2.0 / 3.0) * mean_ev * kElementaryCharge / kElectronMass);
@@ -24,5 +26,7 @@ int map_status(uint32_t st);
 const char* status_text(int code);
 // Wait for the context's stream and turn the sticky device status into an error code.
 int sync_status(mcs_ctx* c);
+// (threads per block, particles per thread, CTAs per SM) of an FP32 mesh-step shape.
+int mesh_shape_info(int shape, int* block, int* ppt, int* minb);
 constexpr int kMomentPartialsMin = 148 * 2 * (MCS_MOMENTS_BASE + kMaxRows);
 }  // namespace mcs

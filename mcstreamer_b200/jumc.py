@@ -163,6 +163,12 @@ class Population:
         """n swarm electrons drawn on the device (origin, weight 1, isotropic Maxwellian)."""
         self.ctx.check(self.ctx.lib.mcs_pop_init_maxwellian(self.h, int(n), float(mean_ev)))
 
+    def init_cloud(self, n: int, centre, sigma: float, energy_ev: float, wmin: float, wmax: float) -> None:
+        """n electrons of a Gaussian cloud drawn on the device (mcs_pop_init_cloud); unsorted."""
+        cx, cy, cz = map(float, centre)
+        self.ctx.check(self.ctx.lib.mcs_pop_init_cloud(self.h, int(n), cx, cy, cz, float(sigma), float(energy_ev),
+                                                       float(wmin), float(wmax)))
+
     def upload(self, p: ParticleArrays) -> None:
         x = np.ascontiguousarray(p.x, dtype=np.float64)
         v = np.ascontiguousarray(p.v, dtype=np.float64)

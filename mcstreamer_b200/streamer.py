@@ -76,6 +76,17 @@ class Grid3D:
             self.ctx.check(self.ctx.lib.mcs_grid_set_efield_range(self.h_, k0 * plane, (k1 - k0) * plane,
                                                                   L.dptr(e)))
 
+    def set_efield_gaussian(self, centre: Sequence[float], sigma: float, rho_peak_e: float,
+                            e_bg: Sequence[float] = (0.0, 0.0, 0.0)) -> None:
+        """The field of gaussian_charge_field(centre, sigma, rho_peak_e, e_bg), computed on the device."""
+        self.ctx.check(self.ctx.lib.mcs_grid_set_efield_gaussian(self.h_, *map(float, centre), float(sigma),
+                                                                 float(rho_peak_e), *map(float, e_bg)))
+
+    def read_efield(self) -> np.ndarray:
+        out = np.zeros((self.nnodes, 3))
+        self.ctx.check(self.ctx.lib.mcs_grid_read_efield(self.h_, L.dptr(out)))
+        return out
+
     def zero(self, which: int = L.Q_PART) -> None:
         self.ctx.check(self.ctx.lib.mcs_grid_zero(self.h_, which))
 
