@@ -240,6 +240,8 @@ MCS_API int mcs_grid_create_cart3d(mcs_ctx* c, int nx, int ny, int nz, double h,
     GridView& v = g->v;
     v.type = GRID_CART3D;
     v.nx = nx; v.ny = ny; v.nz = nz;
+    v.dnx = make_fastdiv((uint32_t)nx);
+    v.dny = make_fastdiv((uint32_t)ny);
     v.h = h; v.inv_h = 1.0 / h; v.x0 = x0; v.y0 = y0; v.z0 = z0;
     const size_t nodes = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
     g->nq = nodes;

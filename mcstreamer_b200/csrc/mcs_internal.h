@@ -28,9 +28,33 @@ struct TableView {
     double param[kMaxRows];
 };
 
+// Unsigned 32-bit division by an invariant divisor with one multiply-high (Granlund &
+// Montgomery, "Division by invariant integers using multiplication", PLDI 1994, fig. 4.1):
+// q = (t + ((n - t) >> s1)) >> s2 with t = umulhi(m, n), exact for every n < 2^32.
+struct FastDiv {
+    uint32_t d, m, s1, s2;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+    int l = 0;
+    while (l < 32 && (1ull << l) < d) ++l;   // ceil(log2 d)
+    FastDiv f;
+    f.d = d;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d + 1) & 0xffffffffull);
+    f.s1 = l < 1 ? (uint32_t)l : 1u;
+    f.s2 = l > 1 ? (uint32_t)(l - 1) : 0u;
+    return f;
+}
+#ifdef __CUDACC__
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, const FastDiv& f) {
+    const uint32_t t = __umulhi(f.m, n);
+    return (t + ((n - t) >> f.s1)) >> f.s2;
+}
+#endif
+
 struct GridView {
     int type;               // 0 none, GRID_CART3D, GRID_CYL
     int nx, ny, nz;         // cart3d cells
+    FastDiv dnx, dny;       // division by nx, ny (cell index -> ix, iy, iz)
     double h, inv_h, x0, y0, z0;
     const float* e32;       // cart3d node field, 4 floats per node (Ex,Ey,Ez,0)
     const double* e64;      // cart3d node field, 3 doubles per node
@@ -40,6 +64,16 @@ struct GridView {
     long long* qfixed;      // tracker deposits (int64, 2^-32 e)
     long long* qpart;       // particle deposits
 };
+
+#ifdef __CUDACC__
+// Linear cell index -> (ix, iy, iz), x fastest.
+__device__ __forceinline__ void cell_split(const GridView& g, uint32_t cell, uint32_t& ix, uint32_t& iy, uint32_t& iz) {
+    const uint32_t r = fast_div(cell, g.dnx);
+    ix = cell - r * (uint32_t)g.nx;
+    iz = fast_div(r, g.dny);
+    iy = r - iz * (uint32_t)g.ny;
+}
+#endif
 
 template <typename T>
 struct PopView {

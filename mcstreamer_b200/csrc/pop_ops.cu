@@ -194,8 +194,8 @@ __device__ __forceinline__ void abs_position(const PopView<T>& P, const GridView
         z = g.z0 + g.h * (double)P.f[2][i];
         return;
     }
-    const uint32_t ix = c % (uint32_t)g.nx, r = c / (uint32_t)g.nx;
-    const uint32_t iy = r % (uint32_t)g.ny, iz = r / (uint32_t)g.ny;
+    uint32_t ix, iy, iz;
+    cell_split(g, c, ix, iy, iz);
     x = g.x0 + g.h * ((double)ix + (double)P.f[0][i]);
     y = g.y0 + g.h * ((double)iy + (double)P.f[1][i]);
     z = g.z0 + g.h * ((double)iz + (double)P.f[2][i]);
@@ -582,10 +582,11 @@ __global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long l
                 cidx = P.cell[i];
                 if (cidx != kOutside) {
                     valid = true;
-                    ix = (int)(cidx % (uint32_t)g.nx);
-                    const uint32_t r = cidx / (uint32_t)g.nx;
-                    iy = (int)(r % (uint32_t)g.ny);
-                    iz = (int)(r / (uint32_t)g.ny);
+                    uint32_t ux, uy, uz;
+                    cell_split(g, cidx, ux, uy, uz);
+                    ix = (int)ux;
+                    iy = (int)uy;
+                    iz = (int)uz;
                     fx = (double)P.f[0][i]; fy = (double)P.f[1][i]; fz = (double)P.f[2][i];
                     charge = (double)P.f[6][i] * val;
                 }

@@ -542,10 +542,11 @@ __device__ __forceinline__ void mesh_abs(const GridView& g, uint32_t cell, doubl
                                          double& y, double& z) {
     double cx = 0.0, cy = 0.0, cz = 0.0;
     if (cell != kOutsideCell) {
-        cx = (double)(cell % (uint32_t)g.nx);
-        const uint32_t r = cell / (uint32_t)g.nx;
-        cy = (double)(r % (uint32_t)g.ny);
-        cz = (double)(r / (uint32_t)g.ny);
+        uint32_t ux, uy, uz;
+        cell_split(g, cell, ux, uy, uz);
+        cx = (double)ux;
+        cy = (double)uy;
+        cz = (double)uz;
     }
     x = g.x0 + g.h * (cx + ox);
     y = g.y0 + g.h * (cy + oy);
@@ -653,10 +654,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 s = (double)P.f[7][i];
                 in = cell0 != kOutsideCell;
                 if (in) {
-                    ix = (int)(cell0 % (uint32_t)g.nx);
-                    const uint32_t r = cell0 / (uint32_t)g.nx;
-                    iy = (int)(r % (uint32_t)g.ny);
-                    iz = (int)(r / (uint32_t)g.ny);
+                    uint32_t ux, uy, uz;
+                    cell_split(g, cell0, ux, uy, uz);
+                    ix = (int)ux;
+                    iy = (int)uy;
+                    iz = (int)uz;
                     load_cell_field(g, ix, iy, iz, cf);
                 } else {
                     cf.zero();
@@ -724,10 +726,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                     cl = P.cell[j];
                     if (cl != kOutsideCell) {
                         valid = true;
-                        dx = (int)(cl % (uint32_t)g.nx);
-                        const uint32_t r = cl / (uint32_t)g.nx;
-                        dy = (int)(r % (uint32_t)g.ny);
-                        dz = (int)(r / (uint32_t)g.ny);
+                        uint32_t ux, uy, uz;
+                        cell_split(g, cl, ux, uy, uz);
+                        dx = (int)ux;
+                        dy = (int)uy;
+                        dz = (int)uz;
                         fx = (double)P.f[0][j]; fy = (double)P.f[1][j]; fz = (double)P.f[2][j];
                         ch = (double)P.f[6][j] * dep_val;
                     }
@@ -748,9 +751,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
                 const uint32_t cl = sg.cell[e];
                 if (!sg.act[e] || cl == kOutsideCell) continue;
-                const int ex = (int)(cl % (uint32_t)g.nx);
-                const uint32_t r = cl / (uint32_t)g.nx;
-                cic_fixed(g.qpart, g.nx, g.ny, ex, (int)(r % (uint32_t)g.ny), (int)(r / (uint32_t)g.ny),
+                uint32_t ux, uy, uz;
+                cell_split(g, cl, ux, uy, uz);
+                cic_fixed(g.qpart, g.nx, g.ny, (int)ux, (int)uy, (int)uz,
                           (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], (double)sg.f[6][e] * dep_val);
             }
         }
