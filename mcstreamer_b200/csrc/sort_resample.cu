@@ -15,6 +15,8 @@
 // a scan of the counts gives each cell its place -- writing them.  Clones are appended in
 // cell order, which is the slot order of the sorted population (the serial reference's
 // append order).  Uniforms: one Philox stream per cell, ctr = {cell, call, k/4, tag}.
+#include <algorithm>
+
 #include "host_util.h"
 #include "pop_ops.h"
 #include "step.cuh"
@@ -267,20 +269,178 @@ __device__ uint32_t resample_segment(const ResampleArgs& a, PopView<T>& P, long 
     return ncl;
 }
 
+// ---------------------------------------------------------------------------------------
+// Warp per segment.  The decisions are those of resample_segment; the work is spread so
+// that the warp's memory accesses are coalesced:
+//  * split cells (p < ntarget): the first ntarget - p particles with w > 2, in index order,
+//    split -- a ballot rank over the cell's particles (no arithmetic order involved);
+//  * merge cells (p > nmax): the serial pass (FP64 weight sums in index order, the clone
+//    positions x) runs on lane 0 over the cell's weights staged in shared memory, and
+//    records the clone sources; the warp then writes the clones to consecutive slots and
+//    removes the originals.
+// ---------------------------------------------------------------------------------------
+constexpr int RS_WARPS = 8;       // warps per block
+constexpr int RS_BUF = 256;       // staged weights per warp (a cell is streamed in chunks)
+constexpr int RS_SRC = 128;       // clone sources a merge can record (ntarget above: serial path)
+
+struct RsShared {
+    double w[RS_WARPS][RS_BUF];
+    uint32_t src[RS_WARPS][RS_SRC];
+};
+
+// End of segment s (exclusive): the next segment's start, or for the last segment the first
+// slot whose key differs (found 32 slots at a time).
+__device__ __forceinline__ long long segment_end(const ResampleArgs& a, long long s, long long nseg, long long b,
+                                                 uint32_t cell) {
+    if (s + 1 < nseg) return (long long)a.start[s + 1];
+    const long long n = *a.n;
+    const int lane = threadIdx.x & 31;
+    for (long long j0 = b; j0 < n; j0 += 32) {
+        const long long j = j0 + lane;
+        const unsigned diff = __ballot_sync(0xffffffffu, j < n && a.key[j] != cell);
+        const unsigned past = __ballot_sync(0xffffffffu, j >= n);
+        const unsigned stop = diff | past;
+        if (stop) return j0 + __ffs(stop) - 1;
+    }
+    return n;
+}
+
 template <typename T>
-__global__ void k_resample_count(ResampleArgs a, PopView<T> P, uint32_t* __restrict__ counts, uint32_t* status) {
+__device__ __forceinline__ void copy_clone(PopView<T>& P, long long d, long long j, T w) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) P.f[q][d] = P.f[q][j];
+    if (P.cell) P.cell[d] = P.cell[j];
+    P.act[d] = 1;
+    P.f[6][d] = w;
+}
+
+// Returns the number of clones of segment s (the same on every lane).
+template <typename T, bool WRITE>
+__device__ uint32_t resample_segment_warp(const ResampleArgs& a, PopView<T>& P, long long s, long long nseg,
+                                          long long clone_base, long long cap, uint32_t* status, RsShared& sh,
+                                          int wid) {
+    const int lane = threadIdx.x & 31;
+    const long long b = a.start[s];
+    const uint32_t cell = a.key[b];
+    const long long e = segment_end(a, s, nseg, b, cell);
+    const long long p0 = e - b;
+    // (the host takes the serial form when ntarget > nmax or ntarget > RS_SRC)
+    if (p0 < a.ntarget) {
+        // split: rank the particles with w > 2 in index order
+        const uint32_t K = (uint32_t)(a.ntarget - p0);
+        uint32_t ranked = 0;
+        for (long long j0 = b; j0 < e && ranked < K; j0 += 32) {
+            const long long j = j0 + lane;
+            double wj = 0.0;
+            bool q = false;
+            if (j < e) {
+                wj = (double)P.f[6][j];
+                q = wj > 2;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, q);
+            const uint32_t r = ranked + __popc(bal & ((1u << lane) - 1u));
+            if (WRITE && q && r < K) {
+                const double wnew = rint(wj / 2.0);   // Julia round: nearest, ties to even
+                const long long d = clone_base + r;
+                if (d < cap) copy_clone<T>(P, d, j, (T)wnew);
+                else atomicOr(status, ST_CAPACITY);
+                P.f[6][j] = (T)(wj - wnew);
+            }
+            ranked += __popc(bal);
+        }
+        return ranked < K ? ranked : K;
+    }
+    if (p0 <= a.nmax) return 0;
+    // merge: pass 1 and pass 2 on lane 0 over staged weights
+    double* wb = sh.w[wid];
+    uint32_t* src = sh.src[wid];
+    Rng rng;
+    rng.init(a.seed, cell, a.call, TAG_CELL_RESAMPLE);
+    double wtotal = 0.0, x = 0.0;
+    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
+        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
+        __syncwarp();
+        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
+        __syncwarp();
+        if (lane == 0) {
+            for (int q = 0; q < m; ++q) {
+                wtotal += wb[q];
+                if (c0 - b + q + 1 == a.nmax) x = 1.0 - pow(1.0 - rng.u64(), 1.0 / (double)a.ntarget);
+            }
+        }
+    }
+    uint32_t ncl = 0;
+    long long pk = 0;
+    double wcum = 0.0;
+    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
+        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
+        __syncwarp();
+        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
+        __syncwarp();
+        if (lane == 0) {
+            for (int q = 0; q < m; ++q) {
+                const double wj = wb[q];
+                while (wtotal * x < wcum + wj && pk < a.ntarget) {
+                    pk += 1;
+                    src[ncl++] = (uint32_t)(c0 - b + q);
+                    if (pk < a.ntarget) x += (1.0 - pow(1.0 - rng.u64(), 1.0 / (double)(a.ntarget - pk))) * (1.0 - x);
+                }
+                wcum += wj;
+            }
+        }
+    }
+    __syncwarp();
+    ncl = __shfl_sync(0xffffffffu, ncl, 0);
+    if (WRITE) {
+        wtotal = __shfl_sync(0xffffffffu, wtotal, 0);
+        const T wc = (T)(wtotal / (double)a.ntarget);
+        for (uint32_t k = lane; k < ncl; k += 32) {
+            const long long d = clone_base + k;
+            if (d < cap) copy_clone<T>(P, d, b + src[k], wc);
+            else atomicOr(status, ST_CAPACITY);
+        }
+        for (long long j = b + lane; j < e; j += 32) P.act[j] = 0;   // remove_particle!
+    }
+    return ncl;
+}
+
+// Counting is latency-bound over millions of small segments: a thread per segment keeps 32
+// segments' loads in flight per warp.
+template <typename T>
+__global__ void __launch_bounds__(128) k_resample_count(ResampleArgs a, PopView<T> P, uint32_t* __restrict__ counts,
+                                                        uint32_t* status) {
     const long long nseg = *a.nseg;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x)
         counts[s] = resample_segment<T, false>(a, P, s, 0, 0, status);
 }
 
+// The serial form, a thread per segment: for ntarget > nmax or ntarget > RS_SRC.
 template <typename T>
-__global__ void k_resample_write(ResampleArgs a, PopView<T> P, const uint32_t* __restrict__ offs,
-                                 const long long* total, uint32_t* status) {
+__global__ void __launch_bounds__(128) k_resample_write_serial(ResampleArgs a, PopView<T> P,
+                                                               const uint32_t* __restrict__ offs,
+                                                               const long long* total, uint32_t* status) {
     const long long nseg = *a.nseg;
     const long long n = *a.n;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x)
         resample_segment<T, true>(a, P, s, n + (long long)offs[s], P.cap, status);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        long long m = n + *total;
+        if (m > P.cap) { m = P.cap; atomicOr(status, ST_CAPACITY); }
+        *P.n_out = m;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_write(ResampleArgs a, PopView<T> P,
+                                                                   const uint32_t* __restrict__ offs,
+                                                                   const long long* total, uint32_t* status) {
+    __shared__ RsShared sh;
+    const long long nseg = *a.nseg;
+    const long long n = *a.n;
+    const int wid = threadIdx.x >> 5;
+    const long long w0 = (long long)blockIdx.x * RS_WARPS + wid, ws = (long long)gridDim.x * RS_WARPS;
+    for (long long s = w0; s < nseg; s += ws)
+        resample_segment_warp<T, true>(a, P, s, nseg, n + (long long)offs[s], P.cap, status, sh, wid);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         long long m = n + *total;
         if (m > P.cap) { m = P.cap; atomicOr(status, ST_CAPACITY); }
@@ -379,7 +539,14 @@ int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
     MCS_CK_LAUNCH(c);
     if (int st = launch_scan(p, p->seg_a, p->seg_b, nseg, total)) return st;
     PopView<T> P = pop_view<T>(p);
-    k_resample_write<T><<<gr, 128, 0, c->stream>>>(a, P, p->seg_b, total, c->d_status);
+    if (ntarget > nmax || ntarget > RS_SRC) {
+        k_resample_write_serial<T><<<gr, 128, 0, c->stream>>>(a, P, p->seg_b, total, c->d_status);
+    } else {
+        int occ = 0;   // the warp-per-segment write pass: all blocks resident, grid-stride over segments
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_resample_write<T>, RS_WARPS * 32, 0);
+        k_resample_write<T><<<std::max(occ, 1) * c->num_sms, RS_WARPS * 32, 0, c->stream>>>(a, P, p->seg_b, total,
+                                                                                              c->d_status);
+    }
     MCS_CK_LAUNCH(c);
     p->cur ^= 1;
     return MCS_OK;

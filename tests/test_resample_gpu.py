@@ -54,7 +54,7 @@ def test_sort_is_stable_by_cell(ctx, mesh):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ntarget,nmax", [(10, 15), (64, 96)])
+@pytest.mark.parametrize("ntarget,nmax", [(10, 15), (64, 96), (20, 15), (200, 300)])
 def test_resample_cells_matches_oracle(ctx, ntarget, nmax):
     n = 150_000
     tab, grid, p0, pop, ofield = _setup(ctx, n, mesh=False)
@@ -69,13 +69,17 @@ def test_resample_cells_matches_oracle(ctx, ntarget, nmax):
     np.testing.assert_array_equal(g.active, o.active)
     np.testing.assert_array_equal(g.x, o.x)
     np.testing.assert_allclose(g.w, o.w, rtol=1e-12)
-    # resample! conserves the total weight (main.jl:303-304 asserts rtol 1e-5)
+    # resample! conserves the total weight (main.jl:303-304 asserts rtol 1e-5) when
+    # ntarget <= nmax; with ntarget > nmax a cell that splits past nmax falls into the
+    # merge branch with x = 0 (resample.jl:31-76), in the reference as here
     w1 = g.w[g.active == 1].sum()
-    assert w1 == pytest.approx(w0, rel=1e-9)
+    if ntarget <= nmax:
+        assert w1 == pytest.approx(w0, rel=1e-9)
     # overfull cells are left with at most ntarget equal-weight particles
     keys = grid.cell_key(g.x[g.active == 1])
     _, counts = np.unique(keys[keys < np.iinfo(np.int64).max], return_counts=True)
-    assert counts.max() <= max(ntarget, nmax)
+    if ntarget <= nmax:
+        assert counts.max() <= max(ntarget, nmax)
     pop.close(); grid.close(); tab.close()
 
 
