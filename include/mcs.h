@@ -202,6 +202,20 @@ MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, doub
  * into MCS_Q_PART. */
 MCS_API int mcs_advance_deposit(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt,
                                 mcs_grid* tracker, mcs_grid* deposit, double val);
+/* advance!(popl, efield, dt, tracker) + density!(deposit, val) for a population that lives
+ * in HOST memory in the Julia layout (x, v as interleaved triples; capacity slots each): the
+ * particles [0, *n) are stepped and written back in place, the secondaries appended after
+ * them in parent order, *n updated.  The population is cut into `chunks` pieces whose
+ * uploads, fused mesh steps and downloads are pipelined over three streams; the result is
+ * the same as mcs_pop_upload + mcs_advance_deposit + mcs_pop_download (random streams keyed
+ * by global slot, int64 deposits), except that no per-step sums are logged.  p is device
+ * workspace for one chunk and its secondaries (capacity >= ceil(n / chunks) plus room); it
+ * keeps its staging buffers between calls.  The caller zeroes the deposit grid.  Pinned host
+ * memory lets the transfers overlap. */
+MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt,
+                                     mcs_grid* tracker, mcs_grid* deposit, double val, double* x, double* v,
+                                     double* w, double* s, uint8_t* active, int64_t* n, int64_t capacity,
+                                     int chunks);
 /* collisions!(mpopl, dt, tracker) (JuMC/src/mixed_population.jl:61-77). */
 MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* tracker);
 /* density!(grid, arr, mpopl, Electron, fields, val) (MCStreamer/src/poisson.jl:65-84)

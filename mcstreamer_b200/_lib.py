@@ -73,6 +73,7 @@ SIGNATURES = {
     "mcs_pop_copy": (i32, [vp, vp]),
     "mcs_advance": (i32, [vp, vp, vp, f64, vp]),
     "mcs_advance_deposit": (i32, [vp, vp, vp, f64, vp, vp, f64]),
+    "mcs_advance_deposit_host": (i32, [vp, vp, vp, f64, vp, vp, f64, pd, pd, pd, pd, pu8, pi64, i64, i32]),
     "mcs_collisions": (i32, [vp, vp, f64, vp]),
     "mcs_deposit": (i32, [vp, vp, f64]),
     "mcs_repack": (i32, [vp]),

@@ -494,6 +494,7 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage); cudaFree(p->d_log);
     for (int q = 0; q < 2; ++q) { cudaFree(p->sort_key[q]); cudaFree(p->sort_val[q]); }
     cudaFree(p->sort_hist); cudaFree(p->sort_hoff); cudaFree(p->seg_a); cudaFree(p->seg_b);
+    free_host_step(p->host_step);
     delete p;
     return MCS_OK;
 }

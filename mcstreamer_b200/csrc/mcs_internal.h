@@ -97,6 +97,7 @@ struct StepCtl {
     char* stage;              // per-CTA secondary staging, stage_stride bytes per CTA
     unsigned long long stage_stride;
     uint32_t stage_cap;       // entries per CTA
+    uint32_t slot_base;       // added to the slot index that keys a particle's random stream
 };
 
 }  // namespace mcs
@@ -140,12 +141,16 @@ struct mcs_field {
     mcs_grid* grid = nullptr;
 };
 
+namespace mcs { struct HostStepBuffers; void free_host_step(HostStepBuffers*); }
+
 struct mcs_pop {
+    mcs::HostStepBuffers* host_step = nullptr;   // cached workspace of mcs_advance_deposit_host
     mcs_ctx* ctx = nullptr;
     int precision = MCS_FP64;
     mcs_grid* cells = nullptr;     // mesh layout when non-null
     long long cap = 0;
     size_t esz = 8;                // bytes per float field
+    uint32_t slot_base = 0;        // stream slot of slot 0 (a chunk of a larger population)
     void* f[8] = {};
     uint32_t* cell = nullptr;
     uint8_t* act = nullptr;

@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
             uint32_t ev = 0;
             if (i < n_entry && P.act[i]) {
                 Event rng;
-                rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
                 T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                 T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
                 const T w = P.f[6][i];
@@ -403,7 +403,7 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
                 double s = (double)P.f[7][i] - C.dt * tab.maxrate;
                 if (s <= 0) {
                     Event rng;
-                    rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                    rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
                     const T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                     T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
                     const T w = P.f[6][i];
@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 if (q >= tile_n || !P.act[base + q]) { sh.cnt[q] = 0; continue; }
                 local = q;
                 i = base + q;
-                rng.init(C.seed, (uint32_t)i, C.step, C.tag);
+                rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
                 const uint32_t cell0 = P.cell[i];
                 ox = P.f[0][i]; oy = P.f[1][i]; oz = P.f[2][i];
                 vx = P.f[3][i]; vy = P.f[4][i]; vz = P.f[5][i];

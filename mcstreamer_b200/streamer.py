@@ -18,7 +18,7 @@ from scipy.special import erf
 
 from . import _lib as L
 from . import constants as co
-from .jumc import Context, Population
+from .jumc import ParticleArrays, Context, Population
 
 
 class DeviceArray:
@@ -184,6 +184,19 @@ def advance_deposit(popl: Population, efield: FieldInterp, dt: float, tracker: O
     popl.ctx.check(popl.ctx.lib.mcs_advance_deposit(popl.h, popl.collisions.h, efield.h, dt,
                                                     tracker.h if tracker is not None else None, grid.h_,
                                                     float(val)))
+
+
+def advance_deposit_host(work: Population, efield: FieldInterp, dt: float, tracker: Optional[CollisionTracker],
+                         grid: Grid3D, host: ParticleArrays, n: int, val: float = -1.0, chunks: int = 4) -> int:
+    """advance_deposit of a host-resident population (arrays of `host`, capacity len(host.w),
+    first n in use): stepped and written back in place with the transfers pipelined over
+    `chunks` pieces; `work` is the device workspace.  Returns the new particle count."""
+    nn = C.c_int64(int(n))
+    work.ctx.check(work.ctx.lib.mcs_advance_deposit_host(
+        work.h, work.collisions.h, efield.h, dt, tracker.h if tracker is not None else None, grid.h_, float(val),
+        L.dptr(host.x), L.dptr(host.v), L.dptr(host.w), L.dptr(host.s), L.u8ptr(host.active), C.byref(nn),
+        len(host.w), int(chunks)))
+    return nn.value
 
 
 # ---------------------------------------------------------------------------------------

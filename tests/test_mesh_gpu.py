@@ -127,3 +127,38 @@ def test_mesh_particles_leaving_and_reentering(ctx):
     bad = particle_mismatch(g, o, 1e-11, xatol=1e-30, vatol=1e-30)
     assert bad.sum() <= 2, f"{bad.sum()} slots differ"
     _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("chunks", [1, 3, 7])
+def test_host_resident_step_equals_device_step(ctx, chunks):
+    """mcs_advance_deposit_host (chunked, pipelined transfers) against upload + fused step +
+    download of the same population: the same particles in the same slots, the same
+    secondaries in the same order, the same int64 charges."""
+    n = 40000
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32", emax_ev=200.0)
+    host_in = pop.download()                     # the cloud as the device layout holds it
+    fld = streamer.FieldInterp(grid)
+    trk = streamer.CollisionTracker(grid)
+    dt = 2e-13
+    grid.zero(L.Q_FIXED); grid.zero(L.Q_PART)
+    streamer.advance_deposit(pop, fld, dt, trk, grid, -1.0)
+    ref = pop.download()
+    q_ref = (grid.read_fixed(L.Q_FIXED), grid.read_fixed(L.Q_PART))
+    assert ref.n > n                            # the step made secondaries
+    cap = 2 * n
+    host = jumc.ParticleArrays.empty(cap)
+    host.x[:n], host.v[:n], host.w[:n], host.s[:n], host.active[:n] = (host_in.x, host_in.v, host_in.w, host_in.s,
+                                                                       host_in.active)
+    work = jumc.Population((n + chunks - 1) // chunks + n // 2, None, tab, precision="fp32", seed=21, mesh=grid)
+    grid.zero(L.Q_FIXED); grid.zero(L.Q_PART)
+    m = streamer.advance_deposit_host(work, fld, dt, trk, grid, host, n, -1.0, chunks=chunks)
+    assert m == ref.n
+    np.testing.assert_array_equal(host.x[:m], ref.x)
+    np.testing.assert_array_equal(host.v[:m], ref.v)
+    np.testing.assert_array_equal(host.w[:m], ref.w)
+    np.testing.assert_array_equal(host.s[:m], ref.s)
+    np.testing.assert_array_equal(host.active[:m], ref.active)
+    np.testing.assert_array_equal(grid.read_fixed(L.Q_FIXED), q_ref[0])
+    np.testing.assert_array_equal(grid.read_fixed(L.Q_PART), q_ref[1])
+    _close(work, pop, grid, tab)
