@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--workload", default="cfg1")
     ap.add_argument("--particles", type=int, default=None, help="override the particle count (per rank)")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-chunks", type=int, default=8, help="chunks of the pipelined host-resident step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="cfg4: arrival window (s)")
@@ -360,7 +361,7 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
     from mcstreamer_b200 import dist as mdist
     from mcstreamer_b200 import jumc
 
-    chunks = 8
+    chunks = max(1, args.e2e_chunks)
     n = parts.n
     cap = 2 * n
     nodes = spec.nodes
@@ -415,9 +416,9 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
         active = float(a[0])
     return {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // args.e2e_steps,
             "d2h_bytes_per_step": d2h // args.e2e_steps, "steps": args.e2e_steps,
-            "path": "mcs_advance_deposit_host on pinned host arrays in the Julia layout (8 chunks: uploads, fused "
-                    "steps and downloads pipelined on three streams) + mcs_grid_read_fixed; CUDA events around "
-                    "each step, the restore of the input cloud outside them"}
+            "path": f"mcs_advance_deposit_host on pinned host arrays in the Julia layout ({chunks} chunks: uploads, "
+                    "fused steps and downloads pipelined on three streams) + mcs_grid_read_fixed; CUDA events "
+                    "around each step, the restore of the input cloud outside them"}
 
 
 # ---------------------------------------------------------------------------------------
