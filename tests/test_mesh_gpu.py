@@ -162,3 +162,33 @@ def test_host_resident_step_equals_device_step(ctx, chunks):
     np.testing.assert_array_equal(grid.read_fixed(L.Q_FIXED), q_ref[0])
     np.testing.assert_array_equal(grid.read_fixed(L.Q_PART), q_ref[1])
     _close(work, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_every_mesh_kernel_shape_gives_the_same_step(ctx):
+    """MCS_OPT_MESH_SHAPE changes block size, tile length and register budget of the FP32 mesh
+    step, never its result: particles, secondaries and charges are bit-identical."""
+    n = 30000
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32", emax_ev=200.0)
+    snap = jumc.Population(3 * n, None, tab, precision="fp32", seed=21, mesh=grid)
+    ctx.check(ctx.lib.mcs_pop_copy(snap.h, pop.h))
+    fld = streamer.FieldInterp(grid)
+    trk = streamer.CollisionTracker(grid)
+    ref = None
+    try:
+        for shape in range(L.MESH_SHAPES):
+            ctx.check(ctx.lib.mcs_ctx_set_option(ctx.h, L.OPT_MESH_SHAPE, shape))
+            ctx.check(ctx.lib.mcs_pop_copy(pop.h, snap.h))
+            ctx.check(ctx.lib.mcs_pop_set_seed(pop.h, 21, 0))
+            grid.zero(L.Q_FIXED); grid.zero(L.Q_PART)
+            streamer.advance_deposit(pop, fld, 2e-13, trk, grid, -1.0)
+            g = pop.download()
+            got = (g.x.tobytes(), g.v.tobytes(), g.w.tobytes(), g.s.tobytes(), g.active.tobytes(),
+                   grid.read_fixed(L.Q_FIXED).tobytes(), grid.read_fixed(L.Q_PART).tobytes())
+            if ref is None:
+                ref = got
+                assert g.n > n
+            assert got == ref, f"shape {shape} differs"
+    finally:
+        ctx.check(ctx.lib.mcs_ctx_set_option(ctx.h, L.OPT_MESH_SHAPE, 0))
+    _close(snap, pop, grid, tab)
