@@ -580,6 +580,15 @@ def batch_cpu_sample(spec, seconds: float, threads: int) -> dict:
                       f"{done_e:.3g} electron steps in {t_used:.1f} s, scaled to {spec.k} solves x {spec.steps} steps"}
 
 
+def _variant_int(fn: str, v: int) -> int:
+    import ctypes as C
+
+    from mcstreamer_b200 import _lib as L
+    out = C.c_int(0)
+    L.check(getattr(L.lib(), fn)(int(v), C.byref(out)))
+    return out.value
+
+
 def run_batch(args):
     import torch
 
@@ -722,6 +731,8 @@ def run_batch(args):
             "solve_time_s": spec.steps * step_ms * 1e-3,
             "electron_steps_per_s": e_steps,
             "autotune": {"variant": chosen, "block": shape[0], "particles_per_thread": shape[1],
+                         "ctas_per_sm_bound": _variant_int("mcs_batch_variant_min_blocks", chosen),
+                         "refill_idle_lanes": _variant_int("mcs_batch_variant_refill", chosen),
                          "trial_ms": [round(float(t), 4) for t in times]},
             "l2": "inputs larger than L2 (44.6M electrons x 33 B = 1.5 GB resident)",
             "plain_drop_in": {

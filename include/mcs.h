@@ -281,7 +281,7 @@ MCS_API int mcs_pop_read_step_log(mcs_pop* p, double* out, int nsteps);
  * (MCS_BATCH_MOMENTS doubles: the MCS_STEP_MOMENTS sums, then the sum over actives of the
  * rate of the table's first ionization row and of its square) stay on the device in a
  * ring of MCS_BATCH_LOG steps. */
-enum { MCS_BATCH_MOMENTS = 14, MCS_BATCH_LOG = 64, MCS_BATCH_VARIANTS = 18 };
+enum { MCS_BATCH_MOMENTS = 14, MCS_BATCH_LOG = 64, MCS_BATCH_VARIANTS = 22 };
 MCS_API int mcs_batch_create(mcs_ctx* ctx, int max_instances, int64_t total_capacity, mcs_batch** out);
 MCS_API int mcs_batch_destroy(mcs_batch* b);
 /* Join: n particles in Julia layout (x, v as n x 3 row-major), region of `capacity` slots. */
@@ -326,6 +326,8 @@ MCS_API int mcs_batch_set_variant(mcs_batch* b, int variant);
 MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt);
 /* Resident CTAs per SM the variant's register budget is set for (1 = compiler's choice). */
 MCS_API int mcs_batch_variant_min_blocks(int variant, int* min_blocks);
+/* Idle lanes (of 32) at which the variant's particle queue writes back and refills. */
+MCS_API int mcs_batch_variant_refill(int variant, int* idle_lanes);
 
 #ifdef __cplusplus
 }

@@ -29,7 +29,7 @@ Q_FIXED, Q_PART = 0, 1
 MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
-B_NU, B_NU2, BATCH_MOMENTS, BATCH_LOG, BATCH_VARIANTS = 12, 13, 14, 64, 18
+B_NU, B_NU2, BATCH_MOMENTS, BATCH_LOG, BATCH_VARIANTS = 12, 13, 14, 64, 22
 OPT_MESH_SHAPE, MESH_SHAPES = 1, 8
 
 vp = C.c_void_p
@@ -110,6 +110,7 @@ SIGNATURES = {
     "mcs_batch_set_variant": (i32, [vp, i32]),
     "mcs_batch_variant_shape": (i32, [i32, pi32, pi32]),
     "mcs_batch_variant_min_blocks": (i32, [i32, pi32]),
+    "mcs_batch_variant_refill": (i32, [i32, pi32]),
     "mcs_pop_read_step_log": (i32, [vp, pd, i32]),
 }
 

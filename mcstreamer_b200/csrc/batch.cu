@@ -184,7 +184,7 @@ struct BShared {
 // Batched advance! (FP32, uniform field per instance, closed-form push between real
 // collisions): the body of k_step_abs<float,...,CLOSED> with instance indirection.
 // ---------------------------------------------------------------------------------------
-template <int BLOCK, int PPT, int MINB>
+template <int BLOCK, int PPT, int MINB, int REFILL>
 __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
     constexpr int TILE = BLOCK * PPT;
     __shared__ BShared<BLOCK> sh;
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
         uint32_t ev = 0;
         for (;;) {
             const unsigned idle = __ballot_sync(0xffffffffu, !have);
-            if (idle != 0xffffffffu && __popc(idle) < 8) goto substep;
+            if (idle != 0xffffffffu && __popc(idle) < REFILL) goto substep;
             if (!have && pending) {
                 B.f[0][i] = x; B.f[1][i] = y; B.f[2][i] = z;
                 B.f[3][i] = vx; B.f[4][i] = vy; B.f[5][i] = vz;
@@ -799,6 +799,7 @@ struct BatchVariant {
     int block, ppt;
     const void* fn;
     int minb = 0;   // resident CTAs per SM the register budget is set for (0: compiler's choice)
+    int refill = 8; // idle lanes of a warp before the particle queue refills
 };
 
 struct mcs_batch {
@@ -828,8 +829,8 @@ struct mcs_batch {
 
 namespace {
 
-template <int BLOCK, int PPT, int MINB = 0>
-const void* bstep_fn() { return reinterpret_cast<const void*>(k_bstep<BLOCK, PPT, MINB>); }
+template <int BLOCK, int PPT, int MINB = 0, int REFILL = 8>
+const void* bstep_fn() { return reinterpret_cast<const void*>(k_bstep<BLOCK, PPT, MINB, REFILL>); }
 
 // The autotuner's space: threads per block x particles per thread, plus shapes that trade
 // registers for resident CTAs (MINB) and longer tiles (16 particles per thread).
@@ -840,6 +841,10 @@ const BatchVariant kVariants[] = {
     {128, 16, bstep_fn<128, 16>()}, {256, 16, bstep_fn<256, 16>()},
     {256, 8, bstep_fn<256, 8, 4>(), 4}, {256, 16, bstep_fn<256, 16, 4>(), 4},
     {128, 8, bstep_fn<128, 8, 8>(), 8}, {512, 8, bstep_fn<512, 8, 2>(), 2},
+    // the particle queue's refill threshold (idle lanes of 32 before finished lanes write
+    // back and refill together) on the 256 x 16, 4 CTAs/SM shape
+    {256, 16, bstep_fn<256, 16, 4, 4>(), 4, 4}, {256, 16, bstep_fn<256, 16, 4, 12>(), 4, 12},
+    {256, 16, bstep_fn<256, 16, 4, 16>(), 4, 16}, {256, 16, bstep_fn<256, 16, 4, 2>(), 4, 2},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 static_assert(kNumVariants == MCS_BATCH_VARIANTS, "variant table and header disagree");
@@ -1384,6 +1389,12 @@ MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt) {
 MCS_API int mcs_batch_variant_min_blocks(int variant, int* min_blocks) {
     if (variant < 0 || variant >= kNumVariants || !min_blocks) return MCS_ERR_ARG;
     *min_blocks = kVariants[variant].minb;
+    return MCS_OK;
+}
+
+MCS_API int mcs_batch_variant_refill(int variant, int* idle_lanes) {
+    if (variant < 0 || variant >= kNumVariants || !idle_lanes) return MCS_ERR_ARG;
+    *idle_lanes = kVariants[variant].refill;
     return MCS_OK;
 }
 
