@@ -85,6 +85,7 @@ SIGNATURES = {
     "mcs_pop_step_log": (i32, [vp, i32]),
     "mcs_moments_noalloc": (i32, [i32, vp, i32, C.POINTER(C.c_void_p), pu8, i64, pd]),
     "mcs_ctx_set_option": (i32, [vp, i32, i32]),
+    "mcs_diag_wait_timeout": (i32, [vp, u32]),
     "mcs_ctx_get_option": (i32, [vp, i32, pi32]),
     "mcs_mesh_shape": (i32, [i32, pi32, pi32, pi32]),
     "mcs_batch_create": (i32, [vp, i32, i64, ph]),

@@ -182,7 +182,8 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // `first` is the first tile of the segment being scanned (0 for a whole population; the
 // first tile of an instance in a batch, so instances are prefixed independently).
 __device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* status, uint32_t first, uint32_t tile,
-                                                       uint32_t epoch, uint32_t count, uint32_t* st_word, bool* ok) {
+                                                       uint32_t epoch, uint32_t count, uint32_t* st_word, bool* ok,
+                                                       uint32_t max_spins = 1u << 24) {
     *ok = true;
     if (tile == first) {
         st_release_u64(&status[tile], tile_word(epoch, 2, count));
@@ -198,7 +199,7 @@ __device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* statu
         const uint32_t e = (uint32_t)(s >> 34);
         const uint32_t f = (uint32_t)(s >> 32) & 3u;
         if (e != ep || f == 0) {
-            if (++spins > (1u << 24)) {  // ~ seconds with the backoff below
+            if (++spins > max_spins) {  // the default is about a second with the backoff below
                 atomicOr(st_word, ST_TIMEOUT);
                 *ok = false;
                 break;
