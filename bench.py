@@ -712,6 +712,16 @@ def run_batch(args):
     b2.close()
     e2e_solves = spec.k / (t_up + spec.steps * t_steps)
 
+    # the batched FP32 form's error against FP64 runs of the same swarms (gas 0, three E/N)
+    from mcstreamer_b200 import swarm as mswarm
+    acc = {}
+    for en, r in mswarm.fp32_batched_vs_fp64(ctx, tables[0], (100.0, 300.0, 1000.0), spec.density, 131072, 600,
+                                             300, spec.dt).items():
+        acc[f"{en:g} Td"] = {
+            key: {"fp32": a32, "fp64": a64, "rel_diff": (a32 - a64) / a64 if a64 else None,
+                  "combined_3sigma_rel": float(np.hypot(e32, e64) / abs(a64)) if a64 else None}
+            for key, (a32, e32, a64, e64) in r.items()}
+
     pk, pk_kind = peaks()
     hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     alg = batch_alg_bytes(0.5 * (n_before + n_after), 0.0)
@@ -735,6 +745,10 @@ def run_batch(args):
                          "refill_idle_lanes": _variant_int("mcs_batch_variant_refill", chosen),
                          "trial_ms": [round(float(t), 4) for t in times]},
             "l2": "inputs larger than L2 (44.6M electrons x 33 B = 1.5 GB resident)",
+            "fp32_vs_fp64": {"how": "batched FP32 against independent FP64 runs (mcs_swarm_run), 131072 "
+                                    "electrons from a 1 eV Maxwellian, gas 0, steps 300-600, batch-means errors; "
+                                    "W = drift (m/s), E = mean energy (eV), k = ionization rate (m^3/s)",
+                             "results": acc},
             "plain_drop_in": {
                 "fp32_solves_per_s": plain32, "fp32_ms_per_step_all": t32,
                 "fp32_calls_solves_per_s": plain32c, "fp32_calls_ms_per_step_all": t32c,

@@ -149,3 +149,62 @@ def stats(samples: Sequence[Sequence[SwarmResult]]) -> dict[str, np.ndarray]:
         out[k] = a.mean(axis=0)
         out[k + "_err"] = a.std(axis=0, ddof=1) / np.sqrt(len(samples)) if len(samples) > 1 else np.zeros(a.shape[1])
     return out
+
+
+def _block_mean(series, block: int) -> tuple[float, float]:
+    """Mean and 3 sigma of the mean from batch means over blocks of `block` samples."""
+    a = np.asarray(series, dtype=np.float64)
+    nb = len(a) // block
+    if nb < 2:
+        return float(a.mean()) if len(a) else 0.0, float("inf")
+    b = a[len(a) - nb * block:].reshape(nb, block).mean(axis=1)
+    return float(b.mean()), float(3.0 * b.std(ddof=1) / np.sqrt(nb))
+
+
+def fp32_batched_vs_fp64(ctx: Context, table: CollisionTable, ens: Sequence[float], density: float, n0: int,
+                         nt: int, warm: int, dt: float, seed: int = 500, chunk: int = 10) -> dict:
+    """The batched FP32 form (SwarmBatch, all E/N in one batch) against independent FP64 runs
+    of the same swarms (mcs_swarm_run, repack every step), each started from n0 electrons of a
+    1 eV Maxwellian.  Over steps [warm, nt): drift W = <v_z>, mean energy <eps> (eV) and the
+    ionization rate coefficient k_ion = <nu_ion>/N, each with 3 sigma of its mean from batch
+    means (blocks of 30 steps; 3 samples for the FP64 rate, read every `chunk` steps).
+    Returns {en: {key: (fp32, 3 sigma, fp64, 3 sigma)}}."""
+    from .batch import SwarmBatch
+    ion = [j for j, p in enumerate(table.proc) if p.kind in (L.IONIZATION, L.IONIZATION_UNIFORM)]
+    f32 = {en: {"W": [], "E": [], "k": []} for en in ens}
+    with SwarmBatch(ctx, len(ens), 4 * n0 * len(ens)) as b:
+        slots = {en: b.add_maxwellian(table, en * co.Td * density, seed + i, n0, 4 * n0, n0, 1.0)
+                 for i, en in enumerate(ens)}
+        for _ in range(nt // chunk):
+            b.step(dt, chunk)
+            for en, k in slots.items():
+                s = b.read_log(k, chunk)
+                c = s[:, L.S_COUNT]
+                f32[en]["W"] += list(s[:, L.S_V + 2] / c)
+                f32[en]["E"] += list(s[:, L.S_E] / c / co.eV)
+                f32[en]["k"] += list(s[:, L.B_NU] / c / density)
+    out = {}
+    for i, en in enumerate(ens):
+        pop = Population(4 * n0, None, table, precision="fp64", seed=seed + 1000 + i)
+        pop.init_maxwellian(n0, 1.0)
+        fld = FixedField(en * co.Td * density, ctx)
+        W, E, K = [], [], []
+        mom = np.zeros((chunk, L.STEP_MOMENTS))
+        try:
+            for _ in range(nt // chunk):
+                ctx.check(ctx.lib.mcs_swarm_run(pop.h, table.h, fld.h, dt, chunk, n0, 0.1, 1, L.dptr(mom)))
+                W += list(mom[:, L.S_V + 2] / mom[:, L.S_COUNT])
+                E += list(mom[:, L.S_E] / mom[:, L.S_COUNT] / co.eV)
+                if ion:
+                    m = pop.moments(table)
+                    K.append(m[L.MOMENTS_BASE + ion[0]] / m[L.M_COUNT] / density)
+        finally:
+            fld.close()
+            pop.close()
+        r = {}
+        for key, ser64, blk in (("W", W[warm:], 30), ("E", E[warm:], 30), ("k", K[warm // chunk:], 3)):
+            a32, e32 = _block_mean(f32[en][key][warm:], 30)
+            a64, e64 = _block_mean(ser64, blk) if len(ser64) else (0.0, float("inf"))
+            r[key] = (a32, e32, a64, e64)
+        out[en] = r
+    return out

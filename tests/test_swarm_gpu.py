@@ -89,3 +89,25 @@ def test_fp32_swarm_coefficients_within_3_sigma_of_fp64(ctx):
         se = np.hypot(out["fp64"][key + "_err"][0], out["fp32"][key + "_err"][0])
         assert abs(a - b) <= 3 * se + 1e-12 * abs(a), (key, a, b, se)
     tab.close()
+
+
+@pytest.mark.gpu
+def test_batched_fp32_coefficients_match_fp64(ctx):
+    """The batched FP32 form against independent FP64 runs of the same swarms at three E/N:
+    drift, mean energy and ionization rate agree within 3 sigma of the combined statistical
+    error, and within 1 % wherever that error is below 0.5 %."""
+    t = lxcat.synthetic_table(0)
+    tab = jumc.CollisionTable(t, ctx)
+    ctx.set_flags(L.FLAG_CLAMP_ENERGY)
+    try:
+        res = swarm.fp32_batched_vs_fp64(ctx, tab, (300.0, 600.0, 1000.0), DENS, 131072, 600, 300, 1e-13)
+    finally:
+        ctx.set_flags(0)
+        tab.close()
+    for en, r in res.items():
+        for key, (a32, e32, a64, e64) in r.items():
+            err3 = np.hypot(e32, e64)
+            assert abs(a32 - a64) <= err3 + 1e-12 * abs(a64), (en, key, a32, a64, err3)
+            if err3 < 0.005 * abs(a64):
+                assert abs(a32 - a64) <= 0.01 * abs(a64), (en, key, a32, a64)
+    assert all(r["k"][2] > 0 for r in res.values())   # ionizing at every E/N tested
