@@ -274,21 +274,37 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
                 ev = 0;
                 tau = 0.f;
                 trem = B.dt;
-                have = trem > 0;
-                if (!have) cnt[q] = 0;   // dt == 0: state unchanged
+                if (!(trem > 0)) { cnt[q] = 0; continue; }   // dt == 0: state unchanged
+                // the first sub-step's decision; an electron with no collision in the step
+                // flies to its end and is written back here
+                if (trem > s * tab.inv_maxrate) {
+                    have = true;
+                } else {
+                    const double t = trem;
+                    s -= t * tab.maxrate;
+                    tau += (float)t;
+                    trem -= t;
+                    const float h2 = 0.5f * tau * tau;
+                    B.f[0][i] = fmaf(ax, h2, fmaf(vx, tau, x));
+                    B.f[1][i] = fmaf(ay, h2, fmaf(vy, tau, y));
+                    B.f[2][i] = fmaf(az, h2, fmaf(vz, tau, z));
+                    B.f[3][i] = fmaf(ax, tau, vx); B.f[4][i] = fmaf(ay, tau, vy); B.f[5][i] = fmaf(az, tau, vz);
+                    B.f[7][i] = (float)s;
+                    cnt[q] = 0;
+                }
             }
             if (!__any_sync(0xffffffffu, have)) break;
         substep:
             if (!have) continue;
             {
-                // one sub-step of advance! with the closed-form push of a uniform field
-                const double tn = s * tab.inv_maxrate;
-                double t;
-                bool collides;
-                if (trem > tn) { t = tn; collides = true; }
-                else { t = trem; collides = false; s -= t * tab.maxrate; }
+                // one collision sub-step of advance! with the closed-form push of a uniform
+                // field (have: the next collision falls inside the step), then the next
+                // sub-step's decision; the free flight to the step's end finishes here, so an
+                // electron takes one loop pass per collision.  The FP64 time arithmetic is
+                // that of the sub-step sequence of advance!, operation for operation.
+                const double t = s * tab.inv_maxrate;
                 tau += (float)t;
-                if (collides) {
+                {
                     float cvx = fmaf(ax, tau, vx), cvy = fmaf(ay, tau, vy), cvz = fmaf(az, tau, vz);
                     Sec<float> sec;
                     const int out = collide_once<float>(sh.rows, tab, C, rng, cvx, cvy, cvz, sec);
@@ -308,8 +324,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
                     }
                     s = (double)M<float>::nlog(uni32(rng.b.y));
                 }
-                trem -= t;
-                if (!(trem > 0)) {
+                trem -= t;   // > 0: the collision was strictly inside the step
+                if (!(trem > s * tab.inv_maxrate)) {
+                    const double tf = trem;
+                    s -= tf * tab.maxrate;
+                    tau += (float)tf;
+                    trem -= tf;
                     const float h2 = 0.5f * tau * tau;
                     x = fmaf(ax, h2, fmaf(vx, tau, x));
                     y = fmaf(ay, h2, fmaf(vy, tau, y));
