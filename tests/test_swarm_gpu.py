@@ -111,3 +111,27 @@ def test_batched_fp32_coefficients_match_fp64(ctx):
             if err3 < 0.005 * abs(a64):
                 assert abs(a32 - a64) <= 0.01 * abs(a64), (en, key, a32, a64)
     assert all(r["k"][2] > 0 for r in res.values())   # ionizing at every E/N tested
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lam", [0.4, 3.0, 12.5, 37.0])
+def test_device_swarm_resample_clone_counts(ctx, lam):
+    """Swarm.resample! on the device: per-particle clone counts equal the oracle's (same
+    Philox streams, same inversion / PTRS sampler) and follow the Poisson law."""
+    from tests.helpers import maxwellian, oracle_pop
+    from tests.test_oracle import _clone_counts, _poisson_chi2_pvalue
+    n = 20000
+    p = maxwellian(n, 7)
+    p.x[:, 0] = np.arange(n) * 1e-9 + 1e-6
+    cap = int((lam + 2) * n) + 10 * n
+    n0 = int(round(n * (1 + lam)))
+    t = lxcat.synthetic_table(0)
+    tab = jumc.CollisionTable(t, ctx)
+    pop = jumc.Population(cap, p, tab, precision="fp64", seed=11)
+    swarm.resample(pop, n0, 0.1)
+    got = _clone_counts(p, pop.download().x, n)
+    pop.close(); tab.close()
+    op = oracle_pop(p, cap, 11)
+    po.swarm_resample(op, n0, 0.1)
+    np.testing.assert_array_equal(got, _clone_counts(p, op.x[:op.n], n))
+    assert _poisson_chi2_pvalue(got, (n0 - n) / n) > 1e-4
