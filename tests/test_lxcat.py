@@ -58,3 +58,17 @@ def test_photoemission_is_rejected():
     recs = [{"kind": "PHOTOEMISSION", "target": "A", "comment": "", "data": [[0, 1e-20], [10, 1e-20]]}]
     with pytest.raises(NotImplementedError):
         lxcat.load_lxcat_records(recs, {"A": 1.0}, lxcat.EnergyGrid(0.0, 1e-18, 11))
+
+
+def test_flat_linear_interpolation_matches_numpy_interp():
+    """Interpolations.jl Gridded(Linear()) with Flat() extrapolation (lxcat.jl:63-64) is
+    piecewise-linear between knots and constant beyond the ends: the semantics of
+    numpy.interp, used here as an independent implementation."""
+    import numpy as np
+
+    from mcstreamer_b200.lxcat import _interp_flat
+    rng = np.random.default_rng(5)
+    x0 = np.sort(rng.uniform(0.0, 100.0, 300))
+    y0 = rng.normal(size=300)
+    x = np.concatenate([rng.uniform(-20.0, 120.0, 5000), x0, [x0[0], x0[-1], -1e9, 1e9]])
+    np.testing.assert_allclose(_interp_flat(x0, y0, x), np.interp(x, x0, y0), rtol=1e-13, atol=1e-13)
