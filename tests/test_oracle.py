@@ -191,3 +191,55 @@ def test_swarm_resample_clone_counts_are_poisson(lam):
     assert abs(counts.mean() - lam_eff) < 5 * np.sqrt(lam_eff / n)
     assert abs(counts.var() / lam_eff - 1) < 0.06
     assert _poisson_chi2_pvalue(counts, lam_eff) > 1e-4
+
+
+def _load(name):
+    return json.loads((GOLDEN / name).read_text())
+
+
+def _pa(d):
+    from mcstreamer_b200.jumc import ParticleArrays
+    return ParticleArrays(np.array(d["x"]), np.array(d["v"]), np.array(d["w"]), np.array(d["s"]),
+                          np.array(d["active"], np.uint8))
+
+
+def _same_arrays(got, want):
+    assert got.n == want.n
+    for f in ("x", "v", "w", "s", "active"):
+        np.testing.assert_array_equal(getattr(got, f), getattr(want, f))
+
+
+def test_golden_swarm_resample_fixture():
+    g = _load("swarm_resample.json")
+    op = oracle_pop(_pa(g["input"]), g["cap"], g["seed"], step=g["step"])
+    assert po.swarm_resample(op, g["n0"][0], 0.1) == 0
+    _same_arrays(oracle_arrays(op), _pa(g["after_clone"]))
+    assert po.swarm_resample(op, g["n0"][1], 0.1) == 0
+    _same_arrays(oracle_arrays(op), _pa(g["after_drop"]))
+    assert po.repack(op) == 0
+    _same_arrays(oracle_arrays(op), _pa(g["after_repack"]))
+
+
+def test_golden_resample_cells_fixture():
+    g = _load("resample_cells.json")
+    nx, ny, nz, h = g["mesh"]
+    op = oracle_pop(_pa(g["input"]), g["cap"], g["seed"])
+    f = po.field_cart3d(nx, ny, nz, h, (0.0, 0.0, 0.0), np.zeros(3 * (nx + 1) * (ny + 1) * (nz + 1)))
+    assert po.sort_cells(op, f) == 0
+    assert po.resample_cells(op, f, g["ntarget"], g["nmax"], 0) == 0
+    _same_arrays(oracle_arrays(op), _pa(g["output"]))
+
+
+def test_golden_deposit_fixture():
+    from mcstreamer_b200.jumc import ParticleArrays
+    g = _load("deposit_cic.json")
+    nx, ny, nz, h = g["mesh"]
+    x, w = np.array(g["x"]), np.array(g["w"])
+    n = len(w)
+    trk = po.tracker_cart3d(nx, ny, nz, h, (0.0, 0.0, 0.0))
+    po.deposit(oracle_pop(ParticleArrays(x, np.zeros((n, 3)), w, np.ones(n), np.ones(n, np.uint8)), n, 0), trk,
+               g["val"])
+    q = trk._q
+    want = np.zeros(g["n_nodes"], np.int64)
+    want[g["nodes"]] = g["q"]
+    np.testing.assert_array_equal(q, want)
