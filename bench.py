@@ -891,6 +891,195 @@ def run_serve(args):
     return 0
 
 
+POISSON_METRIC = "poisson solves/s"
+
+
+def poisson_alg_bytes_gs(M: int, N: int) -> float:
+    """Algorithmic HBM bytes of one red-black pass over M x N cells: the potential read
+    once (8 B per cell: every cell is a neighbour of the updated colour), the right-hand
+    side and the write of the updated half (4 + 4 B per cell)."""
+    return 16.0 * M * N
+
+
+def poisson_oracle_call(spec, qf, qp, threads):
+    """One poisson! of the CPU restatement from a zero potential; returns (seconds, iters)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import poisson_ref as P
+    u = P.cells(spec.M, spec.N)
+    er, ez = P.faces(spec.M, spec.N), P.faces(spec.M, spec.N)
+    conf = P.default_conf(spec.R, spec.L, spec.M, spec.N, levels=spec.levels)
+    t0 = time.perf_counter()
+    _, it1, it2, _ = P.poisson(conf, qf, qp, u, er, ez, spec.eb, spec.R, spec.L)
+    return time.perf_counter() - t0, (it1, it2)
+
+
+def poisson_inputs(spec):
+    from mcstreamer_b200 import workloads
+    p = workloads.poisson_electrons(spec)
+    qf = workloads.poisson_ion_charge(spec)
+    qp = workloads.poisson_electron_charge(spec, p.x, p.w)
+    return p, qf, qp
+
+
+def poisson_config(spec, extra=None):
+    c = {"workload": f"poisson! on the sample grid: R={spec.R:g} m, L={spec.L:g} m, {spec.M}x{spec.N} cells, "
+                     f"{spec.levels} multigrid levels, tolerance 1e8 e, smoothing 2+2, free b.c. at r=R; "
+                     f"{spec.n} channel electrons of weight {spec.weight:g} deposited each call (density!), "
+                     f"analytic ion charge, eb={spec.eb:g} V/m, cold start (u = 0), seed {spec.seed}",
+         "cells": spec.M * spec.N, "l2": "working set (u, q, 3 finest workspace levels: 630 MB) exceeds L2",
+         "parallelism": "1 GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_poisson(args):
+    import ctypes as C
+
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import jumc, lxcat, streamer, workloads
+    from mcstreamer_b200.poisson import MGConfig, PoissonSolver
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        # replicas only: the solve is not sharded
+        import torch.distributed as dist
+        dist.init_process_group("nccl")
+    torch.cuda.set_device(local)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spec = workloads.poisson_spec()
+    parts, qf, qp_host = poisson_inputs(spec)
+    tab = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
+    grid = streamer.GridCyl(spec.R, spec.L, spec.M, spec.N, ctx=ctx)
+    pop = jumc.Population(spec.n, parts, tab, precision="fp64")
+    solver = PoissonSolver(grid, MGConfig(levels=spec.levels))
+    grid.write_fixed(L.Q_FIXED, qf)
+    lib = ctx.lib
+
+    def step():
+        ctx.check(lib.mcs_grid_zero(grid.h_, L.Q_PART))
+        ctx.check(lib.mcs_deposit(pop.h, grid.h_, -1.0))
+        it = (C.c_int * 2)()
+        ctx.check(lib.mcs_poisson_run(solver.h, spec.eb, it))
+        return it[0], it[1]
+
+    iters = []
+    for _ in range(args.warmup):
+        solver.zero(L.PSN_U)
+        iters.append(step())
+    assert np.array_equal(grid.read_fixed(L.Q_PART), qp_host), "device density! differs from the host restatement"
+    n0 = C.c_int64(0)
+    ctx.check(lib.mcs_poisson_launches(solver.h, C.byref(n0)))
+    times = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        for _ in range(args.steps):
+            solver.zero(L.PSN_U)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            iters.append(step())
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+    n1 = C.c_int64(0)
+    ctx.check(lib.mcs_poisson_launches(solver.h, C.byref(n1)))
+    total_ms = float(sum(times))
+    if ws > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = ws * 1e3 / ms
+    gs_ms, res_ms = solver.profile(20)
+    pk, src = peaks()
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    ach = poisson_alg_bytes_gs(spec.M, spec.N) / (gs_ms * 1e-3) / 1e9
+
+    # end to end: host int64 charges in, host face fields out, pinned buffers
+    nq = (spec.M + 2) * (spec.N + 2)
+    nf = 2 * (spec.M + 3) * (spec.N + 3)
+    h_qf = torch.from_numpy(qf).pin_memory()
+    h_qp = torch.from_numpy(qp_host).pin_memory()
+    h_e = torch.empty(nf, dtype=torch.float64).pin_memory()
+    pi64 = C.POINTER(C.c_int64)
+    pd = C.POINTER(C.c_double)
+    e2e_t = []
+    for k in range(args.e2e_steps + 1):
+        solver.zero(L.PSN_U)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.check(lib.mcs_grid_write_fixed(grid.h_, L.Q_FIXED, C.cast(h_qf.data_ptr(), pi64)))
+        ctx.check(lib.mcs_grid_write_fixed(grid.h_, L.Q_PART, C.cast(h_qp.data_ptr(), pi64)))
+        it = (C.c_int * 2)()
+        ctx.check(lib.mcs_poisson_run(solver.h, spec.eb, it))
+        ctx.check(lib.mcs_grid_read_efield(grid.h_, C.cast(h_e.data_ptr(), pd)))
+        if k:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_v = 1.0 / statistics.median(e2e_t)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        sec, it_cpu = poisson_oracle_call(spec, qf, qp_host, threads)
+        cpu = {"value": 1.0 / sec, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"one full poisson! (this workload) by the oracle on {threads} threads: {sec:.2f} s, "
+                         f"fmg! calls {it_cpu}"}
+    launches = int((n1.value - n0.value) / args.steps)
+    it_set = sorted({tuple(i) for i in iters})
+    line = {
+        "metric": POISSON_METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": poisson_config(spec, {"fmg_calls_per_solve": it_set}),
+        "roofline": {"kernel": "k_gs (one red-black pass, finest level)", "bound": "hbm", "achieved": ach,
+                     "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "peak_source": src, "launch_ms": gs_ms, "residual_launch_ms": res_ms,
+                     "alg_bytes_per_launch": poisson_alg_bytes_gs(spec.M, spec.N)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "solves/s", "h2d_bytes_per_step": 2 * nq * 8, "d2h_bytes_per_step": nf * 8,
+                "path": "mcs_grid_write_fixed (qfixed, qpart from pinned host) -> mcs_poisson_run -> "
+                        "mcs_grid_read_efield (er, ez to pinned host)"},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close(); pop.close(); grid.close(); tab.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_poisson(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.poisson_spec()
+    _, qf, qp = poisson_inputs(spec)
+    threads = os.cpu_count() or 1
+    runs = [poisson_oracle_call(spec, qf, qp, threads) for _ in range(max(1, min(args.steps, 3)))]
+    sec = statistics.median(r[0] for r in runs)
+    v = 1.0 / sec
+    line = {
+        "impl": "reference", "metric": POISSON_METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": len(runs), "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": poisson_config(spec),
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"{len(runs)} full poisson! calls of the oracle, fmg! calls {runs[0][1]}"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_batch(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -921,6 +1110,8 @@ def main():
         return run_cfg2(args)
     if args.workload == "cfg3":
         return run_reference_batch(args) if args.impl == "reference" else run_batch(args)
+    if args.workload == "poisson":
+        return run_reference_poisson(args) if args.impl == "reference" else run_poisson(args)
     if args.workload == "cfg4":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU reference arm; "

@@ -89,6 +89,7 @@ typedef struct mcs_grid mcs_grid;
 typedef struct mcs_field mcs_field;
 typedef struct mcs_pop mcs_pop;
 typedef struct mcs_batch mcs_batch;
+typedef struct mcs_poisson mcs_poisson;
 
 /* ---- context ---- */
 MCS_API int mcs_version(void);
@@ -141,8 +142,10 @@ MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e);
  * large field can be streamed from the host in pieces. */
 MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count, const double* e);
 MCS_API int mcs_grid_zero(mcs_grid* g, int which);
-/* cart3d: int64 per node (2^-32 e).  Not available for cyl grids. */
+/* int64 at 2^-32 e: per node (cart3d) or per cell, index i + j*(M+2) (cyl). */
 MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out);
+/* Overwrite a charge array with host int64 values (layout of mcs_grid_read_fixed). */
+MCS_API int mcs_grid_write_fixed(mcs_grid* g, int which, const int64_t* in);
 /* cyl: density per cell (weight/dV, poisson.jl:79-81).  cart3d: charge per node in e. */
 MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out);
 /* Device address and entry count of a charge array (int64), for collectives that sum the
@@ -186,7 +189,7 @@ MCS_API int mcs_pop_init_cloud(mcs_pop* p, int64_t n, double cx, double cy, doub
 /* Node field of a Gaussian charge e*rho_peak*exp(-r^2/2 sigma^2) centred at (cx, cy, cz)
  * plus the uniform background (ebx, eby, ebz), from Gauss's law, computed on the device
  * (cart3d grids). */
-/* The node field of a cart3d grid (3 doubles per node, x fastest), as stored. */
+/* The stored field: cart3d 3 doubles per node (x fastest); cyl the er then the ez faces. */
 MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e);
 MCS_API int mcs_grid_set_efield_gaussian(mcs_grid* g, double cx, double cy, double cz, double sigma,
                                          double rho_peak, double ebx, double eby, double ebz);
@@ -333,6 +336,49 @@ MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt);
 MCS_API int mcs_batch_variant_min_blocks(int variant, int* min_blocks);
 /* Idle lanes (of 32) at which the variant's particle queue writes back and refills. */
 MCS_API int mcs_batch_variant_refill(int variant, int* idle_lanes);
+
+/* ---- Poisson solve: poisson! (MCStreamer/src/poisson.jl:6-58) on a cylindrical grid ----
+ * The multigrid is Multigrid.solve (Multigrid/src/Multigrid.jl:449-467) with MCStreamer's
+ * MGConfig (MCStreamer/src/main.jl:131-144): bc Left/Right/Top Dirichlet, Bottom (axis)
+ * Neumann, CylindricalConnector{1}, g = 1.  Potential u and right-hand side b are
+ * (M+2)x(N+2) doubles indexed i + j*(M+2) (calloc_centers). */
+enum { MCS_PSN_U = 0,         /* potential fields.u */
+       MCS_PSN_B = 1,         /* right-hand side fields.q (charge density, C/m^3) */
+       MCS_PSN_BCOND = 2,     /* free-boundary values at r = R of the last solve, N+2 doubles */
+       MCS_PSN_FREEBC_F = 3   /* f_n of solve_freebc!, N doubles (download only) */
+};
+/* MGConfig(levels, smooth1, smooth2, maxiter, tolerance, s); s <= 0 takes dz^2 / eps0
+ * (main.jl:138).  M and N must be multiples of 2^levels, the coarsest level at most 4096
+ * cells. */
+MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2, int maxiter,
+                               double tolerance, double s, mcs_poisson** out);
+MCS_API int mcs_poisson_destroy(mcs_poisson* p);
+MCS_API int mcs_poisson_upload(mcs_poisson* p, int which, const double* host);
+MCS_API int mcs_poisson_download(mcs_poisson* p, int which, double* host);
+/* Kernels this workspace has launched so far. */
+MCS_API int mcs_poisson_launches(mcs_poisson* p, int64_t* count);
+/* Zero u (MCS_PSN_U) or b (MCS_PSN_B) on the device. */
+MCS_API int mcs_poisson_zero(mcs_poisson* p, int which);
+/* Mean device time (ms) of one finest-level red-black pass and of one finest-level
+ * residual, each launched `reps` times between CUDA events on the context's stream, on
+ * scratch levels (u and b untouched). */
+MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* residual_ms);
+/* Multigrid.solve(mg, u, b, ws) on the device-resident u, b: fmg! calls in *iters, the
+ * last residual RMS in *eps_last (either may be NULL). */
+MCS_API int mcs_poisson_mg_solve(mcs_poisson* p, int* iters, double* eps_last);
+/* solve_freebc!(u, b, grid, mg, ws) (MCStreamer/src/freebc.jl:4-36); iters[2] = fmg! calls
+ * of the two solves.  b gets the inhomogeneous term, as in the reference. */
+MCS_API int mcs_poisson_solve_freebc(mcs_poisson* p, int* iters);
+/* b = Float32((qfixed + qpart) / dV * e) from the grid's int64 cell charges
+ * (poisson.jl:12-34 with the NullDenoiser). */
+MCS_API int mcs_poisson_assemble(mcs_poisson* p);
+/* The grid's face fields from u (poisson.jl:47-57): er = -du/dr, ez = eb - du/dz. */
+MCS_API int mcs_poisson_fields(mcs_poisson* p, double eb);
+/* poisson! after density!: assemble, solve_freebc!, fields; returns after the fields are
+ * written. */
+MCS_API int mcs_poisson_run(mcs_poisson* p, double eb, int* iters);
+/* f_n = L k (I1/I0 + K1/K0)(k R) / 2, k = pi n / L, n = 1..N (freebc.jl:17-20).  Host only. */
+MCS_API int mcs_freebc_coefficients(double L, double R, int N, double* f);
 
 #ifdef __cplusplus
 }

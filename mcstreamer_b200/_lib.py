@@ -26,6 +26,7 @@ NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM = 0, 1, 2,
 FP64, FP32 = 0, 1
 FLAG_CLAMP_ENERGY = 1
 Q_FIXED, Q_PART = 0, 1
+PSN_U, PSN_B, PSN_BCOND, PSN_FREEBC_F = 0, 1, 2, 3
 MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
@@ -113,6 +114,20 @@ SIGNATURES = {
     "mcs_batch_variant_min_blocks": (i32, [i32, pi32]),
     "mcs_batch_variant_refill": (i32, [i32, pi32]),
     "mcs_pop_read_step_log": (i32, [vp, pd, i32]),
+    "mcs_poisson_create": (i32, [vp, i32, i32, i32, i32, f64, f64, C.POINTER(C.c_void_p)]),
+    "mcs_poisson_destroy": (i32, [vp]),
+    "mcs_poisson_upload": (i32, [vp, i32, pd]),
+    "mcs_poisson_download": (i32, [vp, i32, pd]),
+    "mcs_poisson_mg_solve": (i32, [vp, pi32, pd]),
+    "mcs_poisson_solve_freebc": (i32, [vp, pi32]),
+    "mcs_poisson_assemble": (i32, [vp]),
+    "mcs_poisson_fields": (i32, [vp, f64]),
+    "mcs_poisson_run": (i32, [vp, f64, pi32]),
+    "mcs_freebc_coefficients": (i32, [f64, f64, i32, pd]),
+    "mcs_poisson_zero": (i32, [vp, i32]),
+    "mcs_poisson_launches": (i32, [vp, pi64]),
+    "mcs_poisson_profile": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mcs_grid_write_fixed": (i32, [vp, i32, pi64]),
 }
 
 _lib = None

@@ -358,9 +358,14 @@ MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count,
 MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e) {
     if (!g || !e) return MCS_ERR_ARG;
     mcs_ctx* c = g->ctx;
-    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "field read-back needs a cart3d grid");
     if (int st = use_device(c)) return st;
     MCS_CK(c, cudaStreamSynchronize(c->stream));
+    if (g->v.type == GRID_CYL) {
+        const size_t faces = (size_t)(g->v.M + 3) * (g->v.N + 3);
+        MCS_CK(c, cudaMemcpy(e, g->d_er, faces * sizeof(double), cudaMemcpyDeviceToHost));
+        MCS_CK(c, cudaMemcpy(e + faces, g->d_ez, faces * sizeof(double), cudaMemcpyDeviceToHost));
+        return MCS_OK;
+    }
     if (g->d_e32) {
         std::vector<float> tmp(4 * g->nq);
         MCS_CK(c, cudaMemcpy(tmp.data(), g->d_e32, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
@@ -387,6 +392,15 @@ MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out) {
     const int st = sync_status(c);
     MCS_CK(c, cudaMemcpy(out, g->d_q[which], g->nq * sizeof(long long), cudaMemcpyDeviceToHost));
     return st;
+}
+
+MCS_API int mcs_grid_write_fixed(mcs_grid* g, int which, const int64_t* in) {
+    if (!g || !in || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaMemcpyAsync(g->d_q[which], in, g->nq * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    return MCS_OK;
 }
 
 MCS_API int mcs_grid_charge_ptr(mcs_grid* g, int which, void** dptr, int64_t* count) {

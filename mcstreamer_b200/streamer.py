@@ -139,6 +139,19 @@ class GridCyl:
         self.ctx.check(self.ctx.lib.mcs_grid_read_density(self.h_, which, L.dptr(out)))
         return out.reshape(self.N + 2, self.M + 2).T   # (i, j) like calloc_centers
 
+    def write_fixed(self, which: int, q: np.ndarray) -> None:
+        """Overwrite the int64 cell charges (2^-32 e), flat, index i + j*(M+2)."""
+        q = np.ascontiguousarray(q, dtype=np.int64)
+        if q.size != (self.M + 2) * (self.N + 2):
+            raise ValueError("charge array of the wrong size")
+        self.ctx.check(self.ctx.lib.mcs_grid_write_fixed(self.h_, which, L.i64ptr(q)))
+
+    def read_fixed(self, which: int = L.Q_PART) -> np.ndarray:
+        """The int64 cell charges (2^-32 e), flat, index i + j*(M+2)."""
+        out = np.zeros((self.M + 2) * (self.N + 2), dtype=np.int64)
+        self.ctx.check(self.ctx.lib.mcs_grid_read_fixed(self.h_, which, L.i64ptr(out)))
+        return out
+
     def close(self) -> None:
         if self.h_:
             self.ctx.lib.mcs_grid_destroy(self.h_)

@@ -11,6 +11,14 @@ streamer(cfg): the 3-D streamer steps.
 Particles are generated on the host and sorted by cell key (the layout the cell-sorted
 resampling maintains), then uploaded.
 
+poisson_spec(): the electrostatic solve of poisson! on the reference's sample grid
+  (MCStreamer samples/input.toml: R = 1.5 cm, L = 10 cm, 1536 x 10240 cells, 9 multigrid
+  levels, tolerance 1e8 e, 2 + 2 smoothing sweeps): a negative-streamer channel along the
+  axis, 4,194,304 electrons of weight 1.5e6 (radial Gaussian sigma 0.5 mm, z uniform on
+  [2, 6] cm, a tenth of them in a Gaussian head of sigma 1 mm at z = 6 cm) over the
+  analytic ion density of the channel body alone, background field -1.5 MV/m; seed 1.
+  Each solve starts from a zero potential.
+
 batched_swarms(): the batched swarm workload ("cfg3"): 256 instances with E/N log-spaced
   10-1000 Td, electron counts log-uniform 4,096-1,048,576 and one of the synthetic gases
   0, 1, 2 each (seeded, seed 3); N = 2.5e25 m^-3, dt = 1e-13 s, 5000 steps per solve,
@@ -137,3 +145,75 @@ def swarm_instance_particles(spec: BatchedSwarmSpec, k: int) -> ParticleArrays:
     """Initial electrons of instance k: isotropic Maxwellian at spec.mean_ev, at the origin."""
     from .swarm import initial_particles
     return initial_particles(int(spec.n[k]), "maxwellian", int(spec.seeds[k]), mean_ev=spec.mean_ev)
+
+
+@dataclass
+class PoissonSpec:
+    R: float = 0.015
+    L: float = 0.1
+    M: int = 1536
+    N: int = 10240
+    levels: int = 9
+    n: int = 4_194_304
+    weight: float = 1.5e6
+    sigma_r: float = 5e-4
+    z0: float = 0.02
+    z1: float = 0.06
+    head_frac: float = 0.1
+    head_sigma: float = 1e-3
+    eb: float = -1.5e6
+    seed: int = 1
+
+
+def poisson_spec() -> PoissonSpec:
+    return PoissonSpec()
+
+
+def poisson_electrons(spec: PoissonSpec) -> ParticleArrays:
+    """The channel's electrons (at rest: only their positions and weights matter here)."""
+    rng = np.random.default_rng(spec.seed)
+    n = spec.n
+    nh = int(round(spec.head_frac * n))
+    x = np.empty((n, 3))
+    rr = spec.sigma_r * np.sqrt(-2.0 * np.log1p(-rng.random(n)))
+    th = 2.0 * np.pi * rng.random(n)
+    x[:, 0] = rr * np.cos(th)
+    x[:, 1] = rr * np.sin(th)
+    x[:n - nh, 2] = rng.uniform(spec.z0, spec.z1, n - nh)
+    x[n - nh:, 2] = spec.z1 + spec.head_sigma * rng.standard_normal(nh)
+    x[:, 2] = np.clip(x[:, 2], 1e-6, spec.L - 1e-6)
+    p = ParticleArrays.empty(n)
+    p.x[:] = x
+    p.w[:] = spec.weight
+    p.s[:] = 1.0
+    p.active[:] = 1
+    return p
+
+
+def poisson_ion_charge(spec: PoissonSpec) -> np.ndarray:
+    """qfixed: the expected charge of the channel body's electrons, positive, as int64 cell
+    charges (2^-32 e, index i + j*(M+2))."""
+    M, N = spec.M, spec.N
+    dr, dz = spec.R / M, spec.L / N
+    rf = np.arange(M + 1) * dr
+    zf = np.arange(N + 1) * dz
+    # electrons per cell of the body: n_body * P(r-shell) * P(z-slab)
+    n_body = spec.n - int(round(spec.head_frac * spec.n))
+    pr = np.diff(-np.exp(-rf ** 2 / (2 * spec.sigma_r ** 2)))
+    pz = np.diff(np.clip((zf - spec.z0) / (spec.z1 - spec.z0), 0.0, 1.0))
+    q = np.zeros((M + 2, N + 2), order="F")
+    q[1:M + 1, 1:N + 1] = n_body * spec.weight * pr[:, None] * pz[None, :]
+    return np.rint(q * 2.0 ** 32).astype(np.int64).ravel(order="F")
+
+
+def poisson_electron_charge(spec: PoissonSpec, x: np.ndarray, w: np.ndarray) -> np.ndarray:
+    """density!(grid, qpart, electrons, val = -1) as int64 cell charges: nearest cell,
+    rho and z cells by floor, particles outside skipped (poisson.jl:65-84)."""
+    M, N = spec.M, spec.N
+    dr, dz = spec.R / M, spec.L / N
+    i = np.floor(np.hypot(x[:, 0], x[:, 1]) / dr).astype(np.int64) + 1
+    j = np.floor(x[:, 2] / dz).astype(np.int64) + 1
+    ok = (i >= 1) & (i <= M) & (j >= 0) & (j <= N + 1)
+    q = np.zeros((M + 2) * (N + 2), dtype=np.int64)
+    np.add.at(q, i[ok] + j[ok] * (M + 2), np.rint(-w[ok] * 2.0 ** 32).astype(np.int64))
+    return q

@@ -10,15 +10,15 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SRC = HERE / "oracle.cpp"
+SRCS = [HERE / "oracle.cpp", HERE / "poisson.cpp"]
 
 
 def build(verbose: bool = False) -> Path:
-    deps = [SRC, HERE / "oracle.h"]
+    deps = SRCS + [HERE / "oracle.h"]
     if LIB.exists() and LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
         return LIB
     cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-Wall",
-           "-o", str(LIB), str(SRC)]
+           "-o", str(LIB)] + [str(x) for x in SRCS]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")

@@ -101,6 +101,17 @@ int orc_resample_cells(orc_pop* pop, const orc_field* grid, int ntarget, int nma
 /* R10: cart3d CIC int64 from f32 in-cell offsets (device quantisation) or cyl NGP. */
 void orc_deposit(const orc_pop* pop, orc_tracker* trk, double val, int quantize_f32);
 
+/* Cylindrical multigrid (poisson.cpp): Multigrid.solve with MCStreamer's configuration.
+ * Arrays (M+2)x(N+2), index i + j*(M+2).  Returns the number of fmg! calls. */
+int orc_mg_solve(int M, int N, double s, int levels, double tol, int smooth1, int smooth2, int maxiter,
+                 double* u, const double* b, double* eps_last);
+double orc_mg_residual_rms(int M, int N, double s, const double* u, const double* b);
+void orc_mg_apply_bc(double* a, int M, int N);
+void orc_mg_gauss_seidel(double* u, const double* b, int M, int N);
+void orc_mg_residual(double* r, const double* u, const double* b, double s, int M, int N);
+void orc_mg_restrict(double* rh, const double* r, int M, int N);
+void orc_mg_interpolate(double* f, const double* h, int M, int N, int add);
+
 #ifdef __cplusplus
 }
 #endif
