@@ -1011,7 +1011,7 @@ def run_poisson(args):
     pi64 = C.POINTER(C.c_int64)
     pd = C.POINTER(C.c_double)
     e2e_t = []
-    for k in range(args.e2e_steps + 1):
+    for k in range(max(1, args.e2e_steps) + 1):
         solver.zero(L.PSN_U)
         torch.cuda.synchronize()
         t0 = time.perf_counter()

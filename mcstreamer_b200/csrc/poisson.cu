@@ -12,6 +12,7 @@
 // i = 0, M+1 and j = 0, N+1 (element (i, j) at i + j*(M+2)).  Level l has M >> l by N >> l
 // cells.  Levels of at most kSmallCells cells run inside one CTA (their kernels would be
 // launch-bound); the rest run one grid-wide kernel per operation.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -21,13 +22,16 @@
 
 #include "../../include/mcs.h"
 #include "host_util.h"
+#include "mcs_device.cuh"
 #include "mcs_internal.h"
+#include "pop_ops.h"
 
 namespace mcs {
 namespace {
 
 constexpr int kMaxLevels = 16;
 constexpr long kSmallCells = 32768;
+constexpr long kTailSmemBytes = 200 * 1024;   // shared memory of the one-CTA tail
 constexpr int kCtaThreads = 1024;
 constexpr int kThreads = 256;
 constexpr int kCoarsestSweeps = 50;   // mgv! at level == levels (Multigrid.jl:340-346)
@@ -46,6 +50,7 @@ struct LevelView {
 
 struct MgView {
     int levels, smooth1, smooth2, small;
+    int tail_off[kMaxLevels + 1];   // shared-memory offset (doubles) of a tail level's arrays
     int nc;
     const double* ainv;   // inverse of the coarsest Cartesian matrix, nc x nc row-major
     LevelView lv[kMaxLevels + 1];
@@ -61,10 +66,10 @@ __device__ __forceinline__ double dneg(double v) { return -v + 0.0; }   // coef 
 // (Top, Dirichlet), (Bottom, Neumann)).  Left/Right fill the inner rows; Top/Bottom then
 // fill every column, so the corners take Top/Bottom of the Left/Right ghosts.  No thread
 // reads a value that another one writes.
-__device__ void bc_range(double* a, int M, int N, long t0, long dt) {
+__device__ void bc_range(double* a, int M, int N, int t0, int dt) {
     const long ld = M + 2;
-    const long n = (long)max(M + 1, N + 2);
-    for (long t = t0; t < n; t += dt) {
+    const int n = max(M + 1, N + 2);
+    for (int t = t0; t < n; t += dt) {
         if (t >= 1 && t <= M) {
             a[t] = dneg(a[t + ld]);
             a[t + (N + 1) * ld] = dneg(a[t + N * ld]);
@@ -102,13 +107,13 @@ __device__ __forceinline__ double lap5(const double* u, long k, long ld, double 
 // rows 1, 3, ... <= M shifted by parity xor (j even).  An odd M (possible on the coarsest
 // level only) shifts into the ghost row M+1, which the reference updates too.
 __device__ void gs_range(double* u, const double* b, const double* fp, const double* fm, int M, int N,
-                         int parity, long t0, long dt) {
+                         int parity, int t0, int dt) {
     const long ld = M + 2;
     const int hm = (M + 1) >> 1;
-    const long n = (long)hm * N;
-    for (long t = t0; t < n; t += dt) {
-        const int j = 1 + (int)(t / hm);
-        const int i = 1 + 2 * (int)(t - (long)(j - 1) * hm) + (parity ^ ((j & 1) == 0 ? 1 : 0));
+    const int n = hm * N;
+    for (int t = t0; t < n; t += dt) {
+        const int j = 1 + t / hm;
+        const int i = 1 + 2 * (t - (j - 1) * hm) + (parity ^ ((j & 1) == 0 ? 1 : 0));
         const long k = i + j * ld;
         const double l = lap5(u, k, ld, fp[i], fm[i]);
         u[k] += 1.0 * (l + b[k]) / 4.0;
@@ -117,12 +122,12 @@ __device__ void gs_range(double* u, const double* b, const double* fp, const dou
 
 // residual! (Multigrid.jl:186-193): r = s b + L u on the inner cells.
 __device__ void residual_range(double* r, const double* u, const double* b, double s, const double* fp,
-                               const double* fm, int M, int N, long t0, long dt) {
+                               const double* fm, int M, int N, int t0, int dt) {
     const long ld = M + 2;
-    const long n = (long)M * N;
-    for (long t = t0; t < n; t += dt) {
-        const int j = 1 + (int)(t / M);
-        const int i = 1 + (int)(t - (long)(j - 1) * M);
+    const int n = M * N;
+    for (int t = t0; t < n; t += dt) {
+        const int j = 1 + t / M;
+        const int i = 1 + (t - (j - 1) * M);
         const long k = i + j * ld;
         r[k] = s * b[k] + lap5(u, k, ld, fp[i], fm[i]);
     }
@@ -130,12 +135,12 @@ __device__ void residual_range(double* r, const double* u, const double* b, doub
 
 // restrict! (Multigrid.jl:213-226): coarse (I, J) = 4 * (sum of the children in the order
 // (0,0), (0,1), (1,0), (1,1)) / 4.  M, N are the coarse sizes.
-__device__ void restrict_range(double* h, const double* f, int M, int N, long t0, long dt) {
+__device__ void restrict_range(double* h, const double* f, int M, int N, int t0, int dt) {
     const long ldh = M + 2, ldf = 2 * M + 2;
-    const long n = (long)M * N;
-    for (long t = t0; t < n; t += dt) {
-        const int J = 1 + (int)(t / M);
-        const int I = 1 + (int)(t - (long)(J - 1) * M);
+    const int n = M * N;
+    for (int t = t0; t < n; t += dt) {
+        const int J = 1 + t / M;
+        const int I = 1 + (t - (J - 1) * M);
         const long k = (2 * I - 1) + (2 * J - 1) * ldf;
         double s = 0.0;
         s += f[k];
@@ -148,12 +153,12 @@ __device__ void restrict_range(double* h, const double* f, int M, int N, long t0
 
 // interpolate! (Multigrid.jl:232-258): fine child s of (I, J) = sum over sh of w(sh) *
 // coarse[(I, J) + (2s - 1) .* sh], w = 9/16, 3/16, 3/16, 1/16; added or stored.
-__device__ void interp_range(double* f, const double* h, int M, int N, bool add, long t0, long dt) {
+__device__ void interp_range(double* f, const double* h, int M, int N, bool add, int t0, int dt) {
     const long ldh = M + 2, ldf = 2 * M + 2;
-    const long n = (long)M * N;
-    for (long t = t0; t < n; t += dt) {
-        const int J = 1 + (int)(t / M);
-        const int I = 1 + (int)(t - (long)(J - 1) * M);
+    const int n = M * N;
+    for (int t = t0; t < n; t += dt) {
+        const int J = 1 + t / M;
+        const int I = 1 + (t - (J - 1) * M);
         const long kh = I + J * ldh;
 #pragma unroll
         for (int si = 0; si < 2; ++si)
@@ -171,15 +176,15 @@ __device__ void interp_range(double* f, const double* h, int M, int N, bool add,
     }
 }
 
-__device__ void zero_range(double* a, long n, long t0, long dt) {
-    for (long t = t0; t < n; t += dt) a[t] = 0.0;
+__device__ void zero_range(double* a, int n, int t0, int dt) {
+    for (int t = t0; t < n; t += dt) a[t] = 0.0;
 }
 
 // ---------------------------------------------------------------------------------------
 // Grid-wide kernels, one per operation.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ long gtid() { return (long)blockIdx.x * blockDim.x + threadIdx.x; }
-__device__ __forceinline__ long gthreads() { return (long)gridDim.x * blockDim.x; }
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gthreads() { return gridDim.x * blockDim.x; }
 
 __global__ void k_bc(double* a, int M, int N) { bc_range(a, M, N, gtid(), gthreads()); }
 __global__ void k_gs(double* u, const double* b, const double* fp, const double* fm, int M, int N, int parity) {
@@ -258,10 +263,33 @@ __device__ void smooth_cta(const LevelView& L, const double* b, int n) {
     }
 }
 
+// The same sweeps by warp 0 alone (levels of at most 1024 cells: a warp barrier is far
+// cheaper than a block one, and the coarsest level runs 50 sweeps).
+__device__ void smooth_warp(const LevelView& L, const double* b, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int it = 0; it < n; ++it) {
+        bc_range(L.sol, L.M, L.N, lane, 32);
+        __syncwarp();
+        gs_range(L.sol, b, L.fp, L.fm, L.M, L.N, 0, lane, 32);
+        __syncwarp();
+        gs_range(L.sol, b, L.fp, L.fm, L.M, L.N, 1, lane, 32);
+        __syncwarp();
+    }
+}
+
+__device__ void smooth_coarsest(const LevelView& C) {
+    if ((long)(C.M + 2) * (C.N + 2) <= 1024) {
+        if (threadIdx.x < 32) smooth_warp(C, C.res, kCoarsestSweeps);
+        __syncthreads();
+    } else {
+        smooth_cta(C, C.res, kCoarsestSweeps);
+    }
+}
+
 // mgv! (Multigrid.jl:334-377) from level l0 down to the coarsest and back, written as a
 // loop: level l solves into sol[l] with right-hand side res[l].
 __device__ void vcycle_cta(const MgView& V, int l0) {
-    const long t0 = threadIdx.x, dt = blockDim.x;
+    const int t0 = threadIdx.x, dt = blockDim.x;
     for (int l = l0; l < V.levels; ++l) {
         const LevelView& L = V.lv[l];
         const LevelView& H = V.lv[l + 1];
@@ -274,7 +302,7 @@ __device__ void vcycle_cta(const MgView& V, int l0) {
         zero_range(H.sol, (long)(H.M + 2) * (H.N + 2), t0, dt);
         __syncthreads();
     }
-    smooth_cta(V.lv[V.levels], V.lv[V.levels].res, kCoarsestSweeps);
+    smooth_coarsest(V.lv[V.levels]);
     for (int l = V.levels - 1; l >= l0; --l) {
         const LevelView& L = V.lv[l];
         const LevelView& H = V.lv[l + 1];
@@ -286,11 +314,271 @@ __device__ void vcycle_cta(const MgView& V, int l0) {
 
 __global__ void __launch_bounds__(kCtaThreads) k_vcycle_cta(MgView V, int l0) { vcycle_cta(V, l0); }
 
+// ---------------------------------------------------------------------------------------
+// Fused smoothing on the grid-wide levels (even M).  One CTA owns kTileR x kTileZ inner
+// cells and holds them in shared memory with a halo of H = 2 NS + 1 cells, enough for
+// NS red-black sweeps (each half-sweep consumes one cell of halo) plus the residual's
+// stencil, so NS sweeps of the whole level need one read and one write of it.  Every value
+// a CTA writes depends only on cells inside its halo and is computed with the arithmetic
+// of the per-operation kernels above, so the result is the same bit for bit.
+//   TILE_PRE:     x = NS x (apply!, red, black); apply!; r = b + L x; rh = restrict(r);
+//                 the next level's solution cleared (mgv! before its recursion).
+//   TILE_PRE_SET: the same with x = interpolate(xh) first (an FMG stage entering mgv!).
+//   TILE_POST:    x += interpolate(xh); NS x (apply!, red, black) (mgv! after it).
+// A launch reads xin and writes xout (tiles read each other's halo, so not in place).
+// ---------------------------------------------------------------------------------------
+constexpr int kTileR = 128, kTileZ = 32, kTileThreads = 256, kTileWarps = kTileThreads / 32;
+constexpr uint32_t kWaitSpins = 1u << 22;   // bound of every mbarrier wait
+enum { TILE_PRE = 0, TILE_PRE_SET = 1, TILE_POST = 2 };
+
+struct TileArgs {
+    double* xout;
+    const double* xh;    // next coarser solution (TILE_PRE_SET, TILE_POST)
+    double* rh;          // next coarser right-hand side (TILE_PRE, TILE_PRE_SET)
+    double* hzero;       // next coarser solution to clear (TILE_PRE)
+    const double* fp;
+    const double* fm;
+    uint32_t* status;
+    int M, N, tiles_r;
+};
+
+template <int NS>
+struct TileShape {
+    static constexpr int H = 2 * NS + 1;                 // halo
+    static constexpr int LR = kTileR + 2 * H;            // loaded rows (TMA box, 16-byte multiple)
+    static constexpr int LZ = kTileZ + 2 * H;            // loaded columns
+    static constexpr int CR = ((LR / 2 + 4) + 1) & ~1;   // coarse rows for the interpolation
+    static constexpr int CZ = LZ / 2 + 3;
+    static constexpr int SX = (LR * LZ + 15) & ~15;      // doubles per fine array, 128-byte padded
+    static constexpr int SH = (CR * CZ + 15) & ~15;
+    static constexpr int SF = (2 * LR + 15) & ~15;        // connector factors of the rows
+    static constexpr size_t smem = sizeof(double) * (size_t)(2 * SX + SH + SF);
+    static constexpr uint32_t box_bytes = sizeof(double) * LR * LZ;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait on phase 0 of an mbarrier; false when the bound ran out.
+__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < kWaitSpins; ++it) {
+        uint32_t done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+                     " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(a) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// One 2-D tile of a level array into shared memory (TMA, zero fill outside the array).
+__device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// apply! on the ghost cells of the array that lie in the tile: local (ii, jj) holds
+// global (gr0 + ii, gc0 + jj), nr x nz local cells, leading dimension lr.
+__device__ void tile_bc(double* xs, int lr, int nr, int nz, int gr0, int gc0, int M, int N) {
+    auto at = [&](int i, int j) -> double& { return xs[(i - gr0) + (long)(j - gc0) * lr]; };
+    auto has = [&](int i, int j) { return i >= gr0 && i < gr0 + nr && j >= gc0 && j < gc0 + nz; };
+    for (int t = threadIdx.x; t < max(nr, nz); t += blockDim.x) {
+        const int i = gr0 + t, j = gc0 + t;
+        if (t < nr && i >= 1 && i <= M) {   // Left, Right (inner rows)
+            if (has(i, 0) && has(i, 1)) at(i, 0) = dneg(at(i, 1));
+            if (has(i, N + 1) && has(i, N)) at(i, N + 1) = dneg(at(i, N));
+        }
+        if (t < nz && j >= 0 && j <= N + 1) {   // Top, Bottom (every column)
+            const int js = j == 0 ? 1 : (j == N + 1 ? N : j);
+            const bool edge = (j == 0 || j == N + 1);
+            if (has(M + 1, j) && has(M, js)) {
+                const double v = edge ? dneg(at(M, js)) : at(M, js);
+                at(M + 1, j) = dneg(v);
+            }
+            if (has(0, j) && has(1, js)) {
+                const double v = edge ? dneg(at(1, js)) : at(1, js);
+                at(0, j) = v + 0.0;
+            }
+        }
+    }
+}
+
+// One colour of gauss_seidel! on the tile's inner cells whose four neighbours are loaded;
+// a warp per column, each lane the Q = ceil(lr / 64) cells of its rows 2 (lane + 32 q) +
+// odd, whose loads are all issued before the arithmetic.  fps, fms: connector factors of
+// the tile's rows (local index).
+template <int LR>
+__device__ void tile_gs(double* xs, const double* bs, int nr, int nz, int gr0, int gc0, int M, int N,
+                        const double* fps, const double* fms, int color) {
+    constexpr int Q = (LR / 2 + 31) / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int jj = 1 + warp; jj < nz - 1; jj += kTileWarps) {
+        const int j = gc0 + jj;
+        if (j < 1 || j > N) continue;
+        const int odd = (color ^ (gr0 + j)) & 1;
+        double c[Q], up[Q], rt[Q], dn[Q], lf[Q], bb[Q], f1[Q], f2[Q];
+        bool on[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int ii = 2 * (lane + 32 * q) + odd;
+            const int i = gr0 + ii;
+            on[q] = ii >= 1 && ii < nr - 1 && i >= 1 && i <= M;
+            const int k = on[q] ? ii + jj * LR : LR;   // a loaded cell when off
+            c[q] = xs[k];
+            up[q] = xs[k + 1];
+            rt[q] = xs[k + LR];
+            dn[q] = xs[k - 1];
+            lf[q] = xs[k - LR];
+            bb[q] = bs[k];
+            f1[q] = fps[on[q] ? ii : 0];
+            f2[q] = fms[on[q] ? ii : 0];
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            double s = -4.0 * c[q];
+            s += up[q] * f1[q];
+            s += rt[q];
+            s += dn[q] * f2[q];
+            s += lf[q];
+            if (on[q]) xs[2 * (lane + 32 * q) + odd + jj * LR] = c[q] + 1.0 * (s + bb[q]) / 4.0;
+        }
+    }
+}
+
+template <int NS, int MODE>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_smooth_tile(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mb, TileArgs a) {
+    using S = TileShape<NS>;
+    constexpr int H = S::H, LR = S::LR, CR = S::CR, CZ = S::CZ;
+    extern __shared__ __align__(128) double smem[];
+    double* xs = smem;
+    double* bs = smem + S::SX;
+    double* hs = smem + 2 * S::SX;
+    double* fps = hs + S::SH;
+    double* fms = fps + LR;
+    __shared__ __align__(8) unsigned long long bar;
+    const int M = a.M, N = a.N;
+    const long ld = M + 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ti = blockIdx.x % a.tiles_r, tj = blockIdx.x / a.tiles_r;
+    const int r0 = 1 + ti * kTileR, c0 = 1 + tj * kTileZ;
+    const int r1 = min(r0 + kTileR, M + 1), c1 = min(c0 + kTileZ, N + 1);
+    const int gr0 = r0 - H, gc0 = c0 - H;   // both even: the TMA box starts 16-byte aligned
+    const int nr = (r1 - r0) + 2 * H, nz = (c1 - c0) + 2 * H;
+    const int Mh = M / 2, Nh = N / 2;
+    const long ldh = Mh + 2;
+
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bar)) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t bytes = (MODE == TILE_PRE_SET ? 1u : 2u) * S::box_bytes;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(&bar)), "r"(bytes)
+                     : "memory");
+        tma_tile(bs, &mb, gr0, gc0, &bar);
+        if (MODE != TILE_PRE_SET) tma_tile(xs, &mx, gr0, gc0, &bar);
+    }
+    // the connector factors of the tile's rows and the coarse neighbourhood of the tile for
+    // the interpolation, while the copies fly
+    for (int ii = threadIdx.x; ii < LR; ii += kTileThreads) {
+        const int i = gr0 + ii;
+        const bool in = i >= 0 && i <= M + 1;
+        fps[ii] = in ? __ldg(a.fp + i) : 0.0;
+        fms[ii] = in ? __ldg(a.fm + i) : 0.0;
+    }
+    const int Ilo = ((gr0 >> 1) - 1) & ~1, Jlo = (gc0 >> 1) - 1;
+    if (MODE != TILE_PRE) {
+        for (int jj = warp; jj < CZ; jj += kTileWarps) {
+            const int J = Jlo + jj;
+            for (int ii = lane; ii < CR; ii += 32) {
+                const int I = Ilo + ii;
+                hs[ii + jj * CR] = (I >= 0 && I <= Mh + 1 && J >= 0 && J <= Nh + 1) ? __ldg(a.xh + I + J * ldh) : 0.0;
+            }
+        }
+    }
+    if (!mbar_wait0(&bar)) {
+        if (threadIdx.x == 0) atomicOr(a.status, ST_TIMEOUT);
+        mbar_wait0(&bar);   // the copies in flight land before the CTA leaves
+        return;
+    }
+    if (MODE != TILE_PRE) {
+        __syncthreads();
+        // interpolate! (Multigrid.jl:232-258) into (TILE_PRE_SET) or onto (TILE_POST) x
+        for (int jj = warp; jj < nz; jj += kTileWarps) {
+            const int j = gc0 + jj;
+            for (int ii = lane; ii < nr; ii += 32) {
+                const int i = gr0 + ii;
+                const long k = ii + (long)jj * LR;
+                if (i >= 1 && i <= M && j >= 1 && j <= N) {
+                    const int I = (i + 1) >> 1, J = (j + 1) >> 1;
+                    const int di = 2 * ((i + 1) & 1) - 1, dj = (2 * ((j + 1) & 1) - 1) * CR;
+                    const int kh = (I - Ilo) + (J - Jlo) * CR;
+                    double s = 0.0;
+                    s += (9.0 / 16.0) * hs[kh];
+                    s += (3.0 / 16.0) * hs[kh + dj];
+                    s += (3.0 / 16.0) * hs[kh + di];
+                    s += (1.0 / 16.0) * hs[kh + di + dj];
+                    xs[k] = (MODE == TILE_POST) ? xs[k] + s : s;
+                } else if (MODE == TILE_PRE_SET) {
+                    xs[k] = 0.0;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    for (int sw = 0; sw < NS; ++sw) {
+        tile_bc(xs, LR, nr, nz, gr0, gc0, M, N);
+        __syncthreads();
+        tile_gs<LR>(xs, bs, nr, nz, gr0, gc0, M, N, fps, fms, 0);
+        __syncthreads();
+        tile_gs<LR>(xs, bs, nr, nz, gr0, gc0, M, N, fps, fms, 1);
+        __syncthreads();
+    }
+    if (MODE != TILE_POST) {
+        tile_bc(xs, LR, nr, nz, gr0, gc0, M, N);
+        __syncthreads();
+        // residual! (s = 1) and restrict! over the owned coarse cells
+        const int hr = (r1 - r0) >> 1, hz = (c1 - c0) >> 1;
+        const int I0 = (r0 + 1) >> 1, J0 = (c0 + 1) >> 1;
+        for (int q = warp; q < hz; q += kTileWarps) {
+            const int J = J0 + q;
+            for (int p = lane; p < hr; p += 32) {
+                const int I = I0 + p;
+                double s = 0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {   // children (0,0), (0,1), (1,0), (1,1)
+                    const int i = 2 * I - 1 + (c >> 1), j = 2 * J - 1 + (c & 1);
+                    const long k = (i - gr0) + (long)(j - gc0) * LR;
+                    const double r = 1.0 * bs[k] + lap5(xs, k, LR, fps[i - gr0], fms[i - gr0]);
+                    s += r;
+                }
+                a.rh[I + (long)J * ldh] = 4.0 * s / 4.0;
+            }
+        }
+        if (MODE == TILE_PRE) {
+            // xh .= 0 over the owned coarse cells, coarse ghosts by the edge tiles
+            const int ia = (ti == 0) ? 0 : I0, ib = (r1 == M + 1) ? Mh + 2 : I0 + hr;
+            const int ja = (tj == 0) ? 0 : J0, jb = (c1 == N + 1) ? Nh + 2 : J0 + hz;
+            for (int J = ja + warp; J < jb; J += kTileWarps)
+                for (int I = ia + lane; I < ib; I += 32) a.hzero[I + (long)J * ldh] = 0.0;
+        }
+    }
+    // the owned cells, with the array's ghosts by the edge tiles
+    const int ia = (ti == 0) ? 0 : r0, ib = (r1 == M + 1) ? M + 2 : r1;
+    const int ja = (tj == 0) ? 0 : c0, jb = (c1 == N + 1) ? N + 2 : c1;
+    for (int j = ja + warp; j < jb; j += kTileWarps)
+        for (int i = ia + lane; i < ib; i += 32) a.xout[i + (long)j * ld] = xs[(i - gr0) + (long)(j - gc0) * LR];
+}
+
 // The coarse end of fmg! (Multigrid.jl:400-428): the restrictions below level `small`,
 // the direct solve ws.mat \ btop on the coarsest level, and the FMG stages down to level
 // `small`.
-__global__ void __launch_bounds__(kCtaThreads) k_fmg_tail(MgView V) {
-    const long t0 = threadIdx.x, dt = blockDim.x;
+__device__ void fmg_tail_body(const MgView& V) {
+    const int t0 = threadIdx.x, dt = blockDim.x;
     for (int k = V.small; k < V.levels; ++k) {
         restrict_range(V.lv[k + 1].res, V.lv[k].res, V.lv[k + 1].M, V.lv[k + 1].N, t0, dt);
         __syncthreads();
@@ -319,6 +607,69 @@ __global__ void __launch_bounds__(kCtaThreads) k_fmg_tail(MgView V) {
         __syncthreads();
         vcycle_cta(V, l);
     }
+}
+
+__global__ void __launch_bounds__(kCtaThreads) k_fmg_tail(MgView V) { fmg_tail_body(V); }
+
+// The same two tails with the levels from `small` down held in shared memory: level l's
+// res, res1 and sol arrays and its connector factors at tail_off[l] (each array padded to
+// an even number of doubles), and the level table itself in shared memory, so that only
+// level `small`'s arrays travel to and from HBM.
+__host__ __device__ inline int tail_cells(int M, int N) { return ((M + 2) * (N + 2) + 1) & ~1; }
+__host__ __device__ inline int tail_block(int M, int N) { return 3 * tail_cells(M, N) + ((2 * (M + 2) + 1) & ~1); }
+
+__device__ void copy_range(double* dst, const double* src, int n) {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+}
+
+__device__ void tail_setup(MgView& W, const MgView& V, double* sm, int total) {
+    if (threadIdx.x == 0) {
+        W = V;
+        for (int l = V.small; l <= V.levels; ++l) {
+            const int cp = tail_cells(V.lv[l].M, V.lv[l].N);
+            double* base = sm + V.tail_off[l];
+            W.lv[l].res = base;
+            W.lv[l].res1 = base + cp;
+            W.lv[l].sol = base + 2 * cp;
+            W.lv[l].fp = base + 3 * cp;
+            W.lv[l].fm = base + 3 * cp + (V.lv[l].M + 2);
+        }
+    }
+    zero_range(sm, total, threadIdx.x, blockDim.x);
+    __syncthreads();
+    for (int l = V.small; l <= V.levels; ++l) {
+        const int cp = tail_cells(V.lv[l].M, V.lv[l].N);
+        double* base = sm + V.tail_off[l];
+        copy_range(base + 3 * cp, V.lv[l].fp, V.lv[l].M + 2);
+        copy_range(base + 3 * cp + (V.lv[l].M + 2), V.lv[l].fm, V.lv[l].M + 2);
+    }
+}
+
+__global__ void __launch_bounds__(kCtaThreads) k_vcycle_tail_smem(MgView V, int total) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ MgView W;
+    tail_setup(W, V, sm, total);
+    const LevelView& G = V.lv[V.small];
+    const int n = (G.M + 2) * (G.N + 2);
+    copy_range(sm + V.tail_off[V.small], G.res, n);
+    copy_range(sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), G.sol, n);
+    __syncthreads();
+    vcycle_cta(W, V.small);
+    __syncthreads();
+    copy_range(G.sol, sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), n);
+}
+
+__global__ void __launch_bounds__(kCtaThreads) k_fmg_tail_smem(MgView V, int total) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ MgView W;
+    tail_setup(W, V, sm, total);
+    const LevelView& G = V.lv[V.small];
+    const int n = (G.M + 2) * (G.N + 2);
+    copy_range(sm + V.tail_off[V.small], G.res, n);
+    __syncthreads();
+    fmg_tail_body(W);
+    __syncthreads();
+    copy_range(G.sol, sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), n);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -518,7 +869,15 @@ struct mcs_poisson {
     double* partial = nullptr;
     double* dnorm = nullptr;   // {eps, converged}
     double* hnorm = nullptr;   // pinned copy
+    double* sol2[kMaxLevels + 1] = {};   // second solution buffer of the grid-wide levels
+    // TMA descriptors of the grid-wide levels, for 1 and 2 sweeps (box sizes differ)
+    CUtensorMap map_sol[2][2][kMaxLevels + 1];   // [sweeps - 1][buffer][level]
+    CUtensorMap map_res[2][kMaxLevels + 1];
+    int tail_smem = 0;                            // bytes of the shared-memory tail (0: in HBM)
+    bool fused = false;                   // smooth1, smooth2 in {1, 2}: fused tile kernels
     long long launches = 0;    // kernels launched by this workspace
+    cudaGraphExec_t x_check = nullptr, x_work = nullptr;   // the two halves of fmg!
+    long long n_check = 0, n_work = 0;                     // kernels per replay
     int last_iters[2] = {0, 0};
     double last_eps = 0.0;
 };
@@ -534,6 +893,59 @@ int palloc(mcs_poisson* p, double** out, size_t count) {
     p->allocs.push_back(d);
     *out = static_cast<double*>(d);
     return cudaMemset(d, 0, count * sizeof(double)) == cudaSuccess ? MCS_OK : MCS_ERR_CUDA;
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(f);
+    }
+    return fn;
+}
+
+// A level array as a 2-D FP64 tensor (rows M+2 innermost, N+2 columns) read in boxes of
+// box_r x box_c; reads outside the array return zeros.
+int tensor_map(mcs_poisson* p, CUtensorMap* m, const double* base, int M, int N, int box_r, int box_c) {
+    EncodeTiled enc = encode_tiled();
+    if (!enc) return set_err(p->ctx, MCS_ERR_CUDA, "poisson: cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t dims[2] = {(cuuint64_t)(M + 2), (cuuint64_t)(N + 2)};
+    const cuuint64_t strides[1] = {(cuuint64_t)(M + 2) * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)box_r, (cuuint32_t)box_c};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? MCS_OK : set_err(p->ctx, MCS_ERR_CUDA, "poisson: tensor map encoding failed");
+}
+
+template <int NS>
+int tile_maps(mcs_poisson* p) {
+    using S = TileShape<NS>;
+    for (int l = 0; l < p->small; ++l) {
+        const LevelView& L = p->V.lv[l];
+        if (int e = tensor_map(p, &p->map_sol[NS - 1][0][l], L.sol, L.M, L.N, S::LR, S::LZ)) return e;
+        if (int e = tensor_map(p, &p->map_sol[NS - 1][1][l], p->sol2[l], L.M, L.N, S::LR, S::LZ)) return e;
+        if (int e = tensor_map(p, &p->map_res[NS - 1][l], L.res, L.M, L.N, S::LR, S::LZ)) return e;
+    }
+    const void* fns[3] = {(const void*)k_smooth_tile<NS, TILE_PRE>, (const void*)k_smooth_tile<NS, TILE_PRE_SET>,
+                          (const void*)k_smooth_tile<NS, TILE_POST>};
+    for (const void* f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem) != cudaSuccess)
+            return set_err(p->ctx, MCS_ERR_CUDA, "poisson: shared memory attribute failed");
+    return MCS_OK;
+}
+
+int tile_setup(mcs_poisson* p) {
+    if (int e = tile_maps<1>(p)) return e;
+    return tile_maps<2>(p);
 }
 
 int use_dev(mcs_poisson* p) {
@@ -593,8 +1005,24 @@ void coarse_inverse(int Mc, int Nc, std::vector<double>& inv) {
 
 #define PSN_LAUNCH(p) MCS_CK((p)->ctx, cudaGetLastError())
 
-int smooth_grid(mcs_poisson* p, const LevelView& L, const double* b, int n) {
-    cudaStream_t st = p->ctx->stream;
+// The one-CTA tails: mgv! from level `small`, and the coarse end of fmg!.
+void launch_vtail(mcs_poisson* p, cudaStream_t st) {
+    ++p->launches;
+    if (p->tail_smem)
+        k_vcycle_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(p->V, p->tail_smem / (int)sizeof(double));
+    else
+        k_vcycle_cta<<<1, kCtaThreads, 0, st>>>(p->V, p->small);
+}
+
+void launch_ftail(mcs_poisson* p, cudaStream_t st) {
+    ++p->launches;
+    if (p->tail_smem)
+        k_fmg_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(p->V, p->tail_smem / (int)sizeof(double));
+    else
+        k_fmg_tail<<<1, kCtaThreads, 0, st>>>(p->V);
+}
+
+int smooth_grid(mcs_poisson* p, const LevelView& L, const double* b, int n, cudaStream_t st) {
     const long hm = (long)((L.M + 1) >> 1) * L.N;
     for (int it = 0; it < n; ++it) {
         ++p->launches;
@@ -610,13 +1038,12 @@ int smooth_grid(mcs_poisson* p, const LevelView& L, const double* b, int n) {
 
 // mgv! from level l0 (< small) down: grid-wide kernels above `small`, the one-CTA
 // V-cycle from `small` on.
-int vcycle(mcs_poisson* p, int l0) {
-    cudaStream_t st = p->ctx->stream;
+int vcycle(mcs_poisson* p, int l0, cudaStream_t st) {
     const MgView& V = p->V;
     for (int l = l0; l < p->small; ++l) {
         const LevelView& L = V.lv[l];
         const LevelView& H = V.lv[l + 1];
-        if (int e = smooth_grid(p, L, L.res, V.smooth1)) return e;
+        if (int e = smooth_grid(p, L, L.res, V.smooth1, st)) return e;
         ++p->launches;
         k_bc<<<grid_blocks(p, std::max(L.M + 1, L.N + 2)), kThreads, 0, st>>>(L.sol, L.M, L.N);
         ++p->launches;
@@ -626,25 +1053,112 @@ int vcycle(mcs_poisson* p, int l0) {
         k_restrict<<<grid_blocks(p, (long)H.M * H.N), kThreads, 0, st>>>(H.res, L.res1, H.M, H.N);
         MCS_CK(p->ctx, cudaMemsetAsync(H.sol, 0, cells_of(H.M, H.N) * sizeof(double), st));
     }
-    ++p->launches;
-    k_vcycle_cta<<<1, kCtaThreads, 0, st>>>(V, p->small);
+    launch_vtail(p, st);
     for (int l = p->small - 1; l >= l0; --l) {
         const LevelView& L = V.lv[l];
         const LevelView& H = V.lv[l + 1];
         ++p->launches;
         k_interp<<<grid_blocks(p, (long)H.M * H.N), kThreads, 0, st>>>(L.sol, H.sol, H.M, H.N, 1);
-        if (int e = smooth_grid(p, L, L.res, V.smooth2)) return e;
+        if (int e = smooth_grid(p, L, L.res, V.smooth2, st)) return e;
     }
     PSN_LAUNCH(p);
     return MCS_OK;
 }
 
-// fmg! (Multigrid.jl:380-434) on u, b.  *cont = false once the residual is below
-// s * tolerance (nothing else is done then).
-int fmg(mcs_poisson* p, bool* cont) {
-    cudaStream_t st = p->ctx->stream;
+// Which buffer holds each grid-wide level's solution while a graph is recorded; the
+// recorded pointers then follow the same hand-offs on every replay.
+struct Buffers {
+    int cur[kMaxLevels + 1] = {};
+};
+
+double* sol_buf(mcs_poisson* p, const Buffers& B, int l) {
+    return (l < p->small && B.cur[l]) ? p->sol2[l] : p->V.lv[l].sol;
+}
+
+template <int NS, int MODE>
+void launch_tile(mcs_poisson* p, int l, int xbuf, const TileArgs& a, cudaStream_t st) {
+    using S = TileShape<NS>;
+    const int tr = (a.M + kTileR - 1) / kTileR, tz = (a.N + kTileZ - 1) / kTileZ;
+    TileArgs b = a;
+    b.tiles_r = tr;
+    ++p->launches;
+    k_smooth_tile<NS, MODE><<<tr * tz, kTileThreads, S::smem, st>>>(p->map_sol[NS - 1][xbuf][l],
+                                                                      p->map_res[NS - 1][l], b);
+}
+
+// One fused step at level l: TILE_PRE / TILE_PRE_SET (smooth1 sweeps) or TILE_POST
+// (smooth2 sweeps); hands level l's solution to its other buffer.
+void tile_step(mcs_poisson* p, Buffers& B, int l, int mode, cudaStream_t st) {
+    const LevelView& L = p->V.lv[l];
+    TileArgs a{};
+    const int xin = B.cur[l];
+    B.cur[l] ^= 1;
+    a.xout = sol_buf(p, B, l);
+    a.xh = sol_buf(p, B, l + 1);
+    a.rh = p->V.lv[l + 1].res;
+    a.hzero = sol_buf(p, B, l + 1);
+    a.fp = L.fp;
+    a.fm = L.fm;
+    a.status = p->ctx->d_status;
+    a.M = L.M;
+    a.N = L.N;
+    const int ns = mode == TILE_POST ? p->smooth2 : p->smooth1;
+    if (ns == 1) {
+        if (mode == TILE_PRE) launch_tile<1, TILE_PRE>(p, l, xin, a, st);
+        else if (mode == TILE_PRE_SET) launch_tile<1, TILE_PRE_SET>(p, l, xin, a, st);
+        else launch_tile<1, TILE_POST>(p, l, xin, a, st);
+    } else {
+        if (mode == TILE_PRE) launch_tile<2, TILE_PRE>(p, l, xin, a, st);
+        else if (mode == TILE_PRE_SET) launch_tile<2, TILE_PRE_SET>(p, l, xin, a, st);
+        else launch_tile<2, TILE_POST>(p, l, xin, a, st);
+    }
+}
+
+// mgv! from level l0 (< small) with the fused kernels; `set` = the FMG stage entry, whose
+// level-l0 solution starts as the interpolation of the next coarser one.
+int vcycle_fused(mcs_poisson* p, Buffers& B, int l0, bool set, cudaStream_t st) {
+    for (int l = l0; l < p->small; ++l) {
+        const bool first_set = set && l == l0;
+        tile_step(p, B, l, first_set ? TILE_PRE_SET : TILE_PRE, st);
+        if (first_set) {
+            const LevelView& H = p->V.lv[l + 1];
+            MCS_CK(p->ctx, cudaMemsetAsync(sol_buf(p, B, l + 1), 0, cells_of(H.M, H.N) * sizeof(double), st));
+        }
+    }
+    launch_vtail(p, st);
+    for (int l = p->small - 1; l >= l0; --l) tile_step(p, B, l, TILE_POST, st);
+    PSN_LAUNCH(p);
+    return MCS_OK;
+}
+
+int fmg_work_fused(mcs_poisson* p, cudaStream_t st) {
     const MgView& V = p->V;
-    const LevelView& F = V.lv[0];
+    Buffers B;
+    for (int k = 0; k < p->small; ++k) {
+        ++p->launches;
+        k_restrict<<<grid_blocks(p, (long)V.lv[k + 1].M * V.lv[k + 1].N), kThreads, 0, st>>>(
+            V.lv[k + 1].res, V.lv[k].res, V.lv[k + 1].M, V.lv[k + 1].N);
+    }
+    launch_ftail(p, st);
+    for (int l = p->small - 1; l >= 0; --l) {
+        const LevelView& H = V.lv[l + 1];
+        ++p->launches;
+        k_bc<<<grid_blocks(p, std::max(H.M + 1, H.N + 2)), kThreads, 0, st>>>(sol_buf(p, B, l + 1), H.M, H.N);
+        if (int e = vcycle_fused(p, B, l, true, st)) return e;
+    }
+    const long n = (long)cells_of(p->M, p->N);
+    ++p->launches;
+    k_add<<<grid_blocks(p, n), kThreads, 0, st>>>(p->u, sol_buf(p, B, 0), n);
+    ++p->launches;
+    k_bc<<<grid_blocks(p, std::max(p->M + 1, p->N + 2)), kThreads, 0, st>>>(p->u, p->M, p->N);
+    PSN_LAUNCH(p);
+    return MCS_OK;
+}
+
+// The test at the top of fmg! (Multigrid.jl:384-398): apply!, the residual s b + L u and
+// its RMS, copied to the pinned {eps, converged} pair.
+int fmg_check(mcs_poisson* p, cudaStream_t st) {
+    const LevelView& F = p->V.lv[0];
     ++p->launches;
     k_bc<<<grid_blocks(p, std::max(p->M + 1, p->N + 2)), kThreads, 0, st>>>(p->u, p->M, p->N);
     ++p->launches;
@@ -655,20 +1169,20 @@ int fmg(mcs_poisson* p, bool* cont) {
                                             p->s * p->tol, p->dnorm);
     PSN_LAUNCH(p);
     MCS_CK(p->ctx, cudaMemcpyAsync(p->hnorm, p->dnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    MCS_CK(p->ctx, cudaStreamSynchronize(st));
-    p->last_eps = p->hnorm[0];
-    if (p->hnorm[1] != 0.0) {
-        *cont = false;
-        return MCS_OK;
-    }
-    *cont = true;
+    return MCS_OK;
+}
+
+// The rest of fmg! (Multigrid.jl:400-433): restrictions, the coarsest direct solve, the
+// FMG stages with their V-cycles, u += correction, apply!.
+int fmg_work(mcs_poisson* p, cudaStream_t st) {
+    const MgView& V = p->V;
+    const LevelView& F = V.lv[0];
     for (int k = 0; k < p->small; ++k) {
         ++p->launches;
         k_restrict<<<grid_blocks(p, (long)V.lv[k + 1].M * V.lv[k + 1].N), kThreads, 0, st>>>(
             V.lv[k + 1].res, V.lv[k].res, V.lv[k + 1].M, V.lv[k + 1].N);
     }
-    ++p->launches;
-    k_fmg_tail<<<1, kCtaThreads, 0, st>>>(V);
+    launch_ftail(p, st);
     for (int l = p->small - 1; l >= 0; --l) {
         const LevelView& L = V.lv[l];
         const LevelView& H = V.lv[l + 1];
@@ -677,7 +1191,7 @@ int fmg(mcs_poisson* p, bool* cont) {
         k_bc<<<grid_blocks(p, std::max(H.M + 1, H.N + 2)), kThreads, 0, st>>>(H.sol, H.M, H.N);
         ++p->launches;
         k_interp<<<grid_blocks(p, (long)H.M * H.N), kThreads, 0, st>>>(L.sol, H.sol, H.M, H.N, 0);
-        if (int e = vcycle(p, l)) return e;
+        if (int e = vcycle(p, l, st)) return e;
     }
     const long n = (long)cells_of(p->M, p->N);
     ++p->launches;
@@ -686,6 +1200,56 @@ int fmg(mcs_poisson* p, bool* cont) {
     k_bc<<<grid_blocks(p, std::max(p->M + 1, p->N + 2)), kThreads, 0, st>>>(p->u, p->M, p->N);
     PSN_LAUNCH(p);
     return MCS_OK;
+}
+
+// Records `fn` into a graph (on a private stream: the context's stream may be the legacy
+// one, which cannot be captured) and counts the kernels one replay launches.
+template <typename Fn>
+int capture(mcs_poisson* p, Fn fn, cudaGraphExec_t* exec, long long* nlaunch) {
+    cudaStream_t cs;
+    MCS_CK(p->ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    const long long before = p->launches;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int st = e == cudaSuccess ? fn(cs) : MCS_ERR_CUDA;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    *nlaunch = p->launches - before;
+    p->launches = before;
+    if (st || e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return st ? st : set_err(p->ctx, MCS_ERR_CUDA, "poisson: graph capture failed");
+    }
+    e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_err(p->ctx, MCS_ERR_CUDA, "poisson: graph instantiate failed");
+    return MCS_OK;
+}
+
+int replay(mcs_poisson* p, cudaGraphExec_t exec, long long nlaunch) {
+    p->launches += nlaunch;
+    MCS_CK(p->ctx, cudaGraphLaunch(exec, p->ctx->stream));
+    return MCS_OK;
+}
+
+// fmg! (Multigrid.jl:380-434) on u, b.  *cont = false once the residual is below
+// s * tolerance (nothing else is done then).  Both halves replay CUDA graphs.
+int fmg(mcs_poisson* p, bool* cont) {
+    if (!p->x_check) {
+        if (int e = capture(p, [&](cudaStream_t s) { return fmg_check(p, s); }, &p->x_check, &p->n_check)) return e;
+        if (int e = capture(p, [&](cudaStream_t s) { return p->fused ? fmg_work_fused(p, s) : fmg_work(p, s); },
+                            &p->x_work, &p->n_work))
+            return e;
+    }
+    if (int e = replay(p, p->x_check, p->n_check)) return e;
+    MCS_CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
+    p->last_eps = p->hnorm[0];
+    if (p->hnorm[1] != 0.0) {
+        *cont = false;
+        return MCS_OK;
+    }
+    *cont = true;
+    return replay(p, p->x_work, p->n_work);
 }
 
 // Multigrid.solve (Multigrid.jl:449-467): fmg! while it reports work and iter <= maxiter.
@@ -748,6 +1312,8 @@ MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2
     const int M = gv.M, N = gv.N;
     if (levels < 0 || levels > kMaxLevels || smooth1 < 0 || smooth2 < 0 || maxiter < 0 || !(tolerance >= 0))
         return set_err(c, MCS_ERR_ARG, "poisson: bad multigrid configuration");
+    if ((long)(M + 3) * (N + 3) >= (1L << 31))
+        return set_err(c, MCS_ERR_ARG, "poisson: grid above 2^31 cells");
     if (M < 2 || N < 2 || ((M >> levels) << levels) != M || ((N >> levels) << levels) != N)
         return set_err(c, MCS_ERR_ARG, "poisson: M and N must be multiples of 2^levels (and >= 2)");
     const int Mc = M >> levels, Nc = N >> levels;
@@ -778,10 +1344,37 @@ MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2
     p->V.levels = levels;
     p->V.smooth1 = smooth1;
     p->V.smooth2 = smooth2;
+    // The tail (levels small..levels) runs in one CTA: from shared memory when the three
+    // arrays of all its levels fit (the finest such split), else from HBM for the levels
+    // of at most kSmallCells cells.
     p->small = levels;
-    for (int l = 0; l <= levels; ++l)
-        if ((long)(M >> l) * (N >> l) <= kSmallCells) { p->small = l; break; }
+    p->tail_smem = 0;
+    for (int l = 0; l <= levels; ++l) {
+        long tot = 0;
+        for (int k = l; k <= levels; ++k) tot += tail_block(M >> k, N >> k);
+        if (tot * (long)sizeof(double) <= kTailSmemBytes) {
+            p->small = l;
+            p->tail_smem = (int)(tot * sizeof(double));
+            long off = 0;
+            for (int k = l; k <= levels; ++k) {
+                p->V.tail_off[k] = (int)off;
+                off += tail_block(M >> k, N >> k);
+            }
+            break;
+        }
+    }
+    if (!p->tail_smem)
+        for (int l = 0; l <= levels; ++l)
+            if ((long)(M >> l) * (N >> l) <= kSmallCells) { p->small = l; break; }
     p->V.small = p->small;
+    if (p->tail_smem &&
+        (cudaFuncSetAttribute(k_vcycle_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, p->tail_smem) !=
+             cudaSuccess ||
+         cudaFuncSetAttribute(k_fmg_tail_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, p->tail_smem) !=
+             cudaSuccess)) {
+        delete p;
+        return set_err(c, MCS_ERR_CUDA, "poisson: shared memory attribute failed");
+    }
     std::vector<double> tab;
     for (int l = 0; l <= levels; ++l) {
         LevelView& Lv = p->V.lv[l];
@@ -805,6 +1398,12 @@ MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2
             return fail(set_err(c, MCS_ERR_CUDA, "poisson: upload failed"));
         Lv.fp = fpm;
         Lv.fm = fpm + Lv.M + 2;
+    }
+    p->fused = smooth1 >= 1 && smooth1 <= 2 && smooth2 >= 1 && smooth2 <= 2;
+    if (p->fused) {
+        for (int l = 0; l < p->small; ++l)
+            if ((e = palloc(p, &p->sol2[l], cells_of(M >> l, N >> l)))) return fail(e);
+        if ((e = tile_setup(p))) return fail(e);
     }
     std::vector<double> inv;
     coarse_inverse(Mc, Nc, inv);
@@ -838,6 +1437,8 @@ MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2
 MCS_API int mcs_poisson_destroy(mcs_poisson* p) {
     if (!p) return MCS_ERR_ARG;
     if (p->ctx && p->ctx->stream) cudaStreamSynchronize(p->ctx->stream);
+    if (p->x_check) cudaGraphExecDestroy(p->x_check);
+    if (p->x_work) cudaGraphExecDestroy(p->x_work);
     for (void* a : p->allocs) cudaFree(a);
     if (p->hnorm) cudaFreeHost(p->hnorm);
     delete p;
@@ -928,6 +1529,7 @@ MCS_API int mcs_poisson_mg_solve(mcs_poisson* p, int* iters, double* eps_last) {
     if (int e = use_dev(p)) return e;
     int it = 0;
     if (int e = mg_solve(p, &it)) return e;
+    if (int e = sync_status(p->ctx)) return e;
     if (iters) *iters = it;
     if (eps_last) *eps_last = p->last_eps;
     return MCS_OK;
@@ -938,6 +1540,7 @@ MCS_API int mcs_poisson_solve_freebc(mcs_poisson* p, int* iters) {
     if (int e = use_dev(p)) return e;
     int it[2] = {0, 0};
     if (int e = freebc(p, it)) return e;
+    if (int e = sync_status(p->ctx)) return e;
     if (iters) { iters[0] = it[0]; iters[1] = it[1]; }
     return MCS_OK;
 }
@@ -971,8 +1574,7 @@ MCS_API int mcs_poisson_run(mcs_poisson* p, double eb, int* iters) {
     if (int e = mcs_poisson_assemble(p)) return e;
     if (int e = mcs_poisson_solve_freebc(p, iters)) return e;
     if (int e = mcs_poisson_fields(p, eb)) return e;
-    MCS_CK(p->ctx, cudaStreamSynchronize(p->ctx->stream));
-    return MCS_OK;
+    return sync_status(p->ctx);
 }
 
 }  // extern "C"

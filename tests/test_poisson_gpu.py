@@ -14,9 +14,9 @@ from oracle import poisson_ref as P
 from tests.helpers import broad
 
 # (M, N, levels): all in the one-CTA kernels, an odd coarsest level (3 x 20, the ratio of
-# the reference's 1536 x 10240 sample at 9 levels), and grids whose finest one or two
-# levels run grid-wide.
-CASES = [(32, 64, 3), (48, 320, 4), (64, 256, 4), (256, 512, 5), (512, 1024, 6)]
+# the reference's 1536 x 10240 sample at 9 levels), grids whose finest one or two levels
+# run grid-wide, and one whose grid-wide levels end in partial tiles along r and z.
+CASES = [(32, 64, 3), (48, 320, 4), (64, 256, 4), (256, 512, 5), (512, 1024, 6), (320, 1056, 5)]
 
 
 def _geometry(M, N):
@@ -84,6 +84,23 @@ def test_converged_solve_matches_oracle(solver, M, N, levels):
     ito, epso = P.mg_solve(P.default_conf(*_geometry(M, N), M, N, levels=levels), uo, b)
     assert it == ito and it >= 2
     assert eps == pytest.approx(epso, rel=1e-6)
+    assert _rel(s.u, uo) < 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("smooth1,smooth2", [(1, 1), (1, 2), (2, 1), (3, 3)])
+def test_smoothing_counts_match_oracle(solver, smooth1, smooth2):
+    """1 or 2 sweeps take the fused tile kernels, 3 the per-operation kernels."""
+    M, N, levels = 320, 1056, 5
+    s = solver(M, N, levels, smooth1=smooth1, smooth2=smooth2, tolerance=0.0, maxiter=1)
+    b = _rhs(M, N, 17)
+    s.set_q(b)
+    it, _ = s.solve()
+    uo = P.cells(M, N)
+    conf = P.default_conf(*_geometry(M, N), M, N, levels=levels, tolerance=0.0, maxiter=1, smooth1=smooth1,
+                          smooth2=smooth2)
+    ito, _ = P.mg_solve(conf, uo, b)
+    assert it == ito == 2
     assert _rel(s.u, uo) < 1e-12
 
 
