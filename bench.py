@@ -894,6 +894,13 @@ def run_serve(args):
 POISSON_METRIC = "poisson solves/s"
 
 
+def poisson_alg_bytes_tile(M: int, N: int) -> float:
+    """Algorithmic HBM bytes of one fused post-smoothing launch over M x N cells: the level's
+    solution and right-hand side read once (8 + 8 B per cell), the next coarser solution
+    read once (2 B per fine cell) and the smoothed solution written once (8 B per cell)."""
+    return 26.0 * M * N
+
+
 def poisson_alg_bytes_gs(M: int, N: int) -> float:
     """Algorithmic HBM bytes of one red-black pass over M x N cells: the potential read
     once (8 B per cell: every cell is a neighbour of the updated colour), the right-hand
@@ -997,10 +1004,10 @@ def run_poisson(args):
         total_ms = float(t.item())
     ms = total_ms / args.steps
     value = ws * 1e3 / ms
-    gs_ms, res_ms = solver.profile(20)
+    gs_ms, res_ms, tile_ms = solver.profile(20)
     pk, src = peaks()
     hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
-    ach = poisson_alg_bytes_gs(spec.M, spec.N) / (gs_ms * 1e-3) / 1e9
+    ach = poisson_alg_bytes_tile(spec.M, spec.N) / (tile_ms * 1e-3) / 1e9
 
     # end to end: host int64 charges in, host face fields out, pinned buffers
     nq = (spec.M + 2) * (spec.N + 2)
@@ -1038,10 +1045,13 @@ def run_poisson(args):
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": poisson_config(spec, {"fmg_calls_per_solve": it_set}),
-        "roofline": {"kernel": "k_gs (one red-black pass, finest level)", "bound": "hbm", "achieved": ach,
-                     "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
-                     "peak_source": src, "launch_ms": gs_ms, "residual_launch_ms": res_ms,
-                     "alg_bytes_per_launch": poisson_alg_bytes_gs(spec.M, spec.N)},
+        "roofline": {"kernel": "k_smooth_tile<2, TILE_POST> (interpolation + 2 red-black sweeps, finest level)",
+                     "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": None, "peak_source": src, "launch_ms": tile_ms,
+                     "alg_bytes_per_launch": poisson_alg_bytes_tile(spec.M, spec.N),
+                     "unfused_k_gs_launch_ms": gs_ms,
+                     "unfused_k_gs_gbs": poisson_alg_bytes_gs(spec.M, spec.N) / (gs_ms * 1e-3) / 1e9,
+                     "residual_norm_launch_ms": res_ms},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_v, "unit": "solves/s", "h2d_bytes_per_step": 2 * nq * 8, "d2h_bytes_per_step": nf * 8,
                 "path": "mcs_grid_write_fixed (qfixed, qpart from pinned host) -> mcs_poisson_run -> "

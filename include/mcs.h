@@ -359,10 +359,11 @@ MCS_API int mcs_poisson_download(mcs_poisson* p, int which, double* host);
 MCS_API int mcs_poisson_launches(mcs_poisson* p, int64_t* count);
 /* Zero u (MCS_PSN_U) or b (MCS_PSN_B) on the device. */
 MCS_API int mcs_poisson_zero(mcs_poisson* p, int which);
-/* Mean device time (ms) of one finest-level red-black pass and of one finest-level
- * residual, each launched `reps` times between CUDA events on the context's stream, on
- * scratch levels (u and b untouched). */
-MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* residual_ms);
+/* Mean device time (ms) of one finest-level red-black pass, of one finest-level residual
+ * and of one fused finest-level post-smoothing (interpolation + smooth2 sweeps; 0 when the
+ * fused kernels are not in use), each launched `reps` times between CUDA events on the
+ * context's stream, on scratch levels (u and b untouched). */
+MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* residual_ms, float* tile_ms);
 /* Multigrid.solve(mg, u, b, ws) on the device-resident u, b: fmg! calls in *iters, the
  * last residual RMS in *eps_last (either may be NULL). */
 MCS_API int mcs_poisson_mg_solve(mcs_poisson* p, int* iters, double* eps_last);

@@ -126,7 +126,7 @@ SIGNATURES = {
     "mcs_freebc_coefficients": (i32, [f64, f64, i32, pd]),
     "mcs_poisson_zero": (i32, [vp, i32]),
     "mcs_poisson_launches": (i32, [vp, pi64]),
-    "mcs_poisson_profile": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "mcs_poisson_profile": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "mcs_grid_write_fixed": (i32, [vp, i32, pi64]),
 }
 

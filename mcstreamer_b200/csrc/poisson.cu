@@ -12,7 +12,6 @@
 // i = 0, M+1 and j = 0, N+1 (element (i, j) at i + j*(M+2)).  Level l has M >> l by N >> l
 // cells.  Levels of at most kSmallCells cells run inside one CTA (their kernels would be
 // launch-bound); the rest run one grid-wide kernel per operation.
-#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -50,7 +49,6 @@ struct LevelView {
 
 struct MgView {
     int levels, smooth1, smooth2, small;
-    int tail_off[kMaxLevels + 1];   // shared-memory offset (doubles) of a tail level's arrays
     int nc;
     const double* ainv;   // inverse of the coarsest Cartesian matrix, nc x nc row-major
     LevelView lv[kMaxLevels + 1];
@@ -66,7 +64,7 @@ __device__ __forceinline__ double dneg(double v) { return -v + 0.0; }   // coef 
 // (Top, Dirichlet), (Bottom, Neumann)).  Left/Right fill the inner rows; Top/Bottom then
 // fill every column, so the corners take Top/Bottom of the Left/Right ghosts.  No thread
 // reads a value that another one writes.
-__device__ void bc_range(double* a, int M, int N, int t0, int dt) {
+__device__ __forceinline__ void bc_range(double* a, int M, int N, int t0, int dt) {
     const long ld = M + 2;
     const int n = max(M + 1, N + 2);
     for (int t = t0; t < n; t += dt) {
@@ -106,7 +104,7 @@ __device__ __forceinline__ double lap5(const double* u, long k, long ld, double 
 // One pass of gauss_seidel! (Multigrid.jl:168-178, redblack.jl:38-46): in column j the
 // rows 1, 3, ... <= M shifted by parity xor (j even).  An odd M (possible on the coarsest
 // level only) shifts into the ghost row M+1, which the reference updates too.
-__device__ void gs_range(double* u, const double* b, const double* fp, const double* fm, int M, int N,
+__device__ __forceinline__ void gs_range(double* u, const double* b, const double* fp, const double* fm, int M, int N,
                          int parity, int t0, int dt) {
     const long ld = M + 2;
     const int hm = (M + 1) >> 1;
@@ -121,7 +119,7 @@ __device__ void gs_range(double* u, const double* b, const double* fp, const dou
 }
 
 // residual! (Multigrid.jl:186-193): r = s b + L u on the inner cells.
-__device__ void residual_range(double* r, const double* u, const double* b, double s, const double* fp,
+__device__ __forceinline__ void residual_range(double* r, const double* u, const double* b, double s, const double* fp,
                                const double* fm, int M, int N, int t0, int dt) {
     const long ld = M + 2;
     const int n = M * N;
@@ -135,7 +133,7 @@ __device__ void residual_range(double* r, const double* u, const double* b, doub
 
 // restrict! (Multigrid.jl:213-226): coarse (I, J) = 4 * (sum of the children in the order
 // (0,0), (0,1), (1,0), (1,1)) / 4.  M, N are the coarse sizes.
-__device__ void restrict_range(double* h, const double* f, int M, int N, int t0, int dt) {
+__device__ __forceinline__ void restrict_range(double* h, const double* f, int M, int N, int t0, int dt) {
     const long ldh = M + 2, ldf = 2 * M + 2;
     const int n = M * N;
     for (int t = t0; t < n; t += dt) {
@@ -153,7 +151,7 @@ __device__ void restrict_range(double* h, const double* f, int M, int N, int t0,
 
 // interpolate! (Multigrid.jl:232-258): fine child s of (I, J) = sum over sh of w(sh) *
 // coarse[(I, J) + (2s - 1) .* sh], w = 9/16, 3/16, 3/16, 1/16; added or stored.
-__device__ void interp_range(double* f, const double* h, int M, int N, bool add, int t0, int dt) {
+__device__ __forceinline__ void interp_range(double* f, const double* h, int M, int N, bool add, int t0, int dt) {
     const long ldh = M + 2, ldf = 2 * M + 2;
     const int n = M * N;
     for (int t = t0; t < n; t += dt) {
@@ -176,7 +174,7 @@ __device__ void interp_range(double* f, const double* h, int M, int N, bool add,
     }
 }
 
-__device__ void zero_range(double* a, int n, int t0, int dt) {
+__device__ __forceinline__ void zero_range(double* a, int n, int t0, int dt) {
     for (int t = t0; t < n; t += dt) a[t] = 0.0;
 }
 
@@ -215,22 +213,21 @@ __device__ double block_sum(double v, double* sh) {
     return r;
 }
 
-// fmg!'s residual (Multigrid.jl:386-391) with the sum of squares of each block.
+// fmg!'s residual (Multigrid.jl:386-391) with the sum of squares of each block: a block
+// takes columns blockIdx.x + 1, + gridDim.x, ..., its threads the rows.
 __global__ void __launch_bounds__(kThreads) k_residual_norm(double* r, const double* u, const double* b, double s,
                                                            const double* fp, const double* fm, int M, int N,
                                                            double* partial) {
     __shared__ double sh[kThreads];
     const long ld = M + 2;
-    const long n = (long)M * N;
     double acc = 0.0;
-    for (long t = gtid(); t < n; t += gthreads()) {
-        const int j = 1 + (int)(t / M);
-        const int i = 1 + (int)(t - (long)(j - 1) * M);
-        const long k = i + j * ld;
-        const double v = s * b[k] + lap5(u, k, ld, fp[i], fm[i]);
-        r[k] = v;
-        acc = acc + v * v;
-    }
+    for (int j = 1 + blockIdx.x; j <= N; j += gridDim.x)
+        for (int i = 1 + threadIdx.x; i <= M; i += kThreads) {
+            const long k = i + j * ld;
+            const double v = s * b[k] + lap5(u, k, ld, __ldg(fp + i), __ldg(fm + i));
+            r[k] = v;
+            acc = acc + v * v;
+        }
     const double tot = block_sum(acc, sh);
     if (threadIdx.x == 0) partial[blockIdx.x] = tot;
 }
@@ -317,72 +314,70 @@ __global__ void __launch_bounds__(kCtaThreads) k_vcycle_cta(MgView V, int l0) { 
 // ---------------------------------------------------------------------------------------
 // Fused smoothing on the grid-wide levels (even M).  One CTA owns kTileR x kTileZ inner
 // cells and holds them in shared memory with a halo of H = 2 NS + 1 cells, enough for
-// NS red-black sweeps (each half-sweep consumes one cell of halo) plus the residual's
-// stencil, so NS sweeps of the whole level need one read and one write of it.  Every value
-// a CTA writes depends only on cells inside its halo and is computed with the arithmetic
-// of the per-operation kernels above, so the result is the same bit for bit.
+// NS red-black sweeps (half-sweep h only updates the cells h or more away from the loaded
+// edge, the ones whose result is still exact) plus the residual's stencil, so NS sweeps of
+// the whole level cost one read and one write of it.  Every value a CTA writes depends
+// only on cells inside its halo and is computed with the arithmetic of the per-operation
+// kernels above, so the result is the same bit for bit.
 //   TILE_PRE:     x = NS x (apply!, red, black); apply!; r = b + L x; rh = restrict(r);
 //                 the next level's solution cleared (mgv! before its recursion).
 //   TILE_PRE_SET: the same with x = interpolate(xh) first (an FMG stage entering mgv!).
 //   TILE_POST:    x += interpolate(xh); NS x (apply!, red, black) (mgv! after it).
-// A launch reads xin and writes xout (tiles read each other's halo, so not in place).
+// In shared memory each column of the tile is split by row parity (local row ii = 2 m +
+// parity at parity * PL + column * LH + m), so a colour pass reads every operand at unit
+// stride; cp.async gathers the tile into that layout (zero outside the array).  A launch
+// reads xin and writes xout (tiles read each other's halo, so not in place).
 // ---------------------------------------------------------------------------------------
 constexpr int kTileR = 128, kTileZ = 32, kTileThreads = 256, kTileWarps = kTileThreads / 32;
-constexpr uint32_t kWaitSpins = 1u << 22;   // bound of every mbarrier wait
 enum { TILE_PRE = 0, TILE_PRE_SET = 1, TILE_POST = 2 };
 
 struct TileArgs {
+    const double* xin;   // current solution of the level (unused by TILE_PRE_SET)
     double* xout;
+    const double* b;     // right-hand side of the level
     const double* xh;    // next coarser solution (TILE_PRE_SET, TILE_POST)
     double* rh;          // next coarser right-hand side (TILE_PRE, TILE_PRE_SET)
     double* hzero;       // next coarser solution to clear (TILE_PRE)
     const double* fp;
     const double* fm;
-    uint32_t* status;
     int M, N, tiles_r;
 };
 
 template <int NS>
 struct TileShape {
     static constexpr int H = 2 * NS + 1;                 // halo
-    static constexpr int LR = kTileR + 2 * H;            // loaded rows (TMA box, 16-byte multiple)
+    static constexpr int LR = kTileR + 2 * H;            // loaded rows (even)
     static constexpr int LZ = kTileZ + 2 * H;            // loaded columns
-    static constexpr int CR = ((LR / 2 + 4) + 1) & ~1;   // coarse rows for the interpolation
+    static constexpr int LH = LR / 2;                    // rows of one parity per column
+    static constexpr int PL = LH * LZ;                   // doubles per parity plane
+    static constexpr int CR = LR / 2 + 4;                // coarse rows for the interpolation
     static constexpr int CZ = LZ / 2 + 3;
-    static constexpr int SX = (LR * LZ + 15) & ~15;      // doubles per fine array, 128-byte padded
+    static constexpr int SX = (2 * PL + 15) & ~15;       // doubles per fine array
     static constexpr int SH = (CR * CZ + 15) & ~15;
-    static constexpr int SF = (2 * LR + 15) & ~15;        // connector factors of the rows
+    static constexpr int SF = (2 * LR + 15) & ~15;       // connector factors: fp even, odd, fm even, odd
     static constexpr size_t smem = sizeof(double) * (size_t)(2 * SX + SH + SF);
-    static constexpr uint32_t box_bytes = sizeof(double) * LR * LZ;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// Bounded wait on phase 0 of an mbarrier; false when the bound ran out.
-__device__ __forceinline__ bool mbar_wait0(unsigned long long* bar) {
-    const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < kWaitSpins; ++it) {
-        uint32_t done;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
-                     " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(a) : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// One 2-D tile of a level array into shared memory (TMA, zero fill outside the array).
-__device__ __forceinline__ void tma_tile(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                 :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+// 8 bytes global -> shared without passing through registers; zeros when !valid.
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(smem_u32(dst)), "l"(src), "r"(valid ? 8 : 0)
                  : "memory");
 }
 
+template <class S>
+__device__ __forceinline__ int sidx(int ii, int jj) {
+    return (ii & 1) * S::PL + jj * S::LH + (ii >> 1);
+}
+
 // apply! on the ghost cells of the array that lie in the tile: local (ii, jj) holds
-// global (gr0 + ii, gc0 + jj), nr x nz local cells, leading dimension lr.
-__device__ void tile_bc(double* xs, int lr, int nr, int nz, int gr0, int gc0, int M, int N) {
-    auto at = [&](int i, int j) -> double& { return xs[(i - gr0) + (long)(j - gc0) * lr]; };
+// global (gr0 + ii, gc0 + jj), nr x nz local cells.
+template <class S>
+__device__ void tile_bc(double* xs, int nr, int nz, int gr0, int gc0, int M, int N) {
+    auto at = [&](int i, int j) -> double& { return xs[sidx<S>(i - gr0, j - gc0)]; };
     auto has = [&](int i, int j) { return i >= gr0 && i < gr0 + nr && j >= gc0 && j < gc0 + nz; };
     for (int t = threadIdx.x; t < max(nr, nz); t += blockDim.x) {
         const int i = gr0 + t, j = gc0 + t;
@@ -405,35 +400,38 @@ __device__ void tile_bc(double* xs, int lr, int nr, int nz, int gr0, int gc0, in
     }
 }
 
-// One colour of gauss_seidel! on the tile's inner cells whose four neighbours are loaded;
-// a warp per column, each lane the Q = ceil(lr / 64) cells of its rows 2 (lane + 32 q) +
-// odd, whose loads are all issued before the arithmetic.  fps, fms: connector factors of
-// the tile's rows (local index).
-template <int LR>
-__device__ void tile_gs(double* xs, const double* bs, int nr, int nz, int gr0, int gc0, int M, int N,
-                        const double* fps, const double* fms, int color) {
-    constexpr int Q = (LR / 2 + 31) / 32;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int jj = 1 + warp; jj < nz - 1; jj += kTileWarps) {
-        const int j = gc0 + jj;
-        if (j < 1 || j > N) continue;
-        const int odd = (color ^ (gr0 + j)) & 1;
+// One colour of gauss_seidel! on the cells h or more away from the loaded edge.  Work
+// item (column jj, m) is the colour's cell of that column at local row 2 m + parity; a
+// thread takes Q items at a time and issues all their loads before the arithmetic.
+template <class S>
+__device__ void tile_gs(double* xs, const double* bs, const double* ft, int nr, int nz, int gr0, int gc0, int M,
+                        int N, int color, int h) {
+    constexpr int LH = S::LH, PL = S::PL, Q = 4;
+    const int n = LH * nz;
+    for (int t0 = threadIdx.x; t0 < n; t0 += Q * kTileThreads) {
         double c[Q], up[Q], rt[Q], dn[Q], lf[Q], bb[Q], f1[Q], f2[Q];
+        int d[Q];
         bool on[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            const int ii = 2 * (lane + 32 * q) + odd;
-            const int i = gr0 + ii;
-            on[q] = ii >= 1 && ii < nr - 1 && i >= 1 && i <= M;
-            const int k = on[q] ? ii + jj * LR : LR;   // a loaded cell when off
-            c[q] = xs[k];
-            up[q] = xs[k + 1];
-            rt[q] = xs[k + LR];
-            dn[q] = xs[k - 1];
-            lf[q] = xs[k - LR];
-            bb[q] = bs[k];
-            f1[q] = fps[on[q] ? ii : 0];
-            f2[q] = fms[on[q] ? ii : 0];
+            const int t = t0 + q * kTileThreads;
+            const int jj = t / LH, m = t - jj * LH;
+            const int j = gc0 + jj;
+            const int par = (color ^ (gr0 + j)) & 1;
+            const int ii = 2 * m + par, i = gr0 + ii;
+            on[q] = t < n && ii >= h && ii < nr - h && jj >= h && jj < nz - h && i >= 1 && i <= M && j >= 1 &&
+                    j <= N;
+            const int mm = on[q] ? m : 1, jc = on[q] ? jj : 1, pp = on[q] ? par : 0;   // a loaded cell when off
+            d[q] = pp * PL + jc * LH + mm;
+            const int o = (1 - pp) * PL + jc * LH + mm + pp;   // row ii + 1 in the other plane
+            c[q] = xs[d[q]];
+            up[q] = xs[o];
+            dn[q] = xs[o - 1];
+            rt[q] = xs[d[q] + LH];
+            lf[q] = xs[d[q] - LH];
+            bb[q] = bs[d[q]];
+            f1[q] = ft[pp * LH + mm];
+            f2[q] = ft[2 * LH + pp * LH + mm];
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -442,77 +440,69 @@ __device__ void tile_gs(double* xs, const double* bs, int nr, int nz, int gr0, i
             s += rt[q];
             s += dn[q] * f2[q];
             s += lf[q];
-            if (on[q]) xs[2 * (lane + 32 * q) + odd + jj * LR] = c[q] + 1.0 * (s + bb[q]) / 4.0;
+            if (on[q]) xs[d[q]] = c[q] + 1.0 * (s + bb[q]) / 4.0;
         }
     }
 }
 
 template <int NS, int MODE>
-__global__ void __launch_bounds__(kTileThreads, 2)
-    k_smooth_tile(const __grid_constant__ CUtensorMap mx, const __grid_constant__ CUtensorMap mb, TileArgs a) {
+__global__ void __launch_bounds__(kTileThreads, 2) k_smooth_tile(TileArgs a) {
     using S = TileShape<NS>;
-    constexpr int H = S::H, LR = S::LR, CR = S::CR, CZ = S::CZ;
-    extern __shared__ __align__(128) double smem[];
+    constexpr int H = S::H, LR = S::LR, LH = S::LH, PL = S::PL, CR = S::CR, CZ = S::CZ;
+    extern __shared__ __align__(16) double smem[];
     double* xs = smem;
     double* bs = smem + S::SX;
-    double* hs = smem + 2 * S::SX;
-    double* fps = hs + S::SH;
-    double* fms = fps + LR;
-    __shared__ __align__(8) unsigned long long bar;
+    double* hs = bs + S::SX;
+    double* ft = hs + S::SH;
     const int M = a.M, N = a.N;
     const long ld = M + 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ti = blockIdx.x % a.tiles_r, tj = blockIdx.x / a.tiles_r;
     const int r0 = 1 + ti * kTileR, c0 = 1 + tj * kTileZ;
     const int r1 = min(r0 + kTileR, M + 1), c1 = min(c0 + kTileZ, N + 1);
-    const int gr0 = r0 - H, gc0 = c0 - H;   // both even: the TMA box starts 16-byte aligned
+    const int gr0 = r0 - H, gc0 = c0 - H;   // gr0 even: local and global row parities agree
     const int nr = (r1 - r0) + 2 * H, nz = (c1 - c0) + 2 * H;
     const int Mh = M / 2, Nh = N / 2;
     const long ldh = Mh + 2;
+    const int Ilo = (gr0 >> 1) - 2, Jlo = (gc0 >> 1) - 1;
 
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bar)) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // gather x, b, the coarse neighbourhood and the rows' connector factors
+    for (int t = threadIdx.x; t < LR * nz; t += kTileThreads) {
+        const int jj = t / LR, ii = t - jj * LR;
+        const int i = gr0 + ii, j = gc0 + jj;
+        const bool in = ii < nr && i >= 0 && i <= M + 1 && j >= 0 && j <= N + 1;
+        const long k = in ? i + j * ld : 0;
+        const int d = sidx<S>(ii, jj);
+        cp_async8(bs + d, a.b + k, in);
+        if (MODE != TILE_PRE_SET) cp_async8(xs + d, a.xin + k, in);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t bytes = (MODE == TILE_PRE_SET ? 1u : 2u) * S::box_bytes;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(&bar)), "r"(bytes)
-                     : "memory");
-        tma_tile(bs, &mb, gr0, gc0, &bar);
-        if (MODE != TILE_PRE_SET) tma_tile(xs, &mx, gr0, gc0, &bar);
-    }
-    // the connector factors of the tile's rows and the coarse neighbourhood of the tile for
-    // the interpolation, while the copies fly
-    for (int ii = threadIdx.x; ii < LR; ii += kTileThreads) {
-        const int i = gr0 + ii;
-        const bool in = i >= 0 && i <= M + 1;
-        fps[ii] = in ? __ldg(a.fp + i) : 0.0;
-        fms[ii] = in ? __ldg(a.fm + i) : 0.0;
-    }
-    const int Ilo = ((gr0 >> 1) - 1) & ~1, Jlo = (gc0 >> 1) - 1;
     if (MODE != TILE_PRE) {
-        for (int jj = warp; jj < CZ; jj += kTileWarps) {
-            const int J = Jlo + jj;
-            for (int ii = lane; ii < CR; ii += 32) {
-                const int I = Ilo + ii;
-                hs[ii + jj * CR] = (I >= 0 && I <= Mh + 1 && J >= 0 && J <= Nh + 1) ? __ldg(a.xh + I + J * ldh) : 0.0;
-            }
+        for (int t = threadIdx.x; t < CR * CZ; t += kTileThreads) {
+            const int jj = t / CR, ii = t - jj * CR;
+            const int I = Ilo + ii, J = Jlo + jj;
+            const bool in = I >= 0 && I <= Mh + 1 && J >= 0 && J <= Nh + 1;
+            cp_async8(hs + t, a.xh + (in ? I + J * ldh : 0), in);
         }
     }
-    if (!mbar_wait0(&bar)) {
-        if (threadIdx.x == 0) atomicOr(a.status, ST_TIMEOUT);
-        mbar_wait0(&bar);   // the copies in flight land before the CTA leaves
-        return;
+    for (int t = threadIdx.x; t < LR; t += kTileThreads) {
+        const int i = gr0 + t;
+        const bool in = i >= 0 && i <= M + 1;
+        const int d = (t & 1) * LH + (t >> 1);
+        cp_async8(ft + d, a.fp + (in ? i : 0), in);
+        cp_async8(ft + 2 * LH + d, a.fm + (in ? i : 0), in);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+
     if (MODE != TILE_PRE) {
-        __syncthreads();
         // interpolate! (Multigrid.jl:232-258) into (TILE_PRE_SET) or onto (TILE_POST) x
-        for (int jj = warp; jj < nz; jj += kTileWarps) {
-            const int j = gc0 + jj;
-            for (int ii = lane; ii < nr; ii += 32) {
-                const int i = gr0 + ii;
-                const long k = ii + (long)jj * LR;
+        for (int par = 0; par < 2; ++par)
+            for (int t = threadIdx.x; t < LH * nz; t += kTileThreads) {
+                const int jj = t / LH, m = t - jj * LH;
+                const int ii = 2 * m + par;
+                if (ii >= nr) continue;
+                const int i = gr0 + ii, j = gc0 + jj;
+                const int d = par * PL + jj * LH + m;
                 if (i >= 1 && i <= M && j >= 1 && j <= N) {
                     const int I = (i + 1) >> 1, J = (j + 1) >> 1;
                     const int di = 2 * ((i + 1) & 1) - 1, dj = (2 * ((j + 1) & 1) - 1) * CR;
@@ -522,26 +512,26 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                     s += (3.0 / 16.0) * hs[kh + dj];
                     s += (3.0 / 16.0) * hs[kh + di];
                     s += (1.0 / 16.0) * hs[kh + di + dj];
-                    xs[k] = (MODE == TILE_POST) ? xs[k] + s : s;
+                    xs[d] = (MODE == TILE_POST) ? xs[d] + s : s;
                 } else if (MODE == TILE_PRE_SET) {
-                    xs[k] = 0.0;
+                    xs[d] = 0.0;
                 }
             }
-        }
+        __syncthreads();
     }
-    __syncthreads();
     for (int sw = 0; sw < NS; ++sw) {
-        tile_bc(xs, LR, nr, nz, gr0, gc0, M, N);
+        tile_bc<S>(xs, nr, nz, gr0, gc0, M, N);
         __syncthreads();
-        tile_gs<LR>(xs, bs, nr, nz, gr0, gc0, M, N, fps, fms, 0);
+        tile_gs<S>(xs, bs, ft, nr, nz, gr0, gc0, M, N, 0, 2 * sw + 1);
         __syncthreads();
-        tile_gs<LR>(xs, bs, nr, nz, gr0, gc0, M, N, fps, fms, 1);
+        tile_gs<S>(xs, bs, ft, nr, nz, gr0, gc0, M, N, 1, 2 * sw + 2);
         __syncthreads();
     }
     if (MODE != TILE_POST) {
-        tile_bc(xs, LR, nr, nz, gr0, gc0, M, N);
+        tile_bc<S>(xs, nr, nz, gr0, gc0, M, N);
         __syncthreads();
         // residual! (s = 1) and restrict! over the owned coarse cells
+        auto X = [&](int ii, int jj) { return xs[sidx<S>(ii, jj)]; };
         const int hr = (r1 - r0) >> 1, hz = (c1 - c0) >> 1;
         const int I0 = (r0 + 1) >> 1, J0 = (c0 + 1) >> 1;
         for (int q = warp; q < hz; q += kTileWarps) {
@@ -551,9 +541,14 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                 double s = 0.0;
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {   // children (0,0), (0,1), (1,0), (1,1)
-                    const int i = 2 * I - 1 + (c >> 1), j = 2 * J - 1 + (c & 1);
-                    const long k = (i - gr0) + (long)(j - gc0) * LR;
-                    const double r = 1.0 * bs[k] + lap5(xs, k, LR, fps[i - gr0], fms[i - gr0]);
+                    const int ii = 2 * I - 1 + (c >> 1) - gr0, jj = 2 * J - 1 + (c & 1) - gc0;
+                    const int f = (ii & 1) * LH + (ii >> 1);
+                    double l = -4.0 * X(ii, jj);
+                    l += X(ii + 1, jj) * ft[f];
+                    l += X(ii, jj + 1);
+                    l += X(ii - 1, jj) * ft[2 * LH + f];
+                    l += X(ii, jj - 1);
+                    const double r = 1.0 * bs[sidx<S>(ii, jj)] + l;
                     s += r;
                 }
                 a.rh[I + (long)J * ldh] = 4.0 * s / 4.0;
@@ -571,7 +566,7 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     const int ia = (ti == 0) ? 0 : r0, ib = (r1 == M + 1) ? M + 2 : r1;
     const int ja = (tj == 0) ? 0 : c0, jb = (c1 == N + 1) ? N + 2 : c1;
     for (int j = ja + warp; j < jb; j += kTileWarps)
-        for (int i = ia + lane; i < ib; i += 32) a.xout[i + (long)j * ld] = xs[(i - gr0) + (long)(j - gc0) * LR];
+        for (int i = ia + lane; i < ib; i += 32) a.xout[i + (long)j * ld] = xs[sidx<S>(i - gr0, j - gc0)];
 }
 
 // The coarse end of fmg! (Multigrid.jl:400-428): the restrictions below level `small`,
@@ -611,65 +606,156 @@ __device__ void fmg_tail_body(const MgView& V) {
 
 __global__ void __launch_bounds__(kCtaThreads) k_fmg_tail(MgView V) { fmg_tail_body(V); }
 
-// The same two tails with the levels from `small` down held in shared memory: level l's
-// res, res1 and sol arrays and its connector factors at tail_off[l] (each array padded to
-// an even number of doubles), and the level table itself in shared memory, so that only
-// level `small`'s arrays travel to and from HBM.
+// The same two tails with the levels from `small` down held in shared memory: the
+// connector factors of level `small` (those of a coarser level are their first rows: the
+// factor depends on the row index alone), then per level its res, res1 and sol arrays
+// (each padded to an even number of doubles).  Every address is the shared base plus an
+// offset computed here, so the accesses compile to shared-memory instructions; only level
+// `small`'s arrays travel to and from HBM.
 __host__ __device__ inline int tail_cells(int M, int N) { return ((M + 2) * (N + 2) + 1) & ~1; }
-__host__ __device__ inline int tail_block(int M, int N) { return 3 * tail_cells(M, N) + ((2 * (M + 2) + 1) & ~1); }
+__host__ __device__ inline int tail_tables(int M) { return 2 * ((M + 2 + 1) & ~1); }
 
-__device__ void copy_range(double* dst, const double* src, int n) {
-    for (int t = threadIdx.x; t < n; t += blockDim.x) dst[t] = src[t];
+struct TailArgs {
+    int M0, N0, K;           // level `small` sizes, levels below it
+    int s1, s2, nc, total;   // sweeps, coarsest unknowns, shared doubles
+    const double* ainv;
+    const double* gres;      // level `small` right-hand side (HBM)
+    double* gsol;            // level `small` solution (HBM)
+    const double* gfp;       // its connector factors
+    const double* gfm;
+};
+
+struct TailLevel {
+    int M, N;
+    double* res;
+    double* res1;
+    double* sol;
+};
+
+__device__ __forceinline__ TailLevel tail_level(double* sm, const TailArgs& A, int k) {
+    int off = tail_tables(A.M0), M = A.M0, N = A.N0;
+    for (int q = 0; q < k; ++q) {
+        off += 3 * tail_cells(M, N);
+        M >>= 1;
+        N >>= 1;
+    }
+    const int cp = tail_cells(M, N);
+    TailLevel L;
+    L.M = M;
+    L.N = N;
+    L.res = sm + off;
+    L.res1 = sm + off + cp;
+    L.sol = sm + off + 2 * cp;
+    return L;
 }
 
-__device__ void tail_setup(MgView& W, const MgView& V, double* sm, int total) {
-    if (threadIdx.x == 0) {
-        W = V;
-        for (int l = V.small; l <= V.levels; ++l) {
-            const int cp = tail_cells(V.lv[l].M, V.lv[l].N);
-            double* base = sm + V.tail_off[l];
-            W.lv[l].res = base;
-            W.lv[l].res1 = base + cp;
-            W.lv[l].sol = base + 2 * cp;
-            W.lv[l].fp = base + 3 * cp;
-            W.lv[l].fm = base + 3 * cp + (V.lv[l].M + 2);
+__device__ __forceinline__ void tail_smooth(const TailLevel& L, const double* fp, const double* fm, int n, int t0,
+                                            int dt, bool warp_only) {
+    for (int it = 0; it < n; ++it) {
+        bc_range(L.sol, L.M, L.N, t0, dt);
+        if (warp_only) __syncwarp(); else __syncthreads();
+        gs_range(L.sol, L.res, fp, fm, L.M, L.N, 0, t0, dt);
+        if (warp_only) __syncwarp(); else __syncthreads();
+        gs_range(L.sol, L.res, fp, fm, L.M, L.N, 1, t0, dt);
+        if (warp_only) __syncwarp(); else __syncthreads();
+    }
+}
+
+// mgv! from tail level k0 (level small + k0) down to the coarsest and back.
+__device__ __forceinline__ void tail_vcycle(double* sm, const TailArgs& A, int k0) {
+    const double* fp = sm;
+    const double* fm = sm + tail_tables(A.M0) / 2;
+    const int t0 = threadIdx.x, dt = blockDim.x;
+    for (int k = k0; k < A.K; ++k) {
+        const TailLevel L = tail_level(sm, A, k), H = tail_level(sm, A, k + 1);
+        tail_smooth(L, fp, fm, A.s1, t0, dt, false);
+        bc_range(L.sol, L.M, L.N, t0, dt);
+        __syncthreads();
+        residual_range(L.res1, L.sol, L.res, 1.0, fp, fm, L.M, L.N, t0, dt);
+        __syncthreads();
+        restrict_range(H.res, L.res1, H.M, H.N, t0, dt);
+        zero_range(H.sol, (H.M + 2) * (H.N + 2), t0, dt);
+        __syncthreads();
+    }
+    const TailLevel C = tail_level(sm, A, A.K);
+    if ((C.M + 2) * (C.N + 2) <= 1024) {   // the coarsest sweeps by one warp
+        if (threadIdx.x < 32) tail_smooth(C, fp, fm, kCoarsestSweeps, threadIdx.x, 32, true);
+        __syncthreads();
+    } else {
+        tail_smooth(C, fp, fm, kCoarsestSweeps, t0, dt, false);
+    }
+    for (int k = A.K - 1; k >= k0; --k) {
+        const TailLevel L = tail_level(sm, A, k), H = tail_level(sm, A, k + 1);
+        interp_range(L.sol, H.sol, H.M, H.N, true, t0, dt);
+        __syncthreads();
+        tail_smooth(L, fp, fm, A.s2, t0, dt, false);
+    }
+}
+
+__device__ __forceinline__ void tail_load(double* sm, const TailArgs& A, bool with_sol) {
+    zero_range(sm, A.total, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const int m2 = A.M0 + 2;
+    for (int t = threadIdx.x; t < m2; t += blockDim.x) {
+        sm[t] = A.gfp[t];
+        sm[tail_tables(A.M0) / 2 + t] = A.gfm[t];
+    }
+    const TailLevel G = tail_level(sm, A, 0);
+    const int n = (G.M + 2) * (G.N + 2);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        G.res[t] = A.gres[t];
+        if (with_sol) G.sol[t] = A.gsol[t];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void tail_store(double* sm, const TailArgs& A) {
+    __syncthreads();
+    const TailLevel G = tail_level(sm, A, 0);
+    const int n = (G.M + 2) * (G.N + 2);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) A.gsol[t] = G.sol[t];
+}
+
+__global__ void __launch_bounds__(kCtaThreads) k_vcycle_tail_smem(TailArgs A) {
+    extern __shared__ __align__(16) double sm[];
+    tail_load(sm, A, true);
+    tail_vcycle(sm, A, 0);
+    tail_store(sm, A);
+}
+
+// fmg_tail_body on the shared-memory levels.
+__global__ void __launch_bounds__(kCtaThreads) k_fmg_tail_smem(TailArgs A) {
+    extern __shared__ __align__(16) double sm[];
+    const int t0 = threadIdx.x, dt = blockDim.x;
+    tail_load(sm, A, false);
+    for (int k = 0; k < A.K; ++k) {
+        const TailLevel L = tail_level(sm, A, k), H = tail_level(sm, A, k + 1);
+        restrict_range(H.res, L.res, H.M, H.N, t0, dt);
+        __syncthreads();
+    }
+    {
+        const TailLevel C = tail_level(sm, A, A.K);
+        const int ld = C.M + 2;
+        for (int p = t0; p < A.nc; p += dt) {
+            double acc = 0.0;
+            for (int q = 0; q < A.nc; ++q) {
+                const int qi = 1 + q % C.M, qj = 1 + q / C.M;
+                acc = acc + A.ainv[(long)p * A.nc + q] * C.res[qi + qj * ld];
+            }
+            C.sol[(1 + p % C.M) + (1 + p / C.M) * ld] = acc;
         }
+        __syncthreads();
     }
-    zero_range(sm, total, threadIdx.x, blockDim.x);
-    __syncthreads();
-    for (int l = V.small; l <= V.levels; ++l) {
-        const int cp = tail_cells(V.lv[l].M, V.lv[l].N);
-        double* base = sm + V.tail_off[l];
-        copy_range(base + 3 * cp, V.lv[l].fp, V.lv[l].M + 2);
-        copy_range(base + 3 * cp + (V.lv[l].M + 2), V.lv[l].fm, V.lv[l].M + 2);
+    for (int k = A.K - 1; k >= 0; --k) {
+        const TailLevel L = tail_level(sm, A, k), H = tail_level(sm, A, k + 1);
+        zero_range(L.sol, (L.M + 2) * (L.N + 2), t0, dt);
+        bc_range(H.sol, H.M, H.N, t0, dt);
+        __syncthreads();
+        interp_range(L.sol, H.sol, H.M, H.N, false, t0, dt);
+        __syncthreads();
+        tail_vcycle(sm, A, k);
     }
-}
-
-__global__ void __launch_bounds__(kCtaThreads) k_vcycle_tail_smem(MgView V, int total) {
-    extern __shared__ __align__(16) double sm[];
-    __shared__ MgView W;
-    tail_setup(W, V, sm, total);
-    const LevelView& G = V.lv[V.small];
-    const int n = (G.M + 2) * (G.N + 2);
-    copy_range(sm + V.tail_off[V.small], G.res, n);
-    copy_range(sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), G.sol, n);
-    __syncthreads();
-    vcycle_cta(W, V.small);
-    __syncthreads();
-    copy_range(G.sol, sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), n);
-}
-
-__global__ void __launch_bounds__(kCtaThreads) k_fmg_tail_smem(MgView V, int total) {
-    extern __shared__ __align__(16) double sm[];
-    __shared__ MgView W;
-    tail_setup(W, V, sm, total);
-    const LevelView& G = V.lv[V.small];
-    const int n = (G.M + 2) * (G.N + 2);
-    copy_range(sm + V.tail_off[V.small], G.res, n);
-    __syncthreads();
-    fmg_tail_body(W);
-    __syncthreads();
-    copy_range(G.sol, sm + V.tail_off[V.small] + 2 * tail_cells(G.M, G.N), n);
+    tail_store(sm, A);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -870,9 +956,6 @@ struct mcs_poisson {
     double* dnorm = nullptr;   // {eps, converged}
     double* hnorm = nullptr;   // pinned copy
     double* sol2[kMaxLevels + 1] = {};   // second solution buffer of the grid-wide levels
-    // TMA descriptors of the grid-wide levels, for 1 and 2 sweeps (box sizes differ)
-    CUtensorMap map_sol[2][2][kMaxLevels + 1];   // [sweeps - 1][buffer][level]
-    CUtensorMap map_res[2][kMaxLevels + 1];
     int tail_smem = 0;                            // bytes of the shared-memory tail (0: in HBM)
     bool fused = false;                   // smooth1, smooth2 in {1, 2}: fused tile kernels
     long long launches = 0;    // kernels launched by this workspace
@@ -895,46 +978,9 @@ int palloc(mcs_poisson* p, double** out, size_t count) {
     return cudaMemset(d, 0, count * sizeof(double)) == cudaSuccess ? MCS_OK : MCS_ERR_CUDA;
 }
 
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled encode_tiled() {
-    static EncodeTiled fn = nullptr;
-    if (!fn) {
-        void* f = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiled>(f);
-    }
-    return fn;
-}
-
-// A level array as a 2-D FP64 tensor (rows M+2 innermost, N+2 columns) read in boxes of
-// box_r x box_c; reads outside the array return zeros.
-int tensor_map(mcs_poisson* p, CUtensorMap* m, const double* base, int M, int N, int box_r, int box_c) {
-    EncodeTiled enc = encode_tiled();
-    if (!enc) return set_err(p->ctx, MCS_ERR_CUDA, "poisson: cuTensorMapEncodeTiled unavailable");
-    const cuuint64_t dims[2] = {(cuuint64_t)(M + 2), (cuuint64_t)(N + 2)};
-    const cuuint64_t strides[1] = {(cuuint64_t)(M + 2) * sizeof(double)};
-    const cuuint32_t box[2] = {(cuuint32_t)box_r, (cuuint32_t)box_c};
-    const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(base), dims, strides, box, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? MCS_OK : set_err(p->ctx, MCS_ERR_CUDA, "poisson: tensor map encoding failed");
-}
-
 template <int NS>
-int tile_maps(mcs_poisson* p) {
+int tile_attr(mcs_poisson* p) {
     using S = TileShape<NS>;
-    for (int l = 0; l < p->small; ++l) {
-        const LevelView& L = p->V.lv[l];
-        if (int e = tensor_map(p, &p->map_sol[NS - 1][0][l], L.sol, L.M, L.N, S::LR, S::LZ)) return e;
-        if (int e = tensor_map(p, &p->map_sol[NS - 1][1][l], p->sol2[l], L.M, L.N, S::LR, S::LZ)) return e;
-        if (int e = tensor_map(p, &p->map_res[NS - 1][l], L.res, L.M, L.N, S::LR, S::LZ)) return e;
-    }
     const void* fns[3] = {(const void*)k_smooth_tile<NS, TILE_PRE>, (const void*)k_smooth_tile<NS, TILE_PRE_SET>,
                           (const void*)k_smooth_tile<NS, TILE_POST>};
     for (const void* f : fns)
@@ -944,8 +990,8 @@ int tile_maps(mcs_poisson* p) {
 }
 
 int tile_setup(mcs_poisson* p) {
-    if (int e = tile_maps<1>(p)) return e;
-    return tile_maps<2>(p);
+    if (int e = tile_attr<1>(p)) return e;
+    return tile_attr<2>(p);
 }
 
 int use_dev(mcs_poisson* p) {
@@ -1006,10 +1052,28 @@ void coarse_inverse(int Mc, int Nc, std::vector<double>& inv) {
 #define PSN_LAUNCH(p) MCS_CK((p)->ctx, cudaGetLastError())
 
 // The one-CTA tails: mgv! from level `small`, and the coarse end of fmg!.
+TailArgs tail_args(mcs_poisson* p) {
+    const LevelView& G = p->V.lv[p->small];
+    TailArgs A{};
+    A.M0 = G.M;
+    A.N0 = G.N;
+    A.K = p->levels - p->small;
+    A.s1 = p->smooth1;
+    A.s2 = p->smooth2;
+    A.nc = p->V.nc;
+    A.total = p->tail_smem / (int)sizeof(double);
+    A.ainv = p->V.ainv;
+    A.gres = G.res;
+    A.gsol = G.sol;
+    A.gfp = G.fp;
+    A.gfm = G.fm;
+    return A;
+}
+
 void launch_vtail(mcs_poisson* p, cudaStream_t st) {
     ++p->launches;
     if (p->tail_smem)
-        k_vcycle_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(p->V, p->tail_smem / (int)sizeof(double));
+        k_vcycle_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(tail_args(p));
     else
         k_vcycle_cta<<<1, kCtaThreads, 0, st>>>(p->V, p->small);
 }
@@ -1017,7 +1081,7 @@ void launch_vtail(mcs_poisson* p, cudaStream_t st) {
 void launch_ftail(mcs_poisson* p, cudaStream_t st) {
     ++p->launches;
     if (p->tail_smem)
-        k_fmg_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(p->V, p->tail_smem / (int)sizeof(double));
+        k_fmg_tail_smem<<<1, kCtaThreads, p->tail_smem, st>>>(tail_args(p));
     else
         k_fmg_tail<<<1, kCtaThreads, 0, st>>>(p->V);
 }
@@ -1076,14 +1140,13 @@ double* sol_buf(mcs_poisson* p, const Buffers& B, int l) {
 }
 
 template <int NS, int MODE>
-void launch_tile(mcs_poisson* p, int l, int xbuf, const TileArgs& a, cudaStream_t st) {
+void launch_tile(mcs_poisson* p, const TileArgs& a, cudaStream_t st) {
     using S = TileShape<NS>;
     const int tr = (a.M + kTileR - 1) / kTileR, tz = (a.N + kTileZ - 1) / kTileZ;
     TileArgs b = a;
     b.tiles_r = tr;
     ++p->launches;
-    k_smooth_tile<NS, MODE><<<tr * tz, kTileThreads, S::smem, st>>>(p->map_sol[NS - 1][xbuf][l],
-                                                                      p->map_res[NS - 1][l], b);
+    k_smooth_tile<NS, MODE><<<tr * tz, kTileThreads, S::smem, st>>>(b);
 }
 
 // One fused step at level l: TILE_PRE / TILE_PRE_SET (smooth1 sweeps) or TILE_POST
@@ -1091,26 +1154,26 @@ void launch_tile(mcs_poisson* p, int l, int xbuf, const TileArgs& a, cudaStream_
 void tile_step(mcs_poisson* p, Buffers& B, int l, int mode, cudaStream_t st) {
     const LevelView& L = p->V.lv[l];
     TileArgs a{};
-    const int xin = B.cur[l];
+    a.xin = sol_buf(p, B, l);
     B.cur[l] ^= 1;
     a.xout = sol_buf(p, B, l);
+    a.b = L.res;
     a.xh = sol_buf(p, B, l + 1);
     a.rh = p->V.lv[l + 1].res;
     a.hzero = sol_buf(p, B, l + 1);
     a.fp = L.fp;
     a.fm = L.fm;
-    a.status = p->ctx->d_status;
     a.M = L.M;
     a.N = L.N;
     const int ns = mode == TILE_POST ? p->smooth2 : p->smooth1;
     if (ns == 1) {
-        if (mode == TILE_PRE) launch_tile<1, TILE_PRE>(p, l, xin, a, st);
-        else if (mode == TILE_PRE_SET) launch_tile<1, TILE_PRE_SET>(p, l, xin, a, st);
-        else launch_tile<1, TILE_POST>(p, l, xin, a, st);
+        if (mode == TILE_PRE) launch_tile<1, TILE_PRE>(p, a, st);
+        else if (mode == TILE_PRE_SET) launch_tile<1, TILE_PRE_SET>(p, a, st);
+        else launch_tile<1, TILE_POST>(p, a, st);
     } else {
-        if (mode == TILE_PRE) launch_tile<2, TILE_PRE>(p, l, xin, a, st);
-        else if (mode == TILE_PRE_SET) launch_tile<2, TILE_PRE_SET>(p, l, xin, a, st);
-        else launch_tile<2, TILE_POST>(p, l, xin, a, st);
+        if (mode == TILE_PRE) launch_tile<2, TILE_PRE>(p, a, st);
+        else if (mode == TILE_PRE_SET) launch_tile<2, TILE_PRE_SET>(p, a, st);
+        else launch_tile<2, TILE_POST>(p, a, st);
     }
 }
 
@@ -1350,16 +1413,11 @@ MCS_API int mcs_poisson_create(mcs_grid* g, int levels, int smooth1, int smooth2
     p->small = levels;
     p->tail_smem = 0;
     for (int l = 0; l <= levels; ++l) {
-        long tot = 0;
-        for (int k = l; k <= levels; ++k) tot += tail_block(M >> k, N >> k);
+        long tot = tail_tables(M >> l);
+        for (int k = l; k <= levels; ++k) tot += 3 * tail_cells(M >> k, N >> k);
         if (tot * (long)sizeof(double) <= kTailSmemBytes) {
             p->small = l;
             p->tail_smem = (int)(tot * sizeof(double));
-            long off = 0;
-            for (int k = l; k <= levels; ++k) {
-                p->V.tail_off[k] = (int)off;
-                off += tail_block(M >> k, N >> k);
-            }
             break;
         }
     }
@@ -1489,7 +1547,7 @@ MCS_API int mcs_poisson_zero(mcs_poisson* p, int which) {
 // Mean duration of one finest-level red-black pass and one finest-level residual, each
 // launched `reps` times back to back between CUDA events on the context's stream.  They
 // run on the workspace's scratch levels, so u and b are untouched.
-MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* residual_ms) {
+MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* residual_ms, float* tile_ms) {
     if (!p || reps < 1) return MCS_ERR_ARG;
     if (int e = use_dev(p)) return e;
     cudaStream_t st = p->ctx->stream;
@@ -1518,6 +1576,30 @@ MCS_API int mcs_poisson_profile(mcs_poisson* p, int reps, float* gs_ms, float* r
     cudaEventSynchronize(e1);
     cudaEventElapsedTime(&ms, e0, e1);
     if (residual_ms) *residual_ms = ms / reps;
+    if (tile_ms) *tile_ms = 0.0f;
+    if (tile_ms && p->fused && p->small > 0) {
+        // the fused post-smoothing of the finest level: sol -> sol2 with the next level's
+        // solution interpolated on
+        const LevelView& H = p->V.lv[1];
+        TileArgs a{};
+        a.xin = F.sol;
+        a.xout = p->sol2[0];
+        a.b = F.res;
+        a.xh = H.sol;
+        a.fp = F.fp;
+        a.fm = F.fm;
+        a.M = F.M;
+        a.N = F.N;
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < reps; ++r) {
+            if (p->smooth2 == 1) launch_tile<1, TILE_POST>(p, a, st);
+            else launch_tile<2, TILE_POST>(p, a, st);
+        }
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        *tile_ms = ms / reps;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     PSN_LAUNCH(p);

@@ -88,11 +88,12 @@ class PoissonSolver:
     def zero(self, which: int = L.PSN_U) -> None:
         self.ctx.check(self.ctx.lib.mcs_poisson_zero(self.h, which))
 
-    def profile(self, reps: int = 20) -> Tuple[float, float]:
-        """(ms of one finest-level red-black pass, ms of one finest-level residual)."""
-        g, r = C.c_float(0.0), C.c_float(0.0)
-        self.ctx.check(self.ctx.lib.mcs_poisson_profile(self.h, int(reps), C.byref(g), C.byref(r)))
-        return g.value, r.value
+    def profile(self, reps: int = 20) -> Tuple[float, float, float]:
+        """ms of one finest-level red-black pass, one finest-level residual and one fused
+        finest-level post-smoothing launch (0.0 when unfused)."""
+        g, r, t = C.c_float(0.0), C.c_float(0.0), C.c_float(0.0)
+        self.ctx.check(self.ctx.lib.mcs_poisson_profile(self.h, int(reps), C.byref(g), C.byref(r), C.byref(t)))
+        return g.value, r.value, t.value
 
     # -- the reference's functions ---------------------------------------------------------
     def solve(self) -> Tuple[int, float]:
