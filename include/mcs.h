@@ -54,8 +54,10 @@ enum {
     MCS_EXCITATION = 2,          /* param = threshold (J)                         */
     MCS_IONIZATION = 3,          /* param = threshold (J), equal energy sharing   */
     MCS_ATTACHMENT = 4,          /* param = threshold (J), unused                 */
-    MCS_IONIZATION_UNIFORM = 5   /* param = threshold (J), secondary energy uniform on
+    MCS_IONIZATION_UNIFORM = 5,  /* param = threshold (J), secondary energy uniform on
                                     [0, eps - threshold]; no counterpart in JuMC */
+    MCS_PHOTOEMISSION = 6        /* PhotoEmission (electron.jl:88-105, 141-144): param unused;
+                                    the band and weights by mcs_table_set_photoemission */
 };
 
 enum { MCS_FP64 = 0, MCS_FP32 = 1 };
@@ -90,6 +92,7 @@ typedef struct mcs_field mcs_field;
 typedef struct mcs_pop mcs_pop;
 typedef struct mcs_batch mcs_batch;
 typedef struct mcs_poisson mcs_poisson;
+typedef struct mcs_photons mcs_photons;
 
 /* ---- context ---- */
 MCS_API int mcs_version(void);
@@ -336,6 +339,31 @@ MCS_API int mcs_batch_variant_shape(int variant, int* block, int* ppt);
 MCS_API int mcs_batch_variant_min_blocks(int variant, int* min_blocks);
 /* Idle lanes (of 32) at which the variant's particle queue writes back and refills. */
 MCS_API int mcs_batch_variant_refill(int variant, int* idle_lanes);
+
+/* ---- photons: PhotonState (JuMC/src/photon.jl:11-18) and photo-emission ----
+ * PhotoEmission rows of a table (kind MCS_PHOTOEMISSION; electron.jl:88-105, lxcat.jl:86-93):
+ * log(nu_min), log(nu_max) per row (1/s; other rows ignored), photon_multiplier and
+ * photon_weight.  Required before a table with such rows is used. */
+MCS_API int mcs_table_set_photoemission(mcs_table* t, const double* log_numin, const double* log_numax,
+                                        double photon_multiplier, double photon_weight);
+/* A photon population of `capacity` photons in FP64 whose collisions run at maxrate numax
+ * (ZhelezniakCollisions(numax), photon.jl:27-37; MCStreamer/src/main.jl:115-121). */
+MCS_API int mcs_photons_create(mcs_ctx* ctx, int64_t capacity, double numax, uint64_t seed, mcs_photons** out);
+MCS_API int mcs_photons_destroy(mcs_photons* ph);
+/* Julia layout: x, v interleaved triples, nu, w, s one double each, active one byte. */
+MCS_API int mcs_photons_upload(mcs_photons* ph, const double* x, const double* v, const double* nu,
+                               const double* w, const double* s, const uint8_t* active, int64_t n);
+MCS_API int mcs_photons_download(mcs_photons* ph, double* x, double* v, double* nu, double* w, double* s,
+                                 uint8_t* active, int64_t capacity, int64_t* n_out);
+MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n);
+/* advance!(mpopl, efield, dt, tracker) over electrons and photons (mixed_population.jl:24-54):
+ * the electrons (absolute positions), whose photo-emission adds photons in serial parent
+ * order, then every photon (the new ones too): straight flight, photo-ionization adding +w
+ * to the tracker and an electron at rest, appended in serial photon order. */
+MCS_API int mcs_advance_mixed(mcs_pop* electrons, mcs_photons* photons, const mcs_table* t, const mcs_field* f,
+                              double dt, mcs_grid* tracker);
+/* The photon half of mcs_advance_mixed alone. */
+MCS_API int mcs_photon_advance(mcs_photons* photons, mcs_pop* electrons, double dt, mcs_grid* tracker);
 
 /* ---- Poisson solve: poisson! (MCStreamer/src/poisson.jl:6-58) on a cylindrical grid ----
  * The multigrid is Multigrid.solve (Multigrid/src/Multigrid.jl:449-467) with MCStreamer's

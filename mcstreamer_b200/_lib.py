@@ -22,7 +22,7 @@ STATUS_NAMES = {
     9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT",
 }
 # process kinds
-NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM = 0, 1, 2, 3, 4, 5
+NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM, PHOTOEMISSION = 0, 1, 2, 3, 4, 5, 6
 FP64, FP32 = 0, 1
 FLAG_CLAMP_ENERGY = 1
 Q_FIXED, Q_PART = 0, 1
@@ -128,6 +128,14 @@ SIGNATURES = {
     "mcs_poisson_launches": (i32, [vp, pi64]),
     "mcs_poisson_profile": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "mcs_grid_write_fixed": (i32, [vp, i32, pi64]),
+    "mcs_table_set_photoemission": (i32, [vp, pd, pd, f64, f64]),
+    "mcs_photons_create": (i32, [vp, i64, f64, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "mcs_photons_destroy": (i32, [vp]),
+    "mcs_photons_upload": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64]),
+    "mcs_photons_download": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64, pi64]),
+    "mcs_photons_count": (i32, [vp, pi64]),
+    "mcs_advance_mixed": (i32, [vp, vp, vp, vp, f64, vp]),
+    "mcs_photon_advance": (i32, [vp, vp, f64, vp]),
 }
 
 _lib = None

@@ -12,6 +12,7 @@ using namespace mcs;
 namespace mcs {
 
 int map_status(uint32_t st) {
+    if (st & ST_UNSUPPORTED) return MCS_ERR_UNSUPPORTED;
     if (st & ST_TIMEOUT) return MCS_ERR_TIMEOUT;
     if (st & ST_CAPACITY) return MCS_ERR_CAPACITY;
     if (st & ST_OVERFLOW) return MCS_ERR_OVERFLOW;
@@ -29,6 +30,7 @@ const char* status_text(int code) {
     case MCS_ERR_ENERGY_RANGE: return "particle energy outside the collision table";
     case MCS_ERR_FIELD_TOO_HIGH: return "Too high electric field";
     case MCS_ERR_NONFINITE: return "non-finite particle state";
+    case MCS_ERR_UNSUPPORTED: return "a process the kernel does not apply (photo-emission needs mcs_advance_mixed)";
     default: return "";
     }
 }
@@ -81,13 +83,15 @@ int ensure_staging(mcs_pop* p, size_t bytes) {
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Slot of the per-step moments log for the step about to run (nullptr when disabled).
+}  // namespace
+
+namespace mcs {
 double* log_slot(mcs_pop* p) {
     if (!p->d_log || p->log_cap < 1) return nullptr;
     const uint32_t k = (p->step - p->log_step0) % (uint32_t)p->log_cap;
     return p->d_log + (size_t)k * kStepMoments;
 }
-
-}  // namespace
+}  // namespace mcs
 
 extern "C" {
 
@@ -173,7 +177,7 @@ MCS_API int mcs_table_create(mcs_ctx* c, int nrows, int neps, double e0, double 
     if (nrows < 1 || nrows > kMaxRows) return set_err(c, MCS_ERR_ARG, "nrows must be in [1, 32]");
     if (neps < 2 || !(emax > e0) || !(maxrate > 0)) return set_err(c, MCS_ERR_ARG, "bad energy grid or maxrate");
     for (int j = 0; j < nrows; ++j)
-        if (kind[j] < MCS_NULL || kind[j] > MCS_IONIZATION_UNIFORM)
+        if (kind[j] < MCS_NULL || kind[j] > MCS_PHOTOEMISSION)
             return set_err(c, MCS_ERR_UNSUPPORTED, "unsupported collision process kind");
     if (int st = use_device(c)) return st;
     mcs_table* t = new (std::nothrow) mcs_table();
@@ -194,6 +198,7 @@ MCS_API int mcs_table_create(mcs_ctx* c, int nrows, int neps, double e0, double 
     for (int j = 0; j < kMaxRows; ++j) {
         v.kind[j] = j < nrows ? kind[j] : MCS_NULL;
         v.param[j] = j < nrows ? param[j] : 0.0;
+        if (j < nrows && kind[j] == MCS_PHOTOEMISSION) t->photo_rows = true;
     }
     const size_t n64 = (size_t)neps * nrows, n32 = (size_t)neps * v.nrp;
     int st = dalloc(c, &t->d_rate64, n64);
@@ -661,6 +666,7 @@ MCS_API int mcs_pop_download(mcs_pop* p, double* x, double* v, double* w, double
 MCS_API int mcs_advance(mcs_pop* p, const mcs_table* t, const mcs_field* f, double dt, mcs_grid* tracker) {
     if (!p || !t || !f) return MCS_ERR_ARG;
     mcs_ctx* c = p->ctx;
+    if (t->photo_rows) return set_err(c, MCS_ERR_UNSUPPORTED, "photo-emission needs mcs_advance_mixed");
     if (!(dt >= 0)) return set_err(c, MCS_ERR_ARG, "dt must be >= 0");
     if (f->type == FIELD_GRID && !f->grid) return MCS_ERR_ARG;
     if (int st = use_device(c)) return st;
@@ -686,6 +692,7 @@ MCS_API int mcs_advance_deposit(mcs_pop* p, const mcs_table* t, const mcs_field*
                                 mcs_grid* deposit, double val) {
     if (!p || !t || !f || !deposit) return MCS_ERR_ARG;
     mcs_ctx* c = p->ctx;
+    if (t->photo_rows) return set_err(c, MCS_ERR_UNSUPPORTED, "photo-emission needs mcs_advance_mixed");
     if (!p->cells || deposit != p->cells || f->type != FIELD_GRID || f->grid != p->cells ||
         (tracker && tracker != p->cells))
         return set_err(c, MCS_ERR_UNSUPPORTED, "fused step+deposit needs a cell-layout population on one mesh");
@@ -703,6 +710,7 @@ MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* 
     if (!p || !t) return MCS_ERR_ARG;
     mcs_ctx* c = p->ctx;
     if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "collisions! on a cell-layout population");
+    if (t->photo_rows) return set_err(c, MCS_ERR_UNSUPPORTED, "photo-emission needs mcs_advance_mixed");
     if (int st = use_device(c)) return st;
     const int st = p->precision == MCS_FP32 ? launch_collisions<float>(p, t, dt, tracker)
                                             : launch_collisions<double>(p, t, dt, tracker);
@@ -774,6 +782,7 @@ MCS_API int mcs_swarm_run(mcs_pop* p, const mcs_table* t, const mcs_field* f, do
     if (!p || !t || !f || nsteps < 0) return MCS_ERR_ARG;
     mcs_ctx* c = p->ctx;
     if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "swarm loop on a cell-layout population");
+    if (t->photo_rows) return set_err(c, MCS_ERR_UNSUPPORTED, "photo-emission needs mcs_advance_mixed");
     if (int st = use_device(c)) return st;
     double* d_out = nullptr;
     if (int st = dalloc(c, &d_out, (size_t)(nsteps > 0 ? nsteps : 1) * kStepMoments)) return st;

@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
                     float cvx = fmaf(ax, tau, vx), cvy = fmaf(ay, tau, vy), cvz = fmaf(az, tau, vz);
                     Sec<float> sec;
                     const int out = collide_once<float>(sh.rows, tab, C, rng, cvx, cvy, cvz, sec);
+                    if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
                     if (out != OUT_NONE) {
                         const float h2 = 0.5f * tau * tau;
                         x = fmaf(ax, h2, fmaf(vx, tau, x));
@@ -496,33 +497,7 @@ __global__ void k_bempty_moments(BatchDev B) {
     }
 }
 
-__device__ long long poisson_sample_b(Rng& r, double lam) {
-    // Inversion below 10, PTRS (Hoermann 1993) above: the same algorithm as the population path.
-    if (lam <= 0) return 0;
-    if (lam < 10.0) {
-        const double u = r.u64();
-        double pr = exp(-lam), F = pr;
-        long long kk = 0;
-        while (u > F && kk < 1000) { ++kk; pr *= lam / (double)kk; F += pr; }
-        return kk;
-    }
-    const double slam = sqrt(lam), loglam = log(lam);
-    const double b = 0.931 + 2.53 * slam;
-    const double a = -0.059 + 0.02483 * b;
-    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
-    const double vr = 0.9277 - 3.6224 / (b - 2.0);
-    for (int it = 0; it < 1000; ++it) {
-        const double U = r.u64() - 0.5;
-        const double V = r.u64();
-        const double us = 0.5 - fabs(U);
-        const double kf = floor((2.0 * a / us + b) * U + lam + 0.43);
-        if (us >= 0.07 && V <= vr) return (long long)kf;
-        if (kf < 0 || (us < 0.013 && V > us)) continue;
-        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + kf * loglam - lgamma(kf + 1.0))
-            return (long long)kf;
-    }
-    return (long long)floor(lam);
-}
+__device__ __forceinline__ long long poisson_sample_b(Rng& r, double lam) { return poisson_draw(r, lam); }
 
 __device__ __forceinline__ void bcopy_slot(const BatchDev& B, long long dst, long long src) {
 #pragma unroll
@@ -1082,6 +1057,7 @@ MCS_API int mcs_batch_add(mcs_batch* b, const mcs_table* t, double ex, double ey
                           int64_t n0, double tol, int64_t capacity, const double* x, const double* v,
                           const double* w, const double* s, const uint8_t* active, int64_t n, int* slot) {
     if (!b || !t || !slot || capacity < 1 || n < 0 || n > capacity) return MCS_ERR_ARG;
+    if (t && t->photo_rows) return MCS_ERR_UNSUPPORTED;   // photo-emission needs mcs_advance_mixed
     if (n > 0 && (!x || !v || !w || !s || !active)) return MCS_ERR_ARG;
     mcs_ctx* c = b->ctx;
     if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
@@ -1130,6 +1106,7 @@ MCS_API int mcs_batch_add_maxwellian(mcs_batch* b, const mcs_table* t, double ex
                                      uint64_t seed, int64_t n0, double tol, int64_t capacity, int64_t n,
                                      double mean_energy_ev, int* slot) {
     if (!b || !t || !slot || capacity < 1 || n < 0 || n > capacity || !(mean_energy_ev >= 0)) return MCS_ERR_ARG;
+    if (t && t->photo_rows) return MCS_ERR_UNSUPPORTED;   // photo-emission needs mcs_advance_mixed
     mcs_ctx* c = b->ctx;
     if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
     int k = -1;

@@ -72,6 +72,7 @@ inline StepCtl step_ctl(mcs_pop* p, double dt, uint32_t tag, double* moments_out
     s.moments_out = moments_out;
     s.dt = dt;
     s.slot_base = p->slot_base;
+    s.photo = p->photo;
     return s;
 }
 

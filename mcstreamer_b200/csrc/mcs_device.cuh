@@ -18,15 +18,20 @@ enum : uint32_t {
     ST_NONFINITE = 8u,   // NaN/Inf in particle state
     ST_OVERFLOW = 16u,   // a tile produced more secondaries than its staging holds
     ST_TIMEOUT = 32u,    // a bounded wait gave up
+    ST_UNSUPPORTED = 64u,  // a process this kernel does not apply (photo-emission without photons)
 };
 
 // Philox stream tags (4th counter word); must match the oracle.
 enum : uint32_t { TAG_ADVANCE = 0, TAG_SWARM_RESAMPLE = 1, TAG_CELL_RESAMPLE = 2, TAG_INIT = 3,
-                  TAG_COLLISIONS = 4 };
+                  TAG_COLLISIONS = 4, TAG_PHOTON = 5 };
+// Photo-emission streams of collision event j of an electron: the photon count draws from
+// {slot, step, k/4, TAG_PHOTON_COUNT | j}, photon p from {slot, step, p, TAG_PHOTON_DRAW | j}.
+constexpr uint32_t TAG_PHOTON_COUNT = 0x20000000u;
+constexpr uint32_t TAG_PHOTON_DRAW = 0x40000000u;
 
 // Process kinds; must match include/mcs.h.
 enum : int { K_NULL = 0, K_ELASTIC = 1, K_EXCITATION = 2, K_IONIZATION = 3, K_ATTACHMENT = 4,
-             K_IONIZATION_UNIFORM = 5 };
+             K_IONIZATION_UNIFORM = 5, K_PHOTOEMISSION = 6 };
 
 // ---------------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy as 1, 2, 3",
@@ -89,6 +94,35 @@ struct Event {
     }
     __device__ __forceinline__ void second() { c = philox10(U4{slot, step, (j - 1) | 0x80000000u, tag}, k0, k1); }
 };
+
+// rand(Poisson(lam)) from a stream: inversion below 10, PTRS (Hoermann 1993) above; the
+// oracle's algorithm (only the law of the reference's Distributions.Poisson is matched).
+__device__ __forceinline__ long long poisson_draw(Rng& r, double lam) {
+    if (lam <= 0) return 0;
+    if (lam < 10.0) {
+        const double u = r.u64();
+        double pr = exp(-lam), F = pr;
+        long long kk = 0;
+        while (u > F && kk < 1000) { ++kk; pr *= lam / (double)kk; F += pr; }
+        return kk;
+    }
+    const double slam = sqrt(lam), loglam = log(lam);
+    const double b = 0.931 + 2.53 * slam;
+    const double a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < 1000; ++it) {
+        const double U = r.u64() - 0.5;
+        const double V = r.u64();
+        const double us = 0.5 - fabs(U);
+        const double kf = floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return (long long)kf;
+        if (kf < 0 || (us < 0.013 && V > us)) continue;
+        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + kf * loglam - lgamma(kf + 1.0))
+            return (long long)kf;
+    }
+    return (long long)floor(lam);
+}
 
 // Initial electron of slot `slot`: an isotropic Maxwellian velocity whose components have
 // standard deviation `sigma` (m/s) and a free-flight s = -log(u).  Five uniforms of the

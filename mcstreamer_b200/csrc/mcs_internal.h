@@ -26,6 +26,29 @@ struct TableView {
     float ke32, e0n32, maxrate32;  // u = v^2*ke32 - e0n32 in grid units
     int kind[kMaxRows];
     double param[kMaxRows];
+    // PhotoEmission rows (electron.jl:88-105): log(nu_min), log(nu_max) per row,
+    // photon_multiplier, photon_weight; has_pe = 0 when the table has no such row
+    int has_pe;
+    double pe_mult, pe_pw;
+    double pe_lmin[kMaxRows], pe_lmax[kMaxRows];
+};
+
+// One photo-emission event of a step: `nphot` photons of parent slot `slot` (local to the
+// launch), collision event `jev`, at positions [poff, poff + nphot) among that parent's
+// photons of the step.
+struct PhotoEvent {
+    double x, y, z;
+    uint32_t slot, jev, poff, nphot;
+    int row;
+    uint32_t act;
+};
+
+// Where a step kernel records photo-emission (all null: photo-emission is unsupported).
+struct PhotoOut {
+    PhotoEvent* events;
+    uint32_t* count;     // events recorded (device counter)
+    uint32_t cap;        // events room
+    uint32_t* per_slot;  // photons per parent slot (n_entry entries)
 };
 
 // Unsigned 32-bit division by an invariant divisor with one multiply-high (Granlund &
@@ -98,6 +121,7 @@ struct StepCtl {
     unsigned long long stage_stride;
     uint32_t stage_cap;       // entries per CTA
     uint32_t slot_base;       // added to the slot index that keys a particle's random stream
+    PhotoOut photo;           // photo-emission output (k_step_abs only)
 };
 
 }  // namespace mcs
@@ -118,6 +142,7 @@ struct mcs_ctx {
 struct mcs_table {
     mcs_ctx* ctx = nullptr;
     mcs::TableView v{};
+    bool photo_rows = false;   // has MCS_PHOTOEMISSION rows (only mcs_advance_mixed applies them)
     double* d_rate64 = nullptr;
     float* d_rate32 = nullptr;
 };
@@ -151,6 +176,7 @@ struct mcs_pop {
     long long cap = 0;
     size_t esz = 8;                // bytes per float field
     uint32_t slot_base = 0;        // stream slot of slot 0 (a chunk of a larger population)
+    mcs::PhotoOut photo{};         // set by mcs_advance_mixed for the duration of its step
     void* f[8] = {};
     uint32_t* cell = nullptr;
     uint8_t* act = nullptr;

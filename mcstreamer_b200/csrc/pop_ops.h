@@ -26,6 +26,8 @@ int map_status(uint32_t st);
 const char* status_text(int code);
 // Wait for the context's stream and turn the sticky device status into an error code.
 int sync_status(mcs_ctx* c);
+// The slot of the population's per-step sums for its next step (nullptr: no log).
+double* log_slot(mcs_pop* p);
 // (threads per block, particles per thread, CTAs per SM) of an FP32 mesh-step shape.
 int mesh_shape_info(int shape, int* block, int* ppt, int* minb);
 constexpr int kMomentPartialsMin = 148 * 2 * (MCS_MOMENTS_BASE + kMaxRows);

@@ -114,7 +114,7 @@ __device__ __forceinline__ int select_row32(const TableView& t, float v2, float 
 // Outcome of a collision: nothing (null), new particle, removal, velocity change.
 // collide64/collide32 report OUT_NONE for the velocity-changing kinds; collide_once
 // turns that into OUT_CHANGE.
-enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2, OUT_CHANGE = 3 };
+enum { OUT_NONE = 0, OUT_NEW = 1, OUT_REMOVE = 2, OUT_CHANGE = 3, OUT_PHOTO = 4 };
 
 template <typename T>
 struct Sec { T vx, vy, vz, s; };
@@ -165,6 +165,7 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Event
         return OUT_NEW;
     }
     if (kind == K_ATTACHMENT) return OUT_REMOVE;
+    if (kind == K_PHOTOEMISSION) return OUT_PHOTO;   // the electron is unchanged
     return OUT_NONE;
 }
 
@@ -207,6 +208,7 @@ __device__ __forceinline__ int collide32(int kind, float par, float v2, Event& e
         return OUT_NEW;
     }
     if (kind == K_ATTACHMENT) return OUT_REMOVE;
+    if (kind == K_PHOTOEMISSION) return OUT_PHOTO;
     return OUT_NONE;
 }
 

@@ -197,7 +197,7 @@ __device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long lo
 // Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
 template <typename T, typename RowsT>
 __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Event& rng,
-                                            T& vx, T& vy, T& vz, Sec<T>& sec) {
+                                            T& vx, T& vy, T& vz, Sec<T>& sec, int* row_out = nullptr) {
     int j;
     double eng = 0.0;
     float v2 = 0.0f;
@@ -212,6 +212,7 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
         j = select_row32(tab, v2, xi, C.flags, C.status);
     }
     const int kind = j >= 0 ? rows.kind[j] : K_NULL;
+    if (row_out) *row_out = j;
     if (kind == K_NULL) return OUT_NONE;
     int out;
     if constexpr (sizeof(T) == 8) {
@@ -228,6 +229,35 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
         sec.vx = s32.vx; sec.vy = s32.vy; sec.vz = s32.vz; sec.s = s32.s;
     }
     return out == OUT_NONE ? OUT_CHANGE : out;
+}
+
+// apply!(::MultiplePhotonOutcome) of an electron's photo-emission (electron.jl:141-144,
+// collisions.jl:125-141): rand(Poisson(w / photon_multiplier / photon_weight)) photons of
+// collision event `jev` at (x, y, z).  The photons themselves are made after the step, in
+// serial parent order, from the recorded event (photons.cu); `pcnt` counts the parent's
+// photons of the step so far.
+__device__ __forceinline__ void photo_event(const StepCtl& C, const TableView& tab, int row, uint32_t slot_local,
+                                            uint32_t jev, double x, double y, double z, double w, uint8_t act,
+                                            uint32_t& pcnt) {
+    if (!C.photo.events) {
+        atomicOr(C.status, ST_UNSUPPORTED);
+        return;
+    }
+    Rng r;
+    r.init(C.seed, slot_local + C.slot_base, C.step, TAG_PHOTON_COUNT | jev);
+    const long long n = poisson_draw(r, w / tab.pe_mult / tab.pe_pw);
+    if (n <= 0) return;
+    const uint32_t e = atomicAdd(C.photo.count, 1u);
+    if (e < C.photo.cap) {
+        PhotoEvent ev;
+        ev.x = x; ev.y = y; ev.z = z;
+        ev.slot = slot_local; ev.jev = jev; ev.poff = pcnt; ev.nphot = (uint32_t)n;
+        ev.row = row; ev.act = act;
+        C.photo.events[e] = ev;
+    } else {
+        atomicOr(C.status, ST_OVERFLOW);
+    }
+    pcnt += (uint32_t)n;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -260,6 +290,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
             const uint32_t local = jj * BLOCK + threadIdx.x;
             const long long i = base + local;
             uint32_t ev = 0;
+            uint32_t pcnt = 0;   // photons emitted by this particle in this step
             if (i < n_entry && P.act[i]) {
                 Event rng;
                 rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
@@ -305,8 +336,19 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                             cvz = fmaf((float)az, tau, (float)vz);
                         }
                         Sec<T> sec;
-                        const int out = collide_once<T>(sh.rows, tab, C, rng, cvx, cvy, cvz, sec);
-                        if (out != OUT_NONE) {
+                        int row = -1;
+                        const int out = collide_once<T>(sh.rows, tab, C, rng, cvx, cvy, cvz, sec, &row);
+                        if (out == OUT_PHOTO) {
+                            double px = (double)x, py = (double)y, pz = (double)z;
+                            if constexpr (CLOSED) {   // the position at the collision time
+                                const float h2 = 0.5f * tau * tau;
+                                px = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
+                                py = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
+                                pz = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
+                            }
+                            photo_event(C, tab, row, local + (uint32_t)base, rng.j - 1, px, py, pz, (double)w, act,
+                                        pcnt);
+                        } else if (out != OUT_NONE) {
                             if constexpr (CLOSED) {  // settle the segment at the collision time
                                 const float h2 = 0.5f * tau * tau;
                                 x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
@@ -343,6 +385,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                 P.f[7][i] = (T)s;
                 if (!act) P.act[i] = 0;
             }
+            if (C.photo.per_slot && i < n_entry) C.photo.per_slot[i] = pcnt;
             sh.cnt[local] = ev;
         }
         __syncthreads();
@@ -409,6 +452,7 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
                     const T w = P.f[6][i];
                     Sec<T> sec;
                     const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
+                    if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
                     if (out == OUT_NEW) {
                         if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
                         const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
@@ -692,6 +736,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             if (collides) {
                 Sec<T> sec;
                 const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
+                if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
                 if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
                     cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
                               out == OUT_NEW ? (double)w : -(double)w);

@@ -72,6 +72,11 @@ class CollisionTable:
             self.ctx.h, rate.shape[1], rate.shape[0], table.energy.e0, table.energy.emax, L.dptr(rate),
             L.i32ptr(kinds), L.dptr(params), table.maxrate, C.byref(h)))
         self.h = h
+        if getattr(table, "has_photoemission", False):
+            lmin = np.ascontiguousarray(table.pe_lmin)
+            lmax = np.ascontiguousarray(table.pe_lmax)
+            self.ctx.check(self.ctx.lib.mcs_table_set_photoemission(self.h, L.dptr(lmin), L.dptr(lmax),
+                                                                   table.photon_multiplier, table.photon_weight))
 
     def __len__(self) -> int:
         return len(self.proc)
@@ -228,6 +233,71 @@ class Population:
         if self.h:
             self.ctx.lib.mcs_pop_destroy(self.h)
             self.h = None
+
+
+@dataclass
+class PhotonArrays:
+    """Host PhotonState arrays (JuMC/src/photon.jl:11-18), Julia layout."""
+
+    x: np.ndarray        # (n, 3)
+    v: np.ndarray        # (n, 3)
+    nu: np.ndarray       # absorption rate (1/s)
+    w: np.ndarray
+    s: np.ndarray
+    active: np.ndarray   # uint8
+
+    @staticmethod
+    def empty(n: int) -> "PhotonArrays":
+        return PhotonArrays(np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(n), np.zeros(n),
+                            np.zeros(n, np.uint8))
+
+
+class Photons:
+    """The photon population of a streamer run (MCStreamer/src/main.jl:115-121): FP64,
+    collisions at maxrate numax (ZhelezniakCollisions)."""
+
+    def __init__(self, capacity: int, numax: float, seed: int = 0, ctx: Optional[Context] = None,
+                 photons: Optional[PhotonArrays] = None):
+        self.ctx = ctx or Context.default()
+        self.capacity, self.numax = int(capacity), float(numax)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.mcs_photons_create(self.ctx.h, self.capacity, self.numax, int(seed), C.byref(h)))
+        self.h = h
+        if photons is not None:
+            self.upload(photons)
+
+    def upload(self, p: PhotonArrays) -> None:
+        n = len(p.w)
+        a = [np.ascontiguousarray(q, dtype=np.float64) for q in (p.x, p.v, p.nu, p.w, p.s)]
+        act = np.ascontiguousarray(p.active, dtype=np.uint8)
+        self.ctx.check(self.ctx.lib.mcs_photons_upload(self.h, *(L.dptr(q) for q in a), L.u8ptr(act), n))
+
+    def count(self) -> int:
+        n = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_photons_count(self.h, C.byref(n)))
+        return n.value
+
+    def download(self) -> PhotonArrays:
+        n = self.count()
+        out = PhotonArrays.empty(n)
+        nn = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_photons_download(self.h, L.dptr(out.x), L.dptr(out.v), L.dptr(out.nu),
+                                                         L.dptr(out.w), L.dptr(out.s), L.u8ptr(out.active), n,
+                                                         C.byref(nn)))
+        return out
+
+    def close(self) -> None:
+        if self.h:
+            self.ctx.lib.mcs_photons_destroy(self.h)
+            self.h = None
+
+
+def advance_mixed(electrons: "Population", photons: Photons, efield, dt: float, tracker=None) -> None:
+    """advance!(mpopl, efield, dt, tracker) with MultiPopulation(electron, photon)
+    (mixed_population.jl:24-54): photo-emission adds photons, photo-ionization electrons."""
+    electrons.ctx.check(electrons.ctx.lib.mcs_advance_mixed(electrons.h, photons.h, electrons.collisions.h,
+                                                            efield.h, dt,
+                                                            tracker.h if tracker is not None else None))
 
 
 class MultiPopulation:

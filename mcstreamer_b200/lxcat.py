@@ -6,8 +6,10 @@ cross section into a collision rate nu_j(eps) = N * v(eps) * sigma_j(eps) on a u
 energy grid, adds the null-collision row and sorts the rows by their sum over the grid.
 The result feeds mcs_table_create unchanged (CollisionTable, collisions.jl:9-22).
 
-PHOTOEMISSION records (lxcat.jl:57-60,86-93) belong to the photon population, which is
-outside this library's scope; they raise NotImplementedError.
+PHOTOEMISSION records (lxcat.jl:57-60,86-93) give rows of kind PHOTOEMISSION: their cross
+section is scaled by photon_multiplier, and their absorption band nu_min..nu_max = c *
+N(absorber) * chi_min..chi_max is kept as log(nu) per row (PhotoEmission, electron.jl:88-105);
+photon_numax is the photon population's maxrate (MCStreamer/src/main.jl:115-118).
 """
 from __future__ import annotations
 
@@ -19,10 +21,10 @@ from typing import Iterable, Mapping, Sequence
 import numpy as np
 
 from . import constants as co
-from ._lib import ATTACHMENT, ELASTIC, EXCITATION, IONIZATION, IONIZATION_UNIFORM, NULL
+from ._lib import ATTACHMENT, ELASTIC, EXCITATION, IONIZATION, IONIZATION_UNIFORM, NULL, PHOTOEMISSION
 
 KIND_NAMES = {NULL: "NULL", ELASTIC: "ELASTIC", EXCITATION: "EXCITATION", IONIZATION: "IONIZATION",
-              ATTACHMENT: "ATTACHMENT", IONIZATION_UNIFORM: "IONIZATION_UNIFORM"}
+              ATTACHMENT: "ATTACHMENT", IONIZATION_UNIFORM: "IONIZATION_UNIFORM", PHOTOEMISSION: "PHOTOEMISSION"}
 
 
 @dataclass(frozen=True)
@@ -54,6 +56,8 @@ class Process:
     param: float          # threshold (J) or mass ratio
     target: str
     signature: str
+    lmin: float = 0.0     # PHOTOEMISSION: log(nu_min), log(nu_max) (1/s)
+    lmax: float = 0.0
 
 
 @dataclass
@@ -66,10 +70,33 @@ class LXCatTable:
     origperm: np.ndarray   # invperm(perm)
     energy: EnergyGrid
     perm: np.ndarray = field(default=None)
+    photon_multiplier: float = 1.0
+    photon_weight: float = 1.0
 
     @property
     def kinds(self) -> np.ndarray:
         return np.array([p.kind for p in self.proc], dtype=np.int32)
+
+    @property
+    def has_photoemission(self) -> bool:
+        return any(p.kind == PHOTOEMISSION for p in self.proc)
+
+    @property
+    def pe_lmin(self) -> np.ndarray:
+        return np.array([p.lmin for p in self.proc], dtype=np.float64)
+
+    @property
+    def pe_lmax(self) -> np.ndarray:
+        return np.array([p.lmax for p in self.proc], dtype=np.float64)
+
+    @property
+    def photon_numax(self) -> float:
+        """ZhelezniakCollisions(exp(log_numax)) of the first PhotoEmission row
+        (MCStreamer/src/main.jl:115-118)."""
+        for p in self.proc:
+            if p.kind == PHOTOEMISSION:
+                return float(np.exp(p.lmax))
+        raise ValueError("no PHOTOEMISSION process")
 
     @property
     def params(self) -> np.ndarray:
@@ -110,7 +137,7 @@ def _kind_of(item: Mapping) -> int:
     if k == "ATTACHMENT":
         return ATTACHMENT
     if k == "PHOTOEMISSION":
-        raise NotImplementedError("PHOTOEMISSION processes (photon population) are not supported")
+        return PHOTOEMISSION
     raise ValueError(f"unknown process kind {k!r}")
 
 
@@ -121,8 +148,9 @@ def _signature(item: Mapping) -> str:
 
 
 def load_lxcat_records(db: Sequence[Mapping], densities: Mapping[str, float],
-                       energy: EnergyGrid = DEFAULT_ENERGY) -> LXCatTable:
-    """load_lxcat on already-parsed records (lxcat.jl:30-134)."""
+                       energy: EnergyGrid = DEFAULT_ENERGY, photon_weight: float = 1.0,
+                       photon_multiplier: float = 1.0) -> LXCatTable:
+    """load_lxcat on already-parsed records (lxcat.jl:17-134)."""
     eng = energy.values()
     v = np.sqrt(2.0 * eng / co.electron_mass)
     targets: dict[str, list[dict]] = {}
@@ -143,7 +171,7 @@ def load_lxcat_records(db: Sequence[Mapping], densities: Mapping[str, float],
         if "weight_scale" in item:
             cs0 *= item["weight_scale"]
         if item["kind"] == "PHOTOEMISSION":
-            raise NotImplementedError("PHOTOEMISSION processes (photon population) are not supported")
+            cs0 *= photon_multiplier
         item["nu"] = dens * v * _interp_flat(energy0, cs0, eng)
         tgt.append(item)
         nprocs += 1
@@ -163,7 +191,13 @@ def load_lxcat_records(db: Sequence[Mapping], densities: Mapping[str, float],
         for item in ps:
             kind = _kind_of(item)
             par = float(item["mass_ratio"]) if kind == ELASTIC else float(item.get("threshold", 0.0)) * co.eV
-            proc.append(Process(kind, par, name, _signature(item)))
+            pr = Process(kind, par, name, _signature(item))
+            if kind == PHOTOEMISSION:
+                par = 0.0
+                nu_abs = co.speed_of_light * densities[item["absorber"]]
+                pr = Process(kind, 0.0, name, _signature(item), float(np.log(nu_abs * item["chi_min"])),
+                             float(np.log(nu_abs * item["chi_max"])))
+            proc.append(pr)
             rate[i, :] = item["nu"]
             i += 1
 
@@ -175,17 +209,19 @@ def load_lxcat_records(db: Sequence[Mapping], densities: Mapping[str, float],
     perm = np.argsort(-inteng, kind="stable")      # sortperm(inteng, rev=true)
     origperm = np.argsort(perm, kind="stable")      # invperm(perm)
     return LXCatTable([proc[k] for k in perm], np.ascontiguousarray(rate[perm, :]), maxrate, origperm,
-                      energy, perm)
+                      energy, perm, photon_multiplier, photon_weight)
 
 
 def load_lxcat(fnames: Iterable[str | Path], densities: Mapping[str, float],
-               energy: EnergyGrid = DEFAULT_ENERGY) -> LXCatTable:
-    """load_lxcat(fnames, densities, energy) (JuMC/src/lxcat.jl:17)."""
+               energy: EnergyGrid = DEFAULT_ENERGY, photon_weight: float = 1.0,
+               photon_multiplier: float = 1.0) -> LXCatTable:
+    """load_lxcat(fnames, densities, energy; photon_weight, photon_multiplier)
+    (JuMC/src/lxcat.jl:17)."""
     db: list[dict] = []
     for fn in fnames:
         with open(fn) as fd:
             db.extend(json.load(fd))
-    return load_lxcat_records(db, densities, energy)
+    return load_lxcat_records(db, densities, energy, photon_weight, photon_multiplier)
 
 
 # ---------------------------------------------------------------------------------------
@@ -237,3 +273,25 @@ def synthetic_records(variant: int = 0, target: str = "SYN", uniform_sharing: bo
 def synthetic_table(variant: int = 0, energy: EnergyGrid = DEFAULT_ENERGY, density: float = SYNTHETIC_DENSITY,
                     uniform_sharing: bool = True) -> LXCatTable:
     return load_lxcat_records(synthetic_records(variant, uniform_sharing=uniform_sharing), {"SYN": density}, energy)
+
+
+def synthetic_photo_records(target: str = "SYN", absorber: str = "ABS", chi_min: float = 1e-23,
+                            chi_max: float = 6e-21, rescale: float = 2e-3) -> list[dict]:
+    """A synthetic PHOTOEMISSION record in the format the reference reads (kind, target,
+    absorber, chi_min, chi_max, rescale; lxcat.jl:57-60,86-93): a cross section rising
+    linearly from 15.6 eV to 2.5e-20 m^2 at 100 eV, then flat, on the log grid."""
+    e = LOG_GRID_EV
+    return [{"kind": "PHOTOEMISSION", "target": target, "absorber": absorber, "chi_min": chi_min,
+             "chi_max": chi_max, "rescale": rescale, "comment": "synthetic photo-emission",
+             "data": [[float(a), float(b)] for a, b in zip(e, _ramp(e, 15.6, 100.0, 2.5e-20))]}]
+
+
+def synthetic_photo_table(variant: int = 0, energy: EnergyGrid = DEFAULT_ENERGY, density: float = SYNTHETIC_DENSITY,
+                          absorber_density: float = 0.2 * SYNTHETIC_DENSITY, photon_weight: float = 1.0,
+                          photon_multiplier: float = 1000.0, **photo) -> LXCatTable:
+    """Synthetic gas `variant` plus one photo-emission process whose photons are absorbed by a
+    species of density `absorber_density` (the reference's sample input uses
+    photon_multiplier = 1000, photon_weight = 1)."""
+    recs = synthetic_records(variant) + synthetic_photo_records(**photo)
+    return load_lxcat_records(recs, {"SYN": density, "ABS": absorber_density}, energy, photon_weight,
+                              photon_multiplier)

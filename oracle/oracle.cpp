@@ -30,17 +30,19 @@
 namespace {
 
 /* internal status flags, mapped to the public codes by status_code() */
-enum { F_CAP = 1, F_ENERGY = 2, F_FIELD = 4 };
+enum { F_CAP = 1, F_ENERGY = 2, F_FIELD = 4, F_UNSUPPORTED = 8 };
 inline int status_code(int f) {
     if (f & F_CAP) return 3;
     if (f & F_ENERGY) return 4;
     if (f & F_FIELD) return 5;
+    if (f & F_UNSUPPORTED) return 7;
     return 0;
 }
 
 /* ---------------- constants: JuMC/src/constants.jl:50-54 ---------------- */
 const double ELEMENTARY_CHARGE = 1.6021766208e-19;
 const double ELECTRON_MASS = 9.10938356e-31;
+const double SPEED_OF_LIGHT = 299792458.0;   /* co.c (Constants/src/Constants.jl:39) */
 
 /* Yoshida-4 coefficients: JuMC/src/electron.jl:38-46 */
 struct Yoshida {
@@ -361,6 +363,7 @@ int indweight(const orc_table* t, double eng, int64_t* k, double* w, int clamp) 
 }
 
 struct Secondary { double x[3], v[3], w, s; uint8_t active; };
+struct PhotonOut { double x[3], v[3], nu, w, s; uint8_t active; };
 
 struct StepCtx {
     const orc_table* tab;
@@ -370,7 +373,65 @@ struct StepCtx {
     std::vector<Secondary>* out;
     int clamp;
     int status;
+    std::vector<PhotonOut>* photons;   /* photo-emission output (NULL: rows rejected) */
 };
+
+/* Poisson sampler: inversion for lambda < 10, PTRS (Hoermann 1993) otherwise.
+ * The reference draws Distributions.Poisson (Swarm.jl:216); only the law is matched. */
+int64_t poisson_sample(Stream& rng, double lam) {
+    if (lam <= 0) return 0;
+    if (lam < 10.0) {
+        const double u = rng.next();
+        double p = std::exp(-lam), F = p;
+        int64_t k = 0;
+        while (u > F && k < 1000) { ++k; p *= lam / (double)k; F += p; }
+        return k;
+    }
+    const double slam = std::sqrt(lam), loglam = std::log(lam);
+    const double b = 0.931 + 2.53 * slam;
+    const double a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
+    const double vr = 0.9277 - 3.6224 / (b - 2.0);
+    for (int it = 0; it < 1000; ++it) {
+        const double U = rng.next() - 0.5;
+        const double V = rng.next();
+        const double us = 0.5 - std::fabs(U);
+        const double kf = std::floor((2.0 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return (int64_t)kf;
+        if (kf < 0 || (us < 0.013 && V > us)) continue;
+        if (std::log(V) + std::log(invalpha) - std::log(a / (us * us) + b) <=
+            -lam + kf * loglam - std::lgamma(kf + 1.0))
+            return (int64_t)kf;
+    }
+    return (int64_t)std::floor(lam);
+}
+
+/* collide(::PhotoEmission) + apply!(::MultiplePhotonOutcome) (electron.jl:141-144,
+ * collisions.jl:125-141): the electron is unchanged; rand(Poisson(w / multiplier /
+ * photon_weight)) photons at its position, each with randsphere() * c, nu = exp(log_numin +
+ * (log_numax - log_numin) rand()), weight photon_weight, nextcoll() and the electron's
+ * active flag.  No charge is tracked. */
+void photo_emit(StepCtx& c, const Event& rng, int row, const double x[3], double w, uint8_t active) {
+    const orc_table* t = c.tab;
+    const uint64_t seed = (uint64_t)rng.key[0] | ((uint64_t)rng.key[1] << 32);
+    const uint32_t jev = rng.j - 1;
+    Stream cnt(seed, rng.c0, rng.c1, ORC_TAG_PHOTON_COUNT | jev);
+    const int64_t n = poisson_sample(cnt, w / t->pe_mult / t->pe_pw);
+    Stream ps(seed, rng.c0, rng.c1, ORC_TAG_PHOTON_DRAW | jev);
+    const double lmin = t->pe_lmin[row], lmax = t->pe_lmax[row];
+    for (int64_t p = 0; p < n; ++p) {
+        PhotonOut ph;
+        const double uphi = ps.next(), uu = ps.next();
+        double d[3];
+        randsphere(uphi, uu, d);
+        for (int q = 0; q < 3; ++q) { ph.x[q] = x[q]; ph.v[q] = d[q] * SPEED_OF_LIGHT; }
+        ph.nu = std::exp(lmin + (lmax - lmin) * ps.next());
+        ph.w = t->pe_pw;
+        ph.s = -std::log(ps.next());
+        ph.active = active;
+        c.photons->push_back(ph);
+    }
+}
 
 /* do_one_collision!: JuMC/src/collisions.jl:159-192 with collide (electron.jl:108-139),
  * track (collisions.jl:151, gridfields.jl:215-224) and apply! (collisions.jl:96-123). */
@@ -426,6 +487,9 @@ void do_one_collision(StepCtx& c, Event& rng, double x[3], double v[3], double& 
             } else if (kind == ORC_ATTACHMENT) {
                 track_charge(c.trk, x, -w, c.cyl_local);      /* RemoveParticleOutcome: -w */
                 active = 0;
+            } else if (kind == ORC_PHOTOEMISSION) {
+                if (c.photons) photo_emit(c, rng, j, x, w, active);
+                else c.status |= F_UNSUPPORTED;
             }
             /* ORC_NULL: NullOutcome, nothing */
             return;
@@ -449,19 +513,29 @@ void run_chunks(int64_t n, int nthreads, const std::function<void(int, int64_t, 
  * chunks, then appends secondaries in chunk order (== serial parent order). */
 int drive(orc_pop* pop, const orc_table* tab, const orc_field* fld, orc_tracker* trk,
           int nthreads, int clamp,
-          const std::function<void(StepCtx&, int64_t)>& per_particle) {
+          const std::function<void(StepCtx&, int64_t)>& per_particle, orc_photons* ph_out = nullptr) {
     if (nthreads < 1) nthreads = 1;
     const int64_t n_entry = pop->n;
     std::vector<std::vector<Secondary>> outs(nthreads);
+    std::vector<std::vector<PhotonOut>> phs(nthreads);
     std::vector<std::vector<double>> cyl(nthreads);
     std::vector<int> status(nthreads, 0);
     const bool is_cyl = trk && trk->type == ORC_TRACK_CYL;
     run_chunks(n_entry, nthreads, [&](int t, int64_t lo, int64_t hi) {
         if (is_cyl) cyl[t].assign((size_t)(trk->M + 2) * (trk->N + 2), 0.0);
-        StepCtx c{tab, fld, trk, &cyl[t], &outs[t], clamp, 0};
+        StepCtx c{tab, fld, trk, &cyl[t], &outs[t], clamp, 0, ph_out ? &phs[t] : nullptr};
         for (int64_t i = lo; i < hi; ++i) per_particle(c, i);
         status[t] = c.status;
     });
+    /* photons in serial parent order (add_particle!(photons, p2), collisions.jl:138) */
+    if (ph_out)
+        for (int t = 0; t < nthreads; ++t)
+            for (const PhotonOut& ph : phs[t]) {
+                if (ph_out->n >= ph_out->cap) { status[t] |= F_CAP; continue; }
+                const int64_t m = ph_out->n++;
+                for (int q = 0; q < 3; ++q) { ph_out->x[3 * m + q] = ph.x[q]; ph_out->v[3 * m + q] = ph.v[q]; }
+                ph_out->nu[m] = ph.nu; ph_out->w[m] = ph.w; ph_out->s[m] = ph.s; ph_out->active[m] = ph.active;
+            }
     int st = 0;
     for (int t = 0; t < nthreads; ++t) st |= status[t];
     if (is_cyl) {
@@ -507,8 +581,8 @@ int orc_indweight(const orc_table* tab, double eng, int64_t* k, double* w) {
 void orc_yoshida(const orc_field* fld, double x[3], double v[3], double dt) { yoshida(fld, x, v, dt); }
 
 /* advance!: JuMC/src/mixed_population.jl:24-54 */
-int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
-                orc_tracker* trk, int nthreads, int clamp_energy) {
+static int advance_electrons(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
+                             orc_tracker* trk, int nthreads, int clamp_energy, orc_photons* ph_out) {
     const uint64_t seed = pop->seed;
     const uint32_t step = pop->step;
     return drive(pop, tab, fld, trk, nthreads, clamp_energy, [&](StepCtx& c, int64_t i) {
@@ -534,7 +608,91 @@ int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double
         }
         for (int q = 0; q < 3; ++q) { pop->x[3 * i + q] = x[q]; pop->v[3 * i + q] = v[q]; }
         pop->w[i] = w; pop->s[i] = s; pop->active[i] = active;
+    }, ph_out);
+}
+
+int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
+                orc_tracker* trk, int nthreads, int clamp_energy) {
+    return advance_electrons(pop, tab, fld, dt, trk, nthreads, clamp_energy, nullptr);
+}
+
+/* advance! of the photon population (mixed_population.jl:24-54 with the
+ * ZhelezniakCollisions table, photon.jl:27-56): straight flight x + t v; at a collision
+ * xi = rand() * numax and PhotoIonization when nu > xi: the tracker adds +w at the photon
+ * (gridfields.jl:219-222), the photon is removed and an electron at rest with its weight,
+ * nextcoll() and the photon's active flag is added.  A removed photon keeps sub-stepping to
+ * the end of the step, as the reference's loop does, so it can photo-ionize again. */
+int orc_photon_advance(orc_photons* ph, orc_pop* e, double dt, orc_tracker* trk, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    const int64_t n_entry = ph->n;
+    std::vector<std::vector<Secondary>> outs(nthreads);
+    std::vector<std::vector<double>> cyl(nthreads);
+    const bool is_cyl = trk && trk->type == ORC_TRACK_CYL;
+    const double numax = ph->numax;
+    run_chunks(n_entry, nthreads, [&](int t, int64_t lo, int64_t hi) {
+        if (is_cyl) cyl[t].assign((size_t)(trk->M + 2) * (trk->N + 2), 0.0);
+        for (int64_t i = lo; i < hi; ++i) {
+            if (!ph->active[i]) continue;
+            Event rng(ph->seed, (uint32_t)i, ph->step, ORC_TAG_PHOTON);
+            double x[3] = {ph->x[3 * i], ph->x[3 * i + 1], ph->x[3 * i + 2]};
+            const double v[3] = {ph->v[3 * i], ph->v[3 * i + 1], ph->v[3 * i + 2]};
+            const double nu = ph->nu[i], w = ph->w[i];
+            double s = ph->s[i];
+            uint8_t active = 1;
+            double trem = dt;
+            while (trem > 0) {
+                const double tnext = s / numax;
+                double tt;
+                bool collides;
+                if (trem > tnext) { tt = tnext; collides = true; }
+                else { tt = trem; collides = false; s -= tt * numax; }
+                for (int q = 0; q < 3; ++q) x[q] = x[q] + tt * v[q];   /* advance_free, photon.jl:54-56 */
+                if (collides) {
+                    rng.begin();
+                    const double xi = rng.u(U_XI) * numax;
+                    if (nu > xi) {
+                        track_charge(trk, x, w, &cyl[t]);
+                        Secondary sec;
+                        for (int q = 0; q < 3; ++q) { sec.x[q] = x[q]; sec.v[q] = 0.0; }
+                        sec.w = w;
+                        sec.s = nextcoll(rng.u(U_PHI));
+                        sec.active = active;
+                        outs[t].push_back(sec);
+                        active = 0;
+                    }
+                    s = nextcoll(rng.u(U_S));
+                }
+                trem -= tt;
+            }
+            for (int q = 0; q < 3; ++q) ph->x[3 * i + q] = x[q];
+            ph->s[i] = s;
+            ph->active[i] = active;
+        }
     });
+    int st = 0;
+    if (is_cyl) {
+        const size_t m = (size_t)(trk->M + 2) * (trk->N + 2);
+        for (int t = 0; t < nthreads; ++t)
+            for (size_t q = 0; q < m; ++q) trk->qcyl[q] += cyl[t][q];
+    }
+    int64_t n = e->n;
+    for (int t = 0; t < nthreads; ++t)
+        for (const Secondary& sc : outs[t]) {
+            if (n >= e->cap) { st |= F_CAP; continue; }
+            for (int q = 0; q < 3; ++q) { e->x[3 * n + q] = sc.x[q]; e->v[3 * n + q] = sc.v[q]; }
+            e->w[n] = sc.w; e->s[n] = sc.s; e->active[n] = sc.active;
+            ++n;
+        }
+    e->n = n;
+    ph->step += 1;
+    return status_code(st);
+}
+
+int orc_advance_mixed(orc_pop* e, orc_photons* ph, const orc_table* tab, const orc_field* fld, double dt,
+                      orc_tracker* trk, int nthreads, int clamp_energy) {
+    const int st = advance_electrons(e, tab, fld, dt, trk, nthreads, clamp_energy, ph);
+    const int st2 = orc_photon_advance(ph, e, dt, trk, nthreads);
+    return st ? st : st2;
 }
 
 /* collisions!: JuMC/src/mixed_population.jl:61-77 (fixed-step variant, no push) */
@@ -586,35 +744,6 @@ int orc_repack(orc_pop* pop) {
     return 0;
 }
 
-/* Poisson sampler: inversion for lambda < 10, PTRS (Hoermann 1993) otherwise.
- * The reference draws Distributions.Poisson (Swarm.jl:216); only the law is matched. */
-static int64_t poisson_sample(Stream& rng, double lam) {
-    if (lam <= 0) return 0;
-    if (lam < 10.0) {
-        const double u = rng.next();
-        double p = std::exp(-lam), F = p;
-        int64_t k = 0;
-        while (u > F && k < 1000) { ++k; p *= lam / (double)k; F += p; }
-        return k;
-    }
-    const double slam = std::sqrt(lam), loglam = std::log(lam);
-    const double b = 0.931 + 2.53 * slam;
-    const double a = -0.059 + 0.02483 * b;
-    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
-    const double vr = 0.9277 - 3.6224 / (b - 2.0);
-    for (int it = 0; it < 1000; ++it) {
-        const double U = rng.next() - 0.5;
-        const double V = rng.next();
-        const double us = 0.5 - std::fabs(U);
-        const double kf = std::floor((2.0 * a / us + b) * U + lam + 0.43);
-        if (us >= 0.07 && V <= vr) return (int64_t)kf;
-        if (kf < 0 || (us < 0.013 && V > us)) continue;
-        if (std::log(V) + std::log(invalpha) - std::log(a / (us * us) + b) <=
-            -lam + kf * loglam - std::lgamma(kf + 1.0))
-            return (int64_t)kf;
-    }
-    return (int64_t)std::floor(lam);
-}
 
 /* Swarm.resample!: Swarm/src/Swarm.jl:193-223 */
 int orc_swarm_resample(orc_pop* pop, int64_t n0, double tol) {

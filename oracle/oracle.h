@@ -28,11 +28,16 @@ extern "C" {
 
 /* Process kinds (closed set of JuMC CollisionProcess subtypes used on the hot path). */
 enum { ORC_NULL = 0, ORC_ELASTIC = 1, ORC_EXCITATION = 2, ORC_IONIZATION = 3,
-       ORC_ATTACHMENT = 4, ORC_IONIZATION_UNIFORM = 5 };
+       ORC_ATTACHMENT = 4, ORC_IONIZATION_UNIFORM = 5, ORC_PHOTOEMISSION = 6 };
 
 /* Philox stream tags (4th counter word). */
 enum { ORC_TAG_ADVANCE = 0, ORC_TAG_SWARM_RESAMPLE = 1, ORC_TAG_CELL_RESAMPLE = 2,
-       ORC_TAG_INIT = 3, ORC_TAG_COLLISIONS = 4 };
+       ORC_TAG_INIT = 3, ORC_TAG_COLLISIONS = 4, ORC_TAG_PHOTON = 5 };
+/* Photo-emission streams of collision event j of an electron: the photon count draws
+ * from {slot, step, k/4, ORC_TAG_PHOTON_COUNT | j}, photon p from words 4p..4p+3 of
+ * {slot, step, p, ORC_TAG_PHOTON_DRAW | j} (direction phi, u; log-nu fraction; s). */
+#define ORC_TAG_PHOTON_COUNT 0x20000000u
+#define ORC_TAG_PHOTON_DRAW 0x40000000u
 
 typedef struct {
     int nrows;            /* processes incl. the null row */
@@ -43,7 +48,21 @@ typedef struct {
     const int* kind;      /* [nrows] */
     const double* param;  /* [nrows]: threshold (J) or mass ratio */
     double maxrate;       /* s^-1 */
+    /* PhotoEmission rows (electron.jl:88-105): log(nu_min), log(nu_max) per row (NULL when
+     * the table has none), photon_multiplier and photon_weight. */
+    const double* pe_lmin;
+    const double* pe_lmax;
+    double pe_mult, pe_pw;
 } orc_table;
+
+/* Photon population (JuMC/src/photon.jl:11-18): PhotonState x, v, nu, w, s, active. */
+typedef struct {
+    double* x; double* v; double* nu; double* w; double* s; uint8_t* active;
+    int64_t n, cap;
+    uint64_t seed;        /* Philox key of the photon advance */
+    uint32_t step;
+    double numax;         /* ZhelezniakCollisions(numax): the photons' maxrate */
+} orc_photons;
 
 typedef struct {
     double* x; double* v; double* w; double* s; uint8_t* active;
@@ -100,6 +119,14 @@ int orc_resample_cells(orc_pop* pop, const orc_field* grid, int ntarget, int nma
                        uint32_t call);                             /* R11 */
 /* R10: cart3d CIC int64 from f32 in-cell offsets (device quantisation) or cyl NGP. */
 void orc_deposit(const orc_pop* pop, orc_tracker* trk, double val, int quantize_f32);
+
+/* advance!(mpopl, efield, dt, tracker) over the electrons and the photons
+ * (mixed_population.jl:24-54): electrons first, photo-emission appending photons; then every
+ * photon (the new ones included), photo-ionization appending electrons. */
+int orc_advance_mixed(orc_pop* electrons, orc_photons* photons, const orc_table* tab, const orc_field* fld,
+                      double dt, orc_tracker* trk, int nthreads, int clamp_energy);
+/* The photon half alone. */
+int orc_photon_advance(orc_photons* photons, orc_pop* electrons, double dt, orc_tracker* trk, int nthreads);
 
 /* Cylindrical multigrid (poisson.cpp): Multigrid.solve with MCStreamer's configuration.
  * Arrays (M+2)x(N+2), index i + j*(M+2).  Returns the number of fmg! calls. */

@@ -13,13 +13,19 @@ pi64 = C.POINTER(C.c_int64)
 pu8 = C.POINTER(C.c_uint8)
 pi32 = C.POINTER(C.c_int)
 
-NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM = 0, 1, 2, 3, 4, 5
-TAG_ADVANCE, TAG_SWARM_RESAMPLE, TAG_CELL_RESAMPLE, TAG_INIT, TAG_COLLISIONS = 0, 1, 2, 3, 4
+NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM, PHOTOEMISSION = 0, 1, 2, 3, 4, 5, 6
+TAG_ADVANCE, TAG_SWARM_RESAMPLE, TAG_CELL_RESAMPLE, TAG_INIT, TAG_COLLISIONS, TAG_PHOTON = 0, 1, 2, 3, 4, 5
 
 
 class Table(C.Structure):
     _fields_ = [("nrows", C.c_int), ("neps", C.c_int), ("e0", C.c_double), ("de", C.c_double),
-                ("emax", C.c_double), ("rate", pd), ("kind", pi32), ("param", pd), ("maxrate", C.c_double)]
+                ("emax", C.c_double), ("rate", pd), ("kind", pi32), ("param", pd), ("maxrate", C.c_double),
+                ("pe_lmin", pd), ("pe_lmax", pd), ("pe_mult", C.c_double), ("pe_pw", C.c_double)]
+
+
+class Photons(C.Structure):
+    _fields_ = [("x", pd), ("v", pd), ("nu", pd), ("w", pd), ("s", pd), ("active", pu8), ("n", C.c_int64),
+                ("cap", C.c_int64), ("seed", C.c_uint64), ("step", C.c_uint32), ("numax", C.c_double)]
 
 
 class Pop(C.Structure):
@@ -66,6 +72,9 @@ def lib():
         L.orc_sort_cells.argtypes = [C.POINTER(Pop), C.POINTER(Field)]
         L.orc_resample_cells.argtypes = [C.POINTER(Pop), C.POINTER(Field), C.c_int, C.c_int, C.c_uint32]
         L.orc_deposit.argtypes = [C.POINTER(Pop), C.POINTER(Tracker), C.c_double, C.c_int]
+        L.orc_advance_mixed.argtypes = [C.POINTER(Pop), C.POINTER(Photons), C.POINTER(Table), C.POINTER(Field),
+                                        C.c_double, C.POINTER(Tracker), C.c_int, C.c_int]
+        L.orc_photon_advance.argtypes = [C.POINTER(Photons), C.POINTER(Pop), C.c_double, C.POINTER(Tracker), C.c_int]
         _L = L
     return _L
 
@@ -86,17 +95,26 @@ class OracleTable:
     """Keeps numpy buffers alive behind an orc_table."""
 
     def __init__(self, rate_em: np.ndarray, kinds: np.ndarray, params: np.ndarray, e0: float, emax: float,
-                 maxrate: float):
+                 maxrate: float, pe=None):
         self.rate = np.ascontiguousarray(rate_em, dtype=np.float64)
         self.kinds = np.ascontiguousarray(kinds, dtype=np.int32)
         self.params = np.ascontiguousarray(params, dtype=np.float64)
         neps, nrows = self.rate.shape
         self.s = Table(nrows, neps, e0, (emax - e0) / (neps - 1), emax, self.rate.ctypes.data_as(pd),
                        self.kinds.ctypes.data_as(pi32), self.params.ctypes.data_as(pd), maxrate)
+        if pe is not None:   # (lmin per row, lmax per row, photon_multiplier, photon_weight)
+            self.pe_lmin = np.ascontiguousarray(pe[0], dtype=np.float64)
+            self.pe_lmax = np.ascontiguousarray(pe[1], dtype=np.float64)
+            self.s.pe_lmin = self.pe_lmin.ctypes.data_as(pd)
+            self.s.pe_lmax = self.pe_lmax.ctypes.data_as(pd)
+            self.s.pe_mult, self.s.pe_pw = float(pe[2]), float(pe[3])
 
     @classmethod
     def from_lxcat(cls, t):
-        return cls(t.rate_energy_major(), t.kinds, t.params, t.energy.e0, t.energy.emax, t.maxrate)
+        pe = None
+        if getattr(t, "has_photoemission", False):
+            pe = (t.pe_lmin, t.pe_lmax, t.photon_multiplier, t.photon_weight)
+        return cls(t.rate_energy_major(), t.kinds, t.params, t.energy.e0, t.energy.emax, t.maxrate, pe)
 
 
 class OraclePop:
@@ -120,6 +138,43 @@ class OraclePop:
     def arrays(self):
         n = self.p.n
         return self.x[:n].copy(), self.v[:n].copy(), self.w[:n].copy(), self.s[:n].copy(), self.active[:n].copy()
+
+
+class OraclePhotons:
+    """Host photon population (PhotonState, JuMC/src/photon.jl:11-18) with capacity."""
+
+    def __init__(self, cap, numax, seed=0, step=0, x=None, v=None, nu=None, w=None, s=None, active=None):
+        n = 0 if w is None else len(w)
+        self.x = np.zeros((cap, 3)); self.v = np.zeros((cap, 3))
+        self.nu = np.zeros(cap); self.w = np.zeros(cap); self.s = np.zeros(cap)
+        self.active = np.zeros(cap, np.uint8)
+        if n:
+            self.x[:n] = x; self.v[:n] = v; self.nu[:n] = nu; self.w[:n] = w; self.s[:n] = s
+            self.active[:n] = active
+        self.p = Photons(self.x.ctypes.data_as(pd), self.v.ctypes.data_as(pd), self.nu.ctypes.data_as(pd),
+                         self.w.ctypes.data_as(pd), self.s.ctypes.data_as(pd), self.active.ctypes.data_as(pu8),
+                         n, cap, seed, step, numax)
+
+    @property
+    def n(self):
+        return self.p.n
+
+    def arrays(self):
+        n = self.p.n
+        return (self.x[:n].copy(), self.v[:n].copy(), self.nu[:n].copy(), self.w[:n].copy(), self.s[:n].copy(),
+                self.active[:n].copy())
+
+
+def advance_mixed(pop, photons, table, field, dt, tracker=None, threads=None, clamp=False):
+    """advance!(mpopl, efield, dt, tracker) over electrons and photons."""
+    return lib().orc_advance_mixed(C.byref(pop.p), C.byref(photons.p), C.byref(table.s), C.byref(field), dt,
+                                   C.byref(tracker) if tracker is not None else None, threads or nthreads(),
+                                   int(clamp))
+
+
+def photon_advance(photons, pop, dt, tracker=None, threads=None):
+    return lib().orc_photon_advance(C.byref(photons.p), C.byref(pop.p), dt,
+                                    C.byref(tracker) if tracker is not None else None, threads or nthreads())
 
 
 def field_uniform(ex=0.0, ey=0.0, ez=0.0):

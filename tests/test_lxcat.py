@@ -54,10 +54,18 @@ def test_effective_becomes_elastic(tmp_path):
     assert t.proc[ex].param == pytest.approx(5.0 * co.eV)
 
 
-def test_photoemission_is_rejected():
-    recs = [{"kind": "PHOTOEMISSION", "target": "A", "comment": "", "data": [[0, 1e-20], [10, 1e-20]]}]
-    with pytest.raises(NotImplementedError):
-        lxcat.load_lxcat_records(recs, {"A": 1.0}, lxcat.EnergyGrid(0.0, 1e-18, 11))
+def test_photoemission_records_need_their_absorber():
+    """PhotoEmission takes nu_min, nu_max = c * dens[absorber] * chi (lxcat.jl:86-93): a record
+    without an absorber, or with one of no density, fails as the reference's lookup does."""
+    rec = {"kind": "PHOTOEMISSION", "target": "A", "comment": "", "data": [[0, 1e-20], [10, 1e-20]],
+           "chi_min": 1e-23, "chi_max": 1e-21}
+    grid = lxcat.EnergyGrid(0.0, 1e-18, 11)
+    with pytest.raises(KeyError):
+        lxcat.load_lxcat_records([rec], {"A": 1.0}, grid)
+    with pytest.raises(KeyError):
+        lxcat.load_lxcat_records([dict(rec, absorber="B")], {"A": 1.0}, grid)
+    t = lxcat.load_lxcat_records([dict(rec, absorber="A")], {"A": 2.0}, grid, photon_multiplier=10.0)
+    assert t.has_photoemission and t.photon_multiplier == 10.0
 
 
 def test_flat_linear_interpolation_matches_numpy_interp():
