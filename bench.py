@@ -1090,6 +1090,205 @@ def run_reference_poisson(args):
     return 0
 
 
+PHOTON_METRIC = "electron and photon steps/s"
+PHOTON_SAMPLE = (1_048_576, 262_144)   # CPU sample: electrons, photons
+
+
+def photon_alg_bytes(n_photons: float) -> float:
+    """Algorithmic HBM bytes of one photon step over n photons: each photon read once
+    (x, v 48 B, nu, w, s 24 B, active 1 B) and written once (x 24 B, s 8 B, active 1 B, its
+    photo-ionization count 4 B)."""
+    return n_photons * (73.0 + 37.0)
+
+
+def photon_setup_table():
+    from mcstreamer_b200 import lxcat, workloads
+    spec = workloads.photon_step_spec()
+    t = lxcat.synthetic_photo_table(0, photon_multiplier=spec.photon_multiplier, photon_weight=spec.photon_weight)
+    j = list(t.kinds).index(6)
+    return spec, t, float(t.pe_lmin[j]), float(t.pe_lmax[j])
+
+
+def photon_cpu_sample(threads: int) -> dict:
+    """advance! over electrons and photons by the oracle on a bounded sample of the workload."""
+    from mcstreamer_b200 import workloads
+    from oracle import pyoracle as po
+    spec, t, lmin, lmax = photon_setup_table()
+    ne, nph = PHOTON_SAMPLE
+    e = workloads.photon_step_electrons(spec, ne)
+    x, v, nu, w, s, act = workloads.photon_step_photons(spec, lmin, lmax, nph)
+    opop = po.OraclePop(e.x, e.v, e.w, e.s, e.active, cap=3 * ne, seed=spec.seed)
+    oph = po.OraclePhotons(nph + ne, t.photon_numax, seed=spec.seed + 2, x=x, v=v, nu=nu, w=w, s=s, active=act)
+    otab = po.OracleTable.from_lxcat(t)
+    otrk = po.tracker_cyl(spec.R, spec.L, spec.M, spec.N)
+    t0 = time.perf_counter()
+    po.advance_mixed(opop, oph, otab, po.field_uniform(0.0, 0.0, spec.ez), spec.dt, otrk, threads=threads)
+    sec = time.perf_counter() - t0
+    return {"value": (ne + nph) / sec, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"one mixed step of {ne} electrons and {nph} photons of this workload (FP64 oracle, "
+                      f"uniform field, cyl tracker): {sec:.2f} s"}
+
+
+def photon_config(spec, extra=None):
+    c = {"workload": f"advance! over electrons and photons: cyl grid R={spec.R:g} m, L={spec.L:g} m, "
+                     f"{spec.M}x{spec.N} cells, face field ez={spec.ez:g} V/m (FieldInterp), tracker on; "
+                     f"{spec.n_e} electrons (FP32, w={spec.weight:g}, 5 eV Maxwellian, Gaussian cloud sigma "
+                     f"{spec.sigma:g} m) and {spec.n_ph} photons (FP64) restored before every step; synthetic gas 0 "
+                     f"+ photo-emission (photon_multiplier {spec.photon_multiplier:g}, photon_weight "
+                     f"{spec.photon_weight:g}); dt={spec.dt:g} s, seed {spec.seed}",
+         "l2": "particle state (4.2M x 33 B + 1M x 73 B) exceeds L2", "parallelism": "1 GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_photons(args):
+    import ctypes as C
+
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import jumc, streamer, workloads
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl")
+    torch.cuda.set_device(local)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spec, t, lmin, lmax = photon_setup_table()
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.GridCyl(spec.R, spec.L, spec.M, spec.N, ctx=ctx)
+    er = np.zeros((spec.M + 3, spec.N + 3))
+    grid.set_efield(er, np.full_like(er, spec.ez))
+    fld = streamer.FieldInterp(grid)
+    trk = streamer.CollisionTracker(grid)
+    parts = workloads.photon_step_electrons(spec)
+    ph0 = jumc.PhotonArrays(*workloads.photon_step_photons(spec, lmin, lmax))
+    snap_e = jumc.Population(spec.n_e, parts, tab, precision="fp32", seed=spec.seed + 100 * rank)
+    pop = jumc.Population(4 * spec.n_e, None, tab, precision="fp32", seed=spec.seed + 100 * rank)
+    snap_p = jumc.Photons(spec.n_ph, t.photon_numax, seed=spec.seed + 2, ctx=ctx, photons=ph0)
+    phs = jumc.Photons(8 * spec.n_ph, t.photon_numax, seed=spec.seed + 2, ctx=ctx)
+    lib = ctx.lib
+
+    def restore():
+        ctx.check(lib.mcs_pop_copy(pop.h, snap_e.h))
+        ctx.check(lib.mcs_photons_copy(phs.h, snap_p.h))
+
+    def step():
+        ctx.check(lib.mcs_advance_mixed(pop.h, phs.h, tab.h, fld.h, spec.dt, trk.h))
+
+    grid.zero(L.Q_FIXED)
+    for _ in range(args.warmup):
+        restore()
+        step()
+    torch.cuda.synchronize()
+    times, emitted, ph_ms, ph_n, e_after = [], [], [], [], []
+    with ClockSampler(local) as clk:
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            em, ne_, sm, ns = C.c_float(), C.c_int64(), C.c_float(), C.c_int64()
+            ctx.check(lib.mcs_photons_last_timing(phs.h, C.byref(em), C.byref(ne_), C.byref(sm), C.byref(ns)))
+            emitted.append(ne_.value)
+            ph_ms.append(sm.value)
+            ph_n.append(ns.value)
+        torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    if ws > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms = total_ms / args.steps
+    n_part = spec.n_e + spec.n_ph
+    value = ws * n_part * 1e3 / ms
+    pk, src = peaks()
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    step_ms = statistics.median(ph_ms)
+    n_step = statistics.median(ph_n)
+    ach = photon_alg_bytes(n_step) / (step_ms * 1e-3) / 1e9 if step_ms > 0 else 0.0
+
+    # end to end: both populations uploaded from host arrays (Julia layout) into the
+    # workspaces, the mixed step, both downloaded
+    e2e_t, d2h = [], 0
+    for k in range(max(1, args.e2e_steps) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pop.upload(parts)
+        phs.upload(ph0)
+        ctx.check(lib.mcs_advance_mixed(pop.h, phs.h, tab.h, fld.h, spec.dt, trk.h))
+        out_e, out_p = pop.download(), phs.download()
+        dt_ = time.perf_counter() - t0
+        d2h = out_e.n * (8 * 8 + 1) + len(out_p.w) * (10 * 8 + 1)
+        if k:
+            e2e_t.append(dt_)
+    e2e_v = n_part / statistics.median(e2e_t)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = photon_cpu_sample(os.cpu_count() or 1)
+    line = {
+        "metric": PHOTON_METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 electrons, f64 photons", "data": "synthetic",
+        "config": photon_config(spec, {"photons_emitted_per_step": int(statistics.median(emitted)),
+                                       "photons_stepped_per_step": int(n_step),
+                                       "electron_steps_per_s": ws * spec.n_e * 1e3 / ms}),
+        "roofline": {"kernel": "k_photon_step (photon flight + photo-ionization)", "bound": "hbm",
+                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "peak_source": src, "launch_ms": step_ms, "alg_bytes_per_launch": photon_alg_bytes(n_step)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": spec.n_e * (8 * 8 + 1) + spec.n_ph * (10 * 8 + 1),
+                "d2h_bytes_per_step": d2h,
+                "path": "mcs_pop_upload + mcs_photons_upload (host arrays) -> mcs_advance_mixed -> "
+                        "mcs_pop_download + mcs_photons_download"},
+        "clocks": clk.summary(),
+        # k_step_abs, 3 scan kernels, k_photon_emit, k_photon_step, 3 scan kernels,
+        # k_ion_scatter, k_set_count
+        "gpu_launches": 11,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fld.close(); trk_close = getattr(trk, "close", None)
+    if trk_close:
+        trk_close()
+    phs.close(); snap_p.close(); pop.close(); snap_e.close(); grid.close(); tab.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_photons(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.photon_step_spec()
+    threads = os.cpu_count() or 1
+    runs = [photon_cpu_sample(threads) for _ in range(max(1, min(args.steps, 3)))]
+    v = statistics.median(r["value"] for r in runs)
+    line = {
+        "impl": "reference", "metric": PHOTON_METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "steps": len(runs), "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": photon_config(spec),
+        "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": runs[-1]["sample"]},
+        "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_batch(args):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -1122,6 +1321,8 @@ def main():
         return run_reference_batch(args) if args.impl == "reference" else run_batch(args)
     if args.workload == "poisson":
         return run_reference_poisson(args) if args.impl == "reference" else run_poisson(args)
+    if args.workload == "photons":
+        return run_reference_photons(args) if args.impl == "reference" else run_photons(args)
     if args.workload == "cfg4":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU reference arm; "

@@ -356,6 +356,12 @@ MCS_API int mcs_photons_upload(mcs_photons* ph, const double* x, const double* v
 MCS_API int mcs_photons_download(mcs_photons* ph, double* x, double* v, double* nu, double* w, double* s,
                                  uint8_t* active, int64_t capacity, int64_t* n_out);
 MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n);
+/* dst <- src on the device (a snapshot of a photon population). */
+MCS_API int mcs_photons_copy(mcs_photons* dst, const mcs_photons* src);
+/* Device times (ms) of the last mixed advance's photon kernels and the photons they handled:
+ * the emission of the new photons and the photon step. */
+MCS_API int mcs_photons_last_timing(mcs_photons* ph, float* emit_ms, int64_t* emitted, float* step_ms,
+                                    int64_t* stepped);
 /* advance!(mpopl, efield, dt, tracker) over electrons and photons (mixed_population.jl:24-54):
  * the electrons (absolute positions), whose photo-emission adds photons in serial parent
  * order, then every photon (the new ones too): straight flight, photo-ionization adding +w

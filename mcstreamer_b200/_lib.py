@@ -134,6 +134,8 @@ SIGNATURES = {
     "mcs_photons_upload": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64]),
     "mcs_photons_download": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_photons_count": (i32, [vp, pi64]),
+    "mcs_photons_copy": (i32, [vp, vp]),
+    "mcs_photons_last_timing": (i32, [vp, C.POINTER(C.c_float), pi64, C.POINTER(C.c_float), pi64]),
     "mcs_advance_mixed": (i32, [vp, vp, vp, vp, f64, vp]),
     "mcs_photon_advance": (i32, [vp, vp, f64, vp]),
 }

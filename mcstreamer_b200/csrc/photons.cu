@@ -275,6 +275,9 @@ struct mcs_photons {
     uint32_t* d_counts = nullptr;           // [0] photo-emission events, [1] photo-ionizations
     unsigned long long* d_total = nullptr;
     unsigned long long* h_total = nullptr;  // pinned
+    cudaEvent_t ev[4] = {};                 // around k_photon_emit and k_photon_step
+    float emit_ms = 0.0f, step_ms = 0.0f;   // of the last mixed advance
+    long long last_emitted = 0, last_entry = 0;
 };
 
 namespace {
@@ -351,12 +354,17 @@ int photon_half(mcs_photons* ph, mcs_pop* e, double dt, mcs_grid* tracker) {
     MCS_CK(c, cudaStreamSynchronize(st));   // k_photon_emit may still read the scan buffers
     if (int er = grow(c, &ph->d_iev, &ph->iev_cap, std::max(1LL, e->cap))) return er;
     MCS_CK(c, cudaMemsetAsync(ph->d_counts + 1, 0, sizeof(uint32_t), st));
+    ph->last_entry = n_entry;
+    ph->step_ms = 0.0f;
     if (n_entry > 0) {
+        cudaEventRecord(ph->ev[2], st);
         k_photon_step<<<blocks_for(c, n_entry, 256), 256, 0, st>>>(
             photon_view(ph), n_entry, ph->numax, dt, ph->seed, ph->step, grid_view(tracker), ph->d_iev,
             ph->d_counts + 1, (uint32_t)std::min<long long>(ph->iev_cap, 0xffffffffLL), ph->d_islot, c->d_status);
+        cudaEventRecord(ph->ev[3], st);
         MCS_CK_LAUNCH(c);
         if (int er = scan_counts(ph, ph->d_islot, n_entry, st)) return er;
+        cudaEventElapsedTime(&ph->step_ms, ph->ev[2], ph->ev[3]);
         const unsigned long long added = *ph->h_total;
         if (added > 0) {
             int er = MCS_OK;
@@ -409,6 +417,8 @@ MCS_API int mcs_photons_create(mcs_ctx* c, int64_t capacity, double numax, uint6
     if (!e && cudaMallocHost(&ph->h_total, sizeof(unsigned long long)) != cudaSuccess)
         e = set_err(c, MCS_ERR_NOMEM, "photons: pinned allocation failed");
     if (!e && cudaMemset(ph->d_act, 0, (size_t)capacity) != cudaSuccess) e = MCS_ERR_CUDA;
+    for (int q = 0; q < 4 && !e; ++q)
+        if (cudaEventCreate(&ph->ev[q]) != cudaSuccess) e = MCS_ERR_CUDA;
     if (e) {
         mcs_photons_destroy(ph);
         return e;
@@ -431,6 +441,8 @@ MCS_API int mcs_photons_destroy(mcs_photons* ph) {
     cudaFree(ph->d_counts);
     cudaFree(ph->d_total);
     if (ph->h_total) cudaFreeHost(ph->h_total);
+    for (cudaEvent_t v : ph->ev)
+        if (v) cudaEventDestroy(v);
     delete ph;
     return MCS_OK;
 }
@@ -480,6 +492,35 @@ MCS_API int mcs_photons_download(mcs_photons* ph, double* x, double* v, double* 
     MCS_CK(c, cudaMemcpy(s, ph->d_f[8], n * sizeof(double), cudaMemcpyDeviceToHost));
     MCS_CK(c, cudaMemcpy(active, ph->d_act, (size_t)n, cudaMemcpyDeviceToHost));
     return st;
+}
+
+// dst <- src on the device (the first src->n photons and the count).
+MCS_API int mcs_photons_copy(mcs_photons* dst, const mcs_photons* src) {
+    if (!dst || !src || dst->ctx != src->ctx) return MCS_ERR_ARG;
+    mcs_ctx* c = dst->ctx;
+    if (src->n > dst->cap) return set_err(c, MCS_ERR_CAPACITY, "photons: destination too small");
+    MCS_CK(c, cudaSetDevice(c->device));
+    const size_t n = (size_t)src->n;
+    for (int q = 0; q < 9; ++q)
+        MCS_CK(c, cudaMemcpyAsync(dst->d_f[q], src->d_f[q], n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    MCS_CK(c, cudaMemcpyAsync(dst->d_act, src->d_act, n, cudaMemcpyDeviceToDevice, c->stream));
+    dst->n = src->n;
+    dst->step = src->step;
+    return MCS_OK;
+}
+
+// Device times (CUDA events on the context's stream) of the last mixed advance's photon
+// kernels, with the photons they handled: k_photon_emit (emitted) and k_photon_step (entry
+// count of the photon half).
+MCS_API int mcs_photons_last_timing(mcs_photons* ph, float* emit_ms, int64_t* emitted, float* step_ms,
+                                    int64_t* stepped) {
+    if (!ph) return MCS_ERR_ARG;
+    if (ph->last_emitted > 0) cudaEventElapsedTime(&ph->emit_ms, ph->ev[0], ph->ev[1]);
+    if (emit_ms) *emit_ms = ph->emit_ms;
+    if (emitted) *emitted = ph->last_emitted;
+    if (step_ms) *step_ms = ph->step_ms;
+    if (stepped) *stepped = ph->last_entry;
+    return MCS_OK;
 }
 
 MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n) {
@@ -533,15 +574,20 @@ MCS_API int mcs_advance_mixed(mcs_pop* e, mcs_photons* ph, const mcs_table* t, c
     e->cur ^= 1;
     e->step += 1;
     // their photons, in serial parent order
+    ph->emit_ms = 0.0f;
+    ph->last_emitted = 0;
     if (ne0 > 0) {
         if (int q = scan_counts(ph, ph->d_pslot, ne0, st)) return q;
         const unsigned long long added = *ph->h_total;
         if (added > 0) {
+            cudaEventRecord(ph->ev[0], st);
             k_photon_emit<<<blocks_for(c, (long long)added, 256), 256, 0, st>>>(
                 photon_view(ph), ph->d_pev, ph->d_counts, (uint32_t)std::min<long long>(ph->cap, 0xffffffffLL),
                 ph->d_base, ph->n, ph->cap, t->v, e->seed, estep, ebase, c->d_status);
+            cudaEventRecord(ph->ev[1], st);
             MCS_CK_LAUNCH(c);
             ph->n = std::min(ph->n + (long long)added, ph->cap);
+            ph->last_emitted = (long long)added;
         }
     }
     // every photon, the new ones included

@@ -19,6 +19,9 @@ poisson_spec(): the electrostatic solve of poisson! on the reference's sample gr
   analytic ion density of the channel body alone, background field -1.5 MV/m; seed 1.
   Each solve starts from a zero potential.
 
+photon_step_spec(): advance! over electrons and photons (photo-emission, photon flight,
+  photo-ionization) in the cylindrical streamer geometry; see PhotonStepSpec.
+
 batched_swarms(): the batched swarm workload ("cfg3"): 256 instances with E/N log-spaced
   10-1000 Td, electron counts log-uniform 4,096-1,048,576 and one of the synthetic gases
   0, 1, 2 each (seeded, seed 3); N = 2.5e25 m^-3, dt = 1e-13 s, 5000 steps per solve,
@@ -217,3 +220,59 @@ def poisson_electron_charge(spec: PoissonSpec, x: np.ndarray, w: np.ndarray) -> 
     q = np.zeros((M + 2) * (N + 2), dtype=np.int64)
     np.add.at(q, i[ok] + j[ok] * (M + 2), np.rint(-w[ok] * 2.0 ** 32).astype(np.int64))
     return q
+
+
+@dataclass
+class PhotonStepSpec:
+    """advance! over electrons and photons in the cylindrical streamer geometry: a
+    0.5 x 2 mm grid of 128 x 512 cells whose face field is a uniform -15 MV/m; 4,194,304
+    electrons of weight 1e3 in a Gaussian cloud (sigma 100 um) at the axis midpoint, 5 eV
+    Maxwellian, FP32; 1,048,576 photons from the same cloud (isotropic, log-uniform nu over the
+    table's band, weight 1); synthetic gas 0 with its photo-emission process (absorber 20% of
+    the gas, photon_multiplier 1000, photon_weight 1, as the reference's sample input);
+    dt = 1e-12 s; seed 1."""
+    R: float = 5e-4
+    L: float = 2e-3
+    M: int = 128
+    N: int = 512
+    n_e: int = 4_194_304
+    n_ph: int = 1_048_576
+    weight: float = 1e3
+    sigma: float = 1e-4
+    mean_ev: float = 5.0
+    ez: float = -1.5e7
+    dt: float = 1e-12
+    photon_multiplier: float = 1000.0
+    photon_weight: float = 1.0
+    seed: int = 1
+
+
+def photon_step_spec() -> PhotonStepSpec:
+    return PhotonStepSpec()
+
+
+def photon_step_electrons(spec: PhotonStepSpec, n: Optional[int] = None) -> ParticleArrays:
+    n = spec.n_e if n is None else n
+    rng = np.random.default_rng(spec.seed)
+    p = ParticleArrays.empty(n)
+    p.x[:] = rng.normal(0.0, spec.sigma, (n, 3))
+    p.x[:, 2] += 0.5 * spec.L
+    sig = np.sqrt((2.0 / 3.0) * spec.mean_ev * co.eV / co.electron_mass)
+    p.v[:] = rng.normal(0.0, sig, (n, 3))
+    p.w[:] = spec.weight
+    p.s[:] = -np.log(rng.random(n))
+    p.active[:] = 1
+    return p
+
+
+def photon_step_photons(spec: PhotonStepSpec, lmin: float, lmax: float, n: Optional[int] = None):
+    """(x, v, nu, w, s, active) of the initial photons."""
+    n = spec.n_ph if n is None else n
+    rng = np.random.default_rng(spec.seed + 1)
+    x = rng.normal(0.0, spec.sigma, (n, 3))
+    x[:, 2] += 0.5 * spec.L
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    nu = np.exp(lmin + (lmax - lmin) * rng.random(n))
+    return (x, d * co.speed_of_light, nu, np.full(n, spec.photon_weight), -np.log(rng.random(n)),
+            np.ones(n, np.uint8))
