@@ -286,11 +286,22 @@ MCS_API int mcs_grid_create_cyl(mcs_ctx* c, double R, double L, int M, int N, mc
     g->nq = cells;
     int st = dalloc(c, &g->d_er, faces);
     if (!st) st = dalloc(c, &g->d_ez, faces);
+    if (!st) st = dalloc(c, &g->d_erz32, 2 * faces);
     if (!st) st = dalloc(c, &g->d_q[0], cells);
     if (!st) st = dalloc(c, &g->d_q[1], cells);
-    if (st) { cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_q[0]); delete g; return st; }
+    if (st) {
+        cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_erz32); cudaFree(g->d_q[0]); delete g;
+        return st;
+    }
     cudaMemset(g->d_er, 0, faces * sizeof(double));
     cudaMemset(g->d_ez, 0, faces * sizeof(double));
+    cudaMemset(g->d_erz32, 0, 2 * faces * sizeof(float));
+    v.er32 = g->d_erz32;
+    v.ez32 = g->d_erz32 + faces;
+    v.R32 = (float)R;
+    v.L32 = (float)L;
+    v.inv_dr32 = (float)(1.0 / v.dr);
+    v.inv_dz32 = (float)(1.0 / v.dz);
     cudaMemset(g->d_q[0], 0, cells * sizeof(long long));
     cudaMemset(g->d_q[1], 0, cells * sizeof(long long));
     v.er = g->d_er;
@@ -305,7 +316,7 @@ MCS_API int mcs_grid_destroy(mcs_grid* g) {
     if (!g) return MCS_OK;
     cudaSetDevice(g->ctx->device);
     cudaStreamSynchronize(g->ctx->stream);
-    cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_er); cudaFree(g->d_ez);
+    cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_erz32);
     cudaFree(g->d_q[0]); cudaFree(g->d_q[1]);
     delete g;
     return MCS_OK;
@@ -334,6 +345,9 @@ MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e) {
         const size_t faces = (size_t)(g->v.M + 3) * (g->v.N + 3);
         MCS_CK(c, cudaMemcpy(g->d_er, e, faces * sizeof(double), cudaMemcpyHostToDevice));
         MCS_CK(c, cudaMemcpy(g->d_ez, e + faces, faces * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<float> tmp(2 * faces);
+        for (size_t i = 0; i < 2 * faces; ++i) tmp[i] = (float)e[i];
+        MCS_CK(c, cudaMemcpy(g->d_erz32, tmp.data(), tmp.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     return MCS_OK;
 }

@@ -84,6 +84,8 @@ struct GridView {
     double R, L, dr, dz;    // cyl
     int M, N;
     const double* er; const double* ez;  // cyl faces (M+3)x(N+3)
+    const float* er32; const float* ez32;  // their FP32 copies (the FP32 push gathers these)
+    float R32, L32, inv_dr32, inv_dz32;
     long long* qfixed;      // tracker deposits (int64, 2^-32 e)
     long long* qpart;       // particle deposits
 };
@@ -155,6 +157,7 @@ struct mcs_grid {
     double* d_e64 = nullptr;
     double* d_er = nullptr;
     double* d_ez = nullptr;
+    float* d_erz32 = nullptr;   // cyl: FP32 er faces then ez faces
     long long* d_q[2] = {nullptr, nullptr};
     size_t nq = 0;          // entries per charge array
 };

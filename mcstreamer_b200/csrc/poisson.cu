@@ -891,6 +891,14 @@ __global__ void k_faces_edges(double* er, double* ez, int M, int N) {
     }
 }
 
+// FP32 copies of the face fields (the FP32 push gathers them).
+__global__ void k_faces32(const double* er, const double* ez, float* er32, float* ez32, long n) {
+    for (long t = gtid(); t < n; t += gthreads()) {
+        er32[t] = (float)er[t];
+        ez32[t] = (float)ez[t];
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------------------
@@ -1647,6 +1655,9 @@ MCS_API int mcs_poisson_fields(mcs_poisson* p, double eb) {
                                                                                 p->dr, p->dz, p->M, p->N);
     ++p->launches;
     k_faces_edges<<<grid_blocks(p, std::max(p->M, p->N) + 3), kThreads, 0, st>>>(p->g->d_er, p->g->d_ez, p->M, p->N);
+    const long nf = (long)(p->M + 3) * (p->N + 3);
+    ++p->launches;
+    k_faces32<<<grid_blocks(p, nf), kThreads, 0, st>>>(p->g->d_er, p->g->d_ez, p->g->d_erz32, p->g->d_erz32 + nf, nf);
     PSN_LAUNCH(p);
     return MCS_OK;
 }

@@ -382,6 +382,10 @@ struct FieldCyl {
     template <typename T>
     __device__ __forceinline__ void operator()(const GridView& g, T x0, T x1, T x2, T& e0, T& e1, T& e2,
                                                uint32_t* status) const {
+        if constexpr (sizeof(T) == 4) {
+            gather32(g, x0, x1, x2, e0, e1, e2, status);
+            return;
+        }
         const double x = x0, y = x1, z = x2;
         e0 = e1 = e2 = (T)0;
         const double r0 = sqrt(x * x + y * y);
@@ -409,6 +413,38 @@ struct FieldCyl {
         const double a = er1 * x / r, b = er1 * y / r;
         if (sqrt(a * a + b * b + ez1 * ez1) > 1e8) atomicOr(status, ST_FIELD);
         e0 = (T)a; e1 = (T)b; e2 = (T)ez1;
+    }
+
+    // The FP32 push's gather: the same cells and weights in single precision from the FP32
+    // face copies, reciprocal cell sizes, and |E|^2 > 1e16 for the field check.  Indices stay
+    // inside the (M+3) x (N+3) faces: a rounded-up r / dr or z / dz of M or N reads face M+2 or
+    // N+2 at most.
+    __device__ __forceinline__ void gather32(const GridView& g, float x, float y, float z, float& e0, float& e1,
+                                             float& e2, uint32_t* status) const {
+        e0 = e1 = e2 = 0.0f;
+        const float r = sqrtf(fmaf(x, x, y * y));
+        if (!((0.0f < r && r < g.R32) && (0.0f < z && z < g.L32))) return;
+        const float qr = r * g.inv_dr32, qz = z * g.inv_dz32;
+        int i = min((int)qr, g.M), j = min((int)qz, g.N);
+        const float dr_ = qr - (float)i, dz_ = qz - (float)j;
+        int i1, j1;
+        float dr1, dz1;
+        if (dr_ < 0.5f) { i1 = i; dr1 = dr_ + 0.5f; } else { i1 = i + 1; dr1 = dr_ - 0.5f; }
+        if (dz_ < 0.5f) { j1 = j; dz1 = dz_ + 0.5f; } else { j1 = j + 1; dz1 = dz_ - 0.5f; }
+        i += 1; j += 1;
+        const int ld = g.M + 3;
+        const float* er = g.er32;
+        const float* ez = g.ez32;
+        const float a0 = __ldg(er + i + j1 * ld), a1 = __ldg(er + i + 1 + j1 * ld);
+        const float a2 = __ldg(er + i + (j1 + 1) * ld), a3 = __ldg(er + i + 1 + (j1 + 1) * ld);
+        const float b0 = __ldg(ez + i1 + j * ld), b1 = __ldg(ez + i1 + 1 + j * ld);
+        const float b2 = __ldg(ez + i1 + (j + 1) * ld), b3 = __ldg(ez + i1 + 1 + (j + 1) * ld);
+        const float er1 = fmaf(dz1, fmaf(dr_, a3 - a2, a2) - fmaf(dr_, a1 - a0, a0), fmaf(dr_, a1 - a0, a0));
+        const float ez1 = fmaf(dz_, fmaf(dr1, b3 - b2, b2) - fmaf(dr1, b1 - b0, b0), fmaf(dr1, b1 - b0, b0));
+        const float f = er1 / r;
+        const float a = f * x, b = f * y;
+        if (fmaf(a, a, fmaf(b, b, ez1 * ez1)) > 1e16f) atomicOr(status, ST_FIELD);
+        e0 = a; e1 = b; e2 = ez1;
     }
 };
 

@@ -96,3 +96,47 @@ def test_cyl_field_too_high_is_reported(ctx):
         ctx.sync()
     assert "FIELD_TOO_HIGH" in str(ei.value)
     fld.close(); pop.close(); grid.close(); tab.close()
+
+
+@pytest.mark.gpu
+def test_cyl_step_fp32_within_tolerance(ctx):
+    """The FP32 push gathers from FP32 copies of the faces: one step against the FP64 oracle
+    within single-precision tolerance, discrete flips (process choice, sub-step count) counted."""
+    n = 65_536
+    t = lxcat.synthetic_table(0)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.GridCyl(R, LEN, M, N, ctx=ctx)
+    er, ez = _faces()
+    grid.set_efield(er, ez)
+    p0 = _particles(n, 17)
+    pop = jumc.Population(3 * n, p0, tab, precision="fp32", seed=17)
+    fld = streamer.FieldInterp(grid)
+    ofield = po.field_cyl(R, LEN, M, N, er.T.ravel(), ez.T.ravel())
+    opop = oracle_pop(p0, 3 * n, 17)
+    try:
+        jumc.advance(pop, fld, 2e-13)
+        assert po.advance(opop, po.OracleTable.from_lxcat(t), ofield, 2e-13) == 0
+        g, o = pop.download(), oracle_arrays(opop)
+        bad = particle_mismatch(g, o, 1e-5, xatol=1e-12, vatol=1e-2, satol=1e-5, n=n)
+        assert bad.sum() / n < 2e-3, f"flip fraction {bad.sum() / n:.2e}"
+        assert abs(g.n - o.n) <= max(8, 0.01 * (o.n - n))
+    finally:
+        fld.close(); pop.close(); grid.close(); tab.close()
+
+
+@pytest.mark.gpu
+def test_cyl_field_too_high_is_reported_fp32(ctx):
+    t = lxcat.synthetic_table(0)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.GridCyl(R, LEN, M, N, ctx=ctx)
+    er, ez = _faces()
+    grid.set_efield(er, ez * 100.0)
+    pop = jumc.Population(1024, _particles(256, 2), tab, precision="fp32")
+    fld = streamer.FieldInterp(grid)
+    try:
+        with pytest.raises(Exception) as ei:
+            jumc.advance(pop, fld, 1e-14)
+            ctx.sync()
+        assert "FIELD_TOO_HIGH" in str(ei.value)
+    finally:
+        fld.close(); pop.close(); grid.close(); tab.close()
