@@ -1311,6 +1311,190 @@ def run_reference_batch(args):
     return 0
 
 
+FLUID_METRIC = "fluid cell updates/s"
+
+
+def fluid_alg_bytes(M: int, N: int) -> float:
+    """Algorithmic HBM bytes of one fused setdne! + euler! over the (M+4) x (N+4) padded
+    cells: ne, er and ez read once (8 + 8 + 8 B per cell), dne and the updated ne written
+    once (8 + 8 B per cell)."""
+    return 40.0 * (M + 4) * (N + 4)
+
+
+def fluid_config(spec, extra=None):
+    p = spec.poisson
+    c = {"workload": f"setdne! + euler! of the electron fluid on the sample grid: R={p.R:g} m, L={p.L:g} m, "
+                     f"{p.M}x{p.N} cells; fluid where a channel of peak density {spec.peak:g} m^-3 (Gaussian in "
+                     f"r, sigma {p.sigma_r:g} m, z in [{p.z0:g}, {p.z1:g}] m) exceeds {spec.threshold:g} m^-3 "
+                     f"(fluid_threshold); faces from one poisson! of the channel charge (eb={p.eb:g} V/m), "
+                     f"mobility 1e24/nair, dt={spec.dt:g} s",
+         "cells": p.M * p.N, "l2": "ne, dne and the face fields (500 MB) exceed L2", "parallelism": "1 GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def fluid_oracle_step(spec, ne, er, ez):
+    """One setdne! + euler! of the oracle on all host threads; returns seconds."""
+    from oracle import fluid_ref as F
+    p = spec.poisson
+    dne = F.centers(p.M, p.N)
+    t0 = time.perf_counter()
+    F.setdne(ne, dne, er, ez, p.R, p.L, p.M, p.N)
+    F.euler(ne, dne, spec.dt, p.M, p.N)
+    return time.perf_counter() - t0
+
+
+def fluid_faces(spec):
+    """The face fields of one poisson! of the channel charge, computed by the oracle (for the
+    CPU arms, which have no device)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle import poisson_ref as P
+    p = spec.poisson
+    _, qf, qp = poisson_inputs(p)
+    u = P.cells(p.M, p.N)
+    er, ez = P.faces(p.M, p.N), P.faces(p.M, p.N)
+    P.poisson(P.default_conf(p.R, p.L, p.M, p.N, levels=p.levels), qf, qp, u, er, ez, p.eb, p.R, p.L)
+    return er, ez
+
+
+def run_fluid(args):
+    import ctypes as C
+
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import jumc, lxcat, streamer, workloads
+    from mcstreamer_b200.fluid import MOBILITY, Fluid
+    from mcstreamer_b200.poisson import MGConfig, PoissonSolver, read_faces
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        # replicas only: the fluid step is not sharded
+        import torch.distributed as dist
+        dist.init_process_group("nccl")
+    torch.cuda.set_device(local)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spec = workloads.fluid_spec()
+    p = spec.poisson
+    parts, qf, _ = poisson_inputs(p)
+    tab = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
+    grid = streamer.GridCyl(p.R, p.L, p.M, p.N, ctx=ctx)
+    pop = jumc.Population(p.n, parts, tab, precision="fp64")
+    solver = PoissonSolver(grid, MGConfig(levels=p.levels))
+    grid.write_fixed(L.Q_FIXED, qf)
+    grid.zero(L.Q_PART)
+    streamer.density(grid, pop, -1.0)
+    solver.run(p.eb)
+    pop.close(); tab.close()
+    ne0 = workloads.fluid_density(spec)
+    fl = Fluid(grid)
+    fl.upload(ne=ne0)
+    lib = ctx.lib
+    for _ in range(args.warmup):
+        ctx.check(lib.mcs_fluid_step(fl.h, MOBILITY, spec.dt))
+    n0 = fl.launches()
+    times = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.mcs_fluid_step(fl.h, MOBILITY, spec.dt))
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
+    times = [a.elapsed_time(b) for a, b in times]
+    launches = (fl.launches() - n0) // args.steps
+    total_ms = float(sum(times))
+    if ws > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = ws * p.M * p.N / (ms * 1e-3)
+    pk, src = peaks()
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    ach = fluid_alg_bytes(p.M, p.N) / (ms * 1e-3) / 1e9
+
+    # end to end: ne from pinned host, the step, ne and dne back to pinned host
+    npad = (p.M + 4) * (p.N + 4)
+    h_ne = torch.from_numpy(np.ascontiguousarray(ne0.ravel(order="F"))).pin_memory()
+    h_out = torch.empty(2 * npad, dtype=torch.float64).pin_memory()
+    pd = C.POINTER(C.c_double)
+    e2e_t = []
+    for k in range(max(1, args.e2e_steps) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.check(lib.mcs_fluid_upload(fl.h, C.cast(h_ne.data_ptr(), pd), None))
+        ctx.check(lib.mcs_fluid_step(fl.h, MOBILITY, spec.dt))
+        ctx.check(lib.mcs_fluid_download(fl.h, C.cast(h_out.data_ptr(), pd),
+                                         C.cast(h_out.data_ptr() + 8 * npad, pd), None))
+        if k:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_v = p.M * p.N / statistics.median(e2e_t)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        er, ez = read_faces(grid)
+        ne = ne0.copy(order="F")
+        sec = fluid_oracle_step(spec, ne, np.asfortranarray(er), np.asfortranarray(ez))
+        cpu = {"value": p.M * p.N / sec, "unit": "cell-updates/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": f"one setdne! + euler! of this workload by the oracle (OpenMP over the inner "
+                         f"index, as the reference's @batch): {sec:.2f} s"}
+    line = {
+        "metric": FLUID_METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": fluid_config(spec, {"fluid_cells": int((ne0 > 0).sum())}),
+        "roofline": {"kernel": "k_fluid<true> (setnebc! + setdne! + euler!, one launch)", "bound": "hbm",
+                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "peak_source": src, "launch_ms": ms, "alg_bytes_per_launch": fluid_alg_bytes(p.M, p.N)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": 8 * npad,
+                "d2h_bytes_per_step": 16 * npad,
+                "path": "mcs_fluid_upload (ne from pinned host) -> mcs_fluid_step -> mcs_fluid_download "
+                        "(ne, dne to pinned host)"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    fl.close(); solver.close(); grid.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_fluid(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.fluid_spec()
+    p = spec.poisson
+    er, ez = fluid_faces(spec)
+    ne = workloads.fluid_density(spec)
+    runs = [fluid_oracle_step(spec, ne, er, ez) for _ in range(max(1, min(args.steps, 3)))]
+    sec = statistics.median(runs)
+    v = p.M * p.N / sec
+    line = {
+        "impl": "reference", "metric": FLUID_METRIC, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "steps": len(runs), "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": fluid_config(spec),
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": os.cpu_count() or 1, "kind": "port",
+                         "sample": f"{len(runs)} setdne! + euler! steps of the oracle (OpenMP over the inner "
+                                   f"index, as the reference's @batch)"},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -1323,6 +1507,8 @@ def main():
         return run_reference_poisson(args) if args.impl == "reference" else run_poisson(args)
     if args.workload == "photons":
         return run_reference_photons(args) if args.impl == "reference" else run_photons(args)
+    if args.workload == "fluid":
+        return run_reference_fluid(args) if args.impl == "reference" else run_fluid(args)
     if args.workload == "cfg4":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU reference arm; "

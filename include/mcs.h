@@ -92,6 +92,7 @@ typedef struct mcs_field mcs_field;
 typedef struct mcs_pop mcs_pop;
 typedef struct mcs_batch mcs_batch;
 typedef struct mcs_poisson mcs_poisson;
+typedef struct mcs_fluid mcs_fluid;
 typedef struct mcs_photons mcs_photons;
 
 /* ---- context ---- */
@@ -358,6 +359,10 @@ MCS_API int mcs_photons_download(mcs_photons* ph, double* x, double* v, double* 
 MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n);
 /* dst <- src on the device (a snapshot of a photon population). */
 MCS_API int mcs_photons_copy(mcs_photons* dst, const mcs_photons* src);
+/* out[0] = actives(photons), out[1] = weight(photons) (JuMC/src/population.jl:114-131, as
+ * MCStreamer's per-step diagnostics read them, main.jl:272-273): FP64 sums over the active
+ * photons in a fixed order. */
+MCS_API int mcs_photons_moments(mcs_photons* ph, double* out);
 /* Device times (ms) of the last mixed advance's photon kernels and the photons they handled:
  * the emission of the new photons and the photon step. */
 MCS_API int mcs_photons_last_timing(mcs_photons* ph, float* emit_ms, int64_t* emitted, float* step_ms,
@@ -404,8 +409,9 @@ MCS_API int mcs_poisson_mg_solve(mcs_poisson* p, int* iters, double* eps_last);
 /* solve_freebc!(u, b, grid, mg, ws) (MCStreamer/src/freebc.jl:4-36); iters[2] = fmg! calls
  * of the two solves.  b gets the inhomogeneous term, as in the reference. */
 MCS_API int mcs_poisson_solve_freebc(mcs_poisson* p, int* iters);
-/* b = Float32((qfixed + qpart) / dV * e) from the grid's int64 cell charges
- * (poisson.jl:12-34 with the NullDenoiser). */
+/* b = Float32((qfixed + qpart - ne) / dV * e) from the grid's int64 cell charges
+ * (poisson.jl:12-34 with the NullDenoiser); with a fluid on the grid, qfixed adds its FP64
+ * density part and ne is the fluid density, else both are zero. */
 MCS_API int mcs_poisson_assemble(mcs_poisson* p);
 /* The grid's face fields from u (poisson.jl:47-57): er = -du/dr, ez = eb - du/dz. */
 MCS_API int mcs_poisson_fields(mcs_poisson* p, double eb);
@@ -414,6 +420,35 @@ MCS_API int mcs_poisson_fields(mcs_poisson* p, double eb);
 MCS_API int mcs_poisson_run(mcs_poisson* p, double eb, int* iters);
 /* f_n = L k (I1/I0 + K1/K0)(k R) / 2, k = pi n / L, n = 1..N (freebc.jl:17-20).  Host only. */
 MCS_API int mcs_freebc_coefficients(double L, double R, int N, double* f);
+
+/* ---- Electron fluid: MCStreamer/src/fluid.jl on a cylindrical grid ----
+ * The fluid density ne and its derivative dne are (M+4)x(N+4) doubles with two ghost layers
+ * (calloc_centers(T, grid, 2)): the reference's (i, j), i in -1..M+2, j in -1..N+2, at
+ * (i+1) + (j+1)(M+4).  qfd is the FP64 density part of the grid's qfixed, (M+2)x(N+2) at
+ * i + j(M+2).  The fluxes use the grid's face fields er, ez (the last mcs_poisson_fields or
+ * mcs_grid_set_efield).  One fluid per grid; mcs_poisson_assemble subtracts its ne. */
+#define MCS_FLUID_MOBILITY (1e24 / 2.6867811e+25) /* setdne!'s default mobility: 1e24 / co.nair */
+MCS_API int mcs_fluid_create(mcs_grid* g, mcs_fluid** out);
+MCS_API int mcs_fluid_destroy(mcs_fluid* f);
+/* Copy ne (ghosts included) and/or qfd in from the host; either may be NULL. */
+MCS_API int mcs_fluid_upload(mcs_fluid* f, const double* ne, const double* qfd);
+/* Copy ne, dne and/or qfd out to the host; any may be NULL. */
+MCS_API int mcs_fluid_download(mcs_fluid* f, double* ne, double* dne, double* qfd);
+/* setneedle!(fields, sigma_z, sigma_r, position_z, position_r, ne0) (fluid.jl:3-13):
+ * ne += ne0 exp(-rc^2/sigma_r^2 - max(0, zc - position_z)^2/sigma_z^2) on the interior and
+ * qfixed += ne.  position_r is unused, as in the reference. */
+MCS_API int mcs_fluid_set_needle(mcs_fluid* f, double sigma_z, double sigma_r, double position_z, double position_r,
+                                 double ne0);
+/* setdne!(fields, mobility) (fluid.jl:44-98), setnebc! included: Neumann ghosts of ne, then
+ * dne from the Koren-limited upwind fluxes through every z and r face. */
+MCS_API int mcs_fluid_derivatives(mcs_fluid* f, double mobility);
+/* euler!(fields, dt) (fluid.jl:100-111): ne += dt dne on the interior. */
+MCS_API int mcs_fluid_euler(mcs_fluid* f, double dt);
+/* setdne!(fields, mobility) then euler!(fields, dt) (main.jl:308-311) in one kernel; ne, dne
+ * and the ghosts end as the two calls leave them. */
+MCS_API int mcs_fluid_step(mcs_fluid* f, double mobility, double dt);
+/* Kernels this fluid has launched so far. */
+MCS_API int mcs_fluid_launches(mcs_fluid* f, int64_t* count);
 
 #ifdef __cplusplus
 }

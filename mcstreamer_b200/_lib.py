@@ -128,9 +128,19 @@ SIGNATURES = {
     "mcs_poisson_launches": (i32, [vp, pi64]),
     "mcs_poisson_profile": (i32, [vp, i32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "mcs_grid_write_fixed": (i32, [vp, i32, pi64]),
+    "mcs_fluid_create": (i32, [vp, C.POINTER(C.c_void_p)]),
+    "mcs_fluid_destroy": (i32, [vp]),
+    "mcs_fluid_upload": (i32, [vp, pd, pd]),
+    "mcs_fluid_download": (i32, [vp, pd, pd, pd]),
+    "mcs_fluid_set_needle": (i32, [vp, f64, f64, f64, f64, f64]),
+    "mcs_fluid_derivatives": (i32, [vp, f64]),
+    "mcs_fluid_euler": (i32, [vp, f64]),
+    "mcs_fluid_step": (i32, [vp, f64, f64]),
+    "mcs_fluid_launches": (i32, [vp, pi64]),
     "mcs_table_set_photoemission": (i32, [vp, pd, pd, f64, f64]),
     "mcs_photons_create": (i32, [vp, i64, f64, C.c_uint64, C.POINTER(C.c_void_p)]),
     "mcs_photons_destroy": (i32, [vp]),
+    "mcs_photons_moments": (i32, [vp, pd]),
     "mcs_photons_upload": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64]),
     "mcs_photons_download": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_photons_count": (i32, [vp, pi64]),

@@ -316,6 +316,7 @@ MCS_API int mcs_grid_destroy(mcs_grid* g) {
     if (!g) return MCS_OK;
     cudaSetDevice(g->ctx->device);
     cudaStreamSynchronize(g->ctx->stream);
+    if (g->fluid) g->fluid->g = nullptr;
     cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_erz32);
     cudaFree(g->d_q[0]); cudaFree(g->d_q[1]);
     delete g;

@@ -160,6 +160,22 @@ struct mcs_grid {
     float* d_erz32 = nullptr;   // cyl: FP32 er faces then ez faces
     long long* d_q[2] = {nullptr, nullptr};
     size_t nq = 0;          // entries per charge array
+    struct mcs_fluid* fluid = nullptr;   // cyl: the electron fluid on this grid, if any
+};
+
+// The electron fluid of MCStreamer (fluid.jl) on a cylindrical grid: density ne and its
+// derivative dne with two ghost layers ((M+4)x(N+4), (i, j) at (i+1) + (j+1)(M+4)), double
+// buffered for the fused setdne! + euler!, and qfd, the FP64 density part of qfixed
+// ((M+2)x(N+2)) that setneedle! adds to.
+struct mcs_fluid {
+    mcs_ctx* ctx = nullptr;
+    mcs_grid* g = nullptr;
+    int M = 0, N = 0;
+    double* ne[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* dne = nullptr;
+    double* qfd = nullptr;
+    long long launches = 0;
 };
 
 struct mcs_field {

@@ -247,6 +247,49 @@ __global__ void k_ion_scatter(PopView<T> E, const IonEvent* ev, const uint32_t* 
 
 __global__ void k_set_count(long long* n, long long v) { *n = v; }
 
+constexpr int kDiagBlocks = 592, kDiagThreads = 256;
+
+// actives(photons) and weight(photons) (JuMC/src/population.jl:114-131): per-block partials
+// over a fixed grid, then one block sums them in a fixed order, so the totals do not depend
+// on timing.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { sh[2 * warp] = a; sh[2 * warp + 1] = b; }
+    __syncthreads();
+    if (warp == 0) {
+        a = lane < (int)(blockDim.x >> 5) ? sh[2 * lane] : 0.0;
+        b = lane < (int)(blockDim.x >> 5) ? sh[2 * lane + 1] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kDiagThreads) k_photon_sums(const double* __restrict__ w,
+                                                              const uint8_t* __restrict__ act, long long n,
+                                                              double* __restrict__ part) {
+    __shared__ double sh[2 * (kDiagThreads / 32)];
+    double cnt = 0.0, wt = 0.0;
+    for (long long i = blockIdx.x * (long long)kDiagThreads + threadIdx.x; i < n;
+         i += (long long)gridDim.x * kDiagThreads)
+        if (act[i]) { cnt += 1.0; wt += w[i]; }
+    block_sum2(cnt, wt, sh);
+    if (threadIdx.x == 0) { part[2 * blockIdx.x] = cnt; part[2 * blockIdx.x + 1] = wt; }
+}
+
+__global__ void __launch_bounds__(kDiagThreads) k_photon_sums_final(double* part, int nb) {
+    __shared__ double sh[2 * (kDiagThreads / 32)];
+    double cnt = 0.0, wt = 0.0;
+    for (int b = threadIdx.x; b < nb; b += kDiagThreads) { cnt += part[2 * b]; wt += part[2 * b + 1]; }
+    block_sum2(cnt, wt, sh);
+    if (threadIdx.x == 0) { part[2 * nb] = cnt; part[2 * nb + 1] = wt; }
+}
+
 }  // namespace
 }  // namespace mcs
 
@@ -275,6 +318,7 @@ struct mcs_photons {
     uint32_t* d_counts = nullptr;           // [0] photo-emission events, [1] photo-ionizations
     unsigned long long* d_total = nullptr;
     unsigned long long* h_total = nullptr;  // pinned
+    double* d_diag = nullptr;               // per-block (count, weight) partials, then the totals
     cudaEvent_t ev[4] = {};                 // around k_photon_emit and k_photon_step
     float emit_ms = 0.0f, step_ms = 0.0f;   // of the last mixed advance
     long long last_emitted = 0, last_entry = 0;
@@ -414,6 +458,7 @@ MCS_API int mcs_photons_create(mcs_ctx* c, int64_t capacity, double numax, uint6
     if (!e) e = dalloc_n(c, &ph->d_islot, (size_t)capacity);
     if (!e) e = dalloc_n(c, &ph->d_counts, 2);
     if (!e) e = dalloc_n(c, &ph->d_total, 1);
+    if (!e) e = dalloc_n(c, &ph->d_diag, (size_t)(2 * kDiagBlocks + 2));
     if (!e && cudaMallocHost(&ph->h_total, sizeof(unsigned long long)) != cudaSuccess)
         e = set_err(c, MCS_ERR_NOMEM, "photons: pinned allocation failed");
     if (!e && cudaMemset(ph->d_act, 0, (size_t)capacity) != cudaSuccess) e = MCS_ERR_CUDA;
@@ -440,6 +485,7 @@ MCS_API int mcs_photons_destroy(mcs_photons* ph) {
     cudaFree(ph->d_sums);
     cudaFree(ph->d_counts);
     cudaFree(ph->d_total);
+    cudaFree(ph->d_diag);
     if (ph->h_total) cudaFreeHost(ph->h_total);
     for (cudaEvent_t v : ph->ev)
         if (v) cudaEventDestroy(v);
@@ -526,6 +572,21 @@ MCS_API int mcs_photons_last_timing(mcs_photons* ph, float* emit_ms, int64_t* em
 MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n) {
     if (!ph || !n) return MCS_ERR_ARG;
     *n = ph->n;
+    return MCS_OK;
+}
+
+MCS_API int mcs_photons_moments(mcs_photons* ph, double* out) {
+    if (!ph || !out) return MCS_ERR_ARG;
+    mcs_ctx* c = ph->ctx;
+    out[0] = out[1] = 0.0;
+    if (ph->n == 0) return MCS_OK;
+    MCS_CK(c, cudaSetDevice(c->device));
+    const int nb = (int)std::min<long long>(kDiagBlocks, (ph->n + kDiagThreads - 1) / kDiagThreads);
+    k_photon_sums<<<nb, kDiagThreads, 0, c->stream>>>(ph->d_f[7], ph->d_act, ph->n, ph->d_diag);
+    k_photon_sums_final<<<1, kDiagThreads, 0, c->stream>>>(ph->d_diag, nb);
+    MCS_CK(c, cudaGetLastError());
+    MCS_CK(c, cudaMemcpyAsync(out, ph->d_diag + 2 * nb, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
     return MCS_OK;
 }
 

@@ -837,9 +837,11 @@ __global__ void k_top_ghost(double* u, int M, int N, const double* bcond) {
 }
 
 // q of poisson! (poisson.jl:17-34) from the int64 cell charges: densities q * 2^-32 / dV,
-// q0 = (qfixed + qpart - ne) e with ne = 0, through the NullDenoiser's Float32 copy.
-// Ghost cells are zero.
-__global__ void k_assemble(double* b, const long long* qf, const long long* qp, int M, int N, double dr, double dz) {
+// q0 = (qfixed + qpart - ne) e through the NullDenoiser's Float32 copy.  qfixed is the int64
+// deposit plus qfd, its FP64 density part (the fluid's needle), and ne the fluid density
+// ((M+4)x(N+4)); both are zero without a fluid (null pointers).  Ghost cells are zero.
+__global__ void k_assemble(double* b, const long long* qf, const long long* qp, const double* qfd,
+                           const double* ne, int M, int N, double dr, double dz) {
     const long ld = M + 2;
     const long n = (long)(M + 2) * (N + 2);
     for (long t = gtid(); t < n; t += gthreads()) {
@@ -852,8 +854,9 @@ __global__ void k_assemble(double* b, const long long* qf, const long long* qp, 
             const double df = (double)qf[t] * 0x1p-32 / dv;
             const double dp = (double)qp[t] * 0x1p-32 / dv;
             double q0 = df;
+            if (qfd) q0 = q0 + qfd[t];
             q0 = q0 + dp;
-            q0 = q0 - 0.0;
+            q0 = q0 - (ne ? ne[(long)(i + 1) + (long)(j + 1) * (M + 4)] : 0.0);
             q0 = q0 * kElementaryCharge;
             v = (double)__double2float_rn(q0);
         }
@@ -1640,8 +1643,10 @@ MCS_API int mcs_poisson_assemble(mcs_poisson* p) {
     if (int e = use_dev(p)) return e;
     const long n = (long)cells_of(p->M, p->N);
     ++p->launches;
-    k_assemble<<<grid_blocks(p, n), kThreads, 0, p->ctx->stream>>>(p->b, p->g->d_q[MCS_Q_FIXED],
-                                                                   p->g->d_q[MCS_Q_PART], p->M, p->N, p->dr, p->dz);
+    const mcs_fluid* fl = p->g->fluid;
+    k_assemble<<<grid_blocks(p, n), kThreads, 0, p->ctx->stream>>>(
+        p->b, p->g->d_q[MCS_Q_FIXED], p->g->d_q[MCS_Q_PART], fl ? fl->qfd : nullptr, fl ? fl->ne[fl->cur] : nullptr,
+        p->M, p->N, p->dr, p->dz);
     PSN_LAUNCH(p);
     return MCS_OK;
 }

@@ -277,6 +277,18 @@ class Photons:
         self.ctx.check(self.ctx.lib.mcs_photons_count(self.h, C.byref(n)))
         return n.value
 
+    def moments(self) -> np.ndarray:
+        """[actives, weight] over the active photons (population.jl:114-131)."""
+        out = np.zeros(2)
+        self.ctx.check(self.ctx.lib.mcs_photons_moments(self.h, L.dptr(out)))
+        return out
+
+    def actives(self) -> int:
+        return int(self.moments()[0])
+
+    def weight(self) -> float:
+        return float(self.moments()[1])
+
     def download(self) -> PhotonArrays:
         n = self.count()
         out = PhotonArrays.empty(n)

@@ -212,6 +212,19 @@ def advance_deposit_host(work: Population, efield: FieldInterp, dt: float, track
     return nn.value
 
 
+def diagnostics(popl: Population, photons=None) -> dict:
+    """The per-step diagnostics of nsteps (MCStreamer/src/main.jl:269-279): meanenergy and
+    maxenergy of the electrons (J), their actives and weight, and the photons' actives and
+    weight (zero without active photons).  Device reductions: FP64 sums in a fixed order."""
+    m = popl.moments()
+    ph = photons.moments() if photons is not None else np.zeros(2)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        mean = np.float64(m[L.M_WE]) / np.float64(m[L.M_W])
+    return {"mean_energy": float(mean), "max_energy": float(m[L.M_EMAX]),
+            "active_superelectrons": int(m[L.M_COUNT]), "physical_electrons": float(m[L.M_W]),
+            "active_superphotons": int(ph[0]), "physical_photons": float(ph[1]) if ph[0] > 0 else 0.0}
+
+
 # ---------------------------------------------------------------------------------------
 # Field of the streamer workloads: a uniform background plus a Gaussian charge cloud.
 # ---------------------------------------------------------------------------------------

@@ -276,3 +276,33 @@ def photon_step_photons(spec: PhotonStepSpec, lmin: float, lmax: float, n: Optio
     nu = np.exp(lmin + (lmax - lmin) * rng.random(n))
     return (x, d * co.speed_of_light, nu, np.full(n, spec.photon_weight), -np.log(rng.random(n)),
             np.ones(n, np.uint8))
+
+
+# ---------------------------------------------------------------------------------------
+# The electron fluid: the sample grid with fluid_threshold = 1e20 (samples/input.toml), the
+# cells of a channel denser than the threshold carried by the fluid (initdens.jl:78-82).
+# ---------------------------------------------------------------------------------------
+@dataclass
+class FluidSpec:
+    poisson: PoissonSpec = field(default_factory=PoissonSpec)
+    peak: float = 1e21          # channel density on the axis (m^-3)
+    threshold: float = 1e20     # fluid_threshold (m^-3)
+    dt: float = 1e-12
+
+
+def fluid_spec() -> FluidSpec:
+    return FluidSpec()
+
+
+def fluid_density(spec: FluidSpec) -> np.ndarray:
+    """ne (M+4, N+4), Fortran order, two ghost layers: the channel body of the Poisson
+    workload (Gaussian in r of width sigma_r, z0 <= z <= z1) at a peak density `peak`, where
+    it exceeds the threshold, zero elsewhere."""
+    p = spec.poisson
+    M, N = p.M, p.N
+    rc = (np.arange(M) + 0.5) * (p.R / M)
+    zc = (np.arange(N) + 0.5) * (p.L / N)
+    dens = spec.peak * np.exp(-rc[:, None] ** 2 / (2 * p.sigma_r ** 2)) * ((zc >= p.z0) & (zc <= p.z1))[None, :]
+    ne = np.zeros((M + 4, N + 4), order="F")
+    ne[2:M + 2, 2:N + 2] = np.where(dens > spec.threshold, dens, 0.0)
+    return ne

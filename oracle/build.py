@@ -10,7 +10,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SRCS = [HERE / "oracle.cpp", HERE / "poisson.cpp"]
+SRCS = [HERE / "oracle.cpp", HERE / "poisson.cpp", HERE / "fluid.cpp"]
 
 
 def build(verbose: bool = False) -> Path:

@@ -117,15 +117,19 @@ def cell_volumes(R, L, M, N):
     return 2.0 * np.pi * rc * dr * dz
 
 
-def assemble_charge(qfixed, qpart, R, L, M, N):
+def assemble_charge(qfixed, qpart, R, L, M, N, qfd=None, ne=None):
     """q of poisson! from int64 cell charges (2^-32 elementary charges, index i + j*(M+2)):
-    q0 = (qfixed + qpart - ne) e as densities, then the NullDenoiser's Float32 copy."""
+    q0 = (qfixed + qpart - ne) e as densities, then the NullDenoiser's Float32 copy.  qfixed
+    is the int64 deposit plus qfd, its FP64 density part ((M+2)x(N+2), the needle's); ne is
+    the fluid density ((M+4)x(N+4) with two ghost layers), zero without a fluid."""
     dv = cell_volumes(R, L, M, N)[:, None]
     qf = np.asarray(qfixed, dtype=np.int64).reshape((M + 2, N + 2), order="F")[1:M + 1, 1:N + 1]
     qp = np.asarray(qpart, dtype=np.int64).reshape((M + 2, N + 2), order="F")[1:M + 1, 1:N + 1]
     df = qf.astype(np.float64) * 2.0 ** -32 / dv
     dp = qp.astype(np.float64) * 2.0 ** -32 / dv
-    q0 = ((df + dp) - 0.0) * ELEMENTARY_CHARGE
+    fd = 0.0 if qfd is None else np.asarray(qfd).reshape((M + 2, N + 2), order="F")[1:M + 1, 1:N + 1]
+    nd = 0.0 if ne is None else np.asarray(ne).reshape((M + 4, N + 4), order="F")[2:M + 2, 2:N + 2]
+    q0 = (((df + fd) + dp) - nd) * ELEMENTARY_CHARGE
     b = cells(M, N)
     b[1:M + 1, 1:N + 1] = q0.astype(np.float32).astype(np.float64)
     return b

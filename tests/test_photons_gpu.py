@@ -139,3 +139,33 @@ def test_photon_capacity_is_an_error(ctx):
         assert ph.count() == 50
     finally:
         fld.close(); ph.close(); pop.close(); tab.close()
+
+
+@pytest.mark.gpu
+def test_step_diagnostics(ctx):
+    """The per-step line of nsteps (main.jl:269-279) from the device reductions against serial
+    sums over the downloaded populations (population.jl:114-158)."""
+    n = 20_000
+    t = lxcat.synthetic_photo_table(0, photon_multiplier=1000.0, photon_weight=1.0)
+    tab = jumc.CollisionTable(t, ctx)
+    pop = jumc.Population(20 * n, _electrons(n, 21), tab, precision="fp64", seed=5)
+    ph = jumc.Photons(1_000_000, t.photon_numax, seed=3, ctx=ctx)
+    fld = jumc.FixedField(-1e7, ctx)
+    try:
+        d0 = streamer.diagnostics(pop, ph)
+        assert d0["active_superphotons"] == 0 and d0["physical_photons"] == 0.0
+        for _ in range(2):
+            jumc.advance_mixed(pop, ph, fld, DT)
+        d = streamer.diagnostics(pop, ph)
+        g, gp = pop.download(), ph.download()
+        act = g.active.astype(bool)
+        en = 0.5 * co.electron_mass * np.einsum("ij,ij->i", g.v, g.v)
+        assert d["active_superelectrons"] == int(act.sum())
+        assert d["physical_electrons"] == pytest.approx(float(g.w[act].sum()), rel=1e-13)
+        assert d["mean_energy"] == pytest.approx(float((g.w[act] * en[act]).sum() / g.w[act].sum()), rel=1e-12)
+        assert d["max_energy"] == pytest.approx(float(en.max()), rel=1e-15)
+        pa = gp.active.astype(bool)
+        assert d["active_superphotons"] == int(pa.sum()) > 0
+        assert d["physical_photons"] == pytest.approx(float(gp.w[pa].sum()), rel=1e-13)
+    finally:
+        fld.close(); ph.close(); pop.close(); tab.close()
