@@ -1495,6 +1495,185 @@ def run_reference_fluid(args):
     return 0
 
 
+INIT_METRIC = "initfromfiles! electrons/s"
+
+
+def init_alg_bytes(cells: int, electrons: int, esz: int) -> float:
+    """Algorithmic HBM bytes of one initfromfiles!: ne and q read by both passes (32 B per
+    cell), the counts written and read twice (12 B), the bases written and read (16 B),
+    qfixed's density part written (8 B); each electron's x, v, w, s written (8 values of esz
+    bytes) and its active flag (1 B)."""
+    return cells * (32.0 + 12.0 + 16.0 + 8.0) + electrons * (8.0 * esz + 1.0)
+
+
+def init_config(spec, extra=None):
+    f = spec.fluid
+    p = f.poisson
+    c = {"workload": f"initfromfiles!(PoissonInitSampling({spec.p}), ...) on the sample grid: R={p.R:g} m, "
+                     f"L={p.L:g} m, {p.M}x{p.N} cells; ne a channel of peak {f.peak:g} m^-3 (Gaussian in r, sigma "
+                     f"{p.sigma_r:g} m, z in [{p.z0:g}, {p.z1:g}] m), q = 1 % of its charge; fluid_threshold "
+                     f"{f.threshold:g} m^-3 (cells above go to the fluid); FP32 electrons, seed {spec.seed}",
+         "cells": p.M * p.N, "l2": "ne, q (252 MB) and the electrons exceed L2", "parallelism": "1 GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def init_oracle_call(spec, ne, q):
+    """One initfromfiles! of the oracle (serial, as the reference's loop); returns (s, n)."""
+    from oracle import initdens_ref as I
+    p = spec.fluid.poisson
+    t0 = time.perf_counter()
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, p.R, p.L, p.M, p.N, I.POISSON, spec.p,
+                                       fluid_threshold=spec.fluid.threshold, seed=spec.seed, cap=12_000_000)
+    return time.perf_counter() - t0, len(w)
+
+
+def run_init(args):
+    import ctypes as C
+
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import jumc, lxcat, streamer, workloads
+    from mcstreamer_b200.fluid import Fluid
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        # replicas only: one grid's initialisation is not sharded
+        import torch.distributed as dist
+        dist.init_process_group("nccl")
+    torch.cuda.set_device(local)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spec = workloads.init_spec()
+    p = spec.fluid.poisson
+    ne, q = workloads.init_densities(spec)
+    cap = 12_000_000
+    tab = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
+    grid = streamer.GridCyl(p.R, p.L, p.M, p.N, ctx=ctx)
+    fl = Fluid(grid)
+    pop = jumc.Population(cap, None, tab, precision="fp32", seed=spec.seed)
+    lib = ctx.lib
+    d_ne = torch.from_numpy(np.ascontiguousarray(ne.ravel(order="F"))).cuda()
+    d_q = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).cuda()
+    added = C.c_int64()
+
+    def step():
+        ctx.check(lib.mcs_pop_upload(pop.h, None, None, None, None, None, 0))
+        ctx.check(lib.mcs_init_from_density_device(pop.h, grid.h_, C.c_void_p(d_ne.data_ptr()),
+                                                   C.c_void_p(d_q.data_ptr()), L.INIT_POISSON, spec.p,
+                                                   spec.fluid.threshold, spec.seed, C.byref(added)))
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        for _ in range(args.steps):
+            ctx.check(lib.mcs_pop_upload(pop.h, None, None, None, None, None, 0))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.mcs_init_from_density_device(pop.h, grid.h_, C.c_void_p(d_ne.data_ptr()),
+                                                       C.c_void_p(d_q.data_ptr()), L.INIT_POISSON, spec.p,
+                                                       spec.fluid.threshold, spec.seed, C.byref(added)))
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+    n_el = added.value
+    total_ms = float(sum(times))
+    if ws > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms = total_ms / args.steps
+    value = ws * n_el / (ms * 1e-3)
+    pk, src = peaks()
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    alg = init_alg_bytes(p.M * p.N, n_el, 4)
+    ach = alg / (ms * 1e-3) / 1e9
+
+    # end to end: ne, q from pinned host memory; the electrons back into pinned host arrays
+    h_ne = torch.from_numpy(np.ascontiguousarray(ne.ravel(order="F"))).pin_memory()
+    h_q = torch.from_numpy(np.ascontiguousarray(q.ravel(order="F"))).pin_memory()
+    hx = torch.empty((cap, 3), dtype=torch.float64).pin_memory()
+    hv = torch.empty((cap, 3), dtype=torch.float64).pin_memory()
+    hw = torch.empty(cap, dtype=torch.float64).pin_memory()
+    hs = torch.empty(cap, dtype=torch.float64).pin_memory()
+    ha = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    pd = C.POINTER(C.c_double)
+    e2e_t = []
+    nn = C.c_int64()
+    for k in range(max(1, args.e2e_steps) + 1):
+        ctx.check(lib.mcs_pop_upload(pop.h, None, None, None, None, None, 0))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.check(lib.mcs_init_from_density(pop.h, grid.h_, C.cast(h_ne.data_ptr(), pd), C.cast(h_q.data_ptr(), pd),
+                                            L.INIT_POISSON, spec.p, spec.fluid.threshold, spec.seed,
+                                            C.byref(added)))
+        ctx.check(lib.mcs_pop_download(pop.h, C.cast(hx.data_ptr(), pd), C.cast(hv.data_ptr(), pd),
+                                       C.cast(hw.data_ptr(), pd), C.cast(hs.data_ptr(), pd),
+                                       C.cast(ha.data_ptr(), C.POINTER(C.c_uint8)), cap, C.byref(nn)))
+        if k:
+            e2e_t.append(time.perf_counter() - t0)
+    e2e_v = n_el / statistics.median(e2e_t)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        sec, n_cpu = init_oracle_call(spec, ne, q)
+        cpu = {"value": n_cpu / sec, "unit": "electrons/s", "cores": 1, "kind": "port",
+               "sample": f"one full initfromfiles! of this workload by the oracle's serial loop (the reference's "
+                         f"loop is serial): {sec:.2f} s, {n_cpu} electrons"}
+    line = {
+        "metric": INIT_METRIC, "value": value, "unit": "electrons/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 sampling, f32 electrons", "data": "synthetic",
+        "config": init_config(spec, {"electrons": n_el, "fluid_cells": int((ne > spec.fluid.threshold).sum())}),
+        "roofline": {"kernel": "mcs_init_from_density_device (k_init_count, scan, k_init_place)", "bound": "hbm",
+                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "peak_source": src, "launch_ms": ms, "alg_bytes_per_launch": alg},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "electrons/s", "h2d_bytes_per_step": 16 * p.M * p.N,
+                "d2h_bytes_per_step": 65 * n_el,
+                "path": "mcs_init_from_density (ne, q from pinned host) -> mcs_pop_download (electrons to "
+                        "pinned host, Julia layout)"},
+        "clocks": clk.summary(),
+        "gpu_launches": 6,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    pop.close(); fl.close(); grid.close(); tab.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_init(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.init_spec()
+    ne, q = workloads.init_densities(spec)
+    runs = [init_oracle_call(spec, ne, q) for _ in range(max(1, min(args.steps, 2)))]
+    sec = statistics.median(r[0] for r in runs)
+    v = runs[0][1] / sec
+    line = {
+        "impl": "reference", "metric": INIT_METRIC, "value": v, "unit": "electrons/s", "n_gpus": args.gpus,
+        "steps": len(runs), "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": init_config(spec),
+        "cpu_baseline": {"value": v, "unit": "electrons/s", "cores": 1, "kind": "port",
+                         "sample": f"{len(runs)} full initfromfiles! calls of the oracle's serial loop"},
+        "e2e": {"value": v, "unit": "electrons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -1509,6 +1688,8 @@ def main():
         return run_reference_photons(args) if args.impl == "reference" else run_photons(args)
     if args.workload == "fluid":
         return run_reference_fluid(args) if args.impl == "reference" else run_fluid(args)
+    if args.workload == "init":
+        return run_reference_init(args) if args.impl == "reference" else run_init(args)
     if args.workload == "cfg4":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU reference arm; "

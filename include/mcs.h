@@ -145,6 +145,7 @@ MCS_API int mcs_grid_set_efield(mcs_grid* g, const double* e);
 /* cart3d only: nodes [node0, node0 + count) of the node field (3 doubles per node), so a
  * large field can be streamed from the host in pieces. */
 MCS_API int mcs_grid_set_efield_range(mcs_grid* g, int64_t node0, int64_t count, const double* e);
+/* Zero a charge array; MCS_Q_FIXED also zeroes qfixed's FP64 density part on a cylindrical grid. */
 MCS_API int mcs_grid_zero(mcs_grid* g, int which);
 /* int64 at 2^-32 e: per node (cart3d) or per cell, index i + j*(M+2) (cyl). */
 MCS_API int mcs_grid_read_fixed(mcs_grid* g, int which, int64_t* out);
@@ -449,6 +450,28 @@ MCS_API int mcs_fluid_euler(mcs_fluid* f, double dt);
 MCS_API int mcs_fluid_step(mcs_fluid* f, double mobility, double dt);
 /* Kernels this fluid has launched so far. */
 MCS_API int mcs_fluid_launches(mcs_fluid* f, int64_t* count);
+
+/* ---- Initial electrons from density files: initfromfiles! (MCStreamer/src/initdens.jl:64-159) ----
+ * ne and q (electron density m^-3, charge density C/m^3) are M x N doubles with r fastest,
+ * as loadinit returns them.  Per cell, in the reference's order: above fluid_threshold the
+ * cell goes to the fluid (ne) and qfixed = q/e + ne; else nsample(method, ne, q, dV) draws
+ * the electron count and weight and sets qfixed's density part, and the electrons are
+ * placed uniformly in (r, z) and in angle, at rest, with s = nextcoll(), appended to p in
+ * cell order.  method: NoiselessInitSampling(ppc) or PoissonInitSampling(ppc).  A finite
+ * fluid_threshold needs a fluid on the grid (mcs_fluid_create); pass +inf otherwise.  More
+ * electrons than p's free capacity is MCS_ERR_CAPACITY and changes nothing.  *added gets
+ * the electrons appended. */
+enum { MCS_INIT_NOISELESS = 0, MCS_INIT_POISSON = 1 };
+MCS_API int mcs_init_from_density(mcs_pop* p, mcs_grid* g, const double* ne, const double* q, int method,
+                                  int64_t ppc, double fluid_threshold, uint64_t seed, int64_t* added);
+/* qfixed's FP64 density part on a cylindrical grid ((M+2)x(N+2), index i + j(M+2)): the
+ * densities setneedle! and initfromfiles! put into qfixed, which poisson! adds to the int64
+ * deposit's densities.  Reads zeros where nothing has been set. */
+MCS_API int mcs_grid_read_qfixed_density(mcs_grid* g, double* out);
+MCS_API int mcs_grid_write_qfixed_density(mcs_grid* g, const double* in);
+/* The same with ne and q already in device memory of the context's device. */
+MCS_API int mcs_init_from_density_device(mcs_pop* p, mcs_grid* g, const double* ne, const double* q, int method,
+                                         int64_t ppc, double fluid_threshold, uint64_t seed, int64_t* added);
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ FP64, FP32 = 0, 1
 FLAG_CLAMP_ENERGY = 1
 Q_FIXED, Q_PART = 0, 1
 PSN_U, PSN_B, PSN_BCOND, PSN_FREEBC_F = 0, 1, 2, 3
+INIT_NOISELESS, INIT_POISSON = 0, 1
 MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
@@ -137,6 +138,10 @@ SIGNATURES = {
     "mcs_fluid_euler": (i32, [vp, f64]),
     "mcs_fluid_step": (i32, [vp, f64, f64]),
     "mcs_fluid_launches": (i32, [vp, pi64]),
+    "mcs_init_from_density": (i32, [vp, vp, pd, pd, i32, i64, f64, C.c_uint64, pi64]),
+    "mcs_grid_read_qfixed_density": (i32, [vp, pd]),
+    "mcs_grid_write_qfixed_density": (i32, [vp, pd]),
+    "mcs_init_from_density_device": (i32, [vp, vp, vp, vp, i32, i64, f64, C.c_uint64, pi64]),
     "mcs_table_set_photoemission": (i32, [vp, pd, pd, f64, f64]),
     "mcs_photons_create": (i32, [vp, i64, f64, C.c_uint64, C.POINTER(C.c_void_p)]),
     "mcs_photons_destroy": (i32, [vp]),

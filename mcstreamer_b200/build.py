@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
                  "-Xptxas", "-warn-spills", "--expt-relaxed-constexpr"]
 PER_FILE = {"step_f64.cu": ["-fmad=false"], "poisson.cu": ["-fmad=false"], "photons.cu": ["-fmad=false"],
-            "fluid.cu": ["-fmad=false"]}
+            "fluid.cu": ["-fmad=false"], "init.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:

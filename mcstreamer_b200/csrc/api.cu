@@ -318,6 +318,8 @@ MCS_API int mcs_grid_destroy(mcs_grid* g) {
     cudaStreamSynchronize(g->ctx->stream);
     if (g->fluid) g->fluid->g = nullptr;
     cudaFree(g->d_e32); cudaFree(g->d_e64); cudaFree(g->d_er); cudaFree(g->d_ez); cudaFree(g->d_erz32);
+    cudaFree(g->d_qfd);
+    cudaFree(g->d_init_ws);
     cudaFree(g->d_q[0]); cudaFree(g->d_q[1]);
     delete g;
     return MCS_OK;
@@ -402,6 +404,8 @@ MCS_API int mcs_grid_zero(mcs_grid* g, int which) {
     mcs_ctx* c = g->ctx;
     if (int st = use_device(c)) return st;
     MCS_CK(c, cudaMemsetAsync(g->d_q[which], 0, g->nq * sizeof(long long), c->stream));
+    if (which == MCS_Q_FIXED && g->d_qfd)
+        MCS_CK(c, cudaMemsetAsync(g->d_qfd, 0, (size_t)(g->v.M + 2) * (g->v.N + 2) * sizeof(double), c->stream));
     return MCS_OK;
 }
 

@@ -227,6 +227,21 @@ FluidArgs args(mcs_fluid* f, double mob, double dt) {
 }
 
 }  // namespace
+
+double* grid_qfd(mcs_grid* g) {
+    if (g->d_qfd) return g->d_qfd;
+    const size_t n = (size_t)(g->v.M + 2) * (g->v.N + 2);
+    if (falloc(g->ctx, &g->d_qfd, n)) return nullptr;
+    if (cudaMemsetAsync(g->d_qfd, 0, n * sizeof(double), g->ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(g->ctx->stream) != cudaSuccess) {
+        cudaFree(g->d_qfd);
+        g->d_qfd = nullptr;
+        set_err(g->ctx, MCS_ERR_CUDA, "qfixed density: device initialisation failed");
+        return nullptr;
+    }
+    return g->d_qfd;
+}
+
 }  // namespace mcs
 
 using namespace mcs;
@@ -247,20 +262,19 @@ MCS_API int mcs_fluid_create(mcs_grid* g, mcs_fluid** out) {
     f->g = g;
     f->M = g->v.M;
     f->N = g->v.N;
-    const size_t n = padded(f), nq = (size_t)(f->M + 2) * (f->N + 2);
+    const size_t n = padded(f);
     int st = falloc(c, &f->ne[0], n);
     if (!st) st = falloc(c, &f->ne[1], n);
     if (!st) st = falloc(c, &f->dne, n);
-    if (!st) st = falloc(c, &f->qfd, nq);
+    if (!st && !grid_qfd(g)) st = MCS_ERR_NOMEM;
     if (st) {
-        cudaFree(f->ne[0]); cudaFree(f->ne[1]); cudaFree(f->dne); cudaFree(f->qfd);
+        cudaFree(f->ne[0]); cudaFree(f->ne[1]); cudaFree(f->dne);
         delete f;
         return st;
     }
     cudaMemsetAsync(f->ne[0], 0, n * sizeof(double), c->stream);
     cudaMemsetAsync(f->ne[1], 0, n * sizeof(double), c->stream);
     cudaMemsetAsync(f->dne, 0, n * sizeof(double), c->stream);
-    cudaMemsetAsync(f->qfd, 0, nq * sizeof(double), c->stream);
     MCS_CK(c, cudaStreamSynchronize(c->stream));
     g->fluid = f;
     *out = f;
@@ -272,7 +286,7 @@ MCS_API int mcs_fluid_destroy(mcs_fluid* f) {
     cudaSetDevice(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
     if (f->g && f->g->fluid == f) f->g->fluid = nullptr;
-    cudaFree(f->ne[0]); cudaFree(f->ne[1]); cudaFree(f->dne); cudaFree(f->qfd);
+    cudaFree(f->ne[0]); cudaFree(f->ne[1]); cudaFree(f->dne);
     delete f;
     return MCS_OK;
 }
@@ -284,7 +298,7 @@ MCS_API int mcs_fluid_upload(mcs_fluid* f, const double* ne, const double* qfd) 
     if (ne)
         MCS_CK(c, cudaMemcpyAsync(f->ne[f->cur], ne, padded(f) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     if (qfd)
-        MCS_CK(c, cudaMemcpyAsync(f->qfd, qfd, (size_t)(f->M + 2) * (f->N + 2) * sizeof(double),
+        MCS_CK(c, cudaMemcpyAsync(f->g->d_qfd, qfd, (size_t)(f->M + 2) * (f->N + 2) * sizeof(double),
                                   cudaMemcpyHostToDevice, c->stream));
     MCS_CK(c, cudaStreamSynchronize(c->stream));
     return MCS_OK;
@@ -298,7 +312,7 @@ MCS_API int mcs_fluid_download(mcs_fluid* f, double* ne, double* dne, double* qf
         MCS_CK(c, cudaMemcpyAsync(ne, f->ne[f->cur], padded(f) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (dne) MCS_CK(c, cudaMemcpyAsync(dne, f->dne, padded(f) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (qfd)
-        MCS_CK(c, cudaMemcpyAsync(qfd, f->qfd, (size_t)(f->M + 2) * (f->N + 2) * sizeof(double),
+        MCS_CK(c, cudaMemcpyAsync(qfd, f->g->d_qfd, (size_t)(f->M + 2) * (f->N + 2) * sizeof(double),
                                   cudaMemcpyDeviceToHost, c->stream));
     MCS_CK(c, cudaStreamSynchronize(c->stream));
     return MCS_OK;
@@ -310,7 +324,7 @@ MCS_API int mcs_fluid_set_needle(mcs_fluid* f, double sigma_z, double sigma_r, d
     (void)position_r;   // taken and unused by setneedle!
     if (int e = use(f)) return e;
     ++f->launches;
-    k_needle<<<fluid_grid(f, f->N), dim3(BX, BY), 0, f->ctx->stream>>>(f->ne[f->cur], f->qfd, f->M, f->N,
+    k_needle<<<fluid_grid(f, f->N), dim3(BX, BY), 0, f->ctx->stream>>>(f->ne[f->cur], f->g->d_qfd, f->M, f->N,
                                                                         f->g->v.dr, f->g->v.dz, sigma_z, sigma_r,
                                                                         position_z, ne0);
     MCS_CK(f->ctx, cudaGetLastError());

@@ -23,7 +23,10 @@ enum : uint32_t {
 
 // Philox stream tags (4th counter word); must match the oracle.
 enum : uint32_t { TAG_ADVANCE = 0, TAG_SWARM_RESAMPLE = 1, TAG_CELL_RESAMPLE = 2, TAG_INIT = 3,
-                  TAG_COLLISIONS = 4, TAG_PHOTON = 5 };
+                  TAG_COLLISIONS = 4, TAG_PHOTON = 5, TAG_DENSITY = 6 };
+// initfromfiles!: cell c's count draws from {c, 0, k/4, TAG_DENSITY}, its electron k from the four
+// words of {c, k, 0, TAG_DENSITY | TAG_DENSITY_PARTICLE} (r, z, phi, s).
+constexpr uint32_t TAG_DENSITY_PARTICLE = 0x40000000u;
 // Photo-emission streams of collision event j of an electron: the photon count draws from
 // {slot, step, k/4, TAG_PHOTON_COUNT | j}, photon p from {slot, step, p, TAG_PHOTON_DRAW | j}.
 constexpr uint32_t TAG_PHOTON_COUNT = 0x20000000u;

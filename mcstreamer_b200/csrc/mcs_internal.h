@@ -161,12 +161,14 @@ struct mcs_grid {
     long long* d_q[2] = {nullptr, nullptr};
     size_t nq = 0;          // entries per charge array
     struct mcs_fluid* fluid = nullptr;   // cyl: the electron fluid on this grid, if any
+    double* d_qfd = nullptr;  // cyl: FP64 density part of qfixed, (M+2)x(N+2), made on first use
+    void* d_init_ws = nullptr;   // initfromfiles! workspace (counts, bases, scan sums), kept
+    size_t init_ws_bytes = 0;
 };
 
 // The electron fluid of MCStreamer (fluid.jl) on a cylindrical grid: density ne and its
 // derivative dne with two ghost layers ((M+4)x(N+4), (i, j) at (i+1) + (j+1)(M+4)), double
-// buffered for the fused setdne! + euler!, and qfd, the FP64 density part of qfixed
-// ((M+2)x(N+2)) that setneedle! adds to.
+// buffered for the fused setdne! + euler!.  setneedle! adds to the grid's d_qfd.
 struct mcs_fluid {
     mcs_ctx* ctx = nullptr;
     mcs_grid* g = nullptr;
@@ -174,9 +176,14 @@ struct mcs_fluid {
     double* ne[2] = {nullptr, nullptr};
     int cur = 0;
     double* dne = nullptr;
-    double* qfd = nullptr;
     long long launches = 0;
 };
+
+namespace mcs {
+// The grid's FP64 density part of qfixed, allocated (zeroed) on first use; nullptr on failure
+// with the context's error set.
+double* grid_qfd(mcs_grid* g);
+}  // namespace mcs
 
 struct mcs_field {
     mcs_ctx* ctx = nullptr;

@@ -838,8 +838,8 @@ __global__ void k_top_ghost(double* u, int M, int N, const double* bcond) {
 
 // q of poisson! (poisson.jl:17-34) from the int64 cell charges: densities q * 2^-32 / dV,
 // q0 = (qfixed + qpart - ne) e through the NullDenoiser's Float32 copy.  qfixed is the int64
-// deposit plus qfd, its FP64 density part (the fluid's needle), and ne the fluid density
-// ((M+4)x(N+4)); both are zero without a fluid (null pointers).  Ghost cells are zero.
+// deposit plus qfd, its FP64 density part (setneedle!, initfromfiles!), and ne the fluid
+// density ((M+4)x(N+4)); either is zero when absent (null pointer).  Ghost cells are zero.
 __global__ void k_assemble(double* b, const long long* qf, const long long* qp, const double* qfd,
                            const double* ne, int M, int N, double dr, double dz) {
     const long ld = M + 2;
@@ -1645,7 +1645,7 @@ MCS_API int mcs_poisson_assemble(mcs_poisson* p) {
     ++p->launches;
     const mcs_fluid* fl = p->g->fluid;
     k_assemble<<<grid_blocks(p, n), kThreads, 0, p->ctx->stream>>>(
-        p->b, p->g->d_q[MCS_Q_FIXED], p->g->d_q[MCS_Q_PART], fl ? fl->qfd : nullptr, fl ? fl->ne[fl->cur] : nullptr,
+        p->b, p->g->d_q[MCS_Q_FIXED], p->g->d_q[MCS_Q_PART], p->g->d_qfd, fl ? fl->ne[fl->cur] : nullptr,
         p->M, p->N, p->dr, p->dz);
     PSN_LAUNCH(p);
     return MCS_OK;

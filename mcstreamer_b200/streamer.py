@@ -146,6 +146,20 @@ class GridCyl:
             raise ValueError("charge array of the wrong size")
         self.ctx.check(self.ctx.lib.mcs_grid_write_fixed(self.h_, which, L.i64ptr(q)))
 
+    def read_qfixed_density(self) -> np.ndarray:
+        """qfixed's FP64 density part (setneedle!, initfromfiles!), (M+2, N+2) like
+        calloc_centers."""
+        out = np.zeros((self.M + 2) * (self.N + 2))
+        self.ctx.check(self.ctx.lib.mcs_grid_read_qfixed_density(self.h_, L.dptr(out)))
+        return out.reshape((self.M + 2, self.N + 2), order="F")
+
+    def write_qfixed_density(self, a: np.ndarray) -> None:
+        a = np.asarray(a, dtype=np.float64)
+        if a.shape != (self.M + 2, self.N + 2):
+            raise ValueError(f"expected shape {(self.M + 2, self.N + 2)}, got {a.shape}")
+        flat = np.ascontiguousarray(a.ravel(order="F"))
+        self.ctx.check(self.ctx.lib.mcs_grid_write_qfixed_density(self.h_, L.dptr(flat)))
+
     def read_fixed(self, which: int = L.Q_PART) -> np.ndarray:
         """The int64 cell charges (2^-32 e), flat, index i + j*(M+2)."""
         out = np.zeros((self.M + 2) * (self.N + 2), dtype=np.int64)

@@ -306,3 +306,31 @@ def fluid_density(spec: FluidSpec) -> np.ndarray:
     ne = np.zeros((M + 4, N + 4), order="F")
     ne[2:M + 2, 2:N + 2] = np.where(dens > spec.threshold, dens, 0.0)
     return ne
+
+
+# ---------------------------------------------------------------------------------------
+# initfromfiles! on the sample grid: the fluid workload's channel as the init files' electron
+# density, PoissonInitSampling(ntarget = 10) and fluid_threshold = 1e20 (samples/input.toml).
+# ---------------------------------------------------------------------------------------
+@dataclass
+class InitSpec:
+    fluid: FluidSpec = field(default_factory=FluidSpec)
+    p: int = 10
+    seed: int = 1
+
+
+def init_spec() -> InitSpec:
+    return InitSpec()
+
+
+def init_densities(spec: InitSpec):
+    """(ne, q) as loadinit returns them, (M, N) Fortran-ordered: the channel of peak
+    `fluid.peak` (m^-3) everywhere, and a net charge of 1 % of its electron density."""
+    f = spec.fluid
+    p = f.poisson
+    rc = (np.arange(p.M) + 0.5) * (p.R / p.M)
+    zc = (np.arange(p.N) + 0.5) * (p.L / p.N)
+    ne = f.peak * np.exp(-rc[:, None] ** 2 / (2 * p.sigma_r ** 2)) * ((zc >= p.z0) & (zc <= p.z1))[None, :]
+    ne = np.asfortranarray(ne)
+    q = np.asfortranarray(0.01 * 1.6021766208e-19 * ne)
+    return ne, q

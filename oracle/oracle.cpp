@@ -945,3 +945,91 @@ void orc_deposit(const orc_pop* pop, orc_tracker* trk, double val, int quantize_
 }
 
 }  // extern "C"
+
+/* ---------------- initfromfiles!: MCStreamer/src/initdens.jl:64-159 ---------------- */
+namespace {
+
+struct CellSample {
+    int64_t nume;
+    double qf, w;
+};
+
+/* randround: initdens.jl:145-159 */
+int64_t randround(Stream& rng, double x) {
+    const double m = std::floor(x);
+    const double f = x - m;
+    return rng.next() > f ? (int64_t)m : (int64_t)m + 1;
+}
+
+/* nsample(::NoiselessInitSampling) :109-127 and nsample(::PoissonInitSampling) :130-142 */
+CellSample nsample(int method, int64_t p, double ne, double q, double V, Stream& rng) {
+    CellSample c{};
+    const double pf = (double)p;
+    if (method == ORC_INIT_NOISELESS) {
+        const double n = ne * V;
+        if (n < 1) {
+            c.nume = poisson_sample(rng, n);
+            c.w = 1.0;
+        } else if (n < pf) {
+            c.nume = randround(rng, n);
+            c.w = 1.0;
+        } else {
+            c.nume = p;
+            c.w = n / pf;
+        }
+        c.qf = q / ELEMENTARY_CHARGE + c.w * (double)c.nume / V;
+    } else {
+        const double a = ne * V / pf;
+        c.w = (a > 1.0 || std::isnan(a)) ? a : 1.0;                 /* max(1, ...) */
+        c.nume = poisson_sample(rng, ne * V / c.w);
+        const double ni = ne + q / ELEMENTARY_CHARGE;
+        const double b = std::fabs(ni) * V / pf;
+        const double wi = (b > 1.0 || std::isnan(b)) ? b : 1.0;
+        const int64_t numi = poisson_sample(rng, std::fabs(ni) * V / wi);
+        const double sg = ni > 0 ? 1.0 : (ni < 0 ? -1.0 : ni);       /* sign(ni) */
+        c.qf = sg * (double)numi * wi / V;
+    }
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t orc_init_from_density(int M, int N, double R, double L, const double* ne, const double* q, int method,
+                              int64_t p, double fluid_threshold, uint64_t seed, int64_t cap, double* x, double* w,
+                              double* s, double* qfd, double* ne_fluid) {
+    const double dr = R / M, dz = L / N;
+    int64_t n = 0;
+    for (int j = 1; j <= N; ++j)
+        for (int i = 1; i <= M; ++i) {
+            const uint32_t c = (uint32_t)((i - 1) + (int64_t)(j - 1) * M);
+            const double rc = ((double)(i - 1) + 0.5) * dr;
+            const double V = 2.0 * M_PI * rc * dr * dz;                  /* dV(grid, i), grid.jl:76 */
+            const double nec = ne[c], qc = q[c];
+            if (nec > fluid_threshold) {
+                ne_fluid[(i + 1) + (int64_t)(j + 1) * (M + 4)] = nec;
+                qfd[i + (int64_t)j * (M + 2)] = qc / ELEMENTARY_CHARGE + nec;
+                continue;
+            }
+            Stream rng(seed, c, 0u, ORC_TAG_DENSITY);
+            const CellSample cs = nsample(method, p, nec, qc, V, rng);
+            qfd[i + (int64_t)j * (M + 2)] = cs.qf;
+            for (int64_t k = 0; k < cs.nume; ++k) {
+                if (n >= cap) return -1;                                   /* "Particle limit reached" */
+                Stream pr(seed, c, (uint32_t)k, ORC_TAG_DENSITY | ORC_TAG_DENSITY_PARTICLE);
+                const double r = dr * pr.next() + (double)(i - 1) * dr;   /* rf[i] = (i - 1) dr */
+                const double z = dz * pr.next() + (double)(j - 1) * dz;
+                const double phi = 2.0 * M_PI * pr.next();
+                x[3 * n] = r * std::cos(phi);
+                x[3 * n + 1] = r * std::sin(phi);
+                x[3 * n + 2] = z;
+                w[n] = cs.w;
+                s[n] = -std::log(pr.next());                               /* nextcoll() */
+                ++n;
+            }
+        }
+    return n;
+}
+
+}  // extern "C"

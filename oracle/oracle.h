@@ -32,7 +32,11 @@ enum { ORC_NULL = 0, ORC_ELASTIC = 1, ORC_EXCITATION = 2, ORC_IONIZATION = 3,
 
 /* Philox stream tags (4th counter word). */
 enum { ORC_TAG_ADVANCE = 0, ORC_TAG_SWARM_RESAMPLE = 1, ORC_TAG_CELL_RESAMPLE = 2,
-       ORC_TAG_INIT = 3, ORC_TAG_COLLISIONS = 4, ORC_TAG_PHOTON = 5 };
+       ORC_TAG_INIT = 3, ORC_TAG_COLLISIONS = 4, ORC_TAG_PHOTON = 5, ORC_TAG_DENSITY = 6 };
+/* initfromfiles!: cell c's count draws from {c, 0, k/4, ORC_TAG_DENSITY}; its electron k from
+ * the four words of {c, k, 0, ORC_TAG_DENSITY | ORC_TAG_DENSITY_PARTICLE} (r, z, phi, s). */
+#define ORC_TAG_DENSITY_PARTICLE 0x40000000u
+enum { ORC_INIT_NOISELESS = 0, ORC_INIT_POISSON = 1 };
 /* Photo-emission streams of collision event j of an electron: the photon count draws
  * from {slot, step, k/4, ORC_TAG_PHOTON_COUNT | j}, photon p from words 4p..4p+3 of
  * {slot, step, p, ORC_TAG_PHOTON_DRAW | j} (direction phi, u; log-nu fraction; s). */
@@ -138,6 +142,15 @@ void orc_mg_gauss_seidel(double* u, const double* b, int M, int N);
 void orc_mg_residual(double* r, const double* u, const double* b, double s, int M, int N);
 void orc_mg_restrict(double* rh, const double* r, int M, int N);
 void orc_mg_interpolate(double* f, const double* h, int M, int N, int add);
+
+/* initfromfiles!(method, fields, loader; fluid_threshold, maxp) (MCStreamer/src/initdens.jl:
+ * 64-102) over densities ne, q (M x N doubles, r fastest): electrons (x 3 per electron, w, s;
+ * at rest, active) in cell order, qfixed's density part qfd ((M+2)x(N+2)) set per cell and
+ * the fluid density ne_fluid ((M+4)x(N+4)) above the threshold.  Returns the electrons
+ * written, or -1 when more than cap would be. */
+int64_t orc_init_from_density(int M, int N, double R, double L, const double* ne, const double* q, int method,
+                              int64_t p, double fluid_threshold, uint64_t seed, int64_t cap, double* x, double* w,
+                              double* s, double* qfd, double* ne_fluid);
 
 #ifdef __cplusplus
 }

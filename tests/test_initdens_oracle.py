@@ -1,0 +1,95 @@
+"""initfromfiles!'s CPU restatement (orc_init_from_density) pinned without a GPU against what
+the reference's code defines (MCStreamer/src/initdens.jl:64-159): the noiseless sampler's
+three regimes, the Poisson sampler's expected counts and charge, the fluid cells, electrons
+placed in their own cell at rest, in the serial cell order, with s ~ Exp(1).  No reference
+test exists for initfromfiles!."""
+import numpy as np
+import pytest
+import scipy.stats as ss
+
+from oracle import initdens_ref as I
+
+E = 1.6021766208e-19
+R, LEN = 1e-3, 2e-3
+
+
+def _vol(M, N):
+    dr, dz = R / M, LEN / N
+    rc = (np.arange(M) + 0.5) * dr
+    return (2.0 * np.pi * rc * dr * dz)[:, None] * np.ones((1, N))
+
+
+def _cells(x, M, N):
+    r = np.hypot(x[:, 0], x[:, 1])
+    return np.floor(r / (R / M)).astype(int), np.floor(x[:, 2] / (LEN / N)).astype(int)
+
+
+def test_noiseless_regimes_and_charge():
+    M, N, p = 12, 10, 10
+    V = _vol(M, N)
+    n = np.empty((M, N))
+    n[:4] = 0.4            # Poisson(n)
+    n[4:8] = 3.6           # randround(n)
+    n[8:] = 57.0           # p electrons of weight n / p
+    ne = n / V
+    q = 0.3 * E * ne
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, R, LEN, M, N, I.NOISELESS, p, seed=4)
+    i, j = _cells(x, M, N)
+    cnt = np.zeros((M, N), int)
+    np.add.at(cnt, (i, j), 1)
+    assert set(np.unique(cnt[4:8])) <= {3, 4}
+    assert (cnt[8:] == p).all()
+    assert cnt[:4].max() <= 6
+    np.testing.assert_allclose(w[i >= 8], 57.0 / p, rtol=1e-15)
+    assert (w[i < 8] == 1.0).all()
+    # qf = q / e + w nume / V
+    wc = np.where(np.arange(M)[:, None] >= 8, 57.0 / p, 1.0)
+    np.testing.assert_allclose(qfd[1:M + 1, 1:N + 1], q / E + wc * cnt / V, rtol=1e-14)
+    assert (nf == 0).all()
+    # electrons at rest in their own cell, in serial cell order (r fastest)
+    order = i + M * j
+    assert (np.diff(order) >= 0).all()
+    assert ss.kstest(s, "expon").pvalue > 1e-4
+
+
+def test_noiseless_means():
+    M, N, p = 40, 50, 10
+    V = _vol(M, N)
+    for nval, tol in ((0.4, 0.05), (3.6, 0.02)):
+        ne = np.full((M, N), nval) / V
+        x, w, s, qfd, nf = I.initfromfiles(ne, 0 * ne, R, LEN, M, N, I.NOISELESS, p, seed=7)
+        assert abs(len(w) / (M * N) - nval) < 5 * np.sqrt(nval / (M * N)) + 1e-9, (len(w), nval)
+
+
+def test_poisson_sampler_expectations():
+    """PoissonInitSampling: E[nume] w = ne V; E[qf] V = |ni| V sign(ni) with ni = ne + q/e."""
+    M, N, p = 30, 40, 10
+    V = _vol(M, N)
+    ne = np.full((M, N), 23.0) / V          # w = 2.3, nume ~ Poisson(10)
+    q = -1.7 * E * ne                        # ni = -0.7 ne
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, R, LEN, M, N, I.POISSON, p, seed=2)
+    np.testing.assert_allclose(w, 2.3, rtol=1e-14)
+    tot = len(w) * 2.3
+    assert abs(tot - 23.0 * M * N) < 5 * 2.3 * np.sqrt(10 * M * N)
+    charge = (qfd[1:M + 1, 1:N + 1] * V).sum()
+    assert charge < 0
+    assert abs(charge + 0.7 * 23.0 * M * N) < 5 * np.sqrt(0.7 * 23.0 * 1.61 * M * N)
+    # the ions' weight wi = max(1, |ni| V / p): qf is a multiple of wi / V
+    k = -qfd[1:M + 1, 1:N + 1] * V / 1.61
+    np.testing.assert_allclose(k, np.round(k), atol=1e-9)
+
+
+def test_fluid_cells_and_capacity():
+    M, N, p = 8, 6, 5
+    V = _vol(M, N)
+    ne = np.full((M, N), 2.0) / V
+    ne[2:4, 1:3] = 1e21
+    q = np.full((M, N), 1e-3)
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, R, LEN, M, N, I.NOISELESS, p, fluid_threshold=1e20, seed=1)
+    np.testing.assert_array_equal(nf[4:6, 3:5], 1e21)
+    assert (nf > 0).sum() == 4
+    np.testing.assert_array_equal(qfd[3:5, 2:4], 1e-3 / E + 1e21)
+    i, j = _cells(x, M, N)
+    assert not ((i >= 2) & (i < 4) & (j >= 1) & (j < 3)).any()
+    n, *_ = I.initfromfiles(ne, q, R, LEN, M, N, I.NOISELESS, p, fluid_threshold=1e20, seed=1, cap=len(w) - 1)
+    assert n == -1
