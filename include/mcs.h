@@ -364,6 +364,9 @@ MCS_API int mcs_photons_copy(mcs_photons* dst, const mcs_photons* src);
  * MCStreamer's per-step diagnostics read them, main.jl:272-273): FP64 sums over the active
  * photons in a fixed order. */
 MCS_API int mcs_photons_moments(mcs_photons* ph, double* out);
+/* repack!(photons) (JuMC/src/population.jl:191-215): the inactive photons removed with the
+ * reference's permutation (the k-th hole filled from the k-th active counted from the end). */
+MCS_API int mcs_photons_repack(mcs_photons* ph);
 /* Device times (ms) of the last mixed advance's photon kernels and the photons they handled:
  * the emission of the new photons and the photon step. */
 MCS_API int mcs_photons_last_timing(mcs_photons* ph, float* emit_ms, int64_t* emitted, float* step_ms,

@@ -146,6 +146,7 @@ SIGNATURES = {
     "mcs_photons_create": (i32, [vp, i64, f64, C.c_uint64, C.POINTER(C.c_void_p)]),
     "mcs_photons_destroy": (i32, [vp]),
     "mcs_photons_moments": (i32, [vp, pd]),
+    "mcs_photons_repack": (i32, [vp]),
     "mcs_photons_upload": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64]),
     "mcs_photons_download": (i32, [vp, pd, pd, pd, pd, pd, pu8, i64, pi64]),
     "mcs_photons_count": (i32, [vp, pi64]),

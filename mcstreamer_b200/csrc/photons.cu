@@ -215,6 +215,40 @@ __global__ void __launch_bounds__(kDiagThreads) k_photon_sums_final(double* part
     if (threadIdx.x == 0) { part[2 * nb] = cnt; part[2 * nb + 1] = wt; }
 }
 
+// repack! of the photon population (JuMC/src/population.jl:191-215): with A actives, the
+// k-th hole below A (ascending) takes the k-th active at or above A counted from the end.
+// From the exclusive scan base[] of the active flags: a hole i < A has rank i - base[i], an
+// active i >= A has rank A - 1 - base[i].
+__global__ void k_photon_flags(const uint8_t* act, long long n, uint32_t* flags) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        flags[i] = act[i] ? 1u : 0u;
+}
+
+__global__ void k_photon_holes(const uint8_t* act, const unsigned long long* base, const unsigned long long* total,
+                               uint32_t* hole_at) {
+    const long long A = (long long)*total;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < A; i += (long long)gridDim.x * blockDim.x)
+        if (!act[i]) hole_at[i - (long long)base[i]] = (uint32_t)i;
+}
+
+struct PhotonRaw {
+    double* f[9];
+    uint8_t* act;
+};
+
+__global__ void k_photon_fill(PhotonRaw P, const unsigned long long* base, const unsigned long long* total, long long n,
+                              const uint32_t* hole_at) {
+    const long long A = (long long)*total;
+    for (long long i = A + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (!P.act[i]) continue;
+        const long long h = hole_at[A - 1 - (long long)base[i]];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) P.f[q][h] = P.f[q][i];
+        P.act[h] = 1;
+    }
+}
+
 }  // namespace
 }  // namespace mcs
 
@@ -498,6 +532,31 @@ MCS_API int mcs_photons_count(mcs_photons* ph, int64_t* n) {
     if (!ph || !n) return MCS_ERR_ARG;
     *n = ph->n;
     return MCS_OK;
+}
+
+MCS_API int mcs_photons_repack(mcs_photons* ph) {
+    if (!ph) return MCS_ERR_ARG;
+    mcs_ctx* c = ph->ctx;
+    if (ph->n == 0) return MCS_OK;
+    MCS_CK(c, cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    const long long n = ph->n;
+    const int g = blocks_for(c, n, 256);
+    k_photon_flags<<<g, 256, 0, st>>>(ph->d_act, n, ph->d_islot);
+    MCS_CK_LAUNCH(c);
+    if (int e = scan_counts(ph, ph->d_islot, n, st)) return e;   // bases in d_base, A in *h_total
+    const long long A = (long long)*ph->h_total;
+    if (A < n) {
+        if (int e = grow(c, &ph->d_pslot, &ph->pslot_cap, std::max(1LL, A))) return e;
+        k_photon_holes<<<g, 256, 0, st>>>(ph->d_act, ph->d_base, ph->d_total, ph->d_pslot);
+        PhotonRaw R;
+        for (int q = 0; q < 9; ++q) R.f[q] = ph->d_f[q];
+        R.act = ph->d_act;
+        k_photon_fill<<<g, 256, 0, st>>>(R, ph->d_base, ph->d_total, n, ph->d_pslot);
+        MCS_CK_LAUNCH(c);
+    }
+    ph->n = A;
+    return sync_status(c);
 }
 
 MCS_API int mcs_photons_moments(mcs_photons* ph, double* out) {

@@ -286,6 +286,10 @@ class Photons:
     def actives(self) -> int:
         return int(self.moments()[0])
 
+    def repack(self) -> None:
+        """repack!(photons) (population.jl:191-215)."""
+        self.ctx.check(self.ctx.lib.mcs_photons_repack(self.h))
+
     def weight(self) -> float:
         return float(self.moments()[1])
 

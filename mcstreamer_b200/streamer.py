@@ -226,6 +226,12 @@ def advance_deposit_host(work: Population, efield: FieldInterp, dt: float, track
     return nn.value
 
 
+def resample(popl: Population, grid, ntarget: int, nmax: int) -> None:
+    """resample!(popl, fields, ntarget, nmax) (MCStreamer/src/resample.jl:7-77): the stable
+    cell sort, then the per-cell roulette and splitting."""
+    popl.ctx.check(popl.ctx.lib.mcs_resample_cells(popl.h, grid.h_, int(ntarget), int(nmax)))
+
+
 def diagnostics(popl: Population, photons=None) -> dict:
     """The per-step diagnostics of nsteps (MCStreamer/src/main.jl:269-279): meanenergy and
     maxenergy of the electrons (J), their actives and weight, and the photons' actives and

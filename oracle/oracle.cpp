@@ -744,6 +744,28 @@ int orc_repack(orc_pop* pop) {
     return 0;
 }
 
+/* repack!(photons): the same loop over the photon arrays. */
+int orc_photons_repack(orc_photons* ph) {
+    if (ph->n == 0) return 0;
+    int64_t l = ph->n - 1;
+    while (l >= 0 && !ph->active[l]) --l;
+    if (l < 0) { ph->n = 0; return 0; }
+    auto copy = [&](int64_t dst, int64_t src) {
+        for (int q = 0; q < 3; ++q) { ph->x[3 * dst + q] = ph->x[3 * src + q]; ph->v[3 * dst + q] = ph->v[3 * src + q]; }
+        ph->nu[dst] = ph->nu[src]; ph->w[dst] = ph->w[src]; ph->s[dst] = ph->s[src]; ph->active[dst] = ph->active[src];
+    };
+    int64_t i = 0;
+    while (i <= l) {
+        if (!ph->active[i]) {
+            copy(i, l);
+            --l;
+            while (!ph->active[l]) --l;
+        }
+        ++i;
+    }
+    ph->n = l + 1;
+    return 0;
+}
 
 /* Swarm.resample!: Swarm/src/Swarm.jl:193-223 */
 int orc_swarm_resample(orc_pop* pop, int64_t n0, double tol) {

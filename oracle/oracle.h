@@ -148,6 +148,8 @@ void orc_mg_interpolate(double* f, const double* h, int M, int N, int add);
  * at rest, active) in cell order, qfixed's density part qfd ((M+2)x(N+2)) set per cell and
  * the fluid density ne_fluid ((M+4)x(N+4)) above the threshold.  Returns the electrons
  * written, or -1 when more than cap would be. */
+/* repack!(photons) (JuMC/src/population.jl:191-215). */
+int orc_photons_repack(orc_photons* ph);
 int64_t orc_init_from_density(int M, int N, double R, double L, const double* ne, const double* q, int method,
                               int64_t p, double fluid_threshold, uint64_t seed, int64_t cap, double* x, double* w,
                               double* s, double* qfd, double* ne_fluid);

@@ -198,10 +198,11 @@ def efield_faces(u, eb, R, L, er, ez):
     er[:, N + 1] = er[:, N]
 
 
-def poisson(conf: MGConf, qfixed, qpart, u, er, ez, eb, R, L):
-    """poisson! after density!: returns (b, it1, it2, bcond); u, er, ez updated in place."""
+def poisson(conf: MGConf, qfixed, qpart, u, er, ez, eb, R, L, qfd=None, ne=None):
+    """poisson! after density!: returns (b, it1, it2, bcond); u, er, ez updated in place.
+    qfd and ne: qfixed's FP64 density part and the fluid density (see assemble_charge)."""
     M, N = u.shape[0] - 2, u.shape[1] - 2
-    b = assemble_charge(qfixed, qpart, R, L, M, N)
+    b = assemble_charge(qfixed, qpart, R, L, M, N, qfd=qfd, ne=ne)
     it1, it2, bcond = solve_freebc(conf, u, b, R, L)
     efield_faces(u, eb, R, L, er, ez)
     return b, it1, it2, bcond

@@ -75,6 +75,7 @@ def lib():
         L.orc_advance_mixed.argtypes = [C.POINTER(Pop), C.POINTER(Photons), C.POINTER(Table), C.POINTER(Field),
                                         C.c_double, C.POINTER(Tracker), C.c_int, C.c_int]
         L.orc_photon_advance.argtypes = [C.POINTER(Photons), C.POINTER(Pop), C.c_double, C.POINTER(Tracker), C.c_int]
+        L.orc_photons_repack.argtypes = [C.POINTER(Photons)]
         _L = L
     return _L
 
@@ -170,6 +171,10 @@ def advance_mixed(pop, photons, table, field, dt, tracker=None, threads=None, cl
     return lib().orc_advance_mixed(C.byref(pop.p), C.byref(photons.p), C.byref(table.s), C.byref(field), dt,
                                    C.byref(tracker) if tracker is not None else None, threads or nthreads(),
                                    int(clamp))
+
+
+def photons_repack(photons):
+    return lib().orc_photons_repack(C.byref(photons.p))
 
 
 def photon_advance(photons, pop, dt, tracker=None, threads=None):

@@ -169,3 +169,30 @@ def test_step_diagnostics(ctx):
         assert d["physical_photons"] == pytest.approx(float(gp.w[pa].sum()), rel=1e-13)
     finally:
         fld.close(); ph.close(); pop.close(); tab.close()
+
+
+@pytest.mark.gpu
+def test_photon_repack_matches_oracle(ctx):
+    """repack!(photons): the reference's hole-filling permutation (population.jl:191-215)."""
+    n = 100_003
+    rng = np.random.default_rng(8)
+    d = rng.normal(size=(n, 3))
+    p = jumc.PhotonArrays(rng.normal(size=(n, 3)), d, rng.random(n), rng.random(n), rng.random(n),
+                          (rng.random(n) < 0.6).astype(np.uint8))
+    p.active[-5:] = 0
+    ph = jumc.Photons(n, 9e12, ctx=ctx, photons=p)
+    oph = po.OraclePhotons(n, 9e12, x=p.x, v=p.v, nu=p.nu, w=p.w, s=p.s, active=p.active)
+    try:
+        ph.repack()
+        po.photons_repack(oph)
+        g = ph.download()
+        x, v, nu, w, s, act = oph.arrays()
+        assert len(g.w) == oph.n == int(p.active.sum())
+        np.testing.assert_array_equal(g.x, x)
+        np.testing.assert_array_equal(g.nu, nu)
+        np.testing.assert_array_equal(g.s, s)
+        assert (g.active == 1).all()
+        ph.repack()                       # nothing left to move
+        assert ph.count() == oph.n
+    finally:
+        ph.close()
