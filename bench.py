@@ -1674,6 +1674,243 @@ def run_reference_init(args):
     return 0
 
 
+LOOP_METRIC = "streamer loop steps/s"
+
+
+def loop_config(spec, extra=None):
+    f = spec.fluid
+    p = f.poisson
+    c = {"workload": f"nsteps of the sample input on the sample grid: R={p.R:g} m, L={p.L:g} m, {p.M}x{p.N} cells, "
+                     f"{p.levels} multigrid levels, eb={p.eb:g} V/m; electrons from initfromfiles!("
+                     f"PoissonInitSampling({spec.p})) of a channel of peak {f.peak:g} m^-3, fluid above "
+                     f"{f.threshold:g} m^-3; synthetic gas 0 + photo-emission (photon_multiplier 1000); dt=1e-12 s, "
+                     f"poisson!, resample!(ntarget=10, nmax=15) and the fluid every step; FP32 electrons, FP64 "
+                     f"photons; seed {spec.seed}",
+         "cells": p.M * p.N, "l2": "fields (1.5 GB) and particles exceed L2", "parallelism": "1 GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def loop_build(ctx, spec, precision="fp32"):
+    """The device state of the loop benchmark, initialised from the init workload."""
+    from mcstreamer_b200 import jumc, loop, lxcat, streamer, workloads
+    from mcstreamer_b200.fluid import Fluid
+    from mcstreamer_b200.initdens import PoissonInitSampling, initfromfiles
+    from mcstreamer_b200.poisson import MGConfig, PoissonSolver
+    p = spec.fluid.poisson
+    t = lxcat.synthetic_photo_table(0, photon_multiplier=1000.0, photon_weight=1.0)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.GridCyl(p.R, p.L, p.M, p.N, ctx=ctx)
+    solver = PoissonSolver(grid, MGConfig(levels=p.levels))
+    fl = Fluid(grid)
+    pop = jumc.Population(30_000_000, None, tab, precision=precision, seed=spec.seed)
+    ne, q = workloads.init_densities(spec)
+    initfromfiles(PoissonInitSampling(spec.p), grid, pop, ne=ne, q=q, fluid_threshold=spec.fluid.threshold,
+                  seed=spec.seed)
+    ph = jumc.Photons(8_000_000, t.photon_numax, seed=spec.seed + 1, ctx=ctx)
+    st = loop.Streamer(grid, solver, pop, streamer.FieldInterp(grid), ph, fl)
+    return st, tab, t
+
+
+def loop_close(st, tab):
+    st.efield.close(); st.photons.close(); st.fluid.close(); st.electrons.close(); st.solver.close(); st.grid.close()
+    tab.close()
+
+
+def loop_oracle_step(spec, x, w, s, er, ez, qfixed, qpart, qfd, ne, u):
+    """One nsteps step of the oracle chain over the given state (FP64, all host threads):
+    poisson!, advance! (electrons, photons, tracker), repack!, resample!, setdne!/euler!,
+    repack!.  Returns (seconds, electrons after the step)."""
+    import numpy as np
+
+    from mcstreamer_b200 import lxcat
+    from oracle import fluid_ref as F
+    from oracle import poisson_ref as P
+    from oracle import pyoracle as po
+    p = spec.fluid.poisson
+    t = lxcat.synthetic_photo_table(0, photon_multiplier=1000.0, photon_weight=1.0)
+    n = len(w)
+    opop = po.OraclePop(x, np.zeros((n, 3)), w, s, np.ones(n, np.uint8), cap=3 * n + 1000, seed=spec.seed)
+    oph = po.OraclePhotons(8_000_000, t.photon_numax, seed=spec.seed + 1)
+    otab = po.OracleTable.from_lxcat(t)
+    otrk = po.tracker_cyl(p.R, p.L, p.M, p.N)
+    t0 = time.perf_counter()
+    P.poisson(P.default_conf(p.R, p.L, p.M, p.N, levels=p.levels), qfixed, qpart, u, er, ez, p.eb, p.R, p.L,
+              qfd=qfd, ne=ne)
+    ofield = po.field_cyl(p.R, p.L, p.M, p.N, er.T.ravel(), ez.T.ravel())
+    po.advance_mixed(opop, oph, otab, ofield, 1e-12, otrk, clamp=True)
+    po.photons_repack(oph)
+    po.repack(opop)
+    po.sort_cells(opop, ofield)
+    po.resample_cells(opop, ofield, 10, 15, 0)
+    ne2 = np.asfortranarray(ne.reshape((p.M + 4, p.N + 4), order="F").copy())
+    dne = F.centers(p.M, p.N)
+    F.setdne(ne2, dne, er, ez, p.R, p.L, p.M, p.N)
+    F.euler(ne2, dne, 1e-12, p.M, p.N)
+    po.repack(opop)
+    return time.perf_counter() - t0, opop.n
+
+
+def run_loop(args):
+    import ctypes as C
+    import tempfile
+
+    import torch
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import fieldsio, jumc, loop, workloads
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        # replicas only: one streamer's loop is not sharded
+        import torch.distributed as dist
+        dist.init_process_group("nccl")
+    torch.cuda.set_device(local)
+    ctx = jumc.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    spec = workloads.loop_spec()
+    p = spec.fluid.poisson
+    st, tab, _ = loop_build(ctx, spec)
+    n_init = st.electrons.nparticles()
+    kw = dict(ntarget=10, nmax=15, eb=p.eb, dt=1e-12, dt_poisson=1e-12, dt_output=1e-10, dt_resample=1e-12)
+    loop.nsteps(st, args.warmup, **kw)
+    launches0 = st.solver.launches() + st.fluid.launches()
+    times, electron_steps = [], 0
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        for _ in range(args.steps):
+            n_before = st.electrons.nparticles() + st.photons.count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            d = loop.nsteps(st, 1, **kw)
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            electron_steps += n_before
+        torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    if ws > 1:
+        tt = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms = total_ms / args.steps
+    value = ws * 1e3 / ms
+    last = st.log[-1]
+    launches = (st.solver.launches() + st.fluid.launches() - launches0) // args.steps
+    gs_ms, res_ms, tile_ms = st.solver.profile(5)
+    pk, src = peaks()
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    ach = poisson_alg_bytes_tile(p.M, p.N) / (tile_ms * 1e-3) / 1e9
+    loop_close(st, tab)
+
+    # end to end: host init densities in, K steps with their diagnostics lines, one savefields
+    ne, q = workloads.init_densities(spec)
+    k_e2e = max(1, args.e2e_steps)
+    with tempfile.TemporaryDirectory() as tmp:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, tab, _ = loop_build(ctx, spec)
+        loop.nsteps(st, k_e2e, **kw)
+        fieldsio.savefields(f"{tmp}/fields.h5", st.grid, st.solver, st.fluid)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        loop_close(st, tab)
+    e2e_v = k_e2e / e2e_s
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = loop_cpu_sample(ctx, spec)
+    line = {
+        "metric": LOOP_METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 electrons, f64 fields and photons", "data": "synthetic",
+        "config": loop_config(spec, {"electrons_initial": n_init, "electrons_last": last["active_superelectrons"],
+                                     "photons_last": last["active_superphotons"],
+                                     "particle_steps_per_s": ws * electron_steps / (total_ms * 1e-3)}),
+        "roofline": {"kernel": "k_smooth_tile<2, TILE_POST> (poisson!, the loop's largest fixed cost)",
+                     "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": None, "peak_source": src, "launch_ms": tile_ms,
+                     "alg_bytes_per_launch": poisson_alg_bytes_tile(p.M, p.N)},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_v, "unit": "steps/s", "h2d_bytes_per_step": 16 * p.M * p.N / k_e2e,
+                "d2h_bytes_per_step": 48 * k_e2e + (2 * (p.M + 2) * (p.N + 2) * 8 * 6) / k_e2e,
+                "path": f"initfromfiles! from host densities, {k_e2e} nsteps with their diagnostics lines, one "
+                        "savefields (h5export layout) to disk"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+        "gpu_launches_counts": "per step, poisson! and the fluid only (the advance, resample! and repack! kernels "
+                               "are not counted)",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def loop_cpu_sample(ctx, spec):
+    """One oracle-chain step from the state the device loop starts from."""
+    import numpy as np
+
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200.poisson import read_faces
+    p = spec.fluid.poisson
+    st, tab, _ = loop_build(ctx, spec, precision="fp64")
+    g = st.electrons.download()
+    ne, _, qfd = st.fluid.download()
+    qf = st.grid.read_fixed(L.Q_FIXED)
+    from mcstreamer_b200.streamer import density
+    st.grid.zero(L.Q_PART)
+    density(st.grid, st.electrons, -1.0)
+    qp = st.grid.read_fixed(L.Q_PART)
+    loop_close(st, tab)
+    from oracle import poisson_ref as P
+    u = P.cells(p.M, p.N)
+    er, ez = P.faces(p.M, p.N), P.faces(p.M, p.N)
+    sec, n_after = loop_oracle_step(spec, g.x, g.w, g.s, er, ez, qf, qp, qfd.ravel(order="F"), ne.ravel(order="F"), u)
+    threads = os.cpu_count() or 1
+    return {"value": 1.0 / sec, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"one nsteps step of this workload by the oracle chain on {threads} threads (poisson!, advance!, "
+                      f"repack!, resample!, fluid; {len(g.w)} electrons): {sec:.1f} s"}
+
+
+def run_reference_loop(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    from mcstreamer_b200 import workloads
+    from oracle import initdens_ref as I
+    from oracle import poisson_ref as P
+    spec = workloads.loop_spec()
+    p = spec.fluid.poisson
+    ne, q = workloads.init_densities(spec)
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, p.R, p.L, p.M, p.N, I.POISSON, spec.p,
+                                       fluid_threshold=spec.fluid.threshold, seed=spec.seed, cap=12_000_000)
+    qp = workloads.poisson_electron_charge(p, x, w)
+    u = P.cells(p.M, p.N)
+    er, ez = P.faces(p.M, p.N), P.faces(p.M, p.N)
+    qf = np.zeros_like(qp)
+    sec, n_after = loop_oracle_step(spec, x, w, s, er, ez, qf, qp, qfd.ravel(order="F"), nf.ravel(order="F"), u)
+    v = 1.0 / sec
+    threads = os.cpu_count() or 1
+    line = {
+        "impl": "reference", "metric": LOOP_METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+        "steps": 1, "warmup": 0, "ms_per_step": 1e3 * sec, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": loop_config(spec),
+        "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port",
+                         "sample": f"one nsteps step of the oracle chain ({len(w)} electrons)"},
+        "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -1690,6 +1927,8 @@ def main():
         return run_reference_fluid(args) if args.impl == "reference" else run_fluid(args)
     if args.workload == "init":
         return run_reference_init(args) if args.impl == "reference" else run_init(args)
+    if args.workload == "loop":
+        return run_reference_loop(args) if args.impl == "reference" else run_loop(args)
     if args.workload == "cfg4":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the served workload has no CPU reference arm; "

@@ -88,6 +88,12 @@ class PoissonSolver:
     def zero(self, which: int = L.PSN_U) -> None:
         self.ctx.check(self.ctx.lib.mcs_poisson_zero(self.h, which))
 
+    def launches(self) -> int:
+        """Kernels this workspace has launched so far (graph nodes included)."""
+        n = C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_poisson_launches(self.h, C.byref(n)))
+        return n.value
+
     def profile(self, reps: int = 20) -> Tuple[float, float, float]:
         """ms of one finest-level red-black pass, one finest-level residual and one fused
         finest-level post-smoothing launch (0.0 when unfused)."""

@@ -334,3 +334,12 @@ def init_densities(spec: InitSpec):
     ne = np.asfortranarray(ne)
     q = np.asfortranarray(0.01 * 1.6021766208e-19 * ne)
     return ne, q
+
+
+def loop_spec() -> InitSpec:
+    """The streamer loop's initial state: initfromfiles! over a channel of peak 1e17 m^-3 with
+    the fluid above 5e16 m^-3.  Electron weights max(1, ne dV / p) stay below ~2e3 on the sample
+    grid, so photo-emission (photon_multiplier 1000) makes about one photon per event, as in
+    the photon workload; the 1e21 m^-3 channel of the init workload would weigh electrons at up
+    to 6e6 and emit thousands of photons per event."""
+    return InitSpec(fluid=FluidSpec(peak=1e17, threshold=5e16))
