@@ -27,6 +27,7 @@ import sys
 import tempfile
 import time
 from pathlib import Path
+from typing import Optional
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -170,6 +171,28 @@ class CpuSample:
         return {"value": m / dt, "unit": UNIT, "cores": self.threads, "kind": "port",
                 "sample": f"1 step (advance! + tracker + density!) of the first {m} particles of the same "
                           f"cloud, FP64 oracle, {self.threads} threads, {dt:.2f} s per step"}
+
+
+# Warp instructions per electron step of k_step_mesh<float,256,8,3> on the cfg1 workload,
+# from the ncu capture summarised in profiles/k_step_mesh_cfg1_full.md (780.4 M warp
+# instructions over 4,194,304 electrons).
+MESH_WARP_INST_PER_STEP = {"cfg1": 780.4e6 / 4_194_304}
+
+
+def issue_roofline(workload: str, n_active: float, kernel_ms: float, clocks) -> Optional[dict]:
+    """The bound the step kernel actually meets: warp instructions issued per second against
+    one instruction per cycle on each of the 4 schedulers of every SM at the sampled clock."""
+    per = MESH_WARP_INST_PER_STEP.get(workload)
+    if per is None or not clocks or not clocks.get("sm_mhz"):
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    achieved = per * n_active / (kernel_ms * 1e-3)
+    peak = sms * 4 * clocks["sm_mhz"] * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
+            "frac": achieved / peak, "warp_inst_per_electron_step": per,
+            "source": "instruction count from the ncu capture in profiles/k_step_mesh_cfg1_full.md; peak = SMs x 4 "
+                      "schedulers x sampled SM clock"}
 
 
 def cpu_sample(spec, seconds: float, threads: int) -> dict:
@@ -338,7 +361,8 @@ def run_mine(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
                          "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
-                         "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+                         "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "issue": issue_roofline(args.workload, n_active, kmean, clocks)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
