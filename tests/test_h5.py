@@ -182,3 +182,28 @@ def test_loaders_read_the_reference_layouts(tmp_path):
     np.testing.assert_array_equal(ne3, ne)
     np.testing.assert_array_equal(q3, q)
     assert (dr3, dz3) == (1e-5, 2e-5)
+
+
+def test_edge_values(tmp_path):
+    """Empty datasets, booleans (stored as uint8), integer scalars, a group with no links."""
+    p = tmp_path / "e.h5"
+    with h5.Writer(str(p)) as w:
+        w.write("empty", np.zeros(0))
+        w.write("flags", np.array([True, False, True]))
+        w.write("n", 7)
+        w.write("neg", np.int64(-3))
+        w.create_group("nothing")
+    r = h5.Reader(str(p))
+    assert r["empty"].shape == (0,)
+    np.testing.assert_array_equal(r["flags"], [1, 0, 1])
+    assert r["n"] == 7 and r["neg"] == -3
+    assert r.keys("nothing") == []
+    with pytest.raises(ValueError):
+        with h5.Writer(str(tmp_path / "dup.h5")) as w:
+            w.write("a", 1.0)
+            w.write("a", 2.0)
+    with pytest.raises(ValueError):
+        h5.Reader(str(p)).read("nothing")                # a group is not a dataset
+    (tmp_path / "bad.h5").write_bytes(b"not an hdf5 file at all")
+    with pytest.raises(ValueError):
+        h5.Reader(str(tmp_path / "bad.h5"))

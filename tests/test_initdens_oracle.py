@@ -93,3 +93,18 @@ def test_fluid_cells_and_capacity():
     assert not ((i >= 2) & (i < 4) & (j >= 1) & (j < 3)).any()
     n, *_ = I.initfromfiles(ne, q, R, LEN, M, N, I.NOISELESS, p, fluid_threshold=1e20, seed=1, cap=len(w) - 1)
     assert n == -1
+
+
+def test_empty_and_single_particle_cells():
+    """ne = 0 samples nothing (qfixed = q/e); p = 1 keeps one electron per dense cell."""
+    M, N = 5, 4
+    V = _vol(M, N)
+    x, w, s, qfd, nf = I.initfromfiles(np.zeros((M, N)), np.full((M, N), 2 * E), R, LEN, M, N, I.NOISELESS, 10)
+    assert len(w) == 0
+    np.testing.assert_allclose(qfd[1:M + 1, 1:N + 1], 2.0, rtol=1e-15)
+    x, w, s, qfd, nf = I.initfromfiles(np.zeros((M, N)), np.zeros((M, N)), R, LEN, M, N, I.POISSON, 10)
+    assert len(w) == 0 and (qfd == 0).all()
+    ne = 50.0 / V
+    x, w, s, qfd, nf = I.initfromfiles(ne, 0 * ne, R, LEN, M, N, I.NOISELESS, 1)
+    assert len(w) == M * N
+    np.testing.assert_allclose(w, 50.0, rtol=1e-14)
