@@ -497,7 +497,6 @@ __global__ void k_bempty_moments(BatchDev B) {
     }
 }
 
-__device__ __forceinline__ long long poisson_sample_b(Rng& r, double lam) { return poisson_draw(r, lam); }
 
 __device__ __forceinline__ void bcopy_slot(const BatchDev& B, long long dst, long long src) {
 #pragma unroll
@@ -625,7 +624,7 @@ __global__ void __launch_bounds__(kRBlock) k_bresample(BatchDev B) {
             } else if (sh.mode == MODE_CLONE) {
                 Rng r;
                 r.init(sh.seed, (uint32_t)(l0 + q), sh.step1, TAG_SWARM_RESAMPLE);
-                cnum[q] = (uint32_t)poisson_sample_b(r, sh.lam);
+                cnum[q] = (uint32_t)poisson_draw(r, sh.lam);
                 csum += cnum[q];
             }
             ++alive;

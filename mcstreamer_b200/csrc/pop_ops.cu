@@ -374,34 +374,6 @@ int launch_repack(mcs_pop* p) {
 // ---------------------------------------------------------------------------------------
 // Swarm.resample!(popl, n0, tol): Swarm/src/Swarm.jl:193-223.
 // ---------------------------------------------------------------------------------------
-__device__ long long poisson_sample(Rng& r, double lam) {
-    // Inversion below 10, PTRS (Hoermann 1993) above; same algorithm as the oracle.
-    if (lam <= 0) return 0;
-    if (lam < 10.0) {
-        const double u = r.u64();
-        double pr = exp(-lam), F = pr;
-        long long k = 0;
-        while (u > F && k < 1000) { ++k; pr *= lam / (double)k; F += pr; }
-        return k;
-    }
-    const double slam = sqrt(lam), loglam = log(lam);
-    const double b = 0.931 + 2.53 * slam;
-    const double a = -0.059 + 0.02483 * b;
-    const double invalpha = 1.1239 + 1.1328 / (b - 3.4);
-    const double vr = 0.9277 - 3.6224 / (b - 2.0);
-    for (int it = 0; it < 1000; ++it) {
-        const double U = r.u64() - 0.5;
-        const double V = r.u64();
-        const double us = 0.5 - fabs(U);
-        const double kf = floor((2.0 * a / us + b) * U + lam + 0.43);
-        if (us >= 0.07 && V <= vr) return (long long)kf;
-        if (kf < 0 || (us < 0.013 && V > us)) continue;
-        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + kf * loglam - lgamma(kf + 1.0))
-            return (long long)kf;
-    }
-    return (long long)floor(lam);
-}
-
 __global__ void k_sres_count(uint8_t* __restrict__ act, const long long* n_ptr, const long long* ncur_ptr, long long n0,
                              double tol, unsigned long long seed, uint32_t step, uint32_t* __restrict__ counts) {
     const long long n = *n_ptr, ncur = *ncur_ptr;
@@ -417,7 +389,7 @@ __global__ void k_sres_count(uint8_t* __restrict__ act, const long long* n_ptr, 
             if (drop) {
                 if (r.u64() < pdrop) act[i] = 0;
             } else {
-                c = (uint32_t)poisson_sample(r, lam);
+                c = (uint32_t)poisson_draw(r, lam);
             }
         }
         counts[i] = c;
