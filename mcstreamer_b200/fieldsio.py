@@ -13,11 +13,11 @@ Julia M x N arrays stored as N x M datasets):
 qfixed and qpart are the grid's charge densities (the int64 deposits over dV, qfixed plus its
 FP64 density part), q0 = (qfixed + qpart - ne) e, q the right-hand side poisson! left (the
 Float32 copy plus the free-boundary term), u the potential, er and ez the face fields.  p and
-wtotal are resample!'s per-cell counters; this build keeps them inside its kernel, so they
+wtotal are resample!'s per-cell counters; the resample kernel keeps them to itself, so they
 are written as given, or zero.
 
 `savefields` writes the same file.  The reference's savefields writes a JLD2 container of a
-SavedGridFields (io.jl:56-58); this build writes the fields in h5export's HDF5 layout, which
+SavedGridFields (io.jl:56-58); this module writes the fields in h5export's HDF5 layout, which
 the reference converts JLD2 files into for post-processing (`h5export(from, to)`).
 `load_fields(path)` reads such a file back into a dict of (M, N)-shaped arrays.
 """
