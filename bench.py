@@ -1071,7 +1071,7 @@ def run_poisson(args):
         "config": poisson_config(spec, {"fmg_calls_per_solve": it_set}),
         "roofline": {"kernel": "k_smooth_tile<2, TILE_POST> (interpolation + 2 red-black sweeps, finest level)",
                      "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                     "traffic": None, "peak_source": src, "launch_ms": tile_ms,
+                     "traffic": profiled_traffic("k_smooth_tile_post_sample_grid"), "peak_source": src, "launch_ms": tile_ms,
                      "alg_bytes_per_launch": poisson_alg_bytes_tile(spec.M, spec.N),
                      "unfused_k_gs_launch_ms": gs_ms,
                      "unfused_k_gs_gbs": poisson_alg_bytes_gs(spec.M, spec.N) / (gs_ms * 1e-3) / 1e9,
@@ -1382,6 +1382,12 @@ def fluid_faces(spec):
     return er, ez
 
 
+def profiled_traffic(name: str):
+    """DRAM bytes per launch from a committed ncu summary (profiles/traffic_<name>.json)."""
+    f = ROOT / "profiles" / f"traffic_{name}.json"
+    return json.loads(f.read_text()).get("bytes_per_launch") if f.exists() else None
+
+
 def run_fluid(args):
     import ctypes as C
 
@@ -1476,7 +1482,8 @@ def run_fluid(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": fluid_config(spec, {"fluid_cells": int((ne0 > 0).sum())}),
         "roofline": {"kernel": "k_fluid<true> (setnebc! + setdne! + euler!, one launch)", "bound": "hbm",
-                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": profiled_traffic("k_fluid_sample_grid"),
                      "peak_source": src, "launch_ms": ms, "alg_bytes_per_launch": fluid_alg_bytes(p.M, p.N)},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_v, "unit": "cell-updates/s", "h2d_bytes_per_step": 8 * npad,
@@ -1658,7 +1665,8 @@ def run_init(args):
         "vs_baseline": None, "dtype": "f64 sampling, f32 electrons", "data": "synthetic",
         "config": init_config(spec, {"electrons": n_el, "fluid_cells": int((ne > spec.fluid.threshold).sum())}),
         "roofline": {"kernel": "mcs_init_from_density_device (k_init_count, scan, k_init_place)", "bound": "hbm",
-                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm, "traffic": None,
+                     "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "traffic": profiled_traffic("init_from_density_sample_grid"),
                      "peak_source": src, "launch_ms": ms, "alg_bytes_per_launch": alg},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_v, "unit": "electrons/s", "h2d_bytes_per_step": 16 * p.M * p.N,
@@ -1857,7 +1865,7 @@ def run_loop(args):
                                      "particle_steps_per_s": ws * electron_steps / (total_ms * 1e-3)}),
         "roofline": {"kernel": "k_smooth_tile<2, TILE_POST> (poisson!, the loop's largest fixed cost)",
                      "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                     "traffic": None, "peak_source": src, "launch_ms": tile_ms,
+                     "traffic": profiled_traffic("k_smooth_tile_post_sample_grid"), "peak_source": src, "launch_ms": tile_ms,
                      "alg_bytes_per_launch": poisson_alg_bytes_tile(p.M, p.N)},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_v, "unit": "steps/s", "h2d_bytes_per_step": 16 * p.M * p.N / k_e2e,
