@@ -1530,11 +1530,11 @@ INIT_METRIC = "initfromfiles! electrons/s"
 
 
 def init_alg_bytes(cells: int, electrons: int, esz: int) -> float:
-    """Algorithmic HBM bytes of one initfromfiles!: ne and q read by both passes (32 B per
-    cell), the counts written and read twice (12 B), the bases written and read (16 B),
-    qfixed's density part written (8 B); each electron's x, v, w, s written (8 values of esz
-    bytes) and its active flag (1 B)."""
-    return cells * (32.0 + 12.0 + 16.0 + 8.0) + electrons * (8.0 * esz + 1.0)
+    """Algorithmic HBM bytes of one initfromfiles!: ne and q read once (16 B per cell),
+    qfixed's density part written (8 B per cell), each electron's x, v, w, s written (8 values
+    of esz bytes) and its active flag (1 B).  The two-pass implementation also moves the
+    counts and bases and reads ne and q twice; the ncu traffic shows that excess."""
+    return cells * (16.0 + 8.0) + electrons * (8.0 * esz + 1.0)
 
 
 def init_config(spec, extra=None):
