@@ -400,47 +400,45 @@ __device__ void tile_bc(double* xs, int nr, int nz, int gr0, int gc0, int M, int
     }
 }
 
-// One colour of gauss_seidel! on the cells h or more away from the loaded edge.  Work
-// item (column jj, m) is the colour's cell of that column at local row 2 m + parity; a
-// thread takes Q items at a time and issues all their loads before the arithmetic.
+// One colour of gauss_seidel! on the cells h or more away from the loaded edge.  The
+// colour's cells of every other column lie in one parity plane at the same local rows, so a
+// thread takes one row m across K columns jj0, jj0 + 2, ...: the right neighbour of one cell
+// is the left neighbour of the next, and the row's connector factors are loaded once (lanes
+// take consecutive m, so a warp reads consecutive doubles).  Each cell's arithmetic is the
+// per-operation kernel's, in its order.
 template <class S>
 __device__ void tile_gs(double* xs, const double* bs, const double* ft, int nr, int nz, int gr0, int gc0, int M,
                         int N, int color, int h) {
-    constexpr int LH = S::LH, PL = S::PL, Q = 4;
-    const int n = LH * nz;
-    for (int t0 = threadIdx.x; t0 < n; t0 += Q * kTileThreads) {
-        double c[Q], up[Q], rt[Q], dn[Q], lf[Q], bb[Q], f1[Q], f2[Q];
-        int d[Q];
-        bool on[Q];
+    constexpr int LH = S::LH, PL = S::PL, K = 4;
+    const int runs = (((nz + 1) >> 1) + K - 1) / K;      // runs of K columns per column parity
+    const int n = 2 * runs * LH;
+    for (int t = threadIdx.x; t < n; t += kTileThreads) {
+        const int g = t / LH, m = t - g * LH;
+        const int cls = g & 1, run = g >> 1;
+        const int pp = (color ^ (gc0 + cls)) & 1;         // gr0 is even
+        const int ii = 2 * m + pp, i = gr0 + ii;
+        if (!(ii >= h && ii < nr - h && i >= 1 && i <= M)) continue;
+        const double f1 = ft[pp * LH + m], f2 = ft[2 * LH + pp * LH + m];
+        const int jj0 = cls + 2 * K * run;
+        const int base = pp * PL + m, obase = (1 - pp) * PL + m + pp;   // row ii; row ii + 1
+        double lf = jj0 >= 1 ? xs[base + (jj0 - 1) * LH] : 0.0;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int t = t0 + q * kTileThreads;
-            const int jj = t / LH, m = t - jj * LH;
+        for (int k = 0; k < K; ++k) {
+            const int jj = jj0 + 2 * k;
+            if (jj >= nz) break;
+            const int d = base + jj * LH, o = obase + jj * LH;
+            const double rt = jj + 1 < nz ? xs[d + LH] : 0.0;
             const int j = gc0 + jj;
-            const int par = (color ^ (gr0 + j)) & 1;
-            const int ii = 2 * m + par, i = gr0 + ii;
-            on[q] = t < n && ii >= h && ii < nr - h && jj >= h && jj < nz - h && i >= 1 && i <= M && j >= 1 &&
-                    j <= N;
-            const int mm = on[q] ? m : 1, jc = on[q] ? jj : 1, pp = on[q] ? par : 0;   // a loaded cell when off
-            d[q] = pp * PL + jc * LH + mm;
-            const int o = (1 - pp) * PL + jc * LH + mm + pp;   // row ii + 1 in the other plane
-            c[q] = xs[d[q]];
-            up[q] = xs[o];
-            dn[q] = xs[o - 1];
-            rt[q] = xs[d[q] + LH];
-            lf[q] = xs[d[q] - LH];
-            bb[q] = bs[d[q]];
-            f1[q] = ft[pp * LH + mm];
-            f2[q] = ft[2 * LH + pp * LH + mm];
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            double s = -4.0 * c[q];
-            s += up[q] * f1[q];
-            s += rt[q];
-            s += dn[q] * f2[q];
-            s += lf[q];
-            if (on[q]) xs[d[q]] = c[q] + 1.0 * (s + bb[q]) / 4.0;
+            if (jj >= h && jj < nz - h && j >= 1 && j <= N) {
+                const double c = xs[d], up = xs[o], dn = xs[o - 1], bb = bs[d];
+                double s = -4.0 * c;
+                s += up * f1;
+                s += rt;
+                s += dn * f2;
+                s += lf;
+                xs[d] = c + 1.0 * (s + bb) / 4.0;
+            }
+            lf = rt;
         }
     }
 }
