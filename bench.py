@@ -183,10 +183,13 @@ def issue_roofline(workload: str, n_active: float, kernel_ms: float, clocks) -> 
     """The bound the step kernel actually meets: warp instructions issued per second against
     one instruction per cycle on each of the 4 schedulers of every SM at the sampled clock."""
     per = MESH_WARP_INST_PER_STEP.get(workload)
-    if per is None or not clocks or not clocks.get("sm_mhz"):
+    if per is None or not clocks or not clocks.get("sm_mhz") or not kernel_ms:
         return None
-    import torch
-    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:   # the issue bound is an annotation; never fail the line over it
+        return None
     achieved = per * n_active / (kernel_ms * 1e-3)
     peak = sms * 4 * clocks["sm_mhz"] * 1e6
     return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
