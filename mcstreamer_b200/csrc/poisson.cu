@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kCtaThreads) k_vcycle_cta(MgView V, int l0) { 
 // stride; cp.async gathers the tile into that layout (zero outside the array).  A launch
 // reads xin and writes xout (tiles read each other's halo, so not in place).
 // ---------------------------------------------------------------------------------------
-constexpr int kTileR = 128, kTileZ = 32, kTileThreads = 256, kTileWarps = kTileThreads / 32;
+constexpr int kTileR = 96, kTileZ = 24, kTileThreads = 256, kTileWarps = kTileThreads / 32;
 enum { TILE_PRE = 0, TILE_PRE_SET = 1, TILE_POST = 2 };
 
 struct TileArgs {
@@ -444,7 +444,7 @@ __device__ void tile_gs(double* xs, const double* bs, const double* ft, int nr, 
 }
 
 template <int NS, int MODE>
-__global__ void __launch_bounds__(kTileThreads, 2) k_smooth_tile(TileArgs a) {
+__global__ void __launch_bounds__(kTileThreads, 3) k_smooth_tile(TileArgs a) {
     using S = TileShape<NS>;
     constexpr int H = S::H, LR = S::LR, LH = S::LH, PL = S::PL, CR = S::CR, CZ = S::CZ;
     extern __shared__ __align__(16) double smem[];
