@@ -3,7 +3,6 @@ electron counts, weights and the cells' qfixed densities bit for bit, positions 
 the last place of the device's and the host's cos, sin and log; both samplers, FP64 and FP32
 populations, fluid cells, appending after existing electrons, the capacity error, and the
 HDF5 loader path."""
-import math
 
 import numpy as np
 import pytest

@@ -4,7 +4,6 @@ three regimes, the Poisson sampler's expected counts and charge, the fluid cells
 placed in their own cell at rest, in the serial cell order, with s ~ Exp(1).  No reference
 test exists for initfromfiles!."""
 import numpy as np
-import pytest
 import scipy.stats as ss
 
 from oracle import initdens_ref as I

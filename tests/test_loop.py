@@ -1,6 +1,5 @@
 """nsteps' schedule and call order (MCStreamer/src/main.jl:218-318, timesteps.jl) without a
 GPU: every device call of the loop is replaced by a recorder."""
-import pytest
 
 from mcstreamer_b200 import loop
 

@@ -5,7 +5,6 @@ import numpy as np
 import pytest
 
 from mcstreamer_b200 import _lib as L
-from mcstreamer_b200 import constants as co
 from mcstreamer_b200 import jumc, lxcat, streamer
 from oracle import pyoracle as po
 from tests.helpers import broad, oracle_arrays, oracle_pop, particle_mismatch, vec_relerr

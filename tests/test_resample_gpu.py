@@ -4,7 +4,6 @@ sorted with a stable sort (so both append clones in the same order)."""
 import numpy as np
 import pytest
 
-from mcstreamer_b200 import constants as co
 from mcstreamer_b200 import jumc, lxcat, streamer
 from oracle import pyoracle as po
 from tests.helpers import broad, oracle_arrays, oracle_pop

@@ -1,7 +1,6 @@
 """Serving loop: results are the same alone and in a mix (continuous batching with joins and
 leaves between chunks), memory admission holds requests back until the pool frees, and a
 real-time Poisson run serves everything with latency percentiles."""
-import numpy as np
 import pytest
 
 from mcstreamer_b200 import jumc, lxcat
