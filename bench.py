@@ -1812,19 +1812,28 @@ def run_loop(args):
     kw = dict(ntarget=10, nmax=15, eb=p.eb, dt=1e-12, dt_poisson=1e-12, dt_output=1e-10, dt_resample=1e-12)
     loop.nsteps(st, args.warmup, **kw)
     launches0 = st.solver.launches() + st.fluid.launches()
-    times, electron_steps = [], 0
+    times, electron_steps, phases = [], 0, {}
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         if ws > 1:
             torch.distributed.barrier()
         for _ in range(args.steps):
             n_before = st.electrons.nparticles() + st.photons.count()
+            marks = []
+
+            def mark(name):
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(stream)
+                marks.append((name, ev))
+
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            d = loop.nsteps(st, 1, **kw)
+            loop.nsteps(st, 1, mark=mark, **kw)
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
+            for (name, a), (_, b) in zip(marks, marks[1:]):
+                phases.setdefault(name, []).append(a.elapsed_time(b))
             electron_steps += n_before
         torch.cuda.synchronize()
     total_ms = float(sum(times))
@@ -1865,7 +1874,9 @@ def run_loop(args):
         "vs_baseline": None, "dtype": "f32 electrons, f64 fields and photons", "data": "synthetic",
         "config": loop_config(spec, {"electrons_initial": n_init, "electrons_last": last["active_superelectrons"],
                                      "photons_last": last["active_superphotons"],
-                                     "particle_steps_per_s": ws * electron_steps / (total_ms * 1e-3)}),
+                                     "particle_steps_per_s": ws * electron_steps / (total_ms * 1e-3),
+                                     "phase_ms": {k: statistics.mean(v) for k, v in phases.items()},
+                                     "step_ms_each": times}),
         "roofline": {"kernel": "k_smooth_tile<2, TILE_POST> (poisson!, the loop's largest fixed cost)",
                      "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "traffic": profiled_traffic("k_smooth_tile_post_sample_grid"), "peak_source": src, "launch_ms": tile_ms,

@@ -71,26 +71,36 @@ def poisson_step(s: Streamer, eb: float):
 
 def nsteps(s: Streamer, n: int, ntarget: int, nmax: int, eb: float, dt: float, dt_poisson: float,
            dt_output: float, dt_resample: float, outpath: Optional[str] = None, check_weights: bool = True,
-           on_step: Optional[Callable[[int, dict], None]] = None) -> List[dict]:
-    """Advance the simulation by n steps; returns the per-step diagnostics."""
+           on_step: Optional[Callable[[int, dict], None]] = None,
+           mark: Optional[Callable[[str], None]] = None) -> List[dict]:
+    """Advance the simulation by n steps; returns the per-step diagnostics.  `mark(name)`, if
+    given, is called as each part of a step begins ("poisson", "output", "advance",
+    "diagnostics", "resample", "fluid", "repack") and with "end" after the last, e.g. to
+    record a CUDA event on the context's stream."""
     poisson = TimeStepper(dt_poisson)
     output = TimeStepper(dt_output)
     resampler = TimeStepper(dt_resample, start=dt)
     out: List[dict] = []
+    tick = mark if mark is not None else (lambda name: None)
     for i in range(1, n + 1):
         t = (i - 1) * dt
+        tick("poisson")
         if poisson.atstep(t) is not None:
             poisson_step(s, eb)
+        tick("output")
         j = output.atstep(t)
         if j is not None and outpath:
             os.makedirs(outpath, exist_ok=True)
             fieldsio.savefields(os.path.join(outpath, f"{j:04d}.h5"), s.grid, s.solver, s.fluid)
+        tick("advance")
         if s.photons is not None:
             jumc.advance_mixed(s.electrons, s.photons, s.efield, dt, s.tracker)
         else:
             jumc.advance(s.electrons, s.efield, dt, s.tracker)
+        tick("diagnostics")
         d = diagnostics(s.electrons, s.photons)
         d.update(step=i, t=t)
+        tick("resample")
         if resampler.atstep(t) is not None:
             if s.photons is not None:
                 s.photons.repack()
@@ -106,9 +116,12 @@ def nsteps(s: Streamer, n: int, ntarget: int, nmax: int, eb: float, dt: float, d
                 if not math.isclose(post, post2, rel_tol=1e-5):
                     raise AssertionError("resampling is not conserving the number of particles")
             d["resampled"] = True
+        tick("fluid")
         if s.fluid is not None:
             s.fluid.step(dt)
+        tick("repack")
         jumc.repack(s.electrons)
+        tick("end")
         out.append(d)
         s.log.append(d)
         if on_step is not None:
