@@ -1,0 +1,37 @@
+"""The TOML front end's host parts (MCStreamer/src/main.jl): geteb's units and sampseg's
+seed distribution, without a GPU."""
+import math
+
+import numpy as np
+import pytest
+
+from mcstreamer_b200 import constants as co
+from mcstreamer_b200.run import geteb, sampseg
+
+
+def test_geteb_units():
+    """geteb (main.jl:349-360): -eb times the unit's scale; Td scales with nair."""
+    assert geteb({"eb": 15.0, "field_units": "kV/cm"}) == -1.5e6
+    assert geteb({"eb": 2.0, "field_units": "MV/m"}) == -2e6
+    assert geteb({"eb": 7.0, "field_units": "V/m"}) == -7.0
+    assert geteb({"eb": 100.0}) == -100.0 * (co.Td * co.nair)
+    assert geteb({"eb": 100.0, "nair": 2.5e25}) == -100.0 * (co.Td * 2.5e25)
+    with pytest.raises(KeyError):
+        geteb({"eb": 1.0, "field_units": "furlong"})
+
+
+def test_sampseg_distribution():
+    """sampseg(z0, z1, w) (main.jl:320-341): with probability l / (l + sqrt(2 pi) w) a point
+    of the segment blurred in x, y; else a 3-D Gaussian around the nearer end."""
+    z0, z1, w, n = 1e-3, 1.4e-3, 5e-5, 40_000
+    x = sampseg(z0, z1, w, n, np.random.default_rng(1))
+    p = (z1 - z0) / (z1 - z0 + math.sqrt(2 * math.pi) * w)
+    inside = (x[:, 2] >= z0) & (x[:, 2] <= z1)
+    # points on the segment, plus the end caps' half-Gaussians that fall back onto it: none
+    # (the cap draws put z beyond the end they belong to)
+    assert abs(inside.mean() - p) < 5 * math.sqrt(p * (1 - p) / n)
+    assert abs(x[:, 0].std() - w) < 0.02 * w and abs(x[:, 1].std() - w) < 0.02 * w
+    below = x[:, 2] < z0
+    assert abs(below.mean() - (1 - p) / 2) < 5 * math.sqrt(0.25 / n)
+    with pytest.raises(ValueError):
+        sampseg(1.0, 0.5, w, 1, np.random.default_rng(0))
