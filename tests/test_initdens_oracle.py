@@ -3,7 +3,10 @@ the reference's code defines (MCStreamer/src/initdens.jl:64-159): the noiseless 
 three regimes, the Poisson sampler's expected counts and charge, the fluid cells, electrons
 placed in their own cell at rest, in the serial cell order, with s ~ Exp(1).  No reference
 test exists for initfromfiles!."""
+import math
+
 import numpy as np
+import pytest
 import scipy.stats as ss
 
 from oracle import initdens_ref as I
@@ -107,3 +110,114 @@ def test_empty_and_single_particle_cells():
     x, w, s, qfd, nf = I.initfromfiles(ne, 0 * ne, R, LEN, M, N, I.NOISELESS, 1)
     assert len(w) == M * N
     np.testing.assert_allclose(w, 50.0, rtol=1e-14)
+
+
+def _py_initfromfiles(ne, q, M, N, method, p, thr, seed):
+    """initfromfiles! restated in plain Python from the reference's statements (the draws
+    taken word by word from the same Philox streams, the Poisson sampler written out
+    again), for a small grid."""
+    from oracle import pyoracle as po
+    dr, dz = R / M, LEN / N
+
+    class Stream:
+        def __init__(self, c0, c1, tag):
+            self.c0, self.c1, self.tag, self.k = c0, c1, tag, 0
+
+        def next(self):
+            u = po.uniform(seed, self.c0, self.c1, self.tag, self.k)
+            self.k += 1
+            return u
+
+    def poisson(rng, lam):
+        if lam <= 0:
+            return 0
+        if lam < 10.0:
+            u = rng.next()
+            pr = math.exp(-lam)
+            F = pr
+            k = 0
+            while u > F and k < 1000:
+                k += 1
+                pr *= lam / k
+                F += pr
+            return k
+        slam, loglam = math.sqrt(lam), math.log(lam)
+        b = 0.931 + 2.53 * slam
+        a = -0.059 + 0.02483 * b
+        invalpha = 1.1239 + 1.1328 / (b - 3.4)
+        vr = 0.9277 - 3.6224 / (b - 2.0)
+        for _ in range(1000):
+            U = rng.next() - 0.5
+            V = rng.next()
+            us = 0.5 - abs(U)
+            kf = math.floor((2.0 * a / us + b) * U + lam + 0.43)
+            if us >= 0.07 and V <= vr:
+                return kf
+            if kf < 0 or (us < 0.013 and V > us):
+                continue
+            if math.log(V) + math.log(invalpha) - math.log(a / (us * us) + b) <= -lam + kf * loglam - math.lgamma(kf + 1.0):
+                return kf
+        return math.floor(lam)
+
+    xs, ws, ss = [], [], []
+    qfd = np.zeros((M + 2, N + 2))
+    nf = np.zeros((M + 4, N + 4))
+    for j in range(1, N + 1):
+        for i in range(1, M + 1):
+            c = (i - 1) + (j - 1) * M
+            V = 2.0 * math.pi * (((i - 1) + 0.5) * dr) * dr * dz
+            nec, qc = ne[i - 1, j - 1], q[i - 1, j - 1]
+            if nec > thr:
+                nf[i + 1, j + 1] = nec
+                qfd[i, j] = qc / E + nec
+                continue
+            rng = Stream(c, 0, 6)
+            if method == I.NOISELESS:
+                n = nec * V
+                if n < 1:
+                    nume, w = poisson(rng, n), 1.0
+                elif n < p:
+                    m = math.floor(n)
+                    nume, w = (int(m) if rng.next() > n - m else int(m) + 1), 1.0
+                else:
+                    nume, w = p, n / p
+                qf = qc / E + w * nume / V
+            else:
+                w = max(1.0, nec * V / p)
+                nume = poisson(rng, nec * V / w)
+                ni = nec + qc / E
+                wi = max(1.0, abs(ni) * V / p)
+                numi = poisson(rng, abs(ni) * V / wi)
+                qf = math.copysign(1.0, ni) * numi * wi / V if ni != 0 else 0.0 * numi * wi / V
+            qfd[i, j] = qf
+            for k in range(nume):
+                u = [po.uniform(seed, c, k, 6 | 0x40000000, t) for t in range(4)]
+                r = dr * u[0] + (i - 1) * dr
+                z = dz * u[1] + (j - 1) * dz
+                phi = 2.0 * math.pi * u[2]
+                xs.append((r * math.cos(phi), r * math.sin(phi), z))
+                ws.append(w)
+                ss.append(-math.log(u[3]))
+    return np.array(xs).reshape(-1, 3), np.array(ws), np.array(ss), qfd, nf
+
+
+@pytest.mark.parametrize("method", [I.NOISELESS, I.POISSON])
+def test_oracle_agrees_with_a_python_restatement(method):
+    """The C++ loop and a plain-Python restatement written apart agree bit for bit: counts,
+    weights, positions, s, qfixed and the fluid cells, over all sampler branches."""
+    M, N, p = 6, 8, 10
+    V = _vol(M, N)
+    rng = np.random.default_rng(4)
+    n = 10 ** rng.uniform(-2, 2.5, (M, N))            # Poisson(n < 1), randround, p electrons
+    n[0, 0] = 0.0
+    ne = np.asfortranarray(n / V)
+    ne[5, 7] = 3e21                                    # one fluid cell
+    q = np.asfortranarray(E * ne * rng.uniform(-1.5, 1.5, (M, N)))
+    x, w, s, qfd, nf = I.initfromfiles(ne, q, R, LEN, M, N, method, p, fluid_threshold=1e21, seed=9)
+    x2, w2, s2, qfd2, nf2 = _py_initfromfiles(ne, q, M, N, method, p, 1e21, 9)
+    assert len(w) == len(w2) > 50
+    np.testing.assert_array_equal(w, w2)
+    np.testing.assert_array_equal(x, x2)
+    np.testing.assert_array_equal(s, s2)
+    np.testing.assert_array_equal(qfd, qfd2)
+    np.testing.assert_array_equal(nf, nf2)
