@@ -122,7 +122,14 @@ def main(finput: str, tmax: Optional[float] = None, run: bool = True, precision:
     grid = streamer.GridCyl(R, Lz, M, N, ctx=ctx)
     solver = PoissonSolver(grid, MGConfig(levels=int(inp.get("poisson_levels", 9))))
     cap = int(capacity) if capacity is not None else maxp
-    electrons = jumc.Population(cap, None, tab, precision=precision, seed=seed)
+    try:
+        electrons = jumc.Population(cap, None, tab, precision=precision, seed=seed)
+    except L.MCSError as e:
+        solver.close(); grid.close(); tab.close()
+        if e.code != L.ERR_NOMEM:
+            raise
+        raise L.MCSError(e.code, f"{cap} electrons do not fit on the device (maxp = {maxp} sizes the "
+                                 f"reference's host arrays); pass capacity= and photon_capacity=") from e
     fluid = None
     if "init_files" in inp:
         init = inp["init_files"]
