@@ -94,33 +94,54 @@ class Run:
         self.table.close()
 
 
+def read_input(finput: str, tmax: Optional[float] = None) -> dict:
+    """The settings main takes from the input file, resolved as main.jl does: the parsed
+    TOML under "input", with the cross-section and init-file paths made relative to the
+    input's folder, the background field eb (V/m), the number of steps fld(tmax, dt), the
+    Poisson levels and the output path."""
+    with open(finput, "rb") as f:
+        inp = tomllib.load(f)
+    here = os.path.dirname(os.path.abspath(finput))
+    dt = float(inp["dt"])
+    tmax = float(inp["tmax"]) if tmax is None else float(tmax)
+    out = {"input": inp, "here": here, "dt": dt, "tmax": tmax, "steps": int(tmax // dt),   # fld(tmax, dt)
+           "eb": geteb(inp), "seed": int(inp.get("rng_seed", 0)), "nair": float(inp.get("nair", co.nair)),
+           "poisson_levels": int(inp.get("poisson_levels", 9)),
+           "cross_sections": [os.path.join(here, f) for f in inp["cross_sections"]],
+           "outpath": os.path.splitext(os.path.abspath(finput))[0]}
+    if "init_files" in inp:
+        init = inp["init_files"]
+        out["init_files"] = {"ne_file": os.path.join(here, init["ne_file"]),
+                             "q_file": os.path.join(here, init["q_file"]),
+                             "method": init.get("method", "noiseless"), "format": init.get("format", "am"),
+                             "fluid_threshold": float(init.get("fluid_threshold", math.inf))}
+    return out
+
+
 def main(finput: str, tmax: Optional[float] = None, run: bool = True, precision: str = "fp32",
          capacity: Optional[int] = None, photon_capacity: Optional[int] = None,
          ctx: Optional[jumc.Context] = None) -> Run:
     """MCStreamer.main(finput; tmax, run) on the device."""
-    with open(finput, "rb") as f:
-        inp = tomllib.load(f)
-    here = os.path.dirname(os.path.abspath(finput))
+    cfg = read_input(finput, tmax)
+    inp = cfg["input"]
+    here = cfg["here"]
     ctx = ctx or jumc.Context.default()
-    seed = int(inp.get("rng_seed", 0))
-    nair = float(inp.get("nair", co.nair))
+    seed, nair = cfg["seed"], cfg["nair"]
     dom = inp["domain"]
     R, Lz, M, N = float(dom["R"]), float(dom["L"]), int(dom["M"]), int(dom["N"])
     nmax, ntarget, maxp, n = int(inp["nmax"]), int(inp["ntarget"]), int(float(inp["maxp"])), int(inp["n"])
     pi = inp.get("photoionization", {})
-    table = lxcat.load_lxcat([os.path.join(here, f) for f in inp["cross_sections"]],
+    table = lxcat.load_lxcat(cfg["cross_sections"],
                              {"N2": nair * 0.79, "O2": nair * 0.21}, lxcat.DEFAULT_ENERGY,
                              photon_weight=float(pi.get("photon_weight", 1.0)),
                              photon_multiplier=float(pi.get("photon_multiplier", 1.0)))
     tab = jumc.CollisionTable(table, ctx)
-    dt = float(inp["dt"])
-    tmax = float(inp["tmax"]) if tmax is None else float(tmax)
-    eb = geteb(inp)
+    dt, eb = cfg["dt"], cfg["eb"]
     if "denoise" in inp:
         warnings.warn("the [denoise] model is not supported; poisson! runs with the NullDenoiser")
 
     grid = streamer.GridCyl(R, Lz, M, N, ctx=ctx)
-    solver = PoissonSolver(grid, MGConfig(levels=int(inp.get("poisson_levels", 9))))
+    solver = PoissonSolver(grid, MGConfig(levels=cfg["poisson_levels"]))
     cap = int(capacity) if capacity is not None else maxp
     try:
         electrons = jumc.Population(cap, None, tab, precision=precision, seed=seed)
@@ -131,13 +152,11 @@ def main(finput: str, tmax: Optional[float] = None, run: bool = True, precision:
         raise L.MCSError(e.code, f"{cap} electrons do not fit on the device (maxp = {maxp} sizes the "
                                  f"reference's host arrays); pass capacity= and photon_capacity=") from e
     fluid = None
-    if "init_files" in inp:
-        init = inp["init_files"]
-        method = {"poisson": PoissonInitSampling, "noiseless": NoiselessInitSampling}[
-            init.get("method", "noiseless")](ntarget)
-        loader = {"am": AMLoader, "afivo": AfivoLoader}[init.get("format", "am")](
-            os.path.join(here, init["ne_file"]), os.path.join(here, init["q_file"]))
-        threshold = float(init.get("fluid_threshold", math.inf))
+    if "init_files" in cfg:
+        init = cfg["init_files"]
+        method = {"poisson": PoissonInitSampling, "noiseless": NoiselessInitSampling}[init["method"]](ntarget)
+        loader = {"am": AMLoader, "afivo": AfivoLoader}[init["format"]](init["ne_file"], init["q_file"])
+        threshold = init["fluid_threshold"]
         if math.isfinite(threshold):
             fluid = Fluid(grid)
         initfromfiles(method, grid, electrons, loader, fluid_threshold=threshold, seed=seed)
@@ -164,9 +183,9 @@ def main(finput: str, tmax: Optional[float] = None, run: bool = True, precision:
         photons = jumc.Photons(int(photon_capacity) if photon_capacity is not None else maxp, table.photon_numax,
                                seed=seed + 1, ctx=ctx)
     s = loop.Streamer(grid, solver, electrons, streamer.FieldInterp(grid), photons, fluid)
-    outpath = os.path.splitext(os.path.abspath(finput))[0]
+    outpath = cfg["outpath"]
     iv = inp["interval"]
-    steps = int(math.floor(tmax / dt))
+    steps = cfg["steps"]
     diags: List[dict] = []
     if run:
         diags = loop.nsteps(s, steps, ntarget, nmax, eb, dt, float(iv["poisson"]), float(iv["output"]),

@@ -35,3 +35,32 @@ def test_sampseg_distribution():
     assert abs(below.mean() - (1 - p) / 2) < 5 * math.sqrt(0.25 / n)
     with pytest.raises(ValueError):
         sampseg(1.0, 0.5, w, 1, np.random.default_rng(0))
+
+
+def test_read_input_resolves_like_main(tmp_path):
+    """Paths relative to the input's folder, fld(tmax, dt) steps, the default Poisson levels
+    and nair, the init-file settings with their defaults, the output path."""
+    from mcstreamer_b200.run import read_input
+
+    d = tmp_path / "case"
+    d.mkdir()
+    (d / "input.toml").write_text("""
+eb = 100.0
+dt = 1e-12
+tmax = 1.05e-10
+rng_seed = 7
+cross_sections = ["../cs/a.json", "b.json"]
+[init_files]
+ne_file = "afivo/ne.hdf"
+q_file = "afivo/q.hdf"
+format = "afivo"
+""")
+    c = read_input(str(d / "input.toml"))
+    assert c["cross_sections"] == [str(d / "../cs/a.json"), str(d / "b.json")]
+    assert c["steps"] == 105 and c["seed"] == 7 and c["poisson_levels"] == 9
+    assert c["eb"] == -100.0 * (co.Td * co.nair)
+    init = c["init_files"]
+    assert init["ne_file"] == str(d / "afivo/ne.hdf") and init["method"] == "noiseless"
+    assert init["format"] == "afivo" and math.isinf(init["fluid_threshold"])
+    assert c["outpath"] == str(d / "input")
+    assert read_input(str(d / "input.toml"), tmax=3e-12)["steps"] == 3
