@@ -1,5 +1,6 @@
 """nsteps' schedule and call order (MCStreamer/src/main.jl:218-318, timesteps.jl) without a
 GPU: every device call of the loop is replaced by a recorder."""
+import pytest
 
 from mcstreamer_b200 import loop
 
@@ -60,3 +61,31 @@ def test_nsteps_call_order(monkeypatch, tmp_path):
     assert rec.calls == want
     assert [d["step"] for d in out] == [1, 2, 3, 4, 5]
     assert [bool(d.get("resampled")) for d in out] == [True, False, False, True, False]
+
+
+def test_nsteps_without_photons_or_fluid(monkeypatch):
+    """Electrons only: advance! instead of the mixed advance, no photon repack!, no fluid;
+    a weight change across resample! fails as the reference's assertion does."""
+    rec = _Rec()
+    monkeypatch.setattr(loop, "density", rec("density"))
+    monkeypatch.setattr(loop, "diagnostics", lambda e, p: {})
+    monkeypatch.setattr(loop, "resample", rec("resample"))
+    monkeypatch.setattr(loop.jumc, "advance", rec("advance"))
+    monkeypatch.setattr(loop.jumc, "advance_mixed", rec("mixed"))
+    monkeypatch.setattr(loop.jumc, "repack", rec("repack"))
+    s = loop.Streamer(grid=_Obj(rec, "grid"), solver=_Obj(rec, "solver"), electrons=_Pop(rec), efield=None,
+                      tracker=object())
+    loop.nsteps(s, 2, 10, 15, -1.5e6, 1.0, 1.0, 10.0, 1.0)
+    assert rec.calls == ["grid.zero", "density", "solver.run", "advance", "repack", "resample", "repack"] * 2
+
+    class Shrinking(_Pop):
+        def __init__(self, rec):
+            super().__init__(rec)
+            self.w = [1.0, 0.5]
+
+        def weight(self):
+            return self.w.pop(0) if len(self.w) > 1 else self.w[0]
+
+    s.electrons = Shrinking(rec)
+    with pytest.raises(AssertionError, match="repackaging"):
+        loop.nsteps(s, 1, 10, 15, -1.5e6, 1.0, 1.0, 10.0, 1.0)
