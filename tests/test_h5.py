@@ -207,3 +207,30 @@ def test_edge_values(tmp_path):
     (tmp_path / "bad.h5").write_bytes(b"not an hdf5 file at all")
     with pytest.raises(ValueError):
         h5.Reader(str(tmp_path / "bad.h5"))
+
+
+def test_reads_a_header_continued_in_another_block(tmp_path):
+    """A version-1 object header whose dataset messages sit in a continuation block
+    (message 0x10: address and length of the next block), as libraries write when a
+    header outgrows its first chunk."""
+    p = tmp_path / "c.h5"
+    with h5.Writer(str(p)) as w:
+        w.write("d", np.arange(5.0))
+    b = bytearray(p.read_bytes())
+    # find the dataset's header: the symbol-table node's only entry
+    btree = struct.unpack_from("<Q", b, 80)[0]
+    snod = struct.unpack_from("<Q", b, btree + 32)[0]
+    hdr = struct.unpack_from("<Q", b, snod + 8 + 8)[0]
+    nmsg, _, size = struct.unpack_from("<HII", b, hdr + 2)
+    msgs = bytes(b[hdr + 16:hdr + 16 + size])
+    # move every message to a block at the end of the file and leave a continuation behind
+    cont_addr = len(b)
+    b += msgs
+    cont = struct.pack("<HHB3x", 0x10, 16, 0) + struct.pack("<QQ", cont_addr, len(msgs))
+    b[hdr + 16:hdr + 16 + len(cont)] = cont
+    b[hdr + 16 + len(cont):hdr + 16 + size] = b"\0" * (size - len(cont))   # a NIL message's worth
+    struct.pack_into("<H", b, hdr + 2, nmsg + 1)
+    struct.pack_into("<I", b, hdr + 8, len(cont))
+    struct.pack_into("<Q", b, 40, len(b))          # end-of-file address
+    p.write_bytes(bytes(b))
+    np.testing.assert_array_equal(h5.Reader(str(p))["d"], np.arange(5.0))

@@ -144,3 +144,35 @@ def test_loader_reads_photoemission_records():
     hi = e > 200 * co.eV
     np.testing.assert_allclose(t.rate[j][hi], lxcat.SYNTHETIC_DENSITY * v[hi] * 2.5e-20 * 2e-3 * 500.0, rtol=1e-12)
     assert t.photon_multiplier == 500.0 and t.photon_weight == 3.0
+
+
+def test_photon_repack_is_the_reference_permutation():
+    """repack!(photons) (population.jl:191-215): the k-th hole from the start takes the
+    k-th active photon from the end, until they meet; checked against that loop written
+    again here."""
+    n = 257
+    rng = np.random.default_rng(6)
+    x, v, nu, w, s, act = _photons(n, 1e12, seed=6)
+    act = (rng.random(n) < 0.55).astype(np.uint8)
+    act[-3:] = 0
+    ph = po.OraclePhotons(n, 9e12, x=x, v=v, nu=nu, w=w, s=s, active=act)
+    po.photons_repack(ph)
+    idx = list(range(n))
+    a = act.astype(bool).tolist()
+    last = n - 1
+    while not a[last]:
+        last -= 1
+    i = 0
+    while i <= last:
+        if not a[i]:
+            idx[i], a[i] = idx[last], True
+            last -= 1
+            while not a[last]:
+                last -= 1
+        i += 1
+    idx = idx[:last + 1]
+    assert ph.n == len(idx) == int(act.sum())
+    xp, vp, nup, wp, sp, ap = ph.arrays()
+    np.testing.assert_array_equal(xp, x[idx])
+    np.testing.assert_array_equal(nup, nu[idx])
+    assert (ap == 1).all()
