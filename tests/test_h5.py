@@ -234,3 +234,51 @@ def test_reads_a_header_continued_in_another_block(tmp_path):
     struct.pack_into("<Q", b, 40, len(b))          # end-of-file address
     p.write_bytes(bytes(b))
     np.testing.assert_array_equal(h5.Reader(str(p))["d"], np.arange(5.0))
+
+
+def test_h5export_layout_and_fields(tmp_path, monkeypatch):
+    """h5export (plot.jl:210-238) from stand-ins of the device objects: the grid scalars and
+    coordinates, each array's slice (cells [1:M, 1:N], er [1:M+1, 1:N], ez [1:M, 1:N+1]) and
+    q0 = (qfixed + qpart - ne) e, read back with the Julia shapes."""
+    from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import constants as co
+    from mcstreamer_b200 import fieldsio
+
+    M, N = 4, 6
+    rng = np.random.default_rng(7)
+    dens = {L.Q_FIXED: rng.random((M + 2, N + 2)), L.Q_PART: -rng.random((M + 2, N + 2))}
+    qfd = rng.random((M + 2, N + 2))
+    ne = rng.random((M + 4, N + 4))
+    er, ez = rng.random((M + 3, N + 3)), rng.random((M + 3, N + 3))
+
+    class Grid:
+        R, L, M, N = 1e-3, 2e-3, 4, 6
+        read_density = staticmethod(lambda which: dens[which])
+        read_qfixed_density = staticmethod(lambda: qfd)
+
+    class Solver:
+        q = rng.random((M + 2, N + 2))
+        u = rng.random((M + 2, N + 2))
+
+    class Fl:
+        download = staticmethod(lambda: (ne, None, None))
+
+    monkeypatch.setattr(fieldsio, "read_faces", lambda g: (er, ez))
+    p = tmp_path / "f.h5"
+    fieldsio.h5export(str(p), Grid, Solver, Fl, p=np.arange(M * N).reshape(M, N))
+    f = fieldsio.load_fields(str(p))
+    g = f["grid"]
+    assert (g["R"], g["L"], g["M"], g["N"]) == (1e-3, 2e-3, M, N)
+    np.testing.assert_allclose(g["rc"], (np.arange(M) + 0.5) * 1e-3 / M, rtol=1e-15)
+    assert g["zf"].shape == (N + 1,)
+    qf = dens[L.Q_FIXED] + qfd
+    np.testing.assert_array_equal(f["qfixed"], qf[1:M + 1, 1:N + 1])
+    np.testing.assert_array_equal(f["q0"], ((qf + dens[L.Q_PART])[1:M + 1, 1:N + 1] - ne[2:M + 2, 2:N + 2])
+                                  * co.elementary_charge)
+    np.testing.assert_array_equal(f["u"], Solver.u[1:M + 1, 1:N + 1])
+    np.testing.assert_array_equal(f["er"], er[1:M + 2, 1:N + 1])
+    np.testing.assert_array_equal(f["ez"], ez[1:M + 1, 1:N + 2])
+    np.testing.assert_array_equal(f["p"], np.arange(M * N).reshape(M, N))
+    assert (f["wtotal"] == 0).all() and f["p"].dtype == np.int64
+    r = h5.Reader(str(p))
+    assert r.read("er", julia=False).shape == (N, M + 1)        # HDF5.jl's dataset dims
