@@ -64,3 +64,28 @@ format = "afivo"
     assert init["format"] == "afivo" and math.isinf(init["fluid_threshold"])
     assert c["outpath"] == str(d / "input")
     assert read_input(str(d / "input.toml"), tmax=3e-12)["steps"] == 3
+
+
+def test_sampseg_point_seed():
+    """z1 = z0 (the default when [seed] has no z1): a 3-D Gaussian of width w at z0."""
+    x = sampseg(1e-3, 1e-3, 2e-5, 20_000, np.random.default_rng(2))
+    assert abs(x[:, 2].mean() - 1e-3) < 5 * 2e-5 / math.sqrt(20_000)
+    np.testing.assert_allclose(x.std(axis=0), 2e-5, rtol=0.03)
+
+
+def test_cross_sections_take_the_air_densities(tmp_path):
+    """main.jl:46-47: N2 at 0.79 and O2 at 0.21 of nair; a record's rate scales with its
+    target's density (load_lxcat, lxcat.jl:17-134)."""
+    import json
+
+    from mcstreamer_b200 import lxcat
+    recs = lxcat.synthetic_records(0, target="N2")
+    f = tmp_path / "cs.json"
+    f.write_text(json.dumps(recs))
+    nair = 2.5e25
+    a = lxcat.load_lxcat([f], {"N2": nair * 0.79, "O2": nair * 0.21})
+    recs_o2 = lxcat.synthetic_records(0, target="O2")
+    f2 = tmp_path / "cs2.json"
+    f2.write_text(json.dumps(recs_o2))
+    b = lxcat.load_lxcat([f2], {"N2": nair * 0.79, "O2": nair * 0.21})
+    assert a.maxrate / b.maxrate == pytest.approx(0.79 / 0.21, rel=1e-12)
