@@ -282,6 +282,9 @@ MCS_API int mcs_grid_create_cyl(mcs_ctx* c, double R, double L, int M, int N, mc
     v.R = R; v.L = L; v.M = M; v.N = N;
     v.dr = R / M;
     v.dz = L / N;
+    double zc0, zc1;
+    centre_range(R, M, &v.rc0, &v.rc1, &v.drc);
+    centre_range(L, N, &zc0, &zc1, &v.dzc);
     const size_t faces = (size_t)(M + 3) * (N + 3), cells = (size_t)(M + 2) * (N + 2);
     g->nq = cells;
     int st = dalloc(c, &g->d_er, faces);
@@ -300,8 +303,8 @@ MCS_API int mcs_grid_create_cyl(mcs_ctx* c, double R, double L, int M, int N, mc
     v.ez32 = g->d_erz32 + faces;
     v.R32 = (float)R;
     v.L32 = (float)L;
-    v.inv_dr32 = (float)(1.0 / v.dr);
-    v.inv_dz32 = (float)(1.0 / v.dz);
+    v.inv_dr32 = (float)(1.0 / v.drc);
+    v.inv_dz32 = (float)(1.0 / v.dzc);
     cudaMemset(g->d_q[0], 0, cells * sizeof(long long));
     cudaMemset(g->d_q[1], 0, cells * sizeof(long long));
     v.er = g->d_er;
@@ -447,8 +450,8 @@ MCS_API int mcs_grid_read_density(mcs_grid* g, int which, double* out) {
             for (int i = 0; i < M + 2; ++i) {
                 const size_t k = (size_t)i + (size_t)j * (M + 2);
                 if (i < 1 || i > M) { out[k] = 0.0; continue; }
-                const double rc = ((double)(i - 1) + 0.5) * g->v.dr;  // grid.rc[i]
-                const double dV = 2.0 * M_PI * rc * g->v.dr * g->v.dz;  // grid.jl:76
+                const double rc = lerpi(i - 1, M > 1 ? M - 1 : 1, g->v.rc0, g->v.rc1);  // grid.rc[i]
+                const double dV = 2.0 * M_PI * rc * g->v.drc * g->v.dzc;                 // grid.jl:76
                 out[k] = (double)q[k] * 0x1p-32 / dV;
             }
     }

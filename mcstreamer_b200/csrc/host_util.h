@@ -38,6 +38,25 @@ inline PopView<T> pop_view(mcs_pop* p) {
     return v;
 }
 
+// Julia's LinRange arithmetic, which MCStreamer's Grid relies on (grid.jl:33-41): getindex
+// r[j+1] = lerpi(j, lendiv, start, stop) = (1 - j/lendiv) start + (j/lendiv) stop, and
+// step(r) = (stop - start) / lendiv with lendiv = max(1, len - 1).
+inline double lerpi(long long j, long long d, double a, double b) {
+    const double t = (double)j / (double)d;
+    return (1.0 - t) * a + t * b;
+}
+
+// The cell-centre range of one axis: faces f = LinRange(0, len, m + 1) and
+// c = 0.5 * (f[2:end] + f[1:end-1]), a LinRange from 0.5 (f[2] + f[1]) to 0.5 (f[m+1] + f[m])
+// of m points.  Returns its first and last point and step(c) (dr(grid) / dz(grid)).
+inline void centre_range(double len, int m, double* first, double* last, double* step) {
+    const double f1 = lerpi(0, m, 0.0, len), f2 = lerpi(1, m, 0.0, len);
+    const double fm = lerpi(m - 1, m, 0.0, len), fm1 = lerpi(m, m, 0.0, len);
+    *first = 0.5 * (f2 + f1);
+    *last = 0.5 * (fm1 + fm);
+    *step = (*last - *first) / (double)(m > 1 ? m - 1 : 1);
+}
+
 // Same arithmetic as the oracle's Yoshida constants (JuMC/src/electron.jl:38-46).
 struct YoshidaHost {
     double c1, c2, c3, c4, d1, d2, d3;

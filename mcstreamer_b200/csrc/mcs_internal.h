@@ -81,7 +81,9 @@ struct GridView {
     double h, inv_h, x0, y0, z0;
     const float* e32;       // cart3d node field, 4 floats per node (Ex,Ey,Ez,0)
     const double* e64;      // cart3d node field, 3 doubles per node
-    double R, L, dr, dz;    // cyl
+    double R, L, dr, dz;    // cyl: R / M, L / N (step(grid.rf), step(grid.zf): cellindex)
+    double drc, dzc;        // cyl: step(grid.rc), step(grid.zc) in Julia's LinRange arithmetic (FieldInterp, dV)
+    double rc0, rc1;        // cyl: first and last cell centre of grid.rc (rc[i] by lerpi, for dV)
     int M, N;
     const double* er; const double* ez;  // cyl faces (M+3)x(N+3)
     const float* er32; const float* ez32;  // their FP32 copies (the FP32 push gathers these)

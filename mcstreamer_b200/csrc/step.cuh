@@ -391,11 +391,11 @@ struct FieldCyl {
         const double r0 = sqrt(x * x + y * y);
         if (!((0.0 < r0 && r0 < g.R) && (0.0 < z && z < g.L))) return;
         double r = r0;
-        if (r == 0.0) r = g.dr / 10.0;
-        const double qr = r / g.dr;
+        if (r == 0.0) r = g.drc / 10.0;
+        const double qr = r / g.drc;              // normdivrem(r - first(rf), dr(grid))
         long long i = (long long)trunc(qr);
         const double dr_ = qr - (double)i;
-        const double qz = z / g.dz;
+        const double qz = z / g.dzc;
         long long j = (long long)trunc(qz);
         const double dz_ = qz - (double)j;
         long long i1, j1;
@@ -416,9 +416,9 @@ struct FieldCyl {
     }
 
     // The FP32 push's gather: the same cells and weights in single precision from the FP32
-    // face copies, reciprocal cell sizes, and |E|^2 > 1e16 for the field check.  Indices stay
-    // inside the (M+3) x (N+3) faces: a rounded-up r / dr or z / dz of M or N reads face M+2 or
-    // N+2 at most.
+    // face copies, reciprocal cell sizes (of step(grid.rc), step(grid.zc)), and
+    // |E|^2 > 1e16 for the field check.  Indices stay inside the (M+3) x (N+3) faces: a
+    // rounded-up r / dr or z / dz of M or N reads face M+2 or N+2 at most.
     __device__ __forceinline__ void gather32(const GridView& g, float x, float y, float z, float& e0, float& e1,
                                              float& e2, uint32_t* status) const {
         e0 = e1 = e2 = 0.0f;

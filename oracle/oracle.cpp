@@ -157,6 +157,29 @@ inline double julia_fld(double x, double y) {
     return std::nearbyint((x - m) / y);
 }
 
+/* Base range.jl lerpi(j, d, a, b) = (1 - j/d) a + (j/d) b: LinRange getindex r[j+1]. */
+inline double lerpi(int64_t j, int64_t d, double a, double b) {
+    const double t = (double)j / (double)d;
+    return (1.0 - t) * a + t * b;
+}
+
+/* Grid's cell-centre range of one axis (MCStreamer/src/grid.jl:33-41): faces
+ * f = LinRange(0, len, m + 1), c = 0.5 * (f[2:end] + f[1:end-1]) = LinRange(0.5 (f[2] + f[1]),
+ * 0.5 (f[m+1] + f[m]), m).  first/last point and step(c) = dr(grid) / dz(grid). */
+struct CentreRange {
+    double first, last, step;
+    int64_t lendiv;
+    CentreRange(double len, int m) {
+        const double f1 = lerpi(0, m, 0.0, len), f2 = lerpi(1, m, 0.0, len);
+        const double fm = lerpi(m - 1, m, 0.0, len), fm1 = lerpi(m, m, 0.0, len);
+        first = 0.5 * (f2 + f1);
+        last = 0.5 * (fm1 + fm);
+        lendiv = m > 1 ? m - 1 : 1;
+        step = (last - first) / (double)lendiv;
+    }
+    double at(int64_t i) const { return lerpi(i - 1, lendiv, first, last); }   /* c[i], 1-based */
+};
+
 /* LinRange getindex (0-based j): lerpi(j, lendiv, start, stop), Base range.jl */
 inline double linrange_at(const orc_table* t, int64_t j) {
     const double lendiv = (double)(t->neps - 1);
@@ -222,7 +245,7 @@ int efield_cyl(const orc_field* f, const double x[3], double e[3]) {
     const double r0 = std::sqrt(x[0] * x[0] + x[1] * x[1]);
     /* inside: grid.jl:45-49 with rf = LinRange(0, R, M+1), zf = LinRange(0, L, N+1) */
     if (!((0.0 < r0 && r0 < f->R) && (0.0 < x[2] && x[2] < f->L))) return 0;
-    const double drc = f->R / f->M, dzc = f->L / f->N;  /* step(grid.rc), step(grid.zc) */
+    const double drc = CentreRange(f->R, f->M).step, dzc = CentreRange(f->L, f->N).step;  /* dr(grid), dz(grid) */
     double r = r0;
     if (r == 0.0) r = drc / 10.0;
     int64_t i, j, i1, j1;
@@ -338,8 +361,8 @@ void track_charge(orc_tracker* t, const double x[3], double val, std::vector<dou
     if (!(fi >= 1.0 && fi <= (double)t->M)) return;      /* checkbounds(grid.rc, i) */
     if (!(fj >= 0.0 && fj <= (double)t->N + 1.0)) return; /* checkbounds(qfixed, j) */
     const int64_t i = (int64_t)fi, j = (int64_t)fj;
-    const double rc = ((double)(i - 1) + 0.5) * drf;
-    const double dV = 2.0 * M_PI * rc * drf * dzf;
+    const CentreRange rcr(t->R, t->M);
+    const double dV = 2.0 * M_PI * rcr.at(i) * rcr.step * CentreRange(t->L, t->N).step;   /* grid.jl:76 */
     (*cyl_local)[i + j * (t->M + 2)] += val / dV;
 }
 
