@@ -44,7 +44,8 @@ enum {
     MCS_ERR_UNSUPPORTED = 7,    /* combination not implemented (e.g. user-defined process) */
     MCS_ERR_OVERFLOW = 8,       /* a tile produced more secondaries than its staging holds */
     MCS_ERR_NOMEM = 9,          /* device allocation failed */
-    MCS_ERR_TIMEOUT = 10        /* a bounded device-side wait gave up */
+    MCS_ERR_TIMEOUT = 10,       /* a bounded device-side wait gave up */
+    MCS_ERR_UNIFORMS = 11       /* a particle needed more injected uniforms than it was given */
 };
 
 /* ---- collision process kinds (JuMC/src/electron.jl:70-84, collisions.jl:3) ---- */
@@ -229,6 +230,26 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
                                      mcs_grid* tracker, mcs_grid* deposit, double val, double* x, double* v,
                                      double* w, double* s, uint8_t* active, int64_t* n, int64_t capacity,
                                      int chunks);
+/* Uniform source of advance! and collisions!.  The reference draws Julia's rand()
+ * (JuMC/src/util.jl:5,8,17, collisions.jl:166, mixed_population.jl:48; rand() in a
+ * single-threaded run is one serial stream); the library draws counter-based Philox streams
+ * (MCS_UNIFORMS_PHILOX, the default).  MCS_UNIFORMS_INJECTED makes the following steps take
+ * each particle's draws from caller-given values instead, so that a recorded run of the
+ * reference can be replayed particle by particle: slot i < nslots consumes u[offsets[i]],
+ * u[offsets[i] + 1], ... (offsets has nslots + 1 entries, u has offsets[nslots] values in
+ * (0, 1]) in the order the reference draws them for that particle -- per collision: xi;
+ * then elastic and excitation phi, u (randsphere); ionization phi, u, phi, u and the
+ * secondary's nextcoll() (MCS_IONIZATION_UNIFORM: its sharing fraction first); attachment
+ * and null nothing; then the particle's new nextcoll().  A slot's position carries over to
+ * the next step; a particle that needs a value beyond its range (or a slot >= nslots that
+ * draws) fails the step with MCS_ERR_UNIFORMS.  The values are copied to the device.
+ * Photo-emission keeps its Philox streams; mesh-layout populations and
+ * mcs_advance_deposit[_host] reject the mode (MCS_ERR_UNSUPPORTED).  MCS_UNIFORMS_PHILOX
+ * (u and offsets ignored) switches back.  Replaces no reference function: it feeds the
+ * reference's rand() calls. */
+enum { MCS_UNIFORMS_PHILOX = 0, MCS_UNIFORMS_INJECTED = 1 };
+MCS_API int mcs_set_uniform_source(mcs_pop* p, int mode, const double* u, const int64_t* offsets,
+                                   int64_t nslots);
 /* collisions!(mpopl, dt, tracker) (JuMC/src/mixed_population.jl:61-77). */
 MCS_API int mcs_collisions(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* tracker);
 /* density!(grid, arr, mpopl, Electron, fields, val) (MCStreamer/src/poisson.jl:65-84)

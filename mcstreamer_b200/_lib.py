@@ -15,12 +15,13 @@ LIB_PATH = Path(__file__).resolve().parent / "libmcs_b200.so"
 
 # status codes (include/mcs.h)
 OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_ENERGY_RANGE, ERR_FIELD_TOO_HIGH = 0, 1, 2, 3, 4, 5
-ERR_NONFINITE, ERR_UNSUPPORTED, ERR_OVERFLOW, ERR_NOMEM, ERR_TIMEOUT = 6, 7, 8, 9, 10
+ERR_NONFINITE, ERR_UNSUPPORTED, ERR_OVERFLOW, ERR_NOMEM, ERR_TIMEOUT, ERR_UNIFORMS = 6, 7, 8, 9, 10, 11
 STATUS_NAMES = {
     0: "MCS_OK", 1: "MCS_ERR_ARG", 2: "MCS_ERR_CUDA", 3: "MCS_ERR_CAPACITY", 4: "MCS_ERR_ENERGY_RANGE",
     5: "MCS_ERR_FIELD_TOO_HIGH", 6: "MCS_ERR_NONFINITE", 7: "MCS_ERR_UNSUPPORTED", 8: "MCS_ERR_OVERFLOW",
-    9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT",
+    9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT", 11: "MCS_ERR_UNIFORMS",
 }
+UNIFORMS_PHILOX, UNIFORMS_INJECTED = 0, 1
 # process kinds
 NULL, ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, IONIZATION_UNIFORM, PHOTOEMISSION = 0, 1, 2, 3, 4, 5, 6
 FP64, FP32 = 0, 1
@@ -77,6 +78,7 @@ SIGNATURES = {
     "mcs_advance_deposit": (i32, [vp, vp, vp, f64, vp, vp, f64]),
     "mcs_advance_deposit_host": (i32, [vp, vp, vp, f64, vp, vp, f64, pd, pd, pd, pd, pu8, pi64, i64, i32]),
     "mcs_collisions": (i32, [vp, vp, f64, vp]),
+    "mcs_set_uniform_source": (i32, [vp, i32, pd, pi64, i64]),
     "mcs_deposit": (i32, [vp, vp, f64]),
     "mcs_repack": (i32, [vp]),
     "mcs_swarm_resample": (i32, [vp, i64, f64]),

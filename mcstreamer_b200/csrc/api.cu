@@ -1,4 +1,5 @@
 // api.cu -- the extern "C" entry points declared in include/mcs.h.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -19,6 +20,7 @@ int map_status(uint32_t st) {
     if (st & ST_ENERGY) return MCS_ERR_ENERGY_RANGE;
     if (st & ST_FIELD) return MCS_ERR_FIELD_TOO_HIGH;
     if (st & ST_NONFINITE) return MCS_ERR_NONFINITE;
+    if (st & ST_UNIFORMS) return MCS_ERR_UNIFORMS;
     return MCS_OK;
 }
 
@@ -31,6 +33,7 @@ const char* status_text(int code) {
     case MCS_ERR_FIELD_TOO_HIGH: return "Too high electric field";
     case MCS_ERR_NONFINITE: return "non-finite particle state";
     case MCS_ERR_UNSUPPORTED: return "a process the kernel does not apply (photo-emission needs mcs_advance_mixed)";
+    case MCS_ERR_UNIFORMS: return "a particle needed more injected uniforms than it was given";
     default: return "";
     }
 }
@@ -535,6 +538,7 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage); cudaFree(p->d_log);
     for (int q = 0; q < 2; ++q) { cudaFree(p->sort_key[q]); cudaFree(p->sort_val[q]); }
     cudaFree(p->sort_hist); cudaFree(p->sort_hoff); cudaFree(p->seg_a); cudaFree(p->seg_b);
+    cudaFree(p->d_inj_u); cudaFree(p->d_inj_pos); cudaFree(p->d_inj_end);
     free_host_step(p->host_step);
     delete p;
     return MCS_OK;
@@ -544,6 +548,39 @@ MCS_API int mcs_pop_set_seed(mcs_pop* p, uint64_t seed, uint32_t step) {
     if (!p) return MCS_ERR_ARG;
     p->seed = seed;
     p->step = step;
+    return MCS_OK;
+}
+
+MCS_API int mcs_set_uniform_source(mcs_pop* p, int mode, const double* u, const int64_t* offsets, int64_t nslots) {
+    if (!p) return MCS_ERR_ARG;
+    mcs_ctx* c = p->ctx;
+    if (mode == MCS_UNIFORMS_PHILOX) {
+        p->inj = false;
+        return MCS_OK;
+    }
+    if (mode != MCS_UNIFORMS_INJECTED || nslots < 0 || !offsets) return set_err(c, MCS_ERR_ARG, "uniform source mode");
+    if (p->cells) return set_err(c, MCS_ERR_UNSUPPORTED, "injected uniforms on a mesh-layout population");
+    if (offsets[0] < 0) return set_err(c, MCS_ERR_ARG, "negative uniform offset");
+    for (int64_t i = 0; i < nslots; ++i)
+        if (offsets[i + 1] < offsets[i]) return set_err(c, MCS_ERR_ARG, "uniform offsets must not decrease");
+    const int64_t total = offsets[nslots];
+    if (total > 0 && !u) return set_err(c, MCS_ERR_ARG, "no uniforms");
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));   // steps in flight still read the old values
+    cudaFree(p->d_inj_u); cudaFree(p->d_inj_pos); cudaFree(p->d_inj_end);
+    p->d_inj_u = nullptr; p->d_inj_pos = nullptr; p->d_inj_end = nullptr;
+    p->inj = false;
+    int st = dalloc(c, &p->d_inj_u, (size_t)std::max<int64_t>(total, 1));
+    if (!st) st = dalloc(c, &p->d_inj_pos, (size_t)std::max<int64_t>(nslots, 1));
+    if (!st) st = dalloc(c, &p->d_inj_end, (size_t)std::max<int64_t>(nslots, 1));
+    if (st) return st;
+    if (total > 0) MCS_CK(c, cudaMemcpy(p->d_inj_u, u, (size_t)total * sizeof(double), cudaMemcpyHostToDevice));
+    if (nslots > 0) {
+        MCS_CK(c, cudaMemcpy(p->d_inj_pos, offsets, (size_t)nslots * sizeof(int64_t), cudaMemcpyHostToDevice));
+        MCS_CK(c, cudaMemcpy(p->d_inj_end, offsets + 1, (size_t)nslots * sizeof(int64_t), cudaMemcpyHostToDevice));
+    }
+    p->inj_n = nslots;
+    p->inj = true;
     return MCS_OK;
 }
 

@@ -92,6 +92,10 @@ inline StepCtl step_ctl(mcs_pop* p, double dt, uint32_t tag, double* moments_out
     s.dt = dt;
     s.slot_base = p->slot_base;
     s.photo = p->photo;
+    s.inj_u = p->inj ? p->d_inj_u : nullptr;
+    s.inj_pos = p->inj ? p->d_inj_pos : nullptr;
+    s.inj_end = p->inj ? p->d_inj_end : nullptr;
+    s.inj_n = p->inj ? p->inj_n : 0;
     return s;
 }
 

@@ -19,6 +19,7 @@ enum : uint32_t {
     ST_OVERFLOW = 16u,   // a tile produced more secondaries than its staging holds
     ST_TIMEOUT = 32u,    // a bounded wait gave up
     ST_UNSUPPORTED = 64u,  // a process this kernel does not apply (photo-emission without photons)
+    ST_UNIFORMS = 128u,    // a particle ran past its injected uniforms
 };
 
 // Philox stream tags (4th counter word); must match the oracle.
@@ -85,6 +86,15 @@ __device__ __forceinline__ float uni32(uint32_t w) { return __uint2float_rn(w | 
 // c = Philox(seed; {slot, step, j | 2^31, tag}) -- secondary direction, secondary s and the
 // energy-sharing fraction.  Every colliding lane generates its block at the same point of
 // the sub-step, so the generator runs converged across the warp.
+//
+// The collision code reads the draws through named accessors, called in the order the
+// reference draws them (xi; the process's own draws; the new s), which is what lets the
+// injected source below replay a serial stream.  T = double gives the FP64 uniform, float
+// the FP32 one.
+template <typename T> __device__ __forceinline__ T uni_t(uint32_t w);
+template <> __device__ __forceinline__ double uni_t<double>(uint32_t w) { return uni64(w); }
+template <> __device__ __forceinline__ float uni_t<float>(uint32_t w) { return uni32(w); }
+
 struct Event {
     uint32_t k0, k1, slot, step, tag, j;
     U4 b, c;
@@ -96,6 +106,56 @@ struct Event {
         ++j;
     }
     __device__ __forceinline__ void second() { c = philox10(U4{slot, step, (j - 1) | 0x80000000u, tag}, k0, k1); }
+    __device__ __forceinline__ uint32_t jev() const { return j - 1; }   // index of the current event
+    template <typename T> __device__ __forceinline__ T xi() { return uni_t<T>(b.x); }
+    template <typename T> __device__ __forceinline__ T phi1() { return uni_t<T>(b.z); }
+    template <typename T> __device__ __forceinline__ T cos1() { return uni_t<T>(b.w); }
+    template <typename T> __device__ __forceinline__ T phi2() { return uni_t<T>(c.x); }
+    template <typename T> __device__ __forceinline__ T cos2() { return uni_t<T>(c.y); }
+    template <typename T> __device__ __forceinline__ T s2() { return uni_t<T>(c.z); }
+    template <typename T> __device__ __forceinline__ T share() { return uni_t<T>(c.w); }
+    template <typename T> __device__ __forceinline__ T snew() { return uni_t<T>(b.y); }
+    __device__ __forceinline__ void finish() {}
+};
+
+// Injected uniforms (mcs_set_uniform_source): the particle of slot `slot` reads its own
+// caller-given values one after the other, in whatever order the collision code asks for
+// them -- the reference's serial order.  Running past the range raises ST_UNIFORMS and
+// reads 0.5, so the step still ends; finish() stores the position for the next step.
+struct EventInj {
+    const double* u;
+    long long* pos_out;
+    long long pos, end;
+    uint32_t* status;
+    uint32_t j, slot;
+    bool has;   // the slot has a range
+    __device__ __forceinline__ void bind(const double* u_, long long* pos_, const long long* end_, long long n,
+                                         uint32_t* status_) {
+        u = u_; pos_out = pos_; status = status_;
+        has = (long long)slot < n;
+        if (has) { pos = pos_[slot]; end = end_[slot]; }
+        else { pos = 0; end = 0; }
+    }
+    __device__ __forceinline__ void init(uint64_t, uint32_t slot_, uint32_t, uint32_t) { slot = slot_; j = 0; }
+    __device__ __forceinline__ void begin() { ++j; }
+    __device__ __forceinline__ void second() {}
+    __device__ __forceinline__ uint32_t jev() const { return j - 1; }
+    __device__ __forceinline__ double next() {
+        if (pos < end) return __ldg(u + pos++);
+        atomicOr(status, ST_UNIFORMS);
+        return 0.5;
+    }
+    template <typename T> __device__ __forceinline__ T xi() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T phi1() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T cos1() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T phi2() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T cos2() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T s2() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T share() { return (T)next(); }
+    template <typename T> __device__ __forceinline__ T snew() { return (T)next(); }
+    __device__ __forceinline__ void finish() {
+        if (has) pos_out[slot] = pos;
+    }
 };
 
 // rand(Poisson(lam)) from a stream: inversion below 10, PTRS (Hoermann 1993) above; the

@@ -126,6 +126,11 @@ struct StepCtl {
     uint32_t stage_cap;       // entries per CTA
     uint32_t slot_base;       // added to the slot index that keys a particle's random stream
     PhotoOut photo;           // photo-emission output (k_step_abs only)
+    // injected uniforms (mcs_set_uniform_source): slot i reads inj_u[inj_pos[i] .. inj_end[i])
+    const double* inj_u;
+    long long* inj_pos;
+    const long long* inj_end;
+    long long inj_n;          // slots with a range
 };
 
 }  // namespace mcs
@@ -237,4 +242,10 @@ struct mcs_pop {
     double* d_log = nullptr;       // per-step fused moments, log_cap entries of kStepMoments
     int log_cap = 0;
     uint32_t log_step0 = 0;
+    // injected uniforms (mcs_set_uniform_source)
+    bool inj = false;
+    double* d_inj_u = nullptr;
+    long long* d_inj_pos = nullptr;   // next value of each slot
+    long long* d_inj_end = nullptr;   // end of each slot's range
+    long long inj_n = 0;
 };

@@ -120,9 +120,12 @@ template <typename T>
 struct Sec { T vx, vy, vz, s; };
 
 // collide: JuMC/src/electron.jl:108-139.  FP64 follows the reference's expressions.  The
-// event's block b supplies the direction (b.z, b.w); ionization draws block c for the
-// secondary's direction (c.x, c.y), its free-flight time (c.z) and the sharing fraction (c.w).
-__device__ __forceinline__ int collide64(int kind, double par, double eng, Event& e, double& vx, double& vy,
+// draws are read in the reference's order (the event's accessors, mcs_device.cuh): a
+// direction is phi then u (randsphere, util.jl:4-12); ionization draws the primary's
+// direction, the secondary's and then the secondary's free flight (electron.jl:121-125); the
+// uniform-sharing ionization draws its sharing fraction first.
+template <class Ev>
+__device__ __forceinline__ int collide64(int kind, double par, double eng, Ev& e, double& vx, double& vy,
                                          double& vz, Sec<double>& sec) {
     const double m = kElectronMass;
     if (kind == K_ELASTIC) {
@@ -131,7 +134,8 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Event
         const double dx = vx - cx, dy = vy - cy, dz = vz - cz;
         const double nrm = sqrt(dx * dx + dy * dy + dz * dz);
         double ux, uy, uz;
-        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
+        const double a = e.template phi1<double>(), b = e.template cos1<double>();
+        M<double>::dir(a, b, ux, uy, uz);
         vx = ux * nrm + cx; vy = uy * nrm + cy; vz = uz * nrm + cz;
         return OUT_NONE;
     }
@@ -139,7 +143,8 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Event
         const double E1 = fmax(0.0, eng - par);
         const double va = sqrt(2.0 * E1 / m);
         double ux, uy, uz;
-        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
+        const double a = e.template phi1<double>(), b = e.template cos1<double>();
+        M<double>::dir(a, b, ux, uy, uz);
         vx = ux * va; vy = uy * va; vz = uz * va;
         return OUT_NONE;
     }
@@ -151,16 +156,18 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Event
             va1 = va2 = sqrt(2.0 * E1 / m);
         } else {
             const double Ea = fmax(0.0, eng - par);
-            const double E2 = uni64(e.c.w) * Ea;
+            const double E2 = e.template share<double>() * Ea;
             const double E1 = Ea - E2;
             va1 = sqrt(2.0 * E1 / m);
             va2 = sqrt(2.0 * E2 / m);
         }
         double ux, uy, uz, wx, wy, wz;
-        M<double>::dir(uni64(e.b.z), uni64(e.b.w), ux, uy, uz);
-        M<double>::dir(uni64(e.c.x), uni64(e.c.y), wx, wy, wz);
+        const double a1 = e.template phi1<double>(), b1 = e.template cos1<double>();
+        M<double>::dir(a1, b1, ux, uy, uz);
+        const double a2 = e.template phi2<double>(), b2 = e.template cos2<double>();
+        M<double>::dir(a2, b2, wx, wy, wz);
         sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
-        sec.s = -log(uni64(e.c.z));
+        sec.s = -log(e.template s2<double>());
         vx = ux * va1; vy = uy * va1; vz = uz * va1;
         return OUT_NEW;
     }
@@ -170,21 +177,24 @@ __device__ __forceinline__ int collide64(int kind, double par, double eng, Event
 }
 
 // FP32: energies in v^2 units (par = 2*threshold/m), the same draws as collide64.
-__device__ __forceinline__ int collide32(int kind, float par, float v2, Event& e, float& vx, float& vy, float& vz,
+template <class Ev>
+__device__ __forceinline__ int collide32(int kind, float par, float v2, Ev& e, float& vx, float& vy, float& vz,
                                          Sec<float>& sec) {
     if (kind == K_ELASTIC) {
         const float cx = par * vx, cy = par * vy, cz = par * vz;
         const float dx = vx - cx, dy = vy - cy, dz = vz - cz;
         const float nrm = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         float ux, uy, uz;
-        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
+        const float a = e.template phi1<float>(), b = e.template cos1<float>();
+        M<float>::dir(a, b, ux, uy, uz);
         vx = fmaf(ux, nrm, cx); vy = fmaf(uy, nrm, cy); vz = fmaf(uz, nrm, cz);
         return OUT_NONE;
     }
     if (kind == K_EXCITATION) {
         const float va = sqrtf(fmaxf(0.0f, v2 - par));
         float ux, uy, uz;
-        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
+        const float a = e.template phi1<float>(), b = e.template cos1<float>();
+        M<float>::dir(a, b, ux, uy, uz);
         vx = ux * va; vy = uy * va; vz = uz * va;
         return OUT_NONE;
     }
@@ -195,15 +205,17 @@ __device__ __forceinline__ int collide32(int kind, float par, float v2, Event& e
         if (kind == K_IONIZATION) {
             va1 = va2 = sqrtf(0.5f * ea);
         } else {
-            const float f2 = uni32(e.c.w);
+            const float f2 = e.template share<float>();
             va1 = sqrtf(ea - f2 * ea);
             va2 = sqrtf(f2 * ea);
         }
         float ux, uy, uz, wx, wy, wz;
-        M<float>::dir(uni32(e.b.z), uni32(e.b.w), ux, uy, uz);
-        M<float>::dir(uni32(e.c.x), uni32(e.c.y), wx, wy, wz);
+        const float a1 = e.template phi1<float>(), b1 = e.template cos1<float>();
+        M<float>::dir(a1, b1, ux, uy, uz);
+        const float a2 = e.template phi2<float>(), b2 = e.template cos2<float>();
+        M<float>::dir(a2, b2, wx, wy, wz);
         sec.vx = wx * va2; sec.vy = wy * va2; sec.vz = wz * va2;
-        sec.s = M<float>::nlog(uni32(e.c.z));
+        sec.s = M<float>::nlog(e.template s2<float>());
         vx = ux * va1; vy = uy * va1; vz = uz * va1;
         return OUT_NEW;
     }

@@ -3,6 +3,8 @@
 //   k_collisions collisions! (fixed-step collision sampling, no push)
 //   k_step_mesh  3-D mesh, (cell, in-cell offset) layout, fused tracker + deposit
 #pragma once
+#include <type_traits>
+
 #include "step.cuh"
 
 namespace mcs {
@@ -195,8 +197,8 @@ __device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long lo
 
 // Shared collision body: select a process for velocity (vx, vy, vz) and apply it in place.
 // Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
-template <typename T, typename RowsT>
-__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Event& rng,
+template <typename T, typename RowsT, class Ev>
+__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Ev& rng,
                                             T& vx, T& vy, T& vz, Sec<T>& sec, int* row_out = nullptr) {
     int j;
     double eng = 0.0;
@@ -204,11 +206,11 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
     rng.begin();
     if constexpr (sizeof(T) == 8) {
         eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
-        const double xi = uni64(rng.b.x) * tab.maxrate;
+        const double xi = rng.template xi<double>() * tab.maxrate;
         j = select_row64(tab, eng, xi, C.flags, C.status);
     } else {
         v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
-        const float xi = uni32(rng.b.x) * tab.maxrate32;
+        const float xi = rng.template xi<float>() * tab.maxrate32;
         j = select_row32(tab, v2, xi, C.flags, C.status);
     }
     const int kind = j >= 0 ? rows.kind[j] : K_NULL;
@@ -267,7 +269,7 @@ __device__ __forceinline__ void photo_event(const StepCtl& C, const TableView& t
 // between real collisions is x0 + v0*tau + a*tau^2/2 and null sub-steps cost no push; the
 // sub-step sequence, draws and decisions are those of advance!.
 // ---------------------------------------------------------------------------------------
-template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
+template <typename T, int BLOCK, int PPT, class Field, bool CLOSED, class Ev = Event>
 __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab, GridView fgrid, GridView tgrid,
                                                     StepCtl C, Field field, YoshidaC Y, double ax, double ay,
                                                     double az) {
@@ -292,8 +294,10 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
             uint32_t ev = 0;
             uint32_t pcnt = 0;   // photons emitted by this particle in this step
             if (i < n_entry && P.act[i]) {
-                Event rng;
+                Ev rng;
                 rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
+                if constexpr (!std::is_same<Ev, Event>::value)
+                    rng.bind(C.inj_u, C.inj_pos, C.inj_end, C.inj_n, C.status);
                 T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                 T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
                 const T w = P.f[6][i];
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                                 py = fmaf((float)ay, h2, fmaf((float)vy, tau, (float)y));
                                 pz = fmaf((float)az, h2, fmaf((float)vz, tau, (float)z));
                             }
-                            photo_event(C, tab, row, local + (uint32_t)base, rng.j - 1, px, py, pz, (double)w, act,
+                            photo_event(C, tab, row, local + (uint32_t)base, rng.jev(), px, py, pz, (double)w, act,
                                         pcnt);
                         } else if (out != OUT_NONE) {
                             if constexpr (CLOSED) {  // settle the segment at the collision time
@@ -366,11 +370,12 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                             if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
                             act = 0;  // the particle keeps sub-stepping (mixed_population.jl:32)
                         }
-                        if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
-                        else s = (double)M<float>::nlog(uni32(rng.b.y));
+                        if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
+                        else s = (double)M<float>::nlog(rng.template snew<float>());
                     }
                     trem -= t;
                 }
+                rng.finish();
                 if constexpr (CLOSED) {
                     const float h2 = 0.5f * tau * tau;
                     x = fmaf((float)ax, h2, fmaf((float)vx, tau, (float)x));
@@ -424,7 +429,7 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
 // ---------------------------------------------------------------------------------------
 // collisions!(mpopl, dt, tracker): JuMC/src/mixed_population.jl:61-77 (no push).
 // ---------------------------------------------------------------------------------------
-template <typename T, int BLOCK, int PPT>
+template <typename T, int BLOCK, int PPT, class Ev = Event>
 __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView tab, GridView tgrid, StepCtl C) {
     constexpr int TILE = BLOCK * PPT;
     __shared__ TileShared<T, BLOCK, TILE> sh;
@@ -445,8 +450,10 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
             if (i < n_entry && P.act[i]) {
                 double s = (double)P.f[7][i] - C.dt * tab.maxrate;
                 if (s <= 0) {
-                    Event rng;
+                    Ev rng;
                     rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
+                    if constexpr (!std::is_same<Ev, Event>::value)
+                        rng.bind(C.inj_u, C.inj_pos, C.inj_end, C.inj_n, C.status);
                     const T x = P.f[0][i], y = P.f[1][i], z = P.f[2][i];
                     T vx = P.f[3][i], vy = P.f[4][i], vz = P.f[5][i];
                     const T w = P.f[6][i];
@@ -461,8 +468,9 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
                         if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
                         P.act[i] = 0;
                     }
-                    if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
-                    else s = (double)M<float>::nlog(uni32(rng.b.y));
+                    if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
+                    else s = (double)M<float>::nlog(rng.template snew<float>());
+                    rng.finish();
                     P.f[3][i] = vx; P.f[4][i] = vy; P.f[5][i] = vz;
                 }
                 P.f[7][i] = (T)s;
@@ -746,8 +754,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 } else if (out == OUT_REMOVE) {
                     act = 0;
                 }
-                if constexpr (sizeof(T) == 8) s = -log(uni64(rng.b.y));
-                else s = (double)M<float>::nlog(uni32(rng.b.y));
+                if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
+                else s = (double)M<float>::nlog(rng.template snew<float>());
             }
             trem -= t;
             if (!(trem > 0)) {

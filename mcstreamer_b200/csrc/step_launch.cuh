@@ -1,6 +1,8 @@
 // step_launch.cuh -- host launchers of the step kernels, instantiated per precision by
 // step_f32.cu and step_f64.cu.
 #pragma once
+#include <type_traits>
+
 #include "host_util.h"
 #include "step_kernel.cuh"
 
@@ -27,12 +29,16 @@ int attach_stage(mcs_pop* p, int grid, StepCtl& C) {
     return MCS_OK;
 }
 
-template <typename T, int BLOCK, int PPT, class Field, bool CLOSED>
+template <typename T, int BLOCK, int PPT, class Field, bool CLOSED, class Ev = Event>
 int launch_abs_variant(mcs_pop* p, const mcs_table* t, const GridView& fg, const GridView& tg, const Field& fld,
                        double dt, double ax, double ay, double az, double* mom) {
+    if constexpr (std::is_same<Ev, Event>::value) {
+        if (p->inj)   // the same kernel reading the caller's uniforms (mcs_set_uniform_source)
+            return launch_abs_variant<T, BLOCK, PPT, Field, CLOSED, EventInj>(p, t, fg, tg, fld, dt, ax, ay, az, mom);
+    }
     mcs_ctx* c = p->ctx;
     constexpr int TILE = BLOCK * PPT;
-    auto kern = k_step_abs<T, BLOCK, PPT, Field, CLOSED>;
+    auto kern = k_step_abs<T, BLOCK, PPT, Field, CLOSED, Ev>;
     const long long max_tiles = (p->cap + TILE - 1) / TILE;
     const int grid = persistent_grid(c, kern, BLOCK, max_tiles);
     YoshidaHost yh;
@@ -67,6 +73,7 @@ int launch_step_abs_impl(mcs_pop* p, const mcs_table* t, const mcs_field* f, dou
 template <typename T, int BLOCK, int PPT, int MINB = 1>
 int launch_step_mesh_impl(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
     mcs_ctx* c = p->ctx;
+    if (p->inj) return set_err(c, MCS_ERR_UNSUPPORTED, "injected uniforms on a mesh-layout population");
     constexpr int TILE = BLOCK * PPT;
     auto kern = k_step_mesh<T, BLOCK, PPT, MINB>;
     const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
@@ -79,11 +86,14 @@ int launch_step_mesh_impl(mcs_pop* p, const mcs_table* t, double dt, bool tracki
     return MCS_OK;
 }
 
-template <typename T, int BLOCK, int PPT>
+template <typename T, int BLOCK, int PPT, class Ev = Event>
 int launch_collisions_impl(mcs_pop* p, const mcs_table* t, double dt, mcs_grid* trk) {
+    if constexpr (std::is_same<Ev, Event>::value) {
+        if (p->inj) return launch_collisions_impl<T, BLOCK, PPT, EventInj>(p, t, dt, trk);
+    }
     mcs_ctx* c = p->ctx;
     constexpr int TILE = BLOCK * PPT;
-    auto kern = k_collisions<T, BLOCK, PPT>;
+    auto kern = k_collisions<T, BLOCK, PPT, Ev>;
     const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
     StepCtl C = step_ctl(p, dt, TAG_COLLISIONS, nullptr);
     if (int st = attach_stage<T, TILE>(p, grid, C)) return st;

@@ -9,7 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 from dataclasses import dataclass
-from typing import Optional
+from typing import Optional, Sequence
 
 import numpy as np
 
@@ -163,6 +163,23 @@ class Population:
         s = C.c_uint32()
         self.ctx.check(self.ctx.lib.mcs_pop_get_step(self.h, C.byref(s)))
         return s.value
+
+    def set_uniforms(self, per_slot: Optional[Sequence[Sequence[float]]]) -> None:
+        """Feed the following steps' draws from given values instead of the Philox streams
+        (mcs_set_uniform_source): per_slot[i] are slot i's uniforms in the order the
+        reference's serial run draws them (rand() in util.jl:5,8,17, collisions.jl:166).
+        None returns to the streams."""
+        lib = self.ctx.lib
+        if per_slot is None:
+            self.ctx.check(lib.mcs_set_uniform_source(self.h, L.UNIFORMS_PHILOX, None, None, 0))
+            return
+        lens = np.array([len(a) for a in per_slot], dtype=np.int64)
+        offsets = np.zeros(len(lens) + 1, dtype=np.int64)
+        np.cumsum(lens, out=offsets[1:])
+        u = np.concatenate([np.asarray(a, dtype=np.float64) for a in per_slot]) if len(lens) else np.zeros(0)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self.ctx.check(lib.mcs_set_uniform_source(self.h, L.UNIFORMS_INJECTED, L.dptr(u), L.i64ptr(offsets),
+                                                  len(lens)))
 
     def init_maxwellian(self, n: int, mean_ev: float = 1.0) -> None:
         """n swarm electrons drawn on the device (origin, weight 1, isotropic Maxwellian)."""

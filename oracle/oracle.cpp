@@ -30,8 +30,9 @@
 namespace {
 
 /* internal status flags, mapped to the public codes by status_code() */
-enum { F_CAP = 1, F_ENERGY = 2, F_FIELD = 4, F_UNSUPPORTED = 8 };
+enum { F_CAP = 1, F_ENERGY = 2, F_FIELD = 4, F_UNSUPPORTED = 8, F_UNIFORMS = 16 };
 inline int status_code(int f) {
+    if (f & F_UNIFORMS) return 11;
     if (f & F_CAP) return 3;
     if (f & F_ENERGY) return 4;
     if (f & F_FIELD) return 5;
@@ -110,22 +111,48 @@ struct Stream {
  *   C = Philox(seed; {slot, step, j | 2^31, tag})      -> secondary direction, secondary s,
  *                                                         energy-sharing fraction
  * so every colliding particle generates exactly one block per event. */
+/* Injected uniforms: slot i reads u[pos[i]] .. u[end[i] - 1] in the order its draws are made
+ * (the reference's serial rand() order); see orc_advance_injected. */
+struct Injected {
+    const double* u;
+    int64_t* pos;
+    const int64_t* end;
+    int64_t nslots;
+};
+
 struct Event {
     uint32_t key[2];
     uint32_t c0, c1, tag, j;
     uint32_t b[4], c[4];
     bool have_c;
+    const Injected* inj = nullptr;   /* non-null: sequential injected values instead of Philox */
+    int64_t pos = 0, end = 0;
+    int* status = nullptr;
     Event(uint64_t seed, uint32_t slot, uint32_t step, uint32_t tag_) : c0(slot), c1(step), tag(tag_), j(0) {
         key[0] = (uint32_t)seed; key[1] = (uint32_t)(seed >> 32);
         have_c = false;
     }
+    void inject(const Injected* in, int64_t slot, int* st) {
+        inj = in;
+        status = st;
+        if (in && slot < in->nslots) { pos = in->pos[slot]; end = in->end[slot]; }
+    }
+    void finish(int64_t slot) {
+        if (inj && slot < inj->nslots) inj->pos[slot] = pos;
+    }
     void begin() {
-        const uint32_t ctr[4] = {c0, c1, j, tag};
+        ++j;
+        if (inj) return;
+        const uint32_t ctr[4] = {c0, c1, j - 1, tag};
         philox10(ctr, key, b);
         have_c = false;
-        ++j;
     }
     double u(int idx) {  /* Julia rand() draws of this event */
+        if (inj) {
+            if (pos < end) return inj->u[pos++];
+            *status |= F_UNIFORMS;
+            return 0.5;
+        }
         if (idx < 4) return word_to_uniform(b[idx]);
         if (!have_c) {
             const uint32_t ctr[4] = {c0, c1, (j - 1) | 0x80000000u, tag};
@@ -476,12 +503,14 @@ void do_one_collision(StepCtx& c, Event& rng, double x[3], double v[3], double& 
                 const double vcm[3] = {f * v[0], f * v[1], f * v[2]};
                 const double dv[3] = {v[0] - vcm[0], v[1] - vcm[1], v[2] - vcm[2]};
                 const double nrm = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
-                double d[3]; randsphere(rng.u(U_PHI), rng.u(U_COS), d);
+                const double uphi = rng.u(U_PHI), ucos = rng.u(U_COS);
+                double d[3]; randsphere(uphi, ucos, d);
                 for (int q = 0; q < 3; ++q) v[q] = d[q] * nrm + vcm[q];
             } else if (kind == ORC_EXCITATION) {
                 const double E1 = std::max(0.0, eng - par);
                 const double vabs = std::sqrt(2.0 * E1 / ELECTRON_MASS);
-                double d[3]; randsphere(rng.u(U_PHI), rng.u(U_COS), d);
+                const double uphi = rng.u(U_PHI), ucos = rng.u(U_COS);
+                double d[3]; randsphere(uphi, ucos, d);
                 for (int q = 0; q < 3; ++q) v[q] = d[q] * vabs;
             } else if (kind == ORC_IONIZATION || kind == ORC_IONIZATION_UNIFORM) {
                 double va1, va2;
@@ -497,8 +526,10 @@ void do_one_collision(StepCtx& c, Event& rng, double x[3], double v[3], double& 
                     va2 = std::sqrt(2.0 * E2 / ELECTRON_MASS);
                 }
                 double d1[3], d2[3];
-                randsphere(rng.u(U_PHI), rng.u(U_COS), d1);
-                randsphere(rng.u(U_PHI2), rng.u(U_COS2), d2);
+                const double uphi1 = rng.u(U_PHI), ucos1 = rng.u(U_COS);
+                randsphere(uphi1, ucos1, d1);
+                const double uphi2 = rng.u(U_PHI2), ucos2 = rng.u(U_COS2);
+                randsphere(uphi2, ucos2, d2);
                 Secondary sec;
                 for (int q = 0; q < 3; ++q) { sec.x[q] = x[q]; sec.v[q] = d2[q] * va2; }
                 sec.w = w;
@@ -605,12 +636,14 @@ void orc_yoshida(const orc_field* fld, double x[3], double v[3], double dt) { yo
 
 /* advance!: JuMC/src/mixed_population.jl:24-54 */
 static int advance_electrons(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
-                             orc_tracker* trk, int nthreads, int clamp_energy, orc_photons* ph_out) {
+                             orc_tracker* trk, int nthreads, int clamp_energy, orc_photons* ph_out,
+                             const Injected* inj = nullptr) {
     const uint64_t seed = pop->seed;
     const uint32_t step = pop->step;
     return drive(pop, tab, fld, trk, nthreads, clamp_energy, [&](StepCtx& c, int64_t i) {
         if (!pop->active[i]) return;                 /* l.active || continue */
         Event rng(seed, (uint32_t)i, step, ORC_TAG_ADVANCE);
+        rng.inject(inj, i, &c.status);
         double x[3] = {pop->x[3 * i], pop->x[3 * i + 1], pop->x[3 * i + 2]};
         double v[3] = {pop->v[3 * i], pop->v[3 * i + 1], pop->v[3 * i + 2]};
         double w = pop->w[i], s = pop->s[i];
@@ -629,6 +662,7 @@ static int advance_electrons(orc_pop* pop, const orc_table* tab, const orc_field
             }
             trem -= t;
         }
+        rng.finish(i);
         for (int q = 0; q < 3; ++q) { pop->x[3 * i + q] = x[q]; pop->v[3 * i + q] = v[q]; }
         pop->w[i] = w; pop->s[i] = s; pop->active[i] = active;
     }, ph_out);
@@ -637,6 +671,13 @@ static int advance_electrons(orc_pop* pop, const orc_table* tab, const orc_field
 int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
                 orc_tracker* trk, int nthreads, int clamp_energy) {
     return advance_electrons(pop, tab, fld, dt, trk, nthreads, clamp_energy, nullptr);
+}
+
+int orc_advance_injected(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
+                         orc_tracker* trk, int nthreads, int clamp_energy, const double* u, int64_t* pos,
+                         const int64_t* end, int64_t nslots) {
+    const Injected inj{u, pos, end, nslots};
+    return advance_electrons(pop, tab, fld, dt, trk, nthreads, clamp_energy, nullptr, &inj);
 }
 
 /* advance! of the photon population (mixed_population.jl:24-54 with the

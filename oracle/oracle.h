@@ -103,6 +103,11 @@ int orc_advance(orc_pop* pop, const orc_table* tab, const orc_field* fld, double
                 orc_tracker* trk, int nthreads, int clamp_energy);
 int orc_collisions(orc_pop* pop, const orc_table* tab, double dt, orc_tracker* trk,
                    int nthreads, int clamp_energy);
+/* advance! with injected uniforms: slot i < nslots reads u[pos[i]] .. u[end[i] - 1] in the
+ * reference's serial draw order (pos[i] is advanced); running out returns 11. */
+int orc_advance_injected(orc_pop* pop, const orc_table* tab, const orc_field* fld, double dt,
+                         orc_tracker* trk, int nthreads, int clamp_energy, const double* u, int64_t* pos,
+                         const int64_t* end, int64_t nslots);
 
 /* ---- helpers exposed for unit known-answer tests ---- */
 void orc_efield(const orc_field* fld, const double x[3], double e[3]);

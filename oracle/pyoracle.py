@@ -61,6 +61,8 @@ def lib():
                                   C.POINTER(Tracker), C.c_int, C.c_int]
         L.orc_collisions.argtypes = [C.POINTER(Pop), C.POINTER(Table), C.c_double, C.POINTER(Tracker), C.c_int,
                                      C.c_int]
+        L.orc_advance_injected.argtypes = [C.POINTER(Pop), C.POINTER(Table), C.POINTER(Field), C.c_double,
+                                           C.POINTER(Tracker), C.c_int, C.c_int, pd, pi64, pi64, C.c_int64]
         L.orc_efield.argtypes = [C.POINTER(Field), pd, pd]
         L.orc_yoshida.argtypes = [C.POINTER(Field), pd, pd, C.c_double]
         L.orc_indweight.argtypes = [C.POINTER(Table), C.c_double, pi64, pd]
@@ -236,6 +238,20 @@ def nthreads():
 def advance(pop: OraclePop, table: OracleTable, field, dt, tracker=None, threads=None, clamp=False):
     return lib().orc_advance(C.byref(pop.p), C.byref(table.s), C.byref(field), dt,
                              C.byref(tracker) if tracker is not None else None, threads or nthreads(), int(clamp))
+
+
+def advance_injected(pop: OraclePop, table: OracleTable, field, dt, per_slot, tracker=None, threads=None,
+                     clamp=False):
+    """advance! with each slot's draws taken from per_slot[i] in the reference's serial order."""
+    lens = np.array([len(a) for a in per_slot], dtype=np.int64)
+    end = np.cumsum(lens).astype(np.int64)
+    pos = (end - lens).astype(np.int64)
+    u = np.ascontiguousarray(np.concatenate([np.asarray(a, np.float64) for a in per_slot]) if len(lens) else
+                             np.zeros(1))
+    return lib().orc_advance_injected(C.byref(pop.p), C.byref(table.s), C.byref(field), dt,
+                                      C.byref(tracker) if tracker is not None else None, threads or nthreads(),
+                                      int(clamp), u.ctypes.data_as(pd), pos.ctypes.data_as(pi64),
+                                      end.ctypes.data_as(pi64), len(lens))
 
 
 def collisions(pop, table, dt, tracker=None, threads=None, clamp=False):

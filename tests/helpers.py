@@ -5,6 +5,8 @@ import numpy as np
 
 from mcstreamer_b200 import constants as co
 from mcstreamer_b200.jumc import ParticleArrays
+from mcstreamer_b200 import lxcat
+from oracle import jumc_ref as R
 from oracle import pyoracle as po
 
 
@@ -73,3 +75,31 @@ def particle_mismatch(g: ParticleArrays, o: ParticleArrays, rtol: float, xatol: 
     bad |= relerr(g.s[:n], o.s[:n], satol) > rtol
     bad |= g.active[:n] != o.active[:n]
     return bad
+
+
+def attaching_table(uniform_sharing: bool):
+    """Synthetic gas 1 with attachment raised to 3e-20 m^2 below 5 eV, so that removals (and
+    the sub-stepping of removed electrons) happen often in a few steps."""
+    recs = lxcat.synthetic_records(1, uniform_sharing=uniform_sharing)
+    for r in recs:
+        if r["kind"] == "ATTACHMENT":
+            r["data"] = [[e, 3e-20 if e < 5.0 else 0.0] for e, _ in r["data"]]
+    return lxcat.load_lxcat_records(recs, {"SYN": lxcat.SYNTHETIC_DENSITY}, lxcat.DEFAULT_ENERGY)
+
+
+def serial_run(rt, p, efield, dt, seed, tracker=None, steps=1):
+    """Run the restatement with one serial uniform stream (numpy's generator, values in
+    (0, 1]) and record every slot's draws per step: the injected-uniform input."""
+    gen = np.random.default_rng(seed)
+    rp = R.Population(p.x, p.v, p.w, p.s, p.active, 16 * len(p.w))
+    per_step = []
+    for _ in range(steps):
+        recs = {}
+
+        def draws(i):
+            recs[i] = R.CountingSource(lambda: 1.0 - gen.random())
+            return recs[i]
+        n = rp.n
+        R.advance(rp, rt, efield, dt, tracker=tracker, draws=draws)
+        per_step.append([recs[i].values if i in recs else [] for i in range(n)])
+    return rp, per_step

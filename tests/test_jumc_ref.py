@@ -15,7 +15,7 @@ from mcstreamer_b200 import constants as co
 from mcstreamer_b200 import lxcat, streamer
 from oracle import jumc_ref as R
 from oracle import pyoracle as po
-from tests.helpers import broad, oracle_arrays, oracle_pop
+from tests.helpers import attaching_table, broad, oracle_arrays, oracle_pop, serial_run
 
 # Philox4x32-10 known-answer vectors (Random123 kat_vectors)
 KAT = [
@@ -37,16 +37,6 @@ def assert_same(rp: R.Population, op, what: str):
     assert rp.n == o.n, f"{what}: {rp.n} particles, oracle {o.n}"
     for name, mine, theirs in (("x", x, o.x), ("v", v, o.v), ("w", w, o.w), ("s", s, o.s), ("active", a, o.active)):
         np.testing.assert_array_equal(mine, theirs[:o.n], err_msg=f"{what}: {name}")
-
-
-def attaching_table(uniform_sharing: bool):
-    """Synthetic gas 1 with attachment raised to 3e-20 m^2 below 5 eV, so that removals (and
-    the sub-stepping of removed electrons) happen often in a few steps."""
-    recs = lxcat.synthetic_records(1, uniform_sharing=uniform_sharing)
-    for r in recs:
-        if r["kind"] == "ATTACHMENT":
-            r["data"] = [[e, 3e-20 if e < 5.0 else 0.0] for e, _ in r["data"]]
-    return lxcat.load_lxcat_records(recs, {"SYN": lxcat.SYNTHETIC_DENSITY}, lxcat.DEFAULT_ENERGY)
 
 
 @pytest.mark.parametrize("variant,uniform_sharing,emax", [(0, True, 120.0), (2, False, 120.0), ("att", False, 30.0),
@@ -226,3 +216,29 @@ def test_serial_draws_replay_reproduces_a_run():
     for x, y in zip(a.arrays(), b.arrays()):
         np.testing.assert_array_equal(x, y)
     assert sum(len(r.values) for r in recs.values()) > 4 * 120
+
+
+@pytest.mark.parametrize("uniform_sharing", [True, False])
+def test_oracle_injected_uniforms_replay_the_serial_run(uniform_sharing):
+    """orc_advance_injected fed each particle's draws of a serial run reproduces that run
+    bit for bit over three steps (secondaries draw in the steps after they appear)."""
+    t = attaching_table(uniform_sharing)
+    rt, ot = R.Table.from_lxcat(t), po.OracleTable.from_lxcat(t)
+    p = broad(250, 3, emax_ev=60.0)
+    ez = 5 * 100 * co.Td * 2.5e25
+    rp, per_step = serial_run(rt, p, R.FixedField([0.0, 0.0, ez]), 4e-13, 7, steps=3)
+    op = oracle_pop(p, 16 * len(p.w), 3)
+    for k, per in enumerate(per_step):
+        assert po.advance_injected(op, ot, po.field_uniform(0, 0, ez), 4e-13, per, threads=3) == 0
+    assert_same(rp, op, "injected")
+    assert sum(len(a) for a in per_step[-1]) > 1000
+
+
+def test_oracle_injected_uniforms_running_out_is_reported():
+    t = lxcat.synthetic_table(0)
+    rt, ot = R.Table.from_lxcat(t), po.OracleTable.from_lxcat(t)
+    p = broad(50, 2)
+    _, per_step = serial_run(rt, p, R.FixedField([0.0, 0.0, 1e7]), 4e-13, 2)
+    short = [a[:-1] for a in per_step[0]]
+    op = oracle_pop(p, 1000, 2)
+    assert po.advance_injected(op, ot, po.field_uniform(0, 0, 1e7), 4e-13, short) == 11
