@@ -45,7 +45,11 @@ enum {
     MCS_ERR_OVERFLOW = 8,       /* a tile produced more secondaries than its staging holds */
     MCS_ERR_NOMEM = 9,          /* device allocation failed */
     MCS_ERR_TIMEOUT = 10,       /* a bounded device-side wait gave up */
-    MCS_ERR_UNIFORMS = 11       /* a particle needed more injected uniforms than it was given */
+    MCS_ERR_UNIFORMS = 11,      /* a particle needed more injected uniforms than it was given */
+    MCS_ERR_CHARGE_RANGE = 12   /* a charge beyond the int64 fixed-point range of the deposits
+                                   (2^-32 e units): |w * val| >= 2^30 e for one particle, or a
+                                   node / cell sum of 2^30 e or more (within a factor 2 of the
+                                   2^31 e where the sums would wrap) */
 };
 
 /* ---- collision process kinds (JuMC/src/electron.jl:70-84, collisions.jl:3) ---- */

@@ -16,10 +16,11 @@ LIB_PATH = Path(__file__).resolve().parent / "libmcs_b200.so"
 # status codes (include/mcs.h)
 OK, ERR_ARG, ERR_CUDA, ERR_CAPACITY, ERR_ENERGY_RANGE, ERR_FIELD_TOO_HIGH = 0, 1, 2, 3, 4, 5
 ERR_NONFINITE, ERR_UNSUPPORTED, ERR_OVERFLOW, ERR_NOMEM, ERR_TIMEOUT, ERR_UNIFORMS = 6, 7, 8, 9, 10, 11
+ERR_CHARGE_RANGE = 12
 STATUS_NAMES = {
     0: "MCS_OK", 1: "MCS_ERR_ARG", 2: "MCS_ERR_CUDA", 3: "MCS_ERR_CAPACITY", 4: "MCS_ERR_ENERGY_RANGE",
     5: "MCS_ERR_FIELD_TOO_HIGH", 6: "MCS_ERR_NONFINITE", 7: "MCS_ERR_UNSUPPORTED", 8: "MCS_ERR_OVERFLOW",
-    9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT", 11: "MCS_ERR_UNIFORMS",
+    9: "MCS_ERR_NOMEM", 10: "MCS_ERR_TIMEOUT", 11: "MCS_ERR_UNIFORMS", 12: "MCS_ERR_CHARGE_RANGE",
 }
 UNIFORMS_PHILOX, UNIFORMS_INJECTED = 0, 1
 # process kinds

@@ -21,6 +21,7 @@ int map_status(uint32_t st) {
     if (st & ST_FIELD) return MCS_ERR_FIELD_TOO_HIGH;
     if (st & ST_NONFINITE) return MCS_ERR_NONFINITE;
     if (st & ST_UNIFORMS) return MCS_ERR_UNIFORMS;
+    if (st & ST_CHARGE) return MCS_ERR_CHARGE_RANGE;
     return MCS_OK;
 }
 
@@ -34,6 +35,7 @@ const char* status_text(int code) {
     case MCS_ERR_NONFINITE: return "non-finite particle state";
     case MCS_ERR_UNSUPPORTED: return "a process the kernel does not apply (photo-emission needs mcs_advance_mixed)";
     case MCS_ERR_UNIFORMS: return "a particle needed more injected uniforms than it was given";
+    case MCS_ERR_CHARGE_RANGE: return "a charge beyond the int64 fixed-point range (2^30 e per particle or node)";
     default: return "";
     }
 }

@@ -20,7 +20,14 @@ enum : uint32_t {
     ST_TIMEOUT = 32u,    // a bounded wait gave up
     ST_UNSUPPORTED = 64u,  // a process this kernel does not apply (photo-emission without photons)
     ST_UNIFORMS = 128u,    // a particle ran past its injected uniforms
+    ST_CHARGE = 256u,      // a charge beyond the int64 fixed-point range of the deposits
 };
+
+// Int64 fixed-point deposits count charge in units of 2^-32 e: one particle's charge must
+// stay below 2^30 e (W < 2^62), and a node or cell sum at or above 2^62 units (2^30 e) is
+// reported before it can reach 2^63.
+constexpr double kMaxDepositCharge = 0x1p30;
+constexpr long long kMaxNodeCharge = 1LL << 62;
 
 // Philox stream tags (4th counter word); must match the oracle.
 enum : uint32_t { TAG_ADVANCE = 0, TAG_SWARM_RESAMPLE = 1, TAG_CELL_RESAMPLE = 2, TAG_INIT = 3,

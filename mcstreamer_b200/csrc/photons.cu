@@ -123,7 +123,7 @@ __global__ void k_photon_step(PhotonView P, long long n_entry, double numax, dou
                     rng.begin();
                     const double xi = uni64(rng.b.x) * numax;
                     if (nu > xi) {
-                        if (tracking) track_abs(tg, x, y, z, w);
+                        if (tracking) track_abs(tg, x, y, z, w, status);
                         const uint32_t e = atomicAdd(iev_count, 1u);
                         if (e < iev_cap) {
                             IonEvent E;

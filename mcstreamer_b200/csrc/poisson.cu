@@ -839,13 +839,18 @@ __global__ void k_top_ghost(double* u, int M, int N, const double* bcond) {
 // deposit plus qfd, its FP64 density part (setneedle!, initfromfiles!), and ne the fluid
 // density ((M+4)x(N+4)); either is zero when absent (null pointer).  Ghost cells are zero.
 __global__ void k_assemble(double* b, const long long* qf, const long long* qp, const double* qfd,
-                           const double* ne, int M, int N, double dr, double dz) {
+                           const double* ne, int M, int N, double dr, double dz, uint32_t* status) {
     const long ld = M + 2;
     const long n = (long)(M + 2) * (N + 2);
     for (long t = gtid(); t < n; t += gthreads()) {
         const int j = (int)(t / ld);
         const int i = (int)(t - (long)j * ld);
         double v = 0.0;
+        // a cell sum within a factor 2 of where the int64 2^-32 e sums would wrap
+        const unsigned long long uf = (unsigned long long)qf[t], up = (unsigned long long)qp[t];
+        const unsigned long long af = qf[t] < 0 ? 0ull - uf : uf, ap = qp[t] < 0 ? 0ull - up : up;
+        if (af >= (unsigned long long)kMaxNodeCharge || ap >= (unsigned long long)kMaxNodeCharge)
+            atomicOr(status, ST_CHARGE);
         if (i >= 1 && i <= M && j >= 1 && j <= N) {
             const double rc = ((double)(i - 1) + 0.5) * dr;
             const double dv = 2.0 * M_PI * rc * dr * dz;
@@ -1644,7 +1649,7 @@ MCS_API int mcs_poisson_assemble(mcs_poisson* p) {
     const mcs_fluid* fl = p->g->fluid;
     k_assemble<<<grid_blocks(p, n), kThreads, 0, p->ctx->stream>>>(
         p->b, p->g->d_q[MCS_Q_FIXED], p->g->d_q[MCS_Q_PART], p->g->d_qfd, fl ? fl->ne[fl->cur] : nullptr,
-        p->M, p->N, p->dr, p->dz);
+        p->M, p->N, p->dr, p->dz, p->ctx->d_status);
     PSN_LAUNCH(p);
     return MCS_OK;
 }

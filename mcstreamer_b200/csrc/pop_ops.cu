@@ -539,7 +539,8 @@ int launch_moments(mcs_pop* p, const mcs_table* t, double* d_out, int nm) {
 // w*val (density = q*2^-32/dV on read).
 // ---------------------------------------------------------------------------------------
 template <typename T>
-__global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long long* __restrict__ q) {
+__global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long long* __restrict__ q,
+                          uint32_t* status) {
     const long long n = *P.n_in;
     const long long stride = (long long)gridDim.x * blockDim.x;
     if (mesh) {
@@ -563,7 +564,7 @@ __global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long l
                     charge = (double)P.f[6][i] * val;
                 }
             }
-            cic_fixed_warp(q, g.nx, g.ny, valid, cidx, ix, iy, iz, fx, fy, fz, charge);
+            cic_fixed_warp(q, g.nx, g.ny, valid, cidx, ix, iy, iz, fx, fy, fz, charge, status);
         }
         return;
     }
@@ -574,9 +575,9 @@ __global__ void k_deposit(PopView<T> P, GridView g, int mesh, double val, long l
             int ix, iy, iz;
             double fx, fy, fz;
             if (cart_locate(g, P.f[0][i], P.f[1][i], P.f[2][i], ix, iy, iz, fx, fy, fz))
-                cic_fixed(q, g.nx, g.ny, ix, iy, iz, fx, fy, fz, charge);
+                cic_fixed(q, g.nx, g.ny, ix, iy, iz, fx, fy, fz, charge, status);
         } else {
-            cyl_track(g, q, P.f[0][i], P.f[1][i], P.f[2][i], charge);
+            cyl_track(g, q, P.f[0][i], P.f[1][i], P.f[2][i], charge, status);
         }
     }
 }
@@ -586,9 +587,11 @@ int launch_deposit(mcs_pop* p, mcs_grid* g, double val) {
     const int gr = grid_for(c, p->cap, 256);
     const int mesh = p->cells != nullptr;
     if (p->precision == MCS_FP32)
-        k_deposit<float><<<gr, 256, 0, c->stream>>>(pop_view<float>(p), g->v, mesh, val, g->d_q[MCS_Q_PART]);
+        k_deposit<float><<<gr, 256, 0, c->stream>>>(pop_view<float>(p), g->v, mesh, val, g->d_q[MCS_Q_PART],
+                                                     c->d_status);
     else
-        k_deposit<double><<<gr, 256, 0, c->stream>>>(pop_view<double>(p), g->v, mesh, val, g->d_q[MCS_Q_PART]);
+        k_deposit<double><<<gr, 256, 0, c->stream>>>(pop_view<double>(p), g->v, mesh, val, g->d_q[MCS_Q_PART],
+                                                      c->d_status);
     MCS_CK_LAUNCH(c);
     return MCS_OK;
 }

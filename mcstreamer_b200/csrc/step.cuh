@@ -229,7 +229,11 @@ __device__ __forceinline__ int collide32(int kind, float par, float v2, Ev& e, f
 // (seven rounded corners, the eighth takes the remainder: node sum == llrint(q*2^32)).
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ void cic_fixed(long long* q, int nx, int ny, int ix, int iy, int iz, double fx,
-                                          double fy, double fz, double charge) {
+                                          double fy, double fz, double charge, uint32_t* status) {
+    if (!(fabs(charge) < kMaxDepositCharge)) {   // also NaN
+        atomicOr(status, ST_CHARGE);
+        return;
+    }
     const long long W = __double2ll_rn(charge * 0x1p32);
     const double Wd = (double)W;
     const double gx[2] = {1.0 - fx, fx}, gy[2] = {1.0 - fy, fy}, gz[2] = {1.0 - fz, fz};
@@ -255,9 +259,14 @@ __device__ __forceinline__ void cic_fixed(long long* q, int nx, int ny, int ix, 
 // run issues the eight atomics, so a warp inside one cell makes 8 atomics instead of 256.
 // Integer sums: the node totals are bit-identical to per-particle atomics.
 __device__ __forceinline__ void cic_fixed_warp(long long* q, int nx, int ny, bool valid, uint32_t cell, int ix, int iy,
-                                               int iz, double fx, double fy, double fz, double charge) {
+                                               int iz, double fx, double fy, double fz, double charge,
+                                               uint32_t* status) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    if (valid && !(fabs(charge) < kMaxDepositCharge)) {
+        atomicOr(status, ST_CHARGE);
+        valid = false;
+    }
     long long v[8];
     if (valid) {
         const long long W = __double2ll_rn(charge * 0x1p32);
@@ -316,7 +325,11 @@ __device__ __forceinline__ bool cart_locate(const GridView& g, double x, double 
 // density!/track1 do (1 <= i <= M, 0 <= j <= N+1).  Stored as int64 weight sums;
 // density = q * 2^-32 / dV(i) on read.
 __device__ __forceinline__ void cyl_track(const GridView& g, long long* q, double x, double y, double z,
-                                          double charge) {
+                                          double charge, uint32_t* status) {
+    if (!(fabs(charge) < kMaxDepositCharge)) {
+        atomicOr(status, ST_CHARGE);
+        return;
+    }
     const double rho = sqrt(x * x + y * y);
     double fi = floor(rho / g.dr);
     if (__fma_rn(fi, g.dr, -rho) > 0.0) fi -= 1.0;
@@ -330,14 +343,15 @@ __device__ __forceinline__ void cyl_track(const GridView& g, long long* q, doubl
 }
 
 // CollisionTracker at an absolute position (gridfields.jl:203-224).
-__device__ __forceinline__ void track_abs(const GridView& g, double x, double y, double z, double charge) {
+__device__ __forceinline__ void track_abs(const GridView& g, double x, double y, double z, double charge,
+                                          uint32_t* status) {
     if (g.type == GRID_CART3D) {
         int ix, iy, iz;
         double fx, fy, fz;
         if (cart_locate(g, x, y, z, ix, iy, iz, fx, fy, fz))
-            cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, fx, fy, fz, charge);
+            cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, fx, fy, fz, charge, status);
     } else if (g.type == GRID_CYL) {
-        cyl_track(g, g.qfixed, x, y, z, charge);
+        cyl_track(g, g.qfixed, x, y, z, charge, status);
     }
 }
 

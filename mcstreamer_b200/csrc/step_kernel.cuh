@@ -363,11 +363,11 @@ __global__ void __launch_bounds__(BLOCK) k_step_abs(PopView<T> P, TableView tab,
                             vx = cvx; vy = cvy; vz = cvz;
                         }
                         if (out == OUT_NEW) {
-                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
+                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w, C.status);
                             const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
                             stage(sg, &sh.count, local, ev++, vals, 0u, act, C.status);
                         } else if (out == OUT_REMOVE) {
-                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
+                            if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w, C.status);
                             act = 0;  // the particle keeps sub-stepping (mixed_population.jl:32)
                         }
                         if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
@@ -461,11 +461,11 @@ __global__ void __launch_bounds__(BLOCK) k_collisions(PopView<T> P, TableView ta
                     const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
                     if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
                     if (out == OUT_NEW) {
-                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w);
+                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, (double)w, C.status);
                         const T vals[8] = {x, y, z, sec.vx, sec.vy, sec.vz, w, sec.s};
                         stage(sg, &sh.count, local, ev++, vals, 0u, (uint8_t)1, C.status);
                     } else if (out == OUT_REMOVE) {
-                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w);
+                        if (tracking) track_abs(tgrid, (double)x, (double)y, (double)z, -(double)w, C.status);
                         P.act[i] = 0;
                     }
                     if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
                 if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
                     cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
-                              out == OUT_NEW ? (double)w : -(double)w);
+                              out == OUT_NEW ? (double)w : -(double)w, C.status);
                 if (out == OUT_NEW) {
                     const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
                     stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                         ch = (double)P.f[6][j] * dep_val;
                     }
                 }
-                cic_fixed_warp(g.qpart, g.nx, g.ny, valid, cl, dx, dy, dz, fx, fy, fz, ch);
+                cic_fixed_warp(g.qpart, g.nx, g.ny, valid, cl, dx, dy, dz, fx, fy, fz, ch, C.status);
             }
         }
 
@@ -806,8 +806,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 if (!sg.act[e] || cl == kOutsideCell) continue;
                 uint32_t ux, uy, uz;
                 cell_split(g, cl, ux, uy, uz);
-                cic_fixed(g.qpart, g.nx, g.ny, (int)ux, (int)uy, (int)uz,
-                          (double)sg.f[0][e], (double)sg.f[1][e], (double)sg.f[2][e], (double)sg.f[6][e] * dep_val);
+                cic_fixed(g.qpart, g.nx, g.ny, (int)ux, (int)uy, (int)uz, (double)sg.f[0][e], (double)sg.f[1][e],
+                          (double)sg.f[2][e], (double)sg.f[6][e] * dep_val, C.status);
             }
         }
         if (C.moments_out) {

@@ -52,13 +52,18 @@ class Streamer:
     electrons: jumc.Population
     efield: object                      # streamer.FieldInterp(grid)
     photons: Optional[jumc.Photons] = None
-    fluid: Optional[object] = None      # fluid.Fluid
+    fluid: Optional[object] = None      # fluid.Fluid: its ne enters poisson!'s charge (poisson.jl:24)
     tracker: Optional[CollisionTracker] = None
+    # the reference's hasfluid (MCStreamer/src/main.jl:173-180): setdne! + euler! run only
+    # when the input has a [needle]; an init-file fluid without one keeps its ne fixed
+    hasfluid: Optional[bool] = None
     log: List[dict] = field(default_factory=list)
 
     def __post_init__(self):
         if self.tracker is None:
             self.tracker = CollisionTracker(self.grid)
+        if self.hasfluid is None:
+            self.hasfluid = self.fluid is not None
 
 
 def poisson_step(s: Streamer, eb: float):
@@ -117,7 +122,7 @@ def nsteps(s: Streamer, n: int, ntarget: int, nmax: int, eb: float, dt: float, d
                     raise AssertionError("resampling is not conserving the number of particles")
             d["resampled"] = True
         tick("fluid")
-        if s.fluid is not None:
+        if s.fluid is not None and s.hasfluid:
             s.fluid.step(dt)
         tick("repack")
         jumc.repack(s.electrons)

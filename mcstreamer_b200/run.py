@@ -182,7 +182,10 @@ def main(finput: str, tmax: Optional[float] = None, run: bool = True, precision:
     if table.has_photoemission:
         photons = jumc.Photons(int(photon_capacity) if photon_capacity is not None else maxp, table.photon_numax,
                                seed=seed + 1, ctx=ctx)
-    s = loop.Streamer(grid, solver, electrons, streamer.FieldInterp(grid), photons, fluid)
+    # main.jl:173-180 sets hasfluid from [needle] alone, after initfromfiles! set it for a
+    # finite fluid_threshold: an init-file fluid without a needle is never stepped
+    s = loop.Streamer(grid, solver, electrons, streamer.FieldInterp(grid), photons, fluid,
+                      hasfluid="needle" in inp)
     outpath = cfg["outpath"]
     iv = inp["interval"]
     steps = cfg["steps"]

@@ -111,11 +111,20 @@ method = "poisson"
 format = "afivo"
 fluid_threshold = 2e19
 """)
+    r0 = main(finput, ctx=ctx, tmax=2e-12, run=False, photon_capacity=2_000_000)
+    try:
+        ne_fluid0 = r0.streamer.fluid.download()[0]
+    finally:
+        r0.close()
     r = main(finput, ctx=ctx, tmax=2e-12, photon_capacity=2_000_000)
     try:
         assert r.steps == 2
         s = r.streamer
         assert s.fluid is not None and (s.fluid.download()[0] > 0).sum() > 0
+        # no [needle]: the reference's hasfluid is false (main.jl:173-180), so the init-file
+        # fluid keeps the density initfromfiles! gave it
+        assert not s.hasfluid
+        np.testing.assert_array_equal(s.fluid.download()[0], ne_fluid0)
         assert s.electrons.nparticles() > 1000
         assert math.isfinite(r.diagnostics[-1]["mean_energy"])
     finally:

@@ -20,7 +20,10 @@ MAX_PARTICLES = 67108864
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_noalloc_moments_match_population_moments_on_two_calls(precision):
+@pytest.mark.parametrize("n", [100_003, 3 * 8192, 0])
+def test_noalloc_moments_match_population_moments_on_two_calls(precision, n):
+    """An uneven size, a size that ends exactly on a chunk boundary (8192 particles per
+    chunk) and the empty population (counts and sums 0, the maximum energy -inf)."""
     import torch
 
     from mcstreamer_b200 import jumc, lxcat
@@ -28,12 +31,14 @@ def test_noalloc_moments_match_population_moments_on_two_calls(precision):
 
     ctx = jumc.Context(0)
     tab = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
-    n = 100_003
-    p = broad(n, 13, spread=1e-4)
-    p.w[:] = np.random.default_rng(5).uniform(0.5, 2.0, n)
+    m = max(n, 1)
+    p = broad(m, 13, spread=1e-4)
+    p.w[:] = np.random.default_rng(5).uniform(0.5, 2.0, m)
     p.active[::5] = 0
-    pop = jumc.Population(n, p, tab, precision=precision, seed=1)
+    pop = jumc.Population(m, p if n else None, tab, precision=precision, seed=1)
     ref = pop.moments()  # the existing entry point, MCS_MOMENTS_BASE sums
+    if n == 0:
+        assert ref[L.M_COUNT] == 0 and ref[L.M_EMAX] == -np.inf
 
     dev = torch.device("cuda:0")
     dtype = torch.float32 if precision == "fp32" else torch.float64
