@@ -42,14 +42,16 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
-    ap.add_argument("--workload", default="cfg1")
+    ap.add_argument("--workload", default="cfg2")
     ap.add_argument("--particles", type=int, default=None, help="override the particle count (per rank)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--e2e-chunks", type=int, default=8, help="chunks of the pipelined host-resident step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-cfg1", action="store_true", help="cfg2: skip the cfg1 kernel sub-record")
+    ap.add_argument("--cap-factor", type=float, default=6.0, help="cfg2: population capacity / initial electrons")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="cfg4: arrival window (s)")
     ap.add_argument("--serve-limit", type=float, default=240.0, help="cfg4: wall-clock limit of the serving run (s)")
@@ -449,20 +451,212 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
 
 
 # ---------------------------------------------------------------------------------------
-# Large streamer step ("cfg2"): 67M electrons on a 512x512x1024 mesh; every 10th step also
-# sorts the population by cell and resamples it to 64 per cell.  As in cfg1 every step
-# starts from the same input cloud (restored device to device outside the timed windows):
-# at 600 Td the population multiplies by about 1.3 per step, so consecutive steps would
-# outgrow any capacity between resamplings.
+# The headline workload ("cfg2", the default): the large streamer run.  67,108,864
+# electrons (log-uniform weights 1e2..1e4, Gaussian cloud sigma 50 um, 1 eV) on a
+# 512x512x1024 mesh (h = 2 um) in the Gaussian-charge field plus -15 MV/m, dt = 2e-13 s,
+# seed 2.  The population evolves from step to step -- ionization grows it by a few per cent
+# a step, the secondaries are staged and appended in parent order, the tracker deposits
+# their ions -- and every 10th step (steps 9, 19, ...) ends with resample!(ntarget = 64,
+# nmax = 96), which sorts by cell first.  W warm-up steps are the first W steps of that run
+# and the K timed steps the next K; a step is zero(qpart) + the fused push/collide/track/
+# deposit launch (+ the resample on its step).
 # ---------------------------------------------------------------------------------------
+CFG2_PERIOD, CFG2_NTARGET, CFG2_NMAX = 10, 64, 96
+
+
+def source_sha(files) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for f in files:
+        h.update((ROOT / f).read_bytes())
+    return h.hexdigest()[:16]
+
+
+def profile_record(name: str) -> Optional[dict]:
+    """A committed per-kernel record (profiles/<name>.json) with the sha of the sources it was
+    measured on; `stale` is set when those sources have changed since."""
+    p = ROOT / "profiles" / f"{name}.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    files = d.get("sources")
+    if files:
+        d["stale"] = source_sha(files) != d.get("source_sha")
+    return d
+
+
+class SubMeshOracle:
+    """The oracle (FP64 restatement, all host threads) stepping a sample of the streamer
+    workload on the box of the mesh within `half` cells of its centre: the node field of that
+    box and two int64 deposit grids of its size (the full 270M-node cfg2 mesh does not fit
+    the oracle's host arrays in a bounded run).  The cloud has sigma 25 cells; a particle
+    beyond the box (over 5 sigma out) sees no field and deposits nothing."""
+
+    def __init__(self, spec, threads: int, half: int = 128):
+        from mcstreamer_b200 import lxcat, workloads
+        from oracle import pyoracle as po
+        self.po, self.spec, self.threads = po, spec, threads
+        self.tab = po.OracleTable.from_lxcat(lxcat.synthetic_table(0))
+        c = (spec.nx // 2, spec.ny // 2, spec.nz // 2)
+        self.i0 = [max(0, ci - half) for ci in c]
+        self.nc = [min(n, ci + half) - i0 for n, ci, i0 in zip((spec.nx, spec.ny, spec.nz), c, self.i0)]
+        self.origin = tuple(spec.h * i for i in self.i0)
+        nx, ny, nz = self.nc
+        fn = workloads.streamer_field_fn(spec)
+        xs = self.origin[0] + spec.h * np.arange(nx + 1)
+        ys = self.origin[1] + spec.h * np.arange(ny + 1)
+        plane = (nx + 1) * (ny + 1)
+        e = np.empty(((nz + 1) * plane, 3))
+        for k0 in range(0, nz + 1, 32):
+            k1 = min(nz + 1, k0 + 32)
+            Z, Y, X = np.meshgrid(self.origin[2] + spec.h * np.arange(k0, k1), ys, xs, indexing="ij")
+            e[k0 * plane:k1 * plane] = fn(X.ravel(), Y.ravel(), Z.ravel())
+        e = e.astype(np.float32).astype(np.float64)        # the device field is FP32
+        self.field = po.field_cart3d(nx, ny, nz, spec.h, self.origin, e.reshape(-1))
+
+    def step(self, op) -> float:
+        po, spec = self.po, self.spec
+        nx, ny, nz = self.nc
+        trk = po.tracker_cart3d(nx, ny, nz, spec.h, self.origin)
+        dep = po.tracker_cart3d(nx, ny, nz, spec.h, self.origin)
+        t0 = time.perf_counter()
+        po.advance(op, self.tab, self.field, spec.dt, tracker=trk, threads=self.threads, clamp=True)
+        po.deposit(op, dep, -1.0)
+        return time.perf_counter() - t0
+
+
+def cfg2_sample(spec, m: int, seed: int):
+    """m electrons of the cfg2 cloud distribution (the device draws the full cloud itself)."""
+    from mcstreamer_b200 import workloads
+    return workloads.streamer_particles(workloads.streamer_spec(spec.name, n=m))
+
+
+def oracle_rate(sub: SubMeshOracle, parts, seconds: float, seed: int) -> dict:
+    """Electron steps/s of the oracle on `parts`, sized down so one step takes about
+    `seconds` (a strided subsample of the given particles)."""
+    po = sub.po
+    probe = min(parts.n, 32768)
+    idx = np.linspace(0, parts.n - 1, probe).astype(np.int64)
+    op = po.OraclePop(parts.x[idx], parts.v[idx], parts.w[idx], parts.s[idx], parts.active[idx], cap=4 * probe,
+                      seed=seed)
+    dt = sub.step(op)
+    m = int(min(parts.n, max(probe, probe * seconds / max(dt, 1e-3))))
+    idx = np.linspace(0, parts.n - 1, m).astype(np.int64)
+    op = po.OraclePop(parts.x[idx], parts.v[idx], parts.w[idx], parts.s[idx], parts.active[idx], cap=4 * m,
+                      seed=seed)
+    active = float(parts.active[idx].sum())
+    dt = sub.step(op)
+    return {"value": active / dt, "unit": UNIT, "cores": sub.threads, "kind": "port", "m": m, "seconds": dt}
+
+
+def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
+    """The same steps through the C ABI with the population in HOST memory (the plain drop-in
+    for a Julia Population): the population entering the first timed step is downloaded into
+    pinned host arrays in the Julia layout (65 B per electron), and mcs_advance_deposit_host
+    steps it in place -- uploads, fused steps and downloads pipelined over chunks -- after
+    which the deposit grid is read back to pinned host memory, every step.  No resample! is
+    called (the library has no host-resident resample; it is one step in ten of the device
+    run)."""
+    import ctypes as C
+
+    from mcstreamer_b200 import jumc
+    n = pop.nparticles()
+    cap = int(n * 1.25) + 1024
+    chunks = max(1, args.e2e_chunks)
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    x, v = pinned((cap, 3), torch.float64), pinned((cap, 3), torch.float64)
+    w, s, a = pinned((cap,), torch.float64), pinned((cap,), torch.float64), pinned((cap,), torch.uint8)
+    hq = pinned((spec.nodes,), torch.int64)
+    nn = C.c_int64()
+    lib = ctx.lib
+    ctx.check(lib.mcs_pop_download(pop.h, L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), cap, C.byref(nn)))
+    work = jumc.Population(int(1.5 * ((cap + chunks - 1) // chunks)) + 4096, None, pop.collisions, precision="fp32",
+                           seed=spec.seed, mesh=grid)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = active = 0.0
+    h2d = d2h = 0
+    for k in range(args.e2e_steps + 1):
+        n_in = nn.value
+        act_in = float(a[:n_in].sum())
+        torch.cuda.synchronize()
+        t0.record(stream)
+        grid.zero(L.Q_PART)
+        ctx.check(lib.mcs_advance_deposit_host(work.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0,
+                                               L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), C.byref(nn),
+                                               cap, chunks))
+        ctx.check(lib.mcs_grid_read_fixed(grid.h_, L.Q_PART, L.i64ptr(hq)))
+        t1.record(stream)
+        torch.cuda.synchronize()
+        if k == 0:
+            continue   # warm-up: the workspace's staging buffers are allocated here
+        ms += t0.elapsed_time(t1)
+        active += act_in
+        h2d += n_in * 65
+        d2h += nn.value * 65 + spec.nodes * 8
+    work.close()
+    steps = args.e2e_steps
+    m = nn.value
+    host = jumc.ParticleArrays(x[:m], v[:m], w[:m], s[:m], a[:m])
+    return host, {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // steps,
+            "d2h_bytes_per_step": d2h // steps, "steps": steps, "electrons_at_start": n,
+            "path": f"mcs_advance_deposit_host on pinned host arrays in the Julia layout ({chunks} chunks: uploads, "
+                    "fused steps and downloads pipelined on three streams) + mcs_grid_read_fixed of the 2.15 GB "
+                    "deposit grid, every step; the population entering the first timed step, evolving; CUDA "
+                    "events around each step; no resample! (no host-resident entry point)"}
+
+
+def cfg1_kernel_record(ctx, table, stream, torch, L, steps: int = 20, warmup: int = 5) -> dict:
+    """cfg1's kernel datum (4,194,304 electrons, 128x128x256 mesh, every step over the same
+    1 eV input cloud restored device to device outside the windows)."""
+    from mcstreamer_b200 import jumc, streamer, workloads
+    spec = workloads.streamer_spec("cfg1")
+    grid = streamer.Grid3D(spec.nx, spec.ny, spec.nz, spec.h, precision="fp32", ctx=ctx)
+    grid.set_efield_gaussian(spec.centre, workloads.CHARGE_SIGMA, workloads.CHARGE_PEAK, workloads.E_BACKGROUND)
+    snap = jumc.Population(spec.n, None, table, precision="fp32", seed=spec.seed, mesh=grid)
+    snap.init_cloud(spec.n, spec.centre, workloads.CLOUD_SIGMA, workloads.CLOUD_ENERGY_EV, *spec.weight)
+    ctx.check(ctx.lib.mcs_sort_cells(snap.h, grid.h_))
+    pop = jumc.Population(2 * spec.n, None, table, precision="fp32", seed=spec.seed, mesh=grid)
+    fld, trk = streamer.FieldInterp(grid), streamer.CollisionTracker(grid)
+    grid.zero(L.Q_FIXED)
+    kms = []
+    for k in range(warmup + steps):
+        ctx.check(ctx.lib.mcs_pop_copy(pop.h, snap.h))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        grid.zero(L.Q_PART)
+        e0.record(stream)
+        streamer.advance_deposit(pop, fld, spec.dt, trk, grid, -1.0)
+        e1.record(stream)
+        if k >= warmup:
+            kms.append((e0, e1))
+    torch.cuda.synchronize()
+    ctx.sync()
+    km = float(np.mean([a.elapsed_time(b) for a, b in kms]))
+    alg = alg_bytes_per_launch(spec.n, 0.0, spec.nodes)
+    fld.close()
+    pop.close(); snap.close(); grid.close()
+    return {"workload": "cfg1: 4,194,304 electrons (w 1e3) on 128x128x256 cells, h 4 um, 1 eV cloud restored before "
+                        "each step", "kernel_ms": km, "electron_steps_per_s": spec.n / (km * 1e-3),
+            "alg_bytes_per_launch": alg, "achieved_gbs": alg / (km * 1e-3) / 1e9}
+
+
 def run_cfg2(args):
     import torch
 
     from mcstreamer_b200 import _lib as L
+    from mcstreamer_b200 import dist as mdist
     from mcstreamer_b200 import jumc, lxcat, streamer, workloads
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     spec = workloads.streamer_spec("cfg2", n=args.particles)
     ctx = jumc.Context(local)
     stream = torch.cuda.current_stream()
@@ -471,84 +665,216 @@ def run_cfg2(args):
     grid = streamer.Grid3D(spec.nx, spec.ny, spec.nz, spec.h, precision="fp32", ctx=ctx)
     t_setup = time.perf_counter()
     grid.set_efield_gaussian(spec.centre, workloads.CHARGE_SIGMA, workloads.CHARGE_PEAK, workloads.E_BACKGROUND)
-    snap = jumc.Population(spec.n, None, table, precision="fp32", seed=spec.seed, mesh=grid)
-    snap.init_cloud(spec.n, spec.centre, workloads.CLOUD_SIGMA, workloads.CLOUD_ENERGY_EV, *spec.weight)
-    ctx.check(ctx.lib.mcs_sort_cells(snap.h, grid.h_))
-    pop = jumc.Population(3 * spec.n, None, table, precision="fp32", seed=spec.seed, mesh=grid)
-    ctx.sync()
-    t_setup = time.perf_counter() - t_setup
+    seed = spec.seed + 1000 * rank
+    cap = int(args.cap_factor * spec.n)
+    pop = jumc.Population(cap, None, table, precision="fp32", seed=seed, mesh=grid)
+    pop.init_cloud(spec.n, spec.centre, workloads.CLOUD_SIGMA, workloads.CLOUD_ENERGY_EV, *spec.weight)
+    ctx.check(ctx.lib.mcs_sort_cells(pop.h, grid.h_))
     fld = streamer.FieldInterp(grid)
     trk = streamer.CollisionTracker(grid)
-    ntarget, nmax, period = 64, 96, 10
-    ctx.check(ctx.lib.mcs_pop_step_log(pop.h, 1))
+    qpart = torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}") if ws > 1 else None
+    grid.zero(L.Q_FIXED)
+    total = args.warmup + args.steps
+    ctx.check(ctx.lib.mcs_pop_step_log(pop.h, total))
+    ctx.sync()
+    t_setup = time.perf_counter() - t_setup
 
-    def one(k, ev):
-        ctx.check(ctx.lib.mcs_pop_copy(pop.h, snap.h))
+    act_in = [float(spec.n)]            # active electrons entering step k
+    resampled = {}                      # step -> active electrons after its resample!
+
+    def step(k, ev):
         ev[0].record(stream)
         grid.zero(L.Q_PART)
         ev[1].record(stream)
         streamer.advance_deposit(pop, fld, spec.dt, trk, grid, -1.0)
         ev[2].record(stream)
-        if (k + 1) % period == 0:   # resample! sorts the population by cell first
-            ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, ntarget, nmax))
+        if qpart is not None:
+            mdist.allreduce_int64_(qpart)
+        if (k + 1) % CFG2_PERIOD == 0:      # resample! sorts the population by cell first
+            ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, CFG2_NTARGET, CFG2_NMAX))
         ev[3].record(stream)
 
-    grid.zero(L.Q_FIXED)
-    warm = max(args.warmup, period)
-    for k in range(warm):
-        one(k, [torch.cuda.Event(enable_timing=True) for _ in range(4)])
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(total)]
+    for k in range(args.warmup):
+        step(k, evs[k])
+        if (k + 1) % CFG2_PERIOD == 0:     # outside the step windows: the count entering step k+1
+            resampled[k] = float(pop.moments()[L.M_COUNT])
     torch.cuda.synchronize()
     ctx.sync()
-    steps = max(period, (args.steps // period) * period)
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    n_first = pop.nparticles()
     with ClockSampler(local) as clk:
-        for k in range(steps):
-            one(warm + k, evs[k])
+        for k in range(args.warmup, total):
+            step(k, evs[k])
+            if (k + 1) % CFG2_PERIOD == 0:
+                resampled[k] = float(pop.moments()[L.M_COUNT])
         torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
     ctx.sync()
-    log = np.zeros((1, L.STEP_MOMENTS))
-    ctx.check(ctx.lib.mcs_pop_read_step_log(pop.h, L.dptr(log), 1))
-    n_post = float(log[0, L.S_COUNT])
-    after = pop.nparticles()
-    step_ms = [e[0].elapsed_time(e[3]) for e in evs]
-    kern_ms = [e[1].elapsed_time(e[2]) for e in evs]
-    res_ms = [e[2].elapsed_time(e[3]) for k, e in enumerate(evs) if (warm + k + 1) % period == 0]
-    total_ms = float(sum(step_ms))
-    value = spec.n * steps / (total_ms * 1e-3)
+    log = np.zeros((total, L.STEP_MOMENTS))
+    ctx.check(ctx.lib.mcs_pop_read_step_log(pop.h, L.dptr(log), total))
+    post = log[:, L.S_COUNT]
+    for k in range(1, total):
+        act_in.append(resampled.get(k - 1, post[k - 1]))
+    timed = range(args.warmup, total)
+    step_ms = float(sum(evs[k][0].elapsed_time(evs[k][3]) for k in timed))
+    bracket_ms = evs[args.warmup][0].elapsed_time(evs[total - 1][3])
+    kern = [evs[k][1].elapsed_time(evs[k][2]) for k in timed]
+    res_ms = [evs[k][2].elapsed_time(evs[k][3]) for k in timed if (k + 1) % CFG2_PERIOD == 0]
+    active_timed = float(sum(act_in[k] for k in timed))
+    sec = [post[k] - act_in[k] for k in timed]
+    clocks = clk.summary()
+
+    if dist is not None:
+        t = torch.tensor([step_ms, active_timed, bracket_ms], device=f"cuda:{local}", dtype=torch.float64)
+        mx, sm = t.clone(), t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_max, active_all, bracket_max = float(mx[0]), float(sm[1]), float(mx[2])
+    else:
+        ms_max, active_all, bracket_max = step_ms, active_timed, bracket_ms
+    value = active_all / (ms_max * 1e-3)
+    kmean = float(np.mean(kern))
+    mean_in = float(np.mean([act_in[k] for k in timed]))
+    mean_sec = float(np.mean(sec))
     pk, pk_kind = peaks()
     hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
-    kmean = float(np.mean(kern_ms))
-    alg = alg_bytes_per_launch(spec.n, max(0.0, n_post - spec.n), spec.nodes)
+    alg = alg_bytes_per_launch(mean_in, max(0.0, mean_sec), spec.nodes)
+    alg_particles = alg_bytes_per_launch(mean_in, max(0.0, mean_sec), 0)
     achieved = alg / (kmean * 1e-3) / 1e9
+    tr = profile_record("traffic_k_step_mesh_cfg2")
+    issue = profile_record("issue_k_step_mesh_cfg1")
+
+    e2e = host = None
+    if args.e2e_steps > 0 and ws == 1:
+        host, e2e = cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L)
     cpu = None
-    if not args.no_cpu:
-        cpu = cpu_sample(workloads.streamer_spec("cfg1"), args.cpu_seconds, os.cpu_count() or 1)
-        cpu["sample"] = "cfg1 cloud and mesh (the 270M-node cfg2 field does not fit the oracle's host arrays " \
-                        "within the bench's time; same gas, field and per-electron work): " + cpu["sample"]
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        # one oracle step of a strided sample of the evolved population (the host copy the
+        # e2e leg stepped, else a download)
+        parts = host if host is not None else pop.download()
+        sub = SubMeshOracle(spec, os.cpu_count() or 1)
+        r = oracle_rate(sub, parts, args.cpu_seconds, seed)
+        cpu = {k: r[k] for k in ("value", "unit", "cores", "kind")}
+        cpu["sample"] = (f"1 step (advance! + tracker + density!) of {r['m']} electrons taken evenly from the "
+                         f"{parts.n} of the evolved cfg2 population, FP64 oracle on {r['cores']} threads, on the "
+                         f"{sub.nc[0]}x{sub.nc[1]}x{sub.nc[2]}-cell box of the mesh around the cloud, "
+                         f"{r['seconds']:.2f} s")
+    cfg1 = None
+    if rank == 0 and not args.no_cfg1:
+        cfg1 = cfg1_kernel_record(ctx, table, stream, torch, L)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": f"streamer run cfg2: {spec.nx}x{spec.ny}x{spec.nz} mesh h={spec.h:g} m, {spec.n} electrons "
+                            f"per GPU at the start (w log-uniform {spec.weight[0]:g}..{spec.weight[1]:g}, Gaussian "
+                            f"cloud sigma=50um, 1 eV), Gaussian charge sigma=40um peak 1e20 e/m^3 + -15 MV/m, "
+                            f"synthetic gas 0, dt={spec.dt:g} s, seed {spec.seed}; the population evolves; "
+                            f"resample!(ntarget={CFG2_NTARGET}, nmax={CFG2_NMAX}) after every {CFG2_PERIOD}th step; "
+                            f"warm-up = steps 0..{args.warmup - 1}, timed = steps {args.warmup}..{total - 1}",
+                "electrons_entering_first_timed_step": act_in[args.warmup], "slots_at_first_timed_step": n_first,
+                "mean_active_per_timed_step": mean_in, "secondaries_per_step": mean_sec,
+                "secondaries_note": "post-step minus entering active electrons (ionizations minus attachments)",
+                "active_per_step": [act_in[k] for k in range(total)],
+                "step_kernel_ms": kmean, "resample_ms": res_ms,
+                "capacity_slots": cap, "setup_s": t_setup,
+                "l2": "inputs larger than L2 (>= 67M electrons x 37 B = 2.5 GB, mesh 4.3 GB field + 2.15 GB charges)",
+                "step_timing": "CUDA events around each step (zero(qpart) + fused step kernel (+ int64 all-reduce) "
+                               "+ resample! on its steps), summed over the K timed steps; the active-electron "
+                               "count read after a resample! lies between two steps' windows",
+                "ms_per_step_bracket": bracket_max / args.steps,
+                "parallelism": f"dp{ws} (independent clouds, int64 all-reduce of the deposit grid)" if ws > 1
+                               else "1 GPU",
+            },
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": tr.get("bytes_per_launch") if tr and not tr.get("stale") else None,
+                         "traffic_source": (tr.get("note") if tr else None),
+                         "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
+                         "alg_bytes_per_launch": alg, "alg_bytes_particles_only": alg_particles,
+                         "frac_particles_only": alg_particles / (kmean * 1e-3) / 1e9 / hbm,
+                         "alg_note": "70 B per entering electron + 37 B per secondary + 28 B per mesh node (field "
+                                     "read, charge read-modify-write) per launch; the cloud covers about 1 % of "
+                                     "the mesh, so the node term is an upper bound",
+                         "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "issue": issue_roofline_from(issue, mean_in, kmean, clocks)},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "cfg1": cfg1,
+            "clocks": clocks,
+            "gpu_launches": args.steps * 2 + sum(1 for k in timed if (k + 1) % CFG2_PERIOD == 0) * 21,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def issue_roofline_from(rec: Optional[dict], n_active: float, kernel_ms: float, clocks) -> Optional[dict]:
+    """Warp instructions per electron step from a committed ncu record (only when the kernel's
+    sources are unchanged since the capture) against one instruction per cycle on each of the
+    4 schedulers of every SM at the sampled clock."""
+    if not rec or rec.get("stale") or not clocks or not clocks.get("sm_mhz") or not kernel_ms:
+        return {"available": False, "why": "no ncu record for the current kernel sources"} if rec else None
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:
+        return None
+    per = rec["warp_inst_per_electron_step"]
+    achieved = per * n_active / (kernel_ms * 1e-3)
+    peak = sms * 4 * clocks["sm_mhz"] * 1e6
+    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
+            "frac": achieved / peak, "warp_inst_per_electron_step": per, "source": rec.get("note")}
+
+
+def run_reference_cfg2(args):
+    """The oracle on the cfg2 workload: a sample of the cfg2 cloud on the mesh box around it,
+    evolved W untimed steps and then K timed steps (each a bounded sample), all host threads."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    from mcstreamer_b200 import workloads
+    spec = workloads.streamer_spec("cfg2")
+    threads = os.cpu_count() or 1
+    sub = SubMeshOracle(spec, threads)
+    per_step = min(2.0, max(0.5, 60.0 / max(1, args.steps + args.warmup)))
+    parts = cfg2_sample(spec, 32768, spec.seed)
+    probe = sub.po.OraclePop(parts.x, parts.v, parts.w, parts.s, parts.active, cap=4 * parts.n, seed=spec.seed)
+    dt = sub.step(probe)
+    m = int(max(32768, 32768 * per_step / max(dt, 1e-3)))
+    parts = cfg2_sample(spec, m, spec.seed)
+    cap = 8 * m
+    op = sub.po.OraclePop(parts.x, parts.v, parts.w, parts.s, parts.active, cap=cap, seed=spec.seed)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        if op.n > cap // 2:
+            break
+        act = float(op.active[:op.n].sum())
+        t = sub.step(op)
+        sub.po.repack(op)
+        if k >= args.warmup:
+            vals.append(act / t)
+    v = statistics.median(vals) if vals else None
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warm,
-        "ms_per_step": total_ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {
-            "workload": f"streamer step cfg2: {spec.nx}x{spec.ny}x{spec.nz} mesh h={spec.h:g} m, {spec.n} electrons "
-                        f"(w log-uniform {spec.weight[0]:g}..{spec.weight[1]:g}), Gaussian cloud sigma=50um, 1 eV, "
-                        f"synthetic gas 0, dt={spec.dt:g} s, one push+collide+track+deposit launch per step over the "
-                        f"same input cloud, cell sort + resample!(ntarget={ntarget}, nmax={nmax}) of the post-step "
-                        f"population every {period} steps, seed {spec.seed}",
-            "post_step_particles": n_post, "after_resample": after,
-            "step_kernel_ms": kmean, "sort_plus_resample_ms": float(np.mean(res_ms)) if res_ms else None,
-            "setup_s": t_setup, "l2": "inputs larger than L2 (67M electrons x 37 B = 2.5 GB)",
-            "step_timing": "CUDA events around zero(qpart) + step kernel (+ resample!, which sorts by cell first, on "
-                           "every 10th step), summed; the restore of the input cloud is outside the windows",
-            "parallelism": "1 GPU",
-        },
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
-                     "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
-        "cpu_baseline": cpu,
-        "e2e": None,
-        "clocks": clk.summary(),
-        "gpu_launches": steps + (steps // period) * 21,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(vals),
+        "warmup": args.warmup, "ms_per_step": 1e3 * spec.n / v if v else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "streamer run cfg2 (oracle on a sample of the cloud, evolving)", "sample_start": m,
+                   "mesh_box": sub.nc, "h": spec.h, "dt": spec.dt},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{m} electrons of the cfg2 cloud distribution stepped by the FP64 oracle "
+                                   f"(advance! + tracker + density!, repack!) on the {sub.nc[0]}x{sub.nc[1]}x"
+                                   f"{sub.nc[2]}-cell box of the mesh around the cloud; median over the timed steps"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -1961,8 +2287,8 @@ def main():
     args = parse()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "cfg2" and args.impl == "mine":
-        return run_cfg2(args)
+    if args.workload == "cfg2":
+        return run_reference_cfg2(args) if args.impl == "reference" else run_cfg2(args)
     if args.workload == "cfg3":
         return run_reference_batch(args) if args.impl == "reference" else run_batch(args)
     if args.workload == "poisson":
