@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-cfg1", action="store_true", help="cfg2: skip the cfg1 kernel sub-record")
     ap.add_argument("--cap-factor", type=float, default=6.0, help="cfg2: population capacity / initial electrons")
+    ap.add_argument("--replicas", type=int, default=16, help="cfg0: device replicas per precision")
+    ap.add_argument("--oracle-replicas", type=int, default=4, help="cfg0: oracle replicas")
+    ap.add_argument("--cfg0-steps", type=int, default=2000, help="cfg0: steps per run")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="cfg4: arrival window (s)")
     ap.add_argument("--serve-limit", type=float, default=240.0, help="cfg4: wall-clock limit of the serving run (s)")
@@ -877,6 +880,126 @@ def run_reference_cfg2(args):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------------------
+# The plain swarm ("cfg0"): Swarm.swarm at 100 Td -- 65,536 electrons of the synthetic gas
+# 0 at N = 2.5e25 m^-3, 1 eV Maxwellian start, dt = 1e-13 s, 2000 steps, Swarm.resample!
+# to 65,536 (tol 0.1, repack! every step), seeds 0..R-1 -- on the device in FP32 and FP64,
+# and the same runs by the FP64 oracle on the host.  The line reports every coefficient of
+# Swarm.jl:144-161 (W, D_L, D_T, <eps>, k_ion, nu, alpha, eta) with the replica 3 sigma and
+# the FP32 relative error against the oracle.
+# ---------------------------------------------------------------------------------------
+CFG0 = dict(n0=65_536, en_td=100.0, density=2.5e25, dt=1e-13, nt=2000, tol=0.1)
+CFG0_KEYS = ("drift", "diffusion_l", "diffusion_t", "mean_energy", "k_ion", "nu", "alpha", "eta")
+
+
+def cfg0_row(r, table_proc, density):
+    from mcstreamer_b200 import _lib as L
+    ion = [j for j, p in enumerate(table_proc) if p.kind in (L.IONIZATION, L.IONIZATION_UNIFORM)]
+    return {"drift": r.drift, "diffusion_l": r.diffusion_l, "diffusion_t": r.diffusion_t,
+            "mean_energy": r.mean_energy, "k_ion": float(r.k[ion[0]]) / density, "nu": r.nu, "alpha": r.alpha,
+            "eta": r.eta}
+
+
+def cfg0_stats(rows):
+    out = {}
+    for k in CFG0_KEYS:
+        a = np.array([r[k] for r in rows], dtype=np.float64)
+        out[k] = (float(a.mean()), float(3.0 * a.std(ddof=1) / np.sqrt(len(a))) if len(a) > 1 else float("inf"))
+    return out
+
+
+def cfg0_oracle(seed: int, table, steps: int, n0: int, threads: int):
+    from mcstreamer_b200 import constants as co
+    from mcstreamer_b200 import swarm
+    from oracle import pyoracle as po
+    ot = po.OracleTable.from_lxcat(table)
+    eb = CFG0["en_td"] * co.Td * CFG0["density"]
+    p = swarm.initial_particles(n0, "maxwellian", seed)
+    op = po.OraclePop(p.x, p.v, p.w, p.s, p.active, cap=4 * n0, seed=seed)
+    mom, fin = po.swarm_run(op, ot, po.field_uniform(0, 0, eb), CFG0["dt"], steps, n0, CFG0["tol"], 1, threads)
+    return swarm.coefficients(CFG0["en_td"], eb, CFG0["dt"], mom, fin, table.proc)
+
+
+def run_cfg0(args):
+    import torch
+
+    from mcstreamer_b200 import jumc, lxcat, swarm
+    torch.cuda.set_device(0)
+    lt = lxcat.synthetic_table(0)
+    ctx = jumc.Context(0)
+    tab = jumc.CollisionTable(lt, ctx)
+    n0, nt = CFG0["n0"], args.cfg0_steps
+    reps, oreps = args.replicas, args.oracle_replicas
+    rows = {"fp32": [], "fp64": []}
+    res = {"fp32": [], "fp64": []}
+    secs = {}
+    for prec in ("fp32", "fp64"):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in range(reps):
+            r = swarm.swarm_one(tab, CFG0["en_td"], CFG0["density"], n0, CFG0["dt"], nt, maxp=4 * n0,
+                                precision=prec, seed=s, init="maxwellian", tol=CFG0["tol"])
+            res[prec].append(r)
+            rows[prec].append(cfg0_row(r, tab.proc, CFG0["density"]))
+        secs[prec] = time.perf_counter() - t0
+    threads = os.cpu_count() or 1
+    os.environ["ORACLE_THREADS"] = str(threads)
+    t0 = time.perf_counter()
+    orows, ores = [], []
+    for s in range(oreps):
+        r = cfg0_oracle(s, lt, nt, n0, threads)
+        ores.append(r)
+        orows.append(cfg0_row(r, tab.proc, CFG0["density"]))
+    osec = time.perf_counter() - t0
+    # the FP64 device runs follow the oracle's trajectories: same seeds, same coefficients
+    same = {k: max(abs(rows["fp64"][s][k] - orows[s][k]) / max(abs(orows[s][k]), 1e-300) for s in range(oreps))
+            for k in CFG0_KEYS}
+    st32, st64, sto = cfg0_stats(rows["fp32"]), cfg0_stats(rows["fp64"]), cfg0_stats(orows)
+    coeff = {}
+    for k in CFG0_KEYS:
+        m32, e32 = st32[k]
+        mo, eo = sto[k]
+        both = float(np.hypot(e32, eo))
+        coeff[k] = {"fp32": m32, "fp32_3sigma": e32, "fp64_device": st64[k][0], "fp64_device_3sigma": st64[k][1],
+                    "oracle_fp64": mo, "oracle_3sigma": eo,
+                    "fp32_rel_err_vs_oracle": (m32 - mo) / mo if mo else None,
+                    "within_3sigma": bool(abs(m32 - mo) <= both),
+                    "fp64_device_vs_oracle_same_seeds_max_rel": same[k]}
+    half = nt // 2
+    tavg = {}
+    for key in ("drift", "mean_energy"):
+        a32 = np.array([swarm.time_averages(r, half)[key] for r in res["fp32"]])
+        ao = np.array([swarm.time_averages(r, half)[key] for r in ores])
+        m32, e32 = float(a32.mean()), float(3 * a32.std(ddof=1) / np.sqrt(len(a32)))
+        mo, eo = float(ao.mean()), (float(3 * ao.std(ddof=1) / np.sqrt(len(ao))) if len(ao) > 1 else float("inf"))
+        tavg[key] = {"fp32": m32, "fp32_3sigma": e32, "oracle_fp64": mo, "oracle_3sigma": eo,
+                     "fp32_rel_err_vs_oracle": (m32 - mo) / mo, "within_3sigma": bool(abs(m32 - mo) <= np.hypot(e32, eo))}
+    electron_steps = sum(float(r.counts.sum()) for r in res["fp32"])
+    line = {
+        "metric": METRIC, "value": electron_steps / secs["fp32"], "unit": UNIT, "n_gpus": 1, "steps": nt,
+        "warmup": 0, "ms_per_step": 1e3 * secs["fp32"] / (reps * nt), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain swarm cfg0: {n0} electrons, {CFG0['en_td']:g} Td, N={CFG0['density']:g} m^-3, "
+                               f"synthetic gas 0, 1 eV Maxwellian start, dt={CFG0['dt']:g} s, {nt} steps, "
+                               f"Swarm.resample!({n0}, {CFG0['tol']}) + repack! every step, seeds 0..{reps - 1} "
+                               f"(device) and 0..{oreps - 1} (oracle)",
+                   "replicas": reps, "oracle_replicas": oreps, "device_fp32_s": secs["fp32"],
+                   "device_fp64_s": secs["fp64"], "oracle_s": osec, "oracle_threads": threads,
+                   "timing": "wall clock of the replicas' mcs_swarm_run calls (each synchronises)"},
+        "coefficients": coeff,
+        "time_averaged_second_half": tavg,
+        "units": {"drift": "m/s", "diffusion_l": "m^2/s", "diffusion_t": "m^2/s", "mean_energy": "J",
+                  "k_ion": "m^3/s", "nu": "1/s", "alpha": "1/m", "eta": "1/m"},
+        "cpu_baseline": {"value": sum(float(r.counts.sum()) for r in ores) / osec, "unit": UNIT, "cores": threads,
+                         "kind": "port", "sample": f"{oreps} full replicas of the same runs, FP64 oracle"},
+        "e2e": None, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    tab.close()
+    ctx.close()
     return 0
 
 
@@ -2289,6 +2412,12 @@ def main():
         args.warmup = 3
     if args.workload == "cfg2":
         return run_reference_cfg2(args) if args.impl == "reference" else run_cfg2(args)
+    if args.workload == "cfg0":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the oracle replicas run inside the cfg0 line "
+                              "(cpu_baseline); no separate reference arm"}))
+            return 0
+        return run_cfg0(args)
     if args.workload == "cfg3":
         return run_reference_batch(args) if args.impl == "reference" else run_batch(args)
     if args.workload == "poisson":

@@ -74,6 +74,7 @@ class SwarmResult:
     steps: int
     sigma2: np.ndarray = field(repr=False, default=None)
     counts: np.ndarray = field(repr=False, default=None)
+    sums: np.ndarray = field(repr=False, default=None)    # the per-step sums (nt, MCS_STEP_MOMENTS)
 
 
 def initial_particles(n0: int, init: str, seed: int, mean_ev: float = 1.0) -> ParticleArrays:
@@ -90,6 +91,38 @@ def initial_particles(n0: int, init: str, seed: int, mean_ev: float = 1.0) -> Pa
     return p
 
 
+def coefficients(en_td: float, eb: float, dt: float, mom: np.ndarray, mfin: np.ndarray, proc,
+                 l: int = 100) -> SwarmResult:
+    """The Swarm.swarm estimators (Swarm.jl:124-161) from the per-step sums of the run
+    (mom, (nt, MCS_STEP_MOMENTS): sigma^2(t) of the active electrons) and the moments of the
+    final population (mfin, MCS_MOMENTS_BASE + one rate sum per table row): D from the
+    least-squares slope of the last l sigma^2, W = <v_z>, k_j = <nu_j(eps)> and nu, alpha,
+    eta of the final population; the weighted mean energy."""
+    nt = len(mom)
+    cnt = mom[:, L.S_COUNT]
+    X = mom[:, L.S_X:L.S_X + 3] / cnt[:, None]
+    X2 = mom[:, L.S_X2:L.S_X2 + 3] / cnt[:, None]
+    sigma2 = X2 - X ** 2
+    t = np.arange(nt) * dt
+    D = diffusion_fit(t, sigma2, min(l, nt))
+    W = mfin[L.M_V + 2] / mfin[L.M_COUNT]
+    k = mfin[L.MOMENTS_BASE:L.MOMENTS_BASE + len(proc)] / mfin[L.M_COUNT]
+    g = gains(proc)
+    return SwarmResult(
+        en=en_td, mobility=-W / eb, diffusion_l=D[2], diffusion_t=(D[0] + D[1]) / 2,
+        diffusion=(D[0] + D[1] + D[2]) / 3, nu=float(g @ k), alpha=float(np.maximum(g, 0) @ k / abs(W)),
+        eta=float(-np.minimum(g, 0) @ k / abs(W)), drift=W, mean_energy=mfin[L.M_WE] / mfin[L.M_W], k=k,
+        steps=nt, sigma2=sigma2, counts=cnt, sums=mom)
+
+
+def time_averages(r: SwarmResult, start: int) -> dict:
+    """Drift <v_z> and mean energy per electron averaged over steps [start, nt) of the per-step
+    sums: tighter estimates than the final-population values of Swarm.jl:152-156."""
+    m = r.sums[start:]
+    c = m[:, L.S_COUNT]
+    return {"drift": float(np.mean(m[:, L.S_V + 2] / c)), "mean_energy": float(np.mean(m[:, L.S_E] / c))}
+
+
 def swarm_one(table: CollisionTable, en_td: float, density: float, n0: int, dt: float, nt: int,
               maxp: Optional[int] = None, precision: str = "fp64", seed: int = 0, init: str = "cold",
               resampling: bool = True, tol: float = 0.1, l: int = 100, repack_every: int = 1) -> SwarmResult:
@@ -104,21 +137,7 @@ def swarm_one(table: CollisionTable, en_td: float, density: float, n0: int, dt: 
         mom = np.zeros((nt, L.STEP_MOMENTS))
         ctx.check(ctx.lib.mcs_swarm_run(pop.h, table.h, fld.h, dt, nt, n0 if resampling else 0, tol,
                                         repack_every, L.dptr(mom)))
-        cnt = mom[:, L.S_COUNT]
-        X = mom[:, L.S_X:L.S_X + 3] / cnt[:, None]
-        X2 = mom[:, L.S_X2:L.S_X2 + 3] / cnt[:, None]
-        sigma2 = X2 - X ** 2
-        t = np.arange(nt) * dt
-        D = diffusion_fit(t, sigma2, min(l, nt))
-        mfin = pop.moments(table)
-        W = mfin[L.M_V + 2] / mfin[L.M_COUNT]
-        k = mfin[L.MOMENTS_BASE:L.MOMENTS_BASE + len(table)] / mfin[L.M_COUNT]
-        g = gains(table.proc)
-        return SwarmResult(
-            en=en_td, mobility=-W / eb, diffusion_l=D[2], diffusion_t=(D[0] + D[1]) / 2,
-            diffusion=(D[0] + D[1] + D[2]) / 3, nu=float(g @ k), alpha=float(np.maximum(g, 0) @ k / abs(W)),
-            eta=float(-np.minimum(g, 0) @ k / abs(W)), drift=W, mean_energy=mfin[L.M_WE] / mfin[L.M_W], k=k,
-            steps=nt, sigma2=sigma2, counts=cnt)
+        return coefficients(en_td, eb, dt, mom, pop.moments(table), table.proc, l)
     finally:
         fld.close()
         pop.close()

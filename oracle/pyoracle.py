@@ -292,3 +292,25 @@ def efield(field, x):
     e = np.zeros(3)
     lib().orc_efield(C.byref(field), x.ctypes.data_as(pd), e.ctypes.data_as(pd))
     return e
+
+
+def swarm_run(pop: OraclePop, table: OracleTable, field, dt: float, nt: int, n0: int, tol: float = 0.1,
+              repack_every: int = 1, threads=None):
+    """The oracle's Swarm.swarm time loop (Swarm/src/Swarm.jl:124-142): per step advance!, the
+    sums of the active electrons (the first 12 moments: count, sum w, x, x^2, v, energy), then
+    Swarm.resample!(n0, tol) and repack!; returns the (nt, 12) per-step sums and the moments
+    (with the rate sums of `table`) of the final population."""
+    nrows = table.s.nrows
+    mom = np.zeros((nt, 12))
+    buf = np.zeros(18 + nrows)
+    for i in range(nt):
+        st = advance(pop, table, field, dt, threads=threads)
+        if st:
+            raise RuntimeError(f"oracle advance! status {st}")
+        mom[i] = moments(pop)[:12]
+        if n0 > 0:
+            swarm_resample(pop, n0, tol)
+        if repack_every > 0 and (i + 1) % repack_every == 0:
+            repack(pop)
+    buf[:] = moments(pop, table)
+    return mom, buf
