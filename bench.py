@@ -1076,9 +1076,20 @@ def run_batch(args):
     from mcstreamer_b200 import jumc, lxcat, workloads
     from mcstreamer_b200.batch import SwarmBatch
 
+    from mcstreamer_b200 import dist as mdist
+
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     spec = workloads.batched_swarms()
+    # instances are independent: each rank steps its share (dealt by predicted work), no
+    # collective on the data path
+    mine = mdist.my_instances((spec.n * spec.steps).tolist(), rank, ws)
     ctx = jumc.Context(local, clamp_energy=True)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -1090,7 +1101,7 @@ def run_batch(args):
         """Join every instance: electrons drawn on the device, or (host=True) generated on
         the host and uploaded in the Julia layout.  Returns the host->device bytes."""
         nbytes = 0
-        for k in range(spec.k):
+        for k in mine:
             if host:
                 p0 = workloads.swarm_instance_particles(spec, k)
                 b.add(tables[int(spec.gas[k])], float(ez[k]), int(spec.seeds[k]), int(spec.n[k]), int(caps[k]), p0)
@@ -1101,7 +1112,8 @@ def run_batch(args):
         return nbytes
 
     # autotune on a batch a few steps into the run, then a fresh batch for the timed solve
-    b = SwarmBatch(ctx, spec.k, int(caps.sum()))
+    my_caps = int(caps[mine].sum())
+    b = SwarmBatch(ctx, len(mine), my_caps)
     fill(b)
     b.step(spec.dt, args.warmup, graph=True)
     chosen, times = b.autotune(spec.dt, trial_steps=2)
@@ -1110,11 +1122,13 @@ def run_batch(args):
     b.close()
     # the timed region: every instance's whole solve, spec.steps batched steps from the 1 eV
     # Maxwellian start, in CUDA-graph chunks of 100 steps
-    b = SwarmBatch(ctx, spec.k, int(caps.sum()))
+    b = SwarmBatch(ctx, len(mine), my_caps)
     b.set_variant(chosen)
     fill(b)
     b.sync()
-    n_start = float(spec.n.sum())
+    n_start = float(spec.n[mine].sum())
+    if dist is not None:
+        dist.barrier()
     chunk = 100
     e_steps_sum = 0.0
     torch.cuda.synchronize()
@@ -1133,10 +1147,31 @@ def run_batch(args):
     cur = b.read_current()
     n_end = float(cur[:, L.S_COUNT].sum())
     clocks = clk.summary()
+    b.close()
+    e_local = 0.5 * (n_start + n_end) * spec.steps
+    if dist is not None:
+        t = torch.tensor([solve_ms, e_local], device=f"cuda:{local}", dtype=torch.float64)
+        mx, sm = t.clone(), t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        solve_ms, e_local = float(mx[0]), float(sm[1])
     step_ms = solve_ms / spec.steps
     value = spec.k / (solve_ms * 1e-3)
-    e_steps = 0.5 * (n_start + n_end) / (step_ms * 1e-3)
-    b.close()
+    e_steps = e_local / (solve_ms * 1e-3)
+    if ws > 1:
+        if rank == 0:
+            print(json.dumps({
+                "metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": ws, "steps": spec.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"batched swarms cfg3: {spec.k} instances dealt to {ws} ranks by predicted "
+                                       f"work, {spec.steps} steps per solve", "parallelism": f"instances over {ws} GPUs",
+                           "electron_steps_per_s": e_steps, "solve_time_s": solve_ms * 1e-3},
+                "roofline": None, "cpu_baseline": None, "e2e": None, "clocks": clocks,
+                "gpu_launches": spec.steps * 9}), flush=True)
+        dist.barrier()
+        dist.destroy_process_group()
+        return 0
 
     # plain drop-in: each solve alone, all spec.steps steps, on a size-stratified sample (the
     # instances sorted by electron count, every `stride`-th); the serial time of all K is the

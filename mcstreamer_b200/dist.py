@@ -1,7 +1,8 @@
 """Multi-GPU layout of the electron step: one process per GPU over torch.distributed.
 
 * Swarm instances (E/N points, gases, replicas) are independent: they are dealt to ranks
-  by predicted work (electrons x steps, longest first) and need no collective.
+  by predicted work (electrons x steps, longest first; served requests online in arrival
+  order) and need no collective on the data path; results are gathered on the host.
 * The streamer step shards one particle population across ranks on a shared mesh.  The
   only coupling is the deposit: each rank deposits its shard into its own int64 charge
   grid and the grids are summed with an all-reduce, which is exact and independent of
@@ -36,6 +37,51 @@ def balance_instances(work: Sequence[float], world: int) -> list[list[int]]:
         heapq.heappush(heap, (load + float(work[i]), r))
     for lst in out:
         lst.sort()
+    return out
+
+
+def my_instances(work: Sequence[float], rank: int, world: int) -> list[int]:
+    """The instances rank `rank` steps (balance_instances; one rank gets them all)."""
+    if world <= 1:
+        return list(range(len(work)))
+    return balance_instances(work, world)[rank]
+
+
+def shard_requests(requests, rank: int, world: int) -> list:
+    """Online dealing of served requests (arrival order): each request goes to the rank with
+    the least predicted work so far (its electron count), ties to the lower rank.  Every
+    rank computes the same assignment from the same arrival list, so no collective is
+    needed to route a request."""
+    if world <= 1:
+        return list(requests)
+    load = [0.0] * world
+    mine = []
+    for r in sorted(requests, key=lambda q: (q.arrival, q.rid)):
+        k = min(range(world), key=lambda j: (load[j], j))
+        load[k] += float(r.n)
+        if k == rank:
+            mine.append(r)
+    return mine
+
+
+def gather_by_index(local: dict, n: int, group=None) -> list:
+    """Every rank's {instance index: result} merged into one list of n results, on every
+    rank (all_gather_object; results must be picklable)."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size(group) == 1:
+        parts = [local]
+    else:
+        parts = [None] * dist.get_world_size(group)
+        dist.all_gather_object(parts, local, group=group)
+    out = [None] * n
+    for part in parts:
+        for i, v in part.items():
+            if out[i] is not None:
+                raise ValueError(f"instance {i} was stepped by two ranks")
+            out[i] = v
+    missing = [i for i, v in enumerate(out) if v is None]
+    if missing:
+        raise ValueError(f"instances {missing[:8]} were stepped by no rank")
     return out
 
 

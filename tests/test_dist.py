@@ -115,3 +115,66 @@ def test_lost_rank_surfaces_as_error():
     for p in procs:
         p.join(60)
     assert res != "no error"
+
+
+# ---- swarm instances dealt to ranks (no data-path collective), results gathered ----
+INST = [(0, 120.0, 96, 5), (1, 300.0, 400, 6), (2, 800.0, 160, 7), (0, 50.0, 320, 8), (1, 600.0, 64, 9),
+        (2, 200.0, 250, 10), (0, 1000.0, 128, 11)]   # (gas, E/N in Td, electrons, seed)
+
+
+def _instance_result(k):
+    """One tiny swarm instance stepped by the oracle: 15 steps of advance! + Swarm.resample!
+    + repack!; the result is the final population's moments."""
+    from mcstreamer_b200 import constants as co
+    from mcstreamer_b200 import lxcat, swarm
+    from oracle import pyoracle as po
+    gas, en, n, seed = INST[k]
+    t = po.OracleTable.from_lxcat(lxcat.synthetic_table(gas))
+    p = swarm.initial_particles(n, "maxwellian", seed)
+    op = po.OraclePop(p.x, p.v, p.w, p.s, p.active, cap=8 * n, seed=seed)
+    _, fin = po.swarm_run(op, t, po.field_uniform(0, 0, en * co.Td * 2.5e25), 1e-13, 15, n, 0.1, 1, threads=1)
+    return fin.tolist()
+
+
+def _rank_instances(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    work = [n * 15 for _, _, n, _ in INST]
+    mine = mdist.my_instances(work, rank, world)
+    local = {k: _instance_result(k) for k in mine}
+    res = mdist.gather_by_index(local, len(INST))
+    out.put((rank, mine, res))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_instances_gather_to_the_single_process_results():
+    world = 2
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_instances, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [out.get(timeout=180) for _ in range(world)]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    mines = sorted(i for _, mine, _ in got for i in mine)
+    assert mines == list(range(len(INST)))            # every instance on exactly one rank
+    assert all(len(mine) > 0 for _, mine, _ in got)
+    ref = [_instance_result(k) for k in range(len(INST))]
+    for _, _, res in got:                              # every rank holds every result
+        assert res == ref
+
+
+def test_shard_requests_is_a_balanced_partition():
+    from mcstreamer_b200.serve import poisson_requests
+    reqs = poisson_requests(200.0, 5.0, seed=4)
+    parts = [mdist.shard_requests(reqs, r, 4) for r in range(4)]
+    ids = sorted(q.rid for p in parts for q in p)
+    assert ids == sorted(q.rid for q in reqs)
+    loads = [sum(q.n for q in p) for p in parts]
+    assert max(loads) / np.mean(loads) < 1.1
+    assert mdist.shard_requests(reqs, 0, 1) == list(reqs)
