@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--e2e-chunks", type=int, default=8, help="chunks of the pipelined host-resident step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-cfg1", action="store_true", help="cfg2: skip the cfg1 kernel sub-record")
+    ap.add_argument("--mesh-shape", type=int, default=None, help="cfg1/cfg2: MCS_OPT_MESH_SHAPE of the step kernel")
     ap.add_argument("--cap-factor", type=float, default=6.0, help="cfg2: population capacity / initial electrons")
     ap.add_argument("--replicas", type=int, default=16, help="cfg0: device replicas per precision")
     ap.add_argument("--oracle-replicas", type=int, default=4, help="cfg0: oracle replicas")
@@ -260,6 +261,8 @@ def run_mine(args):
     ctx = jumc.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    if args.mesh_shape is not None:
+        ctx.check(ctx.lib.mcs_ctx_set_option(ctx.h, L.OPT_MESH_SHAPE, args.mesh_shape))
     table = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
     grid = streamer.Grid3D(spec.nx, spec.ny, spec.nz, spec.h, precision="fp32", ctx=ctx)
     grid.set_efield_fn(workloads.streamer_field_fn(spec), planes_per_chunk=16)
@@ -648,6 +651,15 @@ def cfg1_kernel_record(ctx, table, stream, torch, L, steps: int = 20, warmup: in
             "alg_bytes_per_launch": alg, "achieved_gbs": alg / (km * 1e-3) / 1e9}
 
 
+def mesh_kernel_name(ctx) -> str:
+    import ctypes as C
+    v = C.c_int()
+    ctx.check(ctx.lib.mcs_ctx_get_option(ctx.h, 1, C.byref(v)))
+    b, p, m = C.c_int(), C.c_int(), C.c_int()
+    ctx.check(ctx.lib.mcs_mesh_shape(v.value, C.byref(b), C.byref(p), C.byref(m)))
+    return f"k_step_mesh<float,{b.value},{p.value},{m.value}>" + (" (event blocks during the push)" if v.value >= 8 else "")
+
+
 def run_cfg2(args):
     import torch
 
@@ -667,6 +679,8 @@ def run_cfg2(args):
     ctx = jumc.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    if args.mesh_shape is not None:
+        ctx.check(ctx.lib.mcs_ctx_set_option(ctx.h, L.OPT_MESH_SHAPE, args.mesh_shape))
     table = jumc.CollisionTable(lxcat.synthetic_table(0), ctx)
     grid = streamer.Grid3D(spec.nx, spec.ny, spec.nz, spec.h, precision="fp32", ctx=ctx)
     t_setup = time.perf_counter()
@@ -803,7 +817,7 @@ def run_cfg2(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": tr.get("bytes_per_launch") if tr and not tr.get("stale") else None,
                          "traffic_source": (tr.get("note") if tr else None),
-                         "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
+                         "kernel": mesh_kernel_name(ctx), "kernel_ms": kmean,
                          "alg_bytes_per_launch": alg, "alg_bytes_particles_only": alg_particles,
                          "frac_particles_only": alg_particles / (kmean * 1e-3) / 1e9 / hbm,
                          "alg_note": "70 B per entering electron + 37 B per secondary + 28 B per mesh node (field "
