@@ -209,8 +209,13 @@ __device__ uint32_t resample_segment(const ResampleArgs& a, PopView<T>& P, long 
     const long long n = *a.n;
     const long long b = a.start[s];
     const uint32_t cell = a.key[b];
-    long long e = b;
-    while (e < n && a.key[e] == cell) ++e;
+    long long e;
+    if (s + 1 < *a.nseg) {
+        e = a.start[s + 1];   // segments are consecutive: no dependent walk over the keys
+    } else {
+        e = b;
+        while (e < n && a.key[e] == cell) ++e;
+    }
     Rng rng;
     rng.init(a.seed, cell, a.call, TAG_CELL_RESAMPLE);
     // pass 1 (resample.jl:16-29): count, total weight, first sample when p reaches nmax
