@@ -182,31 +182,6 @@ class CpuSample:
                           f"cloud, FP64 oracle, {self.threads} threads, {dt:.2f} s per step"}
 
 
-# Warp instructions per electron step of k_step_mesh<float,256,8,3> on the cfg1 workload,
-# from the ncu capture summarised in profiles/k_step_mesh_cfg1_full.md (780.4 M warp
-# instructions over 4,194,304 electrons).
-MESH_WARP_INST_PER_STEP = {"cfg1": 780.4e6 / 4_194_304}
-
-
-def issue_roofline(workload: str, n_active: float, kernel_ms: float, clocks) -> Optional[dict]:
-    """The bound the step kernel actually meets: warp instructions issued per second against
-    one instruction per cycle on each of the 4 schedulers of every SM at the sampled clock."""
-    per = MESH_WARP_INST_PER_STEP.get(workload)
-    if per is None or not clocks or not clocks.get("sm_mhz") or not kernel_ms:
-        return None
-    try:
-        import torch
-        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    except Exception:   # the issue bound is an annotation; never fail the line over it
-        return None
-    achieved = per * n_active / (kernel_ms * 1e-3)
-    peak = sms * 4 * clocks["sm_mhz"] * 1e6
-    return {"bound": "issue", "achieved": achieved, "peak": peak, "unit": "warp instructions/s",
-            "frac": achieved / peak, "warp_inst_per_electron_step": per,
-            "source": "instruction count from the ncu capture in profiles/k_step_mesh_cfg1_full.md; peak = SMs x 4 "
-                      "schedulers x sampled SM clock"}
-
-
 def cpu_sample(spec, seconds: float, threads: int) -> dict:
     return CpuSample(spec, seconds / 2, threads).measure(reps=2)
 
@@ -342,10 +317,8 @@ def run_mine(args):
     hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     alg = alg_bytes_per_launch(n_active, sec_per_step, spec.nodes)
     achieved = alg / (kmean * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / f"traffic_k_step_mesh_{args.workload}.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get("bytes_per_launch")
+    tr = profile_record(f"traffic_k_step_mesh_{args.workload}")
+    traffic = tr.get("bytes_per_launch") if tr and not tr.get("stale") else None
 
     e2e = None
     if args.e2e_steps > 0:
@@ -374,9 +347,10 @@ def run_mine(args):
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "kernel": "k_step_mesh<float,256,8,3>", "kernel_ms": kmean,
+                         "kernel": mesh_kernel_name(ctx), "kernel_ms": kmean,
                          "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "issue": issue_roofline(args.workload, n_active, kmean, clocks)},
+                         "issue": issue_roofline_from(profile_record(f"issue_k_step_mesh_{args.workload}"),
+                                                      n_active, kmean, clocks)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
@@ -489,8 +463,8 @@ def profile_record(name: str) -> Optional[dict]:
         return None
     d = json.loads(p.read_text())
     files = d.get("sources")
-    if files:
-        d["stale"] = source_sha(files) != d.get("source_sha")
+    # a record without the sha of its kernel's sources cannot be shown current
+    d["stale"] = (source_sha(files) != d.get("source_sha")) if files else True
     return d
 
 
