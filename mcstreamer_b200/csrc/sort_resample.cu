@@ -290,6 +290,7 @@ constexpr int RS_SRC = 128;       // clone sources a merge can record (ntarget a
 
 struct RsShared {
     double w[RS_WARPS][RS_BUF];
+    double f[RS_WARPS][RS_SRC];      // merge: f_k = samplemin(ntarget - k) of the cell's draw k
     uint32_t src[RS_WARPS][RS_SRC];
 };
 
@@ -317,6 +318,78 @@ __device__ __forceinline__ void copy_clone(PopView<T>& P, long long d, long long
     if (P.cell) P.cell[d] = P.cell[j];
     P.act[d] = 1;
     P.f[6][d] = w;
+}
+
+// A merging cell (p > nmax) by one warp.  The sample positions of resample.jl:48-52 follow
+// x_1 = samplemin(ntarget) and x_(k+1) = x_k + samplemin(ntarget - k) (1 - x_k), where
+// samplemin draws the cell's k-th uniform: every factor f_k = 1 - (1 - U_k)^(1/(ntarget - k))
+// depends on the draw alone, so the lanes compute them side by side (the pows), and lane 0
+// runs the two serial passes over the staged weights with additions and products only --
+// unfused, in the reference's order -- recording the clone sources.  The warp then writes
+// the clones to consecutive slots and removes the originals.
+template <typename T, bool WRITE>
+__device__ uint32_t merge_segment_warp(const ResampleArgs& a, PopView<T>& P, long long b, long long e, uint32_t cell,
+                                       long long clone_base, long long cap, uint32_t* status, RsShared& sh,
+                                       int wid) {
+    const int lane = threadIdx.x & 31;
+    double* wb = sh.w[wid];
+    double* fk = sh.f[wid];
+    uint32_t* src = sh.src[wid];
+    const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+    for (int k = lane; k < a.ntarget; k += 32) {
+        // word k of the cell's stream {cell, call, k/4, TAG_CELL_RESAMPLE}
+        const U4 blk = philox10(U4{cell, a.call, (uint32_t)k >> 2, TAG_CELL_RESAMPLE}, k0, k1);
+        const uint32_t q = (uint32_t)k & 3u;
+        const uint32_t w = q == 0 ? blk.x : q == 1 ? blk.y : q == 2 ? blk.z : blk.w;
+        fk[k] = 1.0 - pow(1.0 - uni64(w), 1.0 / (double)(a.ntarget - k));
+    }
+    double wtotal = 0.0, x = 0.0;
+    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
+        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
+        __syncwarp();
+        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
+        __syncwarp();
+        if (lane == 0) {
+            for (int q = 0; q < m; ++q) {
+                wtotal = __dadd_rn(wtotal, wb[q]);
+                if (c0 - b + q + 1 == a.nmax) x = fk[0];   // pass 1: samplemin(ntarget)
+            }
+        }
+    }
+    uint32_t ncl = 0;
+    long long pk = 0;
+    double wcum = 0.0;
+    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
+        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
+        __syncwarp();
+        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
+        __syncwarp();
+        if (lane == 0) {
+            for (int q = 0; q < m; ++q) {
+                const double wj = wb[q];
+                while (__dmul_rn(wtotal, x) < __dadd_rn(wcum, wj) && pk < a.ntarget) {
+                    pk += 1;
+                    src[ncl++] = (uint32_t)(c0 - b + q);
+                    if (pk < a.ntarget) x = __dadd_rn(x, __dmul_rn(fk[pk], __dadd_rn(1.0, -x)));
+                }
+                wcum = __dadd_rn(wcum, wj);
+            }
+        }
+    }
+    __syncwarp();
+    ncl = __shfl_sync(0xffffffffu, ncl, 0);
+    if (WRITE) {
+        wtotal = __shfl_sync(0xffffffffu, wtotal, 0);
+        const T wc = (T)(wtotal / (double)a.ntarget);
+        for (uint32_t k = lane; k < ncl; k += 32) {
+            const long long d = clone_base + k;
+            if (d < cap) copy_clone<T>(P, d, b + src[k], wc);
+            else atomicOr(status, ST_CAPACITY);
+        }
+        for (long long j = b + lane; j < e; j += 32) P.act[j] = 0;   // remove_particle!
+    }
+    __syncwarp();
+    return ncl;
 }
 
 // Returns the number of clones of segment s (the same on every lane).
@@ -356,64 +429,69 @@ __device__ uint32_t resample_segment_warp(const ResampleArgs& a, PopView<T>& P, 
         return ranked < K ? ranked : K;
     }
     if (p0 <= a.nmax) return 0;
-    // merge: pass 1 and pass 2 on lane 0 over staged weights
-    double* wb = sh.w[wid];
-    uint32_t* src = sh.src[wid];
-    Rng rng;
-    rng.init(a.seed, cell, a.call, TAG_CELL_RESAMPLE);
-    double wtotal = 0.0, x = 0.0;
-    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
-        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
-        __syncwarp();
-        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
-        __syncwarp();
-        if (lane == 0) {
-            for (int q = 0; q < m; ++q) {
-                wtotal += wb[q];
-                if (c0 - b + q + 1 == a.nmax) x = 1.0 - pow(1.0 - rng.u64(), 1.0 / (double)a.ntarget);
-            }
-        }
-    }
-    uint32_t ncl = 0;
-    long long pk = 0;
-    double wcum = 0.0;
-    for (long long c0 = b; c0 < e; c0 += RS_BUF) {
-        const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
-        __syncwarp();
-        for (int q = lane; q < m; q += 32) wb[q] = (double)P.f[6][c0 + q];
-        __syncwarp();
-        if (lane == 0) {
-            for (int q = 0; q < m; ++q) {
-                const double wj = wb[q];
-                while (wtotal * x < wcum + wj && pk < a.ntarget) {
-                    pk += 1;
-                    src[ncl++] = (uint32_t)(c0 - b + q);
-                    if (pk < a.ntarget) x += (1.0 - pow(1.0 - rng.u64(), 1.0 / (double)(a.ntarget - pk))) * (1.0 - x);
-                }
-                wcum += wj;
-            }
-        }
-    }
-    __syncwarp();
-    ncl = __shfl_sync(0xffffffffu, ncl, 0);
-    if (WRITE) {
-        wtotal = __shfl_sync(0xffffffffu, wtotal, 0);
-        const T wc = (T)(wtotal / (double)a.ntarget);
-        for (uint32_t k = lane; k < ncl; k += 32) {
-            const long long d = clone_base + k;
-            if (d < cap) copy_clone<T>(P, d, b + src[k], wc);
-            else atomicOr(status, ST_CAPACITY);
-        }
-        for (long long j = b + lane; j < e; j += 32) P.act[j] = 0;   // remove_particle!
-    }
-    return ncl;
+    return merge_segment_warp<T, WRITE>(a, P, b, e, cell, clone_base, cap, status, sh, wid);
 }
 
 // Counting is latency-bound over millions of small segments: a thread per segment keeps 32
 // segments' loads in flight per warp.
+// Only merging cells need the serial pass; their segments go to a worklist for the warp
+// kernel below.  A splitting cell (p < ntarget) clones its first ntarget - p particles with
+// w > 2 (resample.jl:62-70); a cell with ntarget <= p <= nmax is left alone.
 template <typename T>
 __global__ void __launch_bounds__(128) k_resample_count(ResampleArgs a, PopView<T> P, uint32_t* __restrict__ counts,
-                                                        uint32_t* status) {
+                                                        uint32_t* __restrict__ merge_list,
+                                                        unsigned long long* merge_n) {
+    const long long nseg = *a.nseg;
+    const long long n = *a.n;
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x) {
+        const long long b = a.start[s];
+        long long e;
+        if (s + 1 < nseg) {
+            e = a.start[s + 1];
+        } else {
+            const uint32_t cell = a.key[b];
+            e = b;
+            while (e < n && a.key[e] == cell) ++e;
+        }
+        const long long p0 = e - b;
+        uint32_t cnt = 0;
+        if (p0 > a.nmax) {
+            merge_list[atomicAdd(merge_n, 1ull)] = (uint32_t)s;
+        } else if (p0 < a.ntarget) {
+            const long long K = a.ntarget - p0;
+            for (long long j = b; j < e && cnt < K; ++j)
+                if ((double)P.f[6][j] > 2) ++cnt;
+        }
+        counts[s] = cnt;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_merge_count(ResampleArgs a, PopView<T> P,
+                                                                         uint32_t* __restrict__ counts,
+                                                                         const uint32_t* __restrict__ merge_list,
+                                                                         const unsigned long long* merge_n) {
+    __shared__ RsShared sh;
+    const long long nm = (long long)*merge_n;
+    const long long n = *a.n;
+    const long long nseg = *a.nseg;
+    const int wid = threadIdx.x >> 5;
+    const long long w0 = (long long)blockIdx.x * RS_WARPS + wid, ws = (long long)gridDim.x * RS_WARPS;
+    for (long long q = w0; q < nm; q += ws) {
+        const long long s = merge_list[q];
+        const long long b = a.start[s];
+        const uint32_t cell = a.key[b];
+        const long long e = segment_end(a, s, nseg, b, cell);
+        (void)n;
+        const uint32_t c = merge_segment_warp<T, false>(a, P, b, e, cell, 0, 0, nullptr, sh, wid);
+        if ((threadIdx.x & 31) == 0) counts[s] = c;
+    }
+}
+
+// The serial form's count, a thread per segment (ntarget > nmax or ntarget > RS_SRC).
+template <typename T>
+__global__ void __launch_bounds__(128) k_resample_count_serial(ResampleArgs a, PopView<T> P,
+                                                               uint32_t* __restrict__ counts, uint32_t* status) {
     const long long nseg = *a.nseg;
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg; s += (long long)gridDim.x * blockDim.x)
         counts[s] = resample_segment<T, false>(a, P, s, 0, 0, status);
@@ -540,8 +618,22 @@ int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
     a.nmax = nmax;
     a.seed = p->seed;
     a.call = p->resample_calls++;
-    k_resample_count<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, c->d_status);
-    MCS_CK_LAUNCH(c);
+    if (ntarget > nmax || ntarget > RS_SRC) {
+        k_resample_count_serial<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, c->d_status);
+        MCS_CK_LAUNCH(c);
+    } else {
+        // merging cells hold more than nmax particles each: at most n / (nmax + 1) of them
+        if (int st = ensure(c, &p->u32b, (size_t)p->cap)) return st;
+        unsigned long long* merge_n = reinterpret_cast<unsigned long long*>(p->counters + 14);
+        MCS_CK(c, cudaMemsetAsync(merge_n, 0, sizeof(unsigned long long), c->stream));
+        k_resample_count<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, p->u32b, merge_n);
+        MCS_CK_LAUNCH(c);
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_resample_merge_count<T>, RS_WARPS * 32, 0);
+        k_resample_merge_count<T><<<std::max(occ, 1) * c->num_sms, RS_WARPS * 32, 0, c->stream>>>(
+            a, pop_view<T>(p), p->seg_a, p->u32b, merge_n);
+        MCS_CK_LAUNCH(c);
+    }
     if (int st = launch_scan(p, p->seg_a, p->seg_b, nseg, total)) return st;
     PopView<T> P = pop_view<T>(p);
     if (ntarget > nmax || ntarget > RS_SRC) {
