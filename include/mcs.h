@@ -202,6 +202,10 @@ MCS_API int mcs_pop_init_cloud(mcs_pop* p, int64_t n, double cx, double cy, doub
  * (cart3d grids). */
 /* The stored field: cart3d 3 doubles per node (x fastest); cyl the er then the ez faces. */
 MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e);
+/* Nodes [node0, node0 + count) of a cart3d grid's field (3 doubles each), and of a charge
+ * array (int64 at 2^-32 e): a window of a large mesh without copying all of it. */
+MCS_API int mcs_grid_read_efield_range(mcs_grid* g, int64_t node0, int64_t count, double* e);
+MCS_API int mcs_grid_read_fixed_range(mcs_grid* g, int which, int64_t node0, int64_t count, int64_t* out);
 MCS_API int mcs_grid_set_efield_gaussian(mcs_grid* g, double cx, double cy, double cz, double sigma,
                                          double rho_peak, double ebx, double eby, double ebz);
 MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src);

@@ -407,6 +407,34 @@ MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e) {
     return MCS_OK;
 }
 
+MCS_API int mcs_grid_read_efield_range(mcs_grid* g, int64_t node0, int64_t count, double* e) {
+    if (!g || !e || node0 < 0 || count < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_ARG, "range read needs a cart3d grid");
+    if ((size_t)(node0 + count) > g->nq) return set_err(c, MCS_ERR_ARG, "node range beyond the mesh");
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    if (g->d_e32) {
+        std::vector<float> tmp(4 * (size_t)count);
+        MCS_CK(c, cudaMemcpy(tmp.data(), g->d_e32 + 4 * node0, tmp.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < count; ++i)
+            for (int d = 0; d < 3; ++d) e[3 * i + d] = tmp[4 * i + d];
+    } else {
+        MCS_CK(c, cudaMemcpy(e, g->d_e64 + 3 * node0, 3 * (size_t)count * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return MCS_OK;
+}
+
+MCS_API int mcs_grid_read_fixed_range(mcs_grid* g, int which, int64_t node0, int64_t count, int64_t* out) {
+    if (!g || !out || (which != MCS_Q_FIXED && which != MCS_Q_PART) || node0 < 0 || count < 0) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if ((size_t)(node0 + count) > g->nq) return set_err(c, MCS_ERR_ARG, "range beyond the charge array");
+    if (int st = use_device(c)) return st;
+    MCS_CK(c, cudaStreamSynchronize(c->stream));
+    MCS_CK(c, cudaMemcpy(out, g->d_q[which] + node0, (size_t)count * sizeof(long long), cudaMemcpyDeviceToHost));
+    return sync_status(c);
+}
+
 MCS_API int mcs_grid_zero(mcs_grid* g, int which) {
     if (!g || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
     mcs_ctx* c = g->ctx;

@@ -95,6 +95,31 @@ class Grid3D:
         self.ctx.check(self.ctx.lib.mcs_grid_read_fixed(self.h_, which, L.i64ptr(out)))
         return out
 
+    def _box_planes(self, lo, hi, read_plane):
+        """Nodes lo..hi (inclusive, (ix, iy, iz)) read z-plane by z-plane, x fastest."""
+        plane = (self.nx + 1) * (self.ny + 1)
+        out = []
+        for k in range(lo[2], hi[2] + 1):
+            a = read_plane(k * plane, plane).reshape(self.ny + 1, self.nx + 1, -1)
+            out.append(a[lo[1]:hi[1] + 1, lo[0]:hi[0] + 1])
+        return np.ascontiguousarray(np.stack(out))
+
+    def read_efield_box(self, lo, hi) -> np.ndarray:
+        """The node field of the box of nodes lo..hi (inclusive), (nodes, 3), x fastest."""
+        def rd(node0, count):
+            e = np.zeros((count, 3))
+            self.ctx.check(self.ctx.lib.mcs_grid_read_efield_range(self.h_, node0, count, L.dptr(e)))
+            return e
+        return self._box_planes(lo, hi, rd).reshape(-1, 3)
+
+    def read_fixed_box(self, which: int, lo, hi) -> np.ndarray:
+        """The int64 charges of the box of nodes lo..hi (inclusive), x fastest."""
+        def rd(node0, count):
+            q = np.zeros(count, dtype=np.int64)
+            self.ctx.check(self.ctx.lib.mcs_grid_read_fixed_range(self.h_, which, node0, count, L.i64ptr(q)))
+            return q
+        return self._box_planes(lo, hi, rd).reshape(-1)
+
     def charge_array(self, which: int = L.Q_PART) -> "DeviceArray":
         """The device int64 charge array, exposed through __cuda_array_interface__ (so a
         collective library can sum it across processes in place)."""
