@@ -75,25 +75,39 @@ __device__ __forceinline__ int select_row64(const TableView& t, double eng, doub
     return -1;
 }
 
-// FP32: u = v^2 * (m/2/step) - e0/step is the position on the energy grid.
-__device__ __forceinline__ int select_row32(const TableView& t, float v2, float xi, uint32_t flags,
-                                            uint32_t* status) {
-    const float u = fmaf(v2, t.ke32, -t.e0n32);
-    int k = (int)u;
+// FP32 selection, u = v^2 * (m/2/step) - e0/step being the position on the energy grid, in
+// two halves so that the first rows' loads are in flight while the caller draws xi:
+// select32_begin places the energy on the grid and loads the first four rows of both
+// columns; select32_finish scans them (and the rest) against xi.
+struct Sel32 {
+    int k;
     float w;
-    if (!(u >= 0.0f && k <= t.neps - 2)) {
-        const bool low = !(u >= 0.0f);
-        k = low ? 0 : t.neps - 2;
-        w = low ? 1.0f : 0.0f;
-        if (!(flags & FLAG_CLAMP)) atomicOr(status, ST_ENERGY);
-    } else {
-        w = (float)(k + 1) - u;
-    }
-    const float4* c0 = reinterpret_cast<const float4*>(t.rate32 + (size_t)k * t.nrp);
-    const float4* c1 = reinterpret_cast<const float4*>(t.rate32 + (size_t)(k + 1) * t.nrp);
+    bool bad;
+    float4 a, b;
+};
+
+__device__ __forceinline__ void select32_begin(const TableView& t, float v2, Sel32& s) {
+    const float u = fmaf(v2, t.ke32, -t.e0n32);
+    const int k = (int)u;
+    const bool low = !(u >= 0.0f);
+    s.bad = low || k > t.neps - 2;
+    s.k = s.bad ? (low ? 0 : t.neps - 2) : k;
+    s.w = s.bad ? (low ? 1.0f : 0.0f) : (float)(k + 1) - u;
+    s.a = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)s.k * t.nrp));
+    s.b = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)(s.k + 1) * t.nrp));
+}
+
+__device__ __forceinline__ int select32_finish(const TableView& t, const Sel32& s, float xi, uint32_t flags,
+                                               uint32_t* status) {
+    if (s.bad && !(flags & FLAG_CLAMP)) atomicOr(status, ST_ENERGY);
+    const float w = s.w;
+    float4 a = s.a, b = s.b;
     const int nq = t.nrp >> 2;
     for (int q = 0; q < nq; ++q) {
-        const float4 a = __ldg(c0 + q), b = __ldg(c1 + q);
+        if (q) {
+            a = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)s.k * t.nrp) + q);
+            b = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)(s.k + 1) * t.nrp) + q);
+        }
         const int j = q << 2;
         float nu = fmaf(w, a.x - b.x, b.x);
         if (nu > xi) return j;

@@ -203,15 +203,19 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
     int j;
     double eng = 0.0;
     float v2 = 0.0f;
-    rng.begin();
     if constexpr (sizeof(T) == 8) {
+        rng.begin();
         eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
         const double xi = rng.template xi<double>() * tab.maxrate;
         j = select_row64(tab, eng, xi, C.flags, C.status);
     } else {
+        // the first rows' loads go out before the event's block is drawn
         v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
+        Sel32 sel;
+        select32_begin(tab, v2, sel);
+        rng.begin();
         const float xi = rng.template xi<float>() * tab.maxrate32;
-        j = select_row32(tab, v2, xi, C.flags, C.status);
+        j = select32_finish(tab, sel, xi, C.flags, C.status);
     }
     const int kind = j >= 0 ? rows.kind[j] : K_NULL;
     if (row_out) *row_out = j;
