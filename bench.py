@@ -682,8 +682,8 @@ def run_cfg2(args):
         ev[1].record(stream)
         streamer.advance_deposit(pop, fld, spec.dt, trk, grid, -1.0)
         ev[2].record(stream)
-        if qpart is not None:
-            mdist.allreduce_int64_(qpart)
+        if qpart is not None:               # the occupied z-slab of the deposit grid only
+            mdist.allreduce_slab_int64_(qpart, (spec.nx + 1) * (spec.ny + 1))
         if (k + 1) % CFG2_PERIOD == 0:      # resample! sorts the population by cell first
             ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, CFG2_NTARGET, CFG2_NMAX))
         ev[3].record(stream)
@@ -785,7 +785,8 @@ def run_cfg2(args):
                                "+ resample! on its steps), summed over the K timed steps; the active-electron "
                                "count read after a resample! lies between two steps' windows",
                 "ms_per_step_bracket": bracket_max / args.steps,
-                "parallelism": f"dp{ws} (independent clouds, int64 all-reduce of the deposit grid)" if ws > 1
+                "parallelism": f"dp{ws} (independent clouds, int64 all-reduce of the occupied z-slab of the deposit "
+                               "grid)" if ws > 1
                                else "1 GPU",
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

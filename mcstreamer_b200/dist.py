@@ -95,6 +95,29 @@ def allreduce_int64_(tensor, group=None):
     return tensor
 
 
+def allreduce_slab_int64_(tensor, plane: int, group=None):
+    """Sum an int64 charge grid over ranks in place, moving only the z-planes that hold
+    charge on some rank: each rank finds its nonzero plane range, one small all-reduce gives
+    the union, and the sum runs over that contiguous slab (planes outside it are zero on every
+    rank).  A cloud that covers a tenth of the mesh's height moves a tenth of the bytes; the
+    result is the full all-reduce's, bit for bit.  Returns the slab's plane range."""
+    import torch
+    import torch.distributed as dist
+    if tensor.dtype != torch.int64:
+        raise TypeError("charge grids are int64 fixed point")
+    planes = tensor.numel() // plane
+    rows = tensor.view(planes, plane).ne(0).any(dim=1)
+    nz = torch.nonzero(rows).flatten()
+    lo = int(nz[0]) if nz.numel() else planes
+    hi = int(nz[-1]) + 1 if nz.numel() else 0
+    rng = torch.tensor([-lo, hi], dtype=torch.int64, device=tensor.device)
+    dist.all_reduce(rng, op=dist.ReduceOp.MAX, group=group)
+    lo, hi = int(-rng[0]), int(rng[1])
+    if hi > lo:
+        dist.all_reduce(tensor[lo * plane:hi * plane], op=dist.ReduceOp.SUM, group=group)
+    return lo, hi
+
+
 def allreduce_charge(grid, which: int, group=None):
     """All-reduce a grid's device charge array in place (the NCCL int64 sum of the shards)."""
     import torch

@@ -178,3 +178,36 @@ def test_shard_requests_is_a_balanced_partition():
     loads = [sum(q.n for q in p) for p in parts]
     assert max(loads) / np.mean(loads) < 1.1
     assert mdist.shard_requests(reqs, 0, 1) == list(reqs)
+
+
+def _rank_slab(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    plane, planes = 50, 40
+    rng = np.random.default_rng(rank)
+    q = np.zeros((planes, plane), dtype=np.int64)
+    z0 = 5 + 12 * rank                                  # the ranks' charge in different planes
+    q[z0:z0 + 9] = rng.integers(-2**40, 2**40, (9, plane))
+    full = torch.from_numpy(q.copy()).reshape(-1)
+    slab = torch.from_numpy(q.copy()).reshape(-1)
+    mdist.allreduce_int64_(full)
+    lo, hi = mdist.allreduce_slab_int64_(slab, plane)
+    out.put((rank, lo, hi, bool(torch.equal(full, slab))))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_slab_allreduce_equals_full_allreduce():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_slab, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [out.get(timeout=120) for _ in range(2)]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    for _, lo, hi, same in got:
+        assert same and (lo, hi) == (5, 26)
