@@ -1313,8 +1313,16 @@ def run_serve(args):
     from mcstreamer_b200.serve import StopRule, SwarmServer, percentiles, poisson_requests
     from mcstreamer_b200.workloads import SWARM_DENSITY, SWARM_DT
 
+    from mcstreamer_b200 import dist as mdist
+
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     ctx = jumc.Context(local, clamp_energy=True)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
@@ -1327,14 +1335,26 @@ def run_serve(args):
 
     def serve(rate: float, seconds: float, seed: int, limit: float):
         reqs = poisson_requests(rate, seconds, seed=seed)
+        # several GPUs: each serves its share of the arrivals (dealt online by predicted work)
+        mine = mdist.shard_requests(reqs, rank, ws)
         srv = SwarmServer(ctx, tables, SWARM_DT, SWARM_DENSITY, budget_bytes=160e9, rule=rule)
+        if dist is not None:
+            dist.barrier()
         t0 = time.perf_counter()
-        got = srv.run(reqs, deadline=limit)
+        got = srv.run(mine, deadline=limit)
         wall = time.perf_counter() - t0
-        info = {"rate": rate, "seconds": seconds, "requests": len(reqs), "completed": len(got),
-                "unfinished_at_limit": srv.unfinished, "wall_s": wall, "gpu_steps": srv.gpu_steps,
-                "pool_slots": srv.pool_slots}
+        unfinished, gpu_steps, pool = srv.unfinished, srv.gpu_steps, srv.pool_slots
         srv.close()
+        if dist is not None:
+            parts = [None] * ws
+            dist.all_gather_object(parts, (got, unfinished, wall, gpu_steps))
+            got = sorted((r for p in parts for r in p[0]), key=lambda r: r.rid)
+            unfinished = sum(p[1] for p in parts)
+            wall = max(p[2] for p in parts)
+            gpu_steps = max(p[3] for p in parts)
+        info = {"rate": rate, "seconds": seconds, "requests": len(reqs), "completed": len(got),
+                "unfinished_at_limit": unfinished, "wall_s": wall, "gpu_steps": gpu_steps,
+                "pool_slots": pool}
         makespan = max(r.finished for r in got) if got else wall
         info["solves_per_s"] = len(got) / makespan if makespan > 0 else 0.0
         info["latency_s"] = percentiles([r.latency for r in got])
@@ -1342,7 +1362,7 @@ def run_serve(args):
         info["settled"] = sum(1 for r in got if r.settled)
         # keeps up: every request answered and the last one no later than 10 % after the
         # arrival window closed
-        info["keeps_up"] = bool(srv.unfinished == 0 and makespan <= 1.1 * seconds)
+        info["keeps_up"] = bool(unfinished == 0 and makespan <= 1.1 * seconds)
         return reqs, got, info
 
     with ClockSampler(local) as clk:
@@ -1354,6 +1374,11 @@ def run_serve(args):
         rate2 = 0.8 * main["solves_per_s"]
         _, _, sustained = serve(rate2, args.serve_seconds, 5, args.serve_limit)
 
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
     # the plain drop-in, one request at a time, on a seeded sample of the served requests:
     # per step mcs_advance + mcs_moments (with the table: the rate estimator) +
     # mcs_swarm_resample + mcs_repack for the request's own stopping step count (a request's
@@ -1395,7 +1420,7 @@ def run_serve(args):
     serial_rate = len(pick) / t_serial if t_serial > 0 else 0.0
     value = main["solves_per_s"]
     line = {
-        "metric": SERVE_METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": main["gpu_steps"],
+        "metric": SERVE_METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": main["gpu_steps"],
         "warmup": 1, "ms_per_step": 1e3 * main["wall_s"] / max(1, main["gpu_steps"]), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {
@@ -1413,7 +1438,7 @@ def run_serve(args):
                                     "mcs_repack) for its stopping step count; solves/s = sample / total time. A "
                                     "serial server's queue at the configured rate grows without bound",
                              "requests": rows},
-            "parallelism": "1 GPU",
+            "parallelism": f"requests dealt over {ws} GPUs" if ws > 1 else "1 GPU",
         },
         "roofline": None,
         "cpu_baseline": None,
@@ -1424,6 +1449,9 @@ def run_serve(args):
         "gpu_launches": main["gpu_steps"] * 9,
     }
     print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
