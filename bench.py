@@ -440,7 +440,7 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
 # seed 2.  The population evolves from step to step -- ionization grows it by a few per cent
 # a step, the secondaries are staged and appended in parent order, the tracker deposits
 # their ions -- and every 10th step (steps 9, 19, ...) ends with resample!(ntarget = 64,
-# nmax = 96), which sorts by cell first.  W warm-up steps are the first W steps of that run
+# nmax = 96), which sorts by cell first; every step ends with repack! (main.jl:313).  W warm-up steps are the first W steps of that run
 # and the K timed steps the next K; a step is zero(qpart) + the fused push/collide/track/
 # deposit launch (+ the resample on its step).
 # ---------------------------------------------------------------------------------------
@@ -631,7 +631,7 @@ def mesh_kernel_name(ctx) -> str:
     ctx.check(ctx.lib.mcs_ctx_get_option(ctx.h, 1, C.byref(v)))
     b, p, m = C.c_int(), C.c_int(), C.c_int()
     ctx.check(ctx.lib.mcs_mesh_shape(v.value, C.byref(b), C.byref(p), C.byref(m)))
-    return f"k_step_mesh<float,{b.value},{p.value},{m.value}>" + (" (event blocks during the push)" if v.value >= 8 else "")
+    return f"k_step_mesh<float,{b.value},{p.value},{m.value}>"
 
 
 def run_cfg2(args):
@@ -686,6 +686,7 @@ def run_cfg2(args):
             mdist.allreduce_slab_int64_(qpart, (spec.nx + 1) * (spec.ny + 1))
         if (k + 1) % CFG2_PERIOD == 0:      # resample! sorts the population by cell first
             ctx.check(ctx.lib.mcs_resample_cells(pop.h, grid.h_, CFG2_NTARGET, CFG2_NMAX))
+        ctx.check(ctx.lib.mcs_repack(pop.h))   # repack! every step, as nsteps does (main.jl:313)
         ev[3].record(stream)
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(total)]
@@ -772,7 +773,8 @@ def run_cfg2(args):
                             f"per GPU at the start (w log-uniform {spec.weight[0]:g}..{spec.weight[1]:g}, Gaussian "
                             f"cloud sigma=50um, 1 eV), Gaussian charge sigma=40um peak 1e20 e/m^3 + -15 MV/m, "
                             f"synthetic gas 0, dt={spec.dt:g} s, seed {spec.seed}; the population evolves; "
-                            f"resample!(ntarget={CFG2_NTARGET}, nmax={CFG2_NMAX}) after every {CFG2_PERIOD}th step; "
+                            f"resample!(ntarget={CFG2_NTARGET}, nmax={CFG2_NMAX}) after every {CFG2_PERIOD}th step, repack! "
+                            f"after every step (main.jl:313); "
                             f"warm-up = steps 0..{args.warmup - 1}, timed = steps {args.warmup}..{total - 1}",
                 "electrons_entering_first_timed_step": act_in[args.warmup], "slots_at_first_timed_step": n_first,
                 "mean_active_per_timed_step": mean_in, "secondaries_per_step": mean_sec,
@@ -782,7 +784,7 @@ def run_cfg2(args):
                 "capacity_slots": cap, "setup_s": t_setup,
                 "l2": "inputs larger than L2 (>= 67M electrons x 37 B = 2.5 GB, mesh 4.3 GB field + 2.15 GB charges)",
                 "step_timing": "CUDA events around each step (zero(qpart) + fused step kernel (+ int64 all-reduce) "
-                               "+ resample! on its steps), summed over the K timed steps; the active-electron "
+                               "+ resample! on its steps + repack!), summed over the K timed steps; the active-electron "
                                "count read after a resample! lies between two steps' windows",
                 "ms_per_step_bracket": bracket_max / args.steps,
                 "parallelism": f"dp{ws} (independent clouds, int64 all-reduce of the occupied z-slab of the deposit "

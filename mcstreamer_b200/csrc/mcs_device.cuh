@@ -125,35 +125,6 @@ struct Event {
     __device__ __forceinline__ void finish() {}
 };
 
-// The same stream with the event's block computed ahead by the kernel (`pre`), so that its
-// integer chain can be interleaved with the push that precedes the collision.
-struct EventPre : Event {
-    U4 pre;
-    __device__ __forceinline__ void begin() { b = pre; ++j; }
-};
-
-// Philox4x32-10 of one counter run a few rounds at a time (R0: index of the first round of
-// the call), bit-identical to philox10.
-struct PhiloxRun {
-    U4 c;
-    uint32_t k0, k1;
-    __device__ __forceinline__ void start(uint32_t a, uint32_t b, uint32_t blk, uint32_t tag, uint32_t key0,
-                                          uint32_t key1) {
-        c = U4{a, b, blk, tag};
-        k0 = key0;
-        k1 = key1;
-    }
-    template <int R0, int N>
-    __device__ __forceinline__ void rounds() {
-#pragma unroll
-        for (int q = 0; q < N; ++q) {
-            if (R0 + q > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
-            const unsigned long long p0 = 0xD2511F53ull * c.x, p1 = 0xCD9E8D57ull * c.z;
-            c = U4{(uint32_t)(p1 >> 32) ^ c.y ^ k0, (uint32_t)p1, (uint32_t)(p0 >> 32) ^ c.w ^ k1, (uint32_t)p0};
-        }
-    }
-};
-
 // Injected uniforms (mcs_set_uniform_source): the particle of slot `slot` reads its own
 // caller-given values one after the other, in whatever order the collision code asks for
 // them -- the reference's serial order.  Running past the range raises ST_UNIFORMS and

@@ -631,10 +631,7 @@ __device__ __forceinline__ bool in_unit_cube(T ox, T oy, T oz) {
     }
 }
 
-// PRE: each sub-step's event block is computed a few Philox rounds at a time between the
-// stages of the push (whose FP32 chains it does not depend on), and used if the sub-step
-// collides -- the same stream, more independent work in flight per lane.
-template <typename T, int BLOCK, int PPT, int MINB = 1, bool PRE = false>
+template <typename T, int BLOCK, int PPT, int MINB = 1>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
                                                      YoshidaC Y, double dep_val) {
     constexpr int TILE = BLOCK * PPT;
@@ -659,7 +656,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
         bool have = false, drained = false;
         uint32_t local = 0;
         long long i = 0;
-        typename std::conditional<PRE, EventPre, Event>::type rng;
+        Event rng;
         T ox = 0, oy = 0, oz = 0, vx = 0, vy = 0, vz = 0, w = 0;
         double s = 0.0, trem = 0.0;
         bool in = false;
@@ -741,30 +738,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             else { t = trem; collides = false; s -= t * tab.maxrate; }
             const T tt = (T)t;
             // advance_free_yoshida (electron.jl:51-62) in cell units
-            if constexpr (PRE) {
-                PhiloxRun pr;
-                pr.start(rng.slot, rng.step, rng.j, rng.tag, rng.k0, rng.k1);
-                pr.template rounds<0, 3>();
-                drift(cd1 * tt);
-                kick(kd1 * tt);
-                pr.template rounds<3, 3>();
-                drift(cd2 * tt);
-                kick(kd2 * tt);
-                pr.template rounds<6, 2>();
-                drift(cd3 * tt);
-                kick(kd3 * tt);
-                pr.template rounds<8, 2>();
-                drift(cd4 * tt);
-                rng.pre = pr.c;
-            } else {
-                drift(cd1 * tt);
-                kick(kd1 * tt);
-                drift(cd2 * tt);
-                kick(kd2 * tt);
-                drift(cd3 * tt);
-                kick(kd3 * tt);
-                drift(cd4 * tt);
-            }
+            drift(cd1 * tt);
+            kick(kd1 * tt);
+            drift(cd2 * tt);
+            kick(kd2 * tt);
+            drift(cd3 * tt);
+            kick(kd3 * tt);
+            drift(cd4 * tt);
             if (collides) {
                 Sec<T> sec;
                 const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);

@@ -13,8 +13,8 @@ from tests.helpers import broad
 R, LEN, M, N = 1e-4, 2e-4, 16, 32
 
 
-def _pop(ctx, tab, w):
-    p = broad(64, 1)
+def _pop(ctx, tab, w, n=64):
+    p = broad(n, 1)
     p.x[:, 0] = 0.3 * R
     p.x[:, 1] = 0.0
     p.x[:, 2] = 0.5 * LEN
@@ -34,10 +34,11 @@ def test_particle_charge_beyond_range_is_reported(ctx):
     assert e.value.code == L.ERR_CHARGE_RANGE
     assert grid.read_fixed(L.Q_PART).sum() == 0      # nothing wrapped into the cells
     pop.close()
-    pop = _pop(ctx, tab, 1e9)          # below: deposited exactly
+    # below the bound: deposited exactly (the cell holds 2 x 1e9 e, under its 2^31 e)
+    pop = _pop(ctx, tab, 1e9, n=2)
     streamer.density(grid, pop, 1.0)
     ctx.sync()
-    assert grid.read_fixed(L.Q_PART).sum() == 64 * round(1e9 * 2 ** 32)
+    assert grid.read_fixed(L.Q_PART).sum() == 2 * round(1e9 * 2 ** 32)
     pop.close(); grid.close(); tab.close()
 
 
