@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--no-cfg1", action="store_true", help="cfg2: skip the cfg1 kernel sub-record")
     ap.add_argument("--mesh-shape", type=int, default=None, help="cfg1/cfg2: MCS_OPT_MESH_SHAPE of the step kernel")
+    ap.add_argument("--pre-steps", type=int, default=0, help="cfg1: evolve the input cloud this many steps first")
     ap.add_argument("--cap-factor", type=float, default=6.0, help="cfg2: population capacity / initial electrons")
     ap.add_argument("--replicas", type=int, default=16, help="cfg0: device replicas per precision")
     ap.add_argument("--oracle-replicas", type=int, default=4, help="cfg0: oracle replicas")
@@ -245,10 +246,22 @@ def run_mine(args):
     seed = spec.seed + 1000 * rank
     # the input batch: a snapshot restored (device to device) before every step, so each
     # timed step is one push+collide+track+deposit launch over the same 4.2M-particle cloud
-    snap = jumc.Population(spec.n, parts, table, precision="fp32", seed=seed, mesh=grid)
-    pop = jumc.Population(2 * spec.n, None, table, precision="fp32", seed=seed, mesh=grid)
     fld = streamer.FieldInterp(grid)
     trk = streamer.CollisionTracker(grid)
+    if args.pre_steps > 0:
+        # an evolved cloud: the input advanced pre_steps steps (repacked, sorted by cell), so
+        # the timed steps see relaxed energies and their real collisions and ionizations
+        evo = jumc.Population(4 * spec.n, parts, table, precision="fp32", seed=seed, mesh=grid)
+        for _ in range(args.pre_steps):
+            streamer.advance_deposit(evo, fld, spec.dt, trk, grid, -1.0)
+            ctx.check(ctx.lib.mcs_repack(evo.h))
+        ctx.check(ctx.lib.mcs_sort_cells(evo.h, grid.h_))
+        ctx.check(ctx.lib.mcs_repack(evo.h))
+        parts = evo.download()
+        evo.close()
+        spec.n = parts.n
+    snap = jumc.Population(spec.n, parts, table, precision="fp32", seed=seed, mesh=grid)
+    pop = jumc.Population(2 * spec.n, None, table, precision="fp32", seed=seed, mesh=grid)
     qpart = torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}") if ws > 1 else None
     n_active = float(parts.active.sum())
 
@@ -339,6 +352,7 @@ def run_mine(args):
                             f"sigma=50um, 1 eV isotropic, synthetic gas 0, dt={spec.dt:g} s, one push+collide+track+"
                             f"CIC-deposit launch per step over the same input cloud",
                 "particles_per_gpu": spec.n, "active_per_step": n_active, "secondaries_per_step": sec_per_step,
+                "input_evolved_steps": args.pre_steps,
                 "step_timing": "CUDA events around zero(qpart)+step kernel(+all-reduce) of each step, summed; the "
                                "device-to-device restore of the input cloud between steps is outside the windows",
                 "ms_per_step_incl_restore": bracket_max / args.steps,
