@@ -60,14 +60,19 @@ def test_config_mesh_step_fp64_matches_oracle(ctx, name, half):
     assert g.n == o.n
     bad = particle_mismatch(g, o, 1e-12, xatol=1e-30, vatol=1e-30)
     assert bad.sum() == 0, f"{bad.sum()} slots differ, worst {vec_relerr(g.x, o.x).max():.3g}"
+    # node totals are exact; a node's value may differ by the per-corner rounding of
+    # fractions that differ at 1e-16 of a position (cell indices up to 1024): a few units of
+    # 2^-32 e, or 1e-12 of the node's charge for the heavy cfg2 weights (up to 1e4 e)
+    def close(a, b):
+        return bool(np.all(np.abs(a - b) <= np.maximum(8, 1e-12 * np.abs(b))))
     qf = grid.read_fixed_box(L.Q_FIXED, lo, hi)
     assert qf.sum() == trk._q.sum()
-    assert np.abs(qf - trk._q).max() <= 8
+    assert close(qf, trk._q)
     qp = grid.read_fixed_box(L.Q_PART, lo, hi)
     dep = po.tracker_cart3d(*nb, spec.h, origin)
     po.deposit(opop, dep, -1.0)
     assert qp.sum() == dep._q.sum() and qp.sum() < 0
-    assert np.abs(qp - dep._q).max() <= 8
+    assert close(qp, dep._q)
     fld.close(); pop.close(); grid.close(); tab.close()
 
 
