@@ -61,10 +61,11 @@ def test_config_mesh_step_fp64_matches_oracle(ctx, name, half):
     bad = particle_mismatch(g, o, 1e-12, xatol=1e-30, vatol=1e-30)
     assert bad.sum() == 0, f"{bad.sum()} slots differ, worst {vec_relerr(g.x, o.x).max():.3g}"
     # node totals are exact; a node's value may differ by the per-corner rounding of
-    # fractions that differ at 1e-16 of a position (cell indices up to 1024): a few units of
-    # 2^-32 e, or 1e-12 of the node's charge for the heavy cfg2 weights (up to 1e4 e)
+    # fractions that differ at 1e-16 of a position (cell indices up to 1024, so ~1e-13 of a
+    # cell): up to ~5 units of 2^-32 e per electron of weight 1e4 at the node -- 32 units where
+    # few electrons meet, 1e-12 of the node's charge where many do
     def close(a, b):
-        return bool(np.all(np.abs(a - b) <= np.maximum(8, 1e-12 * np.abs(b))))
+        return bool(np.all(np.abs(a - b) <= np.maximum(32, 1e-12 * np.abs(b))))
     qf = grid.read_fixed_box(L.Q_FIXED, lo, hi)
     assert qf.sum() == trk._q.sum()
     assert close(qf, trk._q)
