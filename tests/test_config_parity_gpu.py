@@ -65,7 +65,12 @@ def test_config_mesh_step_fp64_matches_oracle(ctx, name, half):
     # cell): up to ~5 units of 2^-32 e per electron of weight 1e4 at the node -- 32 units where
     # few electrons meet, 1e-12 of the node's charge where many do
     def close(a, b):
-        return bool(np.all(np.abs(a - b) <= np.maximum(32, 1e-12 * np.abs(b))))
+        d = np.abs(a - b)
+        bad = d > np.maximum(32, 1e-12 * np.abs(b))
+        if bad.any():
+            k = int(np.argmax(np.where(bad, d, -1)))
+            print(f"worst node {k}: |diff| {d[k]}, value {b[k]}, {int(bad.sum())} nodes beyond the bound")
+        return not bad.any()
     qf = grid.read_fixed_box(L.Q_FIXED, lo, hi)
     assert qf.sum() == trk._q.sum()
     assert close(qf, trk._q)
