@@ -645,7 +645,8 @@ def mesh_kernel_name(ctx) -> str:
     ctx.check(ctx.lib.mcs_ctx_get_option(ctx.h, 1, C.byref(v)))
     b, p, m = C.c_int(), C.c_int(), C.c_int()
     ctx.check(ctx.lib.mcs_mesh_shape(v.value, C.byref(b), C.byref(p), C.byref(m)))
-    return f"k_step_mesh<float,{b.value},{p.value},{m.value}>"
+    refill = {8: 4, 9: 16}.get(v.value, 8)
+    return f"k_step_mesh<float,{b.value},{p.value},{m.value},{refill}>"
 
 
 def run_cfg2(args):

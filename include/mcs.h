@@ -118,10 +118,11 @@ MCS_API int mcs_diag_wait_timeout(mcs_ctx* ctx, uint32_t max_spins);
 /* Tuning options of a context (no counterpart in the reference, which has no kernels).
  * MCS_OPT_MESH_SHAPE selects the kernel shape of the FP32 mesh step (0 .. MCS_MESH_SHAPES-1,
  * 0 = default); every shape computes the same result. */
-enum { MCS_OPT_MESH_SHAPE = 1, MCS_MESH_SHAPES = 8 };
+enum { MCS_OPT_MESH_SHAPE = 1, MCS_MESH_SHAPES = 10 };
 MCS_API int mcs_ctx_set_option(mcs_ctx* ctx, int option, int value);
 MCS_API int mcs_ctx_get_option(mcs_ctx* ctx, int option, int* value);
-/* (threads per block, particles per thread, resident CTAs per SM) of a mesh-step shape. */
+/* (threads per block, particles per thread, resident CTAs per SM) of a mesh-step shape;
+ * shapes 8 and 9 are shape 0 refilling idle lanes at 4 and 16 idle lanes instead of 8. */
 MCS_API int mcs_mesh_shape(int shape, int* block, int* ppt, int* min_blocks);
 /* Waits for queued work; returns (and clears) the sticky device status. */
 MCS_API int mcs_sync(mcs_ctx* ctx);

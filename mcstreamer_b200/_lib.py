@@ -34,7 +34,7 @@ MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
 B_NU, B_NU2, BATCH_MOMENTS, BATCH_LOG, BATCH_VARIANTS = 12, 13, 14, 64, 22
-OPT_MESH_SHAPE, MESH_SHAPES = 1, 8
+OPT_MESH_SHAPE, MESH_SHAPES = 1, 10
 
 vp = C.c_void_p
 i32, i64, u32, u64, f64 = C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_double

@@ -631,7 +631,7 @@ __device__ __forceinline__ bool in_unit_cube(T ox, T oy, T oz) {
     }
 }
 
-template <typename T, int BLOCK, int PPT, int MINB = 1>
+template <typename T, int BLOCK, int PPT, int MINB = 1, int REFILL = 8>
 __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableView tab, GridView g, int tracking, StepCtl C,
                                                      YoshidaC Y, double dep_val) {
     constexpr int TILE = BLOCK * PPT;
@@ -681,11 +681,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
 
         bool pending = false;   // finished particle not yet written back
         for (;;) {
-            // Finished lanes wait until a quarter of the warp is idle (or all of it), then
-            // write back and refill together: the store/load path runs with many lanes
-            // active instead of once per finishing lane.
+            // Finished lanes wait until REFILL lanes of the warp are idle (or all of it),
+            // then write back and refill together: the store/load path runs with many
+            // lanes active instead of once per finishing lane.
             const unsigned idle = __ballot_sync(0xffffffffu, !have);
-            if (idle != 0xffffffffu && __popc(idle) < 8) goto substep;
+            if (idle != 0xffffffffu && __popc(idle) < REFILL) goto substep;
             if (!have && pending) {
                 P.cell[i] = cell_index(g, in, ix, iy, iz);
                 P.f[0][i] = ox; P.f[1][i] = oy; P.f[2][i] = oz;

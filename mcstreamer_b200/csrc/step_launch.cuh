@@ -70,12 +70,12 @@ int launch_step_abs_impl(mcs_pop* p, const mcs_table* t, const mcs_field* f, dou
     return launch_abs_variant<T, BLOCK, PPT, FieldCartAbs, false>(p, t, fg, tg, FieldCartAbs{}, dt, 0, 0, 0, mom);
 }
 
-template <typename T, int BLOCK, int PPT, int MINB = 1>
+template <typename T, int BLOCK, int PPT, int MINB = 1, int REFILL = 8>
 int launch_step_mesh_impl(mcs_pop* p, const mcs_table* t, double dt, bool tracking, double dep_val, double* mom) {
     mcs_ctx* c = p->ctx;
     if (p->inj) return set_err(c, MCS_ERR_UNSUPPORTED, "injected uniforms on a mesh-layout population");
     constexpr int TILE = BLOCK * PPT;
-    auto kern = k_step_mesh<T, BLOCK, PPT, MINB>;
+    auto kern = k_step_mesh<T, BLOCK, PPT, MINB, REFILL>;
     const int grid = persistent_grid(c, kern, BLOCK, (p->cap + TILE - 1) / TILE);
     YoshidaHost yh;
     YoshidaC Y{yh.c1, yh.c2, yh.c3, yh.c4, yh.d1, yh.d2, yh.d3, (-kElementaryCharge) / kElectronMass};
