@@ -645,8 +645,7 @@ def mesh_kernel_name(ctx) -> str:
     ctx.check(ctx.lib.mcs_ctx_get_option(ctx.h, 1, C.byref(v)))
     b, p, m = C.c_int(), C.c_int(), C.c_int()
     ctx.check(ctx.lib.mcs_mesh_shape(v.value, C.byref(b), C.byref(p), C.byref(m)))
-    refill = {8: 4, 9: 16}.get(v.value, 8)
-    return f"k_step_mesh<float,{b.value},{p.value},{m.value},{refill}>"
+    return f"k_step_mesh<float,{b.value},{p.value},{m.value},8>"
 
 
 def run_cfg2(args):
@@ -679,6 +678,7 @@ def run_cfg2(args):
     pop = jumc.Population(cap, None, table, precision="fp32", seed=seed, mesh=grid)
     pop.init_cloud(spec.n, spec.centre, workloads.CLOUD_SIGMA, workloads.CLOUD_ENERGY_EV, *spec.weight)
     ctx.check(ctx.lib.mcs_sort_cells(pop.h, grid.h_))
+    streamer.reserve_resample(pop)   # the resample! scratch, allocated before the timed steps
     fld = streamer.FieldInterp(grid)
     trk = streamer.CollisionTracker(grid)
     qpart = torch.as_tensor(grid.charge_array(L.Q_PART), device=f"cuda:{local}") if ws > 1 else None

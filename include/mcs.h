@@ -118,11 +118,10 @@ MCS_API int mcs_diag_wait_timeout(mcs_ctx* ctx, uint32_t max_spins);
 /* Tuning options of a context (no counterpart in the reference, which has no kernels).
  * MCS_OPT_MESH_SHAPE selects the kernel shape of the FP32 mesh step (0 .. MCS_MESH_SHAPES-1,
  * 0 = default); every shape computes the same result. */
-enum { MCS_OPT_MESH_SHAPE = 1, MCS_MESH_SHAPES = 10 };
+enum { MCS_OPT_MESH_SHAPE = 1, MCS_MESH_SHAPES = 8 };
 MCS_API int mcs_ctx_set_option(mcs_ctx* ctx, int option, int value);
 MCS_API int mcs_ctx_get_option(mcs_ctx* ctx, int option, int* value);
-/* (threads per block, particles per thread, resident CTAs per SM) of a mesh-step shape;
- * shapes 8 and 9 are shape 0 refilling idle lanes at 4 and 16 idle lanes instead of 8. */
+/* (threads per block, particles per thread, resident CTAs per SM) of a mesh-step shape. */
 MCS_API int mcs_mesh_shape(int shape, int* block, int* ppt, int* min_blocks);
 /* Waits for queued work; returns (and clears) the sticky device status. */
 MCS_API int mcs_sync(mcs_ctx* ctx);
@@ -272,6 +271,10 @@ MCS_API int mcs_swarm_resample(mcs_pop* p, int64_t n0, double tol);
 MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid* g);
 /* resample!(popl, fields, ntarget, nmax) (MCStreamer/src/resample.jl:7-77). */
 MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax);
+/* Allocates now, for the population's capacity, the device scratch that mcs_sort_cells and
+ * mcs_resample_cells otherwise allocate on their first call (several GB for 1e8 slots), so
+ * that a time-stepping loop does not pay it inside a step.  No counterpart in the reference. */
+MCS_API int mcs_resample_reserve(mcs_pop* p);
 /* Moments over the population (layout MCS_M_*), table may be NULL (no rate sums). */
 MCS_API int mcs_moments(mcs_pop* p, const mcs_table* t, double* out, int nout);
 

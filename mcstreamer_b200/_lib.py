@@ -34,7 +34,7 @@ MOMENTS_BASE = 18
 M_COUNT, M_W, M_X, M_X2, M_V, M_E, M_WE, M_EMAX, M_WX, M_WX2 = 0, 1, 2, 5, 8, 11, 12, 13, 14, 17
 S_COUNT, S_W, S_X, S_X2, S_V, S_E, STEP_MOMENTS = 0, 1, 2, 5, 8, 11, 12
 B_NU, B_NU2, BATCH_MOMENTS, BATCH_LOG, BATCH_VARIANTS = 12, 13, 14, 64, 22
-OPT_MESH_SHAPE, MESH_SHAPES = 1, 10
+OPT_MESH_SHAPE, MESH_SHAPES = 1, 8
 
 vp = C.c_void_p
 i32, i64, u32, u64, f64 = C.c_int, C.c_int64, C.c_uint32, C.c_uint64, C.c_double
@@ -87,6 +87,7 @@ SIGNATURES = {
     "mcs_swarm_resample": (i32, [vp, i64, f64]),
     "mcs_sort_cells": (i32, [vp, vp]),
     "mcs_resample_cells": (i32, [vp, vp, i32, i32]),
+    "mcs_resample_reserve": (i32, [vp]),
     "mcs_moments": (i32, [vp, vp, pd, i32]),
     "mcs_swarm_run": (i32, [vp, vp, vp, f64, i32, i64, f64, i32, pd]),
     "mcs_pop_step_log": (i32, [vp, i32]),

@@ -190,7 +190,7 @@ MCS_API int mcs_table_create(mcs_ctx* c, int nrows, int neps, double e0, double 
     t->ctx = c;
     TableView& v = t->v;
     v.nrows = nrows;
-    v.nrp = (nrows + 3) & ~3;
+    v.nrp = (nrows + 4) & ~3;   // the total real rate, then the rows, padded to 4
     v.neps = neps;
     v.e0 = e0;
     v.emax = emax;
@@ -210,8 +210,14 @@ MCS_API int mcs_table_create(mcs_ctx* c, int nrows, int neps, double e0, double 
     if (!st) st = dalloc(c, &t->d_rate32, n32);
     if (st) { cudaFree(t->d_rate64); delete t; return st; }
     std::vector<float> r32(n32, 0.0f);
-    for (int k = 0; k < neps; ++k)
-        for (int j = 0; j < nrows; ++j) r32[(size_t)k * v.nrp + j] = (float)rate[(size_t)k * nrows + j];
+    for (int k = 0; k < neps; ++k) {
+        double tot = 0.0;
+        for (int j = 0; j < nrows; ++j) {
+            tot += rate[(size_t)k * nrows + j];
+            r32[(size_t)k * v.nrp + 1 + j] = (float)rate[(size_t)k * nrows + j];
+        }
+        r32[(size_t)k * v.nrp] = (float)tot;
+    }
     cudaError_t e1 = cudaMemcpy(t->d_rate64, rate, n64 * sizeof(double), cudaMemcpyHostToDevice);
     cudaError_t e2 = cudaMemcpy(t->d_rate32, r32.data(), n32 * sizeof(float), cudaMemcpyHostToDevice);
     if (e1 != cudaSuccess || e2 != cudaSuccess) {

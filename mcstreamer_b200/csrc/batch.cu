@@ -164,7 +164,7 @@ __device__ __forceinline__ float rate_row32(const TableView& t, float v2, int j)
     float w;
     if (!(u >= 0.0f && k <= t.neps - 2)) { k = u >= 0.0f ? t.neps - 2 : 0; w = u >= 0.0f ? 0.0f : 1.0f; }
     else w = (float)(k + 1) - u;
-    const float a = __ldg(t.rate32 + (size_t)k * t.nrp + j), b = __ldg(t.rate32 + (size_t)(k + 1) * t.nrp + j);
+    const float a = __ldg(t.rate32 + (size_t)k * t.nrp + 1 + j), b = __ldg(t.rate32 + (size_t)(k + 1) * t.nrp + 1 + j);
     return fmaf(w, a - b, b);
 }
 

@@ -20,7 +20,7 @@ enum FieldType { FIELD_UNIFORM = 0, FIELD_GRID = 1 };
 // ---- kernel-side views (trivially copyable) ----
 struct TableView {
     const double* rate64;   // [neps][nrows]
-    const float* rate32;    // [neps][nrp] (nrp = nrows rounded up to 4)
+    const float* rate32;    // [neps][nrp]: the total real rate, then the rows (nrp = nrows + 1 rounded up to 4)
     int nrows, nrp, neps;
     double e0, emax, step, maxrate, inv_maxrate;
     float ke32, e0n32, maxrate32;  // u = v^2*ke32 - e0n32 in grid units

@@ -533,9 +533,10 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_write(ResampleArg
 
 }  // namespace
 
-// Sort the population by cell key; on return the sorted keys are in *keys_out (device).
-template <typename T>
-int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
+// Scratch of the sort (keys, slots, digit tables and the second set of population arrays)
+// and, with `resample`, of the per-cell resampling, sized for the population's capacity.
+// Allocated once, on first use or by mcs_resample_reserve.
+int reserve_sort_scratch(mcs_pop* p, bool resample) {
     mcs_ctx* c = p->ctx;
     const size_t cap = (size_t)p->cap;
     const long long ntiles_max = (p->cap + STILE - 1) / STILE;
@@ -545,6 +546,25 @@ int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
     }
     if (int st = ensure(c, &p->sort_hist, (size_t)RADIX * ntiles_max)) return st;
     if (int st = ensure(c, &p->sort_hoff, (size_t)RADIX * ntiles_max)) return st;
+    for (int q = 0; q < 8; ++q)
+        if (!p->alt[q] && cudaMalloc(&p->alt[q], cap * p->esz) != cudaSuccess)
+            return set_err(c, MCS_ERR_NOMEM, "sort buffers");
+    if (int st = ensure(c, &p->alt_act, cap)) return st;
+    if (p->cell)
+        if (int st = ensure(c, &p->alt_cell, cap)) return st;
+    if (resample) {
+        if (int st = ensure(c, &p->seg_a, cap)) return st;
+        if (int st = ensure(c, &p->seg_b, cap)) return st;
+    }
+    return MCS_OK;
+}
+
+// Sort the population by cell key; on return the sorted keys are in *keys_out (device).
+template <typename T>
+int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
+    mcs_ctx* c = p->ctx;
+    const long long ntiles_max = (p->cap + STILE - 1) / STILE;
+    if (int st = reserve_sort_scratch(p, false)) return st;
     const uint32_t ncells = grid_cells(g);
     int nbits = 1;
     while (nbits < 32 && ((1ull << nbits) <= (unsigned long long)ncells)) ++nbits;
@@ -571,12 +591,6 @@ int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
         cur ^= 1;
     }
     // permute every population array into the second buffer set, then swap the sets
-    for (int q = 0; q < 8; ++q)
-        if (!p->alt[q] && cudaMalloc(&p->alt[q], cap * p->esz) != cudaSuccess)
-            return set_err(c, MCS_ERR_NOMEM, "sort buffers");
-    if (int st = ensure(c, &p->alt_act, cap)) return st;
-    if (p->cell)
-        if (int st = ensure(c, &p->alt_cell, cap)) return st;
     DstArrays d;
     for (int q = 0; q < 8; ++q) d.f[q] = p->alt[q];
     d.cell = p->cell ? p->alt_cell : nullptr;
@@ -594,9 +608,8 @@ template <typename T>
 int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
     mcs_ctx* c = p->ctx;
     uint32_t* keys = nullptr;
+    if (int st = reserve_sort_scratch(p, true)) return st;
     if (int st = sort_cells_t<T>(p, g, &keys)) return st;
-    if (int st = ensure(c, &p->seg_a, (size_t)p->cap)) return st;
-    if (int st = ensure(c, &p->seg_b, (size_t)p->cap)) return st;
     const uint32_t ncells = grid_cells(g);
     const long long* n_dev = p->d_n + p->cur;
     long long* nseg = reinterpret_cast<long long*>(p->counters + 10);
@@ -623,7 +636,6 @@ int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
         MCS_CK_LAUNCH(c);
     } else {
         // merging cells hold more than nmax particles each: at most n / (nmax + 1) of them
-        if (int st = ensure(c, &p->u32b, (size_t)p->cap)) return st;
         unsigned long long* merge_n = reinterpret_cast<unsigned long long*>(p->counters + 14);
         MCS_CK(c, cudaMemsetAsync(merge_n, 0, sizeof(unsigned long long), c->stream));
         k_resample_count<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, p->u32b, merge_n);
@@ -660,6 +672,12 @@ MCS_API int mcs_sort_cells(mcs_pop* p, mcs_grid* g) {
     if (p->cells && p->cells != g) return set_err(p->ctx, MCS_ERR_UNSUPPORTED, "sort by another mesh");
     if (cudaSetDevice(p->ctx->device) != cudaSuccess) return MCS_ERR_CUDA;
     return p->precision == MCS_FP32 ? sort_cells_t<float>(p, g, nullptr) : sort_cells_t<double>(p, g, nullptr);
+}
+
+MCS_API int mcs_resample_reserve(mcs_pop* p) {
+    if (!p) return MCS_ERR_ARG;
+    if (cudaSetDevice(p->ctx->device) != cudaSuccess) return MCS_ERR_CUDA;
+    return reserve_sort_scratch(p, true);
 }
 
 MCS_API int mcs_resample_cells(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {

@@ -77,8 +77,11 @@ __device__ __forceinline__ int select_row64(const TableView& t, double eng, doub
 
 // FP32 selection, u = v^2 * (m/2/step) - e0/step being the position on the energy grid, in
 // two halves so that the first rows' loads are in flight while the caller draws xi:
-// select32_begin places the energy on the grid and loads the first four rows of both
-// columns; select32_finish scans them (and the rest) against xi.
+// select32_begin places the energy on the grid and loads the first quad of both columns
+// (the total real rate and rows 0-2); select32_finish tests xi against the interpolated
+// total first -- most events are null collisions and end there -- and otherwise scans the
+// rows against xi.  The FP32 mode is statistically, not bitwise, the reference's: the total
+// test and the scan can disagree only within a rounding of the total.
 struct Sel32 {
     int k;
     float w;
@@ -102,15 +105,24 @@ __device__ __forceinline__ int select32_finish(const TableView& t, const Sel32& 
     if (s.bad && !(flags & FLAG_CLAMP)) atomicOr(status, ST_ENERGY);
     const float w = s.w;
     float4 a = s.a, b = s.b;
+    if (!(xi < fmaf(w, a.x - b.x, b.x))) return -1;   // beyond the total real rate: null
+    // row r sits at element r + 1 of the quads
+    float nu = fmaf(w, a.y - b.y, b.y);
+    if (nu > xi) return 0;
+    xi -= nu;
+    nu = fmaf(w, a.z - b.z, b.z);
+    if (nu > xi) return 1 < t.nrows ? 1 : -1;
+    xi -= nu;
+    nu = fmaf(w, a.w - b.w, b.w);
+    if (nu > xi) return 2 < t.nrows ? 2 : -1;
+    xi -= nu;
     const int nq = t.nrp >> 2;
-    for (int q = 0; q < nq; ++q) {
-        if (q) {
-            a = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)s.k * t.nrp) + q);
-            b = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)(s.k + 1) * t.nrp) + q);
-        }
-        const int j = q << 2;
-        float nu = fmaf(w, a.x - b.x, b.x);
-        if (nu > xi) return j;
+    for (int q = 1; q < nq; ++q) {
+        a = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)s.k * t.nrp) + q);
+        b = __ldg(reinterpret_cast<const float4*>(t.rate32 + (size_t)(s.k + 1) * t.nrp) + q);
+        const int j = (q << 2) - 1;
+        nu = fmaf(w, a.x - b.x, b.x);
+        if (nu > xi) return j < t.nrows ? j : -1;
         xi -= nu;
         nu = fmaf(w, a.y - b.y, b.y);
         if (nu > xi) return j + 1 < t.nrows ? j + 1 : -1;

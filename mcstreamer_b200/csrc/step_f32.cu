@@ -13,10 +13,9 @@ int launch_collisions<float>(mcs_pop* p, const mcs_table* t, double dt, mcs_grid
     return launch_collisions_impl<float, 256, 2>(p, t, dt, trk);
 }
 // Kernel shapes of the FP32 mesh step: (threads per block, particles per thread, resident
-// CTAs per SM the register budget is set for); shapes 8 and 9 refill a warp's lanes when 4
-// or 16 of them are idle instead of 8.  Shape 0 is the default.
-const int kMeshShapes[][3] = {{256, 8, 3}, {256, 8, 4}, {256, 16, 3}, {256, 16, 4}, {128, 16, 6}, {128, 16, 8},
-                              {512, 8, 2}, {256, 32, 3}, {256, 8, 3}, {256, 8, 3}};
+// CTAs per SM the register budget is set for).  Shape 0 is the default.
+const int kMeshShapes[][3] = {{256, 8, 3}, {256, 8, 4}, {256, 16, 3}, {256, 16, 4},
+                              {128, 16, 6}, {128, 16, 8}, {512, 8, 2}, {256, 32, 3}};
 constexpr int kNumMeshShapes = sizeof(kMeshShapes) / sizeof(kMeshShapes[0]);
 static_assert(kNumMeshShapes == MCS_MESH_SHAPES, "shape table and header disagree");
 
@@ -30,8 +29,6 @@ int launch_step_mesh<float>(mcs_pop* p, const mcs_table* t, double dt, bool trac
     case 5: return launch_step_mesh_impl<float, 128, 16, 8>(p, t, dt, tracking, dep_val, mom);
     case 6: return launch_step_mesh_impl<float, 512, 8, 2>(p, t, dt, tracking, dep_val, mom);
     case 7: return launch_step_mesh_impl<float, 256, 32, 3>(p, t, dt, tracking, dep_val, mom);
-    case 8: return launch_step_mesh_impl<float, 256, 8, 3, 4>(p, t, dt, tracking, dep_val, mom);
-    case 9: return launch_step_mesh_impl<float, 256, 8, 3, 16>(p, t, dt, tracking, dep_val, mom);
     default: return launch_step_mesh_impl<float, 256, 8, 3>(p, t, dt, tracking, dep_val, mom);
     }
 }

@@ -195,39 +195,42 @@ __device__ __forceinline__ long long next_tile(SH& sh, const StepCtl& C, long lo
     return tile < ntiles ? tile : -1;
 }
 
-// Shared collision body: select a process for velocity (vx, vy, vz) and apply it in place.
-// Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
-template <typename T, typename RowsT, class Ev>
-__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Ev& rng,
-                                            T& vx, T& vy, T& vz, Sec<T>& sec, int* row_out = nullptr) {
-    int j;
-    double eng = 0.0;
-    float v2 = 0.0f;
+// Process selection of one collision event (do_one_collision!, collisions.jl:159-192): draws
+// the event's block and returns the selected row, or -1 for a null collision.
+template <typename T, class Ev>
+__device__ __forceinline__ int select_event(const TableView& tab, const StepCtl& C, Ev& rng, T vx, T vy, T vz) {
     if constexpr (sizeof(T) == 8) {
         rng.begin();
-        eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+        const double eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
         const double xi = rng.template xi<double>() * tab.maxrate;
-        j = select_row64(tab, eng, xi, C.flags, C.status);
+        return select_row64(tab, eng, xi, C.flags, C.status);
     } else {
         // the first rows' loads go out before the event's block is drawn
-        v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
+        const float v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
         Sel32 sel;
         select32_begin(tab, v2, sel);
         rng.begin();
         const float xi = rng.template xi<float>() * tab.maxrate32;
-        j = select32_finish(tab, sel, xi, C.flags, C.status);
+        return select32_finish(tab, sel, xi, C.flags, C.status);
     }
-    const int kind = j >= 0 ? rows.kind[j] : K_NULL;
-    if (row_out) *row_out = j;
-    if (kind == K_NULL) return OUT_NONE;
+}
+
+// The collision of a selected row `j` of kind `kind` (not K_NULL), applied to the velocity
+// in place.  Returns OUT_CHANGE, OUT_NEW (sec filled), OUT_REMOVE or OUT_PHOTO.  The energy
+// is recomputed from the velocity by the selection's expression.
+template <typename T, typename RowsT, class Ev>
+__device__ __forceinline__ int collide_row(const RowsT& rows, int j, int kind, Ev& rng, T& vx, T& vy, T& vz,
+                                           Sec<T>& sec) {
     int out;
     if constexpr (sizeof(T) == 8) {
+        const double eng = 0.5 * kElectronMass * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
         Sec<double> s64;
         double a = vx, b = vy, c = vz;
         out = collide64(kind, (double)rows.par[j], eng, rng, a, b, c, s64);
         vx = a; vy = b; vz = c;
         sec.vx = s64.vx; sec.vy = s64.vy; sec.vz = s64.vz; sec.s = s64.s;
     } else {
+        const float v2 = fmaf(vx, vx, fmaf(vy, vy, vz * vz));
         Sec<float> s32;
         float a = vx, b = vy, c = vz;
         out = collide32(kind, (float)rows.par[j], v2, rng, a, b, c, s32);
@@ -235,6 +238,18 @@ __device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& 
         sec.vx = s32.vx; sec.vy = s32.vy; sec.vz = s32.vz; sec.s = s32.s;
     }
     return out == OUT_NONE ? OUT_CHANGE : out;
+}
+
+// Shared collision body: select a process for velocity (vx, vy, vz) and apply it in place.
+// Returns OUT_NONE (null collision), OUT_CHANGE, OUT_NEW (sec filled) or OUT_REMOVE.
+template <typename T, typename RowsT, class Ev>
+__device__ __forceinline__ int collide_once(const RowsT& rows, const TableView& tab, const StepCtl& C, Ev& rng,
+                                            T& vx, T& vy, T& vz, Sec<T>& sec, int* row_out = nullptr) {
+    const int j = select_event<T>(tab, C, rng, vx, vy, vz);
+    const int kind = j >= 0 ? rows.kind[j] : K_NULL;
+    if (row_out) *row_out = j;
+    if (kind == K_NULL) return OUT_NONE;
+    return collide_row<T>(rows, j, kind, rng, vx, vy, vz, sec);
 }
 
 // apply!(::MultiplePhotonOutcome) of an electron's photo-emission (electron.jl:141-144,
@@ -679,6 +694,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             vx += k * ex; vy += k * ey; vz += k * ez;
         };
 
+        // the collision of a selected row (not a null one) of the lane's particle
+        auto real_collision = [&](int row) {
+            Sec<T> sec;
+            const int out = collide_row<T>(sh.rows, row, sh.rows.kind[row], rng, vx, vy, vz, sec);
+            if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
+            if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
+                cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
+                          out == OUT_NEW ? (double)w : -(double)w, C.status);
+            if (out == OUT_NEW) {
+                const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
+                stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
+            } else if (out == OUT_REMOVE) {
+                act = 0;
+            }
+        };
+
         bool pending = false;   // finished particle not yet written back
         for (;;) {
             // Finished lanes wait until REFILL lanes of the warp are idle (or all of it),
@@ -746,18 +777,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             kick(kd3 * tt);
             drift(cd4 * tt);
             if (collides) {
-                Sec<T> sec;
-                const int out = collide_once<T>(sh.rows, tab, C, rng, vx, vy, vz, sec);
-                if (out == OUT_PHOTO) atomicOr(C.status, ST_UNSUPPORTED);
-                if ((out == OUT_NEW || out == OUT_REMOVE) && tracking && in)
-                    cic_fixed(g.qfixed, g.nx, g.ny, ix, iy, iz, (double)ox, (double)oy, (double)oz,
-                              out == OUT_NEW ? (double)w : -(double)w, C.status);
-                if (out == OUT_NEW) {
-                    const T vals[8] = {ox, oy, oz, sec.vx, sec.vy, sec.vz, w, sec.s};
-                    stage(sg, &sh.count, local, ev++, vals, cell_index(g, in, ix, iy, iz), act, C.status);
-                } else if (out == OUT_REMOVE) {
-                    act = 0;
-                }
+                const int row = select_event<T>(tab, C, rng, vx, vy, vz);
+                if (row >= 0 && sh.rows.kind[row] != K_NULL) real_collision(row);
+                // the next free flight comes from the event's block, whatever the outcome
                 if constexpr (sizeof(T) == 8) s = -log(rng.template snew<double>());
                 else s = (double)M<float>::nlog(rng.template snew<float>());
             }

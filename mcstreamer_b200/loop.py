@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 from typing import Callable, List, Optional
 
 from . import fieldsio, jumc
-from .streamer import CollisionTracker, GridCyl, density, diagnostics, resample
+from .streamer import CollisionTracker, GridCyl, density, diagnostics, reserve_resample, resample
 
 
 class TimeStepper:
@@ -85,6 +85,7 @@ def nsteps(s: Streamer, n: int, ntarget: int, nmax: int, eb: float, dt: float, d
     poisson = TimeStepper(dt_poisson)
     output = TimeStepper(dt_output)
     resampler = TimeStepper(dt_resample, start=dt)
+    reserve_resample(s.electrons)
     out: List[dict] = []
     tick = mark if mark is not None else (lambda name: None)
     for i in range(1, n + 1):

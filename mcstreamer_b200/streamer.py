@@ -257,6 +257,13 @@ def resample(popl: Population, grid, ntarget: int, nmax: int) -> None:
     popl.ctx.check(popl.ctx.lib.mcs_resample_cells(popl.h, grid.h_, int(ntarget), int(nmax)))
 
 
+def reserve_resample(popl: Population) -> None:
+    """Allocate the device scratch of resample! (the cell sort's keys and second population
+    arrays, the segment tables) for the population's capacity now, so that no later
+    resample! allocates inside a time step."""
+    popl.ctx.check(popl.ctx.lib.mcs_resample_reserve(popl.h))
+
+
 def diagnostics(popl: Population, photons=None) -> dict:
     """The per-step diagnostics of nsteps (MCStreamer/src/main.jl:269-279): meanenergy and
     maxenergy of the electrons (J), their actives and weight, and the photons' actives and

@@ -43,6 +43,7 @@ def test_nsteps_call_order(monkeypatch, tmp_path):
     monkeypatch.setattr(loop, "density", rec("density"))
     monkeypatch.setattr(loop, "diagnostics", lambda e, p: {})
     monkeypatch.setattr(loop, "resample", rec("resample"))
+    monkeypatch.setattr(loop, "reserve_resample", lambda p: None)   # scratch allocation only
     monkeypatch.setattr(loop.jumc, "advance_mixed", rec("advance"))
     monkeypatch.setattr(loop.jumc, "repack", rec("repack"))
     monkeypatch.setattr(loop.fieldsio, "savefields", rec("save"))
@@ -70,6 +71,7 @@ def test_nsteps_without_photons_or_fluid(monkeypatch):
     monkeypatch.setattr(loop, "density", rec("density"))
     monkeypatch.setattr(loop, "diagnostics", lambda e, p: {})
     monkeypatch.setattr(loop, "resample", rec("resample"))
+    monkeypatch.setattr(loop, "reserve_resample", lambda p: None)   # scratch allocation only
     monkeypatch.setattr(loop.jumc, "advance", rec("advance"))
     monkeypatch.setattr(loop.jumc, "advance_mixed", rec("mixed"))
     monkeypatch.setattr(loop.jumc, "repack", rec("repack"))
