@@ -550,14 +550,14 @@ MCS_API int mcs_pop_create(mcs_ctx* c, int64_t capacity, int precision, mcs_grid
     size_t npart = (size_t)p->max_tiles * kStepMoments;
     if (npart < (size_t)kMomentPartialsMin) npart = kMomentPartialsMin;
     if (!st) st = dalloc(c, &p->tile_partials, npart);
-    if (!st) st = dalloc(c, &p->counters, 16);
+    if (!st) st = dalloc(c, &p->counters, kCounterWords);
     if (!st) st = dalloc(c, &p->d_moments, MCS_MOMENTS_BASE + kMaxRows);
     if (!st) st = dalloc(c, &p->u32a, (size_t)capacity);
     if (!st) st = dalloc(c, &p->u32b, (size_t)capacity);
     if (st) { mcs_pop_destroy(p); return st; }
     cudaMemset(p->d_n, 0, 2 * sizeof(long long));
     cudaMemset(p->tile_status, 0, (size_t)p->max_tiles * sizeof(unsigned long long));
-    cudaMemset(p->counters, 0, 16 * sizeof(uint32_t));
+    cudaMemset(p->counters, 0, kCounterWords * sizeof(uint32_t));
     cudaMemset(p->act, 0, (size_t)capacity);
     if (cudaDeviceSynchronize() != cudaSuccess) { mcs_pop_destroy(p); return set_err(c, MCS_ERR_CUDA, "pop init"); }
     *out = p;
@@ -571,6 +571,7 @@ MCS_API int mcs_pop_destroy(mcs_pop* p) {
     for (int q = 0; q < 8; ++q) { cudaFree(p->f[q]); cudaFree(p->alt[q]); }
     cudaFree(p->act); cudaFree(p->cell); cudaFree(p->d_n); cudaFree(p->tile_status);
     cudaFree(p->tile_partials); cudaFree(p->counters); cudaFree(p->d_moments); cudaFree(p->staging);
+    cudaFree(p->app_cnt); cudaFree(p->app_off); cudaFree(p->app_excl);
     cudaFree(p->u32a); cudaFree(p->u32b); cudaFree(p->alt_cell); cudaFree(p->alt_act); cudaFree(p->stage); cudaFree(p->d_log);
     for (int q = 0; q < 2; ++q) { cudaFree(p->sort_key[q]); cudaFree(p->sort_val[q]); }
     cudaFree(p->sort_hist); cudaFree(p->sort_hoff); cudaFree(p->seg_a); cudaFree(p->seg_b);

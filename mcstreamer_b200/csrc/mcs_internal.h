@@ -12,6 +12,9 @@ namespace mcs {
 
 constexpr int kMaxRows = 32;      // table rows (processes incl. null)
 constexpr int kStepMoments = 12;  // fused per-step moments, see StepMoment
+// device counter words of a population: [0..1] step tiles, [2..3] scan, [4..7] repack and
+// swarm resample, [8..9] sort, [10..15] resample, [16..17] the mesh step's secondary pool
+constexpr int kCounterWords = 32;
 enum StepMoment { SM_COUNT = 0, SM_W, SM_X, SM_Y, SM_Z, SM_XX, SM_YY, SM_ZZ, SM_VX, SM_VY, SM_VZ, SM_E };
 
 enum GridType { GRID_CART3D = 1, GRID_CYL = 2 };
@@ -117,7 +120,7 @@ struct StepCtl {
     uint32_t step, tag, flags, epoch;
     uint32_t* status;         // sticky status word
     unsigned long long* tile_status;
-    uint32_t* counters;       // [0] tile ticket, [1] CTA done count
+    uint32_t* counters;       // [0] tile ticket, [1] CTA done count (kCounterWords words)
     double* tile_partials;    // [tile][kStepMoments]
     double* moments_out;      // kStepMoments doubles or nullptr
     double dt;
@@ -131,6 +134,15 @@ struct StepCtl {
     long long* inj_pos;
     const long long* inj_end;
     long long inj_n;          // slots with a range
+    // secondary pool of the mesh step: each tile reserves app_cnt[tile] entries at
+    // app_off[tile] (from pool_top), in the order of its parents; k_pool_scan/k_pool_copy
+    // then append them after the population in tile order
+    void* pool_f[8];
+    uint32_t* pool_cell;
+    uint8_t* pool_act;
+    unsigned long long* pool_top;
+    uint32_t* app_cnt;
+    unsigned long long* app_off;
 };
 
 }  // namespace mcs
@@ -222,7 +234,7 @@ struct mcs_pop {
     unsigned long long* tile_status = nullptr;
     long long max_tiles = 0;
     double* tile_partials = nullptr;
-    uint32_t* counters = nullptr;  // 8 words
+    uint32_t* counters = nullptr;  // kCounterWords words
     double* d_moments = nullptr;   // kStepMoments
     void* staging = nullptr;       // host<->device transfer staging
     size_t staging_bytes = 0;
@@ -239,6 +251,10 @@ struct mcs_pop {
     uint32_t* sort_hoff = nullptr;
     uint32_t* seg_a = nullptr;                    // resample segment scratch (cap entries)
     uint32_t* seg_b = nullptr;
+    uint32_t* app_cnt = nullptr;             // mesh step: secondaries per tile
+    unsigned long long* app_off = nullptr;   // their pool offset
+    unsigned long long* app_excl = nullptr;  // and their offset after the population
+    long long app_tiles = 0;
     double* d_log = nullptr;       // per-step fused moments, log_cap entries of kStepMoments
     int log_cap = 0;
     uint32_t log_step0 = 0;

@@ -30,5 +30,9 @@ int sync_status(mcs_ctx* c);
 double* log_slot(mcs_pop* p);
 // (threads per block, particles per thread, CTAs per SM) of an FP32 mesh-step shape.
 int mesh_shape_info(int shape, int* block, int* ppt, int* minb);
+// The population's second set of arrays (cap slots), allocated on first use.
+int reserve_alt(mcs_pop* p);
+// That and the per-tile tables of the mesh step's secondary pool.
+int reserve_mesh_pool(mcs_pop* p);
 constexpr int kMomentPartialsMin = 148 * 2 * (MCS_MOMENTS_BASE + kMaxRows);
 }  // namespace mcs

@@ -533,6 +533,31 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_write(ResampleArg
 
 }  // namespace
 
+// The second set of population arrays (cap slots): the sort's permutation target and the
+// mesh step's secondary pool.
+int reserve_alt(mcs_pop* p) {
+    mcs_ctx* c = p->ctx;
+    const size_t cap = (size_t)p->cap;
+    for (int q = 0; q < 8; ++q)
+        if (!p->alt[q] && cudaMalloc(&p->alt[q], cap * p->esz) != cudaSuccess)
+            return set_err(c, MCS_ERR_NOMEM, "second population arrays");
+    if (int st = ensure(c, &p->alt_act, cap)) return st;
+    if (p->cell)
+        if (int st = ensure(c, &p->alt_cell, cap)) return st;
+    return MCS_OK;
+}
+
+// The mesh step's secondary pool (the second set of arrays) and its per-tile tables.
+int reserve_mesh_pool(mcs_pop* p) {
+    mcs_ctx* c = p->ctx;
+    if (int st = reserve_alt(p)) return st;
+    const size_t nt = (size_t)p->max_tiles;
+    if (int st = ensure(c, &p->app_cnt, nt)) return st;
+    if (int st = ensure(c, &p->app_off, nt)) return st;
+    if (int st = ensure(c, &p->app_excl, nt)) return st;
+    return MCS_OK;
+}
+
 // Scratch of the sort (keys, slots, digit tables and the second set of population arrays)
 // and, with `resample`, of the per-cell resampling, sized for the population's capacity.
 // Allocated once, on first use or by mcs_resample_reserve.
@@ -546,12 +571,7 @@ int reserve_sort_scratch(mcs_pop* p, bool resample) {
     }
     if (int st = ensure(c, &p->sort_hist, (size_t)RADIX * ntiles_max)) return st;
     if (int st = ensure(c, &p->sort_hoff, (size_t)RADIX * ntiles_max)) return st;
-    for (int q = 0; q < 8; ++q)
-        if (!p->alt[q] && cudaMalloc(&p->alt[q], cap * p->esz) != cudaSuccess)
-            return set_err(c, MCS_ERR_NOMEM, "sort buffers");
-    if (int st = ensure(c, &p->alt_act, cap)) return st;
-    if (p->cell)
-        if (int st = ensure(c, &p->alt_cell, cap)) return st;
+    if (int st = reserve_alt(p)) return st;
     if (resample) {
         if (int st = ensure(c, &p->seg_a, cap)) return st;
         if (int st = ensure(c, &p->seg_b, cap)) return st;

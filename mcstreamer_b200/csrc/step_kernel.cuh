@@ -27,6 +27,7 @@ struct TileShared {
     uint32_t excl;
     int ok;
     int last;
+    unsigned long long pool_off;     // mesh step: the tile's first pool entry
 };
 
 // Add one particle to the step sums m[0..kStepMoments).  Every product and sum is rounded
@@ -818,13 +819,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             }
         }
 
-        const uint32_t cnt = tile_append<T, BLOCK, TILE>(
-            sh, sg, C, tile, ntiles, n_entry, P.cap, P.n_out, [&](uint32_t e, long long dst) {
+        // The tile's secondaries go to the pool in their serial order (parent, event), at
+        // entries reserved without waiting for the tiles before it; k_pool_copy appends
+        // the tiles' runs after the population in tile order once every tile is done.
+        const uint32_t cnt = sh.count < sg.cap ? sh.count : sg.cap;
+        block_scan_counts<BLOCK, TILE>(sh);
+        if (threadIdx.x == 0) {
+            const unsigned long long off = cnt ? atomicAdd(C.pool_top, (unsigned long long)cnt) : 0ull;
+            sh.pool_off = off;
+            C.app_cnt[tile] = cnt;
+            C.app_off[tile] = off;
+        }
+        __syncthreads();
+        const unsigned long long poff = sh.pool_off;
+        for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
+            const uint32_t key = sg.key[e];
+            const unsigned long long q = poff + sh.cnt[key >> 16] + (key & 0xffffu);
+            if (q >= (unsigned long long)P.cap) { atomicOr(C.status, ST_CAPACITY); continue; }
 #pragma unroll
-                for (int q = 0; q < 8; ++q) P.f[q][dst] = sg.f[q][e];
-                P.cell[dst] = sg.cell[e];
-                P.act[dst] = sg.act[e];
-            });
+            for (int k = 0; k < 8; ++k) static_cast<T*>(C.pool_f[k])[q] = sg.f[k][e];
+            C.pool_cell[q] = sg.cell[e];
+            C.pool_act[q] = sg.act[e];
+        }
         // secondaries are part of the post-step population: deposit them too
         if (dep_val != 0.0) {
             for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
@@ -847,14 +863,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                     acc.add(x, y, z, P.f[3][j], P.f[4][j], P.f[5][j], P.f[6][j]);
                 }
             }
-            // secondaries in their appended (serial) order (sums independent of staging order)
+            // secondaries in their serial order, from the pool (sums independent of staging order)
             __syncthreads();
-            const long long d0 = n_entry + (long long)sh.excl;
+            const T* const* pf = reinterpret_cast<T* const*>(C.pool_f);
             for (uint32_t r = threadIdx.x; r < cnt; r += BLOCK) {
-                const long long d = d0 + r;
-                if (sh.ok && d < P.cap && P.act[d]) {
-                    mesh_abs(g, P.cell[d], (double)P.f[0][d], (double)P.f[1][d], (double)P.f[2][d], x, y, z);
-                    acc.add(x, y, z, P.f[3][d], P.f[4][d], P.f[5][d], P.f[6][d]);
+                const unsigned long long d = poff + r;
+                if (d < (unsigned long long)P.cap && C.pool_act[d]) {
+                    mesh_abs(g, C.pool_cell[d], (double)pf[0][d], (double)pf[1][d], (double)pf[2][d], x, y, z);
+                    acc.add(x, y, z, pf[3][d], pf[4][d], pf[5][d], pf[6][d]);
                 }
             }
             block_reduce_moments<BLOCK>(sh, acc.m, C.tile_partials + tile * kStepMoments);
@@ -862,6 +878,72 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
         __syncthreads();
     }
     grid_epilogue<BLOCK>(sh, C, ntiles, n_entry, P.n_out);
+}
+
+// ---------------------------------------------------------------------------------------
+// Append of the mesh step's secondaries.  k_step_mesh leaves each tile's secondaries as a run
+// in the pool (app_off[t], app_cnt[t] entries, serial order within the tile); the runs go
+// after the population in tile order, which is the serial reference order (ascending parent).
+// ---------------------------------------------------------------------------------------
+// One block: exclusive scan of the tiles' counts (each thread a contiguous range of tiles),
+// the population count after the step, and the pool's reset for the next launch.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_pool_scan(const long long* n_in, long long* n_out, long long cap, int tile_sz,
+                                                  const uint32_t* cnt, unsigned long long* excl,
+                                                  unsigned long long* pool_top, uint32_t* status) {
+    __shared__ unsigned long long wsum[NT / 32];
+    const long long n_entry = *n_in;
+    const long long ntiles = (n_entry + tile_sz - 1) / tile_sz;
+    const long long per = (ntiles + NT - 1) / NT;
+    const long long t0 = (long long)threadIdx.x * per;
+    const long long t1 = t0 + per < ntiles ? t0 + per : ntiles;
+    unsigned long long sum = 0;
+    for (long long t = t0; t < t1; ++t) sum += cnt[t];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long a = 0;
+        for (int w = 0; w < NT / 32; ++w) { const unsigned long long v = wsum[w]; wsum[w] = a; a += v; }
+        long long n = n_entry + (long long)a;
+        if (n > cap) { n = cap; atomicOr(status, ST_CAPACITY); }
+        *n_out = n;
+        *pool_top = 0;
+    }
+    __syncthreads();
+    unsigned long long run = wsum[wid] + incl - sum;
+    for (long long t = t0; t < t1; ++t) {
+        excl[t] = run;
+        run += cnt[t];
+    }
+}
+
+// Copy each tile's run from the pool to its place after the population (a block per tile).
+template <typename T>
+__global__ void __launch_bounds__(128) k_pool_copy(PopView<T> P, StepCtl C, int tile_sz, const unsigned long long* excl) {
+    const long long n_entry = *P.n_in;
+    const long long ntiles = (n_entry + tile_sz - 1) / tile_sz;
+    const T* const* pf = reinterpret_cast<T* const*>(C.pool_f);
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t c = C.app_cnt[t];
+        const unsigned long long src0 = C.app_off[t];
+        const long long dst0 = n_entry + (long long)excl[t];
+        for (uint32_t r = threadIdx.x; r < c; r += blockDim.x) {
+            const unsigned long long src = src0 + r;
+            const long long dst = dst0 + r;
+            if (dst >= P.cap || src >= (unsigned long long)P.cap) continue;   // flagged by the step / scan
+#pragma unroll
+            for (int q = 0; q < 8; ++q) P.f[q][dst] = pf[q][src];
+            P.cell[dst] = C.pool_cell[src];
+            P.act[dst] = C.pool_act[src];
+        }
+    }
 }
 
 }  // namespace mcs

@@ -4,6 +4,7 @@
 #include <type_traits>
 
 #include "host_util.h"
+#include "pop_ops.h"
 #include "step_kernel.cuh"
 
 namespace mcs {
@@ -81,7 +82,20 @@ int launch_step_mesh_impl(mcs_pop* p, const mcs_table* t, double dt, bool tracki
     YoshidaC Y{yh.c1, yh.c2, yh.c3, yh.c4, yh.d1, yh.d2, yh.d3, (-kElementaryCharge) / kElectronMass};
     StepCtl C = step_ctl(p, dt, TAG_ADVANCE, mom);
     if (int st = attach_stage<T, TILE>(p, grid, C)) return st;
-    kern<<<grid, BLOCK, 0, c->stream>>>(pop_view<T>(p), t->v, p->cells->v, tracking ? 1 : 0, C, Y, dep_val);
+    if (int st = reserve_mesh_pool(p)) return st;
+    for (int q = 0; q < 8; ++q) C.pool_f[q] = p->alt[q];
+    C.pool_cell = p->alt_cell;
+    C.pool_act = p->alt_act;
+    C.pool_top = reinterpret_cast<unsigned long long*>(p->counters + 16);
+    C.app_cnt = p->app_cnt;
+    C.app_off = p->app_off;
+    const PopView<T> P = pop_view<T>(p);
+    kern<<<grid, BLOCK, 0, c->stream>>>(P, t->v, p->cells->v, tracking ? 1 : 0, C, Y, dep_val);
+    MCS_CK_LAUNCH(c);
+    k_pool_scan<1024><<<1, 1024, 0, c->stream>>>(P.n_in, P.n_out, P.cap, TILE, p->app_cnt, p->app_excl, C.pool_top,
+                                                C.status);
+    MCS_CK_LAUNCH(c);
+    k_pool_copy<T><<<c->num_sms * 8, 128, 0, c->stream>>>(P, C, TILE, p->app_excl);
     MCS_CK_LAUNCH(c);
     return MCS_OK;
 }
