@@ -178,7 +178,69 @@ struct BShared {
     long long tile, first, ntl, n_entry;
     uint32_t count, excl, next;
     int k, ok, last;
+    // the CTA's previous tile, whose secondaries wait in ranked buffer pend_par for their
+    // place after the instance (pend < 0: none); par is the current tile's buffer
+    long long pend, pend_first, pend_n_entry, pend_base, pend_cap;
+    uint32_t pend_c;
+    int pend_k, pend_last, pend_par, par;
 };
+
+// Per-CTA slice of the step's staging memory: the staging buffer of stage() (cap entries,
+// unordered), then two ranked buffers (cap entries each: a tile's secondaries at their
+// serial rank within the tile).
+__host__ __device__ inline size_t bstage_bytes(uint32_t cap) { return ((size_t)cap * (8 * sizeof(float) + 9) + 255) & ~(size_t)255; }
+__host__ __device__ inline size_t brank_bytes(uint32_t cap) { return ((size_t)cap * (8 * sizeof(float) + 1) + 255) & ~(size_t)255; }
+
+struct RankBuf {
+    float* f[8];
+    uint8_t* act;
+    __device__ __forceinline__ void init(const BatchDev& B, int par) {
+        char* b = B.stage + (unsigned long long)blockIdx.x * B.stage_stride + bstage_bytes(B.stage_cap) +
+                  (size_t)par * brank_bytes(B.stage_cap);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] = reinterpret_cast<float*>(b + (size_t)q * B.stage_cap * sizeof(float));
+        act = reinterpret_cast<uint8_t*>(b + (size_t)8 * B.stage_cap * sizeof(float));
+    }
+};
+
+// Append the CTA's pending tile: wait (bounded) for the prefix of the instance's tiles
+// before it -- they published their counts when their particles were done, and have had a
+// whole tile of this CTA's time since -- and copy its ranked buffer to its place.
+template <int BLOCK>
+__device__ __forceinline__ void bappend_pending(const BatchDev& B, BShared<BLOCK>& sh, uint32_t epoch) {
+    if (sh.pend < 0) return;
+    if (threadIdx.x == 0) {
+        bool ok = true;
+        uint32_t excl = 0;
+        if (sh.pend != sh.pend_first)
+            excl = tile_lookback_wait(B.tstatus, (uint32_t)sh.pend_first, (uint32_t)sh.pend, epoch, sh.pend_c,
+                                      B.status, &ok);
+        sh.excl = excl;
+        sh.ok = ok;
+        if (sh.pend_last) {
+            long long nn = sh.pend_n_entry + (long long)excl + sh.pend_c;
+            if (nn > sh.pend_cap) { nn = sh.pend_cap; atomicOr(B.status, ST_CAPACITY); }
+            B.n1buf[sh.pend_k] = nn;
+        }
+    }
+    __syncthreads();
+    if (sh.ok) {
+        RankBuf rb;
+        rb.init(B, sh.pend_par);
+        const long long d0 = sh.pend_n_entry + (long long)sh.excl;
+        for (uint32_t r = threadIdx.x; r < sh.pend_c; r += BLOCK) {
+            const long long dl = d0 + r;
+            if (dl >= sh.pend_cap) { atomicOr(B.status, ST_CAPACITY); continue; }
+            const long long d = sh.pend_base + dl;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) B.f[q][d] = rb.f[q][r];
+            B.act[d] = rb.act[r];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sh.pend = -1;
+    __syncthreads();
+}
 
 // ---------------------------------------------------------------------------------------
 // Batched advance! (FP32, uniform field per instance, closed-form push between real
@@ -203,6 +265,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
     C.flags = B.flags;
     C.status = B.status;
     C.tag = TAG_ADVANCE;
+    if (threadIdx.x == 0) {
+        sh.pend = -1;
+        sh.par = 0;
+    }
     for (;;) {
         if (threadIdx.x == 0) {
             const long long g = atomicAdd(&B.counters[0], 1u);
@@ -343,7 +409,8 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
         }
         __syncthreads();
 
-        // ---- ordered append of this tile's secondaries within the instance ----
+        // ---- this tile's secondaries: serial ranks within the tile, the tile's count
+        // published at once (no wait), and the secondaries in the tile's ranked buffer ----
         uint32_t c = sh.count;
         if (c > sg.cap) c = sg.cap;
         {
@@ -364,14 +431,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
             if (threadIdx.x == 0) {
                 uint32_t acc = 0;
                 for (int q = 0; q < BLOCK / 32; ++q) { const uint32_t tq = sh.wtot[q]; sh.wtot[q] = acc; acc += tq; }
-                bool ok;
-                sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)g, epoch, c, B.status, &ok);
-                sh.ok = ok;
-                if (lt == sh.ntl - 1) {
-                    long long nn = n_entry + (long long)sh.excl + c;
-                    if (nn > I.cap) { nn = I.cap; atomicOr(B.status, ST_CAPACITY); }
-                    B.n1buf[k] = nn;
-                }
+                // the instance's first tile knows its prefix (0): inclusive; the others their
+                // aggregate, which the tiles after them sum in their look-back
+                st_release_u64(&B.tstatus[g], tile_word(epoch, g == sh.first ? 2 : 1, c));
             }
             __syncthreads();
             uint32_t run = sh.wtot[wid] + incl - sum;
@@ -379,16 +441,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
             for (int q = 0; q < PER; ++q) { cnt[threadIdx.x * PER + q] = run; run += v[q]; }
             __syncthreads();
         }
-        if (sh.ok) {
-            for (uint32_t e = threadIdx.x; e < c; e += BLOCK) {
-                const uint32_t key = sg.key[e];
-                const long long dl = n_entry + (long long)sh.excl + cnt[key >> 16] + (key & 0xffffu);
-                if (dl >= I.cap) { atomicOr(B.status, ST_CAPACITY); continue; }
-                const long long d = I.base + dl;
+        RankBuf rb;
+        rb.init(B, sh.par);
+        for (uint32_t e = threadIdx.x; e < c; e += BLOCK) {
+            const uint32_t key = sg.key[e];
+            const uint32_t r = cnt[key >> 16] + (key & 0xffffu);
+            if (r >= c) continue;   // only when staging overflowed (ST_OVERFLOW raised)
 #pragma unroll
-                for (int q = 0; q < 8; ++q) B.f[q][d] = sg.f[q][e];
-                B.act[d] = sg.act[e];
-            }
+            for (int q = 0; q < 8; ++q) rb.f[q][r] = sg.f[q][e];
+            rb.act[r] = sg.act[e];
         }
 
         // ---- tile moments (post-step actives incl. secondaries) ----
@@ -410,15 +471,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
                 if (il < n_entry && B.act[i])
                     add(B.f[0][i], B.f[1][i], B.f[2][i], B.f[3][i], B.f[4][i], B.f[5][i], B.f[6][i]);
             }
-            // secondaries in their appended (serial) order
+            // secondaries in their serial order, from the ranked buffer
             __syncthreads();
-            const long long d0 = n_entry + (long long)sh.excl;
-            for (uint32_t r = threadIdx.x; r < c; r += BLOCK) {
-                const long long dl = d0 + r;
-                const long long d = I.base + dl;
-                if (sh.ok && dl < I.cap && B.act[d])
-                    add(B.f[0][d], B.f[1][d], B.f[2][d], B.f[3][d], B.f[4][d], B.f[5][d], B.f[6][d]);
-            }
+            for (uint32_t r = threadIdx.x; r < c; r += BLOCK)
+                if (rb.act[r]) add(rb.f[0][r], rb.f[1][r], rb.f[2][r], rb.f[3][r], rb.f[4][r], rb.f[5][r], rb.f[6][r]);
             const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
             for (int q = 0; q < kBM; ++q) {
@@ -471,7 +527,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_bstep(BatchDev B) {
             }
         }
         __syncthreads();
+        // ---- the CTA's previous tile goes to its place; this one becomes pending ----
+        bappend_pending<BLOCK>(B, sh, epoch);
+        if (threadIdx.x == 0) {
+            sh.pend = g;
+            sh.pend_first = sh.first;
+            sh.pend_n_entry = n_entry;
+            sh.pend_base = I.base;
+            sh.pend_cap = I.cap;
+            sh.pend_c = c;
+            sh.pend_k = k;
+            sh.pend_last = lt == sh.ntl - 1;
+            sh.pend_par = sh.par;
+            sh.par ^= 1;
+        }
+        __syncthreads();
     }
+    bappend_pending<BLOCK>(B, sh, epoch);
     // re-arm the ticket for the next pass
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -949,7 +1021,7 @@ MCS_API int mcs_batch_create(mcs_ctx* c, int max_instances, int64_t total_capaci
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kVariants[v].fn, kVariants[v].block, 0);
         b->grid[v] = std::max(occ, 1) * c->num_sms;
         const uint32_t cap = 4 * kVariants[v].block * kVariants[v].ppt + 2048;
-        const size_t stride = (((size_t)cap * (8 * sizeof(float) + 9)) + 255) & ~(size_t)255;
+        const size_t stride = bstage_bytes(cap) + 2 * brank_bytes(cap);
         b->stage_stride[v] = stride;
         b->stage_cap[v] = cap;
         stage_bytes = std::max(stage_bytes, stride * (size_t)b->grid[v]);

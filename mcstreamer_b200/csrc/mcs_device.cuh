@@ -285,15 +285,12 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
 // Called by one thread.
 // `first` is the first tile of the segment being scanned (0 for a whole population; the
 // first tile of an instance in a batch, so instances are prefixed independently).
-__device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* status, uint32_t first, uint32_t tile,
+// The waiting half, for a tile (not the first) whose aggregate `count` is published already:
+// sums the tiles before it back to one with an inclusive prefix, then publishes its own.
+__device__ __forceinline__ uint32_t tile_lookback_wait(unsigned long long* status, uint32_t first, uint32_t tile,
                                                        uint32_t epoch, uint32_t count, uint32_t* st_word, bool* ok,
                                                        uint32_t max_spins = 1u << 24) {
     *ok = true;
-    if (tile == first) {
-        st_release_u64(&status[tile], tile_word(epoch, 2, count));
-        return 0;
-    }
-    st_release_u64(&status[tile], tile_word(epoch, 1, count));
     uint32_t excl = 0;
     int64_t p = (int64_t)tile - 1;
     uint32_t spins = 0;
@@ -317,6 +314,19 @@ __device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* statu
     }
     st_release_u64(&status[tile], tile_word(epoch, 2, excl + count));
     return excl;
+}
+
+// Publish the tile's count and return the sum of the counts of tiles first..tile-1.
+__device__ __forceinline__ uint32_t tile_lookback_from(unsigned long long* status, uint32_t first, uint32_t tile,
+                                                       uint32_t epoch, uint32_t count, uint32_t* st_word, bool* ok,
+                                                       uint32_t max_spins = 1u << 24) {
+    *ok = true;
+    if (tile == first) {
+        st_release_u64(&status[tile], tile_word(epoch, 2, count));
+        return 0;
+    }
+    st_release_u64(&status[tile], tile_word(epoch, 1, count));
+    return tile_lookback_wait(status, first, tile, epoch, count, st_word, ok, max_spins);
 }
 
 __device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, uint32_t tile, uint32_t epoch,

@@ -731,15 +731,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
             while (!have && !drained) {
                 const uint32_t q = atomicAdd(&sh.next, 1u);
                 if (q >= (uint32_t)TILE) { drained = true; break; }
-                if (q >= tile_n || !P.act[base + q]) { sh.cnt[q] = 0; continue; }
+                if (q >= tile_n) { sh.cnt[q] = 0; continue; }
+                // the slot's flag, cell and state in one round of loads, then the test
+                const long long i2 = base + q;
+                const uint8_t a = P.act[i2];
+                const uint32_t cell0 = P.cell[i2];
+                T f[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) f[k] = P.f[k][i2];
+                if (!a) { sh.cnt[q] = 0; continue; }
                 local = q;
-                i = base + q;
+                i = i2;
                 rng.init(C.seed, (uint32_t)i + C.slot_base, C.step, C.tag);
-                const uint32_t cell0 = P.cell[i];
-                ox = P.f[0][i]; oy = P.f[1][i]; oz = P.f[2][i];
-                vx = P.f[3][i]; vy = P.f[4][i]; vz = P.f[5][i];
-                w = P.f[6][i];
-                s = (double)P.f[7][i];
+                ox = f[0]; oy = f[1]; oz = f[2];
+                vx = f[3]; vy = f[4]; vz = f[5];
+                w = f[6];
+                s = (double)f[7];
                 in = cell0 != kOutsideCell;
                 if (in) {
                     uint32_t ux, uy, uz;
@@ -802,17 +809,21 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
                 uint32_t cl = kOutsideCell;
                 int dx = 0, dy = 0, dz = 0;
                 double fx = 0.0, fy = 0.0, fz = 0.0, ch = 0.0;
-                if (q < tile_n && P.act[j]) {
-                    cl = P.cell[j];
-                    if (cl != kOutsideCell) {
+                if (q < tile_n) {
+                    // all six loads at once (one L2 round trip), then the tests
+                    const uint8_t a = P.act[j];
+                    const uint32_t c0 = P.cell[j];
+                    const T x0 = P.f[0][j], y0 = P.f[1][j], z0 = P.f[2][j], w0 = P.f[6][j];
+                    if (a && c0 != kOutsideCell) {
                         valid = true;
+                        cl = c0;
                         uint32_t ux, uy, uz;
                         cell_split(g, cl, ux, uy, uz);
                         dx = (int)ux;
                         dy = (int)uy;
                         dz = (int)uz;
-                        fx = (double)P.f[0][j]; fy = (double)P.f[1][j]; fz = (double)P.f[2][j];
-                        ch = (double)P.f[6][j] * dep_val;
+                        fx = (double)x0; fy = (double)y0; fz = (double)z0;
+                        ch = (double)w0 * dep_val;
                     }
                 }
                 cic_fixed_warp(g.qpart, g.nx, g.ny, valid, cl, dx, dy, dz, fx, fy, fz, ch, C.status);
@@ -834,7 +845,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_step_mesh(PopView<T> P, TableVi
         const unsigned long long poff = sh.pool_off;
         for (uint32_t e = threadIdx.x; e < cnt; e += BLOCK) {
             const uint32_t key = sg.key[e];
-            const unsigned long long q = poff + sh.cnt[key >> 16] + (key & 0xffffu);
+            const uint32_t rank = sh.cnt[key >> 16] + (key & 0xffffu);
+            if (rank >= cnt) continue;   // only when staging overflowed (ST_OVERFLOW raised)
+            const unsigned long long q = poff + rank;
             if (q >= (unsigned long long)P.cap) { atomicOr(C.status, ST_CAPACITY); continue; }
 #pragma unroll
             for (int k = 0; k < 8; ++k) static_cast<T*>(C.pool_f[k])[q] = sg.f[k][e];
