@@ -65,74 +65,82 @@ __global__ void k_keys(PopView<T> P, GridView g, int mesh, uint32_t ncells, uint
 }
 
 // ---- radix pass: histogram ----
+// The (digit, tile) table is digit-major over the tiles the keys fill (ntiles of n keys),
+// so that its scan covers those tiles only.
 __global__ void __launch_bounds__(SB) k_hist(const uint32_t* __restrict__ key, const long long* n_ptr, int shift,
-                                             uint32_t* __restrict__ hist, long long ntiles_max) {
+                                             uint32_t* __restrict__ hist) {
     __shared__ uint32_t h[RADIX];
     const long long n = *n_ptr;
     const long long ntiles = (n + STILE - 1) / STILE;
-    for (long long tile = blockIdx.x; tile < ntiles_max; tile += gridDim.x) {
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         for (int d = threadIdx.x; d < RADIX; d += SB) h[d] = 0;
         __syncthreads();
-        if (tile < ntiles) {
-            const long long base = tile * STILE;
-            for (int it = 0; it < SI; ++it) {
-                const long long i = base + (long long)it * SB + threadIdx.x;
-                if (i < n) atomicAdd(&h[(key[i] >> shift) & 0xffu], 1u);
-            }
+        const long long base = tile * STILE;
+        for (int it = 0; it < SI; ++it) {
+            const long long i = base + (long long)it * SB + threadIdx.x;
+            if (i < n) atomicAdd(&h[(key[i] >> shift) & 0xffu], 1u);
         }
         __syncthreads();
-        for (int d = threadIdx.x; d < RADIX; d += SB) hist[(long long)d * ntiles_max + tile] = h[d];
+        for (int d = threadIdx.x; d < RADIX; d += SB) hist[(long long)d * ntiles + tile] = h[d];
         __syncthreads();
     }
 }
 
-// ---- radix pass: stable scatter.  Rounds of SB keys (thread t holds key r*SB + t), each
-// ranked by warp match-any and a per-digit prefix over the block's warps. ----
+// Entries of the (digit, tile) table of n keys.
+__global__ void k_hist_entries(const long long* n_ptr, long long* out) {
+    *out = (long long)RADIX * ((*n_ptr + STILE - 1) / STILE);
+}
+
+// ---- radix pass: stable scatter.  Each warp takes a contiguous 32*SI-key share of the
+// tile and counts its keys per digit (warp match-any, the digit group's first lane adds);
+// the warps' counts are prefixed per digit in warp order on top of the tile's offset; then
+// every key goes to that base plus the keys of its digit before it in its warp.  Three
+// barriers per tile. ----
 __global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                 uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                const long long* n_ptr, int shift, const uint32_t* __restrict__ offs,
-                                                long long ntiles_max) {
+                                                const long long* n_ptr, int shift, const uint32_t* __restrict__ offs) {
     constexpr int NW = SB / 32;
-    __shared__ uint32_t run[RADIX];          // keys of each digit placed by earlier rounds
-    __shared__ uint32_t wcnt[NW][RADIX];     // this round: per-warp digit counts -> exclusive prefix
-    __shared__ uint32_t base_off[RADIX];
+    __shared__ uint32_t wc[NW][RADIX];   // per-warp digit counts -> the warp's base per digit
     const long long n = *n_ptr;
     const long long ntiles = (n + STILE - 1) / STILE;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int d = threadIdx.x; d < RADIX; d += SB) {
-            run[d] = 0;
-            base_off[d] = offs[(long long)d * ntiles_max + tile];
+        for (int d = threadIdx.x; d < NW * RADIX; d += SB) (&wc[0][0])[d] = 0;
+        __syncthreads();
+        const long long base = tile * STILE + (long long)wid * (32 * SI);
+        uint32_t k[SI];
+#pragma unroll
+        for (int r = 0; r < SI; ++r) {
+            const long long i = base + (long long)r * 32 + lane;
+            k[r] = i < n ? kin[i] : 0u;
+            const uint32_t dg = i < n ? ((k[r] >> shift) & 0xffu) : 0x100u;
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            if (dg < RADIX && (peers & lt) == 0) wc[wid][dg] += __popc(peers);
+            __syncwarp();
         }
         __syncthreads();
-        const long long base = tile * STILE;
-        for (int r = 0; r < SI; ++r) {
-            for (int d = threadIdx.x; d < NW * RADIX; d += SB) (&wcnt[0][0])[d] = 0;
-            __syncthreads();
-            const long long i = base + (long long)r * SB + threadIdx.x;
-            const bool ok = i < n;
-            const uint32_t k = ok ? kin[i] : 0u;
-            const uint32_t v = ok ? vin[i] : 0u;
-            const uint32_t dg = ok ? ((k >> shift) & 0xffu) : 0x100u;
-            const unsigned peers = __match_any_sync(0xffffffffu, dg);
-            const uint32_t rank_w = __popc(peers & lt);
-            if (ok && rank_w == 0) wcnt[wid][dg] = __popc(peers);
-            __syncthreads();
-            // exclusive prefix over warps per digit, then fold into run[]
-            for (int d = threadIdx.x; d < RADIX; d += SB) {
-                uint32_t acc = run[d];
-                for (int w2 = 0; w2 < NW; ++w2) { const uint32_t c = wcnt[w2][d]; wcnt[w2][d] = acc; acc += c; }
-                run[d] = acc;
-            }
-            __syncthreads();
-            if (ok) {
-                const uint32_t pos = base_off[dg] + wcnt[wid][dg] + rank_w;
-                kout[pos] = k;
-                vout[pos] = v;
-            }
-            __syncthreads();
+        for (int d = threadIdx.x; d < RADIX; d += SB) {
+            uint32_t acc = offs[(long long)d * ntiles + tile];
+            for (int w2 = 0; w2 < NW; ++w2) { const uint32_t c = wc[w2][d]; wc[w2][d] = acc; acc += c; }
         }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < SI; ++r) {
+            const long long i = base + (long long)r * 32 + lane;
+            const uint32_t dg = i < n ? ((k[r] >> shift) & 0xffu) : 0x100u;
+            const unsigned peers = __match_any_sync(0xffffffffu, dg);
+            uint32_t pos = 0;
+            if (dg < RADIX) pos = wc[wid][dg] + __popc(peers & lt);
+            __syncwarp();
+            if (dg < RADIX) {
+                if ((peers & lt) == 0) wc[wid][dg] += __popc(peers);
+                kout[pos] = k[r];
+                vout[pos] = vin[i];
+            }
+            __syncwarp();
+        }
+        __syncthreads();
     }
 }
 
@@ -153,8 +161,6 @@ __global__ void k_gather(PopView<T> P, const uint32_t* __restrict__ perm, DstArr
         d.act[j] = P.act[s];
     }
 }
-
-__global__ void k_set_ll(long long* p, long long v) { *p = v; }
 
 uint32_t grid_cells(const mcs_grid* g) {
     if (g->v.type == GRID_CART3D) return (uint32_t)((long long)g->v.nx * g->v.ny * g->v.nz);
@@ -595,18 +601,18 @@ int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
     k_keys<T><<<gr, 256, 0, c->stream>>>(pop_view<T>(p), g->v, mesh, ncells, p->sort_key[0], p->sort_val[0]);
     MCS_CK_LAUNCH(c);
     long long* nhist = reinterpret_cast<long long*>(p->counters + 8);
-    k_set_ll<<<1, 1, 0, c->stream>>>(nhist, (long long)RADIX * ntiles_max);
+    k_hist_entries<<<1, 1, 0, c->stream>>>(n_dev, nhist);
     MCS_CK_LAUNCH(c);
     int cur = 0;
     long long gs = ntiles_max;
     if (gs > (long long)c->num_sms * 8) gs = (long long)c->num_sms * 8;
     for (int ps = 0; ps < passes; ++ps) {
         const int shift = 8 * ps;
-        k_hist<<<(int)gs, SB, 0, c->stream>>>(p->sort_key[cur], n_dev, shift, p->sort_hist, ntiles_max);
+        k_hist<<<(int)gs, SB, 0, c->stream>>>(p->sort_key[cur], n_dev, shift, p->sort_hist);
         MCS_CK_LAUNCH(c);
         if (int st = launch_scan(p, p->sort_hist, p->sort_hoff, nhist, nullptr)) return st;
         k_scatter<<<(int)gs, SB, 0, c->stream>>>(p->sort_key[cur], p->sort_val[cur], p->sort_key[cur ^ 1],
-                                                 p->sort_val[cur ^ 1], n_dev, shift, p->sort_hoff, ntiles_max);
+                                                 p->sort_val[cur ^ 1], n_dev, shift, p->sort_hoff);
         MCS_CK_LAUNCH(c);
         cur ^= 1;
     }
