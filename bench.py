@@ -58,6 +58,9 @@ def parse():
     ap.add_argument("--oracle-replicas", type=int, default=4, help="cfg0: oracle replicas")
     ap.add_argument("--cfg0-steps", type=int, default=2000, help="cfg0: steps per run")
     ap.add_argument("--plain-stride", type=int, default=4, help="cfg3: plain drop-in measured on every n-th instance")
+    ap.add_argument("--cfg3-profile", action="store_true",
+                    help="cfg3: only W + K batched steps of one kernel variant (a short run to profile)")
+    ap.add_argument("--variant", type=int, default=None, help="cfg3 --cfg3-profile: the k_bstep variant")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="cfg4: arrival window (s)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="cfg4: arrival rate (requests/s)")
@@ -330,7 +333,8 @@ def run_mine(args):
     hbm = float(pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"]))
     alg = alg_bytes_per_launch(n_active, sec_per_step, spec.nodes)
     achieved = alg / (kmean * 1e-3) / 1e9
-    tr = profile_record(f"traffic_k_step_mesh_{args.workload}")
+    rec_tag = "cfg1e" if args.pre_steps > 0 else "cfg1"   # the evolved cloud has its own capture
+    tr = profile_record(f"traffic_k_step_mesh_{rec_tag}")
     traffic = tr.get("bytes_per_launch") if tr and not tr.get("stale") else None
 
     e2e = None
@@ -363,12 +367,12 @@ def run_mine(args):
                          "frac": achieved / hbm, "traffic": traffic,
                          "kernel": mesh_kernel_name(ctx), "kernel_ms": kmean,
                          "alg_bytes_per_launch": alg, "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "issue": issue_roofline_from(profile_record(f"issue_k_step_mesh_{args.workload}"),
+                         "issue": issue_roofline_from(profile_record(f"issue_k_step_mesh_{rec_tag}"),
                                                       n_active, kmean, clocks)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * 3,   # k_step_mesh, k_pool_scan, k_pool_copy
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -756,8 +760,14 @@ def run_cfg2(args):
     alg = alg_bytes_per_launch(mean_in, max(0.0, mean_sec), spec.nodes)
     alg_particles = alg_bytes_per_launch(mean_in, max(0.0, mean_sec), 0)
     achieved = alg / (kmean * 1e-3) / 1e9
-    tr = profile_record("traffic_k_step_mesh_cfg2")
-    issue = profile_record("issue_k_step_mesh_cfg1")
+    # ncu records of the evolved cfg1 cloud (relaxed energies, like cfg2's timed steps): the
+    # full cfg2 workload is too large for a multi-pass capture, so its DRAM traffic is that
+    # capture's bytes per entering electron times cfg2's electrons
+    tr = profile_record("traffic_k_step_mesh_cfg1e")
+    issue = profile_record("issue_k_step_mesh_cfg1e")
+    traffic = None
+    if tr and not tr.get("stale") and tr.get("electrons"):
+        traffic = tr["bytes_per_launch"] / tr["electrons"] * mean_in
 
     e2e = host = None
     if args.e2e_steps > 0 and ws == 1:
@@ -807,8 +817,10 @@ def run_cfg2(args):
                                else "1 GPU",
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": tr.get("bytes_per_launch") if tr and not tr.get("stale") else None,
-                         "traffic_source": (tr.get("note") if tr else None),
+                         "traffic": traffic,
+                         "traffic_source": ("dram bytes per entering electron of one k_step_mesh launch on the "
+                                            "evolved cfg1 cloud (profiles/traffic_k_step_mesh_cfg1e.json) times "
+                                            "the mean entering electrons" if traffic is not None else None),
                          "kernel": mesh_kernel_name(ctx), "kernel_ms": kmean,
                          "alg_bytes_per_launch": alg, "alg_bytes_particles_only": alg_particles,
                          "frac_particles_only": alg_particles / (kmean * 1e-3) / 1e9 / hbm,
@@ -821,7 +833,10 @@ def run_cfg2(args):
             "e2e": e2e,
             "cfg1": cfg1,
             "clocks": clocks,
-            "gpu_launches": args.steps * 2 + sum(1 for k in timed if (k + 1) % CFG2_PERIOD == 0) * 21,
+            # per step: k_step_mesh, k_pool_scan, k_pool_copy, and repack!'s k_scan,
+            # k_repack_holes, k_repack_move; per resample!: 22 (keys, 4 radix passes of
+            # histogram + scan + scatter, gather, segments, counts, merges, writes)
+            "gpu_launches": args.steps * 6 + sum(1 for k in timed if (k + 1) % CFG2_PERIOD == 0) * 22,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -1117,8 +1132,23 @@ def run_batch(args):
                                  int(caps[k]), int(spec.n[k]), spec.mean_ev)
         return nbytes
 
-    # autotune on a batch a few steps into the run, then a fresh batch for the timed solve
     my_caps = int(caps[mine].sum())
+    if args.cfg3_profile:
+        b = SwarmBatch(ctx, len(mine), my_caps)
+        if args.variant is not None:
+            b.set_variant(args.variant)
+        fill(b)
+        b.step(spec.dt, args.warmup, graph=False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.step(spec.dt, args.steps, graph=False)
+        e1.record(stream)
+        b.sync()
+        print(json.dumps({"workload": "cfg3 profile run", "variant": args.variant, "warmup": args.warmup,
+                          "steps": args.steps, "ms_per_step": e0.elapsed_time(e1) / max(args.steps, 1)}), flush=True)
+        b.close()
+        return 0
+    # autotune on a batch a few steps into the run, then a fresh batch for the timed solve
     b = SwarmBatch(ctx, len(mine), my_caps)
     fill(b)
     b.step(spec.dt, args.warmup, graph=True)
@@ -1262,6 +1292,13 @@ def run_batch(args):
     cpu = None
     if not args.no_cpu:
         cpu = batch_cpu_sample(spec, args.cpu_seconds, os.cpu_count() or 1)
+    # DRAM bytes of one launch from the committed ncu record of the autotuner's usual variant
+    # (per entering electron, times this batch's), while the kernel's sources are unchanged
+    brec = profile_record("traffic_k_bstep_cfg3")
+    btraffic = btraffic_src = None
+    if brec and not brec.get("stale") and brec.get("electrons") and chosen == 19:
+        btraffic = brec["bytes_per_launch"] / brec["electrons"] * float(spec.n.sum())
+        btraffic_src = "profiles/traffic_k_bstep_cfg3.json (one launch of variant 19, ncu --set full)"
     line = {
         "metric": BATCH_METRIC, "value": value, "unit": BATCH_UNIT, "n_gpus": 1, "steps": spec.steps,
         "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -1299,7 +1336,8 @@ def run_batch(args):
             "parallelism": "1 GPU",
         },
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": f"k_bstep<{shape[0]},{shape[1]}>", "kernel_ms": kernel_ms,
+                     "traffic": btraffic, "traffic_source": btraffic_src,
+                     "kernel": f"k_bstep<{shape[0]},{shape[1]}>", "kernel_ms": kernel_ms,
                      "step_ms_no_graph": prof_step_ms, "alg_bytes_per_launch": alg,
                      "peak_source": f"{pk_kind} (MEASURED_PEAKS.json hbm_gbs)"},
         "cpu_baseline": cpu,

@@ -232,21 +232,44 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict_
     const long long n = *n_ptr;
     const long long ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // vector accesses when the arrays start on 16-byte boundaries (allocation bases do)
+    const bool vec = ((reinterpret_cast<uintptr_t>(out) | reinterpret_cast<uintptr_t>(in) |
+                       (reinterpret_cast<uintptr_t>(act) & 7u)) & 15u) == 0;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(&counters[0], 1u);
         __syncthreads();
         const long long tile = s_tile;
         if (tile >= ntiles) break;
         const long long base = tile * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+        const bool full = base + SCAN_ITEMS <= n;   // a thread's 8 items as two 16-byte (or one 8-byte) accesses
+        uint32_t c8[SCAN_ITEMS];
+        if (full && vec) {
+            if (in) {
+                const uint4 a = *reinterpret_cast<const uint4*>(in + base);
+                const uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
+                c8[0] = a.x; c8[1] = a.y; c8[2] = a.z; c8[3] = a.w;
+                c8[4] = b.x; c8[5] = b.y; c8[6] = b.z; c8[7] = b.w;
+            } else {
+                const uint2 a = *reinterpret_cast<const uint2*>(act + base);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    c8[q] = ((a.x >> (8 * q)) & 0xffu) != 0;
+                    c8[4 + q] = ((a.y >> (8 * q)) & 0xffu) != 0;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < SCAN_ITEMS; ++q) {
+                const long long i = base + q;
+                c8[q] = i < n ? (in ? in[i] : (uint32_t)(act[i] != 0)) : 0u;
+            }
+        }
         uint32_t v[SCAN_ITEMS];
         uint32_t tsum = 0;
 #pragma unroll
         for (int q = 0; q < SCAN_ITEMS; ++q) {
-            const long long i = base + q;
-            uint32_t c = 0;
-            if (i < n) c = in ? in[i] : (uint32_t)(act[i] != 0);
             v[q] = tsum;
-            tsum += c;
+            tsum += c8[q];
         }
         uint32_t incl = tsum;
 #pragma unroll
@@ -265,10 +288,15 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict_
         }
         __syncthreads();
         const uint32_t off = s_excl + s_warp[wid] + incl - tsum;
+        if (full && vec) {
+            *reinterpret_cast<uint4*>(out + base) = make_uint4(off + v[0], off + v[1], off + v[2], off + v[3]);
+            *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(off + v[4], off + v[5], off + v[6], off + v[7]);
+        } else {
 #pragma unroll
-        for (int q = 0; q < SCAN_ITEMS; ++q) {
-            const long long i = base + q;
-            if (i < n) out[i] = off + v[q];
+            for (int q = 0; q < SCAN_ITEMS; ++q) {
+                const long long i = base + q;
+                if (i < n) out[i] = off + v[q];
+            }
         }
         __syncthreads();
     }

@@ -93,14 +93,17 @@ __global__ void k_hist_entries(const long long* n_ptr, long long* out) {
 
 // ---- radix pass: stable scatter.  Each warp takes a contiguous 32*SI-key share of the
 // tile and counts its keys per digit (warp match-any, the digit group's first lane adds);
-// the warps' counts are prefixed per digit in warp order on top of the tile's offset; then
-// every key goes to that base plus the keys of its digit before it in its warp.  Three
-// barriers per tile. ----
+// a block prefix of those counts gives every key its place in the tile sorted by digit
+// (stable), where it is put in shared memory; the tile then goes out in that order, so that
+// consecutive threads write consecutive slots of each digit's run.  Four barriers per tile.
 __global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                 uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                 const long long* n_ptr, int shift, const uint32_t* __restrict__ offs) {
     constexpr int NW = SB / 32;
-    __shared__ uint32_t wc[NW][RADIX];   // per-warp digit counts -> the warp's base per digit
+    __shared__ uint32_t wc[NW][RADIX];   // per-warp digit counts -> the warp's first tile-local slot per digit
+    __shared__ uint32_t loc[RADIX];      // first tile-local slot of each digit
+    __shared__ uint32_t gofs[RADIX];     // the digit's first slot of this tile in the output
+    __shared__ uint32_t skey[STILE], sval[STILE];
     const long long n = *n_ptr;
     const long long ntiles = (n + STILE - 1) / STILE;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -120,25 +123,56 @@ __global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin
             __syncwarp();
         }
         __syncthreads();
+        // per digit: the warps' counts prefixed in warp order; the digit's tile total
         for (int d = threadIdx.x; d < RADIX; d += SB) {
-            uint32_t acc = offs[(long long)d * ntiles + tile];
+            uint32_t acc = 0;
             for (int w2 = 0; w2 < NW; ++w2) { const uint32_t c = wc[w2][d]; wc[w2][d] = acc; acc += c; }
+            loc[d] = acc;   // the total for now
+            gofs[d] = offs[(long long)d * ntiles + tile];
         }
         __syncthreads();
+        if (threadIdx.x < 32) {   // exclusive prefix of the 256 digit totals by one warp
+            uint32_t t[RADIX / 32], sum = 0;
+#pragma unroll
+            for (int q = 0; q < RADIX / 32; ++q) { t[q] = loc[lane * (RADIX / 32) + q]; sum += t[q]; }
+            uint32_t incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            uint32_t run = incl - sum;
+#pragma unroll
+            for (int q = 0; q < RADIX / 32; ++q) { loc[lane * (RADIX / 32) + q] = run; run += t[q]; }
+        }
+        __syncthreads();
+        uint32_t cnt_tile = 0;   // keys of the tile (all threads)
+        {
+            const long long rest = n - tile * STILE;
+            cnt_tile = rest < STILE ? (uint32_t)rest : (uint32_t)STILE;
+        }
 #pragma unroll
         for (int r = 0; r < SI; ++r) {
             const long long i = base + (long long)r * 32 + lane;
             const uint32_t dg = i < n ? ((k[r] >> shift) & 0xffu) : 0x100u;
             const unsigned peers = __match_any_sync(0xffffffffu, dg);
             uint32_t pos = 0;
-            if (dg < RADIX) pos = wc[wid][dg] + __popc(peers & lt);
+            if (dg < RADIX) pos = loc[dg] + wc[wid][dg] + __popc(peers & lt);
             __syncwarp();
             if (dg < RADIX) {
                 if ((peers & lt) == 0) wc[wid][dg] += __popc(peers);
-                kout[pos] = k[r];
-                vout[pos] = vin[i];
+                skey[pos] = k[r];
+                sval[pos] = vin[i];
             }
             __syncwarp();
+        }
+        __syncthreads();
+        for (uint32_t j = threadIdx.x; j < cnt_tile; j += SB) {
+            const uint32_t kk = skey[j];
+            const uint32_t dg = (kk >> shift) & 0xffu;
+            const uint32_t pos = gofs[dg] + (j - loc[dg]);
+            kout[pos] = kk;
+            vout[pos] = sval[j];
         }
         __syncthreads();
     }
