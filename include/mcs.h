@@ -110,10 +110,11 @@ MCS_API const char* mcs_last_error(const mcs_ctx* ctx);
 MCS_API int mcs_ctx_set_stream(mcs_ctx* ctx, void* stream);
 MCS_API void* mcs_ctx_stream(mcs_ctx* ctx);
 MCS_API int mcs_ctx_set_flags(mcs_ctx* ctx, uint32_t flags);
-/* Failure-detection self-test (no counterpart in the reference): launches one bounded wait
- * (the ordered-append look-back) on a predecessor that never publishes, with at most
- * max_spins checks (1 .. 2^20).  Returns MCS_ERR_TIMEOUT when the wait gave up, raised the
- * status and returned, as every wait in the library does; the context stays usable. */
+/* Failure-detection self-test (no counterpart in the reference): launches the bounded waits
+ * of the ordered-append look-back, in its one-thread and whole-warp forms, on predecessors
+ * that never publish, with at most max_spins checks each (1 .. 2^20).  Returns
+ * MCS_ERR_TIMEOUT when both waits gave up, raised the status and returned, as every wait in
+ * the library does; the context stays usable. */
 MCS_API int mcs_diag_wait_timeout(mcs_ctx* ctx, uint32_t max_spins);
 /* Tuning options of a context (no counterpart in the reference, which has no kernels).
  * MCS_OPT_MESH_SHAPE selects the kernel shape of the FP32 mesh step (0 .. MCS_MESH_SHAPES-1,

@@ -209,14 +209,19 @@ struct RankBuf {
 template <int BLOCK>
 __device__ __forceinline__ void bappend_pending(const BatchDev& B, BShared<BLOCK>& sh, uint32_t epoch) {
     if (sh.pend < 0) return;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {   // warp 0 looks back
         bool ok = true;
         uint32_t excl = 0;
         if (sh.pend != sh.pend_first)
-            excl = tile_lookback_wait(B.tstatus, (uint32_t)sh.pend_first, (uint32_t)sh.pend, epoch, sh.pend_c,
-                                      B.status, &ok);
-        sh.excl = excl;
-        sh.ok = ok;
+            excl = tile_lookback_wait_warp(B.tstatus, (uint32_t)sh.pend_first, (uint32_t)sh.pend, epoch, sh.pend_c,
+                                           B.status, &ok);
+        if (threadIdx.x == 0) {
+            sh.excl = excl;
+            sh.ok = ok;
+        }
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t excl = sh.excl;
         if (sh.pend_last) {
             long long nn = sh.pend_n_entry + (long long)excl + sh.pend_c;
             if (nn > sh.pend_cap) { nn = sh.pend_cap; atomicOr(B.status, ST_CAPACITY); }

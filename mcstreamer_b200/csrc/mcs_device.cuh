@@ -334,4 +334,61 @@ __device__ __forceinline__ uint32_t tile_lookback(unsigned long long* status, ui
     return tile_lookback_from(status, 0u, tile, epoch, count, st_word, ok);
 }
 
+// The waiting half by a whole warp (all 32 lanes call it; every lane gets the prefix): each
+// round reads the status words of the 32 tiles before the window at once, and the window
+// ends at the nearest one with an inclusive prefix once every tile up to it has published.
+// Tiles before `first` count as an inclusive prefix of 0.  Bounded like the one-thread form.
+__device__ __forceinline__ uint32_t tile_lookback_wait_warp(unsigned long long* status, uint32_t first, uint32_t tile,
+                                                            uint32_t epoch, uint32_t count, uint32_t* st_word,
+                                                            bool* ok, uint32_t max_spins = 1u << 24) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t ep = epoch & 0x3fffffffu;
+    uint32_t excl = 0, spins = 0;
+    bool good = true;
+    int64_t p = (int64_t)tile - 1;
+    while (p >= (int64_t)first) {
+        const int64_t q = p - lane;
+        const bool in = q >= (int64_t)first;
+        const unsigned long long s = in ? ld_acquire_u64(&status[q]) : 0ull;
+        const uint32_t e = (uint32_t)(s >> 34), f = (uint32_t)(s >> 32) & 3u;
+        const unsigned incm = __ballot_sync(FULL, !in || (e == ep && f == 2));
+        const unsigned readym = __ballot_sync(FULL, !in || (e == ep && f != 0));
+        const unsigned need = incm ? (FULL >> (31 - (__ffs(incm) - 1))) : FULL;   // lanes up to the inclusive one
+        if ((readym & need) != need) {
+            if (++spins > max_spins) {  // about a second with the backoff below
+                if (lane == 0) atomicOr(st_word, ST_TIMEOUT);
+                good = false;
+                break;
+            }
+            if (spins > 64) __nanosleep(64);
+            continue;
+        }
+        uint32_t v = (in && ((need >> lane) & 1u)) ? (uint32_t)s : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+        excl += v;
+        if (incm) break;
+        p -= 32;
+    }
+    *ok = good;
+    if (lane == 0) st_release_u64(&status[tile], tile_word(epoch, 2, excl + count));
+    return excl;
+}
+
+// Publish the tile's count and return the prefix of tiles first..tile-1, by a whole warp.
+__device__ __forceinline__ uint32_t tile_lookback_from_warp(unsigned long long* status, uint32_t first, uint32_t tile,
+                                                            uint32_t epoch, uint32_t count, uint32_t* st_word,
+                                                            bool* ok) {
+    const int lane = threadIdx.x & 31;
+    if (tile == first) {
+        if (lane == 0) st_release_u64(&status[tile], tile_word(epoch, 2, count));
+        *ok = true;
+        return 0;
+    }
+    if (lane == 0) st_release_u64(&status[tile], tile_word(epoch, 1, count));
+    __syncwarp();
+    return tile_lookback_wait_warp(status, first, tile, epoch, count, st_word, ok);
+}
+
 }  // namespace mcs

@@ -279,12 +279,22 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict_
         }
         if (lane == 31) s_warp[wid] = incl;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for (int q = 0; q < SCAN_BLOCK / 32; ++q) { const uint32_t t = s_warp[q]; s_warp[q] = acc; acc += t; }
+        if (wid == 0) {   // the tile's total, its warps' offsets, and the look-back by warp 0
+            uint32_t t[SCAN_BLOCK / 32], acc = 0;
+#pragma unroll
+            for (int q = 0; q < SCAN_BLOCK / 32; ++q) t[q] = s_warp[q];
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < SCAN_BLOCK / 32; ++q) {
+                if (lane == 0) s_warp[q] = acc;
+                acc += t[q];
+            }
             bool ok;
-            s_excl = tile_lookback(tile_status, (uint32_t)tile, epoch, acc, status, &ok);
-            if (tile == ntiles - 1 && total) *total = (long long)s_excl + acc;
+            const uint32_t ex = tile_lookback_from_warp(tile_status, 0u, (uint32_t)tile, epoch, acc, status, &ok);
+            if (lane == 0) {
+                s_excl = ex;
+                if (tile == ntiles - 1 && total) *total = (long long)ex + acc;
+            }
         }
         __syncthreads();
         const uint32_t off = s_excl + s_warp[wid] + incl - tsum;
