@@ -715,17 +715,21 @@ __global__ void __launch_bounds__(kRBlock) k_bresample(BatchDev B) {
         if (sh.mode == MODE_CLONE) {
             uint32_t ctile;
             const uint32_t off = rblock_scan(sh, csum, &ctile);
-            if (threadIdx.x == 0) {
+            if (threadIdx.x < 32) {   // warp 0 looks back
                 bool ok;
-                sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, ctile, B.status, &ok);
-                sh.ok = ok;
-                if (lt == sh.ntl - 1) {
-                    long long m = n + (long long)sh.excl + ctile;
-                    if (m > sh.cap) { m = sh.cap; atomicOr(B.status, ST_CAPACITY); }
-                    B.tot[sh.k] = m - n;
-                    B.n0buf[sh.k] = m;
-                    if (m > n) atomicAdd(reinterpret_cast<unsigned long long*>(&B.actives[sh.k]),
-                                         (unsigned long long)(m - n));
+                const uint32_t ex =
+                    tile_lookback_from_warp(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, ctile, B.status, &ok);
+                if (threadIdx.x == 0) {
+                    sh.excl = ex;
+                    sh.ok = ok;
+                    if (lt == sh.ntl - 1) {
+                        long long m = n + (long long)ex + ctile;
+                        if (m > sh.cap) { m = sh.cap; atomicOr(B.status, ST_CAPACITY); }
+                        B.tot[sh.k] = m - n;
+                        B.n0buf[sh.k] = m;
+                        if (m > n) atomicAdd(reinterpret_cast<unsigned long long*>(&B.actives[sh.k]),
+                                             (unsigned long long)(m - n));
+                    }
                 }
             }
             __syncthreads();
@@ -763,10 +767,14 @@ __global__ void __launch_bounds__(kRBlock) k_brepack_holes(BatchDev B) {
         for (int q = 0; q < kRItems; ++q) h += (l0 + q < A && !a[q]) ? 1u : 0u;
         uint32_t htile;
         const uint32_t off = rblock_scan(sh, h, &htile);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {   // warp 0 looks back
             bool ok;
-            sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, htile, B.status, &ok);
-            sh.ok = ok;
+            const uint32_t ex =
+                tile_lookback_from_warp(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, htile, B.status, &ok);
+            if (threadIdx.x == 0) {
+                sh.excl = ex;
+                sh.ok = ok;
+            }
         }
         __syncthreads();
         if (sh.ok && h) {
@@ -803,10 +811,14 @@ __global__ void __launch_bounds__(kRBlock) k_brepack_move(BatchDev B) {
         }
         uint32_t mtile;
         const uint32_t off = rblock_scan(sh, m, &mtile);
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < 32) {   // warp 0 looks back
             bool ok;
-            sh.excl = tile_lookback_from(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, mtile, B.status, &ok);
-            sh.ok = ok;
+            const uint32_t ex =
+                tile_lookback_from_warp(B.tstatus, (uint32_t)sh.first, (uint32_t)sh.g, epoch, mtile, B.status, &ok);
+            if (threadIdx.x == 0) {
+                sh.excl = ex;
+                sh.ok = ok;
+            }
         }
         __syncthreads();
         if (sh.ok && m) {

@@ -125,14 +125,17 @@ __device__ __forceinline__ uint32_t tile_append(SH& sh, const Stage<T>& sg, cons
     uint32_t cnt = sh.count;
     if (cnt > sg.cap) cnt = sg.cap;
     block_scan_counts<BLOCK, TILE>(sh);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {   // warp 0 looks back
         bool ok;
-        sh.excl = tile_lookback(C.tile_status, (uint32_t)tile, C.epoch, cnt, C.status, &ok);
-        sh.ok = ok;
-        if (tile == ntiles - 1) {
-            long long n = n_entry + (long long)sh.excl + cnt;
-            if (n > cap) { n = cap; atomicOr(C.status, ST_CAPACITY); }
-            *n_out = n;
+        const uint32_t ex = tile_lookback_from_warp(C.tile_status, 0u, (uint32_t)tile, C.epoch, cnt, C.status, &ok);
+        if (threadIdx.x == 0) {
+            sh.excl = ex;
+            sh.ok = ok;
+            if (tile == ntiles - 1) {
+                long long n = n_entry + (long long)ex + cnt;
+                if (n > cap) { n = cap; atomicOr(C.status, ST_CAPACITY); }
+                *n_out = n;
+            }
         }
     }
     __syncthreads();
