@@ -208,7 +208,12 @@ struct RankBuf {
 // whole tile of this CTA's time since -- and copy its ranked buffer to its place.
 template <int BLOCK>
 __device__ __forceinline__ void bappend_pending(const BatchDev& B, BShared<BLOCK>& sh, uint32_t epoch) {
-    if (sh.pend < 0) return;
+    // every thread reads the pending tile before any goes on: with no pending tile the
+    // caller's thread 0 next makes this tile the pending one, and a thread that read
+    // sh.pend after that write would enter the append alone, out of step with the barriers
+    const bool none = sh.pend < 0;
+    __syncthreads();
+    if (none) return;
     if (threadIdx.x < 32) {   // warp 0 looks back
         bool ok = true;
         uint32_t excl = 0;

@@ -198,3 +198,21 @@ def test_device_maxwellian_matches_restatement(ctx, tables, precision, rtol):
     np.testing.assert_allclose(got.v, v, rtol=rtol, atol=rtol * sigma)
     np.testing.assert_allclose(got.s, -np.log(u[:, 4]), rtol=rtol, atol=0)
     assert (got.x == 0).all() and (got.w == 1).all() and (got.active == 1).all()
+
+
+@pytest.mark.gpu
+def test_many_tile_instances_equal_alone(ctx, tables):
+    """Instances of hundreds of tiles each, ionizing: every tile's secondaries wait for the
+    prefix of the instance's tiles before them (appended after the CTA's next tile), so the
+    appends of one instance are spread over many CTAs at once.  Each instance still equals
+    its run alone, slot for slot."""
+    nt = 12
+    cases = [(1, 600.0, 11, 600000, 1400000), (0, 300.0, 12, 420000, 900000), (2, 1000.0, 13, 250000, 600000)]
+    with SwarmBatch(ctx, 4, 3000000) as b:
+        slots = [_add(b, tables[v], en, seed, n0, cap) for v, en, seed, n0, cap in cases]
+        b.step(DT, nt, graph=True)
+        for (v, en, seed, n0, cap), k in zip(cases, slots):
+            alone, mom = _alone(ctx, tables[v], en, seed, n0, cap, nt)
+            _same(b.download(k), alone)
+            log = b.read_log(k, nt)
+            np.testing.assert_array_equal(log[:, L.S_COUNT], mom[:, L.S_COUNT])

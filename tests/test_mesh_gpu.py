@@ -191,3 +191,80 @@ def test_every_mesh_kernel_shape_gives_the_same_step(ctx):
     finally:
         ctx.check(ctx.lib.mcs_ctx_set_option(ctx.h, L.OPT_MESH_SHAPE, 0))
     _close(snap, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_fp64_three_steps_ragged_tiles_with_attachment(ctx):
+    """Three fused steps (push, collide, track, deposit) of a population that spans several
+    tiles with a ragged last one, with frequent attachment (removed electrons keep
+    sub-stepping, mixed_population.jl:32) and ionization: particles and secondaries slot for
+    slot, charges node for node, against the oracle after every step."""
+    from tests.helpers import attaching_table
+    n = 3 * 2048 + 777
+    t = attaching_table(uniform_sharing=True)
+    tab = jumc.CollisionTable(t, ctx)
+    grid = streamer.Grid3D(NX, NY, NZ, H, precision="fp64", ctx=ctx)
+    e = _field_nodes(grid)
+    grid.set_efield(e)
+    p0 = broad(n, 5, emax_ev=60.0, x0=CENTRE, spread=14e-6)
+    p0.w[:] = 1e3
+    pop = jumc.Population(8 * n, p0, tab, precision="fp64", seed=5, mesh=grid)
+    otab = po.OracleTable.from_lxcat(t)
+    ofield = po.field_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0), e.reshape(-1))
+    opop = oracle_pop(pop.download(), 8 * n, 5)
+    trk = po.tracker_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0))
+    fld = streamer.FieldInterp(grid)
+    grid.zero(L.Q_FIXED)
+    dt = 2e-13
+    removed = 0
+    for _ in range(3):
+        grid.zero(L.Q_PART)
+        streamer.advance_deposit(pop, fld, dt, streamer.CollisionTracker(grid), grid, -1.0)
+        assert po.advance(opop, otab, ofield, dt, tracker=trk) == 0
+        g, o = pop.download(), oracle_arrays(opop)
+        assert g.n == o.n
+        bad = particle_mismatch(g, o, 1e-12, xatol=1e-30, vatol=1e-30)
+        assert bad.sum() == 0, f"{bad.sum()} slots differ"
+        removed = int((g.active[:n] == 0).sum())
+        qf = grid.read_fixed(L.Q_FIXED)
+        assert qf.sum() == trk._q.sum() and np.abs(qf - trk._q).max() <= 8
+        dep = po.tracker_cart3d(NX, NY, NZ, H, (0.0, 0.0, 0.0))
+        po.deposit(opop, dep, -1.0)
+        qp = grid.read_fixed(L.Q_PART)
+        assert qp.sum() == dep._q.sum() and np.abs(qp - dep._q).max() <= 8
+    assert g.n > n and removed > 0          # both ionization and attachment happened
+    _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_step_of_an_empty_population(ctx):
+    """No particles: the step (and its append) leaves the population empty and deposits
+    nothing."""
+    t, tab, grid, p0, pop0, otab, ofield = _setup(ctx, 64, "fp32")
+    pop0.close()
+    pop = jumc.Population(1024, jumc.ParticleArrays.empty(0), tab, precision="fp32", seed=1, mesh=grid)
+    fld = streamer.FieldInterp(grid)
+    grid.zero(L.Q_FIXED)
+    grid.zero(L.Q_PART)
+    for _ in range(2):
+        streamer.advance_deposit(pop, fld, 2e-13, streamer.CollisionTracker(grid), grid, -1.0)
+    ctx.sync()
+    assert pop.nparticles() == 0
+    assert not grid.read_fixed(L.Q_PART).any() and not grid.read_fixed(L.Q_FIXED).any()
+    _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_mesh_step_beyond_capacity_is_reported(ctx):
+    """Secondaries beyond the population's capacity: MCS_ERR_CAPACITY (population.jl:90's
+    error), and the population stops at its capacity."""
+    n = 20000
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32", emax_ev=200.0, capf=1)
+    fld = streamer.FieldInterp(grid)
+    with pytest.raises(L.MCSError) as err:
+        for _ in range(4):
+            streamer.advance_deposit(pop, fld, 2e-13, streamer.CollisionTracker(grid), grid, -1.0)
+        ctx.sync()
+    assert err.value.code == L.ERR_CAPACITY
+    assert pop.nparticles() == n
+    _close(fld, pop, grid, tab)
