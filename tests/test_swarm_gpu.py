@@ -74,8 +74,8 @@ def test_constant_collision_frequency_drift(ctx, precision):
 
 @pytest.mark.gpu
 def test_fp32_swarm_coefficients_within_3_sigma_of_fp64(ctx):
-    """North-star check: the FP32 form reproduces the FP64 swarm coefficients within 3 sigma
-    of the replica standard error (Swarm.stats, Swarm.jl:253-269)."""
+    """The FP32 form reproduces the FP64 swarm coefficients within 3 sigma of the replica
+    standard error (Swarm.stats, Swarm.jl:253-269)."""
     t = lxcat.synthetic_table(0)
     tab = jumc.CollisionTable(t, ctx)
     R, n0, nt, dt = 6, 32768, 600, 1e-13
