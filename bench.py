@@ -555,7 +555,8 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     for a Julia Population): the population entering the first timed step is downloaded into
     pinned host arrays in the Julia layout (65 B per electron), and mcs_advance_deposit_host
     steps it in place -- uploads, fused steps and downloads pipelined over chunks -- after
-    which the deposit grid is read back to pinned host memory, every step.  No resample! is
+    which the deposit grid is brought to pinned host memory (the slab of z-planes that holds
+    charge; the rest of the host array is kept zero), every step.  No resample! is
     called (the library has no host-resident resample; it is one step in ten of the device
     run)."""
     import ctypes as C
@@ -576,6 +577,9 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     ctx.check(lib.mcs_pop_download(pop.h, L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), cap, C.byref(nn)))
     work = jumc.Population(int(1.5 * ((cap + chunks - 1) // chunks)) + 4096, None, pop.collisions, precision="fp32",
                            seed=spec.seed, mesh=grid)
+    hq[:] = 0
+    plane = (spec.nx + 1) * (spec.ny + 1)
+    filled = (0, 0)
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ms = active = 0.0
     h2d = d2h = 0
@@ -588,7 +592,8 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
         ctx.check(lib.mcs_advance_deposit_host(work.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0,
                                                L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), C.byref(nn),
                                                cap, chunks))
-        ctx.check(lib.mcs_grid_read_fixed(grid.h_, L.Q_PART, L.i64ptr(hq)))
+        # the whole deposit grid on the host, moving the z-slab that holds charge
+        filled = grid.read_fixed_planes(L.Q_PART, hq, filled)
         t1.record(stream)
         torch.cuda.synchronize()
         if k == 0:
@@ -596,7 +601,7 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
         ms += t0.elapsed_time(t1)
         active += act_in
         h2d += n_in * 65
-        d2h += nn.value * 65 + spec.nodes * 8
+        d2h += nn.value * 65 + (filled[1] - filled[0]) * plane * 8 + 16
     work.close()
     steps = args.e2e_steps
     m = nn.value
@@ -604,9 +609,11 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     return host, {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // steps,
             "d2h_bytes_per_step": d2h // steps, "steps": steps, "electrons_at_start": n,
             "path": f"mcs_advance_deposit_host on pinned host arrays in the Julia layout ({chunks} chunks: uploads, "
-                    "fused steps and downloads pipelined on three streams) + mcs_grid_read_fixed of the 2.15 GB "
-                    "deposit grid, every step; the population entering the first timed step, evolving; CUDA "
-                    "events around each step; no resample! (no host-resident entry point)"}
+                    "fused steps and downloads pipelined on three streams) + the 2.15 GB deposit grid into a "
+                    "pinned host array, every step, moving the z-planes that hold charge (mcs_grid_fixed_plane_range "
+                    "+ mcs_grid_read_fixed_range; the host array equals the full grid); the population entering the "
+                    "first timed step, evolving; CUDA events around each step; no resample! (no host-resident entry "
+                    "point)", "deposit_planes": [int(filled[0]), int(filled[1])]}
 
 
 def cfg1_kernel_record(ctx, table, stream, torch, L, steps: int = 20, warmup: int = 5) -> dict:

@@ -206,6 +206,10 @@ MCS_API int mcs_grid_read_efield(mcs_grid* g, double* e);
  * array (int64 at 2^-32 e): a window of a large mesh without copying all of it. */
 MCS_API int mcs_grid_read_efield_range(mcs_grid* g, int64_t node0, int64_t count, double* e);
 MCS_API int mcs_grid_read_fixed_range(mcs_grid* g, int which, int64_t node0, int64_t count, int64_t* out);
+/* The z-planes [z0, z1) of a cart3d grid's charge array that hold a nonzero value (z0 = z1
+ * = 0 when all are zero); with mcs_grid_read_fixed_range a caller that keeps the charge on
+ * the host moves only that slab (no counterpart in the reference). */
+MCS_API int mcs_grid_fixed_plane_range(mcs_grid* g, int which, int64_t* z0, int64_t* z1);
 MCS_API int mcs_grid_set_efield_gaussian(mcs_grid* g, double cx, double cy, double cz, double sigma,
                                          double rho_peak, double ebx, double eby, double ebz);
 MCS_API int mcs_pop_copy(mcs_pop* dst, const mcs_pop* src);

@@ -65,6 +65,7 @@ SIGNATURES = {
     "mcs_grid_read_density": (i32, [vp, i32, pd]),
     "mcs_grid_read_efield_range": (i32, [vp, i64, i64, pd]),
     "mcs_grid_read_fixed_range": (i32, [vp, i32, i64, i64, pi64]),
+    "mcs_grid_fixed_plane_range": (i32, [vp, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "mcs_grid_charge_ptr": (i32, [vp, i32, ph, pi64]),
     "mcs_field_uniform": (i32, [vp, f64, f64, f64, ph]),
     "mcs_field_from_grid": (i32, [vp, ph]),

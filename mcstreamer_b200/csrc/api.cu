@@ -72,6 +72,33 @@ int sync_status(mcs_ctx* c) {
 
 namespace {
 
+// First and last node of a charge array holding a nonzero value (range[0] = min, range[1] =
+// max; untouched when every node is zero): one min and one max per CTA go to global atomics.
+__global__ void __launch_bounds__(256) k_nonzero_range(const long long* __restrict__ q, long long n,
+                                                       unsigned long long* range) {
+    __shared__ unsigned long long s_lo, s_hi;
+    if (threadIdx.x == 0) { s_lo = ~0ull; s_hi = 0; }
+    __syncthreads();
+    unsigned long long lo = ~0ull, hi = 0;
+    bool any = false;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        if (q[i] != 0) {
+            if (!any) lo = (unsigned long long)i;
+            hi = (unsigned long long)i;
+            any = true;
+        }
+    if (any) {
+        atomicMin(&s_lo, lo);
+        atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_lo != ~0ull) {
+        atomicMin(&range[0], s_lo);
+        atomicMax(&range[1], s_hi);
+    }
+}
+
 int ensure_staging(mcs_pop* p, size_t bytes) {
     if (p->staging_bytes >= bytes) return MCS_OK;
     if (p->staging) cudaFree(p->staging);
@@ -335,6 +362,7 @@ MCS_API int mcs_grid_destroy(mcs_grid* g) {
     cudaFree(g->d_qfd);
     cudaFree(g->d_init_ws);
     cudaFree(g->d_q[0]); cudaFree(g->d_q[1]);
+    cudaFree(g->d_range);
     delete g;
     return MCS_OK;
 }
@@ -439,6 +467,32 @@ MCS_API int mcs_grid_read_fixed_range(mcs_grid* g, int which, int64_t node0, int
     MCS_CK(c, cudaStreamSynchronize(c->stream));
     MCS_CK(c, cudaMemcpy(out, g->d_q[which] + node0, (size_t)count * sizeof(long long), cudaMemcpyDeviceToHost));
     return sync_status(c);
+}
+
+MCS_API int mcs_grid_fixed_plane_range(mcs_grid* g, int which, int64_t* z0, int64_t* z1) {
+    if (!g || !z0 || !z1 || (which != MCS_Q_FIXED && which != MCS_Q_PART)) return MCS_ERR_ARG;
+    mcs_ctx* c = g->ctx;
+    if (g->v.type != GRID_CART3D) return set_err(c, MCS_ERR_UNSUPPORTED, "plane ranges are of cart3d grids");
+    if (int st = use_device(c)) return st;
+    if (!g->d_range && cudaMalloc(&g->d_range, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+        g->d_range = nullptr;
+        return set_err(c, MCS_ERR_NOMEM, "plane range buffer");
+    }
+    MCS_CK(c, cudaMemsetAsync(g->d_range, 0xff, sizeof(unsigned long long), c->stream));
+    MCS_CK(c, cudaMemsetAsync(g->d_range + 1, 0, sizeof(unsigned long long), c->stream));
+    k_nonzero_range<<<c->num_sms * 4, 256, 0, c->stream>>>(g->d_q[which], (long long)g->nq, g->d_range);
+    MCS_CK_LAUNCH(c);
+    unsigned long long r[2] = {0, 0};
+    MCS_CK(c, cudaMemcpyAsync(r, g->d_range, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+    if (int st = sync_status(c)) return st;
+    const long long plane = (long long)(g->v.nx + 1) * (g->v.ny + 1);
+    if (r[0] == ~0ull) {
+        *z0 = *z1 = 0;
+    } else {
+        *z0 = (int64_t)(r[0] / (unsigned long long)plane);
+        *z1 = (int64_t)(r[1] / (unsigned long long)plane) + 1;
+    }
+    return MCS_OK;
 }
 
 MCS_API int mcs_grid_zero(mcs_grid* g, int which) {

@@ -183,6 +183,7 @@ struct mcs_grid {
     double* d_qfd = nullptr;  // cyl: FP64 density part of qfixed, (M+2)x(N+2), made on first use
     void* d_init_ws = nullptr;   // initfromfiles! workspace (counts, bases, scan sums), kept
     size_t init_ws_bytes = 0;
+    unsigned long long* d_range = nullptr;   // mcs_grid_fixed_plane_range: first, last nonzero node
 };
 
 // The electron fluid of MCStreamer (fluid.jl) on a cylindrical grid: density ne and its

@@ -120,6 +120,31 @@ class Grid3D:
             return q
         return self._box_planes(lo, hi, rd).reshape(-1)
 
+    def read_fixed_planes(self, which: int, out: np.ndarray, filled=(0, 0)) -> tuple:
+        """Bring a charge array into the full host array `out` moving only the z-planes that
+        hold charge: the device finds their range, that slab is copied, and the planes of
+        `filled` (the range an earlier call on the same `out` returned) outside it are zeroed on
+        the host.  `out` must hold zeros outside `filled`.  Returns the new filled range; `out`
+        then equals read_fixed(which) node for node."""
+        plane = (self.nx + 1) * (self.ny + 1)
+        z0, z1 = C.c_int64(), C.c_int64()
+        self.ctx.check(self.ctx.lib.mcs_grid_fixed_plane_range(self.h_, which, C.byref(z0), C.byref(z1)))
+        z0, z1 = z0.value, z1.value
+        if z1 > z0:
+            view = out[z0 * plane:z1 * plane]
+            self.ctx.check(self.ctx.lib.mcs_grid_read_fixed_range(self.h_, which, z0 * plane, (z1 - z0) * plane,
+                                                                  L.i64ptr(view)))
+        f0, f1 = filled
+        if f1 > f0:   # planes of the earlier slab that are now empty
+            if z1 <= z0:
+                out[f0 * plane:f1 * plane] = 0
+            else:
+                if f0 < z0:
+                    out[f0 * plane:min(f1, z0) * plane] = 0
+                if f1 > z1:
+                    out[max(f0, z1) * plane:f1 * plane] = 0
+        return (z0, z1)
+
     def charge_array(self, which: int = L.Q_PART) -> "DeviceArray":
         """The device int64 charge array, exposed through __cuda_array_interface__ (so a
         collective library can sum it across processes in place)."""

@@ -268,3 +268,32 @@ def test_mesh_step_beyond_capacity_is_reported(ctx):
     assert err.value.code == L.ERR_CAPACITY
     assert pop.nparticles() == n
     _close(fld, pop, grid, tab)
+
+
+@pytest.mark.gpu
+def test_charge_read_by_occupied_planes(ctx):
+    """read_fixed_planes moves only the z-slab that holds charge and leaves the host array equal
+    to the full read, also after the cloud moved and left planes empty."""
+    t, tab, grid, p0, pop, otab, ofield = _setup(ctx, 6000, "fp32", spread=5e-6)
+    plane = (NX + 1) * (NY + 1)
+    host = np.zeros((NX + 1) * (NY + 1) * (NZ + 1), dtype=np.int64)
+    grid.zero(L.Q_PART)
+    streamer.density(grid, pop, -1.0)
+    filled = grid.read_fixed_planes(L.Q_PART, host)
+    full = grid.read_fixed(L.Q_PART)
+    np.testing.assert_array_equal(host, full)
+    nz = np.nonzero(full.reshape(NZ + 1, plane).any(axis=1))[0]
+    assert filled == (nz[0], nz[-1] + 1) and filled[1] - filled[0] < NZ + 1
+    # a smaller cloud near the bottom: the earlier slab's planes above it become zero
+    p1 = broad(2000, 7, emax_ev=10.0, x0=(CENTRE[0], CENTRE[1], 6 * H), spread=3e-6)
+    pop2 = jumc.Population(4000, p1, tab, precision="fp32", seed=7, mesh=grid)
+    grid.zero(L.Q_PART)
+    streamer.density(grid, pop2, -1.0)
+    filled2 = grid.read_fixed_planes(L.Q_PART, host, filled)
+    np.testing.assert_array_equal(host, grid.read_fixed(L.Q_PART))
+    assert filled2[1] <= filled[1]
+    # nothing deposited: the slab is empty and the host array all zero
+    grid.zero(L.Q_PART)
+    assert grid.read_fixed_planes(L.Q_PART, host, filled2) == (0, 0)
+    assert not host.any()
+    _close(pop2, pop, grid, tab)
