@@ -9,12 +9,15 @@
 // in ascending original slot order: the order in which the reference's serial passes
 // visit them.
 //
-// mcs_resample_cells: after the sort every cell is a contiguous segment.  One thread per
-// segment restates resample.jl's two passes serially in slot order (so the weight sums and
-// the roulette sequence are the reference's), first only counting the clones, then -- after
-// a scan of the counts gives each cell its place -- writing them.  Clones are appended in
-// cell order, which is the slot order of the sorted population (the serial reference's
-// append order).  Uniforms: one Philox stream per cell, ctr = {cell, call, k/4, tag}.
+// mcs_resample_cells: after the sort every cell is a contiguous segment.  A count pass
+// finds each cell's clones -- a thread per splitting cell, a warp per merging cell, which
+// records its clone sources and total weight -- and, after a scan of the counts gives each
+// cell its place, a write pass appends them.  The decisions are those of resample.jl's
+// serial passes in slot order: the merging cells' weight sums are the serial FP64 sums bit
+// for bit (exact warp sums where the weights allow, else the serial loop).  Clones are
+// appended in cell order, which is the slot order of the sorted population (the serial
+// reference's append order).  Uniforms: one Philox stream per cell, ctr = {cell, call,
+// k/4, tag}.  ntarget > nmax or ntarget > 128 takes a thread-per-cell form of both passes.
 #include <algorithm>
 
 #include "host_util.h"
@@ -184,15 +187,25 @@ struct DstArrays {
     uint8_t* act;
 };
 
+// A sorted key other than ncells belongs to an active particle, and on a mesh population
+// it is the particle's cell: only the particles keyed ncells (inactive, or outside the
+// mesh) read their flag and cell through the permutation.
 template <typename T>
-__global__ void k_gather(PopView<T> P, const uint32_t* __restrict__ perm, DstArrays d) {
+__global__ void k_gather(PopView<T> P, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ key,
+                         uint32_t ncells, DstArrays d) {
     const long long n = *P.n_in;
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
         const uint32_t s = perm[j];
+        const uint32_t k = key[j];
 #pragma unroll
         for (int q = 0; q < 8; ++q) static_cast<T*>(d.f[q])[j] = P.f[q][s];
-        if (d.cell) d.cell[j] = P.cell[s];
-        d.act[j] = P.act[s];
+        if (k != ncells) {
+            if (d.cell) d.cell[j] = k;
+            d.act[j] = 1;
+        } else {
+            if (d.cell) d.cell[j] = P.cell[s];
+            d.act[j] = P.act[s];
+        }
     }
 }
 
@@ -319,9 +332,8 @@ __device__ uint32_t resample_segment(const ResampleArgs& a, PopView<T>& P, long 
 // that the warp's memory accesses are coalesced:
 //  * split cells (p < ntarget): the first ntarget - p particles with w > 2, in index order,
 //    split -- a ballot rank over the cell's particles (no arithmetic order involved);
-//  * merge cells (p > nmax): the serial pass (FP64 weight sums in index order, the clone
-//    positions x) runs on lane 0 over the cell's weights staged in shared memory, and
-//    records the clone sources; the warp then writes the clones to consecutive slots and
+//  * merge cells (p > nmax): the count pass selects the clone sources and records them with
+//    the cell's total weight; the write pass copies the clones to consecutive slots and
 //    removes the originals.
 // ---------------------------------------------------------------------------------------
 constexpr int RS_WARPS = 8;       // warps per block
@@ -330,7 +342,7 @@ constexpr int RS_SRC = 128;       // clone sources a merge can record (ntarget a
 
 struct RsShared {
     double w[RS_WARPS][RS_BUF];
-    double f[RS_WARPS][RS_SRC];      // merge: f_k = samplemin(ntarget - k) of the cell's draw k
+    double f[RS_WARPS][RS_SRC];      // merge: f_k = samplemin(ntarget - k), then the positions t_k
     uint32_t src[RS_WARPS][RS_SRC];
 };
 
@@ -360,21 +372,30 @@ __device__ __forceinline__ void copy_clone(PopView<T>& P, long long d, long long
     P.f[6][d] = w;
 }
 
-// A merging cell (p > nmax) by one warp.  The sample positions of resample.jl:48-52 follow
-// x_1 = samplemin(ntarget) and x_(k+1) = x_k + samplemin(ntarget - k) (1 - x_k), where
-// samplemin draws the cell's k-th uniform: every factor f_k = 1 - (1 - U_k)^(1/(ntarget - k))
-// depends on the draw alone, so the lanes compute them side by side (the pows), and lane 0
-// runs the two serial passes over the staged weights with additions and products only --
-// unfused, in the reference's order -- recording the clone sources.  The warp then writes
-// the clones to consecutive slots and removes the originals.
-template <typename T, bool WRITE>
-__device__ uint32_t merge_segment_warp(const ResampleArgs& a, PopView<T>& P, long long b, long long e, uint32_t cell,
-                                       long long clone_base, long long cap, uint32_t* status, RsShared& sh,
-                                       int wid) {
+// Folds w into the exponent bounds of a cell's weights: emax = the largest exponent, lmin =
+// the exponent of the lowest set bit over all weights.  False for a weight that is
+// negative, -0, subnormal, infinite or NaN.
+__device__ __forceinline__ bool weight_bits(double w, int& emax, int& lmin) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(w);
+    if (u == 0ull) return true;
+    const int ex = (int)(u >> 52);   // sign bit included: a negative weight gives ex >= 0x800
+    if (ex == 0 || ex >= 0x7ff) return false;
+    const unsigned long long m = (u & ((1ull << 52) - 1ull)) | (1ull << 52);
+    emax = max(emax, ex - 1023);
+    lmin = min(lmin, ex - 1075 + (__ffsll((long long)m) - 1));
+    return true;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// f_k = samplemin(ntarget - k) = 1 - (1 - U_k)^(1/(ntarget - k)) of the cell's draws U_k,
+// k < ntarget, into fk (the lanes side by side).
+__device__ __forceinline__ void merge_factors(const ResampleArgs& a, uint32_t cell, double* fk) {
     const int lane = threadIdx.x & 31;
-    double* wb = sh.w[wid];
-    double* fk = sh.f[wid];
-    uint32_t* src = sh.src[wid];
     const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
     for (int k = lane; k < a.ntarget; k += 32) {
         // word k of the cell's stream {cell, call, k/4, TAG_CELL_RESAMPLE}
@@ -383,7 +404,133 @@ __device__ uint32_t merge_segment_warp(const ResampleArgs& a, PopView<T>& P, lon
         const uint32_t w = q == 0 ? blk.x : q == 1 ? blk.y : q == 2 ? blk.z : blk.w;
         fk[k] = 1.0 - pow(1.0 - uni64(w), 1.0 / (double)(a.ntarget - k));
     }
-    double wtotal = 0.0, x = 0.0;
+}
+
+// A merging cell (p > nmax) by one warp: the clone sources of resample.jl:31-76 and the
+// cell's total weight, recorded in sel[0, ncl) and *wt; returns ncl.
+//
+// The sample positions follow x_1 = samplemin(ntarget) and x_(k+1) = x_k + samplemin(ntarget
+// - k) (1 - x_k), where samplemin draws the cell's k-th uniform: every factor f_k = 1 - (1 -
+// U_k)^(1/(ntarget - k)) depends on the draw alone, so the lanes compute them side by side
+// (the pows).  Clone k is the first particle j whose running weight A_j = w_1 + ... + w_j
+// (summed in index order) exceeds t_k = wtotal x_k.
+//
+// Exact form: when every weight is a non-negative multiple of 2^lmin below 2^(emax+1) and
+// p 2^(emax+1) <= 2^(lmin+53), every partial sum of the cell's weights is an integer
+// multiple of 2^lmin below 2^53 of them, so FP64 adds it without rounding, in any order:
+// the warp's prefix sums are then the serial pass's running sums bit for bit.  The x_k
+// recurrence stays serial on lane 0 (unfused, the reference's order); with the t_k
+// non-decreasing, each lane finds its clones' sources by binary search over the running
+// sums staged in shared memory.  Otherwise lane 0 runs both serial passes over the weights
+// staged in shared memory.
+template <typename T>
+__device__ uint32_t merge_select_warp(const ResampleArgs& a, const PopView<T>& P, long long b, long long e,
+                                      uint32_t cell, RsShared& sh, int wid, uint32_t* __restrict__ sel,
+                                      double* __restrict__ wt) {
+    const int lane = threadIdx.x & 31;
+    double* wb = sh.w[wid];
+    double* fk = sh.f[wid];
+    uint32_t* src = sh.src[wid];
+    const int nt = a.ntarget;
+    merge_factors(a, cell, fk);
+    const long long p0 = e - b;
+    // pass 1: the exponent bounds and (exact when they allow) the total
+    int emax = -4096, lmin = 4096;
+    bool ok = true;
+    double part = 0.0;
+    for (long long j = b + lane; j < e; j += 32) {
+        const double w = (double)P.f[6][j];
+        ok = weight_bits(w, emax, lmin) && ok;
+        part += w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        emax = max(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+        lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+    }
+    const int lg = 64 - __clzll((unsigned long long)(p0 - 1));   // ceil(log2 p0), p0 >= 2
+    ok = __all_sync(0xffffffffu, ok) && (emax < -4000 || lg + emax + 1 <= lmin + 53);
+    double wtotal = warp_sum_d(part);
+    __syncwarp();   // fk visible
+    bool refill = false;   // fk overwritten by the t_k
+    if (ok) {
+        refill = true;
+        // t_k = wtotal x_k, serially; a decreasing t (x past 1) would break the search
+        if (lane == 0) {
+            double x = fk[0], tp = 0.0;
+            for (int k = 0; k < nt; ++k) {
+                if (k > 0) x = __dadd_rn(x, __dmul_rn(fk[k], __dadd_rn(1.0, -x)));
+                const double t = __dmul_rn(wtotal, x);
+                if (k > 0 && t < tp) ok = false;
+                fk[k] = t;
+                tp = t;
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+    }
+    if (ok) {
+        // pass 2: running sums by warp scans, a chunk of RS_BUF particles at a time
+        constexpr int KPL = RS_SRC / 32;
+        int jk[KPL];
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) jk[i] = -1;
+        double carry = 0.0;
+        for (long long c0 = b; c0 < e; c0 += RS_BUF) {
+            const int m = (int)((e - c0) < RS_BUF ? (e - c0) : RS_BUF);
+            for (int r = 0; r < m; r += 32) {
+                const int idx = r + lane;
+                double v = idx < m ? (double)P.f[6][c0 + idx] : 0.0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double y = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += y;
+                }
+                const double A = carry + v;
+                if (idx < m) wb[idx] = A;
+                carry = __shfl_sync(0xffffffffu, A, 31);
+            }
+            __syncwarp();
+            const double alast = wb[m - 1];
+#pragma unroll
+            for (int i = 0; i < KPL; ++i) {
+                const int k = lane + 32 * i;
+                if (k < nt && jk[i] < 0) {
+                    const double t = fk[k];
+                    if (t < alast) {
+                        int lo = 0, hi = m - 1;   // the first idx with t < wb[idx]
+                        while (lo < hi) {
+                            const int mid = (lo + hi) >> 1;
+                            if (t < wb[mid]) hi = mid; else lo = mid + 1;
+                        }
+                        jk[i] = (int)(c0 - b) + lo;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        // the selected k form a prefix 0..ncl-1 (t_k non-decreasing)
+        uint32_t cnt = 0;
+#pragma unroll
+        for (int i = 0; i < KPL; ++i) {
+            const int k = lane + 32 * i;
+            if (k < nt && jk[i] >= 0) {
+                sel[k] = (uint32_t)jk[i];
+                ++cnt;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0) *wt = wtotal;
+        return cnt;
+    }
+    // serial form: both passes on lane 0 over staged weights, in index order
+    if (refill) {
+        __syncwarp();
+        merge_factors(a, cell, fk);
+    }
+    wtotal = 0.0;
+    double x = 0.0;
     for (long long c0 = b; c0 < e; c0 += RS_BUF) {
         const long long m = (e - c0) < RS_BUF ? (e - c0) : RS_BUF;
         __syncwarp();
@@ -407,10 +554,10 @@ __device__ uint32_t merge_segment_warp(const ResampleArgs& a, PopView<T>& P, lon
         if (lane == 0) {
             for (int q = 0; q < m; ++q) {
                 const double wj = wb[q];
-                while (__dmul_rn(wtotal, x) < __dadd_rn(wcum, wj) && pk < a.ntarget) {
+                while (__dmul_rn(wtotal, x) < __dadd_rn(wcum, wj) && pk < nt) {
                     pk += 1;
                     src[ncl++] = (uint32_t)(c0 - b + q);
-                    if (pk < a.ntarget) x = __dadd_rn(x, __dmul_rn(fk[pk], __dadd_rn(1.0, -x)));
+                    if (pk < nt) x = __dadd_rn(x, __dmul_rn(fk[pk], __dadd_rn(1.0, -x)));
                 }
                 wcum = __dadd_rn(wcum, wj);
             }
@@ -418,58 +565,10 @@ __device__ uint32_t merge_segment_warp(const ResampleArgs& a, PopView<T>& P, lon
     }
     __syncwarp();
     ncl = __shfl_sync(0xffffffffu, ncl, 0);
-    if (WRITE) {
-        wtotal = __shfl_sync(0xffffffffu, wtotal, 0);
-        const T wc = (T)(wtotal / (double)a.ntarget);
-        for (uint32_t k = lane; k < ncl; k += 32) {
-            const long long d = clone_base + k;
-            if (d < cap) copy_clone<T>(P, d, b + src[k], wc);
-            else atomicOr(status, ST_CAPACITY);
-        }
-        for (long long j = b + lane; j < e; j += 32) P.act[j] = 0;   // remove_particle!
-    }
+    for (uint32_t k = lane; k < ncl; k += 32) sel[k] = src[k];
+    if (lane == 0) *wt = wtotal;
     __syncwarp();
     return ncl;
-}
-
-// Returns the number of clones of segment s (the same on every lane).
-template <typename T, bool WRITE>
-__device__ uint32_t resample_segment_warp(const ResampleArgs& a, PopView<T>& P, long long s, long long nseg,
-                                          long long clone_base, long long cap, uint32_t* status, RsShared& sh,
-                                          int wid) {
-    const int lane = threadIdx.x & 31;
-    const long long b = a.start[s];
-    const uint32_t cell = a.key[b];
-    const long long e = segment_end(a, s, nseg, b, cell);
-    const long long p0 = e - b;
-    // (the host takes the serial form when ntarget > nmax or ntarget > RS_SRC)
-    if (p0 < a.ntarget) {
-        // split: rank the particles with w > 2 in index order
-        const uint32_t K = (uint32_t)(a.ntarget - p0);
-        uint32_t ranked = 0;
-        for (long long j0 = b; j0 < e && ranked < K; j0 += 32) {
-            const long long j = j0 + lane;
-            double wj = 0.0;
-            bool q = false;
-            if (j < e) {
-                wj = (double)P.f[6][j];
-                q = wj > 2;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, q);
-            const uint32_t r = ranked + __popc(bal & ((1u << lane) - 1u));
-            if (WRITE && q && r < K) {
-                const double wnew = rint(wj / 2.0);   // Julia round: nearest, ties to even
-                const long long d = clone_base + r;
-                if (d < cap) copy_clone<T>(P, d, j, (T)wnew);
-                else atomicOr(status, ST_CAPACITY);
-                P.f[6][j] = (T)(wj - wnew);
-            }
-            ranked += __popc(bal);
-        }
-        return ranked < K ? ranked : K;
-    }
-    if (p0 <= a.nmax) return 0;
-    return merge_segment_warp<T, WRITE>(a, P, b, e, cell, clone_base, cap, status, sh, wid);
 }
 
 // Counting is latency-bound over millions of small segments: a thread per segment keeps 32
@@ -506,14 +605,17 @@ __global__ void __launch_bounds__(128) k_resample_count(ResampleArgs a, PopView<
     }
 }
 
+// The merging cells of the worklist, a warp each: their clone counts, sources (sel, ntarget
+// entries per listed cell) and total weights (wt).
 template <typename T>
 __global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_merge_count(ResampleArgs a, PopView<T> P,
                                                                          uint32_t* __restrict__ counts,
                                                                          const uint32_t* __restrict__ merge_list,
-                                                                         const unsigned long long* merge_n) {
+                                                                         const unsigned long long* merge_n,
+                                                                         uint32_t* __restrict__ sel,
+                                                                         double* __restrict__ wt) {
     __shared__ RsShared sh;
     const long long nm = (long long)*merge_n;
-    const long long n = *a.n;
     const long long nseg = *a.nseg;
     const int wid = threadIdx.x >> 5;
     const long long w0 = (long long)blockIdx.x * RS_WARPS + wid, ws = (long long)gridDim.x * RS_WARPS;
@@ -522,8 +624,7 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_merge_count(Resam
         const long long b = a.start[s];
         const uint32_t cell = a.key[b];
         const long long e = segment_end(a, s, nseg, b, cell);
-        (void)n;
-        const uint32_t c = merge_segment_warp<T, false>(a, P, b, e, cell, 0, 0, nullptr, sh, wid);
+        const uint32_t c = merge_select_warp<T>(a, P, b, e, cell, sh, wid, sel + q * a.ntarget, wt + q);
         if ((threadIdx.x & 31) == 0) counts[s] = c;
     }
 }
@@ -553,17 +654,89 @@ __global__ void __launch_bounds__(128) k_resample_write_serial(ResampleArgs a, P
     }
 }
 
+// The write pass.  Split cells (segments with clones that are not on the merge worklist)
+// take SPLIT_LANES lanes each, a warp four of them side by side: they are many and small
+// (p < ntarget), and a group's loads and clone stores cover consecutive slots.  Then the
+// merging cells, a warp each: their clones from the recorded sources, each with weight
+// wtotal / ntarget, and the removal of the originals.
+constexpr int SPLIT_LANES = 8;
+
 template <typename T>
 __global__ void __launch_bounds__(RS_WARPS * 32, 4) k_resample_write(ResampleArgs a, PopView<T> P,
+                                                                   const uint32_t* __restrict__ counts,
                                                                    const uint32_t* __restrict__ offs,
+                                                                   const uint32_t* __restrict__ merge_list,
+                                                                   const unsigned long long* merge_n,
+                                                                   const uint32_t* __restrict__ sel,
+                                                                   const double* __restrict__ wt,
                                                                    const long long* total, uint32_t* status) {
-    __shared__ RsShared sh;
+    constexpr int GPW = 32 / SPLIT_LANES;   // split cells per warp
     const long long nseg = *a.nseg;
     const long long n = *a.n;
-    const int wid = threadIdx.x >> 5;
-    const long long w0 = (long long)blockIdx.x * RS_WARPS + wid, ws = (long long)gridDim.x * RS_WARPS;
-    for (long long s = w0; s < nseg; s += ws)
-        resample_segment_warp<T, true>(a, P, s, nseg, n + (long long)offs[s], P.cap, status, sh, wid);
+    const int lane = threadIdx.x & 31;
+    const int g = lane / SPLIT_LANES, gl = lane % SPLIT_LANES;
+    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long ws = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long s0 = w0 * GPW; s0 < nseg; s0 += ws * GPW) {
+        const long long s = s0 + g;
+        long long b = 0, e = 0, d0 = 0;
+        uint32_t K = 0;   // clones of this group's cell: the first K particles with w > 2 split
+        if (s < nseg) {
+            const uint32_t cnt = counts[s];   // 0: a full cell, or a split cell of light particles
+            if (cnt) {
+                b = a.start[s];
+                if (s + 1 < nseg) {
+                    e = a.start[s + 1];
+                } else {
+                    const uint32_t cell = a.key[b];
+                    e = b;
+                    while (e < n && a.key[e] == cell) ++e;
+                }
+                if (e - b < a.ntarget) {   // merging cells (p > nmax) are written below
+                    K = cnt;
+                    d0 = n + (long long)offs[s];
+                }
+            }
+        }
+        // resample.jl:62-70 by rank among the cell's w > 2 particles in index order
+        uint32_t ranked = 0;
+        for (long long j0 = b; __any_sync(0xffffffffu, ranked < K && j0 < e); j0 += SPLIT_LANES) {
+            const long long j = j0 + gl;
+            double wj = 0.0;
+            bool q = false;
+            if (ranked < K && j < e) {
+                wj = (double)P.f[6][j];
+                q = wj > 2;
+            }
+            const unsigned bg = (__ballot_sync(0xffffffffu, q) >> (g * SPLIT_LANES)) & ((1u << SPLIT_LANES) - 1u);
+            const uint32_t r = ranked + __popc(bg & ((1u << gl) - 1u));
+            if (q && r < K) {
+                const double wnew = rint(wj / 2.0);   // Julia round: nearest, ties to even
+                const long long d = d0 + r;
+                if (d < P.cap) copy_clone<T>(P, d, j, (T)wnew);
+                else atomicOr(status, ST_CAPACITY);
+                P.f[6][j] = (T)(wj - wnew);
+            }
+            ranked += __popc(bg);
+        }
+    }
+    const long long nm = (long long)*merge_n;
+    for (long long q = w0; q < nm; q += ws) {
+        const long long s = merge_list[q];
+        const long long b = a.start[s];
+        const uint32_t cell = a.key[b];
+        const long long e = segment_end(a, s, nseg, b, cell);
+        const uint32_t ncl = counts[s];
+        const long long base = n + (long long)offs[s];
+        const T wc = (T)(wt[q] / (double)a.ntarget);
+        const uint32_t* sq = sel + q * a.ntarget;
+        for (uint32_t k = lane; k < ncl; k += 32) {
+            const long long d = base + k;
+            if (d < P.cap) copy_clone<T>(P, d, b + sq[k], wc);
+            else atomicOr(status, ST_CAPACITY);
+        }
+        for (long long j = b + lane; j < e; j += 32) P.act[j] = 0;   // remove_particle!
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         long long m = n + *total;
         if (m > P.cap) { m = P.cap; atomicOr(status, ST_CAPACITY); }
@@ -655,7 +828,7 @@ int sort_cells_t(mcs_pop* p, mcs_grid* g, uint32_t** keys_out) {
     for (int q = 0; q < 8; ++q) d.f[q] = p->alt[q];
     d.cell = p->cell ? p->alt_cell : nullptr;
     d.act = p->alt_act;
-    k_gather<T><<<gr, 256, 0, c->stream>>>(pop_view<T>(p), p->sort_val[cur], d);
+    k_gather<T><<<gr, 256, 0, c->stream>>>(pop_view<T>(p), p->sort_val[cur], p->sort_key[cur], ncells, d);
     MCS_CK_LAUNCH(c);
     for (int q = 0; q < 8; ++q) std::swap(p->f[q], p->alt[q]);
     std::swap(p->act, p->alt_act);
@@ -691,30 +864,37 @@ int resample_cells_t(mcs_pop* p, mcs_grid* g, int ntarget, int nmax) {
     a.nmax = nmax;
     a.seed = p->seed;
     a.call = p->resample_calls++;
-    if (ntarget > nmax || ntarget > RS_SRC) {
+    const bool serial = ntarget > nmax || ntarget > RS_SRC;
+    // merging cells hold more than nmax particles each: at most n / (nmax + 1) of them, so
+    // their recorded sources (ntarget each, ntarget <= nmax) fit in one cap-slot array (the
+    // sort's permutation, consumed by the gather) and their FP64 totals in another (the
+    // sort's free key buffer, cap 32-bit words)
+    unsigned long long* merge_n = reinterpret_cast<unsigned long long*>(p->counters + 14);
+    const int cur = keys == p->sort_key[1];
+    uint32_t* sel = p->sort_val[cur];
+    double* wt = reinterpret_cast<double*>(p->sort_key[cur ^ 1]);
+    if (serial) {
         k_resample_count_serial<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, c->d_status);
         MCS_CK_LAUNCH(c);
     } else {
-        // merging cells hold more than nmax particles each: at most n / (nmax + 1) of them
-        unsigned long long* merge_n = reinterpret_cast<unsigned long long*>(p->counters + 14);
         MCS_CK(c, cudaMemsetAsync(merge_n, 0, sizeof(unsigned long long), c->stream));
         k_resample_count<T><<<gr, 128, 0, c->stream>>>(a, pop_view<T>(p), p->seg_a, p->u32b, merge_n);
         MCS_CK_LAUNCH(c);
         int occ = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_resample_merge_count<T>, RS_WARPS * 32, 0);
         k_resample_merge_count<T><<<std::max(occ, 1) * c->num_sms, RS_WARPS * 32, 0, c->stream>>>(
-            a, pop_view<T>(p), p->seg_a, p->u32b, merge_n);
+            a, pop_view<T>(p), p->seg_a, p->u32b, merge_n, sel, wt);
         MCS_CK_LAUNCH(c);
     }
     if (int st = launch_scan(p, p->seg_a, p->seg_b, nseg, total)) return st;
     PopView<T> P = pop_view<T>(p);
-    if (ntarget > nmax || ntarget > RS_SRC) {
+    if (serial) {
         k_resample_write_serial<T><<<gr, 128, 0, c->stream>>>(a, P, p->seg_b, total, c->d_status);
     } else {
-        int occ = 0;   // the warp-per-segment write pass: all blocks resident, grid-stride over segments
+        int occ = 0;   // the warp-per-cell write pass: all blocks resident, grid-stride over cells
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_resample_write<T>, RS_WARPS * 32, 0);
-        k_resample_write<T><<<std::max(occ, 1) * c->num_sms, RS_WARPS * 32, 0, c->stream>>>(a, P, p->seg_b, total,
-                                                                                              c->d_status);
+        k_resample_write<T><<<std::max(occ, 1) * c->num_sms, RS_WARPS * 32, 0, c->stream>>>(
+            a, P, p->seg_a, p->seg_b, p->u32b, merge_n, sel, wt, total, c->d_status);
     }
     MCS_CK_LAUNCH(c);
     p->cur ^= 1;
