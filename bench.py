@@ -550,6 +550,43 @@ def oracle_rate(sub: SubMeshOracle, parts, seconds: float, seed: int) -> dict:
     return {"value": active / dt, "unit": UNIT, "cores": sub.threads, "kind": "port", "m": m, "seconds": dt}
 
 
+def host_link_gbs(torch, nbytes: int = 1 << 30, reps: int = 4) -> dict:
+    """Pinned host <-> device copy bandwidth of this GPU (GB/s): each direction alone, and
+    per direction with both running at once on two streams -- the bound of a pipelined
+    host-resident step, whose uploads and downloads overlap."""
+    h_up = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_dn = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_up = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_dn = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s_up, s_dn = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def rate(up: bool, down: bool) -> float:
+        cur = torch.cuda.current_stream()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(cur)
+        s_up.wait_event(e0)
+        s_dn.wait_event(e0)
+        for _ in range(reps):
+            if up:
+                with torch.cuda.stream(s_up):
+                    d_up.copy_(h_up, non_blocking=True)
+            if down:
+                with torch.cuda.stream(s_dn):
+                    h_dn.copy_(d_dn, non_blocking=True)
+        cur.wait_stream(s_up)
+        cur.wait_stream(s_dn)
+        e1.record(cur)
+        torch.cuda.synchronize()
+        return reps * nbytes / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+    rate(True, True)   # warm-up
+    out = {"h2d_gbs": rate(True, False), "d2h_gbs": rate(False, True), "both_gbs_per_direction": rate(True, True)}
+    del h_up, h_dn, d_up, d_dn
+    torch.cuda.empty_cache()
+    return out
+
+
 def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     """The same steps through the C ABI with the population in HOST memory (the plain drop-in
     for a Julia Population): the population entering the first timed step is downloaded into
@@ -606,8 +643,14 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     steps = args.e2e_steps
     m = nn.value
     host = jumc.ParticleArrays(x[:m], v[:m], w[:m], s[:m], a[:m])
+    # the host link's own bound for these bytes: both directions at once, on this GPU, now
+    link = host_link_gbs(torch)
+    bound_ms = max(h2d, d2h) / steps / (link["both_gbs_per_direction"] * 1e9) * 1e3
+    link.update({"bound_ms_per_step": bound_ms, "ms_per_step": ms / steps, "frac": bound_ms / (ms / steps),
+                 "note": "pinned 1 GiB copies timed with CUDA events after the e2e steps; bound = the larger "
+                         "direction's bytes per step at the both-directions rate; frac = bound / measured"})
     return host, {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // steps,
-            "d2h_bytes_per_step": d2h // steps, "steps": steps, "electrons_at_start": n,
+            "d2h_bytes_per_step": d2h // steps, "steps": steps, "electrons_at_start": n, "host_link": link,
             "path": f"mcs_advance_deposit_host on pinned host arrays in the Julia layout ({chunks} chunks: uploads, "
                     "fused steps and downloads pipelined on three streams) + the 2.15 GB deposit grid into a "
                     "pinned host array, every step, moving the z-planes that hold charge (mcs_grid_fixed_plane_range "
