@@ -385,11 +385,12 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
     """The same step through the C ABI with a host-resident population (the plain drop-in for
     a Julia population in host memory): the particles live in pinned host arrays in the Julia
     layout and mcs_advance_deposit_host steps them in place, with uploads, fused steps and
-    downloads pipelined over chunks; the deposit grid is read back every step."""
+    downloads pipelined over chunks; the deposit grid is read back every step.  The byte
+    counts are the library's own (mcs_pop_host_step_bytes)."""
     import ctypes as C
 
     from mcstreamer_b200 import dist as mdist
-    from mcstreamer_b200 import jumc
+    from mcstreamer_b200 import jumc, streamer
 
     chunks = max(1, args.e2e_chunks)
     n = parts.n
@@ -425,6 +426,7 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
         ctx.check(lib.mcs_advance_deposit_host(work.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0,
                                                L.dptr(ox), L.dptr(ov), L.dptr(ow), L.dptr(os_), L.u8ptr(oa),
                                                C.byref(nn), cap, chunks))
+        up, down = streamer.host_step_bytes(work)   # what the call copied (host counters, no device work)
         if ws > 1:
             mdist.allreduce_charge(grid, L.Q_PART)
         ctx.check(lib.mcs_grid_read_fixed(grid.h_, L.Q_PART, L.i64ptr(hq)))
@@ -434,8 +436,8 @@ def run_e2e(args, spec, parts, pop, grid, fld, trk, ctx, stream, torch, L, ws, d
             continue   # warm-up: the workspace's staging buffers are allocated here
         ms += t0.elapsed_time(t1)
         active += n_active
-        h2d += n * 65
-        d2h += nn.value * 65 + nodes * 8
+        h2d += up
+        d2h += down + nodes * 8
     work.close()
     if ws > 1:
         t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
@@ -591,14 +593,16 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     """The same steps through the C ABI with the population in HOST memory (the plain drop-in
     for a Julia Population): the population entering the first timed step is downloaded into
     pinned host arrays in the Julia layout (65 B per electron), and mcs_advance_deposit_host
-    steps it in place -- uploads, fused steps and downloads pipelined over chunks -- after
+    steps it in place -- uploads, fused steps and downloads pipelined over chunks; the weights,
+    which a step leaves unchanged, stay on the host when the upload kept them exactly -- after
     which the deposit grid is brought to pinned host memory (the slab of z-planes that holds
-    charge; the rest of the host array is kept zero), every step.  No resample! is
+    charge; the rest of the host array is kept zero), every step.  The byte counts are the
+    library's own (mcs_pop_host_step_bytes).  No resample! is
     called (the library has no host-resident resample; it is one step in ten of the device
     run)."""
     import ctypes as C
 
-    from mcstreamer_b200 import jumc
+    from mcstreamer_b200 import jumc, streamer
     n = pop.nparticles()
     cap = int(n * 1.25) + 1024
     chunks = max(1, args.e2e_chunks)
@@ -629,6 +633,7 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
         ctx.check(lib.mcs_advance_deposit_host(work.h, pop.collisions.h, fld.h, spec.dt, trk.h, grid.h_, -1.0,
                                                L.dptr(x), L.dptr(v), L.dptr(w), L.dptr(s), L.u8ptr(a), C.byref(nn),
                                                cap, chunks))
+        up, down = streamer.host_step_bytes(work)   # what the call copied (host counters, no device work)
         # the whole deposit grid on the host, moving the z-slab that holds charge
         filled = grid.read_fixed_planes(L.Q_PART, hq, filled)
         t1.record(stream)
@@ -637,8 +642,8 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
             continue   # warm-up: the workspace's staging buffers are allocated here
         ms += t0.elapsed_time(t1)
         active += act_in
-        h2d += n_in * 65
-        d2h += nn.value * 65 + (filled[1] - filled[0]) * plane * 8 + 16
+        h2d += up
+        d2h += down + (filled[1] - filled[0]) * plane * 8 + 16
     work.close()
     steps = args.e2e_steps
     m = nn.value
@@ -652,7 +657,8 @@ def cfg2_e2e(args, spec, pop, grid, fld, trk, ctx, stream, torch, L):
     return host, {"value": active / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d // steps,
             "d2h_bytes_per_step": d2h // steps, "steps": steps, "electrons_at_start": n, "host_link": link,
             "path": f"mcs_advance_deposit_host on pinned host arrays in the Julia layout ({chunks} chunks: uploads, "
-                    "fused steps and downloads pipelined on three streams) + the 2.15 GB deposit grid into a "
+                    "fused steps and downloads pipelined on three streams; unchanged weights are not downloaded) + "
+                    "the 2.15 GB deposit grid into a "
                     "pinned host array, every step, moving the z-planes that hold charge (mcs_grid_fixed_plane_range "
                     "+ mcs_grid_read_fixed_range; the host array equals the full grid); the population entering the "
                     "first timed step, evolving; CUDA events around each step; no resample! (no host-resident entry "

@@ -243,6 +243,13 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
                                      mcs_grid* tracker, mcs_grid* deposit, double val, double* x, double* v,
                                      double* w, double* s, uint8_t* active, int64_t* n, int64_t capacity,
                                      int chunks);
+/* Bytes that the last mcs_advance_deposit_host call on p copied host -> device and device ->
+ * host (0 before the first call).  A particle's weight, which the step leaves unchanged, goes
+ * back to the host only when some weight of its chunk changed on upload (an FP64 weight that
+ * an FP32 population rounds), so the download moves 57 instead of 65 bytes per stepped
+ * particle when none did.  No reference counterpart: a transfer figure of the host-resident
+ * path. */
+MCS_API int mcs_pop_host_step_bytes(const mcs_pop* p, int64_t* h2d, int64_t* d2h);
 /* Uniform source of advance! and collisions!.  The reference draws Julia's rand()
  * (JuMC/src/util.jl:5,8,17, collisions.jl:166, mixed_population.jl:48; rand() in a
  * single-threaded run is one serial stream); the library draws counter-based Philox streams

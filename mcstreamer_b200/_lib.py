@@ -81,6 +81,7 @@ SIGNATURES = {
     "mcs_advance": (i32, [vp, vp, vp, f64, vp]),
     "mcs_advance_deposit": (i32, [vp, vp, vp, f64, vp, vp, f64]),
     "mcs_advance_deposit_host": (i32, [vp, vp, vp, f64, vp, vp, f64, pd, pd, pd, pd, pu8, pi64, i64, i32]),
+    "mcs_pop_host_step_bytes": (i32, [vp, pi64, pi64]),
     "mcs_collisions": (i32, [vp, vp, f64, vp]),
     "mcs_set_uniform_source": (i32, [vp, i32, pd, pi64, i64]),
     "mcs_deposit": (i32, [vp, vp, f64]),

@@ -18,18 +18,24 @@ namespace mcs {
 
 // Workspace of mcs_advance_deposit_host, kept in the population between calls and grown
 // when a call needs more: two Julia-layout staging buffers each way, pinned per-chunk
-// counts, the copy streams and per-chunk events.
+// counts and weight flags, the copy streams and per-chunk events; and the bytes the last
+// call copied each way.
 struct HostStepBuffers {
     double* in[2] = {nullptr, nullptr};    // a chunk's input
     double* out[2] = {nullptr, nullptr};   // a chunk's output (the chunk and its secondaries)
     long long* cnt = nullptr;              // pinned: particles after each chunk's step
+    unsigned int* wl = nullptr;            // pinned: 1 when a chunk's weights changed on upload
+    unsigned int* d_wl = nullptr;          // the flags on the device
     size_t in_bytes = 0, out_bytes = 0;
     int nch = 0;
+    long long h2d = 0, d2h = 0;            // bytes copied by the last call
     cudaStream_t s_in = nullptr, s_out = nullptr;
     std::vector<cudaEvent_t> ev;
     ~HostStepBuffers() {
         for (int q = 0; q < 2; ++q) { cudaFree(in[q]); cudaFree(out[q]); }
         if (cnt) cudaFreeHost(cnt);
+        if (wl) cudaFreeHost(wl);
+        cudaFree(d_wl);
         if (s_in) cudaStreamDestroy(s_in);
         if (s_out) cudaStreamDestroy(s_out);
         for (auto e : ev) cudaEventDestroy(e);
@@ -62,8 +68,14 @@ int ensure_host_step(mcs_pop* p, size_t in_bytes, size_t out_bytes, int nch) {
     B.out_bytes = std::max(B.out_bytes, out_bytes);
     if (B.nch < nch) {
         if (B.cnt) cudaFreeHost(B.cnt);
+        if (B.wl) cudaFreeHost(B.wl);
+        cudaFree(B.d_wl);
         B.cnt = nullptr;
-        if (cudaHostAlloc(&B.cnt, sizeof(long long) * nch, cudaHostAllocDefault) != cudaSuccess)
+        B.wl = nullptr;
+        B.d_wl = nullptr;
+        if (cudaHostAlloc(&B.cnt, sizeof(long long) * nch, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&B.wl, sizeof(unsigned int) * nch, cudaHostAllocDefault) != cudaSuccess ||
+            cudaMalloc(&B.d_wl, sizeof(unsigned int) * nch) != cudaSuccess)
             return set_err(c, MCS_ERR_NOMEM, "host-step counts");
         while ((int)B.ev.size() < 3 * nch) {
             cudaEvent_t e;
@@ -111,6 +123,7 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
     const long long n0 = *n_io;
     if (n0 < 0 || n0 > capacity || !(dt >= 0)) return MCS_ERR_ARG;
     if (cudaSetDevice(c->device) != cudaSuccess) return MCS_ERR_CUDA;
+    if (p->host_step) p->host_step->h2d = p->host_step->d2h = 0;
     if (n0 == 0) return MCS_OK;
     const long long chunk = (n0 + chunks - 1) / chunks;
     const int nch = (int)((n0 + chunk - 1) / chunk);
@@ -123,6 +136,7 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
     const size_t out_bytes = (size_t)out_m * 8 * sizeof(double) + (size_t)out_m;
     if (int r = ensure_host_step(p, in_bytes, out_bytes, nch)) return r;
     HostStepBuffers& B = *p->host_step;
+    B.h2d = B.d2h = 0;
     // per chunk events: uploaded, stepped (staging_in free, outputs staged), downloaded
     auto ev_in = [&](int k) { return B.ev[3 * k]; };
     auto ev_comp = [&](int k) { return B.ev[3 * k + 1]; };
@@ -142,6 +156,7 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
         if (e == cudaSuccess) e = cudaMemcpyAsync(d.s, s + a, m * sizeof(double), cudaMemcpyHostToDevice, B.s_in);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d.a, active + a, (size_t)m, cudaMemcpyHostToDevice, B.s_in);
         if (e == cudaSuccess) e = cudaEventRecord(ev_in(k), B.s_in);
+        B.h2d += m * 65;
         return e == cudaSuccess ? MCS_OK : set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
     };
     auto enqueue_comp = [&](int k) -> int {
@@ -150,7 +165,9 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
         const JView o = jview(B.out[k & 1], out_m);
         cudaStreamWaitEvent(c->stream, ev_in(k), 0);
         if (k >= 2) cudaStreamWaitEvent(c->stream, ev_out(k - 2), 0);   // staging_out[k&1] downloaded
-        if (int r = launch_upload(p, d.x, d.v, d.w, d.s, d.a, m)) return r;
+        if (cudaMemsetAsync(B.d_wl + k, 0, sizeof(unsigned int), c->stream) != cudaSuccess)
+            return set_err(c, MCS_ERR_CUDA, "host-step flag");
+        if (int r = launch_upload(p, d.x, d.v, d.w, d.s, d.a, m, B.d_wl + k)) return r;
         k_set_count<<<1, 1, 0, c->stream>>>(p->d_n + p->cur, m);
         p->step = step0;
         p->slot_base = (uint32_t)a;
@@ -161,6 +178,9 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
         p->cur ^= 1;
         if (int r2 = launch_download(p, o.x, o.v, o.w, o.s, o.a)) return r2;
         cudaError_t e = cudaMemcpyAsync(B.cnt + k, p->d_n + p->cur, sizeof(long long), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(B.wl + k, B.d_wl + k, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream);
+        B.d2h += sizeof(long long) + sizeof(unsigned int);
         if (e == cudaSuccess) e = cudaEventRecord(ev_comp(k), c->stream);
         return e == cudaSuccess ? MCS_OK : set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
     };
@@ -174,19 +194,22 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
         cudaStreamWaitEvent(B.s_out, ev_comp(k), 0);
         const long long ds = n0 + sec_total;
         cudaError_t e = cudaSuccess;
-        const struct { long long dst, src, cnt; } parts[2] = {{a, 0, m}, {ds, m, nsec}};
+        // The step never changes the weight of a particle it is given (its secondaries carry
+        // their own), so the chunk's weights come back only when the upload rounded one.
+        const struct { long long dst, src, cnt; bool w; } parts[2] = {{a, 0, m, B.wl[k] != 0u}, {ds, m, nsec, true}};
         for (const auto& q : parts) {
             if (q.cnt <= 0) continue;
             if (e == cudaSuccess) e = cudaMemcpyAsync(x + 3 * q.dst, o.x + 3 * q.src, 3 * q.cnt * sizeof(double),
                                                       cudaMemcpyDeviceToHost, B.s_out);
             if (e == cudaSuccess) e = cudaMemcpyAsync(v + 3 * q.dst, o.v + 3 * q.src, 3 * q.cnt * sizeof(double),
                                                       cudaMemcpyDeviceToHost, B.s_out);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(w + q.dst, o.w + q.src, q.cnt * sizeof(double),
-                                                      cudaMemcpyDeviceToHost, B.s_out);
+            if (e == cudaSuccess && q.w) e = cudaMemcpyAsync(w + q.dst, o.w + q.src, q.cnt * sizeof(double),
+                                                             cudaMemcpyDeviceToHost, B.s_out);
             if (e == cudaSuccess) e = cudaMemcpyAsync(s + q.dst, o.s + q.src, q.cnt * sizeof(double),
                                                       cudaMemcpyDeviceToHost, B.s_out);
             if (e == cudaSuccess) e = cudaMemcpyAsync(active + q.dst, o.a + q.src, (size_t)q.cnt,
                                                       cudaMemcpyDeviceToHost, B.s_out);
+            B.d2h += q.cnt * (q.w ? 65 : 57);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ev_out(k), B.s_out);
         sec_total += nsec;
@@ -210,6 +233,13 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
     if (st) return st;
     *n_io = n0 + sec_total;
     return sync_status(c);
+}
+
+MCS_API int mcs_pop_host_step_bytes(const mcs_pop* p, int64_t* h2d, int64_t* d2h) {
+    if (!p || !h2d || !d2h) return MCS_ERR_ARG;
+    *h2d = p->host_step ? p->host_step->h2d : 0;
+    *d2h = p->host_step ? p->host_step->d2h : 0;
+    return MCS_OK;
 }
 
 }  // extern "C"

@@ -15,7 +15,7 @@ constexpr uint32_t kOutside = 0xffffffffu;  // mesh layout: particle outside the
 template <typename T>
 __global__ void k_upload(const double* __restrict__ x, const double* __restrict__ v, const double* __restrict__ w,
                          const double* __restrict__ s, const uint8_t* __restrict__ a, long long n, PopView<T> P,
-                         GridView g, int mesh) {
+                         GridView g, int mesh, unsigned int* __restrict__ w_lossy) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double px = x[3 * i], py = x[3 * i + 1], pz = x[3 * i + 2];
         if (mesh) {
@@ -42,7 +42,10 @@ __global__ void k_upload(const double* __restrict__ x, const double* __restrict_
             P.f[0][i] = (T)px; P.f[1][i] = (T)py; P.f[2][i] = (T)pz;
         }
         P.f[3][i] = (T)v[3 * i]; P.f[4][i] = (T)v[3 * i + 1]; P.f[5][i] = (T)v[3 * i + 2];
-        P.f[6][i] = (T)w[i];
+        const double wi = w[i];
+        const T wc = (T)wi;
+        P.f[6][i] = wc;
+        if (w_lossy && !((double)wc == wi)) *w_lossy = 1u;   // the weight does not round-trip
         P.f[7][i] = (T)s[i];
         P.act[i] = a[i] ? 1 : 0;
     }
@@ -636,15 +639,15 @@ int launch_deposit(mcs_pop* p, mcs_grid* g, double val) {
 
 // ---------------------------------------------------------------------------------------
 int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* dw, const double* ds, const uint8_t* da,
-                  long long n) {
+                  long long n, unsigned int* w_lossy) {
     mcs_ctx* c = p->ctx;
     const int gr = grid_for(c, n, 256);
     const GridView gv = grid_view(p->cells);
     const int mesh = p->cells != nullptr;
     if (p->precision == MCS_FP32)
-        k_upload<float><<<gr, 256, 0, c->stream>>>(dx, dv, dw, ds, da, n, pop_view<float>(p), gv, mesh);
+        k_upload<float><<<gr, 256, 0, c->stream>>>(dx, dv, dw, ds, da, n, pop_view<float>(p), gv, mesh, w_lossy);
     else
-        k_upload<double><<<gr, 256, 0, c->stream>>>(dx, dv, dw, ds, da, n, pop_view<double>(p), gv, mesh);
+        k_upload<double><<<gr, 256, 0, c->stream>>>(dx, dv, dw, ds, da, n, pop_view<double>(p), gv, mesh, w_lossy);
     MCS_CK_LAUNCH(c);
     return MCS_OK;
 }

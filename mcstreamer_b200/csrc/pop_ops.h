@@ -11,8 +11,10 @@ int launch_repack(mcs_pop* p);
 int launch_swarm_resample(mcs_pop* p, long long n0, double tol);
 int launch_moments(mcs_pop* p, const mcs_table* t, double* d_out, int nm);
 int launch_deposit(mcs_pop* p, mcs_grid* g, double val);
+// w_lossy (device word, optional) is set to 1 when some uploaded weight changes in the
+// population's precision (FP32 only), so that a download must bring the weights back.
 int launch_upload(mcs_pop* p, const double* dx, const double* dv, const double* dw, const double* ds,
-                  const uint8_t* da, long long n);
+                  const uint8_t* da, long long n, unsigned int* w_lossy = nullptr);
 int launch_download(mcs_pop* p, double* dx, double* dv, double* dw, double* ds, uint8_t* da);
 int grid_for(mcs_ctx* c, long long n, int block);
 int launch_init_maxwellian(mcs_pop* p, long long n, double sigma);

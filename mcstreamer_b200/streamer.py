@@ -276,6 +276,14 @@ def advance_deposit_host(work: Population, efield: FieldInterp, dt: float, track
     return nn.value
 
 
+def host_step_bytes(work: Population) -> tuple:
+    """(host -> device, device -> host) bytes that the last advance_deposit_host call with
+    this workspace copied (mcs_pop_host_step_bytes)."""
+    up, down = C.c_int64(), C.c_int64()
+    work.ctx.check(work.ctx.lib.mcs_pop_host_step_bytes(work.h, C.byref(up), C.byref(down)))
+    return up.value, down.value
+
+
 def resample(popl: Population, grid, ntarget: int, nmax: int) -> None:
     """resample!(popl, fields, ntarget, nmax) (MCStreamer/src/resample.jl:7-77): the stable
     cell sort, then the per-cell roulette and splitting."""

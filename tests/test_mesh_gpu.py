@@ -129,11 +129,13 @@ def test_mesh_particles_leaving_and_reentering(ctx):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("chunks", [1, 3, 7])
-def test_host_resident_step_equals_device_step(ctx, chunks):
+@pytest.mark.parametrize("chunks,weights", [(1, "exact"), (3, "exact"), (7, "exact"), (3, "rounded")])
+def test_host_resident_step_equals_device_step(ctx, chunks, weights):
     """mcs_advance_deposit_host (chunked, pipelined transfers) against upload + fused step +
     download of the same population: the same particles in the same slots, the same
-    secondaries in the same order, the same int64 charges."""
+    secondaries in the same order, the same int64 charges.  With FP32-exact weights the
+    stepped particles' weights stay on the host (57 bytes down per particle); weights that
+    the FP32 upload rounds come back rounded, as a download gives them (65 bytes)."""
     n = 40000
     t, tab, grid, p0, pop, otab, ofield = _setup(ctx, n, "fp32", emax_ev=200.0)
     host_in = pop.download()                     # the cloud as the device layout holds it
@@ -149,10 +151,18 @@ def test_host_resident_step_equals_device_step(ctx, chunks):
     host = jumc.ParticleArrays.empty(cap)
     host.x[:n], host.v[:n], host.w[:n], host.s[:n], host.active[:n] = (host_in.x, host_in.v, host_in.w, host_in.s,
                                                                        host_in.active)
+    if weights == "rounded":
+        host.w[:n] *= 1.0 + 2.0 ** -40          # off the FP32 grid; rounds back to the same float
+        assert not np.array_equal(host.w[:n], host_in.w)
     work = jumc.Population((n + chunks - 1) // chunks + n // 2, None, tab, precision="fp32", seed=21, mesh=grid)
     grid.zero(L.Q_FIXED); grid.zero(L.Q_PART)
     m = streamer.advance_deposit_host(work, fld, dt, trk, grid, host, n, -1.0, chunks=chunks)
     assert m == ref.n
+    chunk = (n + chunks - 1) // chunks
+    nch = (n + chunk - 1) // chunk
+    up, down = streamer.host_step_bytes(work)
+    assert up == 65 * n
+    assert down == 65 * (m - n) + (65 if weights == "rounded" else 57) * n + 12 * nch
     np.testing.assert_array_equal(host.x[:m], ref.x)
     np.testing.assert_array_equal(host.v[:m], ref.v)
     np.testing.assert_array_equal(host.w[:m], ref.w)
