@@ -224,7 +224,7 @@ __global__ void k_download(double* __restrict__ x, double* __restrict__ v, doubl
 // handed out by an atomic ticket).  in == nullptr scans the active flags of the population.
 // total (optional) receives the sum.
 // ---------------------------------------------------------------------------------------
-constexpr int SCAN_BLOCK = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
+constexpr int SCAN_BLOCK = 256, SCAN_ITEMS = 16, SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
 
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict__ in, const uint8_t* __restrict__ act,
                                                      uint32_t* __restrict__ out, const long long* n_ptr,
@@ -237,28 +237,29 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict_
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     // vector accesses when the arrays start on 16-byte boundaries (allocation bases do)
     const bool vec = ((reinterpret_cast<uintptr_t>(out) | reinterpret_cast<uintptr_t>(in) |
-                       (reinterpret_cast<uintptr_t>(act) & 7u)) & 15u) == 0;
+                       reinterpret_cast<uintptr_t>(act)) & 15u) == 0;
     for (;;) {
         if (threadIdx.x == 0) s_tile = atomicAdd(&counters[0], 1u);
         __syncthreads();
         const long long tile = s_tile;
         if (tile >= ntiles) break;
         const long long base = tile * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
-        const bool full = base + SCAN_ITEMS <= n;   // a thread's 8 items as two 16-byte (or one 8-byte) accesses
+        const bool full = base + SCAN_ITEMS <= n;   // a thread's 16 items as four (flags: one) 16-byte accesses
         uint32_t c8[SCAN_ITEMS];
         if (full && vec) {
             if (in) {
-                const uint4 a = *reinterpret_cast<const uint4*>(in + base);
-                const uint4 b = *reinterpret_cast<const uint4*>(in + base + 4);
-                c8[0] = a.x; c8[1] = a.y; c8[2] = a.z; c8[3] = a.w;
-                c8[4] = b.x; c8[5] = b.y; c8[6] = b.z; c8[7] = b.w;
-            } else {
-                const uint2 a = *reinterpret_cast<const uint2*>(act + base);
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    c8[q] = ((a.x >> (8 * q)) & 0xffu) != 0;
-                    c8[4 + q] = ((a.y >> (8 * q)) & 0xffu) != 0;
+                for (int r = 0; r < SCAN_ITEMS / 4; ++r) {
+                    const uint4 a = *reinterpret_cast<const uint4*>(in + base + 4 * r);
+                    c8[4 * r] = a.x; c8[4 * r + 1] = a.y; c8[4 * r + 2] = a.z; c8[4 * r + 3] = a.w;
                 }
+            } else {
+                const uint4 a = *reinterpret_cast<const uint4*>(act + base);
+                const uint32_t wv[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) c8[4 * r + q] = ((wv[r] >> (8 * q)) & 0xffu) != 0;
             }
         } else {
 #pragma unroll
@@ -302,8 +303,10 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan(const uint32_t* __restrict_
         __syncthreads();
         const uint32_t off = s_excl + s_warp[wid] + incl - tsum;
         if (full && vec) {
-            *reinterpret_cast<uint4*>(out + base) = make_uint4(off + v[0], off + v[1], off + v[2], off + v[3]);
-            *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(off + v[4], off + v[5], off + v[6], off + v[7]);
+#pragma unroll
+            for (int r = 0; r < SCAN_ITEMS / 4; ++r)
+                *reinterpret_cast<uint4*>(out + base + 4 * r) =
+                    make_uint4(off + v[4 * r], off + v[4 * r + 1], off + v[4 * r + 2], off + v[4 * r + 3]);
         } else {
 #pragma unroll
             for (int q = 0; q < SCAN_ITEMS; ++q) {
