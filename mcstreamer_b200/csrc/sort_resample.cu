@@ -187,6 +187,10 @@ struct DstArrays {
     uint8_t* act;
 };
 
+// One state array at a time.  A stable sort by cell keeps every particle within a few
+// z-planes of its old place, so the sources that a stretch of destinations reads lie in a
+// window of the old order; one array's share of that window stays in L2 while the stretch
+// is written, all eight arrays' share does not.
 // A sorted key other than ncells belongs to an active particle, and on a mesh population
 // it is the particle's cell: only the particles keyed ncells (inactive, or outside the
 // mesh) read their flag and cell through the permutation.
@@ -194,15 +198,19 @@ template <typename T>
 __global__ void k_gather(PopView<T> P, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ key,
                          uint32_t ncells, DstArrays d) {
     const long long n = *P.n_in;
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
-        const uint32_t s = perm[j];
+    const long long j0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, js = (long long)gridDim.x * blockDim.x;
+    for (int q = 0; q < 8; ++q) {
+        const T* __restrict__ src = P.f[q];
+        T* __restrict__ dst = static_cast<T*>(d.f[q]);
+        for (long long j = j0; j < n; j += js) dst[j] = src[perm[j]];
+    }
+    for (long long j = j0; j < n; j += js) {
         const uint32_t k = key[j];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) static_cast<T*>(d.f[q])[j] = P.f[q][s];
         if (k != ncells) {
             if (d.cell) d.cell[j] = k;
             d.act[j] = 1;
         } else {
+            const uint32_t s = perm[j];
             if (d.cell) d.cell[j] = P.cell[s];
             d.act[j] = P.act[s];
         }
