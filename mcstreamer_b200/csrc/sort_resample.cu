@@ -95,11 +95,12 @@ __global__ void k_hist_entries(const long long* n_ptr, long long* out) {
 }
 
 // ---- radix pass: stable scatter.  Each warp takes a contiguous 32*SI-key share of the
-// tile and counts its keys per digit (warp match-any, the digit group's first lane adds);
-// a block prefix of those counts gives every key its place in the tile sorted by digit
-// (stable), where it is put in shared memory; the tile then goes out in that order, so that
-// consecutive threads write consecutive slots of each digit's run.  Four barriers per tile.
-__global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+// tile and counts its keys per digit (warp match-any, the digit group's first lane adds),
+// keeping each key's rank among the warp's keys of its digit; a block prefix of those
+// counts gives every key its place in the tile sorted by digit (stable), where it is put in
+// shared memory; the tile then goes out in that order, so that consecutive threads write
+// consecutive slots of each digit's run.  Four barriers per tile.
+__global__ void __launch_bounds__(SB, 4) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                 uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                 const long long* n_ptr, int shift, const uint32_t* __restrict__ offs) {
     constexpr int NW = SB / 32;
@@ -116,13 +117,19 @@ __global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin
         __syncthreads();
         const long long base = tile * STILE + (long long)wid * (32 * SI);
         uint32_t k[SI];
+        uint32_t rk[SI / 2];   // each key's rank among the warp's keys of its digit (< 32 SI), two per word
 #pragma unroll
         for (int r = 0; r < SI; ++r) {
             const long long i = base + (long long)r * 32 + lane;
             k[r] = i < n ? kin[i] : 0u;
             const uint32_t dg = i < n ? ((k[r] >> shift) & 0xffu) : 0x100u;
             const unsigned peers = __match_any_sync(0xffffffffu, dg);
-            if (dg < RADIX && (peers & lt) == 0) wc[wid][dg] += __popc(peers);
+            const uint32_t before = dg < RADIX ? wc[wid][dg] : 0u;
+            __syncwarp();
+            const uint32_t rank = before + __popc(peers & lt);
+            if (r & 1) rk[r >> 1] |= rank << 16;
+            else rk[r >> 1] = rank;
+            if (dg < RADIX && (peers & lt) == 0) wc[wid][dg] = before + __popc(peers);
             __syncwarp();
         }
         __syncthreads();
@@ -154,20 +161,16 @@ __global__ void __launch_bounds__(SB) k_scatter(const uint32_t* __restrict__ kin
             const long long rest = n - tile * STILE;
             cnt_tile = rest < STILE ? (uint32_t)rest : (uint32_t)STILE;
         }
+        // wc[wid][d] is now the warp's first place among the tile's keys of digit d
 #pragma unroll
         for (int r = 0; r < SI; ++r) {
             const long long i = base + (long long)r * 32 + lane;
-            const uint32_t dg = i < n ? ((k[r] >> shift) & 0xffu) : 0x100u;
-            const unsigned peers = __match_any_sync(0xffffffffu, dg);
-            uint32_t pos = 0;
-            if (dg < RADIX) pos = loc[dg] + wc[wid][dg] + __popc(peers & lt);
-            __syncwarp();
-            if (dg < RADIX) {
-                if ((peers & lt) == 0) wc[wid][dg] += __popc(peers);
+            if (i < n) {
+                const uint32_t dg = (k[r] >> shift) & 0xffu;
+                const uint32_t pos = loc[dg] + wc[wid][dg] + ((rk[r >> 1] >> (16 * (r & 1))) & 0xffffu);
                 skey[pos] = k[r];
                 sval[pos] = vin[i];
             }
-            __syncwarp();
         }
         __syncthreads();
         for (uint32_t j = threadIdx.x; j < cnt_tile; j += SB) {
