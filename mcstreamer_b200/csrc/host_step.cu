@@ -91,6 +91,8 @@ int ensure_host_step(mcs_pop* p, size_t in_bytes, size_t out_bytes, int nch) {
 }
 
 // Julia layout of m particles in one buffer: x (3m), v (3m), w (m), s (m), active (m bytes).
+constexpr long long kJuliaBytes = 8 * sizeof(double) + 1;   // one particle, 65 bytes
+constexpr long long kJuliaBytesNoW = kJuliaBytes - (long long)sizeof(double);
 struct JView {
     double *x, *v, *w, *s;
     uint8_t* a;
@@ -156,7 +158,7 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
         if (e == cudaSuccess) e = cudaMemcpyAsync(d.s, s + a, m * sizeof(double), cudaMemcpyHostToDevice, B.s_in);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d.a, active + a, (size_t)m, cudaMemcpyHostToDevice, B.s_in);
         if (e == cudaSuccess) e = cudaEventRecord(ev_in(k), B.s_in);
-        B.h2d += m * 65;
+        B.h2d += m * kJuliaBytes;
         return e == cudaSuccess ? MCS_OK : set_err(c, MCS_ERR_CUDA, cudaGetErrorString(e));
     };
     auto enqueue_comp = [&](int k) -> int {
@@ -209,7 +211,7 @@ MCS_API int mcs_advance_deposit_host(mcs_pop* p, const mcs_table* t, const mcs_f
                                                       cudaMemcpyDeviceToHost, B.s_out);
             if (e == cudaSuccess) e = cudaMemcpyAsync(active + q.dst, o.a + q.src, (size_t)q.cnt,
                                                       cudaMemcpyDeviceToHost, B.s_out);
-            B.d2h += q.cnt * (q.w ? 65 : 57);
+            B.d2h += q.cnt * (q.w ? kJuliaBytes : kJuliaBytesNoW);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ev_out(k), B.s_out);
         sec_total += nsec;
