@@ -99,7 +99,8 @@ __global__ void k_hist_entries(const long long* n_ptr, long long* out) {
 // keeping each key's rank among the warp's keys of its digit; a block prefix of those
 // counts gives every key its place in the tile sorted by digit (stable), where it is put in
 // shared memory; the tile then goes out in that order, so that consecutive threads write
-// consecutive slots of each digit's run.  Four barriers per tile.
+// consecutive slots of each digit's run.  Six barriers per tile.  At most 64 registers (4
+// blocks of 256 per SM, a few bytes spilled): the occupancy is worth more than the spill.
 __global__ void __launch_bounds__(SB, 4) k_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                 uint32_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                 const long long* n_ptr, int shift, const uint32_t* __restrict__ offs) {
