@@ -585,8 +585,8 @@ __device__ uint32_t merge_select_warp(const ResampleArgs& a, const PopView<T>& P
 
 // Counting is latency-bound over millions of small segments: a thread per segment keeps 32
 // segments' loads in flight per warp.
-// Only merging cells need the serial pass; their segments go to a worklist for the warp
-// kernel below.  A splitting cell (p < ntarget) clones its first ntarget - p particles with
+// Only merging cells need the weight sums and the clone positions; their segments go to a
+// worklist for the warp kernel below.  A splitting cell (p < ntarget) clones its first ntarget - p particles with
 // w > 2 (resample.jl:62-70); a cell with ntarget <= p <= nmax is left alone.
 template <typename T>
 __global__ void __launch_bounds__(128) k_resample_count(ResampleArgs a, PopView<T> P, uint32_t* __restrict__ counts,
